@@ -1,0 +1,221 @@
+/*
+ * strata_b200.h — C ABI of the B200 relational fixpoint engine.
+ *
+ * This is the drop-in boundary for the semi-naive fixpoint hot path of
+ * Strata/K.  Every entry point takes plain pointers and sizes; nothing here
+ * names a torch or Rust type.  A Rust crate binds it with `extern "C"`, Python
+ * with ctypes (see the `strata_b200` package).
+ *
+ * Conventions (shared by every call):
+ *   - Node / symbol ids are u32 (`SymbolId`, strata-ir/src/dict.rs:19).
+ *   - A binary relation crosses the boundary column-wise: `src[i], dst[i]`.
+ *   - A Trop weight crosses as `int64_t w[i]` plus an optional byte mask
+ *     `inf[i]` (1 = +inf, 0 = Finite(w[i])).  A NULL mask means all finite.
+ *     +inf is therefore distinct from every finite i64, matching
+ *     `Weight::{Finite(i64), PosInf}` (strata-ir/src/trop.rs:35-40).
+ *   - Inputs need not be sorted or deduplicated.  Outputs are sorted by
+ *     `(src, dst)` ascending, deduplicated (Bool) or min-merged (Trop), which
+ *     is `BTreeMap` order over `GroundVal::Sym` ids (strata-eval/src/store.rs:19).
+ *   - Results whose size is unknown in advance are returned in buffers the
+ *     library allocates with malloc; release them with `strata_free`.
+ *   - Every call runs on the context's stream and returns when its result is
+ *     complete.  A context must not be used by two threads at once; separate
+ *     contexts are independent (no process-global state).
+ *   - Errors are `strata_status` codes; `strata_last_error(ctx)` gives the
+ *     message.  The codes map 1:1 onto the reference's error variants:
+ *       STRATA_E_OVERFLOW   <- EvalError::Overflow      (strata-eval/src/naive.rs:31)
+ *       STRATA_E_NEG_CYCLE  <- EvalError::NegativeWeightCycle (naive.rs:45)
+ *       STRATA_E_CUDA       <- GpuError::Cuda           (strata-gpu/src/lib.rs:18)
+ *       STRATA_E_NOT_BUILT  <- GpuError::NotBuilt       (strata-gpu/src/lib.rs:16)
+ */
+#ifndef STRATA_B200_H
+#define STRATA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum strata_status {
+  STRATA_OK = 0,
+  STRATA_E_INVALID = 1,      /* bad argument (NULL pointer, size limit, bad id) */
+  STRATA_E_OOM = 2,          /* device allocation failed or context cap reached */
+  STRATA_E_CUDA = 3,         /* CUDA runtime error */
+  STRATA_E_OVERFLOW = 4,     /* Trop finite (x) overflowed i64 (checked add) */
+  STRATA_E_NEG_CYCLE = 5,    /* Trop stratum exceeded the Bellman-Ford round cap */
+  STRATA_E_TIMEOUT = 6,      /* a bounded device wait gave up (never a hang) */
+  STRATA_E_UNSUPPORTED = 7,  /* rule shape / size outside what the engine runs */
+  STRATA_E_NOT_BUILT = 8,    /* no CUDA device visible to this library */
+  STRATA_E_WEIGHT_RANGE = 9  /* a finite weight equal to INT64_MAX reached the
+                                device (its +inf encoding); never silently mixed */
+} strata_status;
+
+typedef struct strata_ctx strata_ctx;
+
+/* Per-fixpoint statistics filled by the drivers (all optional: pass NULL). */
+typedef struct strata_fix_stats {
+  uint64_t rounds;          /* semi-naive delta rounds executed (bootstrap excluded) */
+  uint64_t candidates;      /* join outputs summed over rounds */
+  uint64_t result_tuples;   /* |final IDB relation| */
+  uint64_t universe;        /* distinct ids in the EDB (Bellman-Ford cap basis) */
+  uint32_t key_bits;        /* significant bits of a packed tuple key */
+  uint32_t weight_bytes;    /* 0 (Bool), 4 (narrow Trop) or 8 (wide Trop) */
+  double   device_ms;       /* device time of the fixpoint (CUDA events) */
+  double   sort_ms, join_ms, diff_ms, merge_ms; /* per-phase device time */
+  uint64_t sort_bytes, join_bytes, diff_bytes, merge_bytes; /* algorithmic bytes */
+  uint32_t sort_launches, join_launches, diff_launches, merge_launches;
+  uint32_t other_launches;
+} strata_fix_stats;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Create a context on CUDA device `device`.  `mem_cap_bytes` bounds the bytes
+ * this context may hold on the device at once (0 = no cap).  Allocations past
+ * the cap fail with STRATA_E_OOM instead of reaching the driver. */
+strata_status strata_ctx_create(int device, uint64_t mem_cap_bytes, strata_ctx** out);
+void strata_ctx_destroy(strata_ctx* ctx);
+/* Use an existing cudaStream_t (passed as void*) for all work; NULL = own stream. */
+strata_status strata_ctx_set_stream(strata_ctx* ctx, void* stream);
+const char* strata_last_error(const strata_ctx* ctx);
+/* Device bytes currently held and the high-water mark. */
+strata_status strata_ctx_mem(const strata_ctx* ctx, uint64_t* in_use, uint64_t* peak);
+/* Enable per-phase CUDA-event timing in strata_fix_stats (adds event records). */
+strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled);
+/* Number of kernels this context launched so far (monotone counter). */
+uint64_t strata_ctx_launches(const strata_ctx* ctx);
+/* Release memory returned by the library. */
+void strata_free(void* p);
+const char* strata_version(void);
+
+/* ---- whole-fixpoint drivers (host buffers) ------------------------------
+ * These mirror strata-gpu's public functions (strata-gpu/src/lib.rs:67-147). */
+
+/* Bool transitive closure: path(X,Y) :- edge(X,Y). path(X,Z) :- edge(X,Y), path(Y,Z).
+ * Replaces `transitive_closure_bool(&[(u32,u32)])` (strata-gpu/src/lib.rs:67). */
+strata_status strata_transitive_closure_bool(strata_ctx* ctx,
+    const uint32_t* src, const uint32_t* dst, uint64_t n_edges,
+    uint32_t** out_src, uint32_t** out_dst, uint64_t* out_n,
+    strata_fix_stats* stats);
+
+/* Trop all-pairs: reach(X,Y) :- edge(X,Y). reach(X,Z) :- edge(X,Y), reach(Y,Z).
+ * Replaces `shortest_paths_trop(&[(u32,u32,i64)])` (strata-gpu/src/lib.rs:84).
+ * The Bellman-Ford cap is the interpreter's: universe + 2 delta rounds
+ * (strata-eval/src/seminaive.rs:96-103). */
+strata_status strata_shortest_paths_trop(strata_ctx* ctx,
+    const uint32_t* src, const uint32_t* dst, const int64_t* w, const uint8_t* inf,
+    uint64_t n_edges,
+    uint32_t** out_src, uint32_t** out_dst, int64_t** out_w, uint8_t** out_inf,
+    uint64_t* out_n, strata_fix_stats* stats);
+
+/* Trop multi-source: dist(S,Y) :- src(S), edge(S,Y). dist(S,Z) :- dist(S,Y), edge(Y,Z).
+ * `sources[i]` with weight `src_w[i]` (NULL = the otimes identity Finite(0), how a
+ * Bool fact enters Trop, strata-ir/src/trop.rs:44-45).  No reference GPU
+ * counterpart; it replaces `run_semi_naive` (strata-eval/src/seminaive.rs:29)
+ * for this rule shape. */
+strata_status strata_mssp_trop(strata_ctx* ctx,
+    const uint32_t* sources, const int64_t* src_w, const uint8_t* src_inf, uint64_t n_sources,
+    const uint32_t* esrc, const uint32_t* edst, const int64_t* ew, const uint8_t* einf,
+    uint64_t n_edges,
+    uint32_t** out_src, uint32_t** out_dst, int64_t** out_w, uint8_t** out_inf,
+    uint64_t* out_n, strata_fix_stats* stats);
+
+/* Triangles of the undirected graph on the edges (self-loops and duplicates
+ * ignored, both directions accepted).  Replaces `count_triangles`
+ * (strata-gpu/src/lib.rs:99, strata-gpu/src/wcoj.rs:136). */
+strata_status strata_count_triangles(strata_ctx* ctx,
+    const uint32_t* a, const uint32_t* b, uint64_t n_edges, uint64_t* out_count);
+
+/* 4-cliques of the undirected graph.  Replaces `count_4cliques`
+ * (strata-gpu/src/lib.rs:114, strata-gpu/src/wcoj.rs:166). */
+strata_status strata_count_4cliques(strata_ctx* ctx,
+    const uint32_t* a, const uint32_t* b, uint64_t n_edges, uint64_t* out_count);
+
+/* The count aggregate  n(count<X>) :- e(X,Y), e(Y,Z), e(X,Z)  over the directed
+ * relation e exactly as given (deduplicated as a set, no orientation).  This is
+ * `eval_aggregate_rule` + `fold_aggregate(Count)` for that body
+ * (strata-eval/src/naive.rs:300-391). */
+strata_status strata_count_triangle_pattern(strata_ctx* ctx,
+    const uint32_t* x, const uint32_t* y, uint64_t n_edges, uint64_t* out_count);
+
+/* Intern u64 term keys: ids[i] = rank of keys[i] among the distinct keys.
+ * Replaces `intern_terms` (strata-gpu/src/lib.rs:133, sort.rs:206). */
+strata_status strata_intern_terms(strata_ctx* ctx,
+    const uint64_t* keys, uint64_t n, uint32_t* ids_out, uint64_t* n_distinct);
+
+/* Σ_v d(v)^2 over the id-oriented simple graph: the binary-plan intermediate
+ * WCOJ avoids.  Replaces `binary_plan_intermediate` (strata-gpu/src/lib.rs:140). */
+strata_status strata_binary_plan_intermediate(strata_ctx* ctx,
+    const uint32_t* a, const uint32_t* b, uint64_t n_edges, uint64_t* out);
+
+/* ---- device-resident drivers ---------------------------------------------
+ * Same fixpoints with inputs already in device memory (pointers from
+ * cudaMalloc / torch).  The result stays on the device in a relation handle. */
+
+typedef struct strata_rel strata_rel;
+
+strata_status strata_tc_bool_dev(strata_ctx* ctx,
+    const uint32_t* d_src, const uint32_t* d_dst, uint64_t n_edges,
+    strata_rel** out, strata_fix_stats* stats);
+strata_status strata_trop_paths_dev(strata_ctx* ctx,
+    const uint32_t* d_src, const uint32_t* d_dst, const int64_t* d_w, const uint8_t* d_inf,
+    uint64_t n_edges, strata_rel** out, strata_fix_stats* stats);
+strata_status strata_mssp_trop_dev(strata_ctx* ctx,
+    const uint32_t* d_sources, const int64_t* d_src_w, const uint8_t* d_src_inf, uint64_t n_sources,
+    const uint32_t* d_esrc, const uint32_t* d_edst, const int64_t* d_ew, const uint8_t* d_einf,
+    uint64_t n_edges, strata_rel** out, strata_fix_stats* stats);
+strata_status strata_count_triangle_pattern_dev(strata_ctx* ctx,
+    const uint32_t* d_x, const uint32_t* d_y, uint64_t n_edges, uint64_t* out_count);
+
+/* Relation handle accessors. */
+strata_status strata_rel_size(const strata_rel* rel, uint64_t* n);
+strata_status strata_rel_is_trop(const strata_rel* rel, int* is_trop);
+/* Copy out into caller buffers of strata_rel_size() entries; w / inf may be
+ * NULL (ignored for Bool relations). */
+strata_status strata_rel_to_host(strata_ctx* ctx, const strata_rel* rel,
+    uint32_t* src, uint32_t* dst, int64_t* w, uint8_t* inf);
+/* Order-independent 64-bit fingerprint of the relation's tuples (and
+ * weights), for parity checks that must not copy the relation out. */
+strata_status strata_rel_fingerprint(strata_ctx* ctx, const strata_rel* rel, uint64_t* fp);
+void strata_rel_free(strata_ctx* ctx, strata_rel* rel);
+
+/* ---- operator surface (device pointers) ----------------------------------
+ * The interpreter's operators (strata-eval/src/seminaive.rs:114-298,
+ * store.rs:34-48) on packed sorted key columns.  A packed key is
+ * (c0 << shift) | c1 in a u32 (key_bytes = 4) or u64 (key_bytes = 8).
+ * `n` is limited to 2^30 - 1 per call. */
+
+/* Stable LSD radix sort of keys (and optional 4- or 8-byte values) on the low
+ * `key_bits` bits.  Sorted output goes to keys_out / vals_out; the inputs are
+ * left unchanged. */
+strata_status strata_op_sort(strata_ctx* ctx, int key_bytes, int val_bytes,
+    const void* d_keys_in, const void* d_vals_in, void* d_keys_out, void* d_vals_out,
+    uint64_t n, int key_bits);
+
+/* Bool dedup + difference (Δ = new \ full, seminaive.rs:192-209): from sorted
+ * keys with duplicates, write the distinct keys absent from sorted unique
+ * `full` to `out` (capacity n); *out_n receives the count.  full may be empty. */
+strata_status strata_op_dedup_diff(strata_ctx* ctx, int key_bytes,
+    const void* d_cand, uint64_t n, const void* d_full, uint64_t n_full,
+    void* d_out, uint64_t* out_n);
+
+/* Trop min-merge + improvement (Relation::combine, store.rs:34-48): from sorted
+ * keys with int64 weights (INT64_MAX = +inf), reduce each key to its minimum;
+ * keys new to `full` or strictly better than full's weight go to out_keys/out_w.
+ * Strictly-better weights are also written into d_full_w in place. */
+strata_status strata_op_min_improve(strata_ctx* ctx, int key_bytes,
+    const void* d_cand, const int64_t* d_cand_w, uint64_t n,
+    const void* d_full, int64_t* d_full_w, uint64_t n_full,
+    void* d_out_keys, int64_t* d_out_w, uint64_t* out_n);
+
+/* Merge two sorted, disjoint key runs (with optional int64 weights) into out. */
+strata_status strata_op_merge(strata_ctx* ctx, int key_bytes,
+    const void* d_a, const int64_t* d_aw, uint64_t na,
+    const void* d_b, const int64_t* d_bw, uint64_t nb,
+    void* d_out, int64_t* d_out_w);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STRATA_B200_H */

@@ -1,0 +1,488 @@
+// sk_capi.cu — the extern "C" boundary declared in include/strata_b200.h.
+//
+// Every entry point validates its arguments, runs inside a try block that
+// turns SkError into a status code (message kept in the context), and leaves
+// no device work in flight when it returns.
+#include "sk_ops.cuh"
+#include "sk_rel.cuh"
+
+#include <cstdlib>
+#include <new>
+
+using sk::DBuf;
+using sk::SkError;
+
+namespace {
+
+#define SK_GUARD_BEGIN try {
+#define SK_GUARD_END(ctx)                                                  \
+  }                                                                        \
+  catch (const SkError& err) {                                             \
+    if (ctx) (ctx)->last_error = err.msg;                                  \
+    cudaGetLastError();                                                    \
+    return err.code;                                                       \
+  }                                                                        \
+  catch (const std::bad_alloc&) {                                          \
+    if (ctx) (ctx)->last_error = "host allocation failed";                 \
+    return STRATA_E_OOM;                                                   \
+  }                                                                        \
+  catch (...) {                                                            \
+    if (ctx) (ctx)->last_error = "unexpected exception";                   \
+    return STRATA_E_CUDA;                                                  \
+  }                                                                        \
+  return STRATA_OK;
+
+strata_status bad(strata_ctx* ctx, const char* msg) {
+  if (ctx) ctx->last_error = msg;
+  return STRATA_E_INVALID;
+}
+
+template <class T>
+T* host_alloc(uint64_t n) {
+  void* p = std::malloc(n ? n * sizeof(T) : 1);
+  if (!p) throw std::bad_alloc();
+  return static_cast<T*>(p);
+}
+
+// Copy a host column to a fresh device buffer.
+template <class T>
+DBuf<T> to_dev(strata_ctx* ctx, const T* h, uint64_t n) {
+  DBuf<T> d(ctx, n + 1);
+  if (n && h) SK_CUDA(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  return d;
+}
+
+strata_status set_device(strata_ctx* ctx) {
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) {
+    ctx->last_error = cudaGetErrorString(e);
+    return STRATA_E_CUDA;
+  }
+  return STRATA_OK;
+}
+
+// Copy a result relation out into malloc'd host columns.
+strata_status rel_out(strata_ctx* ctx, strata_rel* rel, uint32_t** os, uint32_t** od, int64_t** ow,
+                      uint8_t** oi, uint64_t* on) {
+  uint32_t* s = host_alloc<uint32_t>(rel->n);
+  uint32_t* d = host_alloc<uint32_t>(rel->n);
+  int64_t* w = ow ? host_alloc<int64_t>(rel->n) : nullptr;
+  uint8_t* i = oi ? host_alloc<uint8_t>(rel->n) : nullptr;
+  try {
+    sk::rel_to_host(ctx, rel, s, d, w, i);
+  } catch (...) {
+    std::free(s); std::free(d); std::free(w); std::free(i);
+    throw;
+  }
+  *os = s;
+  *od = d;
+  if (ow) *ow = w;
+  if (oi) *oi = i;
+  *on = rel->n;
+  return STRATA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* strata_version(void) { return "strata-b200 0.1.0 (sm_100a)"; }
+
+strata_status strata_ctx_create(int device, uint64_t mem_cap_bytes, strata_ctx** out) {
+  if (!out) return STRATA_E_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return STRATA_E_NOT_BUILT;
+  }
+  if (device < 0 || device >= count) return STRATA_E_INVALID;
+  strata_ctx* ctx = new (std::nothrow) strata_ctx();
+  if (!ctx) return STRATA_E_OOM;
+  ctx->device = device;
+  ctx->cap = mem_cap_bytes;
+  SK_GUARD_BEGIN
+  SK_CUDA(cudaSetDevice(device));
+  SK_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  ctx->own_stream = true;
+  SK_CUDA(cudaMalloc(&ctx->d_status, 256));
+  SK_CUDA(cudaMemset(ctx->d_status, 0, 256));
+  SK_CUDA(cudaMallocHost(&ctx->h_status, 64));
+  SK_CUDA(cudaMallocHost(&ctx->h_scalar, 8 * sizeof(uint64_t)));
+  SK_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+  *out = ctx;
+  }
+  catch (const SkError& err) {
+    cudaGetLastError();
+    strata_ctx_destroy(ctx);
+    return err.code;
+  }
+  return STRATA_OK;
+}
+
+void strata_ctx_destroy(strata_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->sizes) cudaFreeAsync(kv.first, ctx->stream);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->h_status) cudaFreeHost(ctx->h_status);
+  if (ctx->h_scalar) cudaFreeHost(ctx->h_scalar);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+strata_status strata_ctx_set_stream(strata_ctx* ctx, void* stream) {
+  if (!ctx) return STRATA_E_INVALID;
+  SK_GUARD_BEGIN
+  SK_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (stream) {
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    ctx->stream = static_cast<cudaStream_t>(stream);
+    ctx->own_stream = false;
+  } else if (!ctx->own_stream) {
+    SK_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->own_stream = true;
+  }
+  SK_GUARD_END(ctx)
+}
+
+const char* strata_last_error(const strata_ctx* ctx) {
+  return ctx ? ctx->last_error.c_str() : "no context";
+}
+
+strata_status strata_ctx_mem(const strata_ctx* ctx, uint64_t* in_use, uint64_t* peak) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (in_use) *in_use = ctx->in_use;
+  if (peak) *peak = ctx->peak;
+  return STRATA_OK;
+}
+
+strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled) {
+  if (!ctx) return STRATA_E_INVALID;
+  ctx->profiling = enabled != 0;
+  return STRATA_OK;
+}
+
+uint64_t strata_ctx_launches(const strata_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+void strata_free(void* p) { std::free(p); }
+
+// ---- host-buffer drivers ---------------------------------------------------------
+
+strata_status strata_transitive_closure_bool(strata_ctx* ctx, const uint32_t* src, const uint32_t* dst,
+                                             uint64_t n, uint32_t** out_src, uint32_t** out_dst,
+                                             uint64_t* out_n, strata_fix_stats* stats) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out_src || !out_dst || !out_n || (n && (!src || !dst))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  DBuf<uint32_t> ds = to_dev(ctx, src, n), dd = to_dev(ctx, dst, n);
+  sk::EdgeCols e;
+  e.src = ds.p; e.dst = dd.p; e.n = n;
+  strata_rel* rel = sk::fix_tc_bool(ctx, e, stats);
+  try {
+    rel_out(ctx, rel, out_src, out_dst, nullptr, nullptr, out_n);
+  } catch (...) {
+    sk::rel_free(ctx, rel);
+    throw;
+  }
+  sk::rel_free(ctx, rel);
+  SK_CUDA(cudaStreamSynchronize(ctx->stream));
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_shortest_paths_trop(strata_ctx* ctx, const uint32_t* src, const uint32_t* dst,
+                                         const int64_t* w, const uint8_t* inf, uint64_t n,
+                                         uint32_t** out_src, uint32_t** out_dst, int64_t** out_w,
+                                         uint8_t** out_inf, uint64_t* out_n, strata_fix_stats* stats) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out_src || !out_dst || !out_w || !out_inf || !out_n || (n && (!src || !dst || !w)))
+    return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  DBuf<uint32_t> ds = to_dev(ctx, src, n), dd = to_dev(ctx, dst, n);
+  DBuf<int64_t> dw = to_dev(ctx, w, n);
+  DBuf<uint8_t> di;
+  di.ctx = ctx;
+  if (inf) di = to_dev(ctx, inf, n);
+  sk::EdgeCols e;
+  e.src = ds.p; e.dst = dd.p; e.w = dw.p; e.inf = inf ? di.p : nullptr; e.n = n;
+  strata_rel* rel = sk::fix_trop_paths(ctx, e, stats);
+  try {
+    rel_out(ctx, rel, out_src, out_dst, out_w, out_inf, out_n);
+  } catch (...) {
+    sk::rel_free(ctx, rel);
+    throw;
+  }
+  sk::rel_free(ctx, rel);
+  SK_CUDA(cudaStreamSynchronize(ctx->stream));
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_mssp_trop(strata_ctx* ctx, const uint32_t* sources, const int64_t* src_w,
+                               const uint8_t* src_inf, uint64_t ns, const uint32_t* esrc,
+                               const uint32_t* edst, const int64_t* ew, const uint8_t* einf,
+                               uint64_t ne, uint32_t** out_src, uint32_t** out_dst, int64_t** out_w,
+                               uint8_t** out_inf, uint64_t* out_n, strata_fix_stats* stats) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out_src || !out_dst || !out_w || !out_inf || !out_n || (ns && !sources) ||
+      (ne && (!esrc || !edst || !ew)))
+    return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  DBuf<uint32_t> dsrc = to_dev(ctx, sources, ns);
+  DBuf<int64_t> dsw;
+  DBuf<uint8_t> dsi, dei;
+  dsw.ctx = dsi.ctx = dei.ctx = ctx;
+  if (src_w) dsw = to_dev(ctx, src_w, ns);
+  if (src_inf) dsi = to_dev(ctx, src_inf, ns);
+  DBuf<uint32_t> ds = to_dev(ctx, esrc, ne), dd = to_dev(ctx, edst, ne);
+  DBuf<int64_t> dw = to_dev(ctx, ew, ne);
+  if (einf) dei = to_dev(ctx, einf, ne);
+  sk::EdgeCols e;
+  e.src = ds.p; e.dst = dd.p; e.w = dw.p; e.inf = einf ? dei.p : nullptr; e.n = ne;
+  strata_rel* rel = sk::fix_mssp(ctx, dsrc.p, src_w ? dsw.p : nullptr, src_inf ? dsi.p : nullptr, ns, e, stats);
+  try {
+    rel_out(ctx, rel, out_src, out_dst, out_w, out_inf, out_n);
+  } catch (...) {
+    sk::rel_free(ctx, rel);
+    throw;
+  }
+  sk::rel_free(ctx, rel);
+  SK_CUDA(cudaStreamSynchronize(ctx->stream));
+  SK_GUARD_END(ctx)
+}
+
+#define SK_COUNT_ENTRY(NAME, FN)                                                            \
+  strata_status NAME(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n,     \
+                     uint64_t* out) {                                                       \
+    if (!ctx) return STRATA_E_INVALID;                                                      \
+    if (!out || (n && (!a || !b))) return bad(ctx, "NULL argument");                        \
+    if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;                                 \
+    SK_GUARD_BEGIN                                                                          \
+    DBuf<uint32_t> da = to_dev(ctx, a, n), db = to_dev(ctx, b, n);                          \
+    *out = FN(ctx, da.p, db.p, n);                                                          \
+    SK_CUDA(cudaStreamSynchronize(ctx->stream));                                            \
+    SK_GUARD_END(ctx)                                                                       \
+  }
+
+SK_COUNT_ENTRY(strata_count_triangles, sk::count_triangles_undirected)
+SK_COUNT_ENTRY(strata_count_4cliques, sk::count_4cliques_undirected)
+SK_COUNT_ENTRY(strata_count_triangle_pattern, sk::count_triangle_pattern)
+SK_COUNT_ENTRY(strata_binary_plan_intermediate, sk::binary_plan_intermediate)
+#undef SK_COUNT_ENTRY
+
+strata_status strata_intern_terms(strata_ctx* ctx, const uint64_t* keys, uint64_t n, uint32_t* ids_out,
+                                  uint64_t* n_distinct) {
+  if (!ctx) return STRATA_E_INVALID;
+  if ((n && (!keys || !ids_out))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  DBuf<uint64_t> dk = to_dev(ctx, keys, n);
+  DBuf<uint32_t> di(ctx, n + 1);
+  const uint64_t m = sk::intern_terms(ctx, dk.p, n, di.p);
+  if (n) SK_CUDA(cudaMemcpyAsync(ids_out, di.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  SK_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (n_distinct) *n_distinct = m;
+  SK_GUARD_END(ctx)
+}
+
+// ---- device-resident drivers ------------------------------------------------------
+
+strata_status strata_tc_bool_dev(strata_ctx* ctx, const uint32_t* d_src, const uint32_t* d_dst, uint64_t n,
+                                 strata_rel** out, strata_fix_stats* stats) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out || (n && (!d_src || !d_dst))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::EdgeCols e;
+  e.src = d_src; e.dst = d_dst; e.n = n;
+  *out = sk::fix_tc_bool(ctx, e, stats);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_trop_paths_dev(strata_ctx* ctx, const uint32_t* d_src, const uint32_t* d_dst,
+                                    const int64_t* d_w, const uint8_t* d_inf, uint64_t n, strata_rel** out,
+                                    strata_fix_stats* stats) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out || (n && (!d_src || !d_dst || !d_w))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::EdgeCols e;
+  e.src = d_src; e.dst = d_dst; e.w = d_w; e.inf = d_inf; e.n = n;
+  *out = sk::fix_trop_paths(ctx, e, stats);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_mssp_trop_dev(strata_ctx* ctx, const uint32_t* d_sources, const int64_t* d_src_w,
+                                   const uint8_t* d_src_inf, uint64_t ns, const uint32_t* d_esrc,
+                                   const uint32_t* d_edst, const int64_t* d_ew, const uint8_t* d_einf,
+                                   uint64_t ne, strata_rel** out, strata_fix_stats* stats) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out || (ns && !d_sources) || (ne && (!d_esrc || !d_edst || !d_ew))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::EdgeCols e;
+  e.src = d_esrc; e.dst = d_edst; e.w = d_ew; e.inf = d_einf; e.n = ne;
+  *out = sk::fix_mssp(ctx, d_sources, d_src_w, d_src_inf, ns, e, stats);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_count_triangle_pattern_dev(strata_ctx* ctx, const uint32_t* d_x, const uint32_t* d_y,
+                                                uint64_t n, uint64_t* out_count) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out_count || (n && (!d_x || !d_y))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  *out_count = sk::count_triangle_pattern(ctx, d_x, d_y, n);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_rel_size(const strata_rel* rel, uint64_t* n) {
+  if (!rel || !n) return STRATA_E_INVALID;
+  *n = rel->n;
+  return STRATA_OK;
+}
+
+strata_status strata_rel_is_trop(const strata_rel* rel, int* is_trop) {
+  if (!rel || !is_trop) return STRATA_E_INVALID;
+  *is_trop = rel->trop ? 1 : 0;
+  return STRATA_OK;
+}
+
+strata_status strata_rel_to_host(strata_ctx* ctx, const strata_rel* rel, uint32_t* src, uint32_t* dst,
+                                 int64_t* w, uint8_t* inf) {
+  if (!ctx || !rel) return STRATA_E_INVALID;
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::rel_to_host(ctx, rel, src, dst, w, inf);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_rel_fingerprint(strata_ctx* ctx, const strata_rel* rel, uint64_t* fp) {
+  if (!ctx || !rel || !fp) return STRATA_E_INVALID;
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  *fp = sk::rel_fingerprint(ctx, rel);
+  SK_GUARD_END(ctx)
+}
+
+void strata_rel_free(strata_ctx* ctx, strata_rel* rel) {
+  if (ctx) cudaSetDevice(ctx->device);
+  sk::rel_free(ctx, rel);
+}
+
+// ---- operator surface ---------------------------------------------------------------
+
+strata_status strata_op_sort(strata_ctx* ctx, int key_bytes, int val_bytes, const void* d_keys_in,
+                             const void* d_vals_in, void* d_keys_out, void* d_vals_out, uint64_t n,
+                             int key_bits) {
+  if (!ctx) return STRATA_E_INVALID;
+  if ((key_bytes != 4 && key_bytes != 8) || (val_bytes != 0 && val_bytes != 4 && val_bytes != 8))
+    return bad(ctx, "key_bytes must be 4 or 8, val_bytes 0, 4 or 8");
+  if (n && (!d_keys_in || !d_keys_out || (val_bytes && (!d_vals_in || !d_vals_out))))
+    return bad(ctx, "NULL argument");
+  if (key_bits < 0 || key_bits > 8 * key_bytes) return bad(ctx, "key_bits out of range");
+  if (n > sk::kMaxSortN) return bad(ctx, "n exceeds 2^30-1");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  if (n == 0) return STRATA_OK;
+  // Copy the inputs into the output buffers, sort between output and scratch.
+  SK_CUDA(cudaMemcpyAsync(d_keys_out, d_keys_in, n * key_bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (val_bytes)
+    SK_CUDA(cudaMemcpyAsync(d_vals_out, d_vals_in, n * val_bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  auto run = [&](auto kt, auto vt) {
+    using K = decltype(kt);
+    using V = decltype(vt);
+    DBuf<K> ka(ctx, n);
+    DBuf<V> va;
+    va.ctx = ctx;
+    if (val_bytes) va.reserve(n);
+    K* kp = static_cast<K*>(d_keys_out);
+    K* kalt = ka.p;
+    V* vp = static_cast<V*>(d_vals_out);
+    V* valt = va.p;
+    sk::radix_sort<K, V>(ctx, &kp, &kalt, &vp, &valt, val_bytes != 0, n, key_bits, true);
+    if (kp != d_keys_out) {
+      SK_CUDA(cudaMemcpyAsync(d_keys_out, kp, n * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
+      if (val_bytes) SK_CUDA(cudaMemcpyAsync(d_vals_out, vp, n * sizeof(V), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    sk::sync_and_check(ctx);
+  };
+  if (key_bytes == 4) {
+    if (val_bytes == 8) run(uint32_t(), uint64_t()); else run(uint32_t(), uint32_t());
+  } else {
+    if (val_bytes == 8) run(uint64_t(), uint64_t()); else run(uint64_t(), uint32_t());
+  }
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_op_dedup_diff(strata_ctx* ctx, int key_bytes, const void* d_cand, uint64_t n,
+                                   const void* d_full, uint64_t n_full, void* d_out, uint64_t* out_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  if (!out_n || (n && (!d_cand || !d_out)) || (n_full && !d_full)) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  DBuf<uint64_t> cnt(ctx, 1);
+  if (key_bytes == 4)
+    sk::diff_improve<uint32_t, int32_t, false>(ctx, (const uint32_t*)d_cand, nullptr, n, (const uint32_t*)d_full,
+                                               nullptr, n_full, (uint32_t*)d_out, nullptr, cnt.p);
+  else
+    sk::diff_improve<uint64_t, int32_t, false>(ctx, (const uint64_t*)d_cand, nullptr, n, (const uint64_t*)d_full,
+                                               nullptr, n_full, (uint64_t*)d_out, nullptr, cnt.p);
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, cnt.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  sk::sync_and_check(ctx);
+  *out_n = ctx->h_scalar[0];
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_op_min_improve(strata_ctx* ctx, int key_bytes, const void* d_cand, const int64_t* d_cand_w,
+                                    uint64_t n, const void* d_full, int64_t* d_full_w, uint64_t n_full,
+                                    void* d_out_keys, int64_t* d_out_w, uint64_t* out_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  if (!out_n || (n && (!d_cand || !d_cand_w || !d_out_keys || !d_out_w)) || (n_full && (!d_full || !d_full_w)))
+    return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  DBuf<uint64_t> cnt(ctx, 1);
+  if (key_bytes == 4)
+    sk::diff_improve<uint32_t, int64_t, true>(ctx, (const uint32_t*)d_cand, d_cand_w, n, (const uint32_t*)d_full,
+                                              d_full_w, n_full, (uint32_t*)d_out_keys, d_out_w, cnt.p);
+  else
+    sk::diff_improve<uint64_t, int64_t, true>(ctx, (const uint64_t*)d_cand, d_cand_w, n, (const uint64_t*)d_full,
+                                              d_full_w, n_full, (uint64_t*)d_out_keys, d_out_w, cnt.p);
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, cnt.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  sk::sync_and_check(ctx);
+  *out_n = ctx->h_scalar[0];
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_op_merge(strata_ctx* ctx, int key_bytes, const void* d_a, const int64_t* d_aw, uint64_t na,
+                              const void* d_b, const int64_t* d_bw, uint64_t nb, void* d_out, int64_t* d_out_w) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  const bool trop = d_aw || d_bw || d_out_w;
+  if ((na && !d_a) || (nb && !d_b) || ((na || nb) && !d_out)) return bad(ctx, "NULL argument");
+  if (trop && ((na && !d_aw) || (nb && !d_bw) || !d_out_w)) return bad(ctx, "weights must be given for all or none");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  if (key_bytes == 4) {
+    if (trop) sk::merge_disjoint<uint32_t, int64_t, true>(ctx, (const uint32_t*)d_a, d_aw, na, (const uint32_t*)d_b, d_bw, nb, (uint32_t*)d_out, d_out_w);
+    else sk::merge_disjoint<uint32_t, int32_t, false>(ctx, (const uint32_t*)d_a, nullptr, na, (const uint32_t*)d_b, nullptr, nb, (uint32_t*)d_out, nullptr);
+  } else {
+    if (trop) sk::merge_disjoint<uint64_t, int64_t, true>(ctx, (const uint64_t*)d_a, d_aw, na, (const uint64_t*)d_b, d_bw, nb, (uint64_t*)d_out, d_out_w);
+    else sk::merge_disjoint<uint64_t, int32_t, false>(ctx, (const uint64_t*)d_a, nullptr, na, (const uint64_t*)d_b, nullptr, nb, (uint64_t*)d_out, nullptr);
+  }
+  sk::sync_and_check(ctx);
+  SK_GUARD_END(ctx)
+}
+
+}  // extern "C"

@@ -1,0 +1,249 @@
+// sk_common.cuh — context, device memory, error and status plumbing shared by
+// every translation unit of the engine.
+//
+// Errors inside the library are C++ exceptions (SkError) carrying a
+// strata_status; every extern "C" entry point catches them and returns the
+// code, storing the message in the context.  Device-side conditions (Trop
+// overflow, a sentinel collision, a look-back wait that gave up) are bits in a
+// per-context status word that kernels OR into and the host reads at each
+// round boundary.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+#include "../../include/strata_b200.h"
+
+namespace sk {
+
+// ---- device status bits -----------------------------------------------------
+enum : uint32_t {
+  ST_OVERFLOW = 1u,          // finite Trop (x) overflowed int64
+  ST_SENTINEL = 2u,          // a finite sum landed on the +inf encoding
+  ST_LOOKBACK_TIMEOUT = 4u,  // decoupled look-back wait hit its iteration cap
+  ST_BOUNDS = 8u,            // an index failed a bounds check and was skipped
+};
+
+// Iteration cap of every spin-wait in device code.  A wait that reaches it
+// records ST_LOOKBACK_TIMEOUT and proceeds; the host turns that into
+// STRATA_E_TIMEOUT.  Tiles are claimed in launch order, so a predecessor is
+// always resident or finished and the cap is never reached in a correct run.
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+struct SkError {
+  strata_status code;
+  std::string msg;
+};
+
+[[noreturn]] inline void fail(strata_status code, const std::string& msg) {
+  throw SkError{code, msg};
+}
+
+inline void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    fail(e == cudaErrorMemoryAllocation ? STRATA_E_OOM : STRATA_E_CUDA,
+         std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+#define SK_CUDA(call) ::sk::check_cuda((call), #call)
+
+struct PhaseTimer;
+
+}  // namespace sk
+
+// The context: one device, one stream, a capped byte budget, a status word.
+struct strata_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  uint64_t cap = 0;
+  uint64_t in_use = 0;
+  uint64_t peak = 0;
+  std::unordered_map<void*, uint64_t> sizes;
+  std::string last_error;
+  uint32_t* d_status = nullptr;     // device status word
+  uint32_t* h_status = nullptr;     // pinned mirror
+  uint64_t* h_scalar = nullptr;     // pinned scratch for small D2H reads (8 slots)
+  int num_sms = 148;
+  bool profiling = false;
+  uint64_t launches = 0;
+};
+
+namespace sk {
+
+// ---- allocation -------------------------------------------------------------
+
+inline void* dev_alloc(strata_ctx* ctx, uint64_t bytes) {
+  if (bytes == 0) bytes = 16;
+  bytes = (bytes + 255) & ~uint64_t(255);
+  if (ctx->cap && ctx->in_use + bytes > ctx->cap) {
+    fail(STRATA_E_OOM, "device memory cap reached: need " + std::to_string(bytes) +
+                           " B with " + std::to_string(ctx->in_use) + " of " +
+                           std::to_string(ctx->cap) + " B held");
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(STRATA_E_OOM, std::string("cudaMallocAsync(") + std::to_string(bytes) +
+                           "): " + cudaGetErrorString(e));
+  }
+  ctx->sizes[p] = bytes;
+  ctx->in_use += bytes;
+  if (ctx->in_use > ctx->peak) ctx->peak = ctx->in_use;
+  return p;
+}
+
+inline void dev_free(strata_ctx* ctx, void* p) {
+  if (!p) return;
+  auto it = ctx->sizes.find(p);
+  if (it != ctx->sizes.end()) {
+    ctx->in_use -= it->second;
+    ctx->sizes.erase(it);
+  }
+  cudaFreeAsync(p, ctx->stream);
+}
+
+// Owning device buffer (RAII, stream-ordered free).
+template <class T>
+struct DBuf {
+  strata_ctx* ctx = nullptr;
+  T* p = nullptr;
+  uint64_t cap = 0;  // elements
+  DBuf() = default;
+  DBuf(strata_ctx* c, uint64_t n) : ctx(c) { reserve(n); }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : ctx(o.ctx), p(o.p), cap(o.cap) { o.p = nullptr; o.cap = 0; }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      ctx = o.ctx; p = o.p; cap = o.cap;
+      o.p = nullptr; o.cap = 0;
+    }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void release() {
+    if (p && ctx) dev_free(ctx, p);
+    p = nullptr;
+    cap = 0;
+  }
+  // Ensure capacity for n elements (contents not preserved when it grows).
+  void reserve(uint64_t n) {
+    if (n <= cap && p) return;
+    release();
+    uint64_t want = n < 64 ? 64 : n;
+    p = static_cast<T*>(dev_alloc(ctx, want * sizeof(T)));
+    cap = want;
+  }
+  // Grow geometrically (for per-round buffers that are reused).
+  void reserve_grow(uint64_t n) {
+    if (n <= cap && p) return;
+    uint64_t want = cap ? cap : 64;
+    while (want < n) want += want / 2 + 64;
+    reserve(want);
+  }
+  // Give up ownership (the caller frees with dev_free).
+  T* detach() {
+    T* r = p;
+    p = nullptr;
+    cap = 0;
+    return r;
+  }
+  void swap(DBuf& o) {
+    std::swap(ctx, o.ctx);
+    std::swap(p, o.p);
+    std::swap(cap, o.cap);
+  }
+};
+
+// ---- status word ------------------------------------------------------------
+
+inline void reset_status(strata_ctx* ctx) {
+  SK_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
+}
+
+// Synchronize and read the status word; throws on any device-side condition.
+inline void sync_and_check(strata_ctx* ctx) {
+  SK_CUDA(cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  SK_CUDA(cudaStreamSynchronize(ctx->stream));
+  SK_CUDA(cudaGetLastError());
+  uint32_t s = *ctx->h_status;
+  if (s & ST_LOOKBACK_TIMEOUT) fail(STRATA_E_TIMEOUT, "a device look-back wait reached its cap");
+  if (s & ST_BOUNDS) fail(STRATA_E_CUDA, "a device bounds check failed (index skipped)");
+  if (s & ST_OVERFLOW) fail(STRATA_E_OVERFLOW, "tropical weight overflow: a finite sum exceeds i64");
+  if (s & ST_SENTINEL)
+    fail(STRATA_E_WEIGHT_RANGE,
+         "a finite tropical weight equal to i64::MAX cannot be told from +inf on the device");
+}
+
+// Read `count` u64 values from device memory (synchronizing).
+inline void read_u64(strata_ctx* ctx, const uint64_t* d, uint64_t* out, int count) {
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, d, sizeof(uint64_t) * count,
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  SK_CUDA(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(out, ctx->h_scalar, sizeof(uint64_t) * count);
+}
+
+inline void after_launch(strata_ctx* ctx, const char* name) {
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) fail(STRATA_E_CUDA, std::string("launch ") + name + ": " + cudaGetErrorString(e));
+}
+
+inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+inline int bits_for(uint64_t max_value) {  // bits needed to hold 0..max_value
+  int b = 0;
+  while (b < 64 && (max_value >> b) != 0) b++;
+  return b;
+}
+
+// ---- phase timing -------------------------------------------------------------
+// Records a pair of events around a phase when profiling is on and adds the
+// elapsed time once the fixpoint has synchronized.
+struct PhaseTimer {
+  strata_ctx* ctx;
+  struct Rec { cudaEvent_t a, b; double* acc; };
+  std::vector<Rec> recs;
+  int n = 0;
+  explicit PhaseTimer(strata_ctx* c) : ctx(c) { recs.resize(4096); }
+  ~PhaseTimer() {
+    for (int i = 0; i < n; i++) { cudaEventDestroy(recs[i].a); cudaEventDestroy(recs[i].b); }
+  }
+  int begin(double* acc) {
+    if (!ctx->profiling || n >= (int)recs.size()) return -1;
+    Rec& r = recs[n];
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    r.acc = acc;
+    cudaEventRecord(r.a, ctx->stream);
+    return n++;
+  }
+  void end(int id) {
+    if (id < 0) return;
+    cudaEventRecord(recs[id].b, ctx->stream);
+  }
+  void collect() {
+    for (int i = 0; i < n; i++) {
+      float ms = 0;
+      if (cudaEventSynchronize(recs[i].b) == cudaSuccess &&
+          cudaEventElapsedTime(&ms, recs[i].a, recs[i].b) == cudaSuccess)
+        *recs[i].acc += ms;
+      cudaEventDestroy(recs[i].a);
+      cudaEventDestroy(recs[i].b);
+    }
+    n = 0;
+  }
+};
+
+}  // namespace sk

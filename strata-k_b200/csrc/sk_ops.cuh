@@ -1,0 +1,98 @@
+// sk_ops.cuh — host-side entry points of the device operators.  Each function
+// launches its kernels on ctx->stream; none synchronizes unless it says so.
+#pragma once
+
+#include <stdint.h>
+
+#include "sk_common.cuh"
+
+namespace sk {
+
+// Radix sort limit per call (the onesweep look-back words carry 30-bit counts).
+constexpr uint64_t kMaxSortN = (1ull << 30) - 1;
+
+// Stable LSD radix sort (onesweep) of `n` keys on their low `bits` bits, with
+// optional values (V = uint32_t or uint64_t; has_vals selects them).  keys/alt
+// (and vals/valt) are a double buffer: on return `*keys` (and `*vals`) point at
+// the sorted data and `*alt` at the scratch half.  When `skip_trivial` is set
+// the global digit histogram is read back (one synchronization) and passes
+// whose digit is constant are skipped.
+template <class K, class V>
+void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has_vals,
+                uint64_t n, int bits, bool skip_trivial = true);
+
+// Exclusive scan of per-element expand degrees (see sk_relops.cu).
+// pos[i] = sum_{k<i} deg(i); pos[n] = total.  Returns nothing; read pos[n].
+template <class K>
+void expand_offsets(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uint64_t jmask,
+                    const uint32_t* off, uint64_t n_nodes, uint64_t* pos);
+
+// Load-balanced expand: for every Δ tuple i and every CSR neighbour v of its
+// join value, emit  out = (kept(i) << out_pshift) | (v << out_vshift), with
+// Trop weight w = dw[i] (x) ew[e].  `total` = pos[n].
+template <class K, class W, bool TROP>
+void expand_emit(strata_ctx* ctx, const K* dkeys, const W* dw, uint64_t n, const uint64_t* pos,
+                 uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask,
+                 int out_pshift, int out_vshift, const uint32_t* off, uint64_t n_nodes,
+                 const uint32_t* nbr, const W* nbr_w, K* out, W* out_w);
+
+// Reduce sorted keys with duplicates to one row per key (Trop: the minimum
+// weight).  Writes count to *d_count (device).  `out`/`out_w` capacity >= n.
+template <class K, class W, bool TROP>
+void reduce_runs(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, K* out, W* out_w,
+                 uint64_t* d_count);
+
+// Merge the sorted unique `full` with the sorted unique `cand`:
+//   full_out = full ∪ cand (Trop: min weight per key),
+//   delta    = keys of cand new to full (Bool) or new / strictly better (Trop).
+// d_counts[0] = |full_out|, d_counts[1] = |delta|.
+template <class K, class W, bool TROP>
+void merge_diff(strata_ctx* ctx, const K* full, const W* full_w, uint64_t nf, const K* cand,
+                const W* cand_w, uint64_t nc, K* full_out, W* full_out_w, K* delta, W* delta_w,
+                uint64_t* d_counts);
+
+// Plain merge of two sorted disjoint runs.
+template <class K, class W, bool TROP>
+void merge_disjoint(strata_ctx* ctx, const K* a, const W* aw, uint64_t na, const K* b,
+                    const W* bw, uint64_t nb, K* out, W* out_w);
+
+// Dedup + difference against full (operator form): distinct cand keys absent
+// from full; Trop: min-reduced keys new to full or strictly better, with the
+// better weights also written into full_w.  d_count[0] = output count.
+template <class K, class W, bool TROP>
+void diff_improve(strata_ctx* ctx, const K* cand, const W* cand_w, uint64_t nc, const K* full,
+                  W* full_w, uint64_t nf, K* out, W* out_w, uint64_t* d_count);
+
+// CSR offsets from keys sorted by (join << vbits) | v:
+// off[j] = first index with join >= j, for j in [0, n_nodes]; nbr[i] = key & vmask.
+template <class K>
+void build_csr(strata_ctx* ctx, const K* keys, uint64_t m, int vbits, uint64_t n_nodes,
+               uint32_t* off, uint32_t* nbr);
+
+// Count distinct ids below `limit` present in up to three u32 columns.
+uint64_t count_distinct_ids(strata_ctx* ctx, const uint32_t* a, uint64_t na, const uint32_t* b,
+                            uint64_t nb, const uint32_t* c, uint64_t nc, uint64_t limit);
+
+// max over columns (synchronizing).
+uint32_t max_u32(strata_ctx* ctx, const uint32_t* a, uint64_t n);
+
+// Pack two u32 columns into keys (c0 << shift) | c1, optional weight conversion
+// from (int64 w, u8 inf) to W (inf -> WInf<W>).  Sets ST_SENTINEL when a finite
+// weight equals INT64_MAX.
+template <class K, class W, bool TROP>
+void pack_pairs(strata_ctx* ctx, const uint32_t* c0, const uint32_t* c1, const int64_t* w,
+                const uint8_t* inf, uint64_t n, int shift, K* keys, W* ow);
+
+// Unpack keys to columns (and W weights to int64 + inf mask).
+template <class K, class W, bool TROP>
+void unpack_pairs(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int shift,
+                  uint32_t* c0, uint32_t* c1, int64_t* ow, uint8_t* oinf);
+
+// Max |finite weight| over (w, inf) columns (synchronizing); 0 when n == 0.
+uint64_t max_abs_weight(strata_ctx* ctx, const int64_t* w, const uint8_t* inf, uint64_t n);
+
+// Order-independent fingerprint of (keys, weights).
+template <class K, class W, bool TROP>
+uint64_t fingerprint(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int shift);
+
+}  // namespace sk

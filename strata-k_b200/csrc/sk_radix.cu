@@ -1,0 +1,267 @@
+// sk_radix.cu — stable LSD radix sort of packed tuple keys (onesweep).
+//
+// Replaces the reference's 64 one-bit split passes with three host
+// round-trips each (strata-gpu/src/sort.rs:337-365, scan_flags :282-315).
+// Design for sm_100a:
+//   * one upfront kernel computes the digit histograms of every pass from a
+//     single read of the keys (warp-privatised shared-memory counters with
+//     match-any aggregation);
+//   * each 8-bit pass is ONE kernel: a tile of NT*ITEMS keys is loaded
+//     warp-striped (coalesced), ranked with warp-level multisplit (8 ballots
+//     per item), the tile's per-digit counts are published for a decoupled
+//     look-back, keys are staged in shared memory in digit order and written
+//     out in runs (coalesced per digit);
+//   * only the significant `bits` of the key are sorted (a 26-bit key takes 4
+//     passes, not 64) and passes whose digit is constant are skipped.
+#include "sk_ops.cuh"
+#include "sk_prims.cuh"
+
+#include <vector>
+
+namespace sk {
+namespace {
+
+constexpr int RADIX = 256;
+constexpr int NT = 256;  // threads per block == RADIX (one digit per thread)
+constexpr int NW = NT / 32;
+constexpr uint32_t kLb32A = 1u << 30;
+constexpr uint32_t kLb32P = 2u << 30;
+constexpr uint32_t kLb32Mask = (1u << 30) - 1;
+
+template <class K> struct RCfg;
+template <> struct RCfg<uint32_t> { static constexpr int ITEMS = 15; };
+template <> struct RCfg<uint64_t> { static constexpr int ITEMS = 9; };
+
+// Digit histograms of passes [p0, p0 + np), np <= 4.
+template <class K>
+__global__ void __launch_bounds__(NT) k_radix_hist(const K* __restrict__ keys, uint64_t n, int p0,
+                                                   int np, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t sh[4][NW][RADIX];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < 4 * NW * RADIX; i += NT) (&sh[0][0][0])[i] = 0;
+  __syncthreads();
+  const uint64_t stride = (uint64_t)gridDim.x * NT;
+  // Every lane of a warp runs the same number of iterations (match-any needs
+  // the full warp), so loop on the warp's first index.
+  for (uint64_t i0 = (uint64_t)blockIdx.x * NT + (tid & ~31); i0 < n; i0 += stride) {
+    const uint64_t i = i0 + lane;
+    const bool valid = i < n;
+    const K k = valid ? keys[i] : K(0);
+    for (int p = 0; p < np; p++) {
+      const uint32_t d = valid ? (uint32_t)(k >> (8 * (p0 + p))) & 0xffu : 0x100u;
+      const unsigned peers = __match_any_sync(kFull, d);
+      if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&sh[p][warp][d], (uint32_t)__popc(peers));
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < np * RADIX; i += NT) {
+    const int p = i / RADIX, d = i % RADIX;
+    uint32_t s = 0;
+#pragma unroll
+    for (int w = 0; w < NW; w++) s += sh[p][w][d];
+    if (s) atomicAdd(&hist[(p0 + p) * RADIX + d], s);
+  }
+}
+
+// Exclusive scan of each pass's 256 bins (one block per pass).
+__global__ void __launch_bounds__(NT) k_radix_bins(const uint32_t* __restrict__ hist,
+                                                   uint32_t* __restrict__ binoff) {
+  __shared__ uint32_t scratch[NW + 1];
+  const uint32_t v = hist[blockIdx.x * RADIX + threadIdx.x];
+  uint32_t tot;
+  binoff[blockIdx.x * RADIX + threadIdx.x] = block_excl_sum<NT>(v, scratch, &tot);
+}
+
+template <class K, class V, bool HAS_V, int ITEMS>
+__global__ void __launch_bounds__(NT) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
+                                                 const V* __restrict__ vin, V* __restrict__ vout,
+                                                 uint32_t n, int shift, int dbits,
+                                                 const uint32_t* __restrict__ binoff,
+                                                 uint32_t* lookback, uint32_t* tile_counter,
+                                                 uint32_t* status) {
+  constexpr uint32_t TILE = NT * ITEMS;
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_whist[NW][RADIX];
+  __shared__ uint32_t s_dstart[RADIX];
+  __shared__ uint32_t s_gbase[RADIX];
+  __shared__ uint32_t s_scan[NW + 1];
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  K* s_keys = reinterpret_cast<K*>(s_raw);
+  V* s_vals = reinterpret_cast<V*>(s_raw);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < NW * RADIX; i += NT) (&s_whist[0][0])[i] = 0;
+  const uint32_t tile = claim_tile(tile_counter, &s_tile);
+  const uint32_t base = tile * TILE;
+  const uint32_t dmask = (1u << dbits) - 1;
+  const uint32_t wbase = base + (uint32_t)warp * 32u * ITEMS;
+  const unsigned lt = lanemask_lt();
+
+  K key[ITEMS];
+  uint32_t rank[ITEMS];
+#pragma unroll
+  for (int j = 0; j < ITEMS; j++) {
+    const uint32_t idx = wbase + j * 32 + lane;
+    key[j] = (idx < n) ? kin[idx] : K(0);
+  }
+  // Warp-level multisplit: peers = lanes of this warp holding the same digit.
+#pragma unroll
+  for (int j = 0; j < ITEMS; j++) {
+    const uint32_t idx = wbase + j * 32 + lane;
+    const bool valid = idx < n;
+    const uint32_t d = (uint32_t)(key[j] >> shift) & dmask;
+    unsigned peers = __ballot_sync(kFull, valid);
+    for (int b = 0; b < dbits; b++) {
+      const unsigned bb = __ballot_sync(kFull, (d >> b) & 1u);
+      peers &= ((d >> b) & 1u) ? bb : ~bb;
+    }
+    uint32_t prior = valid ? s_whist[warp][d] : 0u;
+    rank[j] = prior + __popc(peers & lt);
+    __syncwarp();
+    if (valid && (peers & lt) == 0) s_whist[warp][d] = prior + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Thread tid owns digit tid: warp-exclusive offsets and the tile count.
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int w = 0; w < NW; w++) {
+    const uint32_t c = s_whist[w][tid];
+    s_whist[w][tid] = cnt;
+    cnt += c;
+  }
+  uint32_t* lb = lookback + (size_t)tile * RADIX;
+  st_volatile(&lb[tid], (tile == 0 ? kLb32P : kLb32A) | cnt);
+  uint32_t tot;
+  s_dstart[tid] = block_excl_sum<NT>(cnt, s_scan, &tot);
+
+  uint32_t excl = 0;
+  if (tile > 0) {
+    bool timed_out = false;
+    for (int64_t t = (int64_t)tile - 1; t >= 0; t--) {
+      uint32_t v, it = 0;
+      do {
+        v = ld_volatile(&lookback[(size_t)t * RADIX + tid]);
+      } while ((v >> 30) == 0 && ++it < kSpinLimit);
+      if ((v >> 30) == 0) { timed_out = true; break; }
+      excl += v & kLb32Mask;
+      if ((v >> 30) == 2) break;
+    }
+    if (timed_out) atomicOr(status, ST_LOOKBACK_TIMEOUT);
+    st_volatile(&lb[tid], kLb32P | (excl + cnt));
+  }
+  s_gbase[tid] = binoff[tid] + excl;
+  __syncthreads();
+
+  // Stage keys in digit order, then write runs out.
+  uint32_t pos[ITEMS];
+#pragma unroll
+  for (int j = 0; j < ITEMS; j++) {
+    const uint32_t idx = wbase + j * 32 + lane;
+    if (idx < n) {
+      const uint32_t d = (uint32_t)(key[j] >> shift) & dmask;
+      pos[j] = s_dstart[d] + s_whist[warp][d] + rank[j];
+      s_keys[pos[j]] = key[j];
+    }
+  }
+  __syncthreads();
+  const uint32_t tile_n = min(TILE, n - base);
+  uint32_t dst[ITEMS];
+#pragma unroll
+  for (int j = 0; j < ITEMS; j++) {
+    const uint32_t i = j * NT + tid;
+    if (i < tile_n) {
+      const K k = s_keys[i];
+      const uint32_t d = (uint32_t)(k >> shift) & dmask;
+      dst[j] = s_gbase[d] + (i - s_dstart[d]);
+      kout[dst[j]] = k;
+    }
+  }
+  if constexpr (HAS_V) {
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < ITEMS; j++) {
+      const uint32_t idx = wbase + j * 32 + lane;
+      if (idx < n) s_vals[pos[j]] = vin[idx];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < ITEMS; j++) {
+      const uint32_t i = j * NT + tid;
+      if (i < tile_n) vout[dst[j]] = s_vals[i];
+    }
+  }
+}
+
+}  // namespace
+
+template <class K, class V>
+void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has_vals,
+                uint64_t n, int bits, bool skip_trivial) {
+  if (n <= 1 || bits <= 0) return;
+  if (n > kMaxSortN) fail(STRATA_E_UNSUPPORTED, "radix sort call limited to 2^30-1 keys");
+  if (bits > (int)(8 * sizeof(K))) bits = 8 * sizeof(K);
+  constexpr int ITEMS = RCfg<K>::ITEMS;
+  constexpr uint32_t TILE = NT * ITEMS;
+  const int passes = (bits + 7) / 8;
+
+  DBuf<uint32_t> hist(ctx, passes * RADIX + passes);
+  uint32_t* counters = hist.p + passes * RADIX;
+  SK_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(uint32_t) * (passes * RADIX + passes), ctx->stream));
+  const int hblocks = (int)std::min<uint64_t>(ceil_div(n, NT * 16), (uint64_t)ctx->num_sms * 4);
+  for (int p0 = 0; p0 < passes; p0 += 4) {
+    const int np = std::min(4, passes - p0);
+    k_radix_hist<K><<<hblocks, NT, 0, ctx->stream>>>(*keys, n, p0, np, hist.p);
+    after_launch(ctx, "k_radix_hist");
+  }
+  DBuf<uint32_t> binoff(ctx, passes * RADIX);
+  k_radix_bins<<<passes, NT, 0, ctx->stream>>>(hist.p, binoff.p);
+  after_launch(ctx, "k_radix_bins");
+
+  bool trivial[8] = {false, false, false, false, false, false, false, false};
+  if (skip_trivial) {
+    std::vector<uint32_t> h(passes * RADIX);
+    SK_CUDA(cudaMemcpyAsync(h.data(), hist.p, sizeof(uint32_t) * passes * RADIX,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    SK_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int p = 0; p < passes; p++)
+      for (int d = 0; d < RADIX; d++)
+        if (h[p * RADIX + d] == n) trivial[p] = true;
+  }
+
+  const uint32_t ntiles = (uint32_t)ceil_div(n, TILE);
+  DBuf<uint32_t> lookback(ctx, (uint64_t)ntiles * RADIX);
+  const size_t smem = (size_t)TILE * (has_vals ? std::max(sizeof(K), sizeof(V)) : sizeof(K));
+  for (int p = 0; p < passes; p++) {
+    if (trivial[p]) continue;
+    SK_CUDA(cudaMemsetAsync(lookback.p, 0, sizeof(uint32_t) * ntiles * RADIX, ctx->stream));
+    const int dbits = std::min(8, bits - 8 * p);
+    if (has_vals) {
+      auto kern = k_onesweep<K, V, true, ITEMS>;
+      SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, *vals, *valt, (uint32_t)n, 8 * p, dbits,
+                                              binoff.p + p * RADIX, lookback.p, counters + p,
+                                              ctx->d_status);
+    } else {
+      auto kern = k_onesweep<K, V, false, ITEMS>;
+      SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, nullptr, nullptr, (uint32_t)n, 8 * p,
+                                              dbits, binoff.p + p * RADIX, lookback.p,
+                                              counters + p, ctx->d_status);
+    }
+    after_launch(ctx, "k_onesweep");
+    std::swap(*keys, *alt);
+    if (has_vals) std::swap(*vals, *valt);
+  }
+}
+
+#define SK_INST_SORT(K, V)                                                                   \
+  template void radix_sort<K, V>(strata_ctx*, K**, K**, V**, V**, bool, uint64_t, int, bool);
+SK_INST_SORT(uint32_t, uint32_t)
+SK_INST_SORT(uint32_t, uint64_t)
+SK_INST_SORT(uint64_t, uint32_t)
+SK_INST_SORT(uint64_t, uint64_t)
+#undef SK_INST_SORT
+
+}  // namespace sk

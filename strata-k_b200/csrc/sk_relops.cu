@@ -1,0 +1,849 @@
+// sk_relops.cu — the interpreter's operator surface on sorted packed keys.
+//
+//   expand_offsets + expand_emit : scan/join/project of Δ against a CSR index
+//       of the EDB relation on the join column (replaces bj_count/bj_emit,
+//       strata-gpu/src/sort.rs:115-145, and bjt_emit :176; the reference
+//       copies the counts to the host for a prefix sum, tc.rs:67-78).
+//   reduce_runs : dedup (Bool ⊕ = OR) or min-by-key (Trop ⊕ = min) of sorted
+//       candidates (flag_unique/scatter_unique, sort.rs:69-111; sort_min_dev
+//       :465-513).
+//   merge_diff  : full ∪ C and Δ' = C ∖ full (Bool) or C's new-or-improved
+//       rows (Trop) in ONE merge-path pass (diff_flag :146, diff_improve :192,
+//       and the concat + full re-sort of tc.rs:124-144 / trop.rs:177-213).
+//   build_csr, pack/unpack, distinct-id count, fingerprint : plumbing.
+//
+// Every kernel is single-pass over its inputs; cross-tile offsets come from
+// the bounded decoupled look-back in sk_prims.cuh.
+#include "sk_ops.cuh"
+#include "sk_prims.cuh"
+
+namespace sk {
+namespace {
+
+constexpr int NT = 256;
+
+// ---------------------------------------------------------------------------
+// expand: offsets
+// ---------------------------------------------------------------------------
+constexpr int EO_ITEMS = 8;
+constexpr uint32_t EO_TILE = NT * EO_ITEMS;
+
+template <class K>
+__global__ void __launch_bounds__(NT)
+    k_expand_offsets(const K* __restrict__ dkeys, uint64_t n, int jshift, uint64_t jmask,
+                     const uint32_t* __restrict__ off, uint64_t n_nodes, uint64_t* __restrict__ pos,
+                     uint64_t* states, uint32_t* counter, uint32_t* status) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint64_t s_warp[NT / 32 + 1];
+  __shared__ uint64_t s_excl;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t tile = claim_tile(counter, &s_tile);
+  const uint64_t wbase = (uint64_t)tile * EO_TILE + (uint64_t)warp * 32 * EO_ITEMS;
+  uint64_t vals[EO_ITEMS];
+  uint64_t carry = 0;
+#pragma unroll
+  for (int j = 0; j < EO_ITEMS; j++) {
+    const uint64_t idx = wbase + j * 32 + lane;
+    uint64_t deg = 0;
+    if (idx < n) {
+      const uint64_t jv = ((uint64_t)dkeys[idx] >> jshift) & jmask;
+      if (jv < n_nodes) deg = (uint64_t)(off[jv + 1] - off[jv]);
+    }
+    const uint64_t incl = warp_incl_sum(deg);
+    vals[j] = carry + incl - deg;
+    carry += __shfl_sync(kFull, incl, 31);
+  }
+  if (lane == 0) s_warp[warp] = carry;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t w = (lane < NT / 32) ? s_warp[lane] : 0;
+    uint64_t wi = warp_incl_sum(w);
+    if (lane < NT / 32) s_warp[lane] = wi - w;
+    const uint64_t agg = __shfl_sync(kFull, wi, NT / 32 - 1);
+    const uint64_t ex = warp_lookback(states, tile, agg, status);
+    if (lane == 0) {
+      s_excl = ex;
+      if (tile == gridDim.x - 1) pos[n] = ex + agg;
+    }
+  }
+  __syncthreads();
+  const uint64_t base = s_excl + s_warp[warp];
+#pragma unroll
+  for (int j = 0; j < EO_ITEMS; j++) {
+    const uint64_t idx = wbase + j * 32 + lane;
+    if (idx < n) pos[idx] = base + vals[j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// expand: load-balanced emit (merge path over item events and outputs)
+// ---------------------------------------------------------------------------
+constexpr int EE_ITEMS = 6;
+constexpr uint32_t EE_TILE = NT * EE_ITEMS;
+
+// #items i with i + pos[i] < d  (i + pos[i] is strictly increasing).
+__device__ __forceinline__ uint64_t mp_items_before(const uint64_t* pos, uint64_t n, uint64_t d) {
+  uint64_t lo = 0, hi = d < n ? d : n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (mid + pos[mid] < d) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+template <class K, class W, bool TROP>
+__global__ void __launch_bounds__(NT)
+    k_expand_emit(const K* __restrict__ dkeys, const W* __restrict__ dw, uint64_t n,
+                  const uint64_t* __restrict__ pos, uint64_t total, int jshift, uint64_t jmask,
+                  int pshift, uint64_t pmask, int out_pshift, int out_vshift,
+                  const uint32_t* __restrict__ off, uint64_t n_nodes, const uint32_t* __restrict__ nbr,
+                  const W* __restrict__ nbr_w, K* __restrict__ out, W* __restrict__ out_w,
+                  uint32_t* status) {
+  __shared__ uint64_t s_pos[EE_TILE + 1];
+  __shared__ uint32_t s_seg[EE_TILE + 1];
+  __shared__ K s_kept[EE_TILE + 1];
+  __shared__ W s_w[TROP ? EE_TILE + 1 : 1];
+  __shared__ uint64_t s_r[4];
+  const int tid = threadIdx.x;
+  const uint64_t L = n + total;
+  const uint64_t d0 = (uint64_t)blockIdx.x * EE_TILE;
+  const uint64_t d1 = d0 + EE_TILE < L ? d0 + EE_TILE : L;
+  if (tid == 0) {
+    const uint64_t i0 = mp_items_before(pos, n, d0);
+    const uint64_t i1 = mp_items_before(pos, n, d1);
+    s_r[0] = i0 > 0 ? i0 - 1 : 0;  // first item that may own an output here
+    s_r[1] = i1;
+    s_r[2] = d0 - i0;              // first output of the tile
+    s_r[3] = d1 - i1;              // one past the last output
+  }
+  __syncthreads();
+  const uint64_t a = s_r[0], i1 = s_r[1], o0 = s_r[2], o1 = s_r[3];
+  const uint32_t cnt = (uint32_t)(i1 - a);  // <= EE_TILE + 1
+  for (uint32_t k = tid; k < cnt; k += NT) {
+    const uint64_t i = a + k;
+    const K key = dkeys[i];
+    const uint64_t jv = ((uint64_t)key >> jshift) & jmask;
+    s_pos[k] = pos[i];
+    s_seg[k] = jv < n_nodes ? off[jv] : 0u;
+    s_kept[k] = (K)(((uint64_t)key >> pshift) & pmask);
+    if constexpr (TROP) s_w[k] = dw[i];
+  }
+  __syncthreads();
+  uint32_t flags = 0;
+  for (uint64_t o = o0 + tid; o < o1; o += NT) {
+    // owner = last loaded item with pos <= o
+    uint32_t lo = 0, hi = cnt;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (s_pos[mid] <= o) lo = mid + 1; else hi = mid;
+    }
+    if (lo == 0) { flags |= ST_BOUNDS; continue; }
+    const uint32_t li = lo - 1;
+    const uint64_t e = (uint64_t)s_seg[li] + (o - s_pos[li]);
+    const uint32_t v = nbr[e];
+    out[o] = (K)(((K)s_kept[li] << out_pshift) | ((K)v << out_vshift));
+    if constexpr (TROP) out_w[o] = trop_mul(s_w[li], nbr_w[e], &flags);
+  }
+  if (flags) atomicOr(status, flags);
+}
+
+// ---------------------------------------------------------------------------
+// reduce_runs: one row per distinct key (Trop: minimum weight)
+// ---------------------------------------------------------------------------
+// Items per thread: odd (conflict-free blocked shared-memory reads); fewer for
+// 8-byte rows so the four staging arrays stay within 48 KB.
+template <class K, class W, bool TROP>
+struct RRCfg {
+  static constexpr int ITEMS = (sizeof(K) + (TROP ? sizeof(W) : 0)) > 8 ? 5 : 9;
+  static constexpr uint32_t TILE = NT * ITEMS;
+};
+
+// First run head at or after p (keys sorted); galloping then binary search.
+template <class K>
+__device__ uint64_t first_head_from(const K* keys, uint64_t n, uint64_t p) {
+  if (p == 0) return 0;
+  if (p >= n) return n;
+  const K prev = keys[p - 1];
+  if (keys[p] != prev) return p;
+  uint64_t step = 1, lo = p, hi;
+  while (true) {
+    hi = lo + step;
+    if (hi >= n) { hi = n; break; }
+    if (keys[hi] != prev) break;
+    lo = hi;
+    step <<= 1;
+  }
+  // keys[lo] == prev, keys[hi] != prev (or hi == n)
+  return upper_bound_dev(keys, lo, hi, prev);
+}
+
+template <class W>
+struct SegMin {  // segmented-min scan state: has a run start, min since it
+  bool h;
+  W m;
+};
+template <class W>
+__device__ __forceinline__ SegMin<W> seg_combine(SegMin<W> a, SegMin<W> b) {
+  SegMin<W> r;
+  r.h = a.h | b.h;
+  r.m = b.h ? b.m : (a.m < b.m ? a.m : b.m);
+  return r;
+}
+
+template <class K, class W, bool TROP>
+__global__ void __launch_bounds__(NT)
+    k_reduce_runs(const K* __restrict__ keys, const W* __restrict__ w, uint64_t n, K* __restrict__ out,
+                  W* __restrict__ out_w, uint64_t* states, uint32_t* counter, uint64_t* d_count,
+                  uint32_t* status) {
+  constexpr int RR_ITEMS = RRCfg<K, W, TROP>::ITEMS;
+  constexpr uint32_t RR_TILE = RRCfg<K, W, TROP>::TILE;
+  __shared__ uint32_t s_tile;
+  __shared__ K s_k[RR_TILE];
+  __shared__ W s_w[TROP ? RR_TILE : 1];
+  __shared__ K s_ok[RR_TILE];
+  __shared__ W s_ow[TROP ? RR_TILE : 1];
+  __shared__ uint32_t s_scan[NT / 32 + 1];
+  __shared__ SegMin<W> s_seg[NT / 32];
+  __shared__ uint64_t s_se[2];
+  __shared__ uint64_t s_excl;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t tile = claim_tile(counter, &s_tile);
+  if (tid == 0) {
+    const uint64_t p0 = (uint64_t)tile * RR_TILE;
+    const uint64_t p1 = p0 + RR_TILE < n ? p0 + RR_TILE : n;
+    s_se[0] = first_head_from(keys, n, p0);
+    s_se[1] = first_head_from(keys, n, p1);
+  }
+  __syncthreads();
+  const uint64_t s = s_se[0], e = s_se[1];
+  uint32_t nout = 0;       // rows staged so far (uniform)
+  W carry_m = W(0);        // min of the open run entering this chunk (Trop)
+  bool carry_h = false;
+  for (uint64_t c = s; c < e; c += RR_TILE) {
+    const uint32_t clen = (uint32_t)((e - c) < RR_TILE ? (e - c) : RR_TILE);
+    for (uint32_t k = tid; k < clen; k += NT) {
+      s_k[k] = keys[c + k];
+      if constexpr (TROP) s_w[k] = w[c + k];
+    }
+    __syncthreads();
+    const uint32_t b = tid * RR_ITEMS;
+    bool head[RR_ITEMS], last[RR_ITEMS];
+    W incl[RR_ITEMS];
+    SegMin<W> run{false, W(0)};
+#pragma unroll
+    for (int j = 0; j < RR_ITEMS; j++) {
+      const uint32_t li = b + j;
+      head[j] = false;
+      last[j] = false;
+      if (li < clen) {
+        const uint64_t gi = c + li;
+        const K kk = s_k[li];
+        head[j] = (gi == s) || (kk != (li > 0 ? s_k[li - 1] : keys[gi - 1]));
+        const uint64_t gn = gi + 1;
+        last[j] = (gn >= e) || (kk != (li + 1 < clen ? s_k[li + 1] : keys[gn]));
+        if constexpr (TROP) {
+          const W wv = s_w[li];
+          if (head[j]) run = SegMin<W>{true, wv};
+          else if (j == 0) run = SegMin<W>{false, wv};  // partial run entering the thread
+          else run = SegMin<W>{run.h, run.m < wv ? run.m : wv};
+          incl[j] = run.m;
+        }
+      }
+    }
+    // Trop: block-wide exclusive segmented scan of the thread aggregates.
+    if constexpr (TROP) {
+      // Items past clen leave run unchanged; an empty thread contributes
+      // the identity {false, +inf}.
+      SegMin<W> agg = (b < clen) ? run : SegMin<W>{false, WInf<W>::v};
+      SegMin<W> inc = agg;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        SegMin<W> t;
+        t.h = __shfl_up_sync(kFull, inc.h, o);
+        t.m = __shfl_up_sync(kFull, inc.m, o);
+        if (lane >= o) inc = seg_combine(t, inc);
+      }
+      if (lane == 31) s_seg[warp] = inc;
+      __syncthreads();
+      SegMin<W> wpre{false, WInf<W>::v};
+      for (int q = 0; q < warp; q++) wpre = seg_combine(wpre, s_seg[q]);
+      SegMin<W> ex;
+      ex.h = __shfl_up_sync(kFull, inc.h, 1);
+      ex.m = __shfl_up_sync(kFull, inc.m, 1);
+      if (lane == 0) ex = SegMin<W>{false, WInf<W>::v};
+      SegMin<W> pre = seg_combine(SegMin<W>{carry_h, carry_h ? carry_m : WInf<W>::v},
+                                  seg_combine(wpre, ex));
+      // Apply the carry to this thread's items up to its first head.
+#pragma unroll
+      for (int j = 0; j < RR_ITEMS; j++) {
+        if (b + j < clen) {
+          if (head[j]) break;
+          incl[j] = pre.m < incl[j] ? pre.m : incl[j];
+        }
+      }
+      // Carry for the next chunk: the block-inclusive state at the chunk end.
+      SegMin<W> tot{false, WInf<W>::v};
+      for (int q = 0; q < NT / 32; q++) tot = seg_combine(tot, s_seg[q]);
+      SegMin<W> nc = seg_combine(SegMin<W>{carry_h, carry_h ? carry_m : WInf<W>::v}, tot);
+      __syncthreads();
+      carry_h = nc.h;
+      carry_m = nc.m;
+    }
+    // Stage the run ends in order.
+    uint32_t mine = 0;
+#pragma unroll
+    for (int j = 0; j < RR_ITEMS; j++) mine += last[j] ? 1u : 0u;
+    uint32_t tot_c;
+    uint32_t at = nout + block_excl_sum<NT>(mine, s_scan, &tot_c);
+#pragma unroll
+    for (int j = 0; j < RR_ITEMS; j++) {
+      if (last[j]) {
+        if (at < RR_TILE) {
+          s_ok[at] = s_k[b + j];
+          if constexpr (TROP) s_ow[at] = incl[j];
+        } else {
+          atomicOr(status, ST_BOUNDS);
+        }
+        at++;
+      }
+    }
+    nout += tot_c;
+    __syncthreads();
+  }
+  if (warp == 0) {
+    const uint64_t ex = warp_lookback(states, tile, (uint64_t)nout, status);
+    if (lane == 0) {
+      s_excl = ex;
+      if (tile == gridDim.x - 1) *d_count = ex + nout;
+    }
+  }
+  __syncthreads();
+  const uint64_t ob = s_excl;
+  const uint32_t lim = nout < RR_TILE ? nout : RR_TILE;
+  for (uint32_t k = tid; k < lim; k += NT) {
+    out[ob + k] = s_ok[k];
+    if constexpr (TROP) out_w[ob + k] = s_ow[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// merge_diff: full ∪ cand and the delta, one merge-path pass
+// ---------------------------------------------------------------------------
+constexpr int MD_ITEMS = 6;
+constexpr uint32_t MD_TILE = NT * MD_ITEMS;
+
+// Merge-path split of diagonal d: #A among the first d merged elements (A wins
+// ties), then moved so that an equal pair A[i-1] == B[j] stays in one tile.
+template <class K>
+__device__ void md_split(const K* A, uint64_t na, const K* B, uint64_t nb, uint64_t d,
+                         uint64_t* oi, uint64_t* oj) {
+  uint64_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (A[mid] <= B[d - mid - 1]) lo = mid + 1; else hi = mid;
+  }
+  uint64_t i = lo, j = d - lo;
+  if (i > 0 && j < nb && A[i - 1] == B[j]) j++;
+  *oi = i;
+  *oj = j;
+}
+
+template <class K, class W, bool TROP, bool WRITE_FULL, bool WRITE_DELTA, bool INPLACE>
+__global__ void __launch_bounds__(NT)
+    k_merge_diff(const K* __restrict__ A, W* Aw, uint64_t na, const K* __restrict__ B,
+                 const W* __restrict__ Bw, uint64_t nb, K* __restrict__ fout, W* __restrict__ fout_w,
+                 K* __restrict__ dout, W* __restrict__ dout_w, uint64_t* fstates, uint64_t* dstates,
+                 uint32_t* counter, uint64_t* d_counts, uint32_t* status) {
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  constexpr uint32_t CAP = MD_TILE + 2;
+  K* s_a = reinterpret_cast<K*>(s_raw);
+  K* s_b = s_a + CAP;
+  W* s_aw = reinterpret_cast<W*>(s_b + CAP);
+  W* s_bw = s_aw + (TROP ? CAP : 0);
+  uint32_t* s_mpre = reinterpret_cast<uint32_t*>(s_bw + (TROP ? CAP : 0));  // CAP + 1
+  uint32_t* s_dpre = s_mpre + CAP + 1;                                      // CAP
+  __shared__ uint32_t s_tile;
+  __shared__ uint64_t s_r[4];
+  __shared__ uint32_t s_scan[NT / 32 + 1];
+  __shared__ uint64_t s_ex[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t tile = claim_tile(counter, &s_tile);
+  const uint64_t L = na + nb;
+  if (tid == 0) {
+    const uint64_t d0 = (uint64_t)tile * MD_TILE;
+    const uint64_t d1 = d0 + MD_TILE < L ? d0 + MD_TILE : L;
+    uint64_t i0, j0, i1, j1;
+    md_split(A, na, B, nb, d0, &i0, &j0);
+    md_split(A, na, B, nb, d1, &i1, &j1);
+    s_r[0] = i0; s_r[1] = j0; s_r[2] = i1; s_r[3] = j1;
+  }
+  __syncthreads();
+  const uint64_t i0 = s_r[0], j0 = s_r[1];
+  const uint32_t acnt = (uint32_t)(s_r[2] - i0);
+  const uint32_t bcnt = (uint32_t)(s_r[3] - j0);
+  for (uint32_t k = tid; k < acnt; k += NT) {
+    s_a[k] = A[i0 + k];
+    if constexpr (TROP) s_aw[k] = Aw[i0 + k];
+  }
+  for (uint32_t k = tid; k < bcnt; k += NT) {
+    s_b[k] = B[j0 + k];
+    if constexpr (TROP) s_bw[k] = Bw[j0 + k];
+  }
+  __syncthreads();
+  // Per B element: rank in A, matched?, delta?
+  constexpr int BI = (MD_TILE + 2 + NT - 1) / NT;
+  uint32_t b_ra[BI];
+  uint32_t mflag = 0, dflag = 0;  // bit per item
+  uint32_t mcount = 0, dcount = 0;
+  const uint32_t bb = tid * BI;
+#pragma unroll
+  for (int q = 0; q < BI; q++) {
+    const uint32_t jb = bb + q;
+    b_ra[q] = 0;
+    if (jb < bcnt) {
+      const K x = s_b[jb];
+      uint32_t lo = 0, hi = acnt;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_a[mid] < x) lo = mid + 1; else hi = mid;
+      }
+      b_ra[q] = lo;
+      const bool m = lo < acnt && s_a[lo] == x;
+      bool dl = !m;
+      if constexpr (TROP) dl = dl || (s_bw[jb] < s_aw[lo]);
+      if (m) { mflag |= 1u << q; mcount++; }
+      if (dl) { dflag |= 1u << q; dcount++; }
+    }
+  }
+  uint32_t mtot, dtot;
+  const uint32_t mex = block_excl_sum<NT>(mcount, s_scan, &mtot);
+  const uint32_t dex = block_excl_sum<NT>(dcount, s_scan, &dtot);
+  {
+    uint32_t mr = mex, dr = dex;
+#pragma unroll
+    for (int q = 0; q < BI; q++) {
+      const uint32_t jb = bb + q;
+      if (jb < bcnt) {
+        s_mpre[jb] = mr;
+        s_dpre[jb] = dr;
+        mr += (mflag >> q) & 1u;
+        dr += (dflag >> q) & 1u;
+      }
+    }
+    if (tid == 0) s_mpre[bcnt] = mtot;
+  }
+  const uint32_t fcnt = acnt + bcnt - mtot;
+  if (warp == 0) {
+    uint64_t ex = 0;
+    if (WRITE_FULL) ex = warp_lookback(fstates, tile, fcnt, status);
+    if (lane == 0) s_ex[0] = ex;
+  } else if (warp == 1) {
+    uint64_t ex = 0;
+    if (WRITE_DELTA) ex = warp_lookback(dstates, tile, dtot, status);
+    if (lane == 0) s_ex[1] = ex;
+  }
+  __syncthreads();
+  const uint64_t fex = s_ex[0], dexg = s_ex[1];
+  if (tile == gridDim.x - 1 && tid == 0) {
+    d_counts[0] = fex + fcnt;
+    d_counts[1] = dexg + dtot;
+  }
+  // B elements: unmatched -> full_out; delta -> delta out.
+#pragma unroll
+  for (int q = 0; q < BI; q++) {
+    const uint32_t jb = bb + q;
+    if (jb < bcnt) {
+      const bool m = (mflag >> q) & 1u;
+      if (WRITE_FULL && !m) {
+        const uint64_t p = fex + b_ra[q] + (jb - s_mpre[jb]);
+        fout[p] = s_b[jb];
+        if constexpr (TROP) fout_w[p] = s_bw[jb];
+      }
+      if (WRITE_DELTA && ((dflag >> q) & 1u)) {
+        const uint64_t p = dexg + s_dpre[jb];
+        dout[p] = s_b[jb];
+        if constexpr (TROP) dout_w[p] = s_bw[jb];
+      }
+      if constexpr (TROP && INPLACE) {
+        if (m && s_bw[jb] < s_aw[b_ra[q]]) Aw[i0 + b_ra[q]] = s_bw[jb];
+      }
+    }
+  }
+  if constexpr (WRITE_FULL) {
+    for (uint32_t ia = tid; ia < acnt; ia += NT) {
+      const K x = s_a[ia];
+      uint32_t lo = 0, hi = bcnt;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_b[mid] < x) lo = mid + 1; else hi = mid;
+      }
+      const uint64_t p = fex + ia + (lo - s_mpre[lo]);
+      fout[p] = x;
+      if constexpr (TROP) {
+        W wv = s_aw[ia];
+        if (lo < bcnt && s_b[lo] == x && s_bw[lo] < wv) wv = s_bw[lo];
+        fout_w[p] = wv;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// plumbing kernels
+// ---------------------------------------------------------------------------
+template <class K>
+__global__ void k_csr_offsets(const K* __restrict__ keys, uint64_t m, int vbits, uint64_t n_nodes,
+                              uint32_t* __restrict__ off) {
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > n_nodes) return;
+  const K probe = (K)((K)j << vbits);
+  uint64_t lo = 0, hi = m;
+  if (j == n_nodes) { off[j] = (uint32_t)m; return; }
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (keys[mid] < probe) lo = mid + 1; else hi = mid;
+  }
+  off[j] = (uint32_t)lo;
+}
+
+template <class K>
+__global__ void k_csr_nbr(const K* __restrict__ keys, uint64_t m, uint64_t vmask, uint32_t* __restrict__ nbr) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) nbr[i] = (uint32_t)((uint64_t)keys[i] & vmask);
+}
+
+__global__ void k_mark_ids(const uint32_t* __restrict__ a, uint64_t n, uint32_t* bitmap, uint64_t limit) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = a[i];
+    if (v < limit) atomicOr(&bitmap[v >> 5], 1u << (v & 31));
+  }
+}
+
+__global__ void k_popcount(const uint32_t* __restrict__ bitmap, uint64_t words, unsigned long long* out) {
+  unsigned long long c = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (uint64_t)gridDim.x * blockDim.x)
+    c += __popc(bitmap[i]);
+  c = warp_sum(c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+__global__ void k_max_u32(const uint32_t* __restrict__ a, uint64_t n, uint32_t* out) {
+  uint32_t m = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    m = a[i] > m ? a[i] : m;
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint32_t t = __shfl_xor_sync(kFull, m, o);
+    m = t > m ? t : m;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__global__ void k_max_abs_w(const int64_t* __restrict__ w, const uint8_t* __restrict__ inf, uint64_t n,
+                            unsigned long long* out) {
+  unsigned long long m = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (inf && inf[i]) continue;
+    const int64_t v = w[i];
+    const unsigned long long a = v < 0 ? (unsigned long long)0 - (unsigned long long)v : (unsigned long long)v;
+    m = a > m ? a : m;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long t = __shfl_xor_sync(kFull, m, o);
+    m = t > m ? t : m;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+template <class K, class W, bool TROP>
+__global__ void k_pack(const uint32_t* __restrict__ c0, const uint32_t* __restrict__ c1,
+                       const int64_t* __restrict__ w, const uint8_t* __restrict__ inf, uint64_t n,
+                       int shift, K* __restrict__ keys, W* __restrict__ ow, uint32_t* status) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = (K)((c0 ? ((K)c0[i] << shift) : K(0)) | (K)c1[i]);  // NULL c0: unary key
+  if constexpr (TROP) {
+    const bool is_inf = inf && inf[i];
+    const int64_t v = w ? w[i] : 0;  // NULL weights = the (x) identity Finite(0)
+    if (is_inf) {
+      ow[i] = WInf<W>::v;
+    } else {
+      if ((int64_t)(W)v == (int64_t)WInf<W>::v || (int64_t)(W)v != v) atomicOr(status, ST_SENTINEL);
+      ow[i] = (W)v;
+    }
+  }
+}
+
+template <class K, class W, bool TROP>
+__global__ void k_unpack(const K* __restrict__ keys, const W* __restrict__ w, uint64_t n, int shift,
+                         uint32_t* __restrict__ c0, uint32_t* __restrict__ c1, int64_t* __restrict__ ow,
+                         uint8_t* __restrict__ oinf) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const K k = keys[i];
+  const K lowmask = shift >= (int)(8 * sizeof(K)) ? ~K(0) : (K)((K(1) << shift) - 1);
+  if (c0) c0[i] = (uint32_t)((uint64_t)k >> shift);
+  if (c1) c1[i] = (uint32_t)(k & lowmask);
+  if constexpr (TROP) {
+    const W v = w[i];
+    const bool is_inf = v == WInf<W>::v;
+    if (ow) ow[i] = is_inf ? 0 : (int64_t)v;
+    if (oinf) oinf[i] = is_inf ? 1 : 0;
+  }
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  // splitmix64 finalizer
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+template <class K, class W, bool TROP>
+__global__ void k_fingerprint(const K* __restrict__ keys, const W* __restrict__ w, uint64_t n, int shift,
+                              unsigned long long* out) {
+  unsigned long long acc = 0;
+  const K lowmask = (K)((K(1) << shift) - 1);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const K k = keys[i];
+    const uint64_t src = (uint64_t)k >> shift, dst = (uint64_t)(k & lowmask);
+    uint64_t h = mix64((src << 32) | dst);
+    if constexpr (TROP) {
+      const W v = w[i];
+      const uint64_t wv = v == WInf<W>::v ? 0xfffffffffffffffull : (uint64_t)(int64_t)v;
+      h = mix64(h ^ mix64(wv + 0x51ull));
+    }
+    acc += h;
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+
+inline int grid_for(strata_ctx* ctx, uint64_t n, int per_block = NT) {
+  uint64_t b = ceil_div(n, per_block);
+  const uint64_t cap = (uint64_t)ctx->num_sms * 8;
+  if (b > cap) b = cap;
+  return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host entry points
+// ---------------------------------------------------------------------------
+template <class K>
+void expand_offsets(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uint64_t jmask,
+                    const uint32_t* off, uint64_t n_nodes, uint64_t* pos) {
+  if (n == 0) {
+    SK_CUDA(cudaMemsetAsync(pos, 0, sizeof(uint64_t), ctx->stream));
+    return;
+  }
+  const uint32_t tiles = (uint32_t)ceil_div(n, EO_TILE);
+  DBuf<uint64_t> states(ctx, tiles + 1);
+  uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles);
+  SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 1), ctx->stream));
+  k_expand_offsets<K><<<tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, pos,
+                                                     states.p, counter, ctx->d_status);
+  after_launch(ctx, "k_expand_offsets");
+}
+
+template <class K, class W, bool TROP>
+void expand_emit(strata_ctx* ctx, const K* dkeys, const W* dw, uint64_t n, const uint64_t* pos,
+                 uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask,
+                 int out_pshift, int out_vshift, const uint32_t* off, uint64_t n_nodes,
+                 const uint32_t* nbr, const W* nbr_w, K* out, W* out_w) {
+  if (total == 0 || n == 0) return;
+  const uint64_t tiles = ceil_div(n + total, EE_TILE);
+  if (tiles > 0x7fffffffull) fail(STRATA_E_UNSUPPORTED, "expand too large for one launch");
+  k_expand_emit<K, W, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(
+      dkeys, dw, n, pos, total, jshift, jmask, pshift, pmask, out_pshift, out_vshift, off, n_nodes,
+      nbr, nbr_w, out, out_w, ctx->d_status);
+  after_launch(ctx, "k_expand_emit");
+}
+
+template <class K, class W, bool TROP>
+void reduce_runs(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, K* out, W* out_w,
+                 uint64_t* d_count) {
+  if (n == 0) {
+    SK_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), ctx->stream));
+    return;
+  }
+  const uint32_t tiles = (uint32_t)ceil_div(n, RRCfg<K, W, TROP>::TILE);
+  DBuf<uint64_t> states(ctx, tiles + 1);
+  uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles);
+  SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 1), ctx->stream));
+  k_reduce_runs<K, W, TROP><<<tiles, NT, 0, ctx->stream>>>(keys, w, n, out, out_w, states.p, counter,
+                                                           d_count, ctx->d_status);
+  after_launch(ctx, "k_reduce_runs");
+}
+
+template <class K, class W, bool TROP, bool WF, bool WD, bool IP>
+static void launch_merge(strata_ctx* ctx, const K* full, W* full_w, uint64_t nf, const K* cand,
+                         const W* cand_w, uint64_t nc, K* fout, W* fout_w, K* dout, W* dout_w,
+                         uint64_t* d_counts) {
+  if (nf + nc == 0) {
+    SK_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(uint64_t), ctx->stream));
+    return;
+  }
+  const uint32_t tiles = (uint32_t)ceil_div(nf + nc, MD_TILE);
+  DBuf<uint64_t> states(ctx, 2ull * tiles + 1);
+  uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + 2ull * tiles);
+  SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (2ull * tiles + 1), ctx->stream));
+  constexpr uint32_t CAP = MD_TILE + 2;
+  const size_t smem = 2 * CAP * sizeof(K) + (TROP ? 2 * CAP * sizeof(W) : 0) + (2 * CAP + 1) * sizeof(uint32_t);
+  auto kern = k_merge_diff<K, W, TROP, WF, WD, IP>;
+  SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<tiles, NT, smem, ctx->stream>>>(full, full_w, nf, cand, cand_w, nc, fout, fout_w, dout,
+                                         dout_w, states.p, states.p + tiles, counter, d_counts,
+                                         ctx->d_status);
+  after_launch(ctx, "k_merge_diff");
+}
+
+template <class K, class W, bool TROP>
+void merge_diff(strata_ctx* ctx, const K* full, const W* full_w, uint64_t nf, const K* cand,
+                const W* cand_w, uint64_t nc, K* full_out, W* full_out_w, K* delta, W* delta_w,
+                uint64_t* d_counts) {
+  launch_merge<K, W, TROP, true, true, false>(ctx, full, const_cast<W*>(full_w), nf, cand, cand_w, nc,
+                                              full_out, full_out_w, delta, delta_w, d_counts);
+}
+
+template <class K, class W, bool TROP>
+void merge_disjoint(strata_ctx* ctx, const K* a, const W* aw, uint64_t na, const K* b,
+                    const W* bw, uint64_t nb, K* out, W* out_w) {
+  DBuf<uint64_t> counts(ctx, 2);
+  launch_merge<K, W, TROP, true, false, false>(ctx, a, const_cast<W*>(aw), na, b, bw, nb, out, out_w,
+                                               nullptr, nullptr, counts.p);
+}
+
+template <class K, class W, bool TROP>
+void diff_improve(strata_ctx* ctx, const K* cand, const W* cand_w, uint64_t nc, const K* full,
+                  W* full_w, uint64_t nf, K* out, W* out_w, uint64_t* d_count) {
+  DBuf<K> ck(ctx, nc + 1);
+  DBuf<W> cw(ctx, TROP ? nc + 1 : 1);
+  DBuf<uint64_t> counts(ctx, 2);
+  reduce_runs<K, W, TROP>(ctx, cand, cand_w, nc, ck.p, cw.p, counts.p);
+  uint64_t nu;
+  read_u64(ctx, counts.p, &nu, 1);
+  launch_merge<K, W, TROP, false, true, true>(ctx, full, full_w, nf, ck.p, cw.p, nu, nullptr, nullptr,
+                                              out, out_w, counts.p);
+  SK_CUDA(cudaMemcpyAsync(d_count, counts.p + 1, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+template <class K>
+void build_csr(strata_ctx* ctx, const K* keys, uint64_t m, int vbits, uint64_t n_nodes,
+               uint32_t* off, uint32_t* nbr) {
+  if (m >= 0xffffffffull) fail(STRATA_E_UNSUPPORTED, "CSR limited to 2^32-1 edges");
+  k_csr_offsets<K><<<(unsigned)ceil_div(n_nodes + 1, NT), NT, 0, ctx->stream>>>(keys, m, vbits, n_nodes, off);
+  after_launch(ctx, "k_csr_offsets");
+  if (m) {
+    const uint64_t vmask = vbits >= 64 ? ~0ull : ((1ull << vbits) - 1);
+    k_csr_nbr<K><<<(unsigned)ceil_div(m, NT), NT, 0, ctx->stream>>>(keys, m, vmask, nbr);
+    after_launch(ctx, "k_csr_nbr");
+  }
+}
+
+uint64_t count_distinct_ids(strata_ctx* ctx, const uint32_t* a, uint64_t na, const uint32_t* b,
+                            uint64_t nb, const uint32_t* c, uint64_t nc, uint64_t limit) {
+  if (limit == 0) return 0;
+  const uint64_t words = ceil_div(limit, 32);
+  DBuf<uint32_t> bm(ctx, words);
+  DBuf<unsigned long long> cnt(ctx, 1);
+  SK_CUDA(cudaMemsetAsync(bm.p, 0, words * 4, ctx->stream));
+  SK_CUDA(cudaMemsetAsync(cnt.p, 0, 8, ctx->stream));
+  const uint32_t* cols[3] = {a, b, c};
+  const uint64_t ns[3] = {na, nb, nc};
+  for (int q = 0; q < 3; q++) {
+    if (!cols[q] || !ns[q]) continue;
+    k_mark_ids<<<grid_for(ctx, ns[q]), NT, 0, ctx->stream>>>(cols[q], ns[q], bm.p, limit);
+    after_launch(ctx, "k_mark_ids");
+  }
+  k_popcount<<<grid_for(ctx, words), NT, 0, ctx->stream>>>(bm.p, words, cnt.p);
+  after_launch(ctx, "k_popcount");
+  uint64_t r;
+  read_u64(ctx, reinterpret_cast<uint64_t*>(cnt.p), &r, 1);
+  return r;
+}
+
+uint32_t max_u32(strata_ctx* ctx, const uint32_t* a, uint64_t n) {
+  if (n == 0) return 0;
+  DBuf<uint64_t> m(ctx, 1);
+  SK_CUDA(cudaMemsetAsync(m.p, 0, 8, ctx->stream));
+  k_max_u32<<<grid_for(ctx, n), NT, 0, ctx->stream>>>(a, n, reinterpret_cast<uint32_t*>(m.p));
+  after_launch(ctx, "k_max_u32");
+  uint64_t r;
+  read_u64(ctx, m.p, &r, 1);
+  return (uint32_t)(r & 0xffffffffull);
+}
+
+uint64_t max_abs_weight(strata_ctx* ctx, const int64_t* w, const uint8_t* inf, uint64_t n) {
+  if (n == 0 || !w) return 0;
+  DBuf<unsigned long long> m(ctx, 1);
+  SK_CUDA(cudaMemsetAsync(m.p, 0, 8, ctx->stream));
+  k_max_abs_w<<<grid_for(ctx, n), NT, 0, ctx->stream>>>(w, inf, n, m.p);
+  after_launch(ctx, "k_max_abs_w");
+  uint64_t r;
+  read_u64(ctx, reinterpret_cast<uint64_t*>(m.p), &r, 1);
+  return r;
+}
+
+template <class K, class W, bool TROP>
+void pack_pairs(strata_ctx* ctx, const uint32_t* c0, const uint32_t* c1, const int64_t* w,
+                const uint8_t* inf, uint64_t n, int shift, K* keys, W* ow) {
+  if (n == 0) return;
+  k_pack<K, W, TROP><<<(unsigned)ceil_div(n, NT), NT, 0, ctx->stream>>>(c0, c1, w, inf, n, shift, keys, ow,
+                                                                       ctx->d_status);
+  after_launch(ctx, "k_pack");
+}
+
+template <class K, class W, bool TROP>
+void unpack_pairs(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int shift, uint32_t* c0,
+                  uint32_t* c1, int64_t* ow, uint8_t* oinf) {
+  if (n == 0) return;
+  k_unpack<K, W, TROP><<<(unsigned)ceil_div(n, NT), NT, 0, ctx->stream>>>(keys, w, n, shift, c0, c1, ow, oinf);
+  after_launch(ctx, "k_unpack");
+}
+
+template <class K, class W, bool TROP>
+uint64_t fingerprint(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int shift) {
+  DBuf<unsigned long long> acc(ctx, 1);
+  SK_CUDA(cudaMemsetAsync(acc.p, 0, 8, ctx->stream));
+  if (n) {
+    k_fingerprint<K, W, TROP><<<grid_for(ctx, n), NT, 0, ctx->stream>>>(keys, w, n, shift, acc.p);
+    after_launch(ctx, "k_fingerprint");
+  }
+  uint64_t r;
+  read_u64(ctx, reinterpret_cast<uint64_t*>(acc.p), &r, 1);
+  return r;
+}
+
+// ---- explicit instantiations ----------------------------------------------------
+template void expand_offsets<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t, uint64_t*);
+template void expand_offsets<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t, uint64_t*);
+template void build_csr<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, uint32_t*, uint32_t*);
+template void build_csr<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, uint64_t, uint32_t*, uint32_t*);
+
+#define SK_INST_KW(K, W, T)                                                                          \
+  template void expand_emit<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, const uint64_t*,     \
+                                     uint64_t, int, uint64_t, int, uint64_t, int, int,               \
+                                     const uint32_t*, uint64_t, const uint32_t*, const W*, K*, W*);  \
+  template void reduce_runs<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, K*, W*, uint64_t*);  \
+  template void merge_diff<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, const K*, const W*,   \
+                                    uint64_t, K*, W*, K*, W*, uint64_t*);                            \
+  template void merge_disjoint<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, const K*,         \
+                                        const W*, uint64_t, K*, W*);                                 \
+  template void diff_improve<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, const K*, W*,       \
+                                      uint64_t, K*, W*, uint64_t*);                                  \
+  template void pack_pairs<K, W, T>(strata_ctx*, const uint32_t*, const uint32_t*, const int64_t*,   \
+                                    const uint8_t*, uint64_t, int, K*, W*);                          \
+  template void unpack_pairs<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, int, uint32_t*,     \
+                                      uint32_t*, int64_t*, uint8_t*);                                \
+  template uint64_t fingerprint<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, int);
+SK_INST_KW(uint32_t, int32_t, false)
+SK_INST_KW(uint64_t, int32_t, false)
+SK_INST_KW(uint32_t, int32_t, true)
+SK_INST_KW(uint64_t, int32_t, true)
+SK_INST_KW(uint32_t, int64_t, true)
+SK_INST_KW(uint64_t, int64_t, true)
+#undef SK_INST_KW
+
+}  // namespace sk

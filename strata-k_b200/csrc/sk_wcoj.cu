@@ -1,0 +1,393 @@
+// sk_wcoj.cu — worst-case-optimal counting joins on a device CSR.
+//
+// The count aggregate  n(count<X>) :- e(X,Y), e(Y,Z), e(X,Z)  counts the body
+// bindings (strata-eval/src/naive.rs:300-391, fold_aggregate Count :391).
+// With out(x) the sorted successors of x in the set e, the bindings are
+//     Σ_{(X,Y) ∈ e} |out(X) ∩ out(Y)|,
+// a leapfrog of two sorted lists per edge.  The reference runs one thread per
+// edge with a serial merge over an id-oriented CSR built on the host
+// (strata-gpu/src/wcoj.rs:27-43, 99-131).  Here the CSR is built on the device
+// (radix sort + run reduction + offsets) and one warp owns a source vertex X:
+// it stages out(X) in shared memory, expands the concatenation of out(Y) over
+// Y ∈ out(X) with a warp scan so the 32 lanes stream the successor lists with
+// coalesced loads, and probes each candidate Z in the staged list.
+#include "sk_ops.cuh"
+#include "sk_prims.cuh"
+#include "sk_rel.cuh"
+
+namespace sk {
+namespace {
+
+constexpr int TC_WARPS = 8;
+constexpr int TC_NT = TC_WARPS * 32;
+constexpr uint32_t TC_STAGE = 1024;  // successor entries staged per warp
+
+__device__ __forceinline__ bool bsearch_u32(const uint32_t* a, uint32_t n, uint32_t x) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo < n && a[lo] == x;
+}
+
+__global__ void __launch_bounds__(TC_NT)
+    k_tri_count(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr, uint64_t n_nodes,
+                uint32_t* counter, unsigned long long* total) {
+  __shared__ uint32_t s_list[TC_WARPS][TC_STAGE];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long count = 0;
+  while (true) {
+    uint32_t u = 0;
+    if (lane == 0) u = atomicAdd(counter, 1u);
+    u = __shfl_sync(kFull, u, 0);
+    if (u >= n_nodes) break;
+    const uint32_t a0 = off[u], du = off[u + 1] - a0;
+    if (du == 0) continue;
+    const bool staged = du <= TC_STAGE;
+    if (staged) {
+      for (uint32_t k = lane; k < du; k += 32) s_list[warp][k] = nbr[a0 + k];
+    }
+    __syncwarp();
+    const uint32_t* A = staged ? s_list[warp] : nbr + a0;
+    for (uint32_t c = 0; c < du; c += 32) {
+      const uint32_t i = c + lane;
+      const bool valid = i < du;
+      const uint32_t v = valid ? A[i] : 0u;
+      const uint64_t dv = (valid && v < n_nodes) ? (uint64_t)(off[v + 1] - off[v]) : 0ull;
+      const uint32_t sv = (valid && v < n_nodes) ? off[v] : 0u;
+      const uint64_t incl = warp_incl_sum(dv);
+      const uint64_t D = __shfl_sync(kFull, incl, 31);
+      for (uint64_t base = 0; base < D; base += 32) {
+        const uint64_t j = base + lane;
+        const bool ok = j < D;
+        // owner lane t = number of lanes whose inclusive prefix is <= j
+        int t = 0;
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+          const uint64_t val = __shfl_sync(kFull, incl, t + s - 1);
+          if (val <= j) t += s;
+        }
+        const uint64_t ex_t = __shfl_sync(kFull, incl - dv, t & 31);
+        const uint32_t sv_t = __shfl_sync(kFull, sv, t & 31);
+        if (ok) {
+          const uint32_t w = nbr[sv_t + (j - ex_t)];
+          if (bsearch_u32(A, du, w)) count++;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  count = warp_sum(count);
+  if (lane == 0 && count) atomicAdd(total, count);
+}
+
+// K4 on a degree-oriented DAG: one thread per oriented edge (u, v); for each
+// common successor w1 count |out(u) ∩ out(v) ∩ out(w1)| by a 3-way leapfrog.
+__global__ void k_k4_count(const uint32_t* __restrict__ eu, const uint32_t* __restrict__ ev, uint64_t m,
+                           const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
+                           unsigned long long* total) {
+  unsigned long long c = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = eu[i], v = ev[i];
+    uint32_t a = off[u];
+    const uint32_t ae = off[u + 1];
+    uint32_t b = off[v];
+    const uint32_t be = off[v + 1];
+    while (a < ae && b < be) {
+      const uint32_t x = nbr[a], y = nbr[b];
+      if (x < y) { a++; continue; }
+      if (x > y) { b++; continue; }
+      const uint32_t w1 = x;
+      uint32_t p = a + 1, q = b + 1, r = off[w1];
+      const uint32_t re = off[w1 + 1];
+      while (p < ae && q < be && r < re) {
+        const uint32_t xp = nbr[p], xq = nbr[q], xr = nbr[r];
+        uint32_t mx = xp > xq ? xp : xq;
+        mx = xr > mx ? xr : mx;
+        if (xp < mx) p++;
+        else if (xq < mx) q++;
+        else if (xr < mx) r++;
+        else { c++; p++; q++; r++; }
+      }
+      a++;
+      b++;
+    }
+  }
+  c = warp_sum(c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(total, c);
+}
+
+// Canonical undirected edge key (min << b) | max; self-loops become the key
+// (2^b-1, 2^b-1), which no real edge can take and which sorts last.
+template <class K>
+__global__ void k_canon(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint64_t n, int bits,
+                        K* __restrict__ keys) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t x = a[i], y = b[i];
+  const K lo = x < y ? x : y, hi = x < y ? y : x;
+  const K sent = (K)((K(1) << bits) - 1);
+  keys[i] = (x == y) ? (K)((sent << bits) | sent) : (K)((lo << bits) | hi);
+}
+
+template <class K>
+__global__ void k_degree(const K* __restrict__ keys, uint64_t m, int bits, uint32_t* __restrict__ deg) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const K k = keys[i];
+  const K mask = (K)((K(1) << bits) - 1);
+  atomicAdd(&deg[(uint64_t)(k >> bits)], 1u);
+  atomicAdd(&deg[(uint64_t)(k & mask)], 1u);
+}
+
+// Orient each undirected edge from lower to higher (degree, id) rank.
+template <class K>
+__global__ void k_orient(K* __restrict__ keys, uint64_t m, int bits, const uint32_t* __restrict__ deg) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const K k = keys[i];
+  const K mask = (K)((K(1) << bits) - 1);
+  const K x = k >> bits, y = k & mask;
+  const uint32_t dx = deg[(uint64_t)x], dy = deg[(uint64_t)y];
+  const bool x_first = dx < dy || (dx == dy && x < y);
+  keys[i] = x_first ? (K)((x << bits) | y) : (K)((y << bits) | x);
+}
+
+template <class K>
+__global__ void k_split(const K* __restrict__ keys, uint64_t m, int bits, uint32_t* __restrict__ eu,
+                        uint32_t* __restrict__ ev) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const K k = keys[i];
+  eu[i] = (uint32_t)(k >> bits);
+  ev[i] = (uint32_t)(k & (K)((K(1) << bits) - 1));
+}
+
+__global__ void k_sum_sq_deg(const uint32_t* __restrict__ off, uint64_t n_nodes, unsigned long long* out) {
+  unsigned long long acc = 0;
+  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n_nodes; u += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long d = off[u + 1] - off[u];
+    acc += d * d;
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+
+__global__ void k_max_u64(const uint64_t* __restrict__ a, uint64_t n, unsigned long long* out) {
+  unsigned long long m = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    m = a[i] > m ? a[i] : m;
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long t = __shfl_xor_sync(kFull, m, o);
+    m = t > m ? t : m;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__global__ void k_intern_map(const uint64_t* __restrict__ keys, uint64_t n, const uint64_t* __restrict__ table,
+                             uint64_t m, uint32_t* __restrict__ ids) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  ids[i] = (uint32_t)lower_bound_dev(table, 0, m, keys[i]);
+}
+
+inline unsigned blocks(uint64_t n, int nt = 256) { return (unsigned)ceil_div(n ? n : 1, nt); }
+
+// Sort + dedup packed keys in `keys` (n), result in out (returns count).
+template <class K>
+uint64_t sort_unique(strata_ctx* ctx, DBuf<K>& keys, uint64_t n, int bits, DBuf<K>& out) {
+  DBuf<K> alt(ctx, n + 1);
+  K* kp = keys.p;
+  K* ka = alt.p;
+  uint32_t* vp = nullptr;
+  uint32_t* va = nullptr;
+  radix_sort<K, uint32_t>(ctx, &kp, &ka, &vp, &va, false, n, bits, true);
+  out.reserve(n + 1);
+  DBuf<uint64_t> cnt(ctx, 1);
+  reduce_runs<K, int32_t, false>(ctx, kp, nullptr, n, out.p, nullptr, cnt.p);
+  uint64_t r;
+  read_u64(ctx, cnt.p, &r, 1);
+  return r;
+}
+
+// Count via the warp-per-vertex kernel over a CSR built from sorted unique keys.
+template <class K>
+uint64_t tri_from_sorted(strata_ctx* ctx, const K* keys, uint64_t m, int bits, uint64_t n_nodes) {
+  DBuf<uint32_t> off(ctx, n_nodes + 1), nbr(ctx, m + 1);
+  build_csr<K>(ctx, keys, m, bits, n_nodes, off.p, nbr.p);
+  DBuf<uint64_t> acc(ctx, 2);
+  SK_CUDA(cudaMemsetAsync(acc.p, 0, 16, ctx->stream));
+  const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(n_nodes, TC_WARPS), (uint64_t)ctx->num_sms * 8);
+  k_tri_count<<<grid ? grid : 1, TC_NT, 0, ctx->stream>>>(off.p, nbr.p, n_nodes,
+                                                          reinterpret_cast<uint32_t*>(acc.p + 1),
+                                                          reinterpret_cast<unsigned long long*>(acc.p));
+  after_launch(ctx, "k_tri_count");
+  uint64_t r;
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, acc.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  sync_and_check(ctx);
+  r = ctx->h_scalar[0];
+  return r;
+}
+
+template <class K>
+uint64_t pattern_impl(strata_ctx* ctx, const uint32_t* x, const uint32_t* y, uint64_t n, int b,
+                      uint64_t n_nodes) {
+  DBuf<K> keys(ctx, n + 1), uniq;
+  uniq.ctx = ctx;
+  pack_pairs<K, int32_t, false>(ctx, x, y, nullptr, nullptr, n, b, keys.p, nullptr);
+  const uint64_t m = sort_unique<K>(ctx, keys, n, 2 * b, uniq);
+  return tri_from_sorted<K>(ctx, uniq.p, m, b, n_nodes);
+}
+
+// Canonicalize, dedup, drop self-loops, orient by (degree, id).  Leaves the
+// oriented sorted keys in `out` and returns their count.
+template <class K>
+uint64_t oriented_edges(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n, int bits,
+                        uint64_t n_nodes, bool by_degree, DBuf<K>& out) {
+  DBuf<K> keys(ctx, n + 1), uniq;
+  uniq.ctx = ctx;
+  k_canon<K><<<blocks(n), 256, 0, ctx->stream>>>(a, b, n, bits, keys.p);
+  after_launch(ctx, "k_canon");
+  uint64_t m = sort_unique<K>(ctx, keys, n, 2 * bits, uniq);
+  if (m) {
+    K last;
+    SK_CUDA(cudaMemcpyAsync(&last, uniq.p + (m - 1), sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
+    SK_CUDA(cudaStreamSynchronize(ctx->stream));
+    const K sent = (K)((K(1) << bits) - 1);
+    if (last == (K)((sent << bits) | sent)) m--;
+  }
+  if (!by_degree || m == 0) {
+    out = std::move(uniq);
+    return m;
+  }
+  DBuf<uint32_t> deg(ctx, n_nodes + 1);
+  SK_CUDA(cudaMemsetAsync(deg.p, 0, (n_nodes + 1) * 4, ctx->stream));
+  k_degree<K><<<blocks(m), 256, 0, ctx->stream>>>(uniq.p, m, bits, deg.p);
+  after_launch(ctx, "k_degree");
+  k_orient<K><<<blocks(m), 256, 0, ctx->stream>>>(uniq.p, m, bits, deg.p);
+  after_launch(ctx, "k_orient");
+  DBuf<K> alt(ctx, m + 1);
+  K* kp = uniq.p;
+  K* ka = alt.p;
+  uint32_t* vp = nullptr;
+  uint32_t* va = nullptr;
+  radix_sort<K, uint32_t>(ctx, &kp, &ka, &vp, &va, false, m, 2 * bits, true);
+  if (kp == uniq.p) out = std::move(uniq);
+  else out = std::move(alt);
+  return m;
+}
+
+template <class K>
+uint64_t tri_undirected_impl(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n, int bits,
+                             uint64_t n_nodes) {
+  DBuf<K> ori;
+  ori.ctx = ctx;
+  const uint64_t m = oriented_edges<K>(ctx, a, b, n, bits, n_nodes, true, ori);
+  if (m == 0) return 0;
+  return tri_from_sorted<K>(ctx, ori.p, m, bits, n_nodes);
+}
+
+template <class K>
+uint64_t k4_impl(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n, int bits, uint64_t n_nodes) {
+  DBuf<K> ori;
+  ori.ctx = ctx;
+  const uint64_t m = oriented_edges<K>(ctx, a, b, n, bits, n_nodes, true, ori);
+  if (m == 0) return 0;
+  DBuf<uint32_t> off(ctx, n_nodes + 1), nbr(ctx, m + 1), eu(ctx, m + 1), ev(ctx, m + 1);
+  build_csr<K>(ctx, ori.p, m, bits, n_nodes, off.p, nbr.p);
+  k_split<K><<<blocks(m), 256, 0, ctx->stream>>>(ori.p, m, bits, eu.p, ev.p);
+  after_launch(ctx, "k_split");
+  DBuf<uint64_t> acc(ctx, 1);
+  SK_CUDA(cudaMemsetAsync(acc.p, 0, 8, ctx->stream));
+  const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(m, 256), (uint64_t)ctx->num_sms * 8);
+  k_k4_count<<<grid ? grid : 1, 256, 0, ctx->stream>>>(eu.p, ev.p, m, off.p, nbr.p,
+                                                       reinterpret_cast<unsigned long long*>(acc.p));
+  after_launch(ctx, "k_k4_count");
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, acc.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  sync_and_check(ctx);
+  return ctx->h_scalar[0];
+}
+
+template <class K>
+uint64_t bpi_impl(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n, int bits, uint64_t n_nodes) {
+  DBuf<K> ori;
+  ori.ctx = ctx;
+  const uint64_t m = oriented_edges<K>(ctx, a, b, n, bits, n_nodes, false, ori);
+  if (m == 0) return 0;
+  DBuf<uint32_t> off(ctx, n_nodes + 1), nbr(ctx, m + 1);
+  build_csr<K>(ctx, ori.p, m, bits, n_nodes, off.p, nbr.p);
+  DBuf<uint64_t> acc(ctx, 1);
+  SK_CUDA(cudaMemsetAsync(acc.p, 0, 8, ctx->stream));
+  k_sum_sq_deg<<<blocks(n_nodes), 256, 0, ctx->stream>>>(off.p, n_nodes, reinterpret_cast<unsigned long long*>(acc.p));
+  after_launch(ctx, "k_sum_sq_deg");
+  uint64_t r;
+  read_u64(ctx, acc.p, &r, 1);
+  return r;
+}
+
+struct Ids {
+  int bits;
+  uint64_t n_nodes;
+};
+
+Ids id_space(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n) {
+  const uint32_t m = std::max(max_u32(ctx, a, n), max_u32(ctx, b, n));
+  return Ids{std::max(1, bits_for(m)), (uint64_t)m + 1};
+}
+
+}  // namespace
+
+uint64_t count_triangle_pattern(strata_ctx* ctx, const uint32_t* x, const uint32_t* y, uint64_t n) {
+  reset_status(ctx);
+  if (n == 0) return 0;
+  const Ids I = id_space(ctx, x, y, n);
+  if (2 * I.bits <= 32) return pattern_impl<uint32_t>(ctx, x, y, n, I.bits, I.n_nodes);
+  return pattern_impl<uint64_t>(ctx, x, y, n, I.bits, I.n_nodes);
+}
+
+uint64_t count_triangles_undirected(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n) {
+  reset_status(ctx);
+  if (n == 0) return 0;
+  const Ids I = id_space(ctx, a, b, n);
+  if (2 * I.bits <= 32) return tri_undirected_impl<uint32_t>(ctx, a, b, n, I.bits, I.n_nodes);
+  return tri_undirected_impl<uint64_t>(ctx, a, b, n, I.bits, I.n_nodes);
+}
+
+uint64_t count_4cliques_undirected(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n) {
+  reset_status(ctx);
+  if (n == 0) return 0;
+  const Ids I = id_space(ctx, a, b, n);
+  if (2 * I.bits <= 32) return k4_impl<uint32_t>(ctx, a, b, n, I.bits, I.n_nodes);
+  return k4_impl<uint64_t>(ctx, a, b, n, I.bits, I.n_nodes);
+}
+
+uint64_t binary_plan_intermediate(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n) {
+  reset_status(ctx);
+  if (n == 0) return 0;
+  const Ids I = id_space(ctx, a, b, n);
+  if (2 * I.bits <= 32) return bpi_impl<uint32_t>(ctx, a, b, n, I.bits, I.n_nodes);
+  return bpi_impl<uint64_t>(ctx, a, b, n, I.bits, I.n_nodes);
+}
+
+uint64_t intern_terms(strata_ctx* ctx, const uint64_t* keys, uint64_t n, uint32_t* ids) {
+  reset_status(ctx);
+  if (n == 0) return 0;
+  DBuf<uint64_t> mx(ctx, 1);
+  SK_CUDA(cudaMemsetAsync(mx.p, 0, 8, ctx->stream));
+  k_max_u64<<<(unsigned)std::min<uint64_t>(ceil_div(n, 256), (uint64_t)ctx->num_sms * 8), 256, 0, ctx->stream>>>(
+      keys, n, reinterpret_cast<unsigned long long*>(mx.p));
+  after_launch(ctx, "k_max_u64");
+  uint64_t maxk;
+  read_u64(ctx, mx.p, &maxk, 1);
+  DBuf<uint64_t> copy(ctx, n + 1), table;
+  table.ctx = ctx;
+  SK_CUDA(cudaMemcpyAsync(copy.p, keys, n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  const uint64_t m = sort_unique<uint64_t>(ctx, copy, n, std::max(1, bits_for(maxk)), table);
+  k_intern_map<<<blocks(n), 256, 0, ctx->stream>>>(keys, n, table.p, m, ids);
+  after_launch(ctx, "k_intern_map");
+  sync_and_check(ctx);
+  return m;
+}
+
+}  // namespace sk

@@ -1,0 +1,134 @@
+"""ctypes binding of ``libstrata_b200.so`` (the C ABI in include/strata_b200.h).
+
+The shared library is built in-tree by ``strata-k_b200/build.py``.  Loading
+fails loudly when it is missing: there is no CPU fallback anywhere in this
+package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libstrata_b200.so"
+
+# strata_status codes (include/strata_b200.h)
+OK = 0
+E_INVALID = 1
+E_OOM = 2
+E_CUDA = 3
+E_OVERFLOW = 4
+E_NEG_CYCLE = 5
+E_TIMEOUT = 6
+E_UNSUPPORTED = 7
+E_NOT_BUILT = 8
+E_WEIGHT_RANGE = 9
+
+STATUS_NAMES = {
+    OK: "OK", E_INVALID: "INVALID", E_OOM: "OOM", E_CUDA: "CUDA", E_OVERFLOW: "OVERFLOW",
+    E_NEG_CYCLE: "NEG_CYCLE", E_TIMEOUT: "TIMEOUT", E_UNSUPPORTED: "UNSUPPORTED",
+    E_NOT_BUILT: "NOT_BUILT", E_WEIGHT_RANGE: "WEIGHT_RANGE",
+}
+
+
+class FixStats(C.Structure):
+    """Mirror of ``strata_fix_stats``."""
+
+    _fields_ = [
+        ("rounds", C.c_uint64), ("candidates", C.c_uint64), ("result_tuples", C.c_uint64),
+        ("universe", C.c_uint64), ("key_bits", C.c_uint32), ("weight_bytes", C.c_uint32),
+        ("device_ms", C.c_double), ("sort_ms", C.c_double), ("join_ms", C.c_double),
+        ("diff_ms", C.c_double), ("merge_ms", C.c_double),
+        ("sort_bytes", C.c_uint64), ("join_bytes", C.c_uint64), ("diff_bytes", C.c_uint64),
+        ("merge_bytes", C.c_uint64),
+        ("sort_launches", C.c_uint32), ("join_launches", C.c_uint32),
+        ("diff_launches", C.c_uint32), ("merge_launches", C.c_uint32),
+        ("other_launches", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+u8p = C.POINTER(C.c_uint8)
+u32p = C.POINTER(C.c_uint32)
+u64p = C.POINTER(C.c_uint64)
+i64p = C.POINTER(C.c_int64)
+vp = C.c_void_p
+ctxp = C.c_void_p
+relp = C.c_void_p
+
+# Every exported symbol with (restype, argtypes); the CPU tests check that the
+# library exports exactly these names.
+SIGNATURES = {
+    "strata_version": (C.c_char_p, []),
+    "strata_ctx_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(ctxp)]),
+    "strata_ctx_destroy": (None, [ctxp]),
+    "strata_ctx_set_stream": (C.c_int, [ctxp, vp]),
+    "strata_last_error": (C.c_char_p, [ctxp]),
+    "strata_ctx_mem": (C.c_int, [ctxp, u64p, u64p]),
+    "strata_ctx_set_profiling": (C.c_int, [ctxp, C.c_int]),
+    "strata_ctx_launches": (C.c_uint64, [ctxp]),
+    "strata_free": (None, [vp]),
+    "strata_transitive_closure_bool": (
+        C.c_int, [ctxp, u32p, u32p, C.c_uint64, C.POINTER(u32p), C.POINTER(u32p), u64p,
+                  C.POINTER(FixStats)]),
+    "strata_shortest_paths_trop": (
+        C.c_int, [ctxp, u32p, u32p, i64p, u8p, C.c_uint64, C.POINTER(u32p), C.POINTER(u32p),
+                  C.POINTER(i64p), C.POINTER(u8p), u64p, C.POINTER(FixStats)]),
+    "strata_mssp_trop": (
+        C.c_int, [ctxp, u32p, i64p, u8p, C.c_uint64, u32p, u32p, i64p, u8p, C.c_uint64,
+                  C.POINTER(u32p), C.POINTER(u32p), C.POINTER(i64p), C.POINTER(u8p), u64p,
+                  C.POINTER(FixStats)]),
+    "strata_count_triangles": (C.c_int, [ctxp, u32p, u32p, C.c_uint64, u64p]),
+    "strata_count_4cliques": (C.c_int, [ctxp, u32p, u32p, C.c_uint64, u64p]),
+    "strata_count_triangle_pattern": (C.c_int, [ctxp, u32p, u32p, C.c_uint64, u64p]),
+    "strata_intern_terms": (C.c_int, [ctxp, u64p, C.c_uint64, u32p, u64p]),
+    "strata_binary_plan_intermediate": (C.c_int, [ctxp, u32p, u32p, C.c_uint64, u64p]),
+    "strata_tc_bool_dev": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.POINTER(relp), C.POINTER(FixStats)]),
+    "strata_trop_paths_dev": (
+        C.c_int, [ctxp, vp, vp, vp, vp, C.c_uint64, C.POINTER(relp), C.POINTER(FixStats)]),
+    "strata_mssp_trop_dev": (
+        C.c_int, [ctxp, vp, vp, vp, C.c_uint64, vp, vp, vp, vp, C.c_uint64, C.POINTER(relp),
+                  C.POINTER(FixStats)]),
+    "strata_count_triangle_pattern_dev": (C.c_int, [ctxp, vp, vp, C.c_uint64, u64p]),
+    "strata_rel_size": (C.c_int, [relp, u64p]),
+    "strata_rel_is_trop": (C.c_int, [relp, C.POINTER(C.c_int)]),
+    "strata_rel_to_host": (C.c_int, [ctxp, relp, u32p, u32p, i64p, u8p]),
+    "strata_rel_fingerprint": (C.c_int, [ctxp, relp, u64p]),
+    "strata_rel_free": (None, [ctxp, relp]),
+    "strata_op_sort": (C.c_int, [ctxp, C.c_int, C.c_int, vp, vp, vp, vp, C.c_uint64, C.c_int]),
+    "strata_op_dedup_diff": (C.c_int, [ctxp, C.c_int, vp, C.c_uint64, vp, C.c_uint64, vp, u64p]),
+    "strata_op_min_improve": (
+        C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp, u64p]),
+    "strata_op_merge": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class LibraryMissing(RuntimeError):
+    """The CUDA library was not built; the engine has no CPU path to fall back to."""
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load the engine library once (fails loudly if it is missing)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = Path(path) if path else LIB_PATH
+        if not p.exists():
+            raise LibraryMissing(
+                f"{p} not found: build it with `python strata-k_b200/build.py` "
+                "(there is no CPU fallback)")
+        lib = C.CDLL(str(p))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib

@@ -1,0 +1,442 @@
+"""The engine's public API, mirroring the reference GPU crate.
+
+Function names, argument meaning and error behaviour follow
+``strata-gpu/src/lib.rs:67-147``:
+
+* ``transitive_closure_bool(edges)``        (lib.rs:67, tc.rs:31)
+* ``shortest_paths_trop(edges)``            (lib.rs:84, trop.rs:51)
+* ``count_triangles(edges)``                (lib.rs:99, wcoj.rs:136)
+* ``count_4cliques(edges)``                 (lib.rs:114, wcoj.rs:166)
+* ``intern_terms(keys)``                    (lib.rs:133, sort.rs:206)
+* ``binary_plan_intermediate(edges)``       (lib.rs:140, wcoj.rs:190)
+
+plus the multi-source Trop fixpoint of the benchmark program
+(``mssp_trop``) and the count aggregate over a directed relation
+(``count_triangle_pattern``).  Inputs need not be sorted or deduplicated;
+outputs are sorted by ``(src, dst)``.  Errors raise :class:`GpuError`
+subclasses; a negative-weight cycle is :class:`NegativeWeightCycle` (the
+reference reports it as ``GpuError::Cuda("negative-weight cycle…")``,
+trop.rs:87-89) and a Trop overflow is :class:`TropOverflow` (the
+interpreter's ``EvalError::Overflow``, strata-eval/src/naive.rs:31).
+
+Every call runs on the GPU through ``libstrata_b200.so``; nothing here
+computes a result on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+
+POS_INF = float("inf")  # how +inf is shown in Python-level tuples
+
+
+class GpuError(Exception):
+    """Error from the GPU engine (mirror of ``GpuError``, strata-gpu/src/lib.rs:14)."""
+
+    code = L.E_CUDA
+
+
+class NotBuilt(GpuError):
+    """No CUDA device / library (``GpuError::NotBuilt``)."""
+
+    code = L.E_NOT_BUILT
+
+
+class Cuda(GpuError):
+    """A CUDA runtime failure (``GpuError::Cuda``)."""
+
+    code = L.E_CUDA
+
+
+class InvalidArgument(GpuError):
+    code = L.E_INVALID
+
+
+class OutOfMemory(GpuError):
+    code = L.E_OOM
+
+
+class TropOverflow(GpuError):
+    """Finite Trop ⊗ overflowed i64 (``EvalError::Overflow``)."""
+
+    code = L.E_OVERFLOW
+
+
+class NegativeWeightCycle(GpuError):
+    """Trop stratum exceeded the Bellman-Ford cap (``EvalError::NegativeWeightCycle``)."""
+
+    code = L.E_NEG_CYCLE
+
+
+class Timeout(GpuError):
+    code = L.E_TIMEOUT
+
+
+class Unsupported(GpuError):
+    code = L.E_UNSUPPORTED
+
+
+class WeightRange(GpuError):
+    """A finite weight equal to i64::MAX cannot be told from +inf on the device."""
+
+    code = L.E_WEIGHT_RANGE
+
+
+_ERRORS = {c.code: c for c in (NotBuilt, Cuda, InvalidArgument, OutOfMemory, TropOverflow,
+                               NegativeWeightCycle, Timeout, Unsupported, WeightRange)}
+
+
+def _raise(code: int, msg: str):
+    raise _ERRORS.get(code, GpuError)(f"{L.STATUS_NAMES.get(code, code)}: {msg}")
+
+
+@dataclass
+class TropRelation:
+    """A Trop relation: columns ``src, dst, w`` and ``inf`` (1 where w = +inf)."""
+
+    src: np.ndarray
+    dst: np.ndarray
+    w: np.ndarray
+    inf: np.ndarray
+    stats: dict = field(default_factory=dict)
+
+    def __len__(self) -> int:
+        return len(self.src)
+
+    def tuples(self) -> list[tuple[int, int, float | int]]:
+        return [(int(s), int(d), POS_INF if i else int(w))
+                for s, d, w, i in zip(self.src, self.dst, self.w, self.inf)]
+
+
+@dataclass
+class BoolRelation:
+    """A Bool relation: columns ``src, dst``."""
+
+    src: np.ndarray
+    dst: np.ndarray
+    stats: dict = field(default_factory=dict)
+
+    def __len__(self) -> int:
+        return len(self.src)
+
+    def tuples(self) -> list[tuple[int, int]]:
+        return list(zip(self.src.tolist(), self.dst.tolist()))
+
+
+def _u32(a) -> np.ndarray:
+    a = np.asarray(a)
+    if a.size and (a.min() < 0 or a.max() > 0xFFFFFFFF):
+        raise InvalidArgument("ids must fit in u32")
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _split_pairs(edges) -> tuple[np.ndarray, np.ndarray]:
+    if isinstance(edges, tuple) and len(edges) == 2 and not np.isscalar(edges[0]):
+        return _u32(edges[0]), _u32(edges[1])
+    a = np.asarray(list(edges) if not isinstance(edges, np.ndarray) else edges)
+    if a.size == 0:
+        return np.zeros(0, np.uint32), np.zeros(0, np.uint32)
+    a = a.reshape(-1, 2)
+    return _u32(a[:, 0]), _u32(a[:, 1])
+
+
+def _split_weighted(edges) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+    """(src, dst, w) triples; w may be POS_INF.  Or a tuple of 3/4 columns."""
+    if isinstance(edges, tuple) and len(edges) in (3, 4) and not np.isscalar(edges[0]):
+        s, d, w = _u32(edges[0]), _u32(edges[1]), np.ascontiguousarray(edges[2], dtype=np.int64)
+        inf = (np.ascontiguousarray(edges[3], dtype=np.uint8) if len(edges) == 4
+               else np.zeros(len(s), np.uint8))
+        return s, d, w, inf
+    rows = list(edges)
+    if not rows:
+        z = np.zeros(0, np.uint32)
+        return z, z, np.zeros(0, np.int64), np.zeros(0, np.uint8)
+    s = _u32([r[0] for r in rows])
+    d = _u32([r[1] for r in rows])
+    inf = np.array([1 if r[2] == POS_INF else 0 for r in rows], dtype=np.uint8)
+    w = np.array([0 if r[2] == POS_INF else int(r[2]) for r in rows], dtype=np.int64)
+    return s, d, w, inf
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class Engine:
+    """A context on one CUDA device (its own stream, byte cap, status word).
+
+    Not thread-safe; create one Engine per thread.  ``mem_cap`` bounds the
+    device bytes the engine may hold (0 = unbounded).
+    """
+
+    def __init__(self, device: int = 0, mem_cap: int = 0, profiling: bool = False):
+        self.lib = L.load()
+        ctx = L.ctxp()
+        rc = self.lib.strata_ctx_create(device, mem_cap, C.byref(ctx))
+        if rc != L.OK:
+            _raise(rc, "cannot create a context on CUDA device %d" % device)
+        self.ctx = ctx
+        self.device = device
+        if profiling:
+            self.lib.strata_ctx_set_profiling(self.ctx, 1)
+
+    # -- plumbing ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.strata_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != L.OK:
+            _raise(rc, self.lib.strata_last_error(self.ctx).decode(errors="replace"))
+
+    def set_stream(self, stream_handle: int | None):
+        """Run on an existing ``cudaStream_t`` (e.g. ``torch.cuda.Stream().cuda_stream``)."""
+        self._check(self.lib.strata_ctx_set_stream(self.ctx, C.c_void_p(stream_handle or 0)))
+
+    def set_profiling(self, on: bool):
+        self._check(self.lib.strata_ctx_set_profiling(self.ctx, 1 if on else 0))
+
+    def launches(self) -> int:
+        return int(self.lib.strata_ctx_launches(self.ctx))
+
+    def mem(self) -> tuple[int, int]:
+        a, b = C.c_uint64(), C.c_uint64()
+        self._check(self.lib.strata_ctx_mem(self.ctx, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def _take(self, p, n, dtype) -> np.ndarray:
+        """Copy a library-malloc'd buffer into numpy and free it."""
+        out = np.ctypeslib.as_array(p, shape=(n,)).copy() if n else np.zeros(0, dtype)
+        self.lib.strata_free(C.cast(p, C.c_void_p))
+        return out.astype(dtype, copy=False)
+
+    # -- whole fixpoints (host buffers) ------------------------------------
+    def transitive_closure_bool(self, edges) -> BoolRelation:
+        s, d = _split_pairs(edges)
+        os_, od = u32p(), u32p()
+        n = C.c_uint64()
+        st = L.FixStats()
+        self._check(self.lib.strata_transitive_closure_bool(
+            self.ctx, _ptr(s, C.c_uint32), _ptr(d, C.c_uint32), len(s), C.byref(os_), C.byref(od),
+            C.byref(n), C.byref(st)))
+        return BoolRelation(self._take(os_, n.value, np.uint32), self._take(od, n.value, np.uint32),
+                            st.as_dict())
+
+    def shortest_paths_trop(self, edges) -> TropRelation:
+        s, d, w, inf = _split_weighted(edges)
+        os_, od, ow, oi = u32p(), u32p(), i64p(), u8p()
+        n = C.c_uint64()
+        st = L.FixStats()
+        self._check(self.lib.strata_shortest_paths_trop(
+            self.ctx, _ptr(s, C.c_uint32), _ptr(d, C.c_uint32), _ptr(w, C.c_int64),
+            _ptr(inf, C.c_uint8), len(s), C.byref(os_), C.byref(od), C.byref(ow), C.byref(oi),
+            C.byref(n), C.byref(st)))
+        m = n.value
+        return TropRelation(self._take(os_, m, np.uint32), self._take(od, m, np.uint32),
+                            self._take(ow, m, np.int64), self._take(oi, m, np.uint8), st.as_dict())
+
+    def mssp_trop(self, sources, edges, source_weights=None, source_inf=None) -> TropRelation:
+        """dist(S,Y) :- src(S), edge(S,Y).  dist(S,Z) :- dist(S,Y), edge(Y,Z)."""
+        src = _u32(sources)
+        sw = None if source_weights is None else np.ascontiguousarray(source_weights, dtype=np.int64)
+        si = None if source_inf is None else np.ascontiguousarray(source_inf, dtype=np.uint8)
+        s, d, w, inf = _split_weighted(edges)
+        os_, od, ow, oi = u32p(), u32p(), i64p(), u8p()
+        n = C.c_uint64()
+        st = L.FixStats()
+        self._check(self.lib.strata_mssp_trop(
+            self.ctx, _ptr(src, C.c_uint32), None if sw is None else _ptr(sw, C.c_int64),
+            None if si is None else _ptr(si, C.c_uint8), len(src),
+            _ptr(s, C.c_uint32), _ptr(d, C.c_uint32), _ptr(w, C.c_int64), _ptr(inf, C.c_uint8),
+            len(s), C.byref(os_), C.byref(od), C.byref(ow), C.byref(oi), C.byref(n), C.byref(st)))
+        m = n.value
+        return TropRelation(self._take(os_, m, np.uint32), self._take(od, m, np.uint32),
+                            self._take(ow, m, np.int64), self._take(oi, m, np.uint8), st.as_dict())
+
+    def _count(self, fn, edges) -> int:
+        a, b = _split_pairs(edges)
+        out = C.c_uint64()
+        self._check(fn(self.ctx, _ptr(a, C.c_uint32), _ptr(b, C.c_uint32), len(a), C.byref(out)))
+        return int(out.value)
+
+    def count_triangles(self, edges) -> int:
+        return self._count(self.lib.strata_count_triangles, edges)
+
+    def count_4cliques(self, edges) -> int:
+        return self._count(self.lib.strata_count_4cliques, edges)
+
+    def count_triangle_pattern(self, edges) -> int:
+        return self._count(self.lib.strata_count_triangle_pattern, edges)
+
+    def binary_plan_intermediate(self, edges) -> int:
+        return self._count(self.lib.strata_binary_plan_intermediate, edges)
+
+    def intern_terms(self, keys) -> np.ndarray:
+        k = np.ascontiguousarray(keys, dtype=np.uint64)
+        ids = np.zeros(len(k), np.uint32)
+        nd = C.c_uint64()
+        self._check(self.lib.strata_intern_terms(self.ctx, _ptr(k, C.c_uint64), len(k),
+                                                 _ptr(ids, C.c_uint32), C.byref(nd)))
+        return ids
+
+    # -- device-resident fixpoints (torch tensors or raw device pointers) ----
+    def tc_bool_dev(self, src, dst, n=None) -> "DeviceRelation":
+        n = _len(src) if n is None else n
+        rel = L.relp()
+        st = L.FixStats()
+        self._check(self.lib.strata_tc_bool_dev(self.ctx, _dp(src), _dp(dst), n, C.byref(rel), C.byref(st)))
+        return DeviceRelation(self, rel, st.as_dict())
+
+    def trop_paths_dev(self, src, dst, w, inf=None, n=None) -> "DeviceRelation":
+        n = _len(src) if n is None else n
+        rel = L.relp()
+        st = L.FixStats()
+        self._check(self.lib.strata_trop_paths_dev(self.ctx, _dp(src), _dp(dst), _dp(w), _dp(inf), n,
+                                                   C.byref(rel), C.byref(st)))
+        return DeviceRelation(self, rel, st.as_dict())
+
+    def mssp_dev(self, sources, esrc, edst, ew, source_weights=None, source_inf=None, einf=None,
+                 n_sources=None, n_edges=None) -> "DeviceRelation":
+        ns = _len(sources) if n_sources is None else n_sources
+        ne = _len(esrc) if n_edges is None else n_edges
+        rel = L.relp()
+        st = L.FixStats()
+        self._check(self.lib.strata_mssp_trop_dev(
+            self.ctx, _dp(sources), _dp(source_weights), _dp(source_inf), ns, _dp(esrc), _dp(edst),
+            _dp(ew), _dp(einf), ne, C.byref(rel), C.byref(st)))
+        return DeviceRelation(self, rel, st.as_dict())
+
+    def count_triangle_pattern_dev(self, x, y, n=None) -> int:
+        n = _len(x) if n is None else n
+        out = C.c_uint64()
+        self._check(self.lib.strata_count_triangle_pattern_dev(self.ctx, _dp(x), _dp(y), n, C.byref(out)))
+        return int(out.value)
+
+
+def _dp(t) -> C.c_void_p | None:
+    """Device pointer of a torch tensor (or an int), None for None."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return C.c_void_p(t)
+    return C.c_void_p(t.data_ptr())
+
+
+def _len(t) -> int:
+    return int(t.numel()) if hasattr(t, "numel") else len(t)
+
+
+class DeviceRelation:
+    """A fixpoint result held on the device (``strata_rel``)."""
+
+    def __init__(self, eng: Engine, rel, stats: dict):
+        self.eng, self.rel, self.stats = eng, rel, stats
+
+    def __len__(self) -> int:
+        n = C.c_uint64()
+        self.eng._check(self.eng.lib.strata_rel_size(self.rel, C.byref(n)))
+        return int(n.value)
+
+    @property
+    def is_trop(self) -> bool:
+        t = C.c_int()
+        self.eng._check(self.eng.lib.strata_rel_is_trop(self.rel, C.byref(t)))
+        return bool(t.value)
+
+    def fingerprint(self) -> int:
+        fp = C.c_uint64()
+        self.eng._check(self.eng.lib.strata_rel_fingerprint(self.eng.ctx, self.rel, C.byref(fp)))
+        return int(fp.value)
+
+    def to_host(self, out=None):
+        """Copy out; ``out`` may supply (pinned) numpy arrays to copy into."""
+        n = len(self)
+        trop = self.is_trop
+        if out is None:
+            s = np.zeros(n, np.uint32)
+            d = np.zeros(n, np.uint32)
+            w = np.zeros(n, np.int64) if trop else None
+            i = np.zeros(n, np.uint8) if trop else None
+        else:
+            s, d, w, i = out
+        self.eng._check(self.eng.lib.strata_rel_to_host(
+            self.eng.ctx, self.rel, _ptr(s, C.c_uint32), _ptr(d, C.c_uint32),
+            _ptr(w, C.c_int64) if w is not None else None, _ptr(i, C.c_uint8) if i is not None else None))
+        if trop:
+            return TropRelation(s[:n], d[:n], w[:n], i[:n], dict(self.stats))
+        return BoolRelation(s[:n], d[:n], dict(self.stats))
+
+    def free(self):
+        if self.rel:
+            self.eng.lib.strata_rel_free(self.eng.ctx, self.rel)
+            self.rel = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ---- module-level functions with the reference's names -----------------------
+_default: dict[int, Engine] = {}
+_dlock = threading.Lock()
+
+
+def default_engine(device: int = 0) -> Engine:
+    """A process-wide engine per device (the reference keeps one `CudaDevice`
+    per module in a OnceLock, strata-gpu/src/sort.rs:221-254)."""
+    with _dlock:
+        if device not in _default:
+            _default[device] = Engine(device)
+        return _default[device]
+
+
+def transitive_closure_bool(edges) -> BoolRelation:
+    return default_engine().transitive_closure_bool(edges)
+
+
+def shortest_paths_trop(edges) -> TropRelation:
+    return default_engine().shortest_paths_trop(edges)
+
+
+def mssp_trop(sources, edges, source_weights=None) -> TropRelation:
+    return default_engine().mssp_trop(sources, edges, source_weights)
+
+
+def count_triangles(edges) -> int:
+    return default_engine().count_triangles(edges)
+
+
+def count_4cliques(edges) -> int:
+    return default_engine().count_4cliques(edges)
+
+
+def count_triangle_pattern(edges) -> int:
+    return default_engine().count_triangle_pattern(edges)
+
+
+def intern_terms(keys) -> np.ndarray:
+    return default_engine().intern_terms(keys)
+
+
+def binary_plan_intermediate(edges) -> int:
+    return default_engine().binary_plan_intermediate(edges)
