@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Benchmark: derived tuples/s of the semi-naive fixpoint on B200.
+
+Workload (default): the Trop multi-source shortest-path program
+
+    dist(S,Y) :- src(S), edge(S,Y).
+    dist(S,Z) :- dist(S,Y), edge(Y,Z).        (min-plus)
+
+on a seeded R-MAT scale-20 graph (1,048,576 node ids, 8,388,608 distinct
+directed edges, a=0.57 b=c=0.19), i64 weights U[1,100], 64 sources.  One
+step = the whole fixpoint from the resident EDB to the final `dist`
+relation.  metric = |dist| / device time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs its own instance (its own graph seed and
+sources; no data-path collective) and `value` sums tuples over ranks divided
+by the max rank time ("scaling": "weak").  `--impl reference` times the
+reference interpreter's algorithm (the CPU restatement in oracle/, nested
+loop `solve`, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT / "strata-k_b200"), str(ROOT / "oracle")]
+
+import numpy as np  # noqa: E402
+
+METRIC = "derived tuples/s (Trop MSSP fixpoint, |dist| / device time)"
+UNIT = "tuples/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--sources", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--out", default=None, help="also write the JSON line here")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_for(rank: int, scale: int, n_sources: int):
+    from strata_b200 import gen
+    return gen.mssp_workload(scale=scale, n_sources=n_sources, seed=2 + 1000 * rank)
+
+
+def config(args, world):
+    return {
+        "workload": f"trop_mssp_rmat{args.scale}_{args.sources}src",
+        "program": "dist(S,Y) :- src(S), edge(S,Y). dist(S,Z) :- dist(S,Y), edge(Y,Z). (Trop)",
+        "graph": f"R-MAT scale {args.scale}, {8 << args.scale} distinct directed edges, "
+                 "a=0.57 b=0.19 c=0.19, i64 weights U[1,100]",
+        "sources": args.sources,
+        "parallelism": f"replicas{world}",
+        "l2": "flushed (256 MiB write) before every timed step",
+    }
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (read-only queries)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_sample(wl, threads: int, n_sample_sources: int, steps: int):
+    """The reference interpreter's algorithm (oracle restatement) on a bounded
+    sample: the bootstrap round of the same program on the full graph for the
+    first `n_sample_sources` sources.  Returns (tuples/s, seconds/step, tuples)."""
+    import oracle as O
+    srcs = wl.sources[:n_sample_sources]
+    sess = O.Session(O.mssp_program(srcs, wl.src, wl.dst, wl.w, wl.source_w[:n_sample_sources]))
+    rates, secs_all, tup = [], [], 0
+    for _ in range(steps):
+        counts, _, secs = sess.run(threads=threads, max_rounds=0)
+        tup = counts["dist"]
+        rates.append(tup / secs if secs > 0 else 0.0)
+        secs_all.append(secs)
+    sess.close()
+    return rates, secs_all, tup
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    wl = workload_for(0, args.scale, args.sources)
+    n_s = min(16, len(wl.sources))
+    t0 = time.time()
+    rates, secs, tup = cpu_sample(wl, cores, n_s, args.warmup + args.steps)
+    timed = secs[args.warmup:]
+    value = tup * len(timed) / sum(timed) if sum(timed) > 0 else 0.0
+    sample = (f"bootstrap round (all derivations of dist(S,Y) :- src(S), edge(S,Y) by the nested-loop "
+              f"solve) for {n_s} of the {len(wl.sources)} sources on the full graph; {tup} tuples per step")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(timed) / max(1, len(timed)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic", "config": config(args, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.time() - t0,
+    }
+    print(json.dumps(line), flush=True)
+    if args.out:
+        Path(args.out).write_text(json.dumps(line) + "\n")
+    return 0
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+
+    import strata_b200 as S
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    wl = workload_for(rank, args.scale, args.sources)
+    eng = S.Engine(local)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+
+    def dev(a, dt):
+        return torch.from_numpy(np.ascontiguousarray(a).astype(dt))
+
+    host = {k: dev(v, dt).pin_memory() for k, v, dt in (
+        ("sources", wl.sources, np.int32), ("sw", wl.source_w, np.int64), ("src", wl.src, np.int32),
+        ("dst", wl.dst, np.int32), ("w", wl.w, np.int64))}
+    with torch.cuda.stream(stream):
+        d = {k: v.to("cuda", non_blocking=True) for k, v in host.items()}
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+    stream.synchronize()
+
+    def step():
+        rel = eng.mssp_dev(d["sources"], d["src"], d["dst"], d["w"], source_weights=d["sw"])
+        return rel
+
+    for _ in range(args.warmup):
+        step().free()
+    # ---- timed region: device-only fixpoints (inputs resident in HBM)
+    eng.set_profiling(True)
+    eng.reset_kernel_stats()
+    clocks = ClockSampler(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = eng.launches()
+    total_ms, tuples, stats = 0.0, 0, None
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)  # L2 flush outside the timed interval
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rel = step()
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        tuples = len(rel)
+        stats = rel.stats
+        rel.free()
+    torch.cuda.synchronize()
+    launches = eng.launches() - launches0
+    clk = clocks.stop()
+    kstats = eng.kernel_stats()
+    eng.set_profiling(False)
+    if pg:
+        t = torch.tensor([total_ms, float(tuples)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        pg.all_reduce(mx, op=pg.ReduceOp.MAX)
+        sm = t.clone()
+        pg.all_reduce(sm, op=pg.ReduceOp.SUM)
+        max_ms, all_tuples = float(mx[0]), float(sm[1])
+    else:
+        max_ms, all_tuples = total_ms, float(tuples)
+    ms_per_step = max_ms / args.steps
+    value = all_tuples * args.steps / (max_ms / 1000.0)
+
+    # ---- e2e: pinned host inputs -> device -> fixpoint -> result on the host
+    e2e = None
+    if not args.no_e2e:
+        n_out = tuples
+        out_host = (torch.empty(n_out, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                    torch.empty(n_out, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                    torch.empty(n_out, dtype=torch.int64).pin_memory().numpy(),
+                    torch.empty(n_out, dtype=torch.uint8).pin_memory().numpy())
+        h2d = sum(v.numel() * v.element_size() for v in host.values())
+        e2e_ms = 0.0
+        for i in range(args.steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            with torch.cuda.stream(stream):
+                dd = {k: v.to("cuda", non_blocking=True) for k, v in host.items()}
+            rel = eng.mssp_dev(dd["sources"], dd["src"], dd["dst"], dd["w"], source_weights=dd["sw"])
+            res = rel.to_host(out=out_host)
+            t1 = time.perf_counter()
+            rel.free()
+            del dd
+            if i > 0:  # first iteration is a warm-up
+                e2e_ms += 1000 * (t1 - t0)
+        d2h = n_out * (4 + 4 + 8 + 1)
+        e2e_val = tuples * args.steps / (e2e_ms / 1000.0)
+        if pg:
+            t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_val = all_tuples * args.steps / (float(t[0]) / 1000.0)
+        e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h),
+               "path": "pinned host columns -> torch H2D -> strata_mssp_trop_dev -> strata_rel_to_host (pinned)"}
+        assert len(res) == tuples
+
+    # ---- roofline of the dominant kernel
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dom = max(kstats.items(), key=lambda kv: kv[1][1])
+    name, (kl, kms, kbytes) = dom
+    achieved = (kbytes / kl) / ((kms / kl) / 1000.0) / 1e9 if kl and kms else 0.0
+    roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_source": peak_src,
+            "unit": "GB/s", "frac": achieved / peak if peak else None,
+            "traffic": None, "launches_per_step": kl / args.steps,
+            "avg_launch_us": 1000 * kms / kl if kl else None,
+            "algorithmic_bytes_per_launch": kbytes / kl if kl else None,
+            "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
+                            "gbs": (v[2] / (v[1] / 1000.0) / 1e9) if v[1] else None}
+                        for k, v in kstats.items() if v[0]}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        n_s = min(16, len(wl.sources))
+        rates, secs, tup = cpu_sample(wl, cores, n_s, 1)
+        cpu = {"value": rates[-1], "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"reference interpreter algorithm (oracle restatement, nested-loop solve) on the "
+                         f"bootstrap round for {n_s} of {len(wl.sources)} sources, full graph: {tup} tuples "
+                         f"in {secs[-1]:.2f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32" if stats["weight_bytes"] == 4 else "int64",
+            "data": "synthetic", "config": config(args, world),
+            "tuples_per_step": int(all_tuples), "rounds": stats["rounds"],
+            "candidates_per_step": stats["candidates"], "key_bits": stats["key_bits"],
+            "weight_bytes": stats["weight_bytes"],
+            "phase_ms": {k: round(stats[k + "_ms"], 3) for k in ("join", "sort", "diff", "merge")},
+            "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+        if args.out:
+            Path(args.out).write_text(json.dumps(line) + "\n")
+    eng.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -85,6 +85,13 @@ strata_status strata_ctx_mem(const strata_ctx* ctx, uint64_t* in_use, uint64_t* 
 strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled);
 /* Number of kernels this context launched so far (monotone counter). */
 uint64_t strata_ctx_launches(const strata_ctx* ctx);
+/* Per-kernel accounting collected while profiling is on: launches, summed
+ * CUDA-event duration and algorithmic bytes moved.  Kernel ids:
+ * 0 radix pass, 1 expand emit, 2 expand offsets, 3 run reduction,
+ * 4 merge/diff, 5 radix histogram, 6 triangle count. */
+strata_status strata_ctx_kernel_stats(strata_ctx* ctx, int kernel, uint64_t* launches,
+                                      double* ms, uint64_t* bytes);
+strata_status strata_ctx_reset_kernel_stats(strata_ctx* ctx);
 /* Release memory returned by the library. */
 void strata_free(void* p);
 const char* strata_version(void);

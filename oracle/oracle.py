@@ -54,6 +54,12 @@ def lib() -> C.CDLL:
         L.sko_interp.argtypes = [i64p, C.c_size_t, C.c_int, C.c_int, C.c_long,
                                  C.POINTER(i64p), C.POINTER(C.c_size_t), C.POINTER(C.c_long)]
         L.sko_free.argtypes = [C.c_void_p]
+        L.sko_session_new.restype = C.c_void_p
+        L.sko_session_new.argtypes = [i64p, C.c_size_t]
+        L.sko_session_run.restype = C.c_int
+        L.sko_session_run.argtypes = [C.c_void_p, C.c_int, C.c_long, i64p, C.POINTER(C.c_long),
+                                      C.POINTER(C.c_double)]
+        L.sko_session_free.argtypes = [C.c_void_p]
         L.sko_fast_tc.restype = C.c_int
         L.sko_fast_tc.argtypes = [u32p, u32p, C.c_size_t, C.POINTER(u32p), C.POINTER(u32p),
                                   C.POINTER(C.c_size_t), C.POINTER(C.c_long)]
@@ -258,6 +264,40 @@ class Prog:
             pos += cnt * width
             db[name] = rows
         return db, int(rounds.value)
+
+
+class Session:
+    """A program loaded once into the interpreter; ``run`` re-evaluates it
+    from the EDB and returns ({pred: count}, rounds, seconds)."""
+
+    def __init__(self, prog: "Prog"):
+        self.prog = prog
+        b = prog.blob()
+        self.h = lib().sko_session_new(_p(b, C.c_int64), len(b))
+        if not self.h:
+            raise OracleError(15)
+
+    def run(self, threads=1, max_rounds=-1):
+        counts = np.zeros(len(self.prog.preds), np.int64)
+        rounds = C.c_long(0)
+        secs = C.c_double(0)
+        rc = lib().sko_session_run(self.h, threads, max_rounds, _p(counts, C.c_int64), C.byref(rounds),
+                                   C.byref(secs))
+        if rc not in (OK, E_ROUND_LIMIT):
+            raise OracleError(rc)
+        return ({p[0]: int(c) for p, c in zip(self.prog.preds, counts)}, int(rounds.value),
+                float(secs.value))
+
+    def close(self):
+        if self.h:
+            lib().sko_session_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def tc_program(src, dst) -> Prog:

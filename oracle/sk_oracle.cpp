@@ -21,6 +21,7 @@
 //      order-independent fingerprints (same mixing as the device's).
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <functional>
@@ -301,6 +302,33 @@ struct Interp {
     }
   }
 
+  // The literal at `pos` ranges over `rows`, split across threads; each
+  // thread runs the identical nested loop on its slice (same derivations).
+  template <class Emit>
+  void par_solve(const Rule& r, Ann id, int pos, const std::vector<std::pair<Tuple, Ann>>& rows,
+                 int threads, Emit& emit) {
+    const int T = std::min<int>(threads, (int)rows.size());
+    std::vector<std::vector<std::pair<Tuple, Ann>>> parts(T);
+    for (size_t k = 0; k < rows.size(); k++) parts[k % T].push_back(rows[k]);
+    std::vector<std::vector<std::pair<Binding2, Ann>>> outs(T);
+    std::vector<int> errs(T, 0);
+    std::vector<std::thread> th;
+    for (int q = 0; q < T; q++) {
+      th.emplace_back([&, q]() {
+        try {
+          Binding2 b((size_t)r.var_count);
+          solve(r.body, 0, b, id, pos, &parts[q], outs[q]);
+        } catch (const EvalError& e) {
+          errs[q] = e.code;
+        }
+      });
+    }
+    for (auto& t : th) t.join();
+    for (int q = 0; q < T; q++)
+      if (errs[q]) throw EvalError{errs[q]};
+    for (int q = 0; q < T; q++) emit(outs[q]);
+  }
+
   // One semi-naive round (seminaive.rs:114-210).  `idb` non-null = delta round.
   using Delta = std::vector<std::vector<std::pair<Tuple, Ann>>>;
   Delta apply_round(int stratum, const std::vector<char>* idb, const Delta* delta, int threads) {
@@ -312,10 +340,18 @@ struct Interp {
         for (auto& s : solved) derived.emplace_back(r.head.pred, ground(r.head.args, s.first, false), s.second);
       };
       if (!idb) {
-        std::vector<std::pair<Binding2, Ann>> solved;
-        Binding2 b((size_t)r.var_count);
-        solve(r.body, 0, b, id, -1, nullptr, solved);
-        emit(solved);
+        if (threads > 1 && !r.body.empty() && !r.body[0].neg && db[r.body[0].atom.pred].rows.size() > 1) {
+          // Scanning the first literal's relation row by row is the same
+          // nested loop; its rows are split across threads.
+          std::vector<std::pair<Tuple, Ann>> rows(db[r.body[0].atom.pred].rows.begin(),
+                                                  db[r.body[0].atom.pred].rows.end());
+          par_solve(r, id, 0, rows, threads, emit);
+        } else {
+          std::vector<std::pair<Binding2, Ann>> solved;
+          Binding2 b((size_t)r.var_count);
+          solve(r.body, 0, b, id, -1, nullptr, solved);
+          emit(solved);
+        }
       } else {
         for (size_t i = 0; i < r.body.size(); i++) {
           const Lit& l = r.body[i];
@@ -328,28 +364,7 @@ struct Interp {
             solve(r.body, 0, b, id, (int)i, &rows, solved);
             emit(solved);
           } else {
-            // The delta literal's rows are split across threads; each thread
-            // runs the identical nested loop on its slice (same derivations).
-            const int T = std::min<int>(threads, (int)rows.size());
-            std::vector<std::vector<std::pair<Tuple, Ann>>> parts(T);
-            for (size_t k = 0; k < rows.size(); k++) parts[k % T].push_back(rows[k]);
-            std::vector<std::vector<std::pair<Binding2, Ann>>> outs(T);
-            std::vector<int> errs(T, 0);
-            std::vector<std::thread> th;
-            for (int q = 0; q < T; q++) {
-              th.emplace_back([&, q]() {
-                try {
-                  Binding2 b((size_t)r.var_count);
-                  solve(r.body, 0, b, id, (int)i, &parts[q], outs[q]);
-                } catch (const EvalError& e) {
-                  errs[q] = e.code;
-                }
-              });
-            }
-            for (auto& t : th) t.join();
-            for (int q = 0; q < T; q++)
-              if (errs[q]) throw EvalError{errs[q]};
-            for (int q = 0; q < T; q++) emit(outs[q]);
+            par_solve(r, id, (int)i, rows, threads, emit);
           }
         }
       }
@@ -546,6 +561,95 @@ int sko_interp(const int64_t* blob, size_t n, int mode, int threads, long max_ro
 }
 
 void sko_free(void* p) { free(p); }
+
+// A loaded program kept between runs (the timed CPU baseline re-runs the
+// fixpoint without re-loading the EDB).  Each run starts from the EDB alone.
+struct SkoSession {
+  Program P;
+  std::vector<Relation> edb;
+};
+
+static Program decode_program(Reader& R, std::vector<Relation>* edb_out) {
+  Program P;
+  const int np = (int)R.next();
+  for (int k = 0; k < np; k++) {
+    Pred p;
+    p.arity = (int)R.next();
+    p.trop = R.next() != 0;
+    p.stratum = (int)R.next();
+    P.preds.push_back(p);
+  }
+  P.num_strata = (int)R.next();
+  const int nr = (int)R.next();
+  for (int k = 0; k < nr; k++) {
+    Rule r;
+    r.var_count = (int)R.next();
+    r.head = read_atom(R);
+    r.agg_op = (int)R.next();
+    r.agg_slot = (int)R.next();
+    r.agg_pos = (int)R.next();
+    const int nb = (int)R.next();
+    for (int q = 0; q < nb; q++) {
+      Lit l;
+      l.neg = R.next() != 0;
+      l.atom = read_atom(R);
+      r.body.push_back(l);
+    }
+    P.rules.push_back(r);
+  }
+  edb_out->clear();
+  for (auto& pr : P.preds) edb_out->push_back(Relation{pr.trop, {}});
+  const long nf = (long)R.next();
+  for (long k = 0; k < nf; k++) {
+    const int pred = (int)R.next();
+    const int ar = (int)R.next();
+    Tuple t;
+    for (int q = 0; q < ar; q++) {
+      GV g;
+      g.tag = (uint8_t)R.next();
+      g.v = R.next();
+      t.push_back(g);
+    }
+    const int wk = (int)R.next();
+    const int64_t wv = R.next();
+    Ann a = wk == 0 ? Ann{false, Weight{false, 0}} : Ann{true, Weight{wk == 2, wk == 2 ? 0 : wv}};
+    if (a.trop != P.preds[pred].trop) throw EvalError{E_ANN_MISMATCH};
+    (*edb_out)[pred].combine(t, a);
+  }
+  return P;
+}
+
+void* sko_session_new(const int64_t* blob, size_t n) {
+  try {
+    Reader R{blob, 0, n};
+    auto* s = new SkoSession();
+    s->P = decode_program(R, &s->edb);
+    return s;
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+// Run the semi-naive fixpoint (at most max_rounds delta rounds; < 0 = all)
+// from the session's EDB.  counts[k] = |relation k| afterwards; *secs = the
+// wall time of run_semi_naive itself (the EDB copy is not timed).
+int sko_session_run(void* h, int threads, long max_rounds, int64_t* counts, long* rounds, double* secs) {
+  auto* s = static_cast<SkoSession*>(h);
+  try {
+    Interp I(s->P);
+    I.db = s->edb;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = I.run_semi_naive(threads, max_rounds, rounds);
+    const auto t1 = std::chrono::steady_clock::now();
+    *secs = std::chrono::duration<double>(t1 - t0).count();
+    for (size_t k = 0; k < s->P.preds.size(); k++) counts[k] = (int64_t)I.db[k].rows.size();
+    return rc;
+  } catch (const EvalError& e) {
+    return e.code;
+  }
+}
+
+void sko_session_free(void* h) { delete static_cast<SkoSession*>(h); }
 
 }  // extern "C"
 

@@ -129,6 +129,8 @@ void strata_ctx_destroy(strata_ctx* ctx) {
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
   if (ctx->h_scalar) cudaFreeHost(ctx->h_scalar);
+  for (auto& r : ctx->krecs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  for (auto e : ctx->event_pool) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -166,6 +168,24 @@ strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled) {
 }
 
 uint64_t strata_ctx_launches(const strata_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+strata_status strata_ctx_kernel_stats(strata_ctx* ctx, int kernel, uint64_t* launches, double* ms,
+                                      uint64_t* bytes) {
+  if (!ctx || kernel < 0 || kernel >= sk::K_NUM) return STRATA_E_INVALID;
+  sk::kprof_collect(ctx);
+  const auto& g = ctx->kagg[kernel];
+  if (launches) *launches = g.launches;
+  if (ms) *ms = g.ms;
+  if (bytes) *bytes = g.bytes;
+  return STRATA_OK;
+}
+
+strata_status strata_ctx_reset_kernel_stats(strata_ctx* ctx) {
+  if (!ctx) return STRATA_E_INVALID;
+  sk::kprof_collect(ctx);
+  for (auto& g : ctx->kagg) g = strata_ctx::KAgg();
+  return STRATA_OK;
+}
 
 void strata_free(void* p) { std::free(p); }
 

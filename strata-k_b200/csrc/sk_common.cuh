@@ -74,6 +74,12 @@ struct strata_ctx {
   int num_sms = 148;
   bool profiling = false;
   uint64_t launches = 0;
+  // Per-kernel CUDA-event accounting (enabled with profiling).
+  struct KRec { int kid; cudaEvent_t a, b; uint64_t bytes; };
+  std::vector<KRec> krecs;
+  std::vector<cudaEvent_t> event_pool;
+  struct KAgg { uint64_t launches = 0; double ms = 0; uint64_t bytes = 0; };
+  KAgg kagg[16];
 };
 
 namespace sk {
@@ -206,6 +212,66 @@ inline int bits_for(uint64_t max_value) {  // bits needed to hold 0..max_value
   int b = 0;
   while (b < 64 && (max_value >> b) != 0) b++;
   return b;
+}
+
+// ---- per-kernel timing ----------------------------------------------------------
+// Kernel ids reported by strata_ctx_kernel_stats.
+enum KernelId : int {
+  K_ONESWEEP = 0,
+  K_EXPAND_EMIT = 1,
+  K_EXPAND_OFFSETS = 2,
+  K_REDUCE_RUNS = 3,
+  K_MERGE_DIFF = 4,
+  K_RADIX_HIST = 5,
+  K_TRI_COUNT = 6,
+  K_NUM = 7,
+};
+
+inline cudaEvent_t take_event(strata_ctx* ctx) {
+  if (!ctx->event_pool.empty()) {
+    cudaEvent_t e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+  return e;
+}
+
+// Returns a handle (or -1 when profiling is off); record the launch between
+// kprof_begin and kprof_end.  `bytes` are the algorithmic bytes of the launch.
+inline int kprof_begin(strata_ctx* ctx, int kid) {
+  if (!ctx->profiling) return -1;
+  strata_ctx::KRec r{kid, take_event(ctx), take_event(ctx), 0};
+  check_cuda(cudaEventRecord(r.a, ctx->stream), "cudaEventRecord");
+  ctx->krecs.push_back(r);
+  return (int)ctx->krecs.size() - 1;
+}
+inline void kprof_end(strata_ctx* ctx, int h, uint64_t bytes) {
+  if (h < 0) return;
+  ctx->krecs[h].bytes = bytes;
+  check_cuda(cudaEventRecord(ctx->krecs[h].b, ctx->stream), "cudaEventRecord");
+}
+// Add output bytes (known only after a count read-back) to the most recent
+// record of kernel `kid`.
+inline void kprof_add_last(strata_ctx* ctx, int kid, uint64_t bytes) {
+  for (auto it = ctx->krecs.rbegin(); it != ctx->krecs.rend(); ++it)
+    if (it->kid == kid) { it->bytes += bytes; return; }
+}
+// Fold finished records into the aggregates (synchronizes on the events).
+inline void kprof_collect(strata_ctx* ctx) {
+  for (auto& r : ctx->krecs) {
+    float ms = 0;
+    if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      auto& g = ctx->kagg[r.kid];
+      g.launches++;
+      g.ms += ms;
+      g.bytes += r.bytes;
+    }
+    ctx->event_pool.push_back(r.a);
+    ctx->event_pool.push_back(r.b);
+  }
+  ctx->krecs.clear();
 }
 
 // ---- phase timing -------------------------------------------------------------

@@ -122,7 +122,7 @@ uint64_t derive(strata_ctx* ctx, const K* dk, const W* dw, uint64_t nd, const Cs
     s.cw2.reserve_grow(T);
   }
   expand_emit<K, W, TROP>(ctx, dk, dw, nd, s.pos.p, T, js.jshift, js.jmask, js.pshift, js.pmask,
-                          js.out_pshift, js.out_vshift, csr.off.p, csr.n_nodes, csr.nbr.p,
+                          js.out_pshift, js.out_vshift, csr.off.p, csr.n_nodes, csr.nbr.p, csr.m,
                           TROP ? csr.w.p : nullptr, s.ck.p, TROP ? s.cw.p : nullptr);
   pt.end(t);
   const uint64_t ksz = sizeof(K), wsz = TROP ? sizeof(W) : 0;
@@ -149,6 +149,7 @@ uint64_t derive(strata_ctx* ctx, const K* dk, const W* dw, uint64_t nd, const Cs
                           s.counts.p);
   uint64_t nu = 0;
   read_u64(ctx, s.counts.p, &nu, 1);
+  kprof_add_last(ctx, K_REDUCE_RUNS, nu * (ksz + wsz));
   pt.end(t);
   a.diff_b += T * (ksz + wsz) + nu * (ksz + wsz);
   a.diff_l += (uint32_t)(ctx->launches - l2);
@@ -180,6 +181,7 @@ void fix_loop(strata_ctx* ctx, Rel<K, W>& full, Rel<K, W>& delta, const Csr<W>& 
                              dnext.k.p, TROP ? dnext.w.p : nullptr, s.counts.p);
       uint64_t c[2];
       read_checked(ctx, s.counts.p, c, 2);
+      kprof_add_last(ctx, K_MERGE_DIFF, (c[0] + c[1]) * (ksz + wsz));
       pt.end(t);
       a.merge_b += (full.n + nu) * (ksz + wsz) + (c[0] + c[1]) * (ksz + wsz);
       a.merge_l += (uint32_t)(ctx->launches - l0);
@@ -336,6 +338,7 @@ strata_rel* run_tc_shape(strata_ctx* ctx, const EdgeCols& e, int b0, int b1, int
   fix_loop<K, W, TROP>(ctx, full, delta, csr, js, key_bits, cap, s, pt, a, &rounds);
   const double ms = et.stop();
   pt.collect();
+  kprof_collect(ctx);
   fill_stats(st, a, rounds, full.n, universe, key_bits, TROP ? sizeof(W) : 0, ms, ctx->launches - l_start);
   return finish_rel<K, W, TROP>(ctx, full, b1);
 }
@@ -455,6 +458,7 @@ strata_rel* run_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
   fix_loop<K, W, true>(ctx, full, delta, csr, js, key_bits, cap, s, pt, a, &rounds);
   const double ms = et.stop();
   pt.collect();
+  kprof_collect(ctx);
   fill_stats(st, a, rounds, full.n, universe, key_bits, sizeof(W), ms, ctx->launches - l_start);
   return finish_rel<K, W, true>(ctx, full, b1);
 }

@@ -34,7 +34,7 @@ template <class K, class W, bool TROP>
 void expand_emit(strata_ctx* ctx, const K* dkeys, const W* dw, uint64_t n, const uint64_t* pos,
                  uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask,
                  int out_pshift, int out_vshift, const uint32_t* off, uint64_t n_nodes,
-                 const uint32_t* nbr, const W* nbr_w, K* out, W* out_w);
+                 const uint32_t* nbr, uint64_t n_nbr, const W* nbr_w, K* out, W* out_w);
 
 // Reduce sorted keys with duplicates to one row per key (Trop: the minimum
 // weight).  Writes count to *d_count (device).  `out`/`out_w` capacity >= n.

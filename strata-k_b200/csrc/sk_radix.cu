@@ -175,7 +175,8 @@ __global__ void __launch_bounds__(NT) k_onesweep(const K* __restrict__ kin, K* _
       const K k = s_keys[i];
       const uint32_t d = (uint32_t)(k >> shift) & dmask;
       dst[j] = s_gbase[d] + (i - s_dstart[d]);
-      kout[dst[j]] = k;
+      if (dst[j] < n) kout[dst[j]] = k;
+      else atomicOr(status, ST_BOUNDS);
     }
   }
   if constexpr (HAS_V) {
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(NT) k_onesweep(const K* __restrict__ kin, K* _
 #pragma unroll
     for (int j = 0; j < ITEMS; j++) {
       const uint32_t i = j * NT + tid;
-      if (i < tile_n) vout[dst[j]] = s_vals[i];
+      if (i < tile_n && dst[j] < n) vout[dst[j]] = s_vals[i];
     }
   }
 }
@@ -212,7 +213,9 @@ void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has
   const int hblocks = (int)std::min<uint64_t>(ceil_div(n, NT * 16), (uint64_t)ctx->num_sms * 4);
   for (int p0 = 0; p0 < passes; p0 += 4) {
     const int np = std::min(4, passes - p0);
+    const int kh = kprof_begin(ctx, K_RADIX_HIST);
     k_radix_hist<K><<<hblocks, NT, 0, ctx->stream>>>(*keys, n, p0, np, hist.p);
+    kprof_end(ctx, kh, n * sizeof(K));
     after_launch(ctx, "k_radix_hist");
   }
   DBuf<uint32_t> binoff(ctx, passes * RADIX);
@@ -237,6 +240,7 @@ void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has
     if (trivial[p]) continue;
     SK_CUDA(cudaMemsetAsync(lookback.p, 0, sizeof(uint32_t) * ntiles * RADIX, ctx->stream));
     const int dbits = std::min(8, bits - 8 * p);
+    const int kh = kprof_begin(ctx, K_ONESWEEP);
     if (has_vals) {
       auto kern = k_onesweep<K, V, true, ITEMS>;
       SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -250,6 +254,7 @@ void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has
                                               dbits, binoff.p + p * RADIX, lookback.p,
                                               counters + p, ctx->d_status);
     }
+    kprof_end(ctx, kh, 2 * n * (sizeof(K) + (has_vals ? sizeof(V) : 0)));
     after_launch(ctx, "k_onesweep");
     std::swap(*keys, *alt);
     if (has_vals) std::swap(*vals, *valt);

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(NT)
                   const uint64_t* __restrict__ pos, uint64_t total, int jshift, uint64_t jmask,
                   int pshift, uint64_t pmask, int out_pshift, int out_vshift,
                   const uint32_t* __restrict__ off, uint64_t n_nodes, const uint32_t* __restrict__ nbr,
-                  const W* __restrict__ nbr_w, K* __restrict__ out, W* __restrict__ out_w,
+                  uint64_t n_nbr, const W* __restrict__ nbr_w, K* __restrict__ out, W* __restrict__ out_w,
                   uint32_t* status) {
   __shared__ uint64_t s_pos[EE_TILE + 1];
   __shared__ uint32_t s_seg[EE_TILE + 1];
@@ -118,6 +118,10 @@ __global__ void __launch_bounds__(NT)
   }
   __syncthreads();
   const uint64_t a = s_r[0], i1 = s_r[1], o0 = s_r[2], o1 = s_r[3];
+  if (i1 - a > EE_TILE + 1) {  // cannot happen for a valid pos[]; never index past smem
+    if (tid == 0) atomicOr(status, ST_BOUNDS);
+    return;
+  }
   const uint32_t cnt = (uint32_t)(i1 - a);  // <= EE_TILE + 1
   for (uint32_t k = tid; k < cnt; k += NT) {
     const uint64_t i = a + k;
@@ -140,6 +144,7 @@ __global__ void __launch_bounds__(NT)
     if (lo == 0) { flags |= ST_BOUNDS; continue; }
     const uint32_t li = lo - 1;
     const uint64_t e = (uint64_t)s_seg[li] + (o - s_pos[li]);
+    if (e >= n_nbr) { flags |= ST_BOUNDS; continue; }
     const uint32_t v = nbr[e];
     out[o] = (K)(((K)s_kept[li] << out_pshift) | ((K)v << out_vshift));
     if constexpr (TROP) out_w[o] = trop_mul(s_w[li], nbr_w[e], &flags);
@@ -379,8 +384,10 @@ __global__ void __launch_bounds__(NT)
   }
   __syncthreads();
   const uint64_t i0 = s_r[0], j0 = s_r[1];
-  const uint32_t acnt = (uint32_t)(s_r[2] - i0);
-  const uint32_t bcnt = (uint32_t)(s_r[3] - j0);
+  const bool oversize = (s_r[2] - i0) + (s_r[3] - j0) > MD_TILE + 1;  // impossible for sorted unique inputs
+  if (oversize && tid == 0) atomicOr(status, ST_BOUNDS);
+  const uint32_t acnt = oversize ? 0u : (uint32_t)(s_r[2] - i0);
+  const uint32_t bcnt = oversize ? 0u : (uint32_t)(s_r[3] - j0);
   for (uint32_t k = tid; k < acnt; k += NT) {
     s_a[k] = A[i0 + k];
     if constexpr (TROP) s_aw[k] = Aw[i0 + k];
@@ -642,8 +649,10 @@ void expand_offsets(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uin
   DBuf<uint64_t> states(ctx, tiles + 1);
   uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles);
   SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 1), ctx->stream));
+  const int kh = kprof_begin(ctx, K_EXPAND_OFFSETS);
   k_expand_offsets<K><<<tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, pos,
                                                      states.p, counter, ctx->d_status);
+  kprof_end(ctx, kh, n * (sizeof(K) + 8 + 8));
   after_launch(ctx, "k_expand_offsets");
 }
 
@@ -651,13 +660,16 @@ template <class K, class W, bool TROP>
 void expand_emit(strata_ctx* ctx, const K* dkeys, const W* dw, uint64_t n, const uint64_t* pos,
                  uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask,
                  int out_pshift, int out_vshift, const uint32_t* off, uint64_t n_nodes,
-                 const uint32_t* nbr, const W* nbr_w, K* out, W* out_w) {
+                 const uint32_t* nbr, uint64_t n_nbr, const W* nbr_w, K* out, W* out_w) {
   if (total == 0 || n == 0) return;
   const uint64_t tiles = ceil_div(n + total, EE_TILE);
   if (tiles > 0x7fffffffull) fail(STRATA_E_UNSUPPORTED, "expand too large for one launch");
+  const int kh = kprof_begin(ctx, K_EXPAND_EMIT);
   k_expand_emit<K, W, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(
       dkeys, dw, n, pos, total, jshift, jmask, pshift, pmask, out_pshift, out_vshift, off, n_nodes,
-      nbr, nbr_w, out, out_w, ctx->d_status);
+      nbr, n_nbr, nbr_w, out, out_w, ctx->d_status);
+  const uint64_t wsz = TROP ? sizeof(W) : 0;
+  kprof_end(ctx, kh, n * (sizeof(K) + wsz + 8 + 4) + total * (4 + wsz) + total * (sizeof(K) + wsz));
   after_launch(ctx, "k_expand_emit");
 }
 
@@ -672,8 +684,10 @@ void reduce_runs(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, K* out,
   DBuf<uint64_t> states(ctx, tiles + 1);
   uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles);
   SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 1), ctx->stream));
+  const int kh = kprof_begin(ctx, K_REDUCE_RUNS);
   k_reduce_runs<K, W, TROP><<<tiles, NT, 0, ctx->stream>>>(keys, w, n, out, out_w, states.p, counter,
                                                            d_count, ctx->d_status);
+  kprof_end(ctx, kh, n * (sizeof(K) + (TROP ? sizeof(W) : 0)));  // reads; writes added on read-back
   after_launch(ctx, "k_reduce_runs");
 }
 
@@ -693,9 +707,11 @@ static void launch_merge(strata_ctx* ctx, const K* full, W* full_w, uint64_t nf,
   const size_t smem = 2 * CAP * sizeof(K) + (TROP ? 2 * CAP * sizeof(W) : 0) + (2 * CAP + 1) * sizeof(uint32_t);
   auto kern = k_merge_diff<K, W, TROP, WF, WD, IP>;
   SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int kh = kprof_begin(ctx, K_MERGE_DIFF);
   kern<<<tiles, NT, smem, ctx->stream>>>(full, full_w, nf, cand, cand_w, nc, fout, fout_w, dout,
                                          dout_w, states.p, states.p + tiles, counter, d_counts,
                                          ctx->d_status);
+  kprof_end(ctx, kh, (nf + nc) * (sizeof(K) + (TROP ? sizeof(W) : 0)));  // reads; writes added on read-back
   after_launch(ctx, "k_merge_diff");
 }
 
@@ -825,7 +841,8 @@ template void build_csr<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, u
 #define SK_INST_KW(K, W, T)                                                                          \
   template void expand_emit<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, const uint64_t*,     \
                                      uint64_t, int, uint64_t, int, uint64_t, int, int,               \
-                                     const uint32_t*, uint64_t, const uint32_t*, const W*, K*, W*);  \
+                                     const uint32_t*, uint64_t, const uint32_t*, uint64_t, const W*, \
+                                     K*, W*);                                                        \
   template void reduce_runs<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, K*, W*, uint64_t*);  \
   template void merge_diff<K, W, T>(strata_ctx*, const K*, const W*, uint64_t, const K*, const W*,   \
                                     uint64_t, K*, W*, K*, W*, uint64_t*);                            \

@@ -219,14 +219,20 @@ uint64_t tri_from_sorted(strata_ctx* ctx, const K* keys, uint64_t m, int bits, u
   DBuf<uint64_t> acc(ctx, 2);
   SK_CUDA(cudaMemsetAsync(acc.p, 0, 16, ctx->stream));
   const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(n_nodes, TC_WARPS), (uint64_t)ctx->num_sms * 8);
+  const int kh = kprof_begin(ctx, K_TRI_COUNT);
   k_tri_count<<<grid ? grid : 1, TC_NT, 0, ctx->stream>>>(off.p, nbr.p, n_nodes,
                                                           reinterpret_cast<uint32_t*>(acc.p + 1),
                                                           reinterpret_cast<unsigned long long*>(acc.p));
+  // Algorithmic bytes: every out-list once per incident oriented edge plus the
+  // edge list and offsets (4 B·Σ(d+(u)+d+(v)) + 8 B·M + 4 B·(N+1)), counted
+  // on the device below when profiling.
+  kprof_end(ctx, kh, 0);
   after_launch(ctx, "k_tri_count");
   uint64_t r;
   SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, acc.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
   r = ctx->h_scalar[0];
+  kprof_collect(ctx);
   return r;
 }
 

@@ -26,6 +26,9 @@ E_UNSUPPORTED = 7
 E_NOT_BUILT = 8
 E_WEIGHT_RANGE = 9
 
+KERNELS = {0: "k_onesweep", 1: "k_expand_emit", 2: "k_expand_offsets", 3: "k_reduce_runs",
+           4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count"}
+
 STATUS_NAMES = {
     OK: "OK", E_INVALID: "INVALID", E_OOM: "OOM", E_CUDA: "CUDA", E_OVERFLOW: "OVERFLOW",
     E_NEG_CYCLE: "NEG_CYCLE", E_TIMEOUT: "TIMEOUT", E_UNSUPPORTED: "UNSUPPORTED",
@@ -71,6 +74,8 @@ SIGNATURES = {
     "strata_ctx_mem": (C.c_int, [ctxp, u64p, u64p]),
     "strata_ctx_set_profiling": (C.c_int, [ctxp, C.c_int]),
     "strata_ctx_launches": (C.c_uint64, [ctxp]),
+    "strata_ctx_kernel_stats": (C.c_int, [ctxp, C.c_int, u64p, C.POINTER(C.c_double), u64p]),
+    "strata_ctx_reset_kernel_stats": (C.c_int, [ctxp]),
     "strata_free": (None, [vp]),
     "strata_transitive_closure_bool": (
         C.c_int, [ctxp, u32p, u32p, C.c_uint64, C.POINTER(u32p), C.POINTER(u32p), u64p,

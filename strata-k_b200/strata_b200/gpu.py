@@ -217,6 +217,18 @@ class Engine:
     def launches(self) -> int:
         return int(self.lib.strata_ctx_launches(self.ctx))
 
+    def kernel_stats(self) -> dict:
+        """{kernel name: (launches, summed ms, algorithmic bytes)} while profiling."""
+        out = {}
+        for kid, name in L.KERNELS.items():
+            n, ms, b = C.c_uint64(), C.c_double(), C.c_uint64()
+            self._check(self.lib.strata_ctx_kernel_stats(self.ctx, kid, C.byref(n), C.byref(ms), C.byref(b)))
+            out[name] = (int(n.value), float(ms.value), int(b.value))
+        return out
+
+    def reset_kernel_stats(self):
+        self._check(self.lib.strata_ctx_reset_kernel_stats(self.ctx))
+
     def mem(self) -> tuple[int, int]:
         a, b = C.c_uint64(), C.c_uint64()
         self._check(self.lib.strata_ctx_mem(self.ctx, C.byref(a), C.byref(b)))

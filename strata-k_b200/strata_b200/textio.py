@@ -1,0 +1,133 @@
+"""The input and output contracts around the fixpoint (host side).
+
+* ``SymbolDict`` — first-seen interning (strata-ir/src/dict.rs:24-43): ids are
+  assigned in order of first sight, so the same input yields the same ids.
+* ``load_tsv`` — Soufflé TSV rows split on tab, empty lines skipped, a Trop
+  predicate's trailing column parsed as an i64 weight, a neural predicate's
+  as a probability in [0, 1] (strata-k/src/input.rs:53-197, 204-234).
+* ``render_db`` — canonical text: relations in name order, tuples in id order,
+  ``pred(a, b)`` with `` = w`` / `` = inf`` for Trop (strata-cli/src/render.rs:29-92,
+  strata-ir/src/output.rs:11).  A non-empty ``queries`` list filters the
+  output like plain ``?q(...)`` queries (render.rs:21-64).
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+
+POS_INF_TOKEN = "inf"
+
+
+class SymbolDict:
+    def __init__(self):
+        self.by_str: dict[str, int] = {}
+        self.by_id: list[str] = []
+
+    def intern(self, s: str) -> int:
+        i = self.by_str.get(s)
+        if i is None:
+            i = len(self.by_id)
+            self.by_id.append(s)
+            self.by_str[s] = i
+        return i
+
+    def get(self, s: str) -> int | None:
+        return self.by_str.get(s)
+
+    def resolve(self, i: int) -> str:
+        return self.by_id[i] if 0 <= i < len(self.by_id) else "?"
+
+    def __len__(self) -> int:
+        return len(self.by_id)
+
+
+class InputError(ValueError):
+    pass
+
+
+def _rows(source) -> list[tuple[int, list[str]]]:
+    if isinstance(source, (str, Path)):
+        text = Path(source).read_text()
+        out = []
+        for i, line in enumerate(text.splitlines()):
+            line = line.rstrip("\r")
+            if not line:
+                continue
+            out.append((i + 1, line.split("\t")))
+        return out
+    return [(i + 1, list(r)) for i, r in enumerate(source)]
+
+
+def load_tsv(source, arity: int, dictionary: SymbolDict, trop: bool = False,
+             neural: bool = False):
+    """Parse rows of ``arity`` symbol columns (+ a trailing weight / probability).
+
+    Returns (list of id columns as uint32 arrays, weights or None).  Errors
+    follow input.rs: wrong column count, empty cell, unparsable trailing value,
+    probability outside [0, 1].
+    """
+    rows = _rows(source)
+    ncols = arity + (1 if (trop or neural) else 0)
+    cols = [np.zeros(len(rows), np.uint32) for _ in range(arity)]
+    weights = np.zeros(len(rows), np.int64) if trop else (np.zeros(len(rows)) if neural else None)
+    for k, (lineno, cells) in enumerate(rows):
+        if len(cells) != ncols:
+            raise InputError(f"{lineno}: expects {ncols} column(s), found {len(cells)}")
+        for c in range(arity):
+            if cells[c] == "":
+                raise InputError(f"{lineno}: empty value in column {c + 1}")
+            cols[c][k] = dictionary.intern(cells[c])
+        if trop:
+            try:
+                weights[k] = int(cells[arity].strip())
+            except ValueError:
+                raise InputError(f"{lineno}: needs a trailing integer weight") from None
+        elif neural:
+            try:
+                p = float(cells[arity].strip())
+            except ValueError:
+                raise InputError(f"{lineno}: needs a trailing probability") from None
+            if not 0.0 <= p <= 1.0:
+                raise InputError(f"{lineno}: probability {p} is outside [0, 1]")
+            weights[k] = p
+    return cols, weights
+
+
+def render_weight(w: int, inf: bool) -> str:
+    return POS_INF_TOKEN if inf else str(int(w))
+
+
+def render_relation(name: str, cols, dictionary: SymbolDict, w=None, inf=None,
+                    queries=None) -> list[str]:
+    """Lines for one relation; ``cols`` are id columns already in id order."""
+    n = len(cols[0]) if cols else 0
+    names = [[dictionary.resolve(int(v)) for v in c] for c in cols]
+    out = []
+    for i in range(n):
+        vals = [names[c][i] for c in range(len(cols))]
+        if queries and not any(_match(q, name, vals) for q in queries):
+            continue
+        line = f"{name}({', '.join(vals)})"
+        if w is not None:
+            line += " = " + render_weight(w[i], bool(inf[i]) if inf is not None else False)
+        out.append(line)
+    return out
+
+
+def _match(q, name, vals) -> bool:
+    qname, pattern = q
+    if qname != name or len(pattern) != len(vals):
+        return False
+    return all(p is None or p == v for p, v in zip(pattern, vals))
+
+
+def render_db(relations: dict, dictionary: SymbolDict, queries=None) -> str:
+    """``relations``: name -> (cols, w, inf) with rows sorted by id tuple."""
+    lines = []
+    for name in sorted(relations):
+        if queries and not any(q[0] == name for q in queries):
+            continue
+        cols, w, inf = relations[name]
+        lines += render_relation(name, cols, dictionary, w, inf, queries)
+    return "".join(l + "\n" for l in lines)

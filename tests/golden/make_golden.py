@@ -1,0 +1,54 @@
+"""Regenerate the golden fixtures of tests/golden/ from the reference tree.
+
+Run in a checkout that has the reference mounted (default /root/reference):
+
+    python tests/golden/make_golden.py [REFERENCE_ROOT]
+
+Fixtures written (small, committed):
+  routing.json — the routing workload's input rows (examples/workloads/routing/
+                 links.tsv) and the three lines its CI test pins
+                 (crates/strata-cli/tests/workloads.rs:26-32).
+  tc_example.json — examples/edges.tsv rows (the tc_tsv.strata input).
+The tests never read the reference tree; they read these files.
+"""
+import json
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+
+
+def tsv_rows(p: Path):
+    rows = []
+    for line in p.read_text().splitlines():
+        line = line.rstrip("\r")
+        if line:
+            rows.append(line.split("\t"))
+    return rows
+
+
+def main(ref: Path) -> None:
+    links = tsv_rows(ref / "examples/workloads/routing/links.tsv")
+    pinned = []
+    src = (ref / "crates/strata-cli/tests/workloads.rs").read_text()
+    for line in src.splitlines():
+        line = line.strip()
+        if line.startswith('"route('):
+            pinned.append(line.strip('",'))
+    (HERE / "routing.json").write_text(json.dumps({
+        "source": "examples/workloads/routing/links.tsv; pinned lines from "
+                  "crates/strata-cli/tests/workloads.rs:26-32",
+        "rows": links,
+        "queries": [["n0_0", "n7_7"], ["n0_0", "n4_4"], ["n7_7", "n0_0"]],
+        "pinned": pinned,
+    }, indent=0))
+    edges = tsv_rows(ref / "examples/edges.tsv")
+    (HERE / "tc_example.json").write_text(json.dumps({
+        "source": "examples/edges.tsv (input of examples/tc_tsv.strata)",
+        "rows": edges,
+    }, indent=0))
+    print(f"routing: {len(links)} rows, pinned {pinned}; tc_example: {len(edges)} rows")
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
