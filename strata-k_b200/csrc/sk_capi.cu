@@ -110,6 +110,19 @@ strata_status strata_ctx_create(int device, uint64_t mem_cap_bytes, strata_ctx**
   SK_CUDA(cudaMallocHost(&ctx->h_status, 64));
   SK_CUDA(cudaMallocHost(&ctx->h_scalar, 8 * sizeof(uint64_t)));
   SK_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+  {
+    // A pool of our own whose freed blocks stay mapped: per-round buffers are
+    // re-used across rounds and calls instead of being re-mapped after every
+    // synchronization (the default release threshold is 0).
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    SK_CUDA(cudaMemPoolCreate(&ctx->pool, &props));
+    uint64_t keep = UINT64_MAX;
+    SK_CUDA(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   *out = ctx;
   }
   catch (const SkError& err) {
@@ -132,6 +145,7 @@ void strata_ctx_destroy(strata_ctx* ctx) {
   for (auto& r : ctx->krecs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   delete ctx;
 }
 

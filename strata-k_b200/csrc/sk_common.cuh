@@ -72,6 +72,7 @@ struct strata_ctx {
   uint32_t* h_status = nullptr;     // pinned mirror
   uint64_t* h_scalar = nullptr;     // pinned scratch for small D2H reads (8 slots)
   int num_sms = 148;
+  cudaMemPool_t pool = nullptr;     // this context's pool (kept mapped between calls)
   bool profiling = false;
   uint64_t launches = 0;
   // Per-kernel CUDA-event accounting (enabled with profiling).
@@ -95,7 +96,8 @@ inline void* dev_alloc(strata_ctx* ctx, uint64_t bytes) {
                            std::to_string(ctx->cap) + " B held");
   }
   void* p = nullptr;
-  cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
+  cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync(&p, bytes, ctx->pool, ctx->stream)
+                            : cudaMallocAsync(&p, bytes, ctx->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
     fail(STRATA_E_OOM, std::string("cudaMallocAsync(") + std::to_string(bytes) +

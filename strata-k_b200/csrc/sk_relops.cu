@@ -134,7 +134,8 @@ __global__ void __launch_bounds__(NT)
   }
   __syncthreads();
   uint32_t flags = 0;
-  for (uint64_t o = o0 + tid; o < o1; o += NT) {
+  const uint64_t o_end = o1 < total ? o1 : total;  // o1 <= total for a valid pos[]
+  for (uint64_t o = o0 + tid; o < o_end; o += NT) {
     // owner = last loaded item with pos <= o
     uint32_t lo = 0, hi = cnt;
     while (lo < hi) {
@@ -326,6 +327,10 @@ __global__ void __launch_bounds__(NT)
   const uint64_t ob = s_excl;
   const uint32_t lim = nout < RR_TILE ? nout : RR_TILE;
   for (uint32_t k = tid; k < lim; k += NT) {
+    if (ob + k >= n) {  // more runs than keys: only unsorted input gets here
+      atomicOr(status, ST_BOUNDS);
+      break;
+    }
     out[ob + k] = s_ok[k];
     if constexpr (TROP) out_w[ob + k] = s_ow[k];
   }
@@ -384,7 +389,10 @@ __global__ void __launch_bounds__(NT)
   }
   __syncthreads();
   const uint64_t i0 = s_r[0], j0 = s_r[1];
-  const bool oversize = (s_r[2] - i0) + (s_r[3] - j0) > MD_TILE + 1;  // impossible for sorted unique inputs
+  // Impossible for sorted unique inputs; checked so unsorted input cannot
+  // index past shared memory.
+  const bool oversize = s_r[2] < i0 || s_r[3] < j0 || (s_r[2] - i0) > MD_TILE + 1 ||
+                        (s_r[3] - j0) > MD_TILE + 1 || (s_r[2] - i0) + (s_r[3] - j0) > MD_TILE + 1;
   if (oversize && tid == 0) atomicOr(status, ST_BOUNDS);
   const uint32_t acnt = oversize ? 0u : (uint32_t)(s_r[2] - i0);
   const uint32_t bcnt = oversize ? 0u : (uint32_t)(s_r[3] - j0);
@@ -463,13 +471,21 @@ __global__ void __launch_bounds__(NT)
       const bool m = (mflag >> q) & 1u;
       if (WRITE_FULL && !m) {
         const uint64_t p = fex + b_ra[q] + (jb - s_mpre[jb]);
-        fout[p] = s_b[jb];
-        if constexpr (TROP) fout_w[p] = s_bw[jb];
+        if (p < na + nb) {
+          fout[p] = s_b[jb];
+          if constexpr (TROP) fout_w[p] = s_bw[jb];
+        } else {
+          atomicOr(status, ST_BOUNDS);
+        }
       }
       if (WRITE_DELTA && ((dflag >> q) & 1u)) {
         const uint64_t p = dexg + s_dpre[jb];
-        dout[p] = s_b[jb];
-        if constexpr (TROP) dout_w[p] = s_bw[jb];
+        if (p < nb) {
+          dout[p] = s_b[jb];
+          if constexpr (TROP) dout_w[p] = s_bw[jb];
+        } else {
+          atomicOr(status, ST_BOUNDS);
+        }
       }
       if constexpr (TROP && INPLACE) {
         if (m && s_bw[jb] < s_aw[b_ra[q]]) Aw[i0 + b_ra[q]] = s_bw[jb];
@@ -485,6 +501,10 @@ __global__ void __launch_bounds__(NT)
         if (s_b[mid] < x) lo = mid + 1; else hi = mid;
       }
       const uint64_t p = fex + ia + (lo - s_mpre[lo]);
+      if (p >= na + nb) {
+        atomicOr(status, ST_BOUNDS);
+        continue;
+      }
       fout[p] = x;
       if constexpr (TROP) {
         W wv = s_aw[ia];

@@ -84,6 +84,9 @@ __global__ void __launch_bounds__(TC_NT)
 
 // K4 on a degree-oriented DAG: one thread per oriented edge (u, v); for each
 // common successor w1 count |out(u) ∩ out(v) ∩ out(w1)| by a 3-way leapfrog.
+// The lists are sorted by id while the DAG follows (degree, id) rank, so the
+// leapfrog runs over the whole of out(u) and out(v): membership in out(w1)
+// already fixes rank(w2) > rank(w1), and each K4 is counted once.
 __global__ void k_k4_count(const uint32_t* __restrict__ eu, const uint32_t* __restrict__ ev, uint64_t m,
                            const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
                            unsigned long long* total) {
@@ -99,7 +102,7 @@ __global__ void k_k4_count(const uint32_t* __restrict__ eu, const uint32_t* __re
       if (x < y) { a++; continue; }
       if (x > y) { b++; continue; }
       const uint32_t w1 = x;
-      uint32_t p = a + 1, q = b + 1, r = off[w1];
+      uint32_t p = off[u], q = off[v], r = off[w1];
       const uint32_t re = off[w1 + 1];
       while (p < ae && q < be && r < re) {
         const uint32_t xp = nbr[p], xq = nbr[q], xr = nbr[r];

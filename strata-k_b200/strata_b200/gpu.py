@@ -243,7 +243,7 @@ class Engine:
     # -- whole fixpoints (host buffers) ------------------------------------
     def transitive_closure_bool(self, edges) -> BoolRelation:
         s, d = _split_pairs(edges)
-        os_, od = u32p(), u32p()
+        os_, od = L.u32p(), L.u32p()
         n = C.c_uint64()
         st = L.FixStats()
         self._check(self.lib.strata_transitive_closure_bool(
@@ -254,7 +254,7 @@ class Engine:
 
     def shortest_paths_trop(self, edges) -> TropRelation:
         s, d, w, inf = _split_weighted(edges)
-        os_, od, ow, oi = u32p(), u32p(), i64p(), u8p()
+        os_, od, ow, oi = L.u32p(), L.u32p(), L.i64p(), L.u8p()
         n = C.c_uint64()
         st = L.FixStats()
         self._check(self.lib.strata_shortest_paths_trop(
@@ -271,7 +271,7 @@ class Engine:
         sw = None if source_weights is None else np.ascontiguousarray(source_weights, dtype=np.int64)
         si = None if source_inf is None else np.ascontiguousarray(source_inf, dtype=np.uint8)
         s, d, w, inf = _split_weighted(edges)
-        os_, od, ow, oi = u32p(), u32p(), i64p(), u8p()
+        os_, od, ow, oi = L.u32p(), L.u32p(), L.i64p(), L.u8p()
         n = C.c_uint64()
         st = L.FixStats()
         self._check(self.lib.strata_mssp_trop(

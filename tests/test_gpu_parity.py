@@ -345,8 +345,9 @@ def test_op_dedup_diff_and_min_improve(engine):
     full = np.unique(rng.integers(0, 5000, 3000).astype(np.uint32))
     out = torch.empty(len(cand), dtype=torch.int32, device="cuda")
     n = C.c_uint64()
-    engine._check(engine.lib.strata_op_dedup_diff(engine.ctx, 4, C.c_void_p(_dev(cand, np.int32).data_ptr()),
-                                                  len(cand), C.c_void_p(_dev(full, np.int32).data_ptr()), len(full),
+    cand_d, full_d = _dev(cand, np.int32), _dev(full, np.int32)  # kept alive across the calls
+    engine._check(engine.lib.strata_op_dedup_diff(engine.ctx, 4, C.c_void_p(cand_d.data_ptr()),
+                                                  len(cand), C.c_void_p(full_d.data_ptr()), len(full),
                                                   C.c_void_p(out.data_ptr()), C.byref(n)))
     want = np.setdiff1d(np.unique(cand), full)
     assert np.array_equal(out.cpu().numpy().view(np.uint32)[:n.value], want)
@@ -354,11 +355,12 @@ def test_op_dedup_diff_and_min_improve(engine):
     cw = rng.integers(0, 100, len(cand)).astype(np.int64)
     fw = rng.integers(0, 100, len(full)).astype(np.int64)
     fw_dev = _dev(fw, np.int64)
+    cw_d = _dev(cw, np.int64)
     ok = torch.empty(len(cand), dtype=torch.int32, device="cuda")
     ow = torch.empty(len(cand), dtype=torch.int64, device="cuda")
     engine._check(engine.lib.strata_op_min_improve(
-        engine.ctx, 4, C.c_void_p(_dev(cand, np.int32).data_ptr()), C.c_void_p(_dev(cw, np.int64).data_ptr()),
-        len(cand), C.c_void_p(_dev(full, np.int32).data_ptr()), C.c_void_p(fw_dev.data_ptr()), len(full),
+        engine.ctx, 4, C.c_void_p(cand_d.data_ptr()), C.c_void_p(cw_d.data_ptr()),
+        len(cand), C.c_void_p(full_d.data_ptr()), C.c_void_p(fw_dev.data_ptr()), len(full),
         C.c_void_p(ok.data_ptr()), C.c_void_p(ow.data_ptr()), C.byref(n)))
     best = {}
     for k, w in zip(cand.tolist(), cw.tolist()):
@@ -379,8 +381,9 @@ def test_op_merge(engine):
     a = np.sort(allk[:20000])
     b = np.sort(allk[20000:])
     out = torch.empty(len(allk), dtype=torch.int64, device="cuda")
-    engine._check(engine.lib.strata_op_merge(engine.ctx, 8, C.c_void_p(_dev(a, np.int64).data_ptr()), None, len(a),
-                                             C.c_void_p(_dev(b, np.int64).data_ptr()), None, len(b),
+    a_d, b_d = _dev(a, np.int64), _dev(b, np.int64)  # kept alive across the call
+    engine._check(engine.lib.strata_op_merge(engine.ctx, 8, C.c_void_p(a_d.data_ptr()), None, len(a),
+                                             C.c_void_p(b_d.data_ptr()), None, len(b),
                                              C.c_void_p(out.data_ptr()), None))
     assert np.array_equal(out.cpu().numpy().view(np.uint64), np.sort(allk))
 
