@@ -222,6 +222,26 @@ strata_status strata_op_merge(strata_ctx* ctx, int key_bytes,
     const void* d_b, const int64_t* d_bw, uint64_t nb,
     void* d_out, int64_t* d_out_w);
 
+/* ---- allocation-free sort ---------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (host callbacks and driver hooks where cudaMalloc is not allowed,
+ * embedders whose allocator owns the whole device, latency-critical loops
+ * that must not enter the allocator): a stable ascending sort of u32 keys on
+ * their low `key_bits` bits (0..32) from d_keys_in into d_keys_out (distinct
+ * caller-owned device buffers; the input is left unchanged), run on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) and finished before the
+ * call returns.  It needs no context and calls no allocator: its temporaries
+ * live in a fixed 4,483,200-byte array inside the library, which every GPU that
+ * loads the library holds until the process exits.  n above
+ * STRATA_NOALLOC_SORT_MAX_KEYS returns STRATA_E_INVALID.  The first call on
+ * each device looks up the array's device address (once per device, with that
+ * device current); make it before any stream capture.  All calls share the
+ * array: calls whose GPU work overlaps race and must be serialized by the
+ * caller. */
+#define STRATA_NOALLOC_SORT_MAX_KEYS (1u << 20)
+strata_status strata_sort_u32_noalloc(const uint32_t* d_keys_in, uint32_t* d_keys_out, uint64_t n,
+                                      int key_bits, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,11 @@ template <class K, class V>
 void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has_vals,
                 uint64_t n, int bits, bool skip_trivial = true);
 
+// Allocation-free u32 key sort on caller-provided scratch (sk_noalloc.cu).
+uint64_t radix_sort_u32_static_bytes(uint64_t max_n);
+void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* out, uint64_t n, int bits,
+                           unsigned char* scratch, uint64_t max_n, uint32_t* h_status);
+
 // Exclusive scan of per-element expand degrees (see sk_relops.cu).
 // pos[i] = sum_{k<i} deg(i); pos[n] = total.  Returns nothing; read pos[n].
 template <class K>

@@ -269,4 +269,46 @@ SK_INST_SORT(uint64_t, uint32_t)
 SK_INST_SORT(uint64_t, uint64_t)
 #undef SK_INST_SORT
 
+// Variant for callers that cannot allocate: every temporary lives in the
+// caller-supplied `scratch` (see sk_noalloc.cu).  Keys only, u32, the last
+// pass always lands in `out`; no host synchronization inside.
+uint64_t radix_sort_u32_static_bytes(uint64_t max_n) {
+  constexpr uint32_t TILE = NT * RCfg<uint32_t>::ITEMS;
+  const uint64_t tiles = ceil_div(max_n, TILE);
+  // hist (4 passes) + bin offsets + tile counters + status + look-back + alt keys
+  return 4 * RADIX * 4 + 4 * RADIX * 4 + 64 + 64 + tiles * RADIX * 4 + max_n * 4;
+}
+
+void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* out, uint64_t n, int bits,
+                           unsigned char* scratch, uint64_t max_n, uint32_t* h_status) {
+  constexpr int ITEMS = RCfg<uint32_t>::ITEMS;
+  constexpr uint32_t TILE = NT * ITEMS;
+  const int passes = (bits + 7) / 8;
+  const uint32_t ntiles = (uint32_t)ceil_div(n, TILE);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(scratch);
+  uint32_t* binoff = hist + 4 * RADIX;
+  uint32_t* counters = binoff + 4 * RADIX;   // 16 slots
+  uint32_t* status = counters + 16;          // 16 slots
+  uint32_t* lookback = status + 16;
+  uint32_t* alt = lookback + ceil_div(max_n, TILE) * RADIX;
+  // Everything that must start at zero is cleared on every call.
+  check_cuda(cudaMemsetAsync(hist, 0, (4 * RADIX + 4 * RADIX + 32) * 4, stream), "cudaMemsetAsync");
+  const int hblocks = (int)std::min<uint64_t>(ceil_div(n, NT * 16), 148 * 4);
+  k_radix_hist<uint32_t><<<hblocks, NT, 0, stream>>>(in, n, 0, passes, hist);
+  k_radix_bins<<<passes, NT, 0, stream>>>(hist, binoff);
+  const size_t smem = (size_t)TILE * sizeof(uint32_t);
+  const uint32_t* src = in;
+  for (int p = 0; p < passes; p++) {
+    // Ping-pong so that the last pass writes `out`.
+    uint32_t* dst = ((passes - 1 - p) % 2 == 0) ? out : alt;
+    check_cuda(cudaMemsetAsync(lookback, 0, sizeof(uint32_t) * ntiles * RADIX, stream), "cudaMemsetAsync");
+    auto kern = k_onesweep<uint32_t, uint32_t, false, ITEMS>;
+    kern<<<ntiles, NT, smem, stream>>>(src, dst, nullptr, nullptr, (uint32_t)n, 8 * p, std::min(8, bits - 8 * p),
+                                       binoff + p * RADIX, lookback, counters + p, status);
+    src = dst;
+  }
+  check_cuda(cudaGetLastError(), "launch");
+  check_cuda(cudaMemcpyAsync(h_status, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync");
+}
+
 }  // namespace sk

@@ -109,6 +109,7 @@ SIGNATURES = {
     "strata_op_min_improve": (
         C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp, u64p]),
     "strata_op_merge": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp]),
+    "strata_sort_u32_noalloc": (C.c_int, [vp, vp, C.c_uint64, C.c_int, vp]),
 }
 
 _lib = None
