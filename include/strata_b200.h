@@ -67,6 +67,7 @@ typedef struct strata_fix_stats {
   uint64_t sort_bytes, join_bytes, diff_bytes, merge_bytes; /* algorithmic bytes */
   uint32_t sort_launches, join_launches, diff_launches, merge_launches;
   uint32_t other_launches;
+  uint32_t plan;            /* 1 sort-merge, 2 direct-addressed (see strata_ctx_set_plan) */
 } strata_fix_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -81,6 +82,13 @@ strata_status strata_ctx_set_stream(strata_ctx* ctx, void* stream);
 const char* strata_last_error(const strata_ctx* ctx);
 /* Device bytes currently held and the high-water mark. */
 strata_status strata_ctx_mem(const strata_ctx* ctx, uint64_t* in_use, uint64_t* peak);
+/* Physical plan of the fixpoint rounds: 0 = automatic (direct-addressed when
+ * the two column domains multiply to a small enough index and the weights
+ * fit int32, else sort-merge), 1 = sort-merge (radix sort + run reduction +
+ * merge-path diff every round), 2 = direct-addressed (a bitmap / int32 index
+ * over (c0, c1); STRATA_E_UNSUPPORTED when it does not apply).  Results are
+ * identical; only speed and memory differ. */
+strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan);
 /* Enable per-phase CUDA-event timing in strata_fix_stats (adds event records). */
 strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled);
 /* Number of kernels this context launched so far (monotone counter). */

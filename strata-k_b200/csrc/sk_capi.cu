@@ -175,6 +175,13 @@ strata_status strata_ctx_mem(const strata_ctx* ctx, uint64_t* in_use, uint64_t* 
   return STRATA_OK;
 }
 
+strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (plan < 0 || plan > 2) return bad(ctx, "plan must be 0 (auto), 1 (sort-merge) or 2 (direct-addressed)");
+  ctx->plan = plan;
+  return STRATA_OK;
+}
+
 strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled) {
   if (!ctx) return STRATA_E_INVALID;
   ctx->profiling = enabled != 0;

@@ -73,6 +73,7 @@ struct strata_ctx {
   uint64_t* h_scalar = nullptr;     // pinned scratch for small D2H reads (8 slots)
   int num_sms = 148;
   cudaMemPool_t pool = nullptr;     // this context's pool (kept mapped between calls)
+  int plan = 0;                     // 0 auto, 1 sort-merge, 2 direct-addressed
   bool profiling = false;
   uint64_t launches = 0;
   // Per-kernel CUDA-event accounting (enabled with profiling).

@@ -1,0 +1,323 @@
+// sk_dense.cu — the direct-addressed plan of the semi-naive round.
+//
+// When the product of the two column domains is small enough (the
+// benchmark's dist(S, Z): 64 × 552,101), a relation is held as a dense
+// index over (c0, c1): a membership bitmap for Bool, an int32 weight array
+// for Trop (ABSENT = INT32_MAX, +inf = INT32_MAX-1).  One round then needs no
+// sort and no merge:
+//
+//   for every candidate (key, w) of Δ ⋈ E:          (load-balanced expand)
+//     Bool:  first = !atomicOr(bit(key))             — dedup and Δ' = new∖full in one op
+//     Trop:  if w < D[key] and w < atomicMin(D[key], w)  — ⊕ = min
+//              first = !atomicOr(mark(key))          — one Δ' entry per improved key
+//     if first: append key to Δ'
+//
+// and Δ' takes its values from D after the round (the merged value of every
+// changed tuple, seminaive.rs:199-206).  A key enters Δ' exactly when some
+// candidate is new (Bool) or strictly below the value the key had when the
+// round started (Trop), which is the interpreter's `Relation::combine`
+// change test (store.rs:34-48), so rounds, Δ sets and the round cap are the
+// same as the sort-merge plan's.  Only the final relation is compacted back
+// into sorted packed keys (index order is key order).
+#include "sk_ops.cuh"
+#include "sk_prims.cuh"
+
+namespace sk {
+namespace {
+
+constexpr int NT = 256;
+constexpr int DE_ITEMS = 8;
+constexpr uint32_t DE_TILE = NT * DE_ITEMS;
+
+__device__ __forceinline__ uint64_t mp_before(const uint64_t* pos, uint64_t n, uint64_t d) {
+  uint64_t lo = 0, hi = d < n ? d : n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (mid + pos[mid] < d) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// splits[t] = #Δ items whose event precedes merged index t*tile (t <= tiles).
+__global__ void k_tile_splits(const uint64_t* __restrict__ pos, uint64_t n, uint64_t total, uint32_t tile,
+                              uint64_t tiles, uint64_t* __restrict__ splits) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > tiles) return;
+  const uint64_t L = n + total;
+  uint64_t d = t * (uint64_t)tile;
+  if (d > L) d = L;
+  splits[t] = mp_before(pos, n, d);
+}
+
+__device__ __forceinline__ uint64_t dense_index(uint64_t key, int b1, uint64_t mask1, uint64_t n1) {
+  return (key >> b1) * n1 + (key & mask1);
+}
+
+template <class K, bool TROP>
+__global__ void __launch_bounds__(NT)
+    k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n,
+                   const uint64_t* __restrict__ pos, uint64_t total, const uint64_t* __restrict__ splits,
+                   int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift, int out_vshift,
+                   const uint32_t* __restrict__ off, uint64_t n_nodes, const uint32_t* __restrict__ nbr,
+                   uint64_t n_nbr, const int32_t* __restrict__ nbr_w, int b1, uint64_t mask1, uint64_t n1,
+                   uint64_t entries, uint32_t* bits, int32_t* D, K* __restrict__ out, uint64_t out_cap,
+                   unsigned long long* out_count, uint32_t* status) {
+  __shared__ uint64_t s_pos[DE_TILE + 1];
+  __shared__ uint32_t s_seg[DE_TILE + 1];
+  __shared__ uint32_t s_kept[DE_TILE + 1];  // one column id
+  __shared__ int32_t s_w[TROP ? DE_TILE + 1 : 1];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const uint64_t L = n + total;
+  const uint64_t d0 = (uint64_t)blockIdx.x * DE_TILE;
+  const uint64_t d1 = d0 + DE_TILE < L ? d0 + DE_TILE : L;
+  const uint64_t i0 = splits[blockIdx.x], i1 = splits[blockIdx.x + 1];
+  const uint64_t a = i0 > 0 ? i0 - 1 : 0;
+  if (i1 < a || i1 - a > DE_TILE + 1 || i1 > n) {
+    if (tid == 0) atomicOr(status, ST_BOUNDS);
+    return;
+  }
+  const uint64_t o0 = d0 - i0, o1 = d1 - i1;
+  const uint32_t cnt = (uint32_t)(i1 - a);
+  for (uint32_t k = tid; k < cnt; k += NT) {
+    const uint64_t i = a + k;
+    const K key = dkeys[i];
+    const uint64_t jv = ((uint64_t)key >> jshift) & jmask;
+    s_pos[k] = pos[i];
+    s_seg[k] = jv < n_nodes ? off[jv] : 0u;
+    s_kept[k] = (uint32_t)(((uint64_t)key >> pshift) & pmask);
+    if constexpr (TROP) s_w[k] = dw[i];
+  }
+  __syncthreads();
+  uint32_t flags = 0;
+  const uint64_t o_end = o1 < total ? o1 : total;
+  for (uint64_t base = o0; base < o_end; base += NT) {
+    const uint64_t o = base + tid;
+    bool app = false;
+    K ok = 0;
+    if (o < o_end) {
+      uint32_t lo = 0, hi = cnt;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_pos[mid] <= o) lo = mid + 1; else hi = mid;
+      }
+      const uint32_t li = lo ? lo - 1 : 0;
+      const uint64_t e = (uint64_t)s_seg[li] + (o - s_pos[li]);
+      if (lo == 0 || e >= n_nbr) {
+        flags |= ST_BOUNDS;
+      } else {
+        const uint32_t v = nbr[e];
+        ok = (K)(((K)s_kept[li] << out_pshift) | ((K)v << out_vshift));
+        const uint64_t ix = dense_index((uint64_t)ok, b1, mask1, n1);
+        if (ix >= entries) {
+          flags |= ST_BOUNDS;
+        } else if constexpr (TROP) {
+          const int32_t cw = trop_mul(s_w[li], nbr_w[e], &flags);
+          if (cw < D[ix]) {
+            const int32_t old = atomicMin(&D[ix], cw);
+            if (cw < old) {
+              const uint32_t bit = 1u << (ix & 31);
+              app = (atomicOr(&bits[ix >> 5], bit) & bit) == 0;
+            }
+          }
+        } else {
+          const uint32_t bit = 1u << (ix & 31);
+          if ((bits[ix >> 5] & bit) == 0) app = (atomicOr(&bits[ix >> 5], bit) & bit) == 0;
+        }
+      }
+    }
+    // warp-aggregated append of the first touches
+    const unsigned m = __ballot_sync(kFull, app);
+    if (m) {
+      unsigned long long basei = 0;
+      const int leader = __ffs(m) - 1;
+      if (lane == leader) basei = atomicAdd(out_count, (unsigned long long)__popc(m));
+      basei = __shfl_sync(kFull, basei, leader);
+      if (app) {
+        const uint64_t at = basei + __popc(m & lanemask_lt());
+        if (at < out_cap) out[at] = ok;
+        else flags |= ST_BOUNDS;
+      }
+    }
+  }
+  if (flags) atomicOr(status, flags);
+}
+
+template <class K>
+__global__ void k_dense_gather(const K* __restrict__ keys, uint64_t n, int b1, uint64_t mask1, uint64_t n1,
+                               uint64_t entries, const int32_t* __restrict__ D, int32_t* __restrict__ w,
+                               uint32_t* status) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t ix = dense_index((uint64_t)keys[i], b1, mask1, n1);
+  if (ix >= entries) { atomicOr(status, ST_BOUNDS); return; }
+  w[i] = D[ix];
+}
+
+// Seed the index from sorted unique keys (and weights).
+template <class K, bool TROP>
+__global__ void k_dense_seed(const K* __restrict__ keys, const int32_t* __restrict__ w, uint64_t n, int b1,
+                             uint64_t mask1, uint64_t n1, uint64_t entries, uint32_t* bits, int32_t* D,
+                             uint32_t* status) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t ix = dense_index((uint64_t)keys[i], b1, mask1, n1);
+  if (ix >= entries) { atomicOr(status, ST_BOUNDS); return; }
+  if constexpr (TROP) D[ix] = w[i];
+  else atomicOr(&bits[ix >> 5], 1u << (ix & 31));
+}
+
+__global__ void k_fill_i32(int32_t* p, uint64_t n, int32_t v) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+// Compact the index back into sorted packed keys (index order = key order).
+constexpr int DC_ITEMS = 8;
+constexpr uint32_t DC_TILE = NT * DC_ITEMS;  // index entries per tile
+
+template <class K, bool TROP>
+__global__ void __launch_bounds__(NT)
+    k_dense_compact(const uint32_t* __restrict__ bits, const int32_t* __restrict__ D, uint64_t entries, int b1,
+                    uint64_t n1, K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap,
+                    uint64_t* states, uint32_t* counter, uint64_t* d_count, uint32_t* status) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_scan[NT / 32 + 1];
+  __shared__ uint64_t s_ex;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t tile = claim_tile(counter, &s_tile);
+  // blocked: thread owns DC_ITEMS consecutive entries
+  const uint64_t b = (uint64_t)tile * DC_TILE + (uint64_t)tid * DC_ITEMS;
+  uint32_t present = 0;
+  int32_t wv[DC_ITEMS];
+#pragma unroll
+  for (int j = 0; j < DC_ITEMS; j++) {
+    const uint64_t ix = b + j;
+    bool p = false;
+    if (ix < entries) {
+      if constexpr (TROP) {
+        wv[j] = D[ix];
+        p = wv[j] != INT32_MAX;
+      } else {
+        p = (bits[ix >> 5] >> (ix & 31)) & 1u;
+      }
+    }
+    present |= (p ? 1u : 0u) << j;
+  }
+  uint32_t tot;
+  const uint32_t ex = block_excl_sum<NT>((uint32_t)__popc(present), s_scan, &tot);
+  if (warp == 0) {
+    const uint64_t e = warp_lookback(states, tile, tot, status);
+    if (lane == 0) {
+      s_ex = e;
+      if (tile == gridDim.x - 1) *d_count = e + tot;
+    }
+  }
+  __syncthreads();
+  uint64_t at = s_ex + ex;
+#pragma unroll
+  for (int j = 0; j < DC_ITEMS; j++) {
+    if ((present >> j) & 1u) {
+      const uint64_t ix = b + j;
+      if (at < out_cap) {
+        out[at] = (K)(((K)(ix / n1) << b1) | (K)(ix % n1));
+        if constexpr (TROP) out_w[at] = wv[j];
+      } else {
+        atomicOr(status, ST_BOUNDS);
+      }
+      at++;
+    }
+  }
+}
+
+inline unsigned grid1(uint64_t n) { return (unsigned)ceil_div(n ? n : 1, NT); }
+
+}  // namespace
+
+uint64_t dense_tile_size() { return DE_TILE; }
+
+template <class K, bool TROP>
+void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n, const uint64_t* pos,
+                  uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift,
+                  int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr, uint64_t n_nbr,
+                  const int32_t* nbr_w, int b1, uint64_t n1, uint64_t entries, uint32_t* bits, int32_t* D,
+                  K* out, uint64_t out_cap, uint64_t* d_out_count, uint64_t* splits_buf) {
+  if (n == 0 || total == 0) return;
+  const uint64_t tiles = ceil_div(n + total, DE_TILE);
+  if (tiles > 0x7fffffffull) fail(STRATA_E_UNSUPPORTED, "expand too large for one launch");
+  k_tile_splits<<<grid1(tiles + 1), NT, 0, ctx->stream>>>(pos, n, total, DE_TILE, tiles, splits_buf);
+  after_launch(ctx, "k_tile_splits");
+  const uint64_t mask1 = b1 >= 64 ? ~0ull : ((1ull << b1) - 1);
+  const int kh = kprof_begin(ctx, K_EXPAND_EMIT);
+  k_expand_dense<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(
+      dkeys, dw, n, pos, total, splits_buf, jshift, jmask, pshift, pmask, out_pshift, out_vshift, off, n_nodes,
+      nbr, n_nbr, nbr_w, b1, mask1, n1, entries, bits, D, out, out_cap,
+      reinterpret_cast<unsigned long long*>(d_out_count), ctx->d_status);
+  // Algorithmic bytes: Δ rows, CSR segments streamed, one 4-byte index probe
+  // per candidate; appends are counted by the caller once their number is known.
+  const uint64_t wsz = TROP ? 4 : 0;
+  kprof_end(ctx, kh, n * (sizeof(K) + wsz + 8 + 4) + total * (4 + wsz) + total * (TROP ? 4 : 4));
+  after_launch(ctx, "k_expand_dense");
+}
+
+template <class K>
+void dense_gather(strata_ctx* ctx, const K* keys, uint64_t n, int b1, uint64_t n1, uint64_t entries,
+                  const int32_t* D, int32_t* w) {
+  if (!n) return;
+  const uint64_t mask1 = (1ull << b1) - 1;
+  k_dense_gather<K><<<grid1(n), NT, 0, ctx->stream>>>(keys, n, b1, mask1, n1, entries, D, w, ctx->d_status);
+  after_launch(ctx, "k_dense_gather");
+}
+
+template <class K, bool TROP>
+void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, int b1, uint64_t n1,
+                uint64_t entries, uint32_t* bits, int32_t* D) {
+  if (TROP) {
+    k_fill_i32<<<(unsigned)std::min<uint64_t>(ceil_div(entries, NT), (uint64_t)ctx->num_sms * 16), NT, 0,
+                 ctx->stream>>>(D, entries, INT32_MAX);
+    after_launch(ctx, "k_fill_i32");
+  }
+  if (!n) return;
+  const uint64_t mask1 = (1ull << b1) - 1;
+  k_dense_seed<K, TROP><<<grid1(n), NT, 0, ctx->stream>>>(keys, w, n, b1, mask1, n1, entries, bits, D, ctx->d_status);
+  after_launch(ctx, "k_dense_seed");
+}
+
+template <class K, bool TROP>
+uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, uint64_t entries, int b1,
+                       uint64_t n1, K* out, int32_t* out_w, uint64_t out_cap) {
+  if (!entries) return 0;
+  const uint64_t tiles = ceil_div(entries, DC_TILE);
+  DBuf<uint64_t> states(ctx, tiles + 2);
+  uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles + 1);
+  SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 2), ctx->stream));
+  k_dense_compact<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(bits, D, entries, b1, n1, out, out_w, out_cap,
+                                                                    states.p, counter, states.p + tiles,
+                                                                    ctx->d_status);
+  after_launch(ctx, "k_dense_compact");
+  uint64_t r;
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, states.p + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  sync_and_check(ctx);
+  r = ctx->h_scalar[0];
+  return r;
+}
+
+#define SK_INST_DENSE(K, T)                                                                               \
+  template void dense_expand<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const uint64_t*,       \
+                                   uint64_t, int, uint64_t, int, uint64_t, int, int, const uint32_t*,      \
+                                   uint64_t, const uint32_t*, uint64_t, const int32_t*, int, uint64_t,     \
+                                   uint64_t, uint32_t*, int32_t*, K*, uint64_t, uint64_t*, uint64_t*);     \
+  template void dense_seed<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, int, uint64_t, uint64_t, \
+                                 uint32_t*, int32_t*);                                                     \
+  template uint64_t dense_compact<K, T>(strata_ctx*, const uint32_t*, const int32_t*, uint64_t, int,       \
+                                        uint64_t, K*, int32_t*, uint64_t);
+SK_INST_DENSE(uint32_t, false)
+SK_INST_DENSE(uint32_t, true)
+SK_INST_DENSE(uint64_t, false)
+SK_INST_DENSE(uint64_t, true)
+#undef SK_INST_DENSE
+template void dense_gather<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, uint64_t,
+                                     const int32_t*, int32_t*);
+template void dense_gather<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, uint64_t, uint64_t,
+                                     const int32_t*, int32_t*);
+
+}  // namespace sk

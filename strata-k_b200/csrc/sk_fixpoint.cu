@@ -20,6 +20,7 @@
 #include "sk_rel.cuh"
 
 #include <cmath>
+#include <type_traits>
 
 namespace sk {
 namespace {
@@ -301,13 +302,115 @@ void fill_stats(strata_fix_stats* st, const Acct& a, uint64_t rounds, uint64_t r
   st->other_launches = (uint32_t)(launches > phase ? launches - phase : 0);
 }
 
+// ---- direct-addressed plan ---------------------------------------------------------
+// Index over (c0, c1) in [0, n0) × [0, n1): a bitmap (Bool relation, or the
+// per-round first-touch marks of a Trop relation) and an int32 weight array.
+struct DenseIdx {
+  DBuf<uint32_t> bits;
+  DBuf<int32_t> D;
+  uint64_t n0 = 0, n1 = 0, entries = 0;
+  uint64_t words() const { return (entries + 31) / 32; }
+};
+
+// Bytes the index needs; the plan is used when they stay within budget.
+inline double dense_bytes(bool trop, uint64_t entries) {
+  return (trop ? 4.0 * (double)entries : 0.0) + (double)entries / 8.0;
+}
+constexpr double kDenseBudget = 16e9;
+
+inline bool want_dense(strata_ctx* ctx, bool trop, bool narrow, uint64_t n0, uint64_t n1) {
+  const long double e = (long double)n0 * (long double)n1;
+  const bool fits = (!trop || narrow) && e < 9.0e18L && dense_bytes(trop, (uint64_t)e) <= kDenseBudget;
+  if (ctx->plan == 1) return false;
+  if (ctx->plan == 2 && !fits)
+    fail(STRATA_E_UNSUPPORTED, "the direct-addressed plan needs int32 weights and an index within 16 GB");
+  return fits;
+}
+
+template <bool TROP>
+void dense_alloc(strata_ctx* ctx, DenseIdx& X, uint64_t n0, uint64_t n1) {
+  X.bits.ctx = X.D.ctx = ctx;
+  X.n0 = n0;
+  X.n1 = n1;
+  X.entries = n0 * n1;
+  X.bits.reserve(X.words() + 1);
+  SK_CUDA(cudaMemsetAsync(X.bits.p, 0, (X.words() + 1) * 4, ctx->stream));
+  if (TROP) X.D.reserve(X.entries + 1);
+}
+
+// One round on the index: Δ' (keys in first-touch order, weights from D).
+template <class K, bool TROP>
+uint64_t dense_round(strata_ctx* ctx, const K* dk, const int32_t* dw, uint64_t nd, const Csr<int32_t>& csr,
+                     const JoinSpec& js, int b1, DenseIdx& X, Rel<K, int32_t>& out, Scratch<K, int32_t>& s,
+                     DBuf<uint64_t>& splits, PhaseTimer& pt, Acct& a) {
+  if (nd == 0) return 0;
+  const uint64_t l0 = ctx->launches;
+  const int t = pt.begin(&a.join_ms);
+  s.pos.reserve_grow(nd + 1);
+  expand_offsets<K>(ctx, dk, nd, js.jshift, js.jmask, csr.off.p, csr.n_nodes, s.pos.p);
+  uint64_t T = 0;
+  read_checked(ctx, s.pos.p + nd, &T, 1);
+  uint64_t cnt = 0;
+  if (T) {
+    if (TROP) SK_CUDA(cudaMemsetAsync(X.bits.p, 0, X.words() * 4, ctx->stream));
+    const uint64_t cap = std::min<uint64_t>(T, X.entries) + 1;
+    out.reserve(cap, TROP);
+    splits.reserve_grow(ceil_div(nd + T, dense_tile_size()) + 2);
+    SK_CUDA(cudaMemsetAsync(s.counts.p, 0, 8, ctx->stream));
+    dense_expand<K, TROP>(ctx, dk, dw, nd, s.pos.p, T, js.jshift, js.jmask, js.pshift, js.pmask, js.out_pshift,
+                          js.out_vshift, csr.off.p, csr.n_nodes, csr.nbr.p, csr.m, TROP ? csr.w.p : nullptr, b1,
+                          X.n1, X.entries, X.bits.p, TROP ? X.D.p : nullptr, out.k.p, cap, s.counts.p,
+                          splits.p);
+    read_checked(ctx, s.counts.p, &cnt, 1);
+    if (TROP) dense_gather<K>(ctx, out.k.p, cnt, b1, X.n1, X.entries, X.D.p, out.w.p);
+    kprof_add_last(ctx, K_EXPAND_EMIT, cnt * (sizeof(K) + (TROP ? 8 : 0)));
+  }
+  pt.end(t);
+  const uint64_t wsz = TROP ? 4 : 0;
+  a.join_b += nd * (sizeof(K) + wsz + 16) + T * (4 + wsz) + T * 4 + cnt * (sizeof(K) + 2 * wsz);
+  a.join_l += (uint32_t)(ctx->launches - l0);
+  a.cands += T;
+  return cnt;
+}
+
+template <class K, bool TROP>
+void fix_loop_dense(strata_ctx* ctx, Rel<K, int32_t>& delta, const Csr<int32_t>& csr, const JoinSpec& js, int b1,
+                    DenseIdx& X, uint64_t cap, Scratch<K, int32_t>& s, PhaseTimer& pt, Acct& a,
+                    uint64_t* rounds_out) {
+  Rel<K, int32_t> dnext;
+  dnext.k.ctx = dnext.w.ctx = ctx;
+  DBuf<uint64_t> splits;
+  splits.ctx = ctx;
+  uint64_t rounds = 0;
+  while (delta.n > 0) {
+    rounds++;
+    const uint64_t nd = dense_round<K, TROP>(ctx, delta.k.p, TROP ? delta.w.p : nullptr, delta.n, csr, js, b1, X,
+                                             dnext, s, splits, pt, a);
+    delta.swap(dnext);
+    delta.n = nd;
+    if (TROP && cap && rounds > cap)
+      fail(STRATA_E_NEG_CYCLE, "negative-weight cycle: tropical stratum diverges");
+  }
+  *rounds_out = rounds;
+}
+
+// Compact the index into a sorted relation.
+template <class K, bool TROP>
+void dense_finish(strata_ctx* ctx, DenseIdx& X, int b1, Rel<K, int32_t>& full, uint64_t upper) {
+  const uint64_t cap = std::min<uint64_t>(upper, X.entries) + 1;
+  full.reserve(cap, TROP);
+  full.n = dense_compact<K, TROP>(ctx, X.bits.p, TROP ? X.D.p : nullptr, X.entries, b1, X.n1, full.k.p,
+                                  TROP ? full.w.p : nullptr, cap);
+}
+
 // ---- TC-shaped drivers: head(X,Z) :- edge(X,Y), head(Y,Z) -----------------------
 template <class K, class W, bool TROP>
 strata_rel* run_tc_shape(strata_ctx* ctx, const EdgeCols& e, int b0, int b1, int bsrc,
                          uint64_t n_nodes_dst, uint64_t universe, uint64_t cap, strata_fix_stats* st,
-                         EventTimer& et, uint64_t l_start) {
+                         EventTimer& et, uint64_t l_start, uint64_t n_nodes_src, bool dense) {
   PhaseTimer pt(ctx);
   Acct a;
+  uint32_t plan = 1;
   const int key_bits = b0 + b1;
   // path0 = normalize(edge): every edge is derived by the base rule.
   Rel<K, W> full, delta;
@@ -335,17 +438,30 @@ strata_rel* run_tc_shape(strata_ctx* ctx, const EdgeCols& e, int b0, int b1, int
   JoinSpec js{b1, low_mask(b0), 0, low_mask(b1), 0, b1};
   Scratch<K, W> s(ctx);
   uint64_t rounds = 0;
-  fix_loop<K, W, TROP>(ctx, full, delta, csr, js, key_bits, cap, s, pt, a, &rounds);
+  if constexpr (std::is_same<W, int32_t>::value) {
+    if (dense) {
+      plan = 2;
+      DenseIdx X;
+      dense_alloc<TROP>(ctx, X, n_nodes_src, n_nodes_dst);
+      if (TROP) dense_seed<K, true>(ctx, full.k.p, full.w.p, full.n, b1, X.n1, X.entries, X.bits.p, X.D.p);
+      else dense_seed<K, false>(ctx, full.k.p, nullptr, full.n, b1, X.n1, X.entries, X.bits.p, nullptr);
+      fix_loop_dense<K, TROP>(ctx, delta, csr, js, b1, X, cap, s, pt, a, &rounds);
+      dense_finish<K, TROP>(ctx, X, b1, full, X.entries);
+    }
+  }
+  if (plan == 1) fix_loop<K, W, TROP>(ctx, full, delta, csr, js, key_bits, cap, s, pt, a, &rounds);
   const double ms = et.stop();
   pt.collect();
   kprof_collect(ctx);
   fill_stats(st, a, rounds, full.n, universe, key_bits, TROP ? sizeof(W) : 0, ms, ctx->launches - l_start);
+  if (st) st->plan = plan;
   return finish_rel<K, W, TROP>(ctx, full, b1);
 }
 
 struct Layout {
   int b0, b1, bsrc;
-  uint64_t n_nodes;
+  uint64_t n_nodes;      // max dst + 1
+  uint64_t n_nodes_src;  // max src + 1
   bool wide_key;
 };
 
@@ -356,6 +472,7 @@ Layout tc_layout(strata_ctx* ctx, const EdgeCols& e) {
   L.b1 = std::max(1, bits_for(md));
   L.bsrc = L.b0;
   L.n_nodes = (uint64_t)md + 1;
+  L.n_nodes_src = (uint64_t)ms + 1;
   L.wide_key = L.b0 + L.b1 > 32;
   return L;
 }
@@ -380,9 +497,12 @@ strata_rel* fix_tc_bool(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats* st
     return rel;
   }
   const Layout L = tc_layout(ctx, e);
+  const bool dense = want_dense(ctx, false, true, L.n_nodes_src, L.n_nodes);
   if (!L.wide_key)
-    return run_tc_shape<uint32_t, int32_t, false>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, 0, 0, st, et, l_start);
-  return run_tc_shape<uint64_t, int32_t, false>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, 0, 0, st, et, l_start);
+    return run_tc_shape<uint32_t, int32_t, false>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, 0, 0, st, et, l_start,
+                                                  L.n_nodes_src, dense);
+  return run_tc_shape<uint64_t, int32_t, false>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, 0, 0, st, et, l_start,
+                                                L.n_nodes_src, dense);
 }
 
 strata_rel* fix_trop_paths(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats* st) {
@@ -401,14 +521,20 @@ strata_rel* fix_trop_paths(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats*
   const uint64_t universe = count_distinct_ids(ctx, e.src, e.n, e.dst, e.n, nullptr, 0, limit);
   const uint64_t cap = universe + 2;
   const bool narrow = narrow_ok(universe, max_abs_weight(ctx, e.w, e.inf, e.n), 0);
+  const bool dense = want_dense(ctx, true, narrow, L.n_nodes_src, L.n_nodes);
+  const uint64_t ns = L.n_nodes_src;
   if (!L.wide_key) {
     if (narrow)
-      return run_tc_shape<uint32_t, int32_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et, l_start);
-    return run_tc_shape<uint32_t, int64_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et, l_start);
+      return run_tc_shape<uint32_t, int32_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et,
+                                                   l_start, ns, dense);
+    return run_tc_shape<uint32_t, int64_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et,
+                                                 l_start, ns, false);
   }
   if (narrow)
-    return run_tc_shape<uint64_t, int32_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et, l_start);
-  return run_tc_shape<uint64_t, int64_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et, l_start);
+    return run_tc_shape<uint64_t, int32_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et,
+                                                 l_start, ns, dense);
+  return run_tc_shape<uint64_t, int64_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et,
+                                               l_start, ns, false);
 }
 
 // ---- MSSP: dist(S,Y) :- src(S), edge(S,Y). dist(S,Z) :- dist(S,Y), edge(Y,Z). ----
@@ -418,7 +544,8 @@ template <class K, class W>
 strata_rel* run_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* src_w,
                      const uint8_t* src_inf, uint64_t ns, const EdgeCols& e, int b0, int b1,
                      int besrc, uint64_t n_nodes_src, uint64_t universe, uint64_t cap,
-                     strata_fix_stats* st, EventTimer& et, uint64_t l_start) {
+                     strata_fix_stats* st, EventTimer& et, uint64_t l_start, uint64_t n0, uint64_t n1,
+                     bool dense) {
   PhaseTimer pt(ctx);
   Acct a;
   const int key_bits = b0 + b1;
@@ -438,28 +565,51 @@ strata_rel* run_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
   else
     build_edge_csr<uint64_t, W, true>(ctx, e, 0, besrc, b1, n_nodes_src, csr);
   Scratch<K, W> s(ctx);
-  // Bootstrap: dist0 = min-reduce(src ⋈ edge), all of it new.
   const JoinSpec boot{0, ~0ull, 0, ~0ull, b1, 0};
-  const uint64_t n0 = derive<K, W, true>(ctx, srcu.k.p, srcu.w.p, srcu.n, csr, boot, key_bits, s, pt, a);
+  // Δ(S,Y): join Y = key & mask(b1), kept S = key >> b1, out = (S << b1) | Z.
+  const JoinSpec step{0, low_mask(b1), b1, low_mask(b0), b1, 0};
+  if constexpr (std::is_same<W, int32_t>::value) {
+    if (dense) {
+      DenseIdx X;
+      dense_alloc<true>(ctx, X, n0, n1);
+      dense_seed<K, true>(ctx, nullptr, nullptr, 0, b1, X.n1, X.entries, X.bits.p, X.D.p);
+      Rel<K, W> delta, full;
+      delta.k.ctx = delta.w.ctx = full.k.ctx = full.w.ctx = ctx;
+      DBuf<uint64_t> splits;
+      splits.ctx = ctx;
+      // Bootstrap: every derivation of src ⋈ edge, all new.
+      delta.n = dense_round<K, true>(ctx, srcu.k.p, srcu.w.p, srcu.n, csr, boot, b1, X, delta, s, splits, pt, a);
+      uint64_t rounds = 0;
+      fix_loop_dense<K, true>(ctx, delta, csr, step, b1, X, cap, s, pt, a, &rounds);
+      dense_finish<K, true>(ctx, X, b1, full, X.entries);
+      const double ms = et.stop();
+      pt.collect();
+      kprof_collect(ctx);
+      fill_stats(st, a, rounds, full.n, universe, key_bits, sizeof(W), ms, ctx->launches - l_start);
+      if (st) st->plan = 2;
+      return finish_rel<K, W, true>(ctx, full, b1);
+    }
+  }
+  // Bootstrap: dist0 = min-reduce(src ⋈ edge), all of it new.
+  const uint64_t nb = derive<K, W, true>(ctx, srcu.k.p, srcu.w.p, srcu.n, csr, boot, key_bits, s, pt, a);
   Rel<K, W> full, delta;
   full.k.ctx = full.w.ctx = delta.k.ctx = delta.w.ctx = ctx;
-  full.reserve(n0 + 1, true);
-  delta.reserve(n0 + 1, true);
-  full.n = delta.n = n0;
-  if (n0) {
-    SK_CUDA(cudaMemcpyAsync(full.k.p, s.uk.p, n0 * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
-    SK_CUDA(cudaMemcpyAsync(full.w.p, s.uw.p, n0 * sizeof(W), cudaMemcpyDeviceToDevice, ctx->stream));
-    SK_CUDA(cudaMemcpyAsync(delta.k.p, s.uk.p, n0 * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
-    SK_CUDA(cudaMemcpyAsync(delta.w.p, s.uw.p, n0 * sizeof(W), cudaMemcpyDeviceToDevice, ctx->stream));
+  full.reserve(nb + 1, true);
+  delta.reserve(nb + 1, true);
+  full.n = delta.n = nb;
+  if (nb) {
+    SK_CUDA(cudaMemcpyAsync(full.k.p, s.uk.p, nb * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
+    SK_CUDA(cudaMemcpyAsync(full.w.p, s.uw.p, nb * sizeof(W), cudaMemcpyDeviceToDevice, ctx->stream));
+    SK_CUDA(cudaMemcpyAsync(delta.k.p, s.uk.p, nb * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
+    SK_CUDA(cudaMemcpyAsync(delta.w.p, s.uw.p, nb * sizeof(W), cudaMemcpyDeviceToDevice, ctx->stream));
   }
-  // Δ(S,Y): join Y = key & mask(b1), kept S = key >> b1, out = (S << b1) | Z.
-  const JoinSpec js{0, low_mask(b1), b1, low_mask(b0), b1, 0};
   uint64_t rounds = 0;
-  fix_loop<K, W, true>(ctx, full, delta, csr, js, key_bits, cap, s, pt, a, &rounds);
+  fix_loop<K, W, true>(ctx, full, delta, csr, step, key_bits, cap, s, pt, a, &rounds);
   const double ms = et.stop();
   pt.collect();
   kprof_collect(ctx);
   fill_stats(st, a, rounds, full.n, universe, key_bits, sizeof(W), ms, ctx->launches - l_start);
+  if (st) st->plan = 1;
   return finish_rel<K, W, true>(ctx, full, b1);
 }
 
@@ -491,14 +641,20 @@ strata_rel* fix_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
   const bool narrow = narrow_ok(universe, max_abs_weight(ctx, e.w, e.inf, e.n),
                                 max_abs_weight(ctx, src_w, src_inf, ns));
   const uint64_t nn = (uint64_t)mes + 1;
+  const uint64_t n0 = (uint64_t)mS + 1, n1 = (uint64_t)med + 1;
+  const bool dense = want_dense(ctx, true, narrow, n0, n1);
   if (b0 + b1 <= 32) {
     if (narrow)
-      return run_mssp<uint32_t, int32_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st, et, l_start);
-    return run_mssp<uint32_t, int64_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st, et, l_start);
+      return run_mssp<uint32_t, int32_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st,
+                                         et, l_start, n0, n1, dense);
+    return run_mssp<uint32_t, int64_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st,
+                                       et, l_start, n0, n1, false);
   }
   if (narrow)
-    return run_mssp<uint64_t, int32_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st, et, l_start);
-  return run_mssp<uint64_t, int64_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st, et, l_start);
+    return run_mssp<uint64_t, int32_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st, et,
+                                       l_start, n0, n1, dense);
+  return run_mssp<uint64_t, int64_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st, et,
+                                     l_start, n0, n1, false);
 }
 
 // ---- relation handles ---------------------------------------------------------------

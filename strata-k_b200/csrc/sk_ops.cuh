@@ -26,6 +26,24 @@ uint64_t radix_sort_u32_static_bytes(uint64_t max_n);
 void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* out, uint64_t n, int bits,
                            unsigned char* scratch, uint64_t max_n, uint32_t* h_status);
 
+// ---- direct-addressed plan (sk_dense.cu) ----
+uint64_t dense_tile_size();
+template <class K, bool TROP>
+void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n, const uint64_t* pos,
+                  uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift,
+                  int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr, uint64_t n_nbr,
+                  const int32_t* nbr_w, int b1, uint64_t n1, uint64_t entries, uint32_t* bits, int32_t* D,
+                  K* out, uint64_t out_cap, uint64_t* d_out_count, uint64_t* splits_buf);
+template <class K>
+void dense_gather(strata_ctx* ctx, const K* keys, uint64_t n, int b1, uint64_t n1, uint64_t entries,
+                  const int32_t* D, int32_t* w);
+template <class K, bool TROP>
+void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, int b1, uint64_t n1,
+                uint64_t entries, uint32_t* bits, int32_t* D);
+template <class K, bool TROP>
+uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, uint64_t entries, int b1,
+                       uint64_t n1, K* out, int32_t* out_w, uint64_t out_cap);
+
 // Exclusive scan of per-element expand degrees (see sk_relops.cu).
 // pos[i] = sum_{k<i} deg(i); pos[n] = total.  Returns nothing; read pos[n].
 template <class K>

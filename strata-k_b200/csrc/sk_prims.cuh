@@ -150,7 +150,8 @@ __device__ __forceinline__ uint64_t upper_bound_dev(const K* a, uint64_t lo, uin
 // are only used when the host has proven every derived sum stays strictly
 // inside the range, so they need no overflow test.
 template <class W> struct WInf;
-template <> struct WInf<int32_t> { static constexpr int32_t v = 0x7fffffff; };
+// int32 keeps INT32_MAX free for "absent" in the direct-addressed plan.
+template <> struct WInf<int32_t> { static constexpr int32_t v = 0x7ffffffe; };
 template <> struct WInf<int64_t> { static constexpr int64_t v = 0x7fffffffffffffffll; };
 
 __device__ __forceinline__ int32_t trop_mul(int32_t a, int32_t b, uint32_t* flags) {

@@ -26,6 +26,8 @@ E_UNSUPPORTED = 7
 E_NOT_BUILT = 8
 E_WEIGHT_RANGE = 9
 
+PLAN_AUTO, PLAN_SORT_MERGE, PLAN_DENSE = 0, 1, 2
+
 KERNELS = {0: "k_onesweep", 1: "k_expand_emit", 2: "k_expand_offsets", 3: "k_reduce_runs",
            4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count"}
 
@@ -48,7 +50,7 @@ class FixStats(C.Structure):
         ("merge_bytes", C.c_uint64),
         ("sort_launches", C.c_uint32), ("join_launches", C.c_uint32),
         ("diff_launches", C.c_uint32), ("merge_launches", C.c_uint32),
-        ("other_launches", C.c_uint32),
+        ("other_launches", C.c_uint32), ("plan", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -73,6 +75,7 @@ SIGNATURES = {
     "strata_last_error": (C.c_char_p, [ctxp]),
     "strata_ctx_mem": (C.c_int, [ctxp, u64p, u64p]),
     "strata_ctx_set_profiling": (C.c_int, [ctxp, C.c_int]),
+    "strata_ctx_set_plan": (C.c_int, [ctxp, C.c_int]),
     "strata_ctx_launches": (C.c_uint64, [ctxp]),
     "strata_ctx_kernel_stats": (C.c_int, [ctxp, C.c_int, u64p, C.POINTER(C.c_double), u64p]),
     "strata_ctx_reset_kernel_stats": (C.c_int, [ctxp]),

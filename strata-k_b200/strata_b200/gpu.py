@@ -211,6 +211,10 @@ class Engine:
         """Run on an existing ``cudaStream_t`` (e.g. ``torch.cuda.Stream().cuda_stream``)."""
         self._check(self.lib.strata_ctx_set_stream(self.ctx, C.c_void_p(stream_handle or 0)))
 
+    def set_plan(self, plan: int):
+        """0 automatic, 1 sort-merge, 2 direct-addressed (results are identical)."""
+        self._check(self.lib.strata_ctx_set_plan(self.ctx, plan))
+
     def set_profiling(self, on: bool):
         self._check(self.lib.strata_ctx_set_profiling(self.ctx, 1 if on else 0))
 

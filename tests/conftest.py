@@ -40,3 +40,12 @@ class Lcg:
 @pytest.fixture
 def lcg():
     return Lcg
+
+
+@pytest.fixture(params=[0, 1], ids=["auto", "sortmerge"])
+def peng(request, engine):
+    """The engine with plan 0 (automatic: direct-addressed where it applies)
+    and plan 1 (sort-merge forced); both must give identical results."""
+    engine.set_plan(request.param)
+    yield engine
+    engine.set_plan(0)

@@ -33,7 +33,8 @@ def _otrop(cols):
 @pytest.mark.parametrize("edges", [
     [(0, 1), (1, 2), (2, 3)], [(0, 1), (1, 0)], [(5, 5), (5, 5), (5, 6)], [],
 ])
-def test_tc_fixed_cases(engine, edges):
+def test_tc_fixed_cases(peng, edges):
+    engine = peng
     got = engine.transitive_closure_bool(edges)
     s = [e[0] for e in edges]
     d = [e[1] for e in edges]
@@ -41,7 +42,8 @@ def test_tc_fixed_cases(engine, edges):
     assert _pairs(got) == list(zip(a.tolist(), b.tolist()))
 
 
-def test_tc_random_small(engine, lcg):
+def test_tc_random_small(peng, lcg):
+    engine = peng
     rng = lcg(0x123456789ABCDEF0)
     for trial in range(200):
         nodes = 3 + rng.upto(8)
@@ -54,7 +56,8 @@ def test_tc_random_small(engine, lcg):
             assert got.stats["rounds"] == r
 
 
-def test_tc_chain_400(engine):
+def test_tc_chain_400(peng):
+    engine = peng
     n = 400
     got = engine.transitive_closure_bool((np.arange(n), np.arange(1, n + 1)))
     assert len(got) == (n + 1) * n // 2
@@ -64,7 +67,8 @@ def test_tc_chain_400(engine):
 
 
 @pytest.mark.parametrize("n,m,seed", [(200, 600, 1), (2000, 6000, 2), (5000, 12000, 3)])
-def test_tc_er_medium_exact(engine, n, m, seed):
+def test_tc_er_medium_exact(peng, n, m, seed):
+    engine = peng
     s, d = gen.er_directed(n, m, seed)
     a, b, r = O.fast_tc(s, d)
     got = engine.transitive_closure_bool((s, d))
@@ -72,8 +76,9 @@ def test_tc_er_medium_exact(engine, n, m, seed):
     assert got.stats["rounds"] == r
 
 
-def test_tc_wide_keys(engine):
+def test_tc_wide_keys(peng):
     """Ids above 2^16 force 64-bit packed keys."""
+    engine = peng
     rng = np.random.default_rng(4)
     s = rng.integers(0, 1 << 31, 3000).astype(np.uint32)
     d = rng.choice(s, 3000).astype(np.uint32)
@@ -83,8 +88,9 @@ def test_tc_wide_keys(engine):
     assert np.array_equal(got.src, a) and np.array_equal(got.dst, b)
 
 
-def test_tc_config_size_fingerprint(engine):
+def test_tc_config_size_fingerprint(peng):
     """ER(10 000, 50 000): count + fingerprint equal a per-source BFS closure."""
+    engine = peng
     w = gen.tc_workload()
     cnt, fp = O.bfs_closure(w.src, w.dst)
     import torch
@@ -99,12 +105,14 @@ def test_tc_config_size_fingerprint(engine):
 
 
 # ------------------------------------------------------------------ Trop all-pairs
-def test_trop_fixed_case(engine):
+def test_trop_fixed_case(peng):
+    engine = peng
     got = engine.shortest_paths_trop([(0, 2, 10), (0, 1, 2), (1, 2, 3)])
     assert _trop(got) == [(0, 1, 2), (0, 2, 5), (1, 2, 3)]
 
 
-def test_trop_random_small(engine, lcg):
+def test_trop_random_small(peng, lcg):
+    engine = peng
     rng = lcg(0xDEADBEEFCAFE1234)
     for trial in range(200):
         nodes = 3 + rng.upto(6)
@@ -116,7 +124,8 @@ def test_trop_random_small(engine, lcg):
         assert _trop(got) == _otrop(want), (trial, edges)
 
 
-def test_trop_weighted_chain_300(engine):
+def test_trop_weighted_chain_300(peng):
+    engine = peng
     n = 300
     got = engine.shortest_paths_trop((np.arange(n), np.arange(1, n + 1), np.arange(1, n + 1)))
     want = []
@@ -128,19 +137,22 @@ def test_trop_weighted_chain_300(engine):
     assert _trop(got) == want
 
 
-def test_trop_overflow_is_error(engine):
+def test_trop_overflow_is_error(peng):
+    engine = peng
     with pytest.raises(S.TropOverflow):
         engine.shortest_paths_trop([(0, 1, I64_MAX - 5), (1, 2, 6)])
     # the context stays usable afterwards
     assert _trop(engine.shortest_paths_trop([(0, 1, 1)])) == [(0, 1, 1)]
 
 
-def test_trop_negative_cycle(engine):
+def test_trop_negative_cycle(peng):
+    engine = peng
     with pytest.raises(S.NegativeWeightCycle):
         engine.shortest_paths_trop([(0, 1, 1), (1, 0, -2)])
 
 
-def test_trop_pos_inf(engine):
+def test_trop_pos_inf(peng):
+    engine = peng
     got = engine.shortest_paths_trop([(0, 1, O.POS_INF), (1, 2, 4), (0, 2, O.POS_INF)])
     assert _trop(got) == [(0, 1, O.POS_INF), (0, 2, O.POS_INF), (1, 2, 4)]
     # a finite derivation improves a +inf tuple
@@ -154,8 +166,9 @@ def test_trop_finite_i64_max_is_reported(engine):
 
 
 @pytest.mark.parametrize("scale_w", [100, 10**12])
-def test_trop_medium_narrow_and_wide(engine, scale_w):
+def test_trop_medium_narrow_and_wide(peng, scale_w):
     """Small weights run in int32 lanes, huge ones in int64 lanes: same answers."""
+    engine = peng
     rng = np.random.default_rng(11)
     n, m = 300, 1500
     s = rng.integers(0, n, m)
@@ -168,7 +181,8 @@ def test_trop_medium_narrow_and_wide(engine, scale_w):
     assert got.stats["rounds"] == want[4]
 
 
-def test_trop_negative_weights_no_cycle(engine):
+def test_trop_negative_weights_no_cycle(peng):
+    engine = peng
     rng = np.random.default_rng(12)
     n = 60
     s = rng.integers(0, n, 200)
@@ -181,7 +195,8 @@ def test_trop_negative_weights_no_cycle(engine):
 
 
 # ------------------------------------------------------------------ MSSP (bench shape)
-def test_mssp_random_small(engine):
+def test_mssp_random_small(peng):
+    engine = peng
     rng = np.random.default_rng(7)
     for trial in range(60):
         n = int(rng.integers(4, 14))
@@ -197,7 +212,8 @@ def test_mssp_random_small(engine):
         assert got.stats["rounds"] == want[4]
 
 
-def test_mssp_rmat_scale12_exact(engine):
+def test_mssp_rmat_scale12_exact(peng):
+    engine = peng
     wl = gen.mssp_workload(scale=12, n_sources=64, seed=5)
     want = O.fast_trop(1, wl.src, wl.dst, wl.w, sources=wl.sources, source_w=wl.source_w)
     got = engine.mssp_trop(wl.sources, (wl.src, wl.dst, wl.w), source_weights=wl.source_w)
@@ -206,7 +222,8 @@ def test_mssp_rmat_scale12_exact(engine):
     assert got.stats["rounds"] == want[4]
 
 
-def test_mssp_rmat_scale16_matches_dijkstra(engine):
+def test_mssp_rmat_scale16_matches_dijkstra(peng):
+    engine = peng
     import torch
     wl = gen.mssp_workload(scale=16, n_sources=64, seed=6)
     cnt, fp = O.dijkstra_mssp(wl.sources, wl.src, wl.dst, wl.w, wl.source_w)
@@ -218,7 +235,8 @@ def test_mssp_rmat_scale16_matches_dijkstra(engine):
     rel.free()
 
 
-def test_mssp_overflow(engine):
+def test_mssp_overflow(peng):
+    engine = peng
     with pytest.raises(S.TropOverflow):
         engine.mssp_trop([0], [(0, 1, 5), (1, 2, I64_MAX - 2)])
 
@@ -394,3 +412,25 @@ def test_launch_counter_and_memory_returned(engine):
     assert engine.launches() > before
     in_use, peak = engine.mem()
     assert in_use == 0 and peak > 0
+
+
+def test_plans_pick_and_agree(engine):
+    """Automatic planning picks the direct-addressed plan for the benchmark
+    shapes; forcing sort-merge gives the same relation and round count."""
+    wl = gen.mssp_workload(scale=11, n_sources=32, seed=8)
+    res = {}
+    for plan in (0, 1, 2):
+        engine.set_plan(plan)
+        r = engine.mssp_trop(wl.sources, (wl.src, wl.dst, wl.w), source_weights=wl.source_w)
+        res[plan] = r
+    engine.set_plan(0)
+    assert res[0].stats["plan"] == 2 and res[1].stats["plan"] == 1 and res[2].stats["plan"] == 2
+    for p in (1, 2):
+        assert np.array_equal(res[0].src, res[p].src) and np.array_equal(res[0].dst, res[p].dst)
+        assert np.array_equal(res[0].w, res[p].w) and res[0].stats["rounds"] == res[p].stats["rounds"]
+    # wide weights cannot use the int32 index: forcing it is an error, auto falls back
+    engine.set_plan(2)
+    with pytest.raises(S.Unsupported):
+        engine.shortest_paths_trop([(0, 1, 10**13), (1, 2, 1)])
+    engine.set_plan(0)
+    assert engine.shortest_paths_trop([(0, 1, 10**13), (1, 2, 1)]).stats["plan"] == 1
