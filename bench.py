@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--sources", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-sort-plan", action="store_true", help="skip the sort-merge plan measurement")
     ap.add_argument("--out", default=None, help="also write the JSON line here")
     return ap.parse_args()
 
@@ -244,6 +245,37 @@ def run_ours(args):
     clk = clocks.stop()
     kstats = eng.kernel_stats()
     eng.set_profiling(False)
+
+    # ---- the sort-merge plan on the same inputs (reported beside the headline)
+    sort_plan = None
+    if not args.no_sort_plan:
+        eng.set_plan(1)
+        step().free()  # warm its buffers
+        eng.set_profiling(True)
+        eng.reset_kernel_stats()
+        sp_ms = 0.0
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rel = step()
+            e1.record(stream)
+            e1.synchronize()
+            sp_ms += e0.elapsed_time(e1)
+            sp_stats = rel.stats
+            assert len(rel) == tuples
+            rel.free()
+        sk = eng.kernel_stats()
+        eng.set_profiling(False)
+        eng.set_plan(0)
+        sort_plan = {"plan": "sort-merge (radix sort + run reduction + merge-path diff per round)",
+                     "ms_per_step": sp_ms / args.steps, "value": tuples * args.steps / (sp_ms / 1000.0),
+                     "phase_ms": {k: round(sp_stats[k + "_ms"], 3) for k in ("setup", "join", "sort", "diff", "merge", "finish")},
+                     "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
+                                     "gbs": (v[2] / (v[1] / 1000.0) / 1e9) if v[1] else None,
+                                     "frac_of_hbm": ((v[2] / (v[1] / 1000.0) / 1e9) / 6548.8) if v[1] else None}
+                                 for k, v in sk.items() if v[0]}}
     if pg:
         t = torch.tensor([total_ms, float(tuples)], dtype=torch.float64, device="cuda")
         mx = t.clone()
@@ -325,11 +357,13 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "int32" if stats["weight_bytes"] == 4 else "int64",
             "data": "synthetic", "config": config(args, world),
+            "plan": {1: "sort-merge", 2: "direct-addressed"}.get(stats["plan"], "?"),
             "tuples_per_step": int(all_tuples), "rounds": stats["rounds"],
             "candidates_per_step": stats["candidates"], "key_bits": stats["key_bits"],
             "weight_bytes": stats["weight_bytes"],
-            "phase_ms": {k: round(stats[k + "_ms"], 3) for k in ("join", "sort", "diff", "merge")},
+            "phase_ms": {k: round(stats[k + "_ms"], 3) for k in ("setup", "join", "sort", "diff", "merge", "finish")},
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+            "sort_merge_plan": sort_plan,
         }
         print(json.dumps(line), flush=True)
         if args.out:

@@ -68,6 +68,8 @@ typedef struct strata_fix_stats {
   uint32_t sort_launches, join_launches, diff_launches, merge_launches;
   uint32_t other_launches;
   uint32_t plan;            /* 1 sort-merge, 2 direct-addressed (see strata_ctx_set_plan) */
+  double   setup_ms;        /* EDB indexing before the first round (profiling on) */
+  double   finish_ms;       /* building the output relation after the last round (profiling on) */
 } strata_fix_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -96,7 +98,7 @@ uint64_t strata_ctx_launches(const strata_ctx* ctx);
 /* Per-kernel accounting collected while profiling is on: launches, summed
  * CUDA-event duration and algorithmic bytes moved.  Kernel ids:
  * 0 radix pass, 1 expand emit, 2 expand offsets, 3 run reduction,
- * 4 merge/diff, 5 radix histogram, 6 triangle count. */
+ * 4 merge/diff, 5 radix histogram, 6 triangle count, 7 direct-addressed expand. */
 strata_status strata_ctx_kernel_stats(strata_ctx* ctx, int kernel, uint64_t* launches,
                                       double* ms, uint64_t* bytes);
 strata_status strata_ctx_reset_kernel_stats(strata_ctx* ctx);

@@ -138,6 +138,7 @@ void strata_ctx_destroy(strata_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& kv : ctx->sizes) cudaFreeAsync(kv.first, ctx->stream);
+  for (auto& kv : ctx->free_blocks) cudaFreeAsync(kv.second, ctx->stream);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_status) cudaFreeHost(ctx->h_status);
@@ -152,6 +153,7 @@ void strata_ctx_destroy(strata_ctx* ctx) {
 strata_status strata_ctx_set_stream(strata_ctx* ctx, void* stream) {
   if (!ctx) return STRATA_E_INVALID;
   SK_GUARD_BEGIN
+  // Cached blocks were freed in the old stream's order: finish it first.
   SK_CUDA(cudaStreamSynchronize(ctx->stream));
   if (stream) {
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);

@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include <cstring>
+#include <map>
 #include <string>
 #include <unordered_map>
 #include <utility>
@@ -64,9 +65,11 @@ struct strata_ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   uint64_t cap = 0;
-  uint64_t in_use = 0;
+  uint64_t in_use = 0;   // bytes of live blocks
+  uint64_t cached = 0;   // bytes of freed blocks kept for reuse
   uint64_t peak = 0;
   std::unordered_map<void*, uint64_t> sizes;
+  std::multimap<uint64_t, void*> free_blocks;  // size -> block, reused in stream order
   std::string last_error;
   uint32_t* d_status = nullptr;     // device status word
   uint32_t* h_status = nullptr;     // pinned mirror
@@ -88,10 +91,43 @@ namespace sk {
 
 // ---- allocation -------------------------------------------------------------
 
+// Size classes: 256 B granules below 1 MiB, then steps of 1/8 of the power of
+// two, so a block freed by one call fits the same request of the next call.
+inline uint64_t size_class(uint64_t bytes) {
+  if (bytes <= (1ull << 20)) return (bytes + 255) & ~uint64_t(255);
+  int hb = 63 - __builtin_clzll(bytes);
+  const uint64_t step = 1ull << (hb - 3);
+  return (bytes + step - 1) & ~(step - 1);
+}
+
+inline void release_cached(strata_ctx* ctx, uint64_t need) {
+  // Return cached blocks to the pool until `need` bytes fit under the cap.
+  while (!ctx->free_blocks.empty() && ctx->cap && ctx->in_use + ctx->cached + need > ctx->cap) {
+    auto it = std::prev(ctx->free_blocks.end());
+    cudaFreeAsync(it->second, ctx->stream);
+    ctx->cached -= it->first;
+    ctx->free_blocks.erase(it);
+  }
+}
+
 inline void* dev_alloc(strata_ctx* ctx, uint64_t bytes) {
   if (bytes == 0) bytes = 16;
-  bytes = (bytes + 255) & ~uint64_t(255);
-  if (ctx->cap && ctx->in_use + bytes > ctx->cap) {
+  bytes = size_class(bytes);
+  // Reuse the smallest cached block that fits (all work is stream ordered on
+  // ctx->stream, so a block freed earlier on it is free for later work).
+  auto it = ctx->free_blocks.lower_bound(bytes);
+  if (it != ctx->free_blocks.end() && it->first <= bytes + bytes / 4) {
+    void* p = it->second;
+    const uint64_t sz = it->first;
+    ctx->free_blocks.erase(it);
+    ctx->cached -= sz;
+    ctx->sizes[p] = sz;
+    ctx->in_use += sz;
+    if (ctx->in_use > ctx->peak) ctx->peak = ctx->in_use;
+    return p;
+  }
+  release_cached(ctx, bytes);
+  if (ctx->cap && ctx->in_use + ctx->cached + bytes > ctx->cap) {
     fail(STRATA_E_OOM, "device memory cap reached: need " + std::to_string(bytes) +
                            " B with " + std::to_string(ctx->in_use) + " of " +
                            std::to_string(ctx->cap) + " B held");
@@ -101,8 +137,18 @@ inline void* dev_alloc(strata_ctx* ctx, uint64_t bytes) {
                             : cudaMallocAsync(&p, bytes, ctx->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    fail(STRATA_E_OOM, std::string("cudaMallocAsync(") + std::to_string(bytes) +
-                           "): " + cudaGetErrorString(e));
+    // Give the cached blocks back and try once more before failing.
+    const uint64_t keep_cap = ctx->cap;
+    ctx->cap = 1;
+    release_cached(ctx, 0);
+    ctx->cap = keep_cap;
+    e = ctx->pool ? cudaMallocFromPoolAsync(&p, bytes, ctx->pool, ctx->stream)
+                  : cudaMallocAsync(&p, bytes, ctx->stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      fail(STRATA_E_OOM, std::string("cudaMallocAsync(") + std::to_string(bytes) +
+                             "): " + cudaGetErrorString(e));
+    }
   }
   ctx->sizes[p] = bytes;
   ctx->in_use += bytes;
@@ -113,11 +159,14 @@ inline void* dev_alloc(strata_ctx* ctx, uint64_t bytes) {
 inline void dev_free(strata_ctx* ctx, void* p) {
   if (!p) return;
   auto it = ctx->sizes.find(p);
-  if (it != ctx->sizes.end()) {
-    ctx->in_use -= it->second;
-    ctx->sizes.erase(it);
+  if (it == ctx->sizes.end()) {
+    cudaFreeAsync(p, ctx->stream);
+    return;
   }
-  cudaFreeAsync(p, ctx->stream);
+  ctx->in_use -= it->second;
+  ctx->cached += it->second;
+  ctx->free_blocks.emplace(it->second, p);
+  ctx->sizes.erase(it);
 }
 
 // Owning device buffer (RAII, stream-ordered free).
@@ -227,7 +276,8 @@ enum KernelId : int {
   K_MERGE_DIFF = 4,
   K_RADIX_HIST = 5,
   K_TRI_COUNT = 6,
-  K_NUM = 7,
+  K_EXPAND_DENSE = 7,
+  K_NUM = 8,
 };
 
 inline cudaEvent_t take_event(strata_ctx* ctx) {

@@ -60,19 +60,27 @@ __global__ void __launch_bounds__(NT)
                    int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift, int out_vshift,
                    const uint32_t* __restrict__ off, uint64_t n_nodes, const uint32_t* __restrict__ nbr,
                    uint64_t n_nbr, const int32_t* __restrict__ nbr_w, int b1, uint64_t mask1, uint64_t n1,
-                   uint64_t entries, uint32_t* bits, int32_t* D, K* __restrict__ out, uint64_t out_cap,
-                   unsigned long long* out_count, uint32_t* status) {
-  __shared__ uint64_t s_pos[DE_TILE + 1];
-  __shared__ uint32_t s_seg[DE_TILE + 1];
-  __shared__ uint32_t s_kept[DE_TILE + 1];  // one column id
-  __shared__ int32_t s_w[TROP ? DE_TILE + 1 : 1];
-  const int tid = threadIdx.x, lane = tid & 31;
+                   uint64_t entries, uint32_t* bits, int32_t* D, uint32_t* marks, uint32_t* status) {
+  constexpr int U = 4;  // outputs in flight per thread
+  // Dynamic shared memory (sizes in dense_expand_smem()):
+  //   s_pos   int32  pos of each local item relative to the tile's first output
+  //   s_seg   u32    CSR segment start of each local item
+  //   s_kept  u32    the kept column id of each local item
+  //   s_w     i32    Trop weight of each local item
+  //   s_owner u16    local owner item of each output of the tile
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  int32_t* s_pos = reinterpret_cast<int32_t*>(s_raw);
+  uint32_t* s_seg = reinterpret_cast<uint32_t*>(s_pos + DE_TILE + 1);
+  uint32_t* s_kept = s_seg + DE_TILE + 1;
+  int32_t* s_w = reinterpret_cast<int32_t*>(s_kept + DE_TILE + 1);
+  uint16_t* s_owner = reinterpret_cast<uint16_t*>(s_w + (TROP ? DE_TILE + 1 : 0));
+  const int tid = threadIdx.x;
   const uint64_t L = n + total;
   const uint64_t d0 = (uint64_t)blockIdx.x * DE_TILE;
   const uint64_t d1 = d0 + DE_TILE < L ? d0 + DE_TILE : L;
   const uint64_t i0 = splits[blockIdx.x], i1 = splits[blockIdx.x + 1];
   const uint64_t a = i0 > 0 ? i0 - 1 : 0;
-  if (i1 < a || i1 - a > DE_TILE + 1 || i1 > n) {
+  if (i1 < a || i1 - a > DE_TILE + 1 || i1 > n || d1 < i1 || d0 < i0) {
     if (tid == 0) atomicOr(status, ST_BOUNDS);
     return;
   }
@@ -82,61 +90,157 @@ __global__ void __launch_bounds__(NT)
     const uint64_t i = a + k;
     const K key = dkeys[i];
     const uint64_t jv = ((uint64_t)key >> jshift) & jmask;
-    s_pos[k] = pos[i];
+    const int64_t rel = (int64_t)pos[i] - (int64_t)o0;  // one item's degree stays below 2^31
+    if (rel < INT32_MIN || rel > INT32_MAX) atomicOr(status, ST_BOUNDS);
+    s_pos[k] = (int32_t)rel;
     s_seg[k] = jv < n_nodes ? off[jv] : 0u;
     s_kept[k] = (uint32_t)(((uint64_t)key >> pshift) & pmask);
     if constexpr (TROP) s_w[k] = dw[i];
   }
   __syncthreads();
   uint32_t flags = 0;
-  const uint64_t o_end = o1 < total ? o1 : total;
-  for (uint64_t base = o0; base < o_end; base += NT) {
-    const uint64_t o = base + tid;
-    bool app = false;
-    K ok = 0;
-    if (o < o_end) {
+  // Serial merge of item events and outputs: thread t walks merged positions
+  // [d0 + t*ITEMS, ...) once and records the owner of every output it meets.
+  // Item a+k sits at merged position (a+k) + pos[a+k]; output o owned by
+  // item i sits at o + i + 1.
+  {
+    const uint64_t p0 = d0 + (uint64_t)tid * DE_ITEMS;
+    if (p0 < d1) {
       uint32_t lo = 0, hi = cnt;
       while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (s_pos[mid] <= o) lo = mid + 1; else hi = mid;
+        if ((int64_t)(a + mid + o0) + s_pos[mid] < (int64_t)p0) lo = mid + 1; else hi = mid;
       }
-      const uint32_t li = lo ? lo - 1 : 0;
-      const uint64_t e = (uint64_t)s_seg[li] + (o - s_pos[li]);
-      if (lo == 0 || e >= n_nbr) {
-        flags |= ST_BOUNDS;
-      } else {
-        const uint32_t v = nbr[e];
-        ok = (K)(((K)s_kept[li] << out_pshift) | ((K)v << out_vshift));
-        const uint64_t ix = dense_index((uint64_t)ok, b1, mask1, n1);
-        if (ix >= entries) {
-          flags |= ST_BOUNDS;
-        } else if constexpr (TROP) {
-          const int32_t cw = trop_mul(s_w[li], nbr_w[e], &flags);
-          if (cw < D[ix]) {
-            const int32_t old = atomicMin(&D[ix], cw);
-            if (cw < old) {
-              const uint32_t bit = 1u << (ix & 31);
-              app = (atomicOr(&bits[ix >> 5], bit) & bit) == 0;
-            }
-          }
+      uint32_t kk = lo;  // local items whose event precedes p0
+      const uint64_t p1 = p0 + DE_ITEMS < d1 ? p0 + DE_ITEMS : d1;
+      for (uint64_t p = p0; p < p1; p++) {
+        if (kk < cnt && (int64_t)(a + kk + o0) + s_pos[kk] == (int64_t)p) {
+          kk++;
         } else {
-          const uint32_t bit = 1u << (ix & 31);
-          if ((bits[ix >> 5] & bit) == 0) app = (atomicOr(&bits[ix >> 5], bit) & bit) == 0;
+          const uint64_t o = p - (a + kk);
+          if (kk == 0 || o < o0 || o - o0 >= DE_TILE) flags |= ST_BOUNDS;
+          else s_owner[o - o0] = (uint16_t)(kk - 1);
         }
       }
     }
-    // warp-aggregated append of the first touches
-    const unsigned m = __ballot_sync(kFull, app);
-    if (m) {
-      unsigned long long basei = 0;
-      const int leader = __ffs(m) - 1;
-      if (lane == leader) basei = atomicAdd(out_count, (unsigned long long)__popc(m));
-      basei = __shfl_sync(kFull, basei, leader);
-      if (app) {
-        const uint64_t at = basei + __popc(m & lanemask_lt());
-        if (at < out_cap) out[at] = ok;
-        else flags |= ST_BOUNDS;
+  }
+  __syncthreads();
+  const uint64_t o_end = o1 < total ? o1 : total;
+  for (uint64_t base = o0; base < o_end; base += (uint64_t)NT * U) {
+    uint32_t li[U], v[U];
+    int32_t ew[U];
+    bool ok[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint64_t o = base + (uint64_t)u * NT + tid;
+      ok[u] = false;
+      v[u] = 0;
+      ew[u] = 0;
+      li[u] = 0;
+      if (o < o_end) {
+        li[u] = s_owner[o - o0];
+        const uint64_t e = (uint64_t)((int64_t)s_seg[li[u]] + ((int64_t)(o - o0) - s_pos[li[u]]));
+        if (li[u] >= cnt || e >= n_nbr) {
+          flags |= ST_BOUNDS;
+        } else {
+          ok[u] = true;
+          v[u] = nbr[e];
+          if constexpr (TROP) ew[u] = nbr_w[e];
+        }
       }
+    }
+    K key[U];
+    uint64_t ix[U];
+    int32_t cur[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      key[u] = (K)(((K)s_kept[li[u]] << out_pshift) | ((K)v[u] << out_vshift));
+      ix[u] = dense_index((uint64_t)key[u], b1, mask1, n1);
+      if (ok[u] && ix[u] >= entries) {
+        flags |= ST_BOUNDS;
+        ok[u] = false;
+      }
+      if (ok[u]) {
+        if constexpr (TROP) cur[u] = D[ix[u]];
+        else cur[u] = (int32_t)bits[ix[u] >> 5];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (!ok[u]) continue;
+      const uint32_t bit = 1u << (ix[u] & 31);
+      if constexpr (TROP) {
+        const int32_t cw = trop_mul(s_w[li[u]], ew[u], &flags);
+        if (cw < cur[u]) {
+          const int32_t old = atomicMin(&D[ix[u]], cw);
+          if (cw < old) atomicOr(&marks[ix[u] >> 5], bit);  // changed this round
+        }
+      } else {
+        if (((uint32_t)cur[u] & bit) == 0) {
+          const uint32_t old = atomicOr(&bits[ix[u] >> 5], bit);
+          if ((old & bit) == 0) atomicOr(&marks[ix[u] >> 5], bit);  // new this round
+        }
+      }
+    }
+  }
+  if (flags) atomicOr(status, flags);
+}
+
+template <bool TROP>
+size_t dense_expand_smem() {
+  return (DE_TILE + 1) * (4 + 4 + 4 + (TROP ? 4 : 0)) + DE_TILE * 2 + 16;
+}
+
+// Δ' of a round: the marked index entries in index (= key) order, with
+// their merged weight (Trop); the marks are cleared for the next round.
+constexpr int MC_WORDS = 1;                    // bitmap words per thread
+constexpr uint32_t MC_TILE = NT * MC_WORDS;    // words per tile
+
+template <class K, bool TROP>
+__global__ void __launch_bounds__(NT)
+    k_marks_compact(uint32_t* marks, uint64_t words, uint64_t entries, int b1, uint64_t n1,
+                    const int32_t* __restrict__ D, K* __restrict__ out, int32_t* __restrict__ out_w,
+                    uint64_t out_cap, uint64_t* states, uint32_t* counter, uint64_t* d_count, uint32_t* status) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_scan[NT / 32 + 1];
+  __shared__ uint64_t s_ex;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t tile = claim_tile(counter, &s_tile);
+  const uint64_t w0 = (uint64_t)tile * MC_TILE + (uint64_t)tid * MC_WORDS;
+  uint32_t wv[MC_WORDS];
+  uint32_t c = 0;
+#pragma unroll
+  for (int j = 0; j < MC_WORDS; j++) {
+    wv[j] = (w0 + j < words) ? marks[w0 + j] : 0u;
+    c += __popc(wv[j]);
+  }
+  uint32_t tot;
+  const uint32_t ex = block_excl_sum<NT>(c, s_scan, &tot);
+  if (warp == 0) {
+    const uint64_t e = warp_lookback(states, tile, tot, status);
+    if (lane == 0) {
+      s_ex = e;
+      if (tile == gridDim.x - 1) *d_count = e + tot;
+    }
+  }
+  __syncthreads();
+  uint64_t at = s_ex + ex;
+  uint32_t flags = 0;
+#pragma unroll
+  for (int j = 0; j < MC_WORDS; j++) {
+    uint32_t m = wv[j];
+    if (m) marks[w0 + j] = 0u;
+    while (m) {
+      const int b = __ffs(m) - 1;
+      m &= m - 1;
+      const uint64_t ix = (w0 + j) * 32 + b;
+      if (ix >= entries || at >= out_cap) {
+        flags |= ST_BOUNDS;
+        continue;
+      }
+      out[at] = (K)(((K)(ix / n1) << b1) | (K)(ix % n1));
+      if constexpr (TROP) out_w[at] = D[ix];
+      at++;
     }
   }
   if (flags) atomicOr(status, flags);
@@ -240,24 +344,46 @@ void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n
                   uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift,
                   int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr, uint64_t n_nbr,
                   const int32_t* nbr_w, int b1, uint64_t n1, uint64_t entries, uint32_t* bits, int32_t* D,
-                  K* out, uint64_t out_cap, uint64_t* d_out_count, uint64_t* splits_buf) {
+                  uint32_t* marks, uint64_t* splits_buf) {
   if (n == 0 || total == 0) return;
   const uint64_t tiles = ceil_div(n + total, DE_TILE);
   if (tiles > 0x7fffffffull) fail(STRATA_E_UNSUPPORTED, "expand too large for one launch");
   k_tile_splits<<<grid1(tiles + 1), NT, 0, ctx->stream>>>(pos, n, total, DE_TILE, tiles, splits_buf);
   after_launch(ctx, "k_tile_splits");
   const uint64_t mask1 = b1 >= 64 ? ~0ull : ((1ull << b1) - 1);
-  const int kh = kprof_begin(ctx, K_EXPAND_EMIT);
-  k_expand_dense<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(
+  const int kh = kprof_begin(ctx, K_EXPAND_DENSE);
+  const size_t smem = dense_expand_smem<TROP>();
+  auto kern = k_expand_dense<K, TROP>;
+  SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(
       dkeys, dw, n, pos, total, splits_buf, jshift, jmask, pshift, pmask, out_pshift, out_vshift, off, n_nodes,
-      nbr, n_nbr, nbr_w, b1, mask1, n1, entries, bits, D, out, out_cap,
-      reinterpret_cast<unsigned long long*>(d_out_count), ctx->d_status);
-  // Algorithmic bytes: Δ rows, CSR segments streamed, one 4-byte index probe
-  // per candidate; appends are counted by the caller once their number is known.
+      nbr, n_nbr, nbr_w, b1, mask1, n1, entries, bits, D, marks, ctx->d_status);
+  // Algorithmic bytes: Δ rows and their offsets, the CSR segments streamed
+  // (neighbour + weight) and one 4-byte index probe per candidate.
   const uint64_t wsz = TROP ? 4 : 0;
-  kprof_end(ctx, kh, n * (sizeof(K) + wsz + 8 + 4) + total * (4 + wsz) + total * (TROP ? 4 : 4));
+  kprof_end(ctx, kh, n * (sizeof(K) + wsz + 8 + 4) + total * (4 + wsz) + total * 4);
   after_launch(ctx, "k_expand_dense");
 }
+
+template <class K, bool TROP>
+uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, uint64_t entries, int b1, uint64_t n1,
+                             const int32_t* D, K* out, int32_t* out_w, uint64_t out_cap, uint64_t* states_buf) {
+  const uint64_t words = (entries + 31) / 32;
+  const uint64_t tiles = ceil_div(words, MC_TILE);
+  SK_CUDA(cudaMemsetAsync(states_buf, 0, sizeof(uint64_t) * (tiles + 2), ctx->stream));
+  uint32_t* counter = reinterpret_cast<uint32_t*>(states_buf + tiles + 1);
+  k_marks_compact<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, entries, b1, n1, D, out, out_w,
+                                                                   out_cap, states_buf, counter, states_buf + tiles,
+                                                                   ctx->d_status);
+  after_launch(ctx, "k_marks_compact");
+  uint64_t r;
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, states_buf + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  sync_and_check(ctx);
+  r = ctx->h_scalar[0];
+  return r;
+}
+
+uint64_t dense_marks_states(uint64_t entries) { return ceil_div((entries + 31) / 32, MC_TILE) + 2; }
 
 template <class K>
 void dense_gather(strata_ctx* ctx, const K* keys, uint64_t n, int b1, uint64_t n1, uint64_t entries,
@@ -305,7 +431,9 @@ uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, 
   template void dense_expand<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const uint64_t*,       \
                                    uint64_t, int, uint64_t, int, uint64_t, int, int, const uint32_t*,      \
                                    uint64_t, const uint32_t*, uint64_t, const int32_t*, int, uint64_t,     \
-                                   uint64_t, uint32_t*, int32_t*, K*, uint64_t, uint64_t*, uint64_t*);     \
+                                   uint64_t, uint32_t*, int32_t*, uint32_t*, uint64_t*);                   \
+  template uint64_t dense_marks_compact<K, T>(strata_ctx*, uint32_t*, uint64_t, int, uint64_t,             \
+                                              const int32_t*, K*, int32_t*, uint64_t, uint64_t*);          \
   template void dense_seed<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, int, uint64_t, uint64_t, \
                                  uint32_t*, int32_t*);                                                     \
   template uint64_t dense_compact<K, T>(strata_ctx*, const uint32_t*, const int32_t*, uint64_t, int,       \

@@ -81,7 +81,8 @@ struct Scratch {
 };
 
 struct Acct {  // per-phase accounting for strata_fix_stats
-  double sort_ms = 0, join_ms = 0, diff_ms = 0, merge_ms = 0;
+  double sort_ms = 0, join_ms = 0, diff_ms = 0, merge_ms = 0, setup_ms = 0, finish_ms = 0;
+  int setup_t = -1;
   uint64_t sort_b = 0, join_b = 0, diff_b = 0, merge_b = 0;
   uint32_t sort_l = 0, join_l = 0, diff_l = 0, merge_l = 0;
   uint64_t cands = 0;
@@ -300,14 +301,18 @@ void fill_stats(strata_fix_stats* st, const Acct& a, uint64_t rounds, uint64_t r
   st->merge_launches = a.merge_l;
   const uint64_t phase = (uint64_t)a.sort_l + a.join_l + a.diff_l + a.merge_l;
   st->other_launches = (uint32_t)(launches > phase ? launches - phase : 0);
+  st->setup_ms = a.setup_ms;
+  st->finish_ms = a.finish_ms;
 }
 
 // ---- direct-addressed plan ---------------------------------------------------------
 // Index over (c0, c1) in [0, n0) × [0, n1): a bitmap (Bool relation, or the
 // per-round first-touch marks of a Trop relation) and an int32 weight array.
 struct DenseIdx {
-  DBuf<uint32_t> bits;
-  DBuf<int32_t> D;
+  DBuf<uint32_t> bits;   // Bool membership
+  DBuf<uint32_t> marks;  // changed in the current round
+  DBuf<int32_t> D;       // Trop weights (INT32_MAX = absent)
+  DBuf<uint64_t> states; // look-back words of the marks compaction
   uint64_t n0 = 0, n1 = 0, entries = 0;
   uint64_t words() const { return (entries + 31) / 32; }
 };
@@ -329,12 +334,17 @@ inline bool want_dense(strata_ctx* ctx, bool trop, bool narrow, uint64_t n0, uin
 
 template <bool TROP>
 void dense_alloc(strata_ctx* ctx, DenseIdx& X, uint64_t n0, uint64_t n1) {
-  X.bits.ctx = X.D.ctx = ctx;
+  X.bits.ctx = X.D.ctx = X.marks.ctx = X.states.ctx = ctx;
   X.n0 = n0;
   X.n1 = n1;
   X.entries = n0 * n1;
-  X.bits.reserve(X.words() + 1);
-  SK_CUDA(cudaMemsetAsync(X.bits.p, 0, (X.words() + 1) * 4, ctx->stream));
+  if (!TROP) {
+    X.bits.reserve(X.words() + 1);
+    SK_CUDA(cudaMemsetAsync(X.bits.p, 0, (X.words() + 1) * 4, ctx->stream));
+  }
+  X.marks.reserve(X.words() + 1);
+  SK_CUDA(cudaMemsetAsync(X.marks.p, 0, (X.words() + 1) * 4, ctx->stream));
+  X.states.reserve(dense_marks_states(X.entries));
   if (TROP) X.D.reserve(X.entries + 1);
 }
 
@@ -352,18 +362,16 @@ uint64_t dense_round(strata_ctx* ctx, const K* dk, const int32_t* dw, uint64_t n
   read_checked(ctx, s.pos.p + nd, &T, 1);
   uint64_t cnt = 0;
   if (T) {
-    if (TROP) SK_CUDA(cudaMemsetAsync(X.bits.p, 0, X.words() * 4, ctx->stream));
     const uint64_t cap = std::min<uint64_t>(T, X.entries) + 1;
     out.reserve(cap, TROP);
     splits.reserve_grow(ceil_div(nd + T, dense_tile_size()) + 2);
-    SK_CUDA(cudaMemsetAsync(s.counts.p, 0, 8, ctx->stream));
     dense_expand<K, TROP>(ctx, dk, dw, nd, s.pos.p, T, js.jshift, js.jmask, js.pshift, js.pmask, js.out_pshift,
                           js.out_vshift, csr.off.p, csr.n_nodes, csr.nbr.p, csr.m, TROP ? csr.w.p : nullptr, b1,
-                          X.n1, X.entries, X.bits.p, TROP ? X.D.p : nullptr, out.k.p, cap, s.counts.p,
+                          X.n1, X.entries, TROP ? nullptr : X.bits.p, TROP ? X.D.p : nullptr, X.marks.p,
                           splits.p);
-    read_checked(ctx, s.counts.p, &cnt, 1);
-    if (TROP) dense_gather<K>(ctx, out.k.p, cnt, b1, X.n1, X.entries, X.D.p, out.w.p);
-    kprof_add_last(ctx, K_EXPAND_EMIT, cnt * (sizeof(K) + (TROP ? 8 : 0)));
+    // Δ' in key order, with merged weights; marks cleared for the next round.
+    cnt = dense_marks_compact<K, TROP>(ctx, X.marks.p, X.entries, b1, X.n1, TROP ? X.D.p : nullptr, out.k.p,
+                                       TROP ? out.w.p : nullptr, cap, X.states.p);
   }
   pt.end(t);
   const uint64_t wsz = TROP ? 4 : 0;
@@ -410,6 +418,7 @@ strata_rel* run_tc_shape(strata_ctx* ctx, const EdgeCols& e, int b0, int b1, int
                          EventTimer& et, uint64_t l_start, uint64_t n_nodes_src, bool dense) {
   PhaseTimer pt(ctx);
   Acct a;
+  a.setup_t = pt.begin(&a.setup_ms);
   uint32_t plan = 1;
   const int key_bits = b0 + b1;
   // path0 = normalize(edge): every edge is derived by the base rule.
@@ -445,11 +454,17 @@ strata_rel* run_tc_shape(strata_ctx* ctx, const EdgeCols& e, int b0, int b1, int
       dense_alloc<TROP>(ctx, X, n_nodes_src, n_nodes_dst);
       if (TROP) dense_seed<K, true>(ctx, full.k.p, full.w.p, full.n, b1, X.n1, X.entries, X.bits.p, X.D.p);
       else dense_seed<K, false>(ctx, full.k.p, nullptr, full.n, b1, X.n1, X.entries, X.bits.p, nullptr);
+      pt.end(a.setup_t);
       fix_loop_dense<K, TROP>(ctx, delta, csr, js, b1, X, cap, s, pt, a, &rounds);
+      const int tf = pt.begin(&a.finish_ms);
       dense_finish<K, TROP>(ctx, X, b1, full, X.entries);
+      pt.end(tf);
     }
   }
-  if (plan == 1) fix_loop<K, W, TROP>(ctx, full, delta, csr, js, key_bits, cap, s, pt, a, &rounds);
+  if (plan == 1) {
+    pt.end(a.setup_t);
+    fix_loop<K, W, TROP>(ctx, full, delta, csr, js, key_bits, cap, s, pt, a, &rounds);
+  }
   const double ms = et.stop();
   pt.collect();
   kprof_collect(ctx);
@@ -548,6 +563,7 @@ strata_rel* run_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
                      bool dense) {
   PhaseTimer pt(ctx);
   Acct a;
+  a.setup_t = pt.begin(&a.setup_ms);
   const int key_bits = b0 + b1;
   // src as a unary Trop relation keyed by S (min over duplicate facts).
   Rel<K, W> srcu;
@@ -577,11 +593,14 @@ strata_rel* run_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
       delta.k.ctx = delta.w.ctx = full.k.ctx = full.w.ctx = ctx;
       DBuf<uint64_t> splits;
       splits.ctx = ctx;
+      pt.end(a.setup_t);
       // Bootstrap: every derivation of src ⋈ edge, all new.
       delta.n = dense_round<K, true>(ctx, srcu.k.p, srcu.w.p, srcu.n, csr, boot, b1, X, delta, s, splits, pt, a);
       uint64_t rounds = 0;
       fix_loop_dense<K, true>(ctx, delta, csr, step, b1, X, cap, s, pt, a, &rounds);
+      const int tf = pt.begin(&a.finish_ms);
       dense_finish<K, true>(ctx, X, b1, full, X.entries);
+      pt.end(tf);
       const double ms = et.stop();
       pt.collect();
       kprof_collect(ctx);
@@ -590,6 +609,7 @@ strata_rel* run_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
       return finish_rel<K, W, true>(ctx, full, b1);
     }
   }
+  pt.end(a.setup_t);
   // Bootstrap: dist0 = min-reduce(src ⋈ edge), all of it new.
   const uint64_t nb = derive<K, W, true>(ctx, srcu.k.p, srcu.w.p, srcu.n, csr, boot, key_bits, s, pt, a);
   Rel<K, W> full, delta;

@@ -33,7 +33,11 @@ void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n
                   uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift,
                   int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr, uint64_t n_nbr,
                   const int32_t* nbr_w, int b1, uint64_t n1, uint64_t entries, uint32_t* bits, int32_t* D,
-                  K* out, uint64_t out_cap, uint64_t* d_out_count, uint64_t* splits_buf);
+                  uint32_t* marks, uint64_t* splits_buf);
+template <class K, bool TROP>
+uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, uint64_t entries, int b1, uint64_t n1,
+                             const int32_t* D, K* out, int32_t* out_w, uint64_t out_cap, uint64_t* states_buf);
+uint64_t dense_marks_states(uint64_t entries);
 template <class K>
 void dense_gather(strata_ctx* ctx, const K* keys, uint64_t n, int b1, uint64_t n1, uint64_t entries,
                   const int32_t* D, int32_t* w);

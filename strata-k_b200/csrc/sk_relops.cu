@@ -546,6 +546,22 @@ __global__ void k_mark_ids(const uint32_t* __restrict__ a, uint64_t n, uint32_t*
   }
 }
 
+// Same marks, OR-ed first into a block-private bitmap in shared memory
+// (hub ids would otherwise hammer a few global words), then flushed once.
+__global__ void k_mark_ids_smem(const uint32_t* __restrict__ a, uint64_t n, uint32_t* bitmap, uint64_t limit,
+                                uint64_t words) {
+  extern __shared__ uint32_t s_bm[];
+  for (uint64_t i = threadIdx.x; i < words; i += blockDim.x) s_bm[i] = 0;
+  __syncthreads();
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = a[i];
+    if (v < limit) atomicOr(&s_bm[v >> 5], 1u << (v & 31));
+  }
+  __syncthreads();
+  for (uint64_t i = threadIdx.x; i < words; i += blockDim.x)
+    if (s_bm[i]) atomicOr(&bitmap[i], s_bm[i]);
+}
+
 __global__ void k_popcount(const uint32_t* __restrict__ bitmap, uint64_t words, unsigned long long* out) {
   unsigned long long c = 0;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (uint64_t)gridDim.x * blockDim.x)
@@ -788,10 +804,21 @@ uint64_t count_distinct_ids(strata_ctx* ctx, const uint32_t* a, uint64_t na, con
   SK_CUDA(cudaMemsetAsync(cnt.p, 0, 8, ctx->stream));
   const uint32_t* cols[3] = {a, b, c};
   const uint64_t ns[3] = {na, nb, nc};
+  const size_t smem = words * 4;
+  const bool private_bm = smem <= 160 * 1024;
+  if (private_bm)
+    SK_CUDA(cudaFuncSetAttribute(k_mark_ids_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int q = 0; q < 3; q++) {
     if (!cols[q] || !ns[q]) continue;
-    k_mark_ids<<<grid_for(ctx, ns[q]), NT, 0, ctx->stream>>>(cols[q], ns[q], bm.p, limit);
-    after_launch(ctx, "k_mark_ids");
+    if (private_bm) {
+      // few blocks: each flushes its whole private bitmap once
+      const int blocks = (int)std::min<uint64_t>(ceil_div(ns[q], 1024 * 32), (uint64_t)ctx->num_sms);
+      k_mark_ids_smem<<<blocks, 1024, smem, ctx->stream>>>(cols[q], ns[q], bm.p, limit, words);
+      after_launch(ctx, "k_mark_ids_smem");
+    } else {
+      k_mark_ids<<<grid_for(ctx, ns[q]), NT, 0, ctx->stream>>>(cols[q], ns[q], bm.p, limit);
+      after_launch(ctx, "k_mark_ids");
+    }
   }
   k_popcount<<<grid_for(ctx, words), NT, 0, ctx->stream>>>(bm.p, words, cnt.p);
   after_launch(ctx, "k_popcount");

@@ -29,7 +29,7 @@ E_WEIGHT_RANGE = 9
 PLAN_AUTO, PLAN_SORT_MERGE, PLAN_DENSE = 0, 1, 2
 
 KERNELS = {0: "k_onesweep", 1: "k_expand_emit", 2: "k_expand_offsets", 3: "k_reduce_runs",
-           4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count"}
+           4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count", 7: "k_expand_dense"}
 
 STATUS_NAMES = {
     OK: "OK", E_INVALID: "INVALID", E_OOM: "OOM", E_CUDA: "CUDA", E_OVERFLOW: "OVERFLOW",
@@ -51,6 +51,7 @@ class FixStats(C.Structure):
         ("sort_launches", C.c_uint32), ("join_launches", C.c_uint32),
         ("diff_launches", C.c_uint32), ("merge_launches", C.c_uint32),
         ("other_launches", C.c_uint32), ("plan", C.c_uint32),
+        ("setup_ms", C.c_double), ("finish_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:
