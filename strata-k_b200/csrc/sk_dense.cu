@@ -6,19 +6,25 @@
 // for Trop (ABSENT = INT32_MAX, +inf = INT32_MAX-1).  One round then needs no
 // sort and no merge:
 //
-//   for every candidate (key, w) of Δ ⋈ E:          (load-balanced expand)
-//     Bool:  first = !atomicOr(bit(key))             — dedup and Δ' = new∖full in one op
-//     Trop:  if w < D[key] and w < atomicMin(D[key], w)  — ⊕ = min
-//              first = !atomicOr(mark(key))          — one Δ' entry per improved key
-//     if first: append key to Δ'
+//   for every candidate (key, w) of Δ ⋈ E:              (load-balanced expand)
+//     Bool:  new = !atomicOr(bit(key))                  — dedup and Δ' = new∖full in one op
+//     Trop:  w < D[key] and w < atomicMin(D[key], w)    — ⊕ = min, strict improvement
+//     if new / improved: set mark(key)
+//   Δ' = the marked entries in index order, with their merged value from D
 //
-// and Δ' takes its values from D after the round (the merged value of every
-// changed tuple, seminaive.rs:199-206).  A key enters Δ' exactly when some
-// candidate is new (Bool) or strictly below the value the key had when the
-// round started (Trop), which is the interpreter's `Relation::combine`
-// change test (store.rs:34-48), so rounds, Δ sets and the round cap are the
-// same as the sort-merge plan's.  Only the final relation is compacted back
-// into sorted packed keys (index order is key order).
+// A key is marked exactly when some candidate is new (Bool) or strictly
+// below the value the key had when the round started (Trop): the
+// interpreter's `Relation::combine` change test (strata-eval/src/store.rs:34-48),
+// and Δ' carries the merged values (seminaive.rs:199-206), so rounds, Δ sets
+// and the round cap equal the sort-merge plan's.
+//
+// Layout.  The index is stored join-column-major: entry (c_j, c_other) at
+// c_j * n_other + c_other, where c_j is the column the NEXT round joins on
+// (c0 for TC's Δ(Y,Z), c1 for MSSP's Δ(S,Y)).  Δ' then comes out of the
+// marks compaction sorted by its join column, and the expand treats a run of
+// Δ tuples with the same join value as one group: each edge of that value is
+// read once for the whole group, and the group's probes of one edge all fall
+// in one index row (cache-resident).
 #include "sk_ops.cuh"
 #include "sk_prims.cuh"
 
@@ -28,6 +34,7 @@ namespace {
 constexpr int NT = 256;
 constexpr int DE_ITEMS = 8;
 constexpr uint32_t DE_TILE = NT * DE_ITEMS;
+constexpr uint32_t kGroupMax = 32;  // group members per expand output (runs are split at multiples of 32)
 
 __device__ __forceinline__ uint64_t mp_before(const uint64_t* pos, uint64_t n, uint64_t d) {
   uint64_t lo = 0, hi = d < n ? d : n;
@@ -49,31 +56,44 @@ __global__ void k_tile_splits(const uint64_t* __restrict__ pos, uint64_t n, uint
   splits[t] = mp_before(pos, n, d);
 }
 
-__device__ __forceinline__ uint64_t dense_index(uint64_t key, int b1, uint64_t mask1, uint64_t n1) {
-  return (key >> b1) * n1 + (key & mask1);
+__device__ __forceinline__ uint64_t dense_index(uint64_t key, const DenseLayout& L) {
+  const uint64_t c0 = key >> L.b1, c1 = key & L.mask1;
+  return L.colmajor ? c1 * L.n0 + c0 : c0 * L.n1 + c1;
 }
 
+template <class K>
+__device__ __forceinline__ K key_of_index(uint64_t ix, const DenseLayout& L) {
+  uint64_t c0, c1;
+  if (L.colmajor) {
+    c1 = ix / L.n0;
+    c0 = ix - c1 * L.n0;
+  } else {
+    c0 = ix / L.n1;
+    c1 = ix - c0 * L.n1;
+  }
+  return (K)(((K)c0 << L.b1) | (K)c1);
+}
+
+// Grouped expand.  pos[] comes from expand_offsets in grouped mode: only the
+// head of each group (a run of equal join value, split at multiples of
+// kGroupMax) carries the degree of its join value, so one expand output is
+// one (group, edge) pair; the thread applies that edge to every member.
 template <class K, bool TROP>
 __global__ void __launch_bounds__(NT)
     k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n,
                    const uint64_t* __restrict__ pos, uint64_t total, const uint64_t* __restrict__ splits,
                    int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift, int out_vshift,
                    const uint32_t* __restrict__ off, uint64_t n_nodes, const uint32_t* __restrict__ nbr,
-                   uint64_t n_nbr, const int32_t* __restrict__ nbr_w, int b1, uint64_t mask1, uint64_t n1,
-                   uint64_t entries, uint32_t* bits, int32_t* D, uint32_t* marks, uint32_t* status) {
-  constexpr int U = 4;  // outputs in flight per thread
+                   uint64_t n_nbr, const int32_t* __restrict__ nbr_w, DenseLayout lay, uint32_t* bits,
+                   int32_t* D, uint32_t* marks, uint32_t* status) {
   // Dynamic shared memory (sizes in dense_expand_smem()):
   //   s_pos   int32  pos of each local item relative to the tile's first output
   //   s_seg   u32    CSR segment start of each local item
-  //   s_kept  u32    the kept column id of each local item
-  //   s_w     i32    Trop weight of each local item
   //   s_owner u16    local owner item of each output of the tile
   extern __shared__ __align__(16) unsigned char s_raw[];
   int32_t* s_pos = reinterpret_cast<int32_t*>(s_raw);
   uint32_t* s_seg = reinterpret_cast<uint32_t*>(s_pos + DE_TILE + 1);
-  uint32_t* s_kept = s_seg + DE_TILE + 1;
-  int32_t* s_w = reinterpret_cast<int32_t*>(s_kept + DE_TILE + 1);
-  uint16_t* s_owner = reinterpret_cast<uint16_t*>(s_w + (TROP ? DE_TILE + 1 : 0));
+  uint16_t* s_owner = reinterpret_cast<uint16_t*>(s_seg + DE_TILE + 1);
   const int tid = threadIdx.x;
   const uint64_t L = n + total;
   const uint64_t d0 = (uint64_t)blockIdx.x * DE_TILE;
@@ -88,14 +108,11 @@ __global__ void __launch_bounds__(NT)
   const uint32_t cnt = (uint32_t)(i1 - a);
   for (uint32_t k = tid; k < cnt; k += NT) {
     const uint64_t i = a + k;
-    const K key = dkeys[i];
-    const uint64_t jv = ((uint64_t)key >> jshift) & jmask;
+    const uint64_t jv = ((uint64_t)dkeys[i] >> jshift) & jmask;
     const int64_t rel = (int64_t)pos[i] - (int64_t)o0;  // one item's degree stays below 2^31
     if (rel < INT32_MIN || rel > INT32_MAX) atomicOr(status, ST_BOUNDS);
     s_pos[k] = (int32_t)rel;
     s_seg[k] = jv < n_nodes ? off[jv] : 0u;
-    s_kept[k] = (uint32_t)(((uint64_t)key >> pshift) & pmask);
-    if constexpr (TROP) s_w[k] = dw[i];
   }
   __syncthreads();
   uint32_t flags = 0;
@@ -126,59 +143,42 @@ __global__ void __launch_bounds__(NT)
   }
   __syncthreads();
   const uint64_t o_end = o1 < total ? o1 : total;
-  for (uint64_t base = o0; base < o_end; base += (uint64_t)NT * U) {
-    uint32_t li[U], v[U];
-    int32_t ew[U];
-    bool ok[U];
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      const uint64_t o = base + (uint64_t)u * NT + tid;
-      ok[u] = false;
-      v[u] = 0;
-      ew[u] = 0;
-      li[u] = 0;
-      if (o < o_end) {
-        li[u] = s_owner[o - o0];
-        const uint64_t e = (uint64_t)((int64_t)s_seg[li[u]] + ((int64_t)(o - o0) - s_pos[li[u]]));
-        if (li[u] >= cnt || e >= n_nbr) {
-          flags |= ST_BOUNDS;
-        } else {
-          ok[u] = true;
-          v[u] = nbr[e];
-          if constexpr (TROP) ew[u] = nbr_w[e];
-        }
-      }
+  for (uint64_t o = o0 + tid; o < o_end; o += NT) {
+    const uint32_t li = s_owner[o - o0];
+    const uint64_t e = (uint64_t)((int64_t)s_seg[li] + ((int64_t)(o - o0) - s_pos[li]));
+    if (li >= cnt || e >= n_nbr) {
+      flags |= ST_BOUNDS;
+      continue;
     }
-    K key[U];
-    uint64_t ix[U];
-    int32_t cur[U];
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      key[u] = (K)(((K)s_kept[li[u]] << out_pshift) | ((K)v[u] << out_vshift));
-      ix[u] = dense_index((uint64_t)key[u], b1, mask1, n1);
-      if (ok[u] && ix[u] >= entries) {
+    const uint32_t v = nbr[e];
+    int32_t ew = 0;
+    if constexpr (TROP) ew = nbr_w[e];
+    // group members: the head and the following items with its join value,
+    // up to the next multiple of kGroupMax
+    const uint64_t h = a + li;
+    const uint64_t jh = ((uint64_t)dkeys[h] >> jshift) & jmask;
+    const uint64_t g_end = min(n, (h / kGroupMax + 1) * kGroupMax);
+    for (uint64_t m = h; m < g_end; m++) {
+      const K mk = dkeys[m];
+      if (m != h && (((uint64_t)mk >> jshift) & jmask) != jh) break;
+      const uint32_t kept = (uint32_t)(((uint64_t)mk >> pshift) & pmask);
+      const K key = (K)(((K)kept << out_pshift) | ((K)v << out_vshift));
+      const uint64_t ix = dense_index((uint64_t)key, lay);
+      if (ix >= lay.entries) {
         flags |= ST_BOUNDS;
-        ok[u] = false;
+        continue;
       }
-      if (ok[u]) {
-        if constexpr (TROP) cur[u] = D[ix[u]];
-        else cur[u] = (int32_t)bits[ix[u] >> 5];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      if (!ok[u]) continue;
-      const uint32_t bit = 1u << (ix[u] & 31);
+      const uint32_t bit = 1u << (ix & 31);
       if constexpr (TROP) {
-        const int32_t cw = trop_mul(s_w[li[u]], ew[u], &flags);
-        if (cw < cur[u]) {
-          const int32_t old = atomicMin(&D[ix[u]], cw);
-          if (cw < old) atomicOr(&marks[ix[u] >> 5], bit);  // changed this round
+        const int32_t cw = trop_mul(dw[m], ew, &flags);
+        if (cw < D[ix]) {
+          const int32_t old = atomicMin(&D[ix], cw);
+          if (cw < old) atomicOr(&marks[ix >> 5], bit);  // changed this round
         }
       } else {
-        if (((uint32_t)cur[u] & bit) == 0) {
-          const uint32_t old = atomicOr(&bits[ix[u] >> 5], bit);
-          if ((old & bit) == 0) atomicOr(&marks[ix[u] >> 5], bit);  // new this round
+        if ((bits[ix >> 5] & bit) == 0) {
+          const uint32_t old = atomicOr(&bits[ix >> 5], bit);
+          if ((old & bit) == 0) atomicOr(&marks[ix >> 5], bit);  // new this round
         }
       }
     }
@@ -186,36 +186,24 @@ __global__ void __launch_bounds__(NT)
   if (flags) atomicOr(status, flags);
 }
 
-template <bool TROP>
-size_t dense_expand_smem() {
-  return (DE_TILE + 1) * (4 + 4 + 4 + (TROP ? 4 : 0)) + DE_TILE * 2 + 16;
-}
-
-// Δ' of a round: the marked index entries in index (= key) order, with
-// their merged weight (Trop); the marks are cleared for the next round.
-constexpr int MC_WORDS = 1;                    // bitmap words per thread
-constexpr uint32_t MC_TILE = NT * MC_WORDS;    // words per tile
+// Δ' of a round: the marked index entries in index order, with their merged
+// weight (Trop); the marks are cleared for the next round.
+constexpr uint32_t MC_TILE = NT;  // bitmap words per tile (one per thread)
 
 template <class K, bool TROP>
 __global__ void __launch_bounds__(NT)
-    k_marks_compact(uint32_t* marks, uint64_t words, uint64_t entries, int b1, uint64_t n1,
-                    const int32_t* __restrict__ D, K* __restrict__ out, int32_t* __restrict__ out_w,
-                    uint64_t out_cap, uint64_t* states, uint32_t* counter, uint64_t* d_count, uint32_t* status) {
+    k_marks_compact(uint32_t* marks, uint64_t words, DenseLayout lay, const int32_t* __restrict__ D,
+                    K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap, uint64_t* states,
+                    uint32_t* counter, uint64_t* d_count, uint32_t* status) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_scan[NT / 32 + 1];
   __shared__ uint64_t s_ex;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t tile = claim_tile(counter, &s_tile);
-  const uint64_t w0 = (uint64_t)tile * MC_TILE + (uint64_t)tid * MC_WORDS;
-  uint32_t wv[MC_WORDS];
-  uint32_t c = 0;
-#pragma unroll
-  for (int j = 0; j < MC_WORDS; j++) {
-    wv[j] = (w0 + j < words) ? marks[w0 + j] : 0u;
-    c += __popc(wv[j]);
-  }
+  const uint64_t w0 = (uint64_t)tile * MC_TILE + tid;
+  uint32_t m = (w0 < words) ? marks[w0] : 0u;
   uint32_t tot;
-  const uint32_t ex = block_excl_sum<NT>(c, s_scan, &tot);
+  const uint32_t ex = block_excl_sum<NT>((uint32_t)__popc(m), s_scan, &tot);
   if (warp == 0) {
     const uint64_t e = warp_lookback(states, tile, tot, status);
     if (lane == 0) {
@@ -226,46 +214,30 @@ __global__ void __launch_bounds__(NT)
   __syncthreads();
   uint64_t at = s_ex + ex;
   uint32_t flags = 0;
-#pragma unroll
-  for (int j = 0; j < MC_WORDS; j++) {
-    uint32_t m = wv[j];
-    if (m) marks[w0 + j] = 0u;
-    while (m) {
-      const int b = __ffs(m) - 1;
-      m &= m - 1;
-      const uint64_t ix = (w0 + j) * 32 + b;
-      if (ix >= entries || at >= out_cap) {
-        flags |= ST_BOUNDS;
-        continue;
-      }
-      out[at] = (K)(((K)(ix / n1) << b1) | (K)(ix % n1));
-      if constexpr (TROP) out_w[at] = D[ix];
-      at++;
+  if (m) marks[w0] = 0u;
+  while (m) {
+    const int b = __ffs(m) - 1;
+    m &= m - 1;
+    const uint64_t ix = w0 * 32 + b;
+    if (ix >= lay.entries || at >= out_cap) {
+      flags |= ST_BOUNDS;
+      continue;
     }
+    out[at] = key_of_index<K>(ix, lay);
+    if constexpr (TROP) out_w[at] = D[ix];
+    at++;
   }
   if (flags) atomicOr(status, flags);
 }
 
-template <class K>
-__global__ void k_dense_gather(const K* __restrict__ keys, uint64_t n, int b1, uint64_t mask1, uint64_t n1,
-                               uint64_t entries, const int32_t* __restrict__ D, int32_t* __restrict__ w,
-                               uint32_t* status) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint64_t ix = dense_index((uint64_t)keys[i], b1, mask1, n1);
-  if (ix >= entries) { atomicOr(status, ST_BOUNDS); return; }
-  w[i] = D[ix];
-}
-
-// Seed the index from sorted unique keys (and weights).
+// Seed the index from keys (and weights).
 template <class K, bool TROP>
-__global__ void k_dense_seed(const K* __restrict__ keys, const int32_t* __restrict__ w, uint64_t n, int b1,
-                             uint64_t mask1, uint64_t n1, uint64_t entries, uint32_t* bits, int32_t* D,
-                             uint32_t* status) {
+__global__ void k_dense_seed(const K* __restrict__ keys, const int32_t* __restrict__ w, uint64_t n,
+                             DenseLayout lay, uint32_t* bits, int32_t* D, uint32_t* status) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint64_t ix = dense_index((uint64_t)keys[i], b1, mask1, n1);
-  if (ix >= entries) { atomicOr(status, ST_BOUNDS); return; }
+  const uint64_t ix = dense_index((uint64_t)keys[i], lay);
+  if (ix >= lay.entries) { atomicOr(status, ST_BOUNDS); return; }
   if constexpr (TROP) D[ix] = w[i];
   else atomicOr(&bits[ix >> 5], 1u << (ix & 31));
 }
@@ -275,29 +247,37 @@ __global__ void k_fill_i32(int32_t* p, uint64_t n, int32_t v) {
     p[i] = v;
 }
 
-// Compact the index back into sorted packed keys (index order = key order).
+// The final relation in key order: ordinal q enumerates (c0, c1) row-major,
+// whatever the index layout.
 constexpr int DC_ITEMS = 8;
-constexpr uint32_t DC_TILE = NT * DC_ITEMS;  // index entries per tile
+constexpr uint32_t DC_TILE = NT * DC_ITEMS;
+
+__device__ __forceinline__ uint64_t index_of_ordinal(uint64_t q, const DenseLayout& L) {
+  if (!L.colmajor) return q;
+  const uint64_t c0 = q / L.n1, c1 = q - c0 * L.n1;
+  return c1 * L.n0 + c0;
+}
 
 template <class K, bool TROP>
 __global__ void __launch_bounds__(NT)
-    k_dense_compact(const uint32_t* __restrict__ bits, const int32_t* __restrict__ D, uint64_t entries, int b1,
-                    uint64_t n1, K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap,
-                    uint64_t* states, uint32_t* counter, uint64_t* d_count, uint32_t* status) {
+    k_dense_compact(const uint32_t* __restrict__ bits, const int32_t* __restrict__ D, DenseLayout lay,
+                    K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap, uint64_t* states,
+                    uint32_t* counter, uint64_t* d_count, uint32_t* status) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_scan[NT / 32 + 1];
   __shared__ uint64_t s_ex;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t tile = claim_tile(counter, &s_tile);
-  // blocked: thread owns DC_ITEMS consecutive entries
   const uint64_t b = (uint64_t)tile * DC_TILE + (uint64_t)tid * DC_ITEMS;
   uint32_t present = 0;
   int32_t wv[DC_ITEMS];
 #pragma unroll
   for (int j = 0; j < DC_ITEMS; j++) {
-    const uint64_t ix = b + j;
+    const uint64_t q = b + j;
     bool p = false;
-    if (ix < entries) {
+    wv[j] = 0;
+    if (q < lay.entries) {
+      const uint64_t ix = index_of_ordinal(q, lay);
       if constexpr (TROP) {
         wv[j] = D[ix];
         p = wv[j] != INT32_MAX;
@@ -321,9 +301,10 @@ __global__ void __launch_bounds__(NT)
 #pragma unroll
   for (int j = 0; j < DC_ITEMS; j++) {
     if ((present >> j) & 1u) {
-      const uint64_t ix = b + j;
+      const uint64_t q = b + j;
       if (at < out_cap) {
-        out[at] = (K)(((K)(ix / n1) << b1) | (K)(ix % n1));
+        const uint64_t c0 = q / lay.n1, c1 = q - c0 * lay.n1;
+        out[at] = (K)(((K)c0 << lay.b1) | (K)c1);
         if constexpr (TROP) out_w[at] = wv[j];
       } else {
         atomicOr(status, ST_BOUNDS);
@@ -335,117 +316,101 @@ __global__ void __launch_bounds__(NT)
 
 inline unsigned grid1(uint64_t n) { return (unsigned)ceil_div(n ? n : 1, NT); }
 
+size_t dense_expand_smem() { return (DE_TILE + 1) * (4 + 4) + DE_TILE * 2 + 16; }
+
 }  // namespace
 
 uint64_t dense_tile_size() { return DE_TILE; }
+uint32_t dense_group_max() { return kGroupMax; }
 
 template <class K, bool TROP>
 void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n, const uint64_t* pos,
-                  uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift,
-                  int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr, uint64_t n_nbr,
-                  const int32_t* nbr_w, int b1, uint64_t n1, uint64_t entries, uint32_t* bits, int32_t* D,
+                  uint64_t total, uint64_t candidates, int jshift, uint64_t jmask, int pshift, uint64_t pmask,
+                  int out_pshift, int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr,
+                  uint64_t n_nbr, const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D,
                   uint32_t* marks, uint64_t* splits_buf) {
   if (n == 0 || total == 0) return;
   const uint64_t tiles = ceil_div(n + total, DE_TILE);
   if (tiles > 0x7fffffffull) fail(STRATA_E_UNSUPPORTED, "expand too large for one launch");
   k_tile_splits<<<grid1(tiles + 1), NT, 0, ctx->stream>>>(pos, n, total, DE_TILE, tiles, splits_buf);
   after_launch(ctx, "k_tile_splits");
-  const uint64_t mask1 = b1 >= 64 ? ~0ull : ((1ull << b1) - 1);
   const int kh = kprof_begin(ctx, K_EXPAND_DENSE);
-  const size_t smem = dense_expand_smem<TROP>();
+  const size_t smem = dense_expand_smem();
   auto kern = k_expand_dense<K, TROP>;
   SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(
-      dkeys, dw, n, pos, total, splits_buf, jshift, jmask, pshift, pmask, out_pshift, out_vshift, off, n_nodes,
-      nbr, n_nbr, nbr_w, b1, mask1, n1, entries, bits, D, marks, ctx->d_status);
-  // Algorithmic bytes: Δ rows and their offsets, the CSR segments streamed
-  // (neighbour + weight) and one 4-byte index probe per candidate.
+  kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(dkeys, dw, n, pos, total, splits_buf, jshift, jmask, pshift,
+                                                   pmask, out_pshift, out_vshift, off, n_nodes, nbr, n_nbr, nbr_w,
+                                                   lay, bits, D, marks, ctx->d_status);
+  // Algorithmic bytes: every Δ row (key, weight, offsets), every CSR edge of
+  // a group read once (neighbour + weight), one 4-byte index probe per
+  // candidate (a candidate = one Δ row × one edge of its join value).
   const uint64_t wsz = TROP ? 4 : 0;
-  kprof_end(ctx, kh, n * (sizeof(K) + wsz + 8 + 4) + total * (4 + wsz) + total * 4);
+  kprof_end(ctx, kh, n * (sizeof(K) + wsz + 8 + 4) + total * (4 + wsz) + candidates * 4);
   after_launch(ctx, "k_expand_dense");
 }
 
 template <class K, bool TROP>
-uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, uint64_t entries, int b1, uint64_t n1,
-                             const int32_t* D, K* out, int32_t* out_w, uint64_t out_cap, uint64_t* states_buf) {
-  const uint64_t words = (entries + 31) / 32;
+uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const int32_t* D, K* out,
+                             int32_t* out_w, uint64_t out_cap, uint64_t* states_buf) {
+  const uint64_t words = (lay.entries + 31) / 32;
   const uint64_t tiles = ceil_div(words, MC_TILE);
   SK_CUDA(cudaMemsetAsync(states_buf, 0, sizeof(uint64_t) * (tiles + 2), ctx->stream));
   uint32_t* counter = reinterpret_cast<uint32_t*>(states_buf + tiles + 1);
-  k_marks_compact<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, entries, b1, n1, D, out, out_w,
-                                                                   out_cap, states_buf, counter, states_buf + tiles,
+  k_marks_compact<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, lay, D, out, out_w, out_cap,
+                                                                   states_buf, counter, states_buf + tiles,
                                                                    ctx->d_status);
   after_launch(ctx, "k_marks_compact");
-  uint64_t r;
   SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, states_buf + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
-  r = ctx->h_scalar[0];
-  return r;
+  return ctx->h_scalar[0];
 }
 
 uint64_t dense_marks_states(uint64_t entries) { return ceil_div((entries + 31) / 32, MC_TILE) + 2; }
 
-template <class K>
-void dense_gather(strata_ctx* ctx, const K* keys, uint64_t n, int b1, uint64_t n1, uint64_t entries,
-                  const int32_t* D, int32_t* w) {
-  if (!n) return;
-  const uint64_t mask1 = (1ull << b1) - 1;
-  k_dense_gather<K><<<grid1(n), NT, 0, ctx->stream>>>(keys, n, b1, mask1, n1, entries, D, w, ctx->d_status);
-  after_launch(ctx, "k_dense_gather");
-}
-
 template <class K, bool TROP>
-void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, int b1, uint64_t n1,
-                uint64_t entries, uint32_t* bits, int32_t* D) {
+void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, const DenseLayout& lay, uint32_t* bits,
+                int32_t* D) {
   if (TROP) {
-    k_fill_i32<<<(unsigned)std::min<uint64_t>(ceil_div(entries, NT), (uint64_t)ctx->num_sms * 16), NT, 0,
-                 ctx->stream>>>(D, entries, INT32_MAX);
+    k_fill_i32<<<(unsigned)std::min<uint64_t>(ceil_div(lay.entries, NT), (uint64_t)ctx->num_sms * 16), NT, 0,
+                 ctx->stream>>>(D, lay.entries, INT32_MAX);
     after_launch(ctx, "k_fill_i32");
   }
   if (!n) return;
-  const uint64_t mask1 = (1ull << b1) - 1;
-  k_dense_seed<K, TROP><<<grid1(n), NT, 0, ctx->stream>>>(keys, w, n, b1, mask1, n1, entries, bits, D, ctx->d_status);
+  k_dense_seed<K, TROP><<<grid1(n), NT, 0, ctx->stream>>>(keys, w, n, lay, bits, D, ctx->d_status);
   after_launch(ctx, "k_dense_seed");
 }
 
 template <class K, bool TROP>
-uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, uint64_t entries, int b1,
-                       uint64_t n1, K* out, int32_t* out_w, uint64_t out_cap) {
-  if (!entries) return 0;
-  const uint64_t tiles = ceil_div(entries, DC_TILE);
+uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, const DenseLayout& lay, K* out,
+                       int32_t* out_w, uint64_t out_cap) {
+  if (!lay.entries) return 0;
+  const uint64_t tiles = ceil_div(lay.entries, DC_TILE);
   DBuf<uint64_t> states(ctx, tiles + 2);
   uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles + 1);
   SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 2), ctx->stream));
-  k_dense_compact<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(bits, D, entries, b1, n1, out, out_w, out_cap,
-                                                                    states.p, counter, states.p + tiles,
-                                                                    ctx->d_status);
+  k_dense_compact<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(bits, D, lay, out, out_w, out_cap, states.p,
+                                                                    counter, states.p + tiles, ctx->d_status);
   after_launch(ctx, "k_dense_compact");
-  uint64_t r;
   SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, states.p + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
-  r = ctx->h_scalar[0];
-  return r;
+  return ctx->h_scalar[0];
 }
 
-#define SK_INST_DENSE(K, T)                                                                               \
-  template void dense_expand<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const uint64_t*,       \
-                                   uint64_t, int, uint64_t, int, uint64_t, int, int, const uint32_t*,      \
-                                   uint64_t, const uint32_t*, uint64_t, const int32_t*, int, uint64_t,     \
-                                   uint64_t, uint32_t*, int32_t*, uint32_t*, uint64_t*);                   \
-  template uint64_t dense_marks_compact<K, T>(strata_ctx*, uint32_t*, uint64_t, int, uint64_t,             \
-                                              const int32_t*, K*, int32_t*, uint64_t, uint64_t*);          \
-  template void dense_seed<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, int, uint64_t, uint64_t, \
-                                 uint32_t*, int32_t*);                                                     \
-  template uint64_t dense_compact<K, T>(strata_ctx*, const uint32_t*, const int32_t*, uint64_t, int,       \
-                                        uint64_t, K*, int32_t*, uint64_t);
+#define SK_INST_DENSE(K, T)                                                                                 \
+  template void dense_expand<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const uint64_t*,         \
+                                   uint64_t, uint64_t, int, uint64_t, int, uint64_t, int, int,               \
+                                   const uint32_t*, uint64_t, const uint32_t*, uint64_t, const int32_t*,     \
+                                   const DenseLayout&, uint32_t*, int32_t*, uint32_t*, uint64_t*);           \
+  template uint64_t dense_marks_compact<K, T>(strata_ctx*, uint32_t*, const DenseLayout&, const int32_t*,    \
+                                              K*, int32_t*, uint64_t, uint64_t*);                            \
+  template void dense_seed<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const DenseLayout&,        \
+                                 uint32_t*, int32_t*);                                                       \
+  template uint64_t dense_compact<K, T>(strata_ctx*, const uint32_t*, const int32_t*, const DenseLayout&, K*, \
+                                        int32_t*, uint64_t);
 SK_INST_DENSE(uint32_t, false)
 SK_INST_DENSE(uint32_t, true)
 SK_INST_DENSE(uint64_t, false)
 SK_INST_DENSE(uint64_t, true)
 #undef SK_INST_DENSE
-template void dense_gather<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, uint64_t,
-                                     const int32_t*, int32_t*);
-template void dense_gather<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, uint64_t, uint64_t,
-                                     const int32_t*, int32_t*);
 
 }  // namespace sk

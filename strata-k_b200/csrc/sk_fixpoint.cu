@@ -313,7 +313,8 @@ struct DenseIdx {
   DBuf<uint32_t> marks;  // changed in the current round
   DBuf<int32_t> D;       // Trop weights (INT32_MAX = absent)
   DBuf<uint64_t> states; // look-back words of the marks compaction
-  uint64_t n0 = 0, n1 = 0, entries = 0;
+  DenseLayout lay{};
+  uint64_t entries = 0;
   uint64_t words() const { return (entries + 31) / 32; }
 };
 
@@ -332,12 +333,12 @@ inline bool want_dense(strata_ctx* ctx, bool trop, bool narrow, uint64_t n0, uin
   return fits;
 }
 
+// `colmajor`: the next round joins on c1 (store c1-major), else on c0.
 template <bool TROP>
-void dense_alloc(strata_ctx* ctx, DenseIdx& X, uint64_t n0, uint64_t n1) {
+void dense_alloc(strata_ctx* ctx, DenseIdx& X, uint64_t n0, uint64_t n1, int b1, bool colmajor) {
   X.bits.ctx = X.D.ctx = X.marks.ctx = X.states.ctx = ctx;
-  X.n0 = n0;
-  X.n1 = n1;
   X.entries = n0 * n1;
+  X.lay = DenseLayout{b1, low_mask(b1), n0, n1, X.entries, colmajor};
   if (!TROP) {
     X.bits.reserve(X.words() + 1);
     SK_CUDA(cudaMemsetAsync(X.bits.p, 0, (X.words() + 1) * 4, ctx->stream));
@@ -357,27 +358,31 @@ uint64_t dense_round(strata_ctx* ctx, const K* dk, const int32_t* dw, uint64_t n
   const uint64_t l0 = ctx->launches;
   const int t = pt.begin(&a.join_ms);
   s.pos.reserve_grow(nd + 1);
-  expand_offsets<K>(ctx, dk, nd, js.jshift, js.jmask, csr.off.p, csr.n_nodes, s.pos.p);
-  uint64_t T = 0;
-  read_checked(ctx, s.pos.p + nd, &T, 1);
+  SK_CUDA(cudaMemsetAsync(s.counts.p, 0, 16, ctx->stream));
+  expand_offsets<K>(ctx, dk, nd, js.jshift, js.jmask, csr.off.p, csr.n_nodes, s.pos.p, dense_group_max(),
+                    s.counts.p + 1);
+  SK_CUDA(cudaMemcpyAsync(s.counts.p, s.pos.p + nd, 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  uint64_t tc[2] = {0, 0};
+  read_checked(ctx, s.counts.p, tc, 2);
+  const uint64_t T = tc[0], cands = tc[1];  // (group, edge) outputs; candidates
   uint64_t cnt = 0;
   if (T) {
-    const uint64_t cap = std::min<uint64_t>(T, X.entries) + 1;
+    const uint64_t cap = std::min<uint64_t>(cands, X.entries) + 1;
     out.reserve(cap, TROP);
     splits.reserve_grow(ceil_div(nd + T, dense_tile_size()) + 2);
-    dense_expand<K, TROP>(ctx, dk, dw, nd, s.pos.p, T, js.jshift, js.jmask, js.pshift, js.pmask, js.out_pshift,
-                          js.out_vshift, csr.off.p, csr.n_nodes, csr.nbr.p, csr.m, TROP ? csr.w.p : nullptr, b1,
-                          X.n1, X.entries, TROP ? nullptr : X.bits.p, TROP ? X.D.p : nullptr, X.marks.p,
-                          splits.p);
-    // Δ' in key order, with merged weights; marks cleared for the next round.
-    cnt = dense_marks_compact<K, TROP>(ctx, X.marks.p, X.entries, b1, X.n1, TROP ? X.D.p : nullptr, out.k.p,
+    dense_expand<K, TROP>(ctx, dk, dw, nd, s.pos.p, T, cands, js.jshift, js.jmask, js.pshift, js.pmask,
+                          js.out_pshift, js.out_vshift, csr.off.p, csr.n_nodes, csr.nbr.p, csr.m,
+                          TROP ? csr.w.p : nullptr, X.lay, TROP ? nullptr : X.bits.p, TROP ? X.D.p : nullptr,
+                          X.marks.p, splits.p);
+    // Δ' sorted by the next join column, with merged weights; marks cleared.
+    cnt = dense_marks_compact<K, TROP>(ctx, X.marks.p, X.lay, TROP ? X.D.p : nullptr, out.k.p,
                                        TROP ? out.w.p : nullptr, cap, X.states.p);
   }
   pt.end(t);
   const uint64_t wsz = TROP ? 4 : 0;
-  a.join_b += nd * (sizeof(K) + wsz + 16) + T * (4 + wsz) + T * 4 + cnt * (sizeof(K) + 2 * wsz);
+  a.join_b += nd * (sizeof(K) + wsz + 16) + T * (4 + wsz) + cands * 4 + cnt * (sizeof(K) + 2 * wsz);
   a.join_l += (uint32_t)(ctx->launches - l0);
-  a.cands += T;
+  a.cands += cands;
   return cnt;
 }
 
@@ -405,9 +410,10 @@ void fix_loop_dense(strata_ctx* ctx, Rel<K, int32_t>& delta, const Csr<int32_t>&
 // Compact the index into a sorted relation.
 template <class K, bool TROP>
 void dense_finish(strata_ctx* ctx, DenseIdx& X, int b1, Rel<K, int32_t>& full, uint64_t upper) {
+  (void)b1;
   const uint64_t cap = std::min<uint64_t>(upper, X.entries) + 1;
   full.reserve(cap, TROP);
-  full.n = dense_compact<K, TROP>(ctx, X.bits.p, TROP ? X.D.p : nullptr, X.entries, b1, X.n1, full.k.p,
+  full.n = dense_compact<K, TROP>(ctx, X.bits.p, TROP ? X.D.p : nullptr, X.lay, full.k.p,
                                   TROP ? full.w.p : nullptr, cap);
 }
 
@@ -451,9 +457,10 @@ strata_rel* run_tc_shape(strata_ctx* ctx, const EdgeCols& e, int b0, int b1, int
     if (dense) {
       plan = 2;
       DenseIdx X;
-      dense_alloc<TROP>(ctx, X, n_nodes_src, n_nodes_dst);
-      if (TROP) dense_seed<K, true>(ctx, full.k.p, full.w.p, full.n, b1, X.n1, X.entries, X.bits.p, X.D.p);
-      else dense_seed<K, false>(ctx, full.k.p, nullptr, full.n, b1, X.n1, X.entries, X.bits.p, nullptr);
+      // Δ(Y,Z) joins on c0: row-major index.
+      dense_alloc<TROP>(ctx, X, n_nodes_src, n_nodes_dst, b1, false);
+      if (TROP) dense_seed<K, true>(ctx, full.k.p, full.w.p, full.n, X.lay, X.bits.p, X.D.p);
+      else dense_seed<K, false>(ctx, full.k.p, nullptr, full.n, X.lay, X.bits.p, nullptr);
       pt.end(a.setup_t);
       fix_loop_dense<K, TROP>(ctx, delta, csr, js, b1, X, cap, s, pt, a, &rounds);
       const int tf = pt.begin(&a.finish_ms);
@@ -587,8 +594,9 @@ strata_rel* run_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
   if constexpr (std::is_same<W, int32_t>::value) {
     if (dense) {
       DenseIdx X;
-      dense_alloc<true>(ctx, X, n0, n1);
-      dense_seed<K, true>(ctx, nullptr, nullptr, 0, b1, X.n1, X.entries, X.bits.p, X.D.p);
+      // Δ(S,Y) joins on c1: column-major index, so Δ' comes out sorted by Y.
+      dense_alloc<true>(ctx, X, n0, n1, b1, true);
+      dense_seed<K, true>(ctx, nullptr, nullptr, 0, X.lay, X.bits.p, X.D.p);
       Rel<K, W> delta, full;
       delta.k.ctx = delta.w.ctx = full.k.ctx = full.w.ctx = ctx;
       DBuf<uint64_t> splits;

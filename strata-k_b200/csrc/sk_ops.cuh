@@ -27,32 +27,43 @@ void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* ou
                            unsigned char* scratch, uint64_t max_n, uint32_t* h_status);
 
 // ---- direct-addressed plan (sk_dense.cu) ----
+// Index over (c0, c1) in [0, n0) × [0, n1); `colmajor` stores (c0, c1) at
+// c1 * n0 + c0 (the join column of the next round first), else c0 * n1 + c1.
+struct DenseLayout {
+  int b1;           // key = (c0 << b1) | c1
+  uint64_t mask1;   // (1 << b1) - 1
+  uint64_t n0, n1;  // column domain sizes
+  uint64_t entries; // n0 * n1
+  bool colmajor;
+};
 uint64_t dense_tile_size();
+uint32_t dense_group_max();
 template <class K, bool TROP>
 void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n, const uint64_t* pos,
-                  uint64_t total, int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift,
-                  int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr, uint64_t n_nbr,
-                  const int32_t* nbr_w, int b1, uint64_t n1, uint64_t entries, uint32_t* bits, int32_t* D,
+                  uint64_t total, uint64_t candidates, int jshift, uint64_t jmask, int pshift, uint64_t pmask,
+                  int out_pshift, int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr,
+                  uint64_t n_nbr, const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D,
                   uint32_t* marks, uint64_t* splits_buf);
 template <class K, bool TROP>
-uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, uint64_t entries, int b1, uint64_t n1,
-                             const int32_t* D, K* out, int32_t* out_w, uint64_t out_cap, uint64_t* states_buf);
+uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const int32_t* D, K* out,
+                             int32_t* out_w, uint64_t out_cap, uint64_t* states_buf);
 uint64_t dense_marks_states(uint64_t entries);
-template <class K>
-void dense_gather(strata_ctx* ctx, const K* keys, uint64_t n, int b1, uint64_t n1, uint64_t entries,
-                  const int32_t* D, int32_t* w);
 template <class K, bool TROP>
-void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, int b1, uint64_t n1,
-                uint64_t entries, uint32_t* bits, int32_t* D);
+void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, const DenseLayout& lay, uint32_t* bits,
+                int32_t* D);
 template <class K, bool TROP>
-uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, uint64_t entries, int b1,
-                       uint64_t n1, K* out, int32_t* out_w, uint64_t out_cap);
+uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, const DenseLayout& lay, K* out,
+                       int32_t* out_w, uint64_t out_cap);
 
 // Exclusive scan of per-element expand degrees (see sk_relops.cu).
 // pos[i] = sum_{k<i} deg(i); pos[n] = total.  Returns nothing; read pos[n].
+// Grouped mode (gmax > 0): only the first item of each run of equal join
+// value (runs split at multiples of gmax) gets its degree; *cand_total (if
+// given) receives the sum of every item's degree, i.e. the candidate count.
 template <class K>
 void expand_offsets(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uint64_t jmask,
-                    const uint32_t* off, uint64_t n_nodes, uint64_t* pos);
+                    const uint32_t* off, uint64_t n_nodes, uint64_t* pos, uint32_t gmax = 0,
+                    uint64_t* cand_total = nullptr);
 
 // Load-balanced expand: for every Δ tuple i and every CSR neighbour v of its
 // join value, emit  out = (kept(i) << out_pshift) | (v << out_vshift), with

@@ -32,7 +32,8 @@ template <class K>
 __global__ void __launch_bounds__(NT)
     k_expand_offsets(const K* __restrict__ dkeys, uint64_t n, int jshift, uint64_t jmask,
                      const uint32_t* __restrict__ off, uint64_t n_nodes, uint64_t* __restrict__ pos,
-                     uint64_t* states, uint32_t* counter, uint32_t* status) {
+                     uint64_t* states, uint32_t* counter, uint32_t* status, uint32_t gmax,
+                     unsigned long long* cand_total) {
   __shared__ uint32_t s_tile;
   __shared__ uint64_t s_warp[NT / 32 + 1];
   __shared__ uint64_t s_excl;
@@ -41,6 +42,7 @@ __global__ void __launch_bounds__(NT)
   const uint64_t wbase = (uint64_t)tile * EO_TILE + (uint64_t)warp * 32 * EO_ITEMS;
   uint64_t vals[EO_ITEMS];
   uint64_t carry = 0;
+  unsigned long long cands = 0;
 #pragma unroll
   for (int j = 0; j < EO_ITEMS; j++) {
     const uint64_t idx = wbase + j * 32 + lane;
@@ -48,12 +50,19 @@ __global__ void __launch_bounds__(NT)
     if (idx < n) {
       const uint64_t jv = ((uint64_t)dkeys[idx] >> jshift) & jmask;
       if (jv < n_nodes) deg = (uint64_t)(off[jv + 1] - off[jv]);
+      cands += deg;
+      // grouped: a follower of a run (same join value, same gmax block) has no outputs
+      if (gmax && idx % gmax != 0 && (((uint64_t)dkeys[idx - 1] >> jshift) & jmask) == jv) deg = 0;
     }
     const uint64_t incl = warp_incl_sum(deg);
     vals[j] = carry + incl - deg;
     carry += __shfl_sync(kFull, incl, 31);
   }
   if (lane == 0) s_warp[warp] = carry;
+  if (cand_total) {
+    cands = warp_sum(cands);
+    if (lane == 0 && cands) atomicAdd(cand_total, cands);
+  }
   __syncthreads();
   if (warp == 0) {
     uint64_t w = (lane < NT / 32) ? s_warp[lane] : 0;
@@ -676,7 +685,7 @@ inline int grid_for(strata_ctx* ctx, uint64_t n, int per_block = NT) {
 // ---------------------------------------------------------------------------
 template <class K>
 void expand_offsets(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uint64_t jmask,
-                    const uint32_t* off, uint64_t n_nodes, uint64_t* pos) {
+                    const uint32_t* off, uint64_t n_nodes, uint64_t* pos, uint32_t gmax, uint64_t* cand_total) {
   if (n == 0) {
     SK_CUDA(cudaMemsetAsync(pos, 0, sizeof(uint64_t), ctx->stream));
     return;
@@ -687,7 +696,8 @@ void expand_offsets(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uin
   SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 1), ctx->stream));
   const int kh = kprof_begin(ctx, K_EXPAND_OFFSETS);
   k_expand_offsets<K><<<tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, pos,
-                                                     states.p, counter, ctx->d_status);
+                                                     states.p, counter, ctx->d_status, gmax,
+                                                     reinterpret_cast<unsigned long long*>(cand_total));
   kprof_end(ctx, kh, n * (sizeof(K) + 8 + 8));
   after_launch(ctx, "k_expand_offsets");
 }
@@ -880,8 +890,10 @@ uint64_t fingerprint(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int
 }
 
 // ---- explicit instantiations ----------------------------------------------------
-template void expand_offsets<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t, uint64_t*);
-template void expand_offsets<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t, uint64_t*);
+template void expand_offsets<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t,
+                                       uint64_t*, uint32_t, uint64_t*);
+template void expand_offsets<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t,
+                                       uint64_t*, uint32_t, uint64_t*);
 template void build_csr<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, uint32_t*, uint32_t*);
 template void build_csr<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, uint64_t, uint32_t*, uint32_t*);
 
