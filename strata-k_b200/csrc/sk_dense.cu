@@ -61,25 +61,12 @@ __device__ __forceinline__ uint64_t dense_index(uint64_t key, const DenseLayout&
   return L.colmajor ? c1 * L.n0 + c0 : c0 * L.n1 + c1;
 }
 
-template <class K>
-__device__ __forceinline__ K key_of_index(uint64_t ix, const DenseLayout& L) {
-  uint64_t c0, c1;
-  if (L.colmajor) {
-    c1 = ix / L.n0;
-    c0 = ix - c1 * L.n0;
-  } else {
-    c0 = ix / L.n1;
-    c1 = ix - c0 * L.n1;
-  }
-  return (K)(((K)c0 << L.b1) | (K)c1);
-}
-
 // Grouped expand.  pos[] comes from expand_offsets in grouped mode: only the
 // head of each group (a run of equal join value, split at multiples of
 // kGroupMax) carries the degree of its join value, so one expand output is
 // one (group, edge) pair; the thread applies that edge to every member.
 template <class K, bool TROP>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 6)
     k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n,
                    const uint64_t* __restrict__ pos, uint64_t total, const uint64_t* __restrict__ splits,
                    int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift, int out_vshift,
@@ -158,27 +145,58 @@ __global__ void __launch_bounds__(NT)
     const uint64_t h = a + li;
     const uint64_t jh = ((uint64_t)dkeys[h] >> jshift) & jmask;
     const uint64_t g_end = min(n, (h / kGroupMax + 1) * kGroupMax);
-    for (uint64_t m = h; m < g_end; m++) {
-      const K mk = dkeys[m];
-      if (m != h && (((uint64_t)mk >> jshift) & jmask) != jh) break;
-      const uint32_t kept = (uint32_t)(((uint64_t)mk >> pshift) & pmask);
-      const K key = (K)(((K)kept << out_pshift) | ((K)v << out_vshift));
-      const uint64_t ix = dense_index((uint64_t)key, lay);
-      if (ix >= lay.entries) {
-        flags |= ST_BOUNDS;
-        continue;
-      }
-      const uint32_t bit = 1u << (ix & 31);
-      if constexpr (TROP) {
-        const int32_t cw = trop_mul(dw[m], ew, &flags);
-        if (cw < D[ix]) {
-          const int32_t old = atomicMin(&D[ix], cw);
-          if (cw < old) atomicOr(&marks[ix >> 5], bit);  // changed this round
+    // Members four at a time so their index probes are in flight together.
+    constexpr int MU = 4;
+    bool more = true;
+    for (uint64_t m0 = h; more && m0 < g_end; m0 += MU) {
+      uint64_t ix[MU];
+      int32_t cw[MU], cur[MU];
+      bool ok[MU];
+#pragma unroll
+      for (int u = 0; u < MU; u++) {
+        const uint64_t m = m0 + u;
+        ok[u] = more && m < g_end;
+        cw[u] = 0;
+        ix[u] = 0;
+        if (ok[u]) {
+          const K mk = dkeys[m];
+          if (m != h && (((uint64_t)mk >> jshift) & jmask) != jh) {
+            ok[u] = false;
+            more = false;  // the run ended
+          } else {
+            const uint32_t kept = (uint32_t)(((uint64_t)mk >> pshift) & pmask);
+            const K key = (K)(((K)kept << out_pshift) | ((K)v << out_vshift));
+            ix[u] = dense_index((uint64_t)key, lay);
+            if (ix[u] >= lay.entries) {
+              flags |= ST_BOUNDS;
+              ok[u] = false;
+            } else if constexpr (TROP) {
+              cw[u] = trop_mul(dw[m], ew, &flags);
+            }
+          }
         }
-      } else {
-        if ((bits[ix >> 5] & bit) == 0) {
-          const uint32_t old = atomicOr(&bits[ix >> 5], bit);
-          if ((old & bit) == 0) atomicOr(&marks[ix >> 5], bit);  // new this round
+      }
+#pragma unroll
+      for (int u = 0; u < MU; u++) {
+        if (ok[u]) {
+          if constexpr (TROP) cur[u] = D[ix[u]];
+          else cur[u] = (int32_t)bits[ix[u] >> 5];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < MU; u++) {
+        if (!ok[u]) continue;
+        const uint32_t bit = 1u << (ix[u] & 31);
+        if constexpr (TROP) {
+          if (cw[u] < cur[u]) {
+            const int32_t old = atomicMin(&D[ix[u]], cw[u]);
+            if (cw[u] < old) atomicOr(&marks[ix[u] >> 5], bit);  // changed this round
+          }
+        } else {
+          if (((uint32_t)cur[u] & bit) == 0) {
+            const uint32_t old = atomicOr(&bits[ix[u] >> 5], bit);
+            if ((old & bit) == 0) atomicOr(&marks[ix[u] >> 5], bit);  // new this round
+          }
         }
       }
     }
@@ -187,46 +205,94 @@ __global__ void __launch_bounds__(NT)
 }
 
 // Δ' of a round: the marked index entries in index order, with their merged
-// weight (Trop); the marks are cleared for the next round.
+// weight (Trop); the marks are cleared for the next round.  Reduce-then-scan:
+// per-tile counts, one-block scan, then the write (no waiting between tiles).
 constexpr uint32_t MC_TILE = NT;  // bitmap words per tile (one per thread)
 
+__global__ void __launch_bounds__(NT) k_marks_count(const uint32_t* __restrict__ marks, uint64_t words,
+                                                    uint64_t* __restrict__ tile_sums) {
+  __shared__ uint32_t s_red[NT / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t w = (uint64_t)blockIdx.x * MC_TILE + tid;
+  uint32_t c = (w < words) ? __popc(marks[w]) : 0u;
+  c = warp_sum(c);
+  if (lane == 0) s_red[warp] = c;
+  __syncthreads();
+  if (tid == 0) {
+    uint64_t t = 0;
+    for (int q = 0; q < NT / 32; q++) t += s_red[q];
+    tile_sums[blockIdx.x] = t;
+  }
+}
+
+// Position of the k-th (0-based) set bit of w (k < popc(w)).
+__device__ __forceinline__ uint32_t select_bit(uint32_t w, uint32_t k) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (int sh = 16; sh >= 1; sh >>= 1) {
+    const uint32_t c = __popc((w >> pos) & ((1u << sh) - 1u));
+    if (k >= c) {
+      k -= c;
+      pos += sh;
+    }
+  }
+  return pos;
+}
+
+// Each warp enumerates the set bits of its 32 words in index order, 32 at a
+// time across the lanes, so the key stores and the weight gathers coalesce.
 template <class K, bool TROP>
 __global__ void __launch_bounds__(NT)
-    k_marks_compact(uint32_t* marks, uint64_t words, DenseLayout lay, const int32_t* __restrict__ D,
-                    K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap, uint64_t* states,
-                    uint32_t* counter, uint64_t* d_count, uint32_t* status) {
-  __shared__ uint32_t s_tile;
+    k_marks_write(uint32_t* marks, uint64_t words, DenseLayout lay, const int32_t* __restrict__ D,
+                  K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap,
+                  const uint64_t* __restrict__ tile_sums, uint32_t* status) {
   __shared__ uint32_t s_scan[NT / 32 + 1];
-  __shared__ uint64_t s_ex;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t tile = claim_tile(counter, &s_tile);
-  const uint64_t w0 = (uint64_t)tile * MC_TILE + tid;
-  uint32_t m = (w0 < words) ? marks[w0] : 0u;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const uint64_t wi = (uint64_t)blockIdx.x * MC_TILE + tid;
+  const uint32_t m = (wi < words) ? marks[wi] : 0u;
+  const uint32_t c = __popc(m);
   uint32_t tot;
-  const uint32_t ex = block_excl_sum<NT>((uint32_t)__popc(m), s_scan, &tot);
-  if (warp == 0) {
-    const uint64_t e = warp_lookback(states, tile, tot, status);
-    if (lane == 0) {
-      s_ex = e;
-      if (tile == gridDim.x - 1) *d_count = e + tot;
-    }
-  }
-  __syncthreads();
-  uint64_t at = s_ex + ex;
+  const uint32_t ex = block_excl_sum<NT>(c, s_scan, &tot);
+  const uint32_t incl = warp_incl_sum(c);
+  const uint32_t wtot = __shfl_sync(kFull, incl, 31);
+  const uint64_t wbase = tile_sums[blockIdx.x] + __shfl_sync(kFull, ex, 0);
+  const uint64_t width = lay.colmajor ? lay.n0 : lay.n1;
+  const uint64_t b = wi * 32;
+  const uint64_t row_b = b / width, col_b = b - row_b * width;  // one division per word
   uint32_t flags = 0;
-  if (m) marks[w0] = 0u;
-  while (m) {
-    const int b = __ffs(m) - 1;
-    m &= m - 1;
-    const uint64_t ix = w0 * 32 + b;
-    if (ix >= lay.entries || at >= out_cap) {
-      flags |= ST_BOUNDS;
-      continue;
+  for (uint32_t s0 = 0; s0 < wtot; s0 += 32) {
+    const uint32_t slot = s0 + lane;
+    // owner lane = number of lanes whose inclusive count is <= slot
+    int t = 0;
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) {
+      const uint32_t v = __shfl_sync(kFull, incl, t + sh - 1);
+      if (v <= slot) t += sh;
     }
-    out[at] = key_of_index<K>(ix, lay);
-    if constexpr (TROP) out_w[at] = D[ix];
-    at++;
+    t &= 31;
+    const uint32_t ex_t = __shfl_sync(kFull, incl - c, t);
+    const uint32_t mw = __shfl_sync(kFull, m, t);
+    const uint64_t rb = __shfl_sync(kFull, row_b, t), cb = __shfl_sync(kFull, col_b, t);
+    const uint64_t wt = __shfl_sync(kFull, wi, t);
+    if (slot < wtot) {
+      const uint32_t bit = select_bit(mw, slot - ex_t);
+      uint64_t row = rb, col = cb + bit;
+      while (col >= width) {
+        col -= width;
+        row++;
+      }
+      const uint64_t ix = wt * 32 + bit;
+      const uint64_t at = wbase + slot;
+      if (ix >= lay.entries || at >= out_cap) {
+        flags |= ST_BOUNDS;
+      } else {
+        const uint64_t c0 = lay.colmajor ? col : row, c1 = lay.colmajor ? row : col;
+        out[at] = (K)(((K)c0 << lay.b1) | (K)c1);
+        if constexpr (TROP) out_w[at] = D[ix];
+      }
+    }
   }
+  if (m) marks[wi] = 0u;
   if (flags) atomicOr(status, flags);
 }
 
@@ -252,12 +318,6 @@ __global__ void k_fill_i32(int32_t* p, uint64_t n, int32_t v) {
 constexpr int DC_ITEMS = 8;
 constexpr uint32_t DC_TILE = NT * DC_ITEMS;
 
-__device__ __forceinline__ uint64_t index_of_ordinal(uint64_t q, const DenseLayout& L) {
-  if (!L.colmajor) return q;
-  const uint64_t c0 = q / L.n1, c1 = q - c0 * L.n1;
-  return c1 * L.n0 + c0;
-}
-
 template <class K, bool TROP>
 __global__ void __launch_bounds__(NT)
     k_dense_compact(const uint32_t* __restrict__ bits, const int32_t* __restrict__ D, DenseLayout lay,
@@ -271,13 +331,21 @@ __global__ void __launch_bounds__(NT)
   const uint64_t b = (uint64_t)tile * DC_TILE + (uint64_t)tid * DC_ITEMS;
   uint32_t present = 0;
   int32_t wv[DC_ITEMS];
+  // (c0, c1) of ordinal b, then stepped: one division per thread.
+  uint64_t q0 = b / lay.n1, q1 = b - q0 * lay.n1;
 #pragma unroll
   for (int j = 0; j < DC_ITEMS; j++) {
     const uint64_t q = b + j;
     bool p = false;
     wv[j] = 0;
+    if (j) {
+      if (++q1 == lay.n1) {
+        q1 = 0;
+        q0++;
+      }
+    }
     if (q < lay.entries) {
-      const uint64_t ix = index_of_ordinal(q, lay);
+      const uint64_t ix = lay.colmajor ? q1 * lay.n0 + q0 : q;
       if constexpr (TROP) {
         wv[j] = D[ix];
         p = wv[j] != INT32_MAX;
@@ -298,12 +366,17 @@ __global__ void __launch_bounds__(NT)
   }
   __syncthreads();
   uint64_t at = s_ex + ex;
+  uint64_t c0 = b / lay.n1, c1 = b - c0 * lay.n1;
 #pragma unroll
   for (int j = 0; j < DC_ITEMS; j++) {
+    if (j) {
+      if (++c1 == lay.n1) {
+        c1 = 0;
+        c0++;
+      }
+    }
     if ((present >> j) & 1u) {
-      const uint64_t q = b + j;
       if (at < out_cap) {
-        const uint64_t c0 = q / lay.n1, c1 = q - c0 * lay.n1;
         out[at] = (K)(((K)c0 << lay.b1) | (K)c1);
         if constexpr (TROP) out_w[at] = wv[j];
       } else {
@@ -351,16 +424,16 @@ void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n
 
 template <class K, bool TROP>
 uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const int32_t* D, K* out,
-                             int32_t* out_w, uint64_t out_cap, uint64_t* states_buf) {
+                             int32_t* out_w, uint64_t out_cap, uint64_t* sums) {
   const uint64_t words = (lay.entries + 31) / 32;
   const uint64_t tiles = ceil_div(words, MC_TILE);
-  SK_CUDA(cudaMemsetAsync(states_buf, 0, sizeof(uint64_t) * (tiles + 2), ctx->stream));
-  uint32_t* counter = reinterpret_cast<uint32_t*>(states_buf + tiles + 1);
-  k_marks_compact<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, lay, D, out, out_w, out_cap,
-                                                                   states_buf, counter, states_buf + tiles,
-                                                                   ctx->d_status);
-  after_launch(ctx, "k_marks_compact");
-  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, states_buf + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  k_marks_count<<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, sums);
+  after_launch(ctx, "k_marks_count");
+  scan_tile_sums(ctx, sums, tiles);
+  k_marks_write<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, lay, D, out, out_w, out_cap, sums,
+                                                                 ctx->d_status);
+  after_launch(ctx, "k_marks_write");
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, sums + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
   return ctx->h_scalar[0];
 }

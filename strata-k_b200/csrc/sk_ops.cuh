@@ -48,6 +48,8 @@ template <class K, bool TROP>
 uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const int32_t* D, K* out,
                              int32_t* out_w, uint64_t out_cap, uint64_t* states_buf);
 uint64_t dense_marks_states(uint64_t entries);
+// In-place exclusive scan of per-tile sums (one block); sums[count] = total.
+void scan_tile_sums(strata_ctx* ctx, uint64_t* sums, uint64_t count);
 template <class K, bool TROP>
 void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, const DenseLayout& lay, uint32_t* bits,
                 int32_t* D);

@@ -25,7 +25,7 @@ constexpr int NT = 256;
 // ---------------------------------------------------------------------------
 // expand: offsets
 // ---------------------------------------------------------------------------
-constexpr int EO_ITEMS = 8;
+constexpr int EO_ITEMS = 16;
 constexpr uint32_t EO_TILE = NT * EO_ITEMS;
 
 template <class K>
@@ -82,6 +82,110 @@ __global__ void __launch_bounds__(NT)
     const uint64_t idx = wbase + j * 32 + lane;
     if (idx < n) pos[idx] = base + vals[j];
   }
+}
+
+// ---------------------------------------------------------------------------
+// reduce-then-scan variant of the offsets (no waiting between tiles): one
+// kernel sums each tile's degrees, one block scans the tile sums, a third
+// kernel writes pos[].  Used where tiles carry little work, so that a
+// look-back chain would dominate.
+// ---------------------------------------------------------------------------
+template <class K>
+__device__ __forceinline__ uint64_t group_degree(const K* dkeys, uint64_t idx, int jshift, uint64_t jmask,
+                                                 const uint32_t* off, uint64_t n_nodes, uint32_t gmax,
+                                                 uint64_t* full_deg) {
+  const uint64_t jv = ((uint64_t)dkeys[idx] >> jshift) & jmask;
+  uint64_t deg = jv < n_nodes ? (uint64_t)(off[jv + 1] - off[jv]) : 0;
+  *full_deg = deg;
+  if (gmax && idx % gmax != 0 && (((uint64_t)dkeys[idx - 1] >> jshift) & jmask) == jv) deg = 0;
+  return deg;
+}
+
+template <class K>
+__global__ void __launch_bounds__(NT)
+    k_deg_count(const K* __restrict__ dkeys, uint64_t n, int jshift, uint64_t jmask,
+                const uint32_t* __restrict__ off, uint64_t n_nodes, uint32_t gmax, uint64_t* __restrict__ tile_sums,
+                unsigned long long* cand_total) {
+  __shared__ uint64_t s_red[NT / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * EO_TILE;
+  uint64_t sum = 0;
+  unsigned long long cands = 0;
+  for (int j = 0; j < EO_ITEMS; j++) {
+    const uint64_t idx = base + (uint64_t)j * NT + tid;
+    if (idx < n) {
+      uint64_t fd;
+      sum += group_degree(dkeys, idx, jshift, jmask, off, n_nodes, gmax, &fd);
+      cands += fd;
+    }
+  }
+  sum = warp_sum(sum);
+  if (cand_total) {
+    cands = warp_sum(cands);
+    if (lane == 0 && cands) atomicAdd(cand_total, cands);
+  }
+  if (lane == 0) s_red[warp] = sum;
+  __syncthreads();
+  if (tid == 0) {
+    uint64_t t = 0;
+    for (int w = 0; w < NT / 32; w++) t += s_red[w];
+    tile_sums[blockIdx.x] = t;
+  }
+}
+
+// In-place exclusive scan of `count` tile sums in one block; sums[count] = total.
+__global__ void __launch_bounds__(1024) k_scan_tile_sums(uint64_t* sums, uint64_t count) {
+  __shared__ uint64_t s_scratch[1024 / 32 + 1];
+  const uint64_t per = (count + 1023) / 1024;
+  const uint64_t b = (uint64_t)threadIdx.x * per;
+  uint64_t local = 0;
+  for (uint64_t i = b; i < b + per && i < count; i++) local += sums[i];
+  uint64_t tot;
+  uint64_t run = block_excl_sum<1024>(local, s_scratch, &tot);
+  for (uint64_t i = b; i < b + per && i < count; i++) {
+    const uint64_t v = sums[i];
+    sums[i] = run;
+    run += v;
+  }
+  if (threadIdx.x == 0) sums[count] = tot;
+}
+
+template <class K>
+__global__ void __launch_bounds__(NT)
+    k_deg_write(const K* __restrict__ dkeys, uint64_t n, int jshift, uint64_t jmask, const uint32_t* __restrict__ off,
+                uint64_t n_nodes, uint32_t gmax, const uint64_t* __restrict__ tile_sums, uint64_t n_tiles,
+                uint64_t* __restrict__ pos) {
+  __shared__ uint64_t s_warp[NT / 32 + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // warp-striped so each warp's 32 x ITEMS items are contiguous (as in the count)
+  const uint64_t base = (uint64_t)blockIdx.x * EO_TILE;
+  uint64_t vals[EO_ITEMS];
+  uint64_t carry = 0;
+  const uint64_t wbase = base + (uint64_t)warp * 32 * EO_ITEMS;
+#pragma unroll
+  for (int j = 0; j < EO_ITEMS; j++) {
+    const uint64_t idx = wbase + j * 32 + lane;
+    uint64_t deg = 0, fd;
+    if (idx < n) deg = group_degree(dkeys, idx, jshift, jmask, off, n_nodes, gmax, &fd);
+    const uint64_t incl = warp_incl_sum(deg);
+    vals[j] = carry + incl - deg;
+    carry += __shfl_sync(kFull, incl, 31);
+  }
+  if (lane == 0) s_warp[warp] = carry;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t w = (lane < NT / 32) ? s_warp[lane] : 0;
+    uint64_t wi = warp_incl_sum(w);
+    if (lane < NT / 32) s_warp[lane] = wi - w;
+  }
+  __syncthreads();
+  const uint64_t b0 = tile_sums[blockIdx.x] + s_warp[warp];
+#pragma unroll
+  for (int j = 0; j < EO_ITEMS; j++) {
+    const uint64_t idx = wbase + j * 32 + lane;
+    if (idx < n) pos[idx] = b0 + vals[j];
+  }
+  if (blockIdx.x == gridDim.x - 1 && tid == 0) pos[n] = tile_sums[n_tiles];
 }
 
 // ---------------------------------------------------------------------------
@@ -691,15 +795,22 @@ void expand_offsets(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uin
     return;
   }
   const uint32_t tiles = (uint32_t)ceil_div(n, EO_TILE);
-  DBuf<uint64_t> states(ctx, tiles + 1);
-  uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles);
-  SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 1), ctx->stream));
+  DBuf<uint64_t> sums(ctx, tiles + 1);
   const int kh = kprof_begin(ctx, K_EXPAND_OFFSETS);
-  k_expand_offsets<K><<<tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, pos,
-                                                     states.p, counter, ctx->d_status, gmax,
-                                                     reinterpret_cast<unsigned long long*>(cand_total));
-  kprof_end(ctx, kh, n * (sizeof(K) + 8 + 8));
-  after_launch(ctx, "k_expand_offsets");
+  // The count uses the same warp-striped item order as the write; only the
+  // per-tile totals matter, so its block-strided loop is equivalent.
+  k_deg_count<K><<<tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, gmax, sums.p,
+                                                reinterpret_cast<unsigned long long*>(cand_total));
+  k_scan_tile_sums<<<1, 1024, 0, ctx->stream>>>(sums.p, tiles);
+  k_deg_write<K><<<tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, gmax, sums.p, tiles, pos);
+  kprof_end(ctx, kh, 2 * n * (sizeof(K) + 8) + n * 8);
+  ctx->launches += 2;
+  after_launch(ctx, "k_deg_write");
+}
+
+void scan_tile_sums(strata_ctx* ctx, uint64_t* sums, uint64_t count) {
+  k_scan_tile_sums<<<1, 1024, 0, ctx->stream>>>(sums, count);
+  after_launch(ctx, "k_scan_tile_sums");
 }
 
 template <class K, class W, bool TROP>
