@@ -47,13 +47,20 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--workload", choices=["mssp", "tc", "tri"], default="mssp",
+                    help="mssp: the headline Trop program; tc / tri: the Bool closure and triangle-count configs")
+    ap.add_argument("--plan", choices=["auto", "sort-merge", "dense"], default="auto")
+    ap.add_argument("--tuned", action="store_true", help="apply the autotuner's cached knob values")
+    ap.add_argument("--scale", type=int, default=None, help="R-MAT scale (mssp: 20, tri: 22)")
     ap.add_argument("--sources", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-sort-plan", action="store_true", help="skip the sort-merge plan measurement")
     ap.add_argument("--out", default=None, help="also write the JSON line here")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.scale is None:
+        args.scale = 22 if args.workload == "tri" else 20
+    return args
 
 
 def dist_env():
@@ -63,21 +70,49 @@ def dist_env():
     return rank, world, local
 
 
-def workload_for(rank: int, scale: int, n_sources: int):
+def workload_for(rank: int, scale: int, n_sources: int, kind: str = "mssp"):
     from strata_b200 import gen
+    if kind == "tc":
+        return gen.tc_workload(seed=1 + 1000 * rank)
+    if kind == "tri":
+        return gen.triangle_workload(scale=scale, seed=3 + 1000 * rank)
     return gen.mssp_workload(scale=scale, n_sources=n_sources, seed=2 + 1000 * rank)
 
 
+PLANS = {"auto": 0, "sort-merge": 1, "dense": 2}
+
+
+def metric_for(kind: str) -> str:
+    return {"mssp": METRIC,
+            "tc": "derived tuples/s (Bool transitive-closure fixpoint, |path| / device time)",
+            "tri": "derived tuples/s (WCOJ triangle pattern count, triangles / device time)"}[kind]
+
+
 def config(args, world):
+    common = {"parallelism": f"replicas{world}", "plan": args.plan,
+              "l2": "flushed (256 MiB write) before every timed step"}
+    if args.workload == "tc":
+        return {"workload": "bool_tc_er_10000n_50000e",
+                "program": "path(X,Y) :- edge(X,Y). path(X,Z) :- edge(X,Y), path(Y,Z).",
+                "graph": "Erdos-Renyi directed, 10,000 nodes, 50,000 distinct edges, no self-loops", **common}
+    if args.workload == "tri":
+        return {"workload": f"wcoj_triangles_rmat{args.scale}",
+                "program": "n(count<X>) :- e(X,Y), e(Y,Z), e(X,Z).",
+                "graph": f"undirected R-MAT scale {args.scale}, {16 << args.scale} edges drawn, "
+                         "deduplicated, oriented by degree", **common}
     return {
         "workload": f"trop_mssp_rmat{args.scale}_{args.sources}src",
         "program": "dist(S,Y) :- src(S), edge(S,Y). dist(S,Z) :- dist(S,Y), edge(Y,Z). (Trop)",
         "graph": f"R-MAT scale {args.scale}, {8 << args.scale} distinct directed edges, "
                  "a=0.57 b=0.19 c=0.19, i64 weights U[1,100]",
-        "sources": args.sources,
-        "parallelism": f"replicas{world}",
-        "l2": "flushed (256 MiB write) before every timed step",
+        "sources": args.sources, **common,
     }
+
+
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of
+# the dominant kernel, from one ncu capture of the named workload; absent
+# (null) when no capture of that workload and kernel exists.
+TRAFFIC: dict = {}
 
 
 # ---------------------------------------------------------------- clocks
@@ -136,21 +171,37 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU baseline
-def cpu_sample(wl, threads: int, n_sample_sources: int, steps: int):
-    """The reference interpreter's algorithm (oracle restatement) on a bounded
-    sample: the bootstrap round of the same program on the full graph for the
-    first `n_sample_sources` sources.  Returns (tuples/s, seconds/step, tuples)."""
+def cpu_sample(kind: str, wl, threads: int, steps: int):
+    """The reference interpreter's algorithm (oracle restatement, nested-loop
+    solve) on a bounded sample of the workload.  Returns (tuples/s per step,
+    seconds per step, tuples, description of the sample)."""
     import oracle as O
-    srcs = wl.sources[:n_sample_sources]
-    sess = O.Session(O.mssp_program(srcs, wl.src, wl.dst, wl.w, wl.source_w[:n_sample_sources]))
+    if kind == "mssp":
+        n_s = min(16, len(wl.sources))
+        prog = O.mssp_program(wl.sources[:n_s], wl.src, wl.dst, wl.w, wl.source_w[:n_s])
+        head, rounds = "dist", 0
+        sample = (f"bootstrap round (all derivations of dist(S,Y) :- src(S), edge(S,Y)) for {n_s} of the "
+                  f"{len(wl.sources)} sources on the full graph")
+    elif kind == "tc":
+        prog = O.tc_program(wl.src, wl.dst)
+        head, rounds = "path", 3
+        sample = "bootstrap plus the first 3 delta rounds of the closure on the full graph"
+    else:
+        lim = 1 << 17
+        keep = (wl.src < lim) & (wl.dst < lim)
+        prog = O.count_program(wl.src[keep], wl.dst[keep])
+        head, rounds = "ntri", -1
+        sample = (f"the count program on the subgraph induced by the first {lim} interned node ids "
+                  f"({int(keep.sum())} of {len(wl.src)} edges)")
+    sess = O.Session(prog)
     rates, secs_all, tup = [], [], 0
     for _ in range(steps):
-        counts, _, secs = sess.run(threads=threads, max_rounds=0)
-        tup = counts["dist"]
+        counts, _, secs = sess.run(threads=threads, max_rounds=rounds)
+        tup = counts[head]
         rates.append(tup / secs if secs > 0 else 0.0)
         secs_all.append(secs)
     sess.close()
-    return rates, secs_all, tup
+    return rates, secs_all, tup, sample
 
 
 def run_reference(args):
@@ -158,18 +209,17 @@ def run_reference(args):
     if rank != 0:
         return 0
     cores = os.cpu_count() or 1
-    wl = workload_for(0, args.scale, args.sources)
-    n_s = min(16, len(wl.sources))
+    wl = workload_for(0, args.scale, args.sources, args.workload)
     t0 = time.time()
-    rates, secs, tup = cpu_sample(wl, cores, n_s, args.warmup + args.steps)
+    rates, secs, tup, sample = cpu_sample(args.workload, wl, cores, args.warmup + args.steps)
     timed = secs[args.warmup:]
     value = tup * len(timed) / sum(timed) if sum(timed) > 0 else 0.0
-    sample = (f"bootstrap round (all derivations of dist(S,Y) :- src(S), edge(S,Y) by the nested-loop "
-              f"solve) for {n_s} of the {len(wl.sources)} sources on the full graph; {tup} tuples per step")
+    sample = f"{sample}; {tup} tuples per step"
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "impl": "reference", "metric": metric_for(args.workload), "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(timed) / max(1, len(timed)),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int64" if args.workload == "mssp" else "u32",
         "data": "synthetic", "config": config(args, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -182,6 +232,78 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- our arm
+class Job:
+    """One workload bound to an engine: its pinned host columns, the fixpoint
+    call on resident device columns, and the host read-back of the result."""
+
+    def __init__(self, kind, wl, eng, torch):
+        self.kind, self.wl, self.eng, self.torch = kind, wl, eng, torch
+        i32, i64 = np.int32, np.int64
+        if kind == "mssp":
+            cols = (("sources", wl.sources, i32), ("sw", wl.source_w, i64), ("src", wl.src, i32),
+                    ("dst", wl.dst, i32), ("w", wl.w, i64))
+        else:
+            cols = (("src", wl.src, i32), ("dst", wl.dst, i32))
+        self.host = {k: torch.from_numpy(np.ascontiguousarray(v).astype(dt)).pin_memory() for k, v, dt in cols}
+        self.entry = {"mssp": "strata_mssp_trop_dev", "tc": "strata_tc_bool_dev",
+                      "tri": "strata_count_triangle_pattern_dev"}[kind]
+
+    def run(self, d):
+        """One fixpoint on device columns `d`: returns (result handle, tuples, stats)."""
+        if self.kind == "mssp":
+            rel = self.eng.mssp_dev(d["sources"], d["src"], d["dst"], d["w"], source_weights=d["sw"])
+        elif self.kind == "tc":
+            rel = self.eng.tc_bool_dev(d["src"], d["dst"])
+        else:
+            return None, self.eng.count_triangle_pattern_dev(d["src"], d["dst"]), None
+        return rel, len(rel), rel.stats
+
+    @staticmethod
+    def free(handle):
+        if handle is not None:
+            handle.free()
+
+    def out_buffers(self, n):
+        torch = self.torch
+        if self.kind == "tri":
+            return None
+        trop = self.kind == "mssp"
+        return (torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                torch.empty(n, dtype=torch.int64).pin_memory().numpy() if trop else None,
+                torch.empty(n, dtype=torch.uint8).pin_memory().numpy() if trop else None)
+
+    def fetch(self, handle, tuples, out):
+        """Result to the host; returns the bytes read back."""
+        if self.kind == "tri":
+            return 8  # the u64 count, returned through the entry point's out-parameter
+        res = handle.to_host(out=out)
+        assert len(res) == tuples
+        return tuples * (4 + 4 + (8 + 1 if self.kind == "mssp" else 0))
+
+
+def _timed_steps(step, free, stream, flush, steps, torch):
+    """`steps` fixpoints, each bracketed by CUDA events on `stream`, with an
+    L2 flush before each outside the interval.  Returns (ms, tuples, stats)."""
+    total_ms, tuples, stats = 0.0, 0, None
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h, tuples, stats = step()
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        free(h)
+    return total_ms, tuples, stats
+
+
+def _kernels(ks):
+    return {k: {"launches": v[0], "ms": round(v[1], 3), "gbs": (v[2] / (v[1] / 1000.0) / 1e9) if v[1] else None}
+            for k, v in ks.items() if v[0]}
+
+
 def run_ours(args):
     import torch
 
@@ -196,28 +318,22 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
-    wl = workload_for(rank, args.scale, args.sources)
-    eng = S.Engine(local)
+    wl = workload_for(rank, args.scale, args.sources, args.workload)
+    eng = S.Engine(local, tuned=args.tuned)
+    eng.set_plan(PLANS[args.plan])
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
-
-    def dev(a, dt):
-        return torch.from_numpy(np.ascontiguousarray(a).astype(dt))
-
-    host = {k: dev(v, dt).pin_memory() for k, v, dt in (
-        ("sources", wl.sources, np.int32), ("sw", wl.source_w, np.int64), ("src", wl.src, np.int32),
-        ("dst", wl.dst, np.int32), ("w", wl.w, np.int64))}
+    job = Job(args.workload, wl, eng, torch)
     with torch.cuda.stream(stream):
-        d = {k: v.to("cuda", non_blocking=True) for k, v in host.items()}
+        d = {k: v.to("cuda", non_blocking=True) for k, v in job.host.items()}
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
     stream.synchronize()
 
     def step():
-        rel = eng.mssp_dev(d["sources"], d["src"], d["dst"], d["w"], source_weights=d["sw"])
-        return rel
+        return job.run(d)
 
     for _ in range(args.warmup):
-        step().free()
+        job.free(step()[0])
     # ---- timed region: device-only fixpoints (inputs resident in HBM)
     eng.set_profiling(True)
     eng.reset_kernel_stats()
@@ -227,19 +343,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     clocks.start()
     launches0 = eng.launches()
-    total_ms, tuples, stats = 0.0, 0, None
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1)  # L2 flush outside the timed interval
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        rel = step()
-        e1.record(stream)
-        e1.synchronize()
-        total_ms += e0.elapsed_time(e1)
-        tuples = len(rel)
-        stats = rel.stats
-        rel.free()
+    total_ms, tuples, stats = _timed_steps(step, job.free, stream, flush, args.steps, torch)
     torch.cuda.synchronize()
     launches = eng.launches() - launches0
     clk = clocks.stop()
@@ -248,34 +352,21 @@ def run_ours(args):
 
     # ---- the sort-merge plan on the same inputs (reported beside the headline)
     sort_plan = None
-    if not args.no_sort_plan:
-        eng.set_plan(1)
-        step().free()  # warm its buffers
+    if not args.no_sort_plan and args.workload != "tri" and args.plan == "auto":
+        eng.set_plan(PLANS["sort-merge"])
+        job.free(step()[0])  # warm its buffers
         eng.set_profiling(True)
         eng.reset_kernel_stats()
-        sp_ms = 0.0
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            rel = step()
-            e1.record(stream)
-            e1.synchronize()
-            sp_ms += e0.elapsed_time(e1)
-            sp_stats = rel.stats
-            assert len(rel) == tuples
-            rel.free()
+        sp_ms, sp_tuples, sp_stats = _timed_steps(step, job.free, stream, flush, args.steps, torch)
+        assert sp_tuples == tuples
         sk = eng.kernel_stats()
         eng.set_profiling(False)
-        eng.set_plan(0)
+        eng.set_plan(PLANS["auto"])
         sort_plan = {"plan": "sort-merge (radix sort + run reduction + merge-path diff per round)",
                      "ms_per_step": sp_ms / args.steps, "value": tuples * args.steps / (sp_ms / 1000.0),
-                     "phase_ms": {k: round(sp_stats[k + "_ms"], 3) for k in ("setup", "join", "sort", "diff", "merge", "finish")},
-                     "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
-                                     "gbs": (v[2] / (v[1] / 1000.0) / 1e9) if v[1] else None,
-                                     "frac_of_hbm": ((v[2] / (v[1] / 1000.0) / 1e9) / 6548.8) if v[1] else None}
-                                 for k, v in sk.items() if v[0]}}
+                     "phase_ms": {k: round(sp_stats[k + "_ms"], 3)
+                                  for k in ("setup", "join", "sort", "diff", "merge", "finish")},
+                     "kernels": _kernels(sk)}
     if pg:
         t = torch.tensor([total_ms, float(tuples)], dtype=torch.float64, device="cuda")
         mx = t.clone()
@@ -291,26 +382,22 @@ def run_ours(args):
     # ---- e2e: pinned host inputs -> device -> fixpoint -> result on the host
     e2e = None
     if not args.no_e2e:
-        n_out = tuples
-        out_host = (torch.empty(n_out, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
-                    torch.empty(n_out, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
-                    torch.empty(n_out, dtype=torch.int64).pin_memory().numpy(),
-                    torch.empty(n_out, dtype=torch.uint8).pin_memory().numpy())
-        h2d = sum(v.numel() * v.element_size() for v in host.values())
-        e2e_ms = 0.0
+        out_host = job.out_buffers(tuples)
+        h2d = sum(v.numel() * v.element_size() for v in job.host.values())
+        e2e_ms, d2h = 0.0, 0
         for i in range(args.steps + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             with torch.cuda.stream(stream):
-                dd = {k: v.to("cuda", non_blocking=True) for k, v in host.items()}
-            rel = eng.mssp_dev(dd["sources"], dd["src"], dd["dst"], dd["w"], source_weights=dd["sw"])
-            res = rel.to_host(out=out_host)
+                dd = {k: v.to("cuda", non_blocking=True) for k, v in job.host.items()}
+            h, n_out, _ = job.run(dd)
+            d2h = job.fetch(h, n_out, out_host)
             t1 = time.perf_counter()
-            rel.free()
+            assert n_out == tuples
+            job.free(h)
             del dd
             if i > 0:  # first iteration is a warm-up
                 e2e_ms += 1000 * (t1 - t0)
-        d2h = n_out * (4 + 4 + 8 + 1)
         e2e_val = tuples * args.steps / (e2e_ms / 1000.0)
         if pg:
             t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
@@ -318,8 +405,8 @@ def run_ours(args):
             e2e_val = all_tuples * args.steps / (float(t[0]) / 1000.0)
         e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
-               "path": "pinned host columns -> torch H2D -> strata_mssp_trop_dev -> strata_rel_to_host (pinned)"}
-        assert len(res) == tuples
+               "path": f"pinned host columns -> torch H2D -> {job.entry}"
+                       + (" (count out-parameter)" if args.workload == "tri" else " -> strata_rel_to_host (pinned)")}
 
     # ---- roofline of the dominant kernel
     peaks = {}
@@ -333,38 +420,37 @@ def run_ours(args):
     achieved = (kbytes / kl) / ((kms / kl) / 1000.0) / 1e9 if kl and kms else 0.0
     roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_source": peak_src,
             "unit": "GB/s", "frac": achieved / peak if peak else None,
-            "traffic": None, "launches_per_step": kl / args.steps,
+            "traffic": TRAFFIC.get((args.workload, name)), "launches_per_step": kl / args.steps,
             "avg_launch_us": 1000 * kms / kl if kl else None,
             "algorithmic_bytes_per_launch": kbytes / kl if kl else None,
-            "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
-                            "gbs": (v[2] / (v[1] / 1000.0) / 1e9) if v[1] else None}
-                        for k, v in kstats.items() if v[0]}}
+            "kernels": _kernels(kstats)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        n_s = min(16, len(wl.sources))
-        rates, secs, tup = cpu_sample(wl, cores, n_s, 1)
+        rates, secs, tup, sample = cpu_sample(args.workload, wl, cores, 1)
         cpu = {"value": rates[-1], "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"reference interpreter algorithm (oracle restatement, nested-loop solve) on the "
-                         f"bootstrap round for {n_s} of {len(wl.sources)} sources, full graph: {tup} tuples "
-                         f"in {secs[-1]:.2f} s"}
+               "sample": f"{sample}: {tup} tuples in {secs[-1]:.2f} s"}
 
     if rank == 0:
+        wb = stats["weight_bytes"] if stats else 0
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "metric": metric_for(args.workload), "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "int32" if stats["weight_bytes"] == 4 else "int64",
+            "dtype": {4: "int32", 8: "int64"}.get(wb, "u32"),
             "data": "synthetic", "config": config(args, world),
-            "plan": {1: "sort-merge", 2: "direct-addressed"}.get(stats["plan"], "?"),
-            "tuples_per_step": int(all_tuples), "rounds": stats["rounds"],
-            "candidates_per_step": stats["candidates"], "key_bits": stats["key_bits"],
-            "weight_bytes": stats["weight_bytes"],
-            "phase_ms": {k: round(stats[k + "_ms"], 3) for k in ("setup", "join", "sort", "diff", "merge", "finish")},
+            "tuples_per_step": int(all_tuples),
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-            "sort_merge_plan": sort_plan,
         }
+        if stats:
+            line.update({
+                "plan": {1: "sort-merge", 2: "direct-addressed"}.get(stats["plan"], "?"),
+                "rounds": stats["rounds"], "candidates_per_step": stats["candidates"],
+                "key_bits": stats["key_bits"], "weight_bytes": stats["weight_bytes"],
+                "phase_ms": {k: round(stats[k + "_ms"], 3)
+                             for k in ("setup", "join", "sort", "diff", "merge", "finish")},
+                "sort_merge_plan": sort_plan})
         print(json.dumps(line), flush=True)
         if args.out:
             Path(args.out).write_text(json.dumps(line) + "\n")

@@ -184,6 +184,23 @@ strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan) {
   return STRATA_OK;
 }
 
+strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (knob != STRATA_KNOB_SORT_ITEMS_U32 && knob != STRATA_KNOB_SORT_ITEMS_U64)
+    return bad(ctx, "unknown knob (1 = radix keys/thread for u32 keys, 2 = for u64 keys)");
+  const int kb = knob == STRATA_KNOB_SORT_ITEMS_U32 ? 4 : 8;
+  if (value != 0) {
+    int c[8];
+    const int nc = sk::radix_items_choices(kb, c, 8);
+    bool ok = false;
+    for (int i = 0; i < nc; i++) ok |= c[i] == value;
+    if (!ok) return bad(ctx, kb == 4 ? "radix keys/thread for u32 keys must be 0, 11, 15, 19 or 23"
+                                     : "radix keys/thread for u64 keys must be 0, 7, 9 or 13");
+  }
+  (kb == 4 ? ctx->tune_items4 : ctx->tune_items8) = value;
+  return STRATA_OK;
+}
+
 strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled) {
   if (!ctx) return STRATA_E_INVALID;
   ctx->profiling = enabled != 0;

@@ -77,6 +77,8 @@ struct strata_ctx {
   int num_sms = 148;
   cudaMemPool_t pool = nullptr;     // this context's pool (kept mapped between calls)
   int plan = 0;                     // 0 auto, 1 sort-merge, 2 direct-addressed
+  int tune_items4 = 0;              // radix keys per thread, u32 keys (0 = default)
+  int tune_items8 = 0;              // radix keys per thread, u64 keys (0 = default)
   bool profiling = false;
   uint64_t launches = 0;
   // Per-kernel CUDA-event accounting (enabled with profiling).

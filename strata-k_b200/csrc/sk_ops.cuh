@@ -21,6 +21,10 @@ template <class K, class V>
 void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has_vals,
                 uint64_t n, int bits, bool skip_trivial = true);
 
+// Keys-per-thread choices of the onesweep tile for 4- or 8-byte keys
+// (strata_ctx_set_knob); returns how many, writes up to max_out.
+int radix_items_choices(int key_bytes, int* out, int max_out);
+
 // Allocation-free u32 key sort on caller-provided scratch (sk_noalloc.cu).
 uint64_t radix_sort_u32_static_bytes(uint64_t max_n);
 void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* out, uint64_t n, int bits,

@@ -32,25 +32,45 @@ template <class K> struct RCfg;
 template <> struct RCfg<uint32_t> { static constexpr int ITEMS = 15; };
 template <> struct RCfg<uint64_t> { static constexpr int ITEMS = 9; };
 
-// Digit histograms of passes [p0, p0 + np), np <= 4.
+// Digit histograms of passes [p0, p0 + np), np <= 4.  Each warp loads HI
+// keys per lane warp-striped (coalesced) and counts into its own shared
+// counters; when all 32 lanes of a full row hold the same digit (long runs of
+// equal high digits are the common case for packed keys) one add of 32
+// replaces 32 atomics.
 template <class K>
 __global__ void __launch_bounds__(NT) k_radix_hist(const K* __restrict__ keys, uint64_t n, int p0,
                                                    int np, uint32_t* __restrict__ hist) {
+  constexpr int HI = 8;
   __shared__ uint32_t sh[4][NW][RADIX];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < 4 * NW * RADIX; i += NT) (&sh[0][0][0])[i] = 0;
   __syncthreads();
-  const uint64_t stride = (uint64_t)gridDim.x * NT;
-  // Every lane of a warp runs the same number of iterations (match-any needs
-  // the full warp), so loop on the warp's first index.
-  for (uint64_t i0 = (uint64_t)blockIdx.x * NT + (tid & ~31); i0 < n; i0 += stride) {
-    const uint64_t i = i0 + lane;
-    const bool valid = i < n;
-    const K k = valid ? keys[i] : K(0);
+  const uint64_t chunk = (uint64_t)NT * HI;
+  for (uint64_t b0 = (uint64_t)blockIdx.x * chunk; b0 < n; b0 += (uint64_t)gridDim.x * chunk) {
+    const uint64_t wb = b0 + (uint64_t)warp * 32 * HI;
+    K k[HI];
+#pragma unroll
+    for (int j = 0; j < HI; j++) {
+      const uint64_t i = wb + j * 32 + lane;
+      k[j] = i < n ? keys[i] : K(0);
+    }
     for (int p = 0; p < np; p++) {
-      const uint32_t d = valid ? (uint32_t)(k >> (8 * (p0 + p))) & 0xffu : 0x100u;
-      const unsigned peers = __match_any_sync(kFull, d);
-      if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&sh[p][warp][d], (uint32_t)__popc(peers));
+      const int sh_bits = 8 * (p0 + p);
+#pragma unroll
+      for (int j = 0; j < HI; j++) {
+        const uint64_t row = wb + j * 32;
+        const uint32_t d = (uint32_t)(k[j] >> sh_bits) & 0xffu;
+        if (row + 31 < n) {  // warp-uniform: the whole row is in range
+          const uint32_t d0 = __shfl_sync(kFull, d, 0);
+          if (__all_sync(kFull, d == d0)) {
+            if (lane == 0) atomicAdd(&sh[p][warp][d0], 32u);
+          } else {
+            atomicAdd(&sh[p][warp][d], 1u);
+          }
+        } else if (row + lane < n) {
+          atomicAdd(&sh[p][warp][d], 1u);
+        }
+      }
     }
   }
   __syncthreads();
@@ -197,13 +217,11 @@ __global__ void __launch_bounds__(NT) k_onesweep(const K* __restrict__ kin, K* _
 
 }  // namespace
 
-template <class K, class V>
-void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has_vals,
-                uint64_t n, int bits, bool skip_trivial) {
-  if (n <= 1 || bits <= 0) return;
-  if (n > kMaxSortN) fail(STRATA_E_UNSUPPORTED, "radix sort call limited to 2^30-1 keys");
-  if (bits > (int)(8 * sizeof(K))) bits = 8 * sizeof(K);
-  constexpr int ITEMS = RCfg<K>::ITEMS;
+namespace {
+
+template <class K, class V, int ITEMS>
+void radix_sort_impl(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has_vals,
+                     uint64_t n, int bits, bool skip_trivial) {
   constexpr uint32_t TILE = NT * ITEMS;
   const int passes = (bits + 7) / 8;
 
@@ -258,6 +276,41 @@ void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has
     after_launch(ctx, "k_onesweep");
     std::swap(*keys, *alt);
     if (has_vals) std::swap(*vals, *valt);
+  }
+}
+
+}  // namespace
+
+// Keys per thread of the onesweep tile, selectable per context (the tuning
+// knobs); the default is RCfg<K>::ITEMS.
+int radix_items_choices(int key_bytes, int* out, int max_out) {
+  static const int c4[] = {11, 15, 19, 23};
+  static const int c8[] = {7, 9, 13};
+  const int* c = key_bytes == 4 ? c4 : c8;
+  const int nc = key_bytes == 4 ? 4 : 3;
+  for (int i = 0; i < nc && i < max_out; i++) out[i] = c[i];
+  return nc;
+}
+
+template <class K, class V>
+void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has_vals,
+                uint64_t n, int bits, bool skip_trivial) {
+  if (n <= 1 || bits <= 0) return;
+  if (n > kMaxSortN) fail(STRATA_E_UNSUPPORTED, "radix sort call limited to 2^30-1 keys");
+  if (bits > (int)(8 * sizeof(K))) bits = 8 * sizeof(K);
+  if constexpr (sizeof(K) == 4) {
+    switch (ctx->tune_items4) {
+      case 11: return radix_sort_impl<K, V, 11>(ctx, keys, alt, vals, valt, has_vals, n, bits, skip_trivial);
+      case 19: return radix_sort_impl<K, V, 19>(ctx, keys, alt, vals, valt, has_vals, n, bits, skip_trivial);
+      case 23: return radix_sort_impl<K, V, 23>(ctx, keys, alt, vals, valt, has_vals, n, bits, skip_trivial);
+      default: return radix_sort_impl<K, V, 15>(ctx, keys, alt, vals, valt, has_vals, n, bits, skip_trivial);
+    }
+  } else {
+    switch (ctx->tune_items8) {
+      case 7: return radix_sort_impl<K, V, 7>(ctx, keys, alt, vals, valt, has_vals, n, bits, skip_trivial);
+      case 13: return radix_sort_impl<K, V, 13>(ctx, keys, alt, vals, valt, has_vals, n, bits, skip_trivial);
+      default: return radix_sort_impl<K, V, 9>(ctx, keys, alt, vals, valt, has_vals, n, bits, skip_trivial);
+    }
   }
 }
 

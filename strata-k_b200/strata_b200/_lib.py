@@ -27,6 +27,7 @@ E_NOT_BUILT = 8
 E_WEIGHT_RANGE = 9
 
 PLAN_AUTO, PLAN_SORT_MERGE, PLAN_DENSE = 0, 1, 2
+KNOB_SORT_ITEMS_U32, KNOB_SORT_ITEMS_U64 = 1, 2
 
 KERNELS = {0: "k_onesweep", 1: "k_expand_emit", 2: "k_expand_offsets", 3: "k_reduce_runs",
            4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count", 7: "k_expand_dense"}
@@ -77,6 +78,7 @@ SIGNATURES = {
     "strata_ctx_mem": (C.c_int, [ctxp, u64p, u64p]),
     "strata_ctx_set_profiling": (C.c_int, [ctxp, C.c_int]),
     "strata_ctx_set_plan": (C.c_int, [ctxp, C.c_int]),
+    "strata_ctx_set_knob": (C.c_int, [ctxp, C.c_int, C.c_int]),
     "strata_ctx_launches": (C.c_uint64, [ctxp]),
     "strata_ctx_kernel_stats": (C.c_int, [ctxp, C.c_int, u64p, C.POINTER(C.c_double), u64p]),
     "strata_ctx_reset_kernel_stats": (C.c_int, [ctxp]),

@@ -174,7 +174,7 @@ class Engine:
     device bytes the engine may hold (0 = unbounded).
     """
 
-    def __init__(self, device: int = 0, mem_cap: int = 0, profiling: bool = False):
+    def __init__(self, device: int = 0, mem_cap: int = 0, profiling: bool = False, tuned: bool = False):
         self.lib = L.load()
         ctx = L.ctxp()
         rc = self.lib.strata_ctx_create(device, mem_cap, C.byref(ctx))
@@ -184,6 +184,9 @@ class Engine:
         self.device = device
         if profiling:
             self.lib.strata_ctx_set_profiling(self.ctx, 1)
+        if tuned:  # knob values cached by `python -m strata_b200.tune` for this GPU
+            from . import tune
+            tune.apply_cached(self)
 
     # -- plumbing ---------------------------------------------------------
     def close(self):
@@ -214,6 +217,10 @@ class Engine:
     def set_plan(self, plan: int):
         """0 automatic, 1 sort-merge, 2 direct-addressed (results are identical)."""
         self._check(self.lib.strata_ctx_set_plan(self.ctx, plan))
+
+    def set_knob(self, knob: int, value: int):
+        """Tuning knob (1: radix keys/thread for u32 keys, 2: for u64 keys; 0 = default)."""
+        self._check(self.lib.strata_ctx_set_knob(self.ctx, knob, value))
 
     def set_profiling(self, on: bool):
         self._check(self.lib.strata_ctx_set_profiling(self.ctx, 1 if on else 0))

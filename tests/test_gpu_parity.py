@@ -434,3 +434,48 @@ def test_plans_pick_and_agree(engine):
         engine.shortest_paths_trop([(0, 1, 10**13), (1, 2, 1)])
     engine.set_plan(0)
     assert engine.shortest_paths_trop([(0, 1, 10**13), (1, 2, 1)]).stats["plan"] == 1
+
+
+@pytest.mark.parametrize("kb,choices", [(4, (11, 15, 19, 23)), (8, (7, 9, 13))])
+def test_sort_knobs_identical(engine, kb, choices):
+    """Every keys-per-thread choice of the radix tile sorts identically
+    (stable, with values) on sizes that end mid-tile for every choice."""
+    import ctypes as C
+    import torch
+    knob = 1 if kb == 4 else 2
+    for n in (1, 4097, 300_001):
+        rng = np.random.default_rng(n + kb)
+        kdt = np.uint32 if kb == 4 else np.uint64
+        bits = 26 if kb == 4 else 41
+        keys = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(kdt)
+        keys[: n // 3] = keys[0]  # a long run of one key (histogram fast path)
+        vals = np.arange(n, dtype=np.uint32)
+        order = np.argsort(keys, kind="stable")
+        ki, vi = _dev(keys, np.int32 if kb == 4 else np.int64), _dev(vals, np.int32)
+        for v in choices:
+            engine.set_knob(knob, v)
+            ko, vo = torch.empty_like(ki), torch.empty_like(vi)
+            engine._check(engine.lib.strata_op_sort(engine.ctx, kb, 4, C.c_void_p(ki.data_ptr()),
+                                                    C.c_void_p(vi.data_ptr()), C.c_void_p(ko.data_ptr()),
+                                                    C.c_void_p(vo.data_ptr()), n, bits))
+            assert np.array_equal(ko.cpu().numpy().view(kdt), keys[order]), v
+            assert np.array_equal(vo.cpu().numpy().view(np.uint32), vals[order]), v
+    engine.set_knob(knob, 0)
+    with pytest.raises(S.InvalidArgument):
+        engine.set_knob(knob, 12)
+    with pytest.raises(S.InvalidArgument):
+        engine.set_knob(3, 0)
+
+
+def test_sort_knobs_fixpoint_identical(engine):
+    """A sort-merge fixpoint gives the same relation under every knob value."""
+    wl = gen.mssp_workload(scale=10, n_sources=8, seed=5)
+    engine.set_plan(1)
+    base = engine.mssp_trop(wl.sources, (wl.src, wl.dst, wl.w), source_weights=wl.source_w)
+    for v in (11, 19, 23):
+        engine.set_knob(1, v)
+        r = engine.mssp_trop(wl.sources, (wl.src, wl.dst, wl.w), source_weights=wl.source_w)
+        assert np.array_equal(base.src, r.src) and np.array_equal(base.dst, r.dst)
+        assert np.array_equal(base.w, r.w)
+    engine.set_knob(1, 0)
+    engine.set_plan(0)
