@@ -184,8 +184,8 @@ def cpu_sample(kind: str, wl, threads: int, steps: int):
                   f"{len(wl.sources)} sources on the full graph")
     elif kind == "tc":
         prog = O.tc_program(wl.src, wl.dst)
-        head, rounds = "path", 3
-        sample = "bootstrap plus the first 3 delta rounds of the closure on the full graph"
+        head, rounds = "path", 2
+        sample = "bootstrap plus the first 2 delta rounds of the closure on the full graph"
     else:
         lim = 1 << 17
         keep = (wl.src < lim) & (wl.dst < lim)

@@ -94,11 +94,14 @@ strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan);
 /* Tuning knobs (speed only; results are identical for every value):
  *   STRATA_KNOB_SORT_ITEMS_U32  keys per thread of a radix tile, u32 keys: 11, 15, 19, 23
  *   STRATA_KNOB_SORT_ITEMS_U64  keys per thread of a radix tile, u64 keys: 7, 9, 13
- * value 0 restores the default (15 / 9).  Other values: STRATA_E_INVALID.
+ *   STRATA_KNOB_TRI_PROBE       triangle membership test: 1 shared-memory hash set,
+ *                               2 binary search of the sorted out-list
+ * value 0 restores the default (15 / 9 / 1).  Other values: STRATA_E_INVALID.
  * The autotuner (strata_b200.tune) sweeps these and caches the best per GPU.
  * No counterpart in the reference (its sort has no tile parameters). */
 #define STRATA_KNOB_SORT_ITEMS_U32 1
 #define STRATA_KNOB_SORT_ITEMS_U64 2
+#define STRATA_KNOB_TRI_PROBE 3
 strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value);
 /* Enable per-phase CUDA-event timing in strata_fix_stats (adds event records). */
 strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled);

@@ -186,8 +186,13 @@ strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan) {
 
 strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value) {
   if (!ctx) return STRATA_E_INVALID;
+  if (knob == STRATA_KNOB_TRI_PROBE) {
+    if (value < 0 || value > 2) return bad(ctx, "triangle probe must be 0 (default), 1 (hash set) or 2 (binary search)");
+    ctx->tune_tri_probe = value;
+    return STRATA_OK;
+  }
   if (knob != STRATA_KNOB_SORT_ITEMS_U32 && knob != STRATA_KNOB_SORT_ITEMS_U64)
-    return bad(ctx, "unknown knob (1 = radix keys/thread for u32 keys, 2 = for u64 keys)");
+    return bad(ctx, "unknown knob (1 = radix keys/thread for u32 keys, 2 = for u64 keys, 3 = triangle probe)");
   const int kb = knob == STRATA_KNOB_SORT_ITEMS_U32 ? 4 : 8;
   if (value != 0) {
     int c[8];

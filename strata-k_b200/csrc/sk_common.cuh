@@ -79,6 +79,7 @@ struct strata_ctx {
   int plan = 0;                     // 0 auto, 1 sort-merge, 2 direct-addressed
   int tune_items4 = 0;              // radix keys per thread, u32 keys (0 = default)
   int tune_items8 = 0;              // radix keys per thread, u64 keys (0 = default)
+  int tune_tri_probe = 0;           // triangle membership test: 0/1 hash set, 2 binary search
   bool profiling = false;
   uint64_t launches = 0;
   // Per-kernel CUDA-event accounting (enabled with profiling).

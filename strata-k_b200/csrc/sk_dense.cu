@@ -64,7 +64,12 @@ __device__ __forceinline__ uint64_t dense_index(uint64_t key, const DenseLayout&
 // Grouped expand.  pos[] comes from expand_offsets in grouped mode: only the
 // head of each group (a run of equal join value, split at multiples of
 // kGroupMax) carries the degree of its join value, so one expand output is
-// one (group, edge) pair; the thread applies that edge to every member.
+// one (group, edge) pair.  A warp takes 32 consecutive outputs (one per
+// lane), flattens their (edge, member) candidates with a warp prefix sum over
+// the group sizes and processes them 32 at a time: lanes that share an edge
+// handle consecutive members of its group, whose index entries are adjacent
+// in one index row, so a warp's probes and atomics touch one or two cache
+// lines instead of 32.
 template <class K, bool TROP>
 __global__ void __launch_bounds__(NT, 6)
     k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n,
@@ -77,11 +82,13 @@ __global__ void __launch_bounds__(NT, 6)
   //   s_pos   int32  pos of each local item relative to the tile's first output
   //   s_seg   u32    CSR segment start of each local item
   //   s_owner u16    local owner item of each output of the tile
+  //   s_g     u8     group size of each local head item (members incl. the head)
   extern __shared__ __align__(16) unsigned char s_raw[];
   int32_t* s_pos = reinterpret_cast<int32_t*>(s_raw);
   uint32_t* s_seg = reinterpret_cast<uint32_t*>(s_pos + DE_TILE + 1);
   uint16_t* s_owner = reinterpret_cast<uint16_t*>(s_seg + DE_TILE + 1);
-  const int tid = threadIdx.x;
+  uint8_t* s_g = reinterpret_cast<uint8_t*>(s_owner + DE_TILE);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t L = n + total;
   const uint64_t d0 = (uint64_t)blockIdx.x * DE_TILE;
   const uint64_t d1 = d0 + DE_TILE < L ? d0 + DE_TILE : L;
@@ -100,6 +107,16 @@ __global__ void __launch_bounds__(NT, 6)
     if (rel < INT32_MIN || rel > INT32_MAX) atomicOr(status, ST_BOUNDS);
     s_pos[k] = (int32_t)rel;
     s_seg[k] = jv < n_nodes ? off[jv] : 0u;
+    // Group size: the head and the following items with its join value, up
+    // to the next multiple of kGroupMax (non-heads own no outputs).
+    const bool head = (i % kGroupMax) == 0 || (((uint64_t)dkeys[i - 1] >> jshift) & jmask) != jv;
+    uint32_t g = 0;
+    if (head) {
+      const uint64_t lim = min(n - i, (uint64_t)(kGroupMax - i % kGroupMax));
+      g = 1;
+      while (g < lim && (((uint64_t)dkeys[i + g] >> jshift) & jmask) == jv) g++;
+    }
+    s_g[k] = (uint8_t)g;
   }
   __syncthreads();
   uint32_t flags = 0;
@@ -130,61 +147,71 @@ __global__ void __launch_bounds__(NT, 6)
   }
   __syncthreads();
   const uint64_t o_end = o1 < total ? o1 : total;
-  for (uint64_t o = o0 + tid; o < o_end; o += NT) {
-    const uint32_t li = s_owner[o - o0];
-    const uint64_t e = (uint64_t)((int64_t)s_seg[li] + ((int64_t)(o - o0) - s_pos[li]));
-    if (li >= cnt || e >= n_nbr) {
-      flags |= ST_BOUNDS;
-      continue;
-    }
-    const uint32_t v = nbr[e];
+  for (uint64_t c = o0 + (uint64_t)warp * 32; c < o_end; c += NT) {
+    const uint64_t o = c + lane;
+    uint32_t g = 0, v = 0;
     int32_t ew = 0;
-    if constexpr (TROP) ew = nbr_w[e];
-    // group members: the head and the following items with its join value,
-    // up to the next multiple of kGroupMax
-    const uint64_t h = a + li;
-    const uint64_t jh = ((uint64_t)dkeys[h] >> jshift) & jmask;
-    const uint64_t g_end = min(n, (h / kGroupMax + 1) * kGroupMax);
-    // Members four at a time so their index probes are in flight together.
-    constexpr int MU = 4;
-    bool more = true;
-    for (uint64_t m0 = h; more && m0 < g_end; m0 += MU) {
-      uint64_t ix[MU];
-      int32_t cw[MU], cur[MU];
-      bool ok[MU];
+    uint64_t h = 0;
+    if (o < o_end) {
+      const uint32_t li = s_owner[o - o0];
+      const uint64_t e = (uint64_t)((int64_t)s_seg[li] + ((int64_t)(o - o0) - s_pos[li]));
+      if (li >= cnt || e >= n_nbr) {
+        flags |= ST_BOUNDS;
+      } else {
+        v = nbr[e];
+        if constexpr (TROP) ew = nbr_w[e];
+        g = s_g[li];
+        h = a + li;
+      }
+    }
+    const uint32_t incl = warp_incl_sum(g);
+    const uint32_t ex = incl - g;
+    const uint32_t T = __shfl_sync(kFull, incl, 31);
+    // Candidates j = 0..T-1 of this chunk: owner lane t (first lane whose
+    // inclusive count exceeds j), member h_t + (j - ex_t), edge v_t.
+    for (uint32_t b0 = 0; b0 < T; b0 += 64) {
+      uint64_t ix[2];
+      int32_t cw[2], cur[2];
+      bool ok[2];
 #pragma unroll
-      for (int u = 0; u < MU; u++) {
-        const uint64_t m = m0 + u;
-        ok[u] = more && m < g_end;
-        cw[u] = 0;
+      for (int u = 0; u < 2; u++) {
+        const uint32_t j = b0 + 32 * u + lane;
+        int t = 0;
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1) {
+          const uint32_t val = __shfl_sync(kFull, incl, t + st - 1);
+          if (val <= j) t += st;
+        }
+        const uint32_t ex_t = __shfl_sync(kFull, ex, t);
+        const uint64_t h_t = __shfl_sync(kFull, h, t);
+        const uint32_t v_t = __shfl_sync(kFull, v, t);
+        const int32_t ew_t = __shfl_sync(kFull, ew, t);
+        ok[u] = j < T;
         ix[u] = 0;
+        cw[u] = 0;
         if (ok[u]) {
+          const uint64_t m = h_t + (j - ex_t);
           const K mk = dkeys[m];
-          if (m != h && (((uint64_t)mk >> jshift) & jmask) != jh) {
+          const uint32_t kept = (uint32_t)(((uint64_t)mk >> pshift) & pmask);
+          const K key = (K)(((K)kept << out_pshift) | ((K)v_t << out_vshift));
+          ix[u] = dense_index((uint64_t)key, lay);
+          if (ix[u] >= lay.entries) {
+            flags |= ST_BOUNDS;
             ok[u] = false;
-            more = false;  // the run ended
-          } else {
-            const uint32_t kept = (uint32_t)(((uint64_t)mk >> pshift) & pmask);
-            const K key = (K)(((K)kept << out_pshift) | ((K)v << out_vshift));
-            ix[u] = dense_index((uint64_t)key, lay);
-            if (ix[u] >= lay.entries) {
-              flags |= ST_BOUNDS;
-              ok[u] = false;
-            } else if constexpr (TROP) {
-              cw[u] = trop_mul(dw[m], ew, &flags);
-            }
+          } else if constexpr (TROP) {
+            cw[u] = trop_mul(dw[m], ew_t, &flags);
           }
         }
       }
 #pragma unroll
-      for (int u = 0; u < MU; u++) {
+      for (int u = 0; u < 2; u++) {
         if (ok[u]) {
           if constexpr (TROP) cur[u] = D[ix[u]];
           else cur[u] = (int32_t)bits[ix[u] >> 5];
         }
       }
 #pragma unroll
-      for (int u = 0; u < MU; u++) {
+      for (int u = 0; u < 2; u++) {
         if (!ok[u]) continue;
         const uint32_t bit = 1u << (ix[u] & 31);
         if constexpr (TROP) {
@@ -389,7 +416,7 @@ __global__ void __launch_bounds__(NT)
 
 inline unsigned grid1(uint64_t n) { return (unsigned)ceil_div(n ? n : 1, NT); }
 
-size_t dense_expand_smem() { return (DE_TILE + 1) * (4 + 4) + DE_TILE * 2 + 16; }
+size_t dense_expand_smem() { return (DE_TILE + 1) * (4 + 4) + DE_TILE * 2 + (DE_TILE + 1) + 16; }
 
 }  // namespace
 

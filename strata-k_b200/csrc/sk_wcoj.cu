@@ -82,6 +82,92 @@ __global__ void __launch_bounds__(TC_NT)
   if (lane == 0 && count) atomicAdd(total, count);
 }
 
+// Hash-probe variant: the warp builds an open-addressing set of out(X) in
+// its shared-memory table (size the next power of two >= 2·d+(X), at most
+// TH_TAB, so at least half the slots stay empty and every probe chain ends at
+// an empty slot), then streams the successor lists of Y ∈ out(X) exactly as
+// above and answers each membership test with ~1-2 table reads instead of a
+// ~log2(d+(X))-step binary search.  A vertex whose out-list does not fit
+// falls back to the binary search over its list in global memory.
+constexpr uint32_t TH_TAB = 2048;
+constexpr uint32_t kEmpty = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t tri_hash(uint32_t z, int lg) { return (z * 0x9E3779B1u) >> (32 - lg); }
+
+__global__ void __launch_bounds__(TC_NT)
+    k_tri_count_hash(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr, uint64_t n_nodes,
+                     uint32_t* counter, unsigned long long* total) {
+  extern __shared__ __align__(16) uint32_t s_tab[];  // TC_WARPS * TH_TAB
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t* tab = s_tab + warp * TH_TAB;
+  unsigned long long count = 0;
+  while (true) {
+    uint32_t u = 0;
+    if (lane == 0) u = atomicAdd(counter, 1u);
+    u = __shfl_sync(kFull, u, 0);
+    if (u >= n_nodes) break;
+    const uint32_t a0 = off[u], du = off[u + 1] - a0;
+    if (du == 0) continue;
+    const bool hashed = du <= TH_TAB / 2;
+    int lg = 5;
+    while (hashed && (1u << lg) < 2 * du) lg++;
+    const uint32_t tmask = (1u << lg) - 1;
+    if (hashed) {
+      for (uint32_t k = lane; k <= tmask; k += 32) tab[k] = kEmpty;
+      __syncwarp();
+      for (uint32_t k = lane; k < du; k += 32) {
+        const uint32_t z = nbr[a0 + k];
+        uint32_t slot = tri_hash(z, lg);
+        // at most tmask+1 steps: the table is at most half full
+        for (uint32_t step = 0; step <= tmask; step++) {
+          const uint32_t prev = atomicCAS(&tab[slot], kEmpty, z);
+          if (prev == kEmpty || prev == z) break;
+          slot = (slot + 1) & tmask;
+        }
+      }
+      __syncwarp();
+    }
+    for (uint32_t c = 0; c < du; c += 32) {
+      const uint32_t i = c + lane;
+      const bool valid = i < du;
+      const uint32_t v = valid ? nbr[a0 + i] : 0u;
+      const uint32_t dv = (valid && v < n_nodes) ? off[v + 1] - off[v] : 0u;
+      const uint32_t sv = (valid && v < n_nodes) ? off[v] : 0u;
+      const uint32_t incl = warp_incl_sum(dv);
+      const uint32_t ex = incl - dv;
+      const uint32_t D = __shfl_sync(kFull, incl, 31);
+      for (uint32_t base = 0; base < D; base += 32) {
+        const uint32_t j = base + lane;
+        int t = 0;
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1) {
+          const uint32_t val = __shfl_sync(kFull, incl, t + st - 1);
+          if (val <= j) t += st;
+        }
+        const uint32_t ex_t = __shfl_sync(kFull, ex, t);
+        const uint32_t sv_t = __shfl_sync(kFull, sv, t);
+        if (j < D) {
+          const uint32_t w = nbr[sv_t + (j - ex_t)];
+          if (hashed) {
+            uint32_t slot = tri_hash(w, lg);
+            for (uint32_t step = 0; step <= tmask; step++) {
+              const uint32_t x = tab[slot];
+              if (x == w) { count++; break; }
+              if (x == kEmpty) break;
+              slot = (slot + 1) & tmask;
+            }
+          } else if (bsearch_u32(nbr + a0, du, w)) {
+            count++;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  count = warp_sum(count);
+  if (lane == 0 && count) atomicAdd(total, count);
+}
+
 // K4 on a degree-oriented DAG: one thread per oriented edge (u, v); for each
 // common successor w1 count |out(u) ∩ out(v) ∩ out(w1)| by a 3-way leapfrog.
 // The lists are sorted by id while the DAG follows (degree, id) rank, so the
@@ -197,6 +283,22 @@ __global__ void k_intern_map(const uint64_t* __restrict__ keys, uint64_t n, cons
 
 inline unsigned blocks(uint64_t n, int nt = 256) { return (unsigned)ceil_div(n ? n : 1, nt); }
 
+// Σ over oriented edges (u, v) of d+(u) + d+(v): the successor-list entries
+// the triangle count streams (its algorithmic bytes; profiling only).
+template <class K>
+__global__ void k_tri_list_sum(const K* __restrict__ keys, uint64_t m, int bits, const uint32_t* __restrict__ off,
+                               uint64_t n_nodes, unsigned long long* out) {
+  unsigned long long s = 0;
+  const K mask = (K)((K(1) << bits) - 1);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t u = (uint64_t)(keys[i] >> bits), v = (uint64_t)(keys[i] & mask);
+    if (u < n_nodes) s += off[u + 1] - off[u];
+    if (v < n_nodes) s += off[v + 1] - off[v];
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
+}
+
 // Sort + dedup packed keys in `keys` (n), result in out (returns count).
 template <class K>
 uint64_t sort_unique(strata_ctx* ctx, DBuf<K>& keys, uint64_t n, int bits, DBuf<K>& out) {
@@ -219,22 +321,35 @@ template <class K>
 uint64_t tri_from_sorted(strata_ctx* ctx, const K* keys, uint64_t m, int bits, uint64_t n_nodes) {
   DBuf<uint32_t> off(ctx, n_nodes + 1), nbr(ctx, m + 1);
   build_csr<K>(ctx, keys, m, bits, n_nodes, off.p, nbr.p);
-  DBuf<uint64_t> acc(ctx, 2);
-  SK_CUDA(cudaMemsetAsync(acc.p, 0, 16, ctx->stream));
+  DBuf<uint64_t> acc(ctx, 3);  // count, vertex counter, list-entry sum
+  SK_CUDA(cudaMemsetAsync(acc.p, 0, 24, ctx->stream));
   const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(n_nodes, TC_WARPS), (uint64_t)ctx->num_sms * 8);
   const int kh = kprof_begin(ctx, K_TRI_COUNT);
-  k_tri_count<<<grid ? grid : 1, TC_NT, 0, ctx->stream>>>(off.p, nbr.p, n_nodes,
-                                                          reinterpret_cast<uint32_t*>(acc.p + 1),
-                                                          reinterpret_cast<unsigned long long*>(acc.p));
+  if (ctx->tune_tri_probe == 2) {
+    k_tri_count<<<grid ? grid : 1, TC_NT, 0, ctx->stream>>>(off.p, nbr.p, n_nodes,
+                                                            reinterpret_cast<uint32_t*>(acc.p + 1),
+                                                            reinterpret_cast<unsigned long long*>(acc.p));
+  } else {
+    const size_t smem = (size_t)TC_WARPS * TH_TAB * sizeof(uint32_t);
+    SK_CUDA(cudaFuncSetAttribute(k_tri_count_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_tri_count_hash<<<grid ? grid : 1, TC_NT, smem, ctx->stream>>>(off.p, nbr.p, n_nodes,
+                                                                     reinterpret_cast<uint32_t*>(acc.p + 1),
+                                                                     reinterpret_cast<unsigned long long*>(acc.p));
+  }
   // Algorithmic bytes: every out-list once per incident oriented edge plus the
-  // edge list and offsets (4 B·Σ(d+(u)+d+(v)) + 8 B·M + 4 B·(N+1)), counted
-  // on the device below when profiling.
-  kprof_end(ctx, kh, 0);
+  // edge list and offsets, 4 B·Σ(d+(u)+d+(v)) + 8 B·M + 4 B·(N+1); the sum is
+  // counted on the device after the timed launch when profiling.
+  kprof_end(ctx, kh, 8 * m + 4 * (n_nodes + 1));
   after_launch(ctx, "k_tri_count");
-  uint64_t r;
-  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, acc.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->profiling && m) {
+    k_tri_list_sum<K><<<(unsigned)std::min<uint64_t>(blocks(m), (uint64_t)ctx->num_sms * 8), 256, 0, ctx->stream>>>(
+        keys, m, bits, off.p, n_nodes, reinterpret_cast<unsigned long long*>(acc.p + 2));
+    after_launch(ctx, "k_tri_list_sum");
+  }
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, acc.p, 24, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
-  r = ctx->h_scalar[0];
+  const uint64_t r = ctx->h_scalar[0];
+  if (ctx->profiling) kprof_add_last(ctx, K_TRI_COUNT, 4 * ctx->h_scalar[2]);
   kprof_collect(ctx);
   return r;
 }

@@ -27,7 +27,7 @@ E_NOT_BUILT = 8
 E_WEIGHT_RANGE = 9
 
 PLAN_AUTO, PLAN_SORT_MERGE, PLAN_DENSE = 0, 1, 2
-KNOB_SORT_ITEMS_U32, KNOB_SORT_ITEMS_U64 = 1, 2
+KNOB_SORT_ITEMS_U32, KNOB_SORT_ITEMS_U64, KNOB_TRI_PROBE = 1, 2, 3
 
 KERNELS = {0: "k_onesweep", 1: "k_expand_emit", 2: "k_expand_offsets", 3: "k_reduce_runs",
            4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count", 7: "k_expand_dense"}

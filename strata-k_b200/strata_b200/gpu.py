@@ -219,7 +219,8 @@ class Engine:
         self._check(self.lib.strata_ctx_set_plan(self.ctx, plan))
 
     def set_knob(self, knob: int, value: int):
-        """Tuning knob (1: radix keys/thread for u32 keys, 2: for u64 keys; 0 = default)."""
+        """Tuning knob (1: radix keys/thread for u32 keys, 2: for u64 keys, 3: triangle
+        probe 1 hash / 2 binary search; 0 = default).  Results never depend on knobs."""
         self._check(self.lib.strata_ctx_set_knob(self.ctx, knob, value))
 
     def set_profiling(self, on: bool):

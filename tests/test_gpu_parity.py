@@ -279,6 +279,29 @@ def test_triangle_pattern_rmat_oriented(engine):
     assert engine.count_triangles((wl.src, wl.dst)) == want
 
 
+@pytest.mark.parametrize("probe", [1, 2])
+def test_triangle_probe_knob(engine, probe):
+    """Both membership tests (shared-memory hash set, binary search) give the
+    oracle's count, including a vertex whose out-list exceeds the hash table
+    (it falls back to the binary search) and R-MAT skew."""
+    engine.set_knob(3, probe)
+    try:
+        big = 3000  # X=0 -> 1..3000, i -> i+1: 2999 triangles through the wide vertex
+        x = np.concatenate([np.zeros(big, np.int64), np.arange(1, big)])
+        y = np.concatenate([np.arange(1, big + 1), np.arange(2, big + 1)])
+        assert engine.count_triangle_pattern((x, y)) == O.count_pattern(x, y) == big - 1
+        wl = gen.triangle_workload(scale=13, edge_factor=16, seed=4)
+        assert engine.count_triangle_pattern((wl.src, wl.dst)) == O.count_pattern(wl.src, wl.dst)
+        rng = np.random.default_rng(probe)
+        for _ in range(10):
+            n = int(rng.integers(5, 2000))
+            m = int(rng.integers(1, 20 * n))
+            a, b = rng.integers(0, n, m), rng.integers(0, n, m)
+            assert engine.count_triangle_pattern((a, b)) == O.count_pattern(a, b)
+    finally:
+        engine.set_knob(3, 0)
+
+
 def test_hub_graph_closed_form(engine):
     h, b = 16, 20000
     e = [(i, j) for i in range(h) for j in range(i + 1, h)]
