@@ -47,8 +47,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["mssp", "tc", "tri"], default="mssp",
-                    help="mssp: the headline Trop program; tc / tri: the Bool closure and triangle-count configs")
+    ap.add_argument("--workload", choices=["mssp", "tc", "tri", "batch"], default="mssp",
+                    help="mssp: the headline Trop program; tc / tri / batch: the Bool closure, triangle-count "
+                         "and batched-reachability configs")
+    ap.add_argument("--instances", type=int, default=4096, help="batch: number of instances")
     ap.add_argument("--plan", choices=["auto", "sort-merge", "dense"], default="auto")
     ap.add_argument("--tuned", action="store_true", help="apply the autotuner's cached knob values")
     ap.add_argument("--scale", type=int, default=None, help="R-MAT scale (mssp: 20, tri: 22)")
@@ -76,6 +78,8 @@ def workload_for(rank: int, scale: int, n_sources: int, kind: str = "mssp"):
         return gen.tc_workload(seed=1 + 1000 * rank)
     if kind == "tri":
         return gen.triangle_workload(scale=scale, seed=3 + 1000 * rank)
+    if kind == "batch":
+        return gen.batch_tc_workload(n_inst=n_sources, seed=4 + 1000 * rank, workers=min(16, os.cpu_count() or 1))
     return gen.mssp_workload(scale=scale, n_sources=n_sources, seed=2 + 1000 * rank)
 
 
@@ -85,7 +89,8 @@ PLANS = {"auto": 0, "sort-merge": 1, "dense": 2}
 def metric_for(kind: str) -> str:
     return {"mssp": METRIC,
             "tc": "derived tuples/s (Bool transitive-closure fixpoint, |path| / device time)",
-            "tri": "derived tuples/s (WCOJ triangle pattern count, triangles / device time)"}[kind]
+            "tri": "derived tuples/s (WCOJ triangle pattern count, triangles / device time)",
+            "batch": "derived tuples/s (batched Bool reachability, sum of |path| over instances / device time)"}[kind]
 
 
 def config(args, world):
@@ -95,6 +100,12 @@ def config(args, world):
         return {"workload": "bool_tc_er_10000n_50000e",
                 "program": "path(X,Y) :- edge(X,Y). path(X,Z) :- edge(X,Y), path(Y,Z).",
                 "graph": "Erdos-Renyi directed, 10,000 nodes, 50,000 distinct edges, no self-loops", **common}
+    if args.workload == "batch":
+        return {"workload": f"batch_tc_{args.instances}x_er_n100_50000_deg2_8",
+                "program": "path(X,Y) :- edge(X,Y). path(X,Z) :- edge(X,Y), path(Y,Z). (per instance)",
+                "graph": f"{args.instances} directed ER instances, nodes log-uniform in [100, 50000], mean "
+                         "out-degree uniform in [2, 8], seeded per instance",
+                "instances": args.instances, **common}
     if args.workload == "tri":
         return {"workload": f"wcoj_triangles_rmat{args.scale}",
                 "program": "n(count<X>) :- e(X,Y), e(Y,Z), e(X,Z).",
@@ -186,6 +197,23 @@ def cpu_sample(kind: str, wl, threads: int, steps: int):
         prog = O.tc_program(wl.src, wl.dst)
         head, rounds = "path", 2
         sample = "bootstrap plus the first 2 delta rounds of the closure on the full graph"
+    elif kind == "batch":
+        # the interpreter on whole instances, smallest first, until ~10 s
+        t_tup, t_sec, k = 0, 0.0, 0
+        for i in np.argsort(wl.nodes, kind="stable"):
+            n, s_, d_ = wl.instance(int(i))
+            sess = O.Session(O.tc_program(s_, d_))
+            counts, _, secs = sess.run(threads=threads)
+            sess.close()
+            t_tup += counts["path"]
+            t_sec += secs
+            k += 1
+            if t_sec > 10.0 or k >= 256:
+                break
+        rate = t_tup / t_sec if t_sec > 0 else 0.0
+        sample = (f"the full semi-naive closure of the {k} smallest of {len(wl)} instances "
+                  f"(n <= {int(wl.nodes[np.argsort(wl.nodes, kind='stable')[k - 1]])})")
+        return [rate] * steps, [t_sec] * steps, t_tup, sample
     else:
         lim = 1 << 17
         keep = (wl.src < lim) & (wl.dst < lim)
@@ -209,7 +237,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     cores = os.cpu_count() or 1
-    wl = workload_for(0, args.scale, args.sources, args.workload)
+    wl = workload_for(0, args.scale, args.instances if args.workload == "batch" else args.sources, args.workload)
     t0 = time.time()
     rates, secs, tup, sample = cpu_sample(args.workload, wl, cores, args.warmup + args.steps)
     timed = secs[args.warmup:]
@@ -239,6 +267,7 @@ class Job:
     def __init__(self, kind, wl, eng, torch):
         self.kind, self.wl, self.eng, self.torch = kind, wl, eng, torch
         i32, i64 = np.int32, np.int64
+        self.mode = 0
         if kind == "mssp":
             cols = (("sources", wl.sources, i32), ("sw", wl.source_w, i64), ("src", wl.src, i32),
                     ("dst", wl.dst, i32), ("w", wl.w, i64))
@@ -246,7 +275,7 @@ class Job:
             cols = (("src", wl.src, i32), ("dst", wl.dst, i32))
         self.host = {k: torch.from_numpy(np.ascontiguousarray(v).astype(dt)).pin_memory() for k, v, dt in cols}
         self.entry = {"mssp": "strata_mssp_trop_dev", "tc": "strata_tc_bool_dev",
-                      "tri": "strata_count_triangle_pattern_dev"}[kind]
+                      "tri": "strata_count_triangle_pattern_dev", "batch": "strata_tc_bool_batch_dev"}[kind]
 
     def run(self, d):
         """One fixpoint on device columns `d`: returns (result handle, tuples, stats)."""
@@ -254,6 +283,9 @@ class Job:
             rel = self.eng.mssp_dev(d["sources"], d["src"], d["dst"], d["w"], source_weights=d["sw"])
         elif self.kind == "tc":
             rel = self.eng.tc_bool_dev(d["src"], d["dst"])
+        elif self.kind == "batch":
+            res = self.eng.tc_bool_batch(self.wl.nodes, self.wl.edge_off, d["src"], d["dst"], mode=self.mode)
+            return None, int(res.counts.sum()), {"batch": res.stats}
         else:
             return None, self.eng.count_triangle_pattern_dev(d["src"], d["dst"]), None
         return rel, len(rel), rel.stats
@@ -265,7 +297,7 @@ class Job:
 
     def out_buffers(self, n):
         torch = self.torch
-        if self.kind == "tri":
+        if self.kind in ("tri", "batch"):
             return None
         trop = self.kind == "mssp"
         return (torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
@@ -277,6 +309,8 @@ class Job:
         """Result to the host; returns the bytes read back."""
         if self.kind == "tri":
             return 8  # the u64 count, returned through the entry point's out-parameter
+        if self.kind == "batch":
+            return len(self.wl) * (8 + 8 + 4)  # per-instance count, fingerprint, rounds
         res = handle.to_host(out=out)
         assert len(res) == tuples
         return tuples * (4 + 4 + (8 + 1 if self.kind == "mssp" else 0))
@@ -318,7 +352,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
-    wl = workload_for(rank, args.scale, args.sources, args.workload)
+    wl = workload_for(rank, args.scale, args.instances if args.workload == "batch" else args.sources, args.workload)
     eng = S.Engine(local, tuned=args.tuned)
     eng.set_plan(PLANS[args.plan])
     stream = torch.cuda.Stream()
@@ -352,7 +386,7 @@ def run_ours(args):
 
     # ---- the sort-merge plan on the same inputs (reported beside the headline)
     sort_plan = None
-    if not args.no_sort_plan and args.workload != "tri" and args.plan == "auto":
+    if not args.no_sort_plan and args.workload in ("mssp", "tc") and args.plan == "auto":
         eng.set_plan(PLANS["sort-merge"])
         job.free(step()[0])  # warm its buffers
         eng.set_profiling(True)
@@ -367,6 +401,18 @@ def run_ours(args):
                      "phase_ms": {k: round(sp_stats[k + "_ms"], 3)
                                   for k in ("setup", "join", "sort", "diff", "merge", "finish")},
                      "kernels": _kernels(sk)}
+    # ---- batched form: the same instances one per launch (host-driven rounds)
+    per_launch = None
+    if args.workload == "batch":
+        job.mode = 1
+        eng.set_profiling(False)
+        pl_ms, pl_tuples, pl_stats = _timed_steps(step, job.free, stream, flush, 1, torch)
+        job.mode = 0
+        assert pl_tuples == tuples
+        per_launch = {"mode": "one instance per launch, same kernels, host-driven rounds (1 step)",
+                      "ms_per_step": pl_ms, "value": pl_tuples / (pl_ms / 1000.0),
+                      "speedup_of_batched": pl_ms / (total_ms / args.steps),
+                      "round_launches": pl_stats["batch"]["round_launches"]}
     if pg:
         t = torch.tensor([total_ms, float(tuples)], dtype=torch.float64, device="cuda")
         mx = t.clone()
@@ -433,7 +479,7 @@ def run_ours(args):
                "sample": f"{sample}: {tup} tuples in {secs[-1]:.2f} s"}
 
     if rank == 0:
-        wb = stats["weight_bytes"] if stats else 0
+        wb = stats.get("weight_bytes", 0) if stats else 0
         line = {
             "metric": metric_for(args.workload), "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -443,9 +489,15 @@ def run_ours(args):
             "tuples_per_step": int(all_tuples),
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
         }
-        if stats:
+        if stats and "batch" in stats:
+            b = stats["batch"]
+            line.update({"dtype": "u32", "plan": "bit rows, batched waves",
+                         "batch": {k: b[k] for k in ("instances", "waves", "graph_launches", "round_launches",
+                                                     "rounds_max", "round_bytes")},
+                         "one_per_launch": per_launch})
+        elif stats:
             line.update({
-                "plan": {1: "sort-merge", 2: "direct-addressed"}.get(stats["plan"], "?"),
+                "plan": {1: "sort-merge", 2: "direct-addressed", 3: "bit rows"}.get(stats["plan"], "?"),
                 "rounds": stats["rounds"], "candidates_per_step": stats["candidates"],
                 "key_bits": stats["key_bits"], "weight_bytes": stats["weight_bytes"],
                 "phase_ms": {k: round(stats[k + "_ms"], 3)

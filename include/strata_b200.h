@@ -88,20 +88,31 @@ strata_status strata_ctx_mem(const strata_ctx* ctx, uint64_t* in_use, uint64_t* 
  * the two column domains multiply to a small enough index and the weights
  * fit int32, else sort-merge), 1 = sort-merge (radix sort + run reduction +
  * merge-path diff every round), 2 = direct-addressed (a bitmap / int32 index
- * over (c0, c1); STRATA_E_UNSUPPORTED when it does not apply).  Results are
- * identical; only speed and memory differ. */
+ * over (c0, c1); STRATA_E_UNSUPPORTED when it does not apply), 3 = bit rows
+ * (Bool transitive closure only: path and Δ as bit rows over the Z domain,
+ * one 128-bit OR joins 128 tuples; STRATA_E_UNSUPPORTED for other programs
+ * or when the three bit matrices exceed 8 GB).  Automatic planning picks bit
+ * rows for Bool closure when they fit.  Results are identical; only speed
+ * and memory differ. */
 strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan);
 /* Tuning knobs (speed only; results are identical for every value):
  *   STRATA_KNOB_SORT_ITEMS_U32  keys per thread of a radix tile, u32 keys: 11, 15, 19, 23
  *   STRATA_KNOB_SORT_ITEMS_U64  keys per thread of a radix tile, u64 keys: 7, 9, 13
  *   STRATA_KNOB_TRI_PROBE       triangle membership test: 1 shared-memory hash set,
  *                               2 binary search of the sorted out-list
- * value 0 restores the default (15 / 9 / 1).  Other values: STRATA_E_INVALID.
+ *   STRATA_KNOB_BATCH_GRAPH_ROUNDS  bit-row rounds per CUDA-graph replay: 2, 4, 8, 16, 32
+ *   STRATA_KNOB_BATCH_BLOCKS_PER_SM resident blocks per SM of the round kernel: 1..32
+ *   STRATA_KNOB_BATCH_BUDGET_MB     cap on one batch wave's device bytes, in MiB (>= 1)
+ * value 0 restores the default (15 / 9 / 2 / 8 / occupancy limit / 70% of
+ * free memory).  Other values: STRATA_E_INVALID.
  * The autotuner (strata_b200.tune) sweeps these and caches the best per GPU.
  * No counterpart in the reference (its sort has no tile parameters). */
 #define STRATA_KNOB_SORT_ITEMS_U32 1
 #define STRATA_KNOB_SORT_ITEMS_U64 2
 #define STRATA_KNOB_TRI_PROBE 3
+#define STRATA_KNOB_BATCH_GRAPH_ROUNDS 4
+#define STRATA_KNOB_BATCH_BLOCKS_PER_SM 5
+#define STRATA_KNOB_BATCH_BUDGET_MB 6
 strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value);
 /* Enable per-phase CUDA-event timing in strata_fix_stats (adds event records). */
 strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled);
@@ -196,6 +207,42 @@ strata_status strata_mssp_trop_dev(strata_ctx* ctx,
     uint64_t n_edges, strata_rel** out, strata_fix_stats* stats);
 strata_status strata_count_triangle_pattern_dev(strata_ctx* ctx,
     const uint32_t* d_x, const uint32_t* d_y, uint64_t n_edges, uint64_t* out_count);
+
+/* ---- batched Bool reachability ------------------------------------------
+ * Many independent transitive closures in one call (the reference computes
+ * one graph per `transitive_closure_bool` call, strata-gpu/src/lib.rs:67 and
+ * tc.rs:31; this is its batched submission).  Instance i has nodes
+ * [0, nodes[i]) and the edges src/dst[edge_off[i] .. edge_off[i+1]) (local
+ * ids; duplicates allowed).  Each closure is summarised, not materialised:
+ *   counts[i] = |path_i|,
+ *   fps[i]    = Σ_{(X,Z) ∈ path_i} mix64(X) · c^Z  mod 2^64,
+ *               mix64 = the splitmix64 finalizer, c = 0x9E3779B97F4A7C15,
+ *   rounds[i] = semi-naive delta rounds (as strata_fix_stats.rounds).
+ * mode 0: batched — instances are packed into memory-bounded waves and each
+ *         semi-naive round of a wave is one persistent kernel over all of its
+ *         active instances, replayed from a captured CUDA graph;
+ * mode 1: one instance per launch — the same kernels, one instance at a time
+ *         with host-driven rounds (the comparison baseline).
+ * nodes / edge_off / outputs are host arrays; src / dst are device arrays
+ * (`_dev`) or host arrays (plain form). */
+typedef struct strata_batch_stats {
+  uint64_t instances;
+  uint64_t waves;           /* memory-bounded groups of instances */
+  uint64_t graph_launches;  /* CUDA-graph replays (mode 0) */
+  uint64_t round_launches;  /* round kernels launched (graph nodes included) */
+  uint64_t rounds_max;      /* most rounds of any instance */
+  uint64_t result_tuples;   /* Σ counts */
+  uint64_t round_bytes;     /* algorithmic bytes of the rounds (profiling on) */
+  uint64_t launches;        /* kernels launched by the call */
+  double   device_ms;       /* CUDA-event time of the whole call */
+} strata_batch_stats;
+
+strata_status strata_tc_bool_batch_dev(strata_ctx* ctx, uint32_t n_inst, const uint32_t* nodes,
+    const uint64_t* edge_off, const uint32_t* d_src, const uint32_t* d_dst, int mode,
+    uint64_t* counts, uint64_t* fps, uint32_t* rounds, strata_batch_stats* stats);
+strata_status strata_tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint32_t* nodes,
+    const uint64_t* edge_off, const uint32_t* src, const uint32_t* dst, int mode,
+    uint64_t* counts, uint64_t* fps, uint32_t* rounds, strata_batch_stats* stats);
 
 /* Relation handle accessors. */
 strata_status strata_rel_size(const strata_rel* rel, uint64_t* n);

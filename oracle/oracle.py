@@ -80,6 +80,25 @@ def lib() -> C.CDLL:
         L.sko_brute_triangles.argtypes = [u32p, u32p, C.c_size_t, C.c_uint32]
         L.sko_brute_4cliques.restype = C.c_uint64
         L.sko_brute_4cliques.argtypes = [u32p, u32p, C.c_size_t, C.c_uint32]
+        L.sko_prov_run.restype = C.c_void_p
+        L.sko_prov_run.argtypes = [i64p, C.c_size_t, C.POINTER(C.c_double), C.c_size_t, i64p, C.c_size_t,
+                                   C.POINTER(C.c_long), C.POINTER(C.c_int)]
+        L.sko_prov_free.argtypes = [C.c_void_p]
+        L.sko_prov_proofs.restype = C.c_long
+        L.sko_prov_proofs.argtypes = [C.c_void_p, C.c_int, i64p, C.c_int, i64p, C.c_size_t]
+        L.sko_prov_relation.restype = C.c_long
+        L.sko_prov_relation.argtypes = [C.c_void_p, C.c_int, i64p, C.c_size_t]
+        L.sko_compile_grad.restype = C.c_int
+        L.sko_compile_grad.argtypes = [i64p, C.c_size_t, C.POINTER(C.c_double), C.c_size_t,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double), i64p]
+        L.sko_prov_tc.restype = C.c_long
+        L.sko_prov_tc.argtypes = [C.c_uint32, u32p, u32p, C.c_size_t, C.POINTER(C.c_double), C.c_size_t,
+                                  u32p, C.c_size_t, u32p, u32p, C.c_size_t, C.c_int, i64p, C.c_size_t,
+                                  i64p, C.POINTER(C.c_long), C.POINTER(C.c_size_t)]
+        L.sko_closure_count_fp.restype = C.c_int
+        L.sko_closure_count_fp.argtypes = [C.c_uint32, u32p, u32p, C.c_uint64, u64p, u64p]
+        L.sko_closure_batch.restype = C.c_int
+        L.sko_closure_batch.argtypes = [C.c_uint32, u32p, u64p, u32p, u32p, C.c_int, u64p, u64p]
         _lib = L
     return _lib
 
@@ -90,6 +109,9 @@ def _p(a, t):
 
 def _col(a, dt):
     return np.ascontiguousarray(np.asarray(a), dtype=dt)
+
+
+PROB = object()  # weight marker of a probabilistic (leaf) fact: proof {+(i+1)}
 
 
 class OracleError(Exception):
@@ -206,7 +228,9 @@ class Prog:
                 for c in range(ar):
                     blk[:, 2 + 2 * c] = 0
                     blk[:, 3 + 2 * c] = np.asarray(cols[c], dtype=np.int64)
-                if weights is None:
+                if weights is PROB:
+                    blk[:, -2] = 3
+                elif weights is None:
                     blk[:, -2] = 0
                 else:
                     infm = np.zeros(n, bool) if inf is None else np.asarray(inf).astype(bool)
@@ -224,6 +248,8 @@ class Prog:
                         rec += [0, int(v)]
                 if weight is None:
                     rec += [0, 0]
+                elif weight is PROB:
+                    rec += [3, 0]
                 elif weight == POS_INF:
                     rec += [2, 0]
                 else:
@@ -397,6 +423,185 @@ def fingerprint(src, dst, w=None, inf=None) -> int:
         wp = _p(keep[-1], C.c_int64)
     return int(L.sko_fingerprint(_p(s, C.c_uint32), _p(d, C.c_uint32), wp,
                                  None if ia is None else _p(ia, C.c_uint8), len(s)))
+
+
+POLY_C = 0x9E3779B97F4A7C15
+
+
+def mix64_np(x) -> np.ndarray:
+    """splitmix64 finalizer on uint64 arrays (wrapping arithmetic)."""
+    z = np.asarray(x, np.uint64) + np.uint64(0x9E3779B97F4A7C15)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def poly_fingerprint(x, z, n: int) -> int:
+    """Σ mix64(X) · c^Z mod 2^64 over tuples (X, Z) with Z < n — the batched
+    reachability summary, computed directly from tuples."""
+    x = np.asarray(x, np.uint64)
+    z = np.asarray(z, np.int64)
+    pw = np.ones(max(n, 1), np.uint64)
+    with np.errstate(over="ignore"):
+        for k in range(1, n):
+            pw[k] = pw[k - 1] * np.uint64(POLY_C)
+        return int((mix64_np(x) * pw[z]).sum(dtype=np.uint64)) if len(x) else 0
+
+
+def closure_count_fp(n, src, dst) -> tuple[int, int]:
+    """|path| and the row-polynomial fingerprint of path = closure(edge) on
+    nodes [0, n) (SCC + DAG oracle)."""
+    s, d = _col(src, np.uint32), _col(dst, np.uint32)
+    c, f = C.c_uint64(), C.c_uint64()
+    rc = lib().sko_closure_count_fp(n, _p(s, C.c_uint32), _p(d, C.c_uint32), len(s), C.byref(c), C.byref(f))
+    if rc:
+        raise ValueError("edge endpoint outside [0, n)")
+    return int(c.value), int(f.value)
+
+
+def closure_batch(nodes, edge_off, src, dst, threads=8) -> tuple[np.ndarray, np.ndarray]:
+    """Per-instance (count, fingerprint) of a batch (see closure_count_fp)."""
+    nd = _col(nodes, np.uint32)
+    eo = _col(edge_off, np.uint64)
+    s, d = _col(src, np.uint32), _col(dst, np.uint32)
+    counts = np.zeros(len(nd), np.uint64)
+    fps = np.zeros(len(nd), np.uint64)
+    rc = lib().sko_closure_batch(len(nd), _p(nd, C.c_uint32), _p(eo, C.c_uint64), _p(s, C.c_uint32),
+                                 _p(d, C.c_uint32), threads, _p(counts, C.c_uint64), _p(fps, C.c_uint64))
+    if rc:
+        raise ValueError("edge endpoint outside its instance's node range")
+    return counts, fps
+
+
+# ---------------------------------------------------------------------------
+# A'. provenance capture, exact compilation, WMC and gradients (FP64)
+# ---------------------------------------------------------------------------
+PROV_ERRS = {20: "NotBool", 21: "BadProbability", 22: "ProofBudget", 23: "SoftAggregate",
+             24: "CircuitBudget"}
+
+
+class ProvError(Exception):
+    def __init__(self, code: int):
+        super().__init__(PROV_ERRS.get(code, ERR_NAMES.get(code, str(code))))
+        self.code = code
+
+
+def _deser(buf, i=0):
+    """[n, (len, lits...)*] -> (list of proofs, next index)."""
+    n = int(buf[i]); i += 1
+    out = []
+    for _ in range(n):
+        ln = int(buf[i]); i += 1
+        out.append([int(x) for x in buf[i:i + ln]]); i += ln
+    return out, i
+
+
+def _ser(proofs) -> np.ndarray:
+    out = [len(proofs)]
+    for p in proofs:
+        out.append(len(p))
+        out += [int(x) for x in p]
+    return np.asarray(out, np.int64)
+
+
+class ProvDb:
+    """The saturated provenance database of a program (run_prov)."""
+
+    def __init__(self, prog: "Prog", probs, modes: dict | None = None, max_proofs: int = 10_000):
+        L = lib()
+        self.prog = prog
+        self.probs = np.ascontiguousarray(probs, np.float64)
+        m = np.zeros(len(prog.preds), np.int64)
+        for name, k in (modes or {}).items():
+            m[prog._pi(name)] = int(k)
+        b = prog.blob()
+        err, rounds = C.c_int(), C.c_long()
+        self.h = L.sko_prov_run(_p(b, C.c_int64), len(b), _p(self.probs, C.c_double), len(self.probs),
+                                _p(m, C.c_int64), max_proofs, C.byref(rounds), C.byref(err))
+        if not self.h:
+            raise ProvError(err.value)
+        self.rounds = rounds.value
+
+    def proofs(self, pred: str, values) -> list | None:
+        vals = []
+        for v in values:
+            vals += [1, int(v[1])] if isinstance(v, tuple) and v[0] == "i" else [0, int(v)]
+        va = np.asarray(vals, np.int64)
+        cap = 1 << 16
+        while True:
+            buf = np.zeros(cap, np.int64)
+            n = lib().sko_prov_proofs(self.h, self.prog._pi(pred), _p(va, C.c_int64), len(values),
+                                      _p(buf, C.c_int64), cap)
+            if n < 0:
+                return None
+            if n <= cap:
+                return _deser(buf)[0]
+            cap = n
+
+    def relation(self, pred: str) -> dict:
+        cap = 1 << 20
+        while True:
+            buf = np.zeros(cap, np.int64)
+            n = lib().sko_prov_relation(self.h, self.prog._pi(pred), _p(buf, C.c_int64), cap)
+            if n <= cap:
+                break
+            cap = n
+        ar = self.prog.preds[self.prog._pi(pred)][1]
+        cnt, i = int(buf[0]), 1
+        out = {}
+        for _ in range(cnt):
+            t = tuple(int(buf[i + 2 * c + 1]) for c in range(ar))
+            i += 2 * ar
+            ps, i = _deser(buf, i)
+            out[t] = ps
+        return out
+
+    def close(self):
+        if self.h:
+            lib().sko_prov_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def compile_grad(proofs, probs, max_nodes: int = 1 << 20):
+    """compile_exact + Circuit::grad (FP64): (P, dP/dp over every leaf, nodes)."""
+    pr = np.ascontiguousarray(probs, np.float64)
+    ser = _ser(proofs)
+    pv, g, nn = C.c_double(), np.zeros(len(pr), np.float64), C.c_int64()
+    rc = lib().sko_compile_grad(_p(ser, C.c_int64), len(pr), _p(pr, C.c_double), max_nodes, C.byref(pv),
+                                _p(g, C.c_double), C.byref(nn))
+    if rc:
+        raise ProvError(rc)
+    return pv.value, g, int(nn.value)
+
+
+def prov_tc(n, src, dst, probs, k, qs, qt, threads=8):
+    """Prov_k capture of path(X,Y) :- edge(X,Y). path(X,Z) :- edge(X,Y), path(Y,Z).
+    restricted to the queried targets; returns ([proofs per query], {target: rounds})."""
+    s, d = _col(src, np.uint32), _col(dst, np.uint32)
+    pr = np.ascontiguousarray(probs, np.float64)
+    qs_, qt_ = _col(qs, np.uint32), _col(qt, np.uint32)
+    targets = np.unique(qt_).astype(np.uint32)
+    rounds = (C.c_long * max(1, len(targets)))()
+    q_off = np.zeros(len(qs_) + 1, np.int64)
+    need = C.c_size_t()
+    cap = max(1024, 64 * len(qs_))
+    while True:
+        buf = np.zeros(cap, np.int64)
+        rc = lib().sko_prov_tc(n, _p(s, C.c_uint32), _p(d, C.c_uint32), len(s), _p(pr, C.c_double), k,
+                               _p(targets, C.c_uint32), len(targets), _p(qs_, C.c_uint32), _p(qt_, C.c_uint32),
+                               len(qs_), threads, _p(buf, C.c_int64), cap, _p(q_off, C.c_int64), rounds,
+                               C.byref(need))
+        if rc == 0:
+            break
+        cap = int(need.value)
+    out = [_deser(buf, int(q_off[q]))[0] for q in range(len(qs_))]
+    return out, {int(t): int(rounds[i]) for i, t in enumerate(targets)}
 
 
 def bfs_closure(src, dst, threads=8):

@@ -26,6 +26,8 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <memory>
+#include <iterator>
 #include <optional>
 #include <queue>
 #include <set>
@@ -471,6 +473,429 @@ Atom read_atom(Reader& r) {
   for (int k = 0; k < ar; k++) a.args.push_back(read_term(r));
   return a;
 }
+
+Program parse_program(Reader& R) {
+  Program P;
+  const int np = (int)R.next();
+  for (int k = 0; k < np; k++) {
+    Pred p;
+    p.arity = (int)R.next();
+    p.trop = R.next() != 0;
+    p.stratum = (int)R.next();
+    P.preds.push_back(p);
+  }
+  P.num_strata = (int)R.next();
+  const int nr = (int)R.next();
+  for (int k = 0; k < nr; k++) {
+    Rule r;
+    r.var_count = (int)R.next();
+    r.head = read_atom(R);
+    r.agg_op = (int)R.next();
+    r.agg_slot = (int)R.next();
+    r.agg_pos = (int)R.next();
+    const int nb = (int)R.next();
+    for (int q = 0; q < nb; q++) {
+      Lit l;
+      l.neg = R.next() != 0;
+      l.atom = read_atom(R);
+      r.body.push_back(l);
+    }
+    P.rules.push_back(r);
+  }
+  return P;
+}
+
+// ===========================================================================
+// A'. Provenance capture (strata-eval/src/provenance.rs) and exact
+//     compilation + weighted model counting (strata-prob/src/compile.rs,
+//     circuit.rs), all in FP64: the oracle of the probabilistic path.
+// ===========================================================================
+enum ProvErr : int {
+  E_NOT_BOOL = 20,       // ProvError::NotBool (provenance.rs:63)
+  E_BAD_PROB = 21,       // ProvError::BadProbability
+  E_PROOF_BUDGET = 22,   // ProvError::ProofBudget
+  E_SOFT_AGG = 23,       // ProvError::SoftAggregate
+  E_CIRCUIT_BUDGET = 24, // compile.rs BudgetExceeded
+};
+
+// A proof: sorted signed literals ±(i+1) (a BTreeSet<i64>); a proof set is an
+// ordered set of proofs (BTreeSet<BTreeSet<i64>>: lexicographic order).
+using Proof = std::vector<int64_t>;
+using ProofSet = std::set<Proof>;
+
+inline bool is_subset(const Proof& a, const Proof& b) {  // a ⊆ b
+  return std::includes(b.begin(), b.end(), a.begin(), a.end());
+}
+
+// insert_minimal (provenance.rs:136-143).
+bool insert_minimal(ProofSet& set, const Proof& proof) {
+  for (auto& kept : set)
+    if (is_subset(kept, proof)) return false;
+  for (auto it = set.begin(); it != set.end();) {
+    if (is_subset(proof, *it)) it = set.erase(it);
+    else ++it;
+  }
+  set.insert(proof);
+  return true;
+}
+
+inline Proof proof_union(const Proof& a, const Proof& b) {
+  Proof u;
+  u.reserve(a.size() + b.size());
+  std::set_union(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(u));
+  return u;
+}
+
+inline bool contradictory(const Proof& p) {
+  for (auto l : p)
+    if (std::binary_search(p.begin(), p.end(), -l)) return true;
+  return false;
+}
+
+// product (provenance.rs:147-158).
+ProofSet product(const ProofSet& acc, const ProofSet& other) {
+  ProofSet out;
+  for (auto& a : acc)
+    for (auto& b : other) {
+      Proof j = proof_union(a, b);
+      if (!contradictory(j)) insert_minimal(out, j);
+    }
+  return out;
+}
+
+// complement (provenance.rs:166-176); false = over budget.
+bool complement(const ProofSet& proofs, size_t max_proofs, ProofSet* out) {
+  ProofSet acc{Proof{}};
+  for (auto& p : proofs) {
+    ProofSet neg;
+    for (auto l : p) neg.insert(Proof{-l});
+    acc = product(acc, neg);
+    if (acc.size() > max_proofs) return false;
+  }
+  *out = acc;
+  return true;
+}
+
+// proof_weight (provenance.rs:179-192): ascending literals, left fold from 1.
+double proof_weight(const Proof& proof, const std::vector<double>& prob) {
+  double w = 1.0;
+  for (auto l : proof) {
+    const double p = prob[(size_t)(std::llabs(l) - 1)];
+    w = w * (l > 0 ? p : 1.0 - p);
+  }
+  return w;
+}
+
+// prune_top_k (provenance.rs:195-212): (weight desc, literals asc), stable.
+void prune_top_k(ProofSet& set, size_t k, const std::vector<double>& prob) {
+  if (set.size() <= k) return;
+  std::vector<std::pair<double, Proof>> scored;
+  for (auto& p : set) scored.emplace_back(proof_weight(p, prob), p);
+  std::stable_sort(scored.begin(), scored.end(), [](const auto& a, const auto& b) {
+    if (b.first < a.first) return true;
+    if (a.first < b.first) return false;
+    return a.second < b.second;
+  });
+  scored.resize(k);
+  set.clear();
+  for (auto& s : scored) set.insert(s.second);
+}
+
+struct ProvInterp {
+  const Program& P;
+  std::vector<std::map<Tuple, ProofSet>> db;
+  std::vector<double> prob;
+  std::vector<int64_t> modes;  // per predicate: 0 exact, k > 0 top-k
+  size_t max_proofs;
+  int cur_stratum = 0;
+  ProvInterp(const Program& p, std::vector<double> probs, std::vector<int64_t> m, size_t maxp)
+      : P(p), db(p.preds.size()), prob(std::move(probs)), modes(std::move(m)), max_proofs(maxp) {}
+
+  // solve_prov (provenance.rs:368-507).
+  void solve(const Rule& r, size_t idx, Binding2& binding, const ProofSet& acc,
+             std::vector<std::tuple<int, Tuple, ProofSet>>& out) {
+    if (idx == r.body.size()) {
+      out.emplace_back(r.head.pred, Interp::ground(r.head.args, binding, false), acc);
+      return;
+    }
+    const Lit& lit = r.body[idx];
+    if (!lit.neg) {
+      for (auto& row : db[lit.atom.pred]) {
+        Binding2 b = binding;
+        if (Interp::unify(lit.atom.args, row.first, b)) {
+          ProofSet next = product(acc, row.second);
+          if (next.empty()) continue;
+          if (next.size() > max_proofs) throw EvalError{E_PROOF_BUDGET};
+          solve(r, idx + 1, b, next, out);
+        }
+      }
+    } else {
+      if (P.preds[lit.atom.pred].stratum >= cur_stratum) throw EvalError{E_NEG_NOT_STRAT};
+      Tuple t = Interp::ground(lit.atom.args, binding, true);
+      auto it = db[lit.atom.pred].find(t);
+      if (it == db[lit.atom.pred].end()) {
+        solve(r, idx + 1, binding, acc, out);
+        return;
+      }
+      if (it->second.count(Proof{})) return;  // certainly present
+      ProofSet negated;
+      if (!complement(it->second, max_proofs, &negated)) throw EvalError{E_PROOF_BUDGET};
+      ProofSet next = product(acc, negated);
+      if (next.empty()) return;
+      if (next.size() > max_proofs) throw EvalError{E_PROOF_BUDGET};
+      solve(r, idx + 1, binding, next, out);
+    }
+  }
+
+  // saturate (provenance.rs:286-362): naive Jacobi rounds per stratum.
+  long saturate() {
+    long rounds = 0;
+    for (int k = 0; k < P.num_strata; k++) {
+      cur_stratum = k;
+      for (auto& r : P.rules)
+        if (P.preds[r.head.pred].stratum == k && r.agg_op >= 0) throw EvalError{E_SOFT_AGG};
+      while (true) {
+        std::vector<std::tuple<int, Tuple, ProofSet>> derived;
+        for (auto& r : P.rules) {
+          if (P.preds[r.head.pred].stratum != k || r.agg_op >= 0) continue;
+          Binding2 b((size_t)r.var_count);
+          solve(r, 0, b, ProofSet{Proof{}}, derived);
+        }
+        rounds++;
+        bool changed = false;
+        for (auto& d : derived) {
+          const int pred = std::get<0>(d);
+          const int64_t topk = modes[(size_t)pred];
+          ProofSet& set = db[(size_t)pred][std::get<1>(d)];
+          ProofSet before;
+          if (topk > 0) before = set;
+          bool local = false;
+          for (auto& proof : std::get<2>(d)) local |= insert_minimal(set, proof);
+          if (local && topk > 0) {
+            prune_top_k(set, (size_t)topk, prob);
+            local = set != before;
+          } else if (local && set.size() > max_proofs) {
+            throw EvalError{E_PROOF_BUDGET};
+          }
+          changed |= local;
+        }
+        if (!changed) break;
+      }
+    }
+    return rounds;
+  }
+};
+
+// ---- exact compilation (compile.rs) and the circuit (circuit.rs) ----------
+struct CNode {
+  int kind;  // 0 leaf, 1 neg leaf, 2 and, 3 or, 4 true, 5 false
+  int64_t leaf;
+  std::vector<size_t> ch;
+};
+
+struct CircuitBuilder {
+  std::vector<CNode> nodes;
+  size_t num_leaves = 0;
+  size_t push(CNode n) {
+    nodes.push_back(std::move(n));
+    return nodes.size() - 1;
+  }
+};
+
+// normalize (compile.rs:30-47).
+std::vector<Proof> dnf_normalize(const std::vector<Proof>& proofs) {
+  std::vector<Proof> sets;
+  for (auto& p : proofs) {
+    Proof q = p;
+    std::sort(q.begin(), q.end());
+    q.erase(std::unique(q.begin(), q.end()), q.end());
+    if (!contradictory(q)) sets.push_back(q);
+  }
+  std::stable_sort(sets.begin(), sets.end(), [](const Proof& a, const Proof& b) { return a.size() < b.size(); });
+  ProofSet min;
+  for (auto& p : sets) {
+    bool absorbed = false;
+    for (auto& kept : min)
+      if (is_subset(kept, p)) { absorbed = true; break; }
+    if (!absorbed) min.insert(p);
+  }
+  return std::vector<Proof>(min.begin(), min.end());
+}
+
+// restrict (compile.rs:153-172).
+ProofSet dnf_restrict(const std::vector<Proof>& dnf, int64_t var, bool value) {
+  const int64_t dies = value ? -var : var, discharged = value ? var : -var;
+  ProofSet out;
+  for (auto& p : dnf) {
+    if (std::binary_search(p.begin(), p.end(), dies)) continue;
+    Proof q;
+    for (auto l : p)
+      if (l != discharged) q.push_back(l);
+    bool absorbed = false;
+    for (auto& kept : out)
+      if (is_subset(kept, q)) { absorbed = true; break; }
+    if (absorbed) continue;
+    for (auto it = out.begin(); it != out.end();) {
+      if (is_subset(q, *it)) it = out.erase(it);
+      else ++it;
+    }
+    out.insert(q);
+  }
+  return out;
+}
+
+struct Shannon {
+  CircuitBuilder& b;
+  std::map<std::vector<Proof>, size_t> memo;
+  size_t max_nodes;
+  size_t run(const std::vector<Proof>& dnf) {  // shannon (compile.rs:103-150)
+    if (b.nodes.size() > max_nodes) throw EvalError{E_CIRCUIT_BUDGET};
+    if (dnf.empty()) return b.push(CNode{5, 0, {}});
+    for (auto& p : dnf)
+      if (p.empty()) return b.push(CNode{4, 0, {}});
+    auto m = memo.find(dnf);
+    if (m != memo.end()) return m->second;
+    std::map<int64_t, size_t> count;
+    for (auto& p : dnf)
+      for (auto l : p) count[std::llabs(l)]++;
+    // most frequent variable; ties to the smallest variable
+    int64_t v = 0;
+    size_t best = 0;
+    for (auto& kv : count)
+      if (kv.second > best) { best = kv.second; v = kv.first; }
+    ProofSet hi_s = dnf_restrict(dnf, v, true), lo_s = dnf_restrict(dnf, v, false);
+    std::vector<Proof> hi(hi_s.begin(), hi_s.end()), lo(lo_s.begin(), lo_s.end());
+    const size_t hi_n = run(hi);
+    const size_t lo_n = run(lo);
+    const size_t leaf = (size_t)(v - 1);
+    b.num_leaves = std::max(b.num_leaves, leaf + 1);
+    const size_t pos = b.push(CNode{0, (int64_t)leaf, {}});
+    const size_t neg = b.push(CNode{1, (int64_t)leaf, {}});
+    const size_t and_hi = b.push(CNode{2, 0, {pos, hi_n}});
+    const size_t and_lo = b.push(CNode{2, 0, {neg, lo_n}});
+    const size_t node = b.push(CNode{3, 0, {and_hi, and_lo}});
+    memo.emplace(dnf, node);
+    return node;
+  }
+};
+
+// Circuit::eval / grad (circuit.rs:43-106), FP64.
+void circuit_grad(const std::vector<CNode>& nodes, size_t root, const std::vector<double>& p, double* value,
+                  std::vector<double>* leaf_g) {
+  std::vector<double> val(nodes.size(), 0.0);
+  for (size_t i = 0; i < nodes.size(); i++) {
+    const CNode& n = nodes[i];
+    switch (n.kind) {
+      case 0: val[i] = p[(size_t)n.leaf]; break;
+      case 1: val[i] = 1.0 - p[(size_t)n.leaf]; break;
+      case 2: { double a = 1.0; for (auto c : n.ch) a = a * val[c]; val[i] = a; break; }
+      case 3: { double a = 0.0; for (auto c : n.ch) a = a + val[c]; val[i] = a; break; }
+      case 4: val[i] = 1.0; break;
+      default: val[i] = 0.0; break;
+    }
+  }
+  *value = nodes.empty() ? 0.0 : val[root];
+  if (!leaf_g || nodes.empty()) return;
+  std::vector<double> g(nodes.size(), 0.0);
+  g[root] = 1.0;
+  for (size_t i = nodes.size(); i-- > 0;) {
+    const double gi = g[i];
+    if (gi == 0.0) continue;
+    const CNode& n = nodes[i];
+    if (n.kind == 0) (*leaf_g)[(size_t)n.leaf] += gi;
+    else if (n.kind == 1) (*leaf_g)[(size_t)n.leaf] -= gi;
+    else if (n.kind == 2) {
+      for (size_t j = 0; j < n.ch.size(); j++) {
+        double sib = 1.0;
+        for (size_t q = 0; q < n.ch.size(); q++)
+          if (q != j) sib = sib * val[n.ch[q]];
+        g[n.ch[j]] += gi * sib;
+      }
+    } else if (n.kind == 3) {
+      for (auto c : n.ch) g[c] += gi;
+    }
+  }
+}
+
+struct ProvHandle {
+  Program P;
+  std::unique_ptr<ProvInterp> I;
+  long rounds = 0;
+};
+
+// ---- the TC-shaped capture restricted to queried targets -------------------
+// path(X,Y) :- edge(X,Y).  path(X,Z) :- edge(X,Y), path(Y,Z).  with `path`
+// Prov_k(k) and every edge fact probabilistic (literal = edge index + 1).
+// For a fixed target t, path(., t) depends only on path(., t) and edge, so
+// the saturation restricted to the queried targets yields the same proof
+// sets for those tuples.  The per-tuple update follows saturate's order:
+// the rule-1 entry, then rule-2 entries by ascending (X, Y) edge order, each
+// inserted with insert_minimal and pruned after its batch.
+struct TcProv {
+  uint32_t n;
+  // out-CSR over distinct edge tuples sorted by (X, Y); each tuple carries
+  // the proofs {i+1} of its edge facts (duplicates give several)
+  std::vector<uint32_t> off, nbr;
+  std::vector<ProofSet> eproofs;
+  std::vector<double> prob;
+  size_t k;
+  void build(uint32_t nodes, const uint32_t* src, const uint32_t* dst, size_t m) {
+    n = nodes;
+    std::vector<uint64_t> key(m);
+    for (size_t i = 0; i < m; i++) key[i] = ((uint64_t)src[i] << 32) | dst[i];
+    std::vector<size_t> ord(m);
+    for (size_t i = 0; i < m; i++) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return key[a] < key[b]; });
+    off.assign(n + 1, 0);
+    nbr.clear();
+    eproofs.clear();
+    for (size_t q = 0; q < m; q++) {
+      const size_t i = ord[q];
+      if (q == 0 || key[i] != key[ord[q - 1]]) {
+        nbr.push_back(dst[i]);
+        eproofs.push_back(ProofSet{});
+        off[src[i] + 1]++;
+      }
+      eproofs.back().insert(Proof{(int64_t)i + 1});
+    }
+    for (uint32_t v = 0; v < n; v++) off[v + 1] += off[v];
+  }
+  // Saturate path(., t); returns rounds.  state[X] = proof set of path(X, t).
+  long run_target(uint32_t t, std::vector<ProofSet>& state) const {
+    state.assign(n, ProofSet{});
+    long rounds = 0;
+    while (true) {
+      rounds++;
+      std::vector<ProofSet> next = state;
+      bool changed = false;
+      for (uint32_t x = 0; x < n; x++) {
+        ProofSet& set = next[x];
+        auto entry = [&](const ProofSet& batch) {
+          ProofSet before = set;
+          bool local = false;
+          for (auto& pr : batch) local |= insert_minimal(set, pr);
+          if (local) {
+            prune_top_k(set, k, prob);
+            local = set != before;
+          }
+          changed |= local;
+        };
+        // rule 1: path(X, t) :- edge(X, t)
+        for (uint32_t q = off[x]; q < off[x + 1]; q++)
+          if (nbr[q] == t) entry(product(ProofSet{Proof{}}, eproofs[q]));
+        // rule 2: path(X, t) :- edge(X, Y), path(Y, t)
+        for (uint32_t q = off[x]; q < off[x + 1]; q++) {
+          const uint32_t y = nbr[q];
+          if (state[y].empty()) continue;
+          entry(product(product(ProofSet{Proof{}}, eproofs[q]), state[y]));
+        }
+      }
+      state.swap(next);
+      if (!changed) break;
+    }
+    return rounds;
+  }
+};
 
 }  // namespace
 
@@ -922,6 +1347,152 @@ void sko_bfs_closure(const uint32_t* src, const uint32_t* dst, size_t n, int thr
   *fp = f;
 }
 
+// ---- per-instance closure count + row-polynomial fingerprint --------------
+// For the batched reachability form the closure of an instance is summarised
+// by |path| and  fp = Σ_{(X,Z) ∈ path} mix64(X) · c^Z  (mod 2^64), c the odd
+// constant kPolyC — order-independent, and computable from bit rows one word
+// at a time.  This oracle is independent of the engine's round structure:
+// strongly connected components (iterative Tarjan, components complete in
+// reverse topological order), then per component C the set R(C) of nodes
+// reachable by a path of length >= 1:
+//   R(C) = (C if C has a cycle) ∪ ⋃_{C -> C'} (C' ∪ R(C')).
+static const uint64_t kPolyC = 0x9e3779b97f4a7c15ull;
+
+struct PolyTables {
+  uint64_t tb[8][256];  // tb[b][v] = Σ_{j ∈ bits(v)} c^(8b + j)
+  PolyTables() {
+    uint64_t pw[64];
+    pw[0] = 1;
+    for (int j = 1; j < 64; j++) pw[j] = pw[j - 1] * kPolyC;
+    for (int b = 0; b < 8; b++)
+      for (int v = 0; v < 256; v++) {
+        uint64_t a = 0;
+        for (int j = 0; j < 8; j++)
+          if (v >> j & 1) a += pw[8 * b + j];
+        tb[b][v] = a;
+      }
+  }
+};
+
+static void closure_count_fp(uint32_t n, const uint32_t* src, const uint32_t* dst, uint64_t m,
+                             const PolyTables& T, uint64_t* count, uint64_t* fp) {
+  std::vector<uint32_t> off(n + 1, 0), adj(m);
+  for (uint64_t i = 0; i < m; i++) off[src[i] + 1]++;
+  for (uint32_t v = 0; v < n; v++) off[v + 1] += off[v];
+  {
+    std::vector<uint32_t> fill(off.begin(), off.end() - 1);
+    for (uint64_t i = 0; i < m; i++) adj[fill[src[i]]++] = dst[i];
+  }
+  // iterative Tarjan
+  std::vector<int64_t> idx(n, -1), low(n, 0);
+  std::vector<int64_t> comp(n, -1);
+  std::vector<uint32_t> stk;
+  std::vector<char> on(n, 0);
+  struct Frame { uint32_t v; uint32_t e; };
+  std::vector<Frame> cs;
+  int64_t next_idx = 0, ncomp = 0;
+  for (uint32_t s0 = 0; s0 < n; s0++) {
+    if (idx[s0] >= 0) continue;
+    idx[s0] = low[s0] = next_idx++;
+    stk.push_back(s0);
+    on[s0] = 1;
+    cs.push_back({s0, off[s0]});
+    while (!cs.empty()) {
+      const uint32_t v = cs.back().v;
+      if (cs.back().e < off[v + 1]) {
+        const uint32_t w = adj[cs.back().e++];
+        if (idx[w] < 0) {
+          idx[w] = low[w] = next_idx++;
+          stk.push_back(w);
+          on[w] = 1;
+          cs.push_back({w, off[w]});
+        } else if (on[w]) {
+          low[v] = std::min(low[v], idx[w]);
+        }
+      } else {
+        if (low[v] == idx[v]) {
+          while (true) {
+            const uint32_t x = stk.back();
+            stk.pop_back();
+            on[x] = 0;
+            comp[x] = ncomp;
+            if (x == v) break;
+          }
+          ncomp++;
+        }
+        cs.pop_back();
+        if (!cs.empty()) {
+          const uint32_t p = cs.back().v;
+          low[p] = std::min(low[p], low[v]);
+        }
+      }
+    }
+  }
+  // members per component, cycle flag, pending predecessor edges
+  std::vector<uint32_t> moff(ncomp + 1, 0), mem(n);
+  for (uint32_t v = 0; v < n; v++) moff[comp[v] + 1]++;
+  for (int64_t c = 0; c < ncomp; c++) moff[c + 1] += moff[c];
+  {
+    std::vector<uint32_t> fill(moff.begin(), moff.end() - 1);
+    for (uint32_t v = 0; v < n; v++) mem[fill[comp[v]]++] = v;
+  }
+  std::vector<char> cyc(ncomp, 0);
+  std::vector<uint64_t> pend(ncomp, 0);
+  for (uint32_t x = 0; x < n; x++)
+    for (uint32_t k = off[x]; k < off[x + 1]; k++) {
+      const uint32_t y = adj[k];
+      if (comp[y] == comp[x]) cyc[comp[x]] = 1;  // an edge inside C (self-loop or cycle)
+      else pend[comp[y]]++;
+    }
+  for (int64_t c = 0; c < ncomp; c++)
+    if (moff[c + 1] - moff[c] > 1) cyc[c] = 1;
+  const size_t W = ((size_t)n + 63) / 64;
+  std::vector<uint64_t> cw(W);  // c^(64 w)
+  {
+    uint64_t c64 = 1;
+    for (int j = 0; j < 64; j++) c64 *= kPolyC;
+    uint64_t a = 1;
+    for (size_t w = 0; w < W; w++) { cw[w] = a; a *= c64; }
+  }
+  std::vector<std::vector<uint64_t>> rstar(ncomp);
+  uint64_t cnt = 0, f = 0;
+  std::vector<uint64_t> R(W);
+  for (int64_t c = 0; c < ncomp; c++) {
+    std::fill(R.begin(), R.end(), 0ull);
+    if (cyc[c])
+      for (uint32_t k = moff[c]; k < moff[c + 1]; k++) R[mem[k] >> 6] |= 1ull << (mem[k] & 63);
+    for (uint32_t k = moff[c]; k < moff[c + 1]; k++) {
+      const uint32_t x = mem[k];
+      for (uint32_t e = off[x]; e < off[x + 1]; e++) {
+        const int64_t c2 = comp[adj[e]];
+        if (c2 == c) continue;
+        const std::vector<uint64_t>& r2 = rstar[c2];
+        for (size_t w = 0; w < W; w++) R[w] |= r2[w];
+        if (--pend[c2] == 0) std::vector<uint64_t>().swap(rstar[c2]);
+      }
+    }
+    uint64_t pc = 0, poly = 0;
+    for (size_t w = 0; w < W; w++) {
+      const uint64_t x = R[w];
+      if (!x) continue;
+      pc += (uint64_t)__builtin_popcountll(x);
+      uint64_t t = 0;
+      for (int b = 0; b < 8; b++) t += T.tb[b][(x >> (8 * b)) & 255];
+      poly += cw[w] * t;
+    }
+    uint64_t msum = 0;
+    for (uint32_t k = moff[c]; k < moff[c + 1]; k++) msum += mix64(mem[k]);
+    cnt += (uint64_t)(moff[c + 1] - moff[c]) * pc;
+    f += msum * poly;
+    if (pend[c]) {
+      rstar[c] = R;
+      for (uint32_t k = moff[c]; k < moff[c + 1]; k++) rstar[c][mem[k] >> 6] |= 1ull << (mem[k] & 63);
+    }
+  }
+  *count = cnt;
+  *fp = f;
+}
+
 // Multi-source shortest non-empty paths by Dijkstra (non-negative finite
 // weights): dist(S, Y) for every Y reachable from S by >= 1 edge, seeded with
 // the source weight.  Count + fingerprint (same mixing as the device).
@@ -1086,6 +1657,205 @@ uint64_t sko_brute_4cliques(const uint32_t* a, const uint32_t* b, size_t n, uint
       }
     }
   return t;
+}
+
+
+// Closure count + row-polynomial fingerprint of one graph on nodes [0, n).
+int sko_closure_count_fp(uint32_t n, const uint32_t* src, const uint32_t* dst, uint64_t m, uint64_t* count,
+                         uint64_t* fp) {
+  for (uint64_t i = 0; i < m; i++)
+    if (src[i] >= n || dst[i] >= n) return 1;
+  static const PolyTables T;
+  closure_count_fp(n, src, dst, m, T, count, fp);
+  return 0;
+}
+
+// The same for a batch of instances (instance i: nodes[i], edges
+// [edge_off[i], edge_off[i+1])), largest first across `threads` threads.
+int sko_closure_batch(uint32_t n_inst, const uint32_t* nodes, const uint64_t* edge_off, const uint32_t* src,
+                      const uint32_t* dst, int threads, uint64_t* counts, uint64_t* fps) {
+  static const PolyTables T;
+  std::vector<uint32_t> order(n_inst);
+  for (uint32_t i = 0; i < n_inst; i++) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return nodes[a] > nodes[b]; });
+  std::atomic<uint32_t> next{0};
+  std::atomic<int> bad{0};
+  auto work = [&]() {
+    while (true) {
+      const uint32_t k = next.fetch_add(1);
+      if (k >= n_inst) break;
+      const uint32_t i = order[k];
+      const uint64_t a = edge_off[i], b = edge_off[i + 1];
+      bool ok = true;
+      for (uint64_t e = a; e < b; e++)
+        if (src[e] >= nodes[i] || dst[e] >= nodes[i]) ok = false;
+      if (!ok) { bad = 1; continue; }
+      closure_count_fp(nodes[i], src + a, dst + a, b - a, T, &counts[i], &fps[i]);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 0; t < std::max(1, threads); t++) th.emplace_back(work);
+  for (auto& t : th) t.join();
+  return bad.load();
+}
+
+
+// ---- provenance capture, compilation and WMC (FP64) ------------------------
+static void put_proofs(const ProofSet& ps, std::vector<int64_t>& out) {
+  out.push_back((int64_t)ps.size());
+  for (auto& p : ps) {
+    out.push_back((int64_t)p.size());
+    for (auto l : p) out.push_back(l);
+  }
+}
+
+// Capture over a program blob whose facts with weight kind 3 are the
+// probabilistic leaves (in blob order, probabilities in `probs`); `modes[p]`
+// is 0 (exact) or k (Prov_k) per predicate.  Returns a handle or null with
+// *err set.
+void* sko_prov_run(const int64_t* blob, size_t n, const double* probs, size_t n_prob, const int64_t* modes,
+                   size_t max_proofs, long* rounds, int* err) {
+  *err = 0;
+  try {
+    Reader R{blob, 0, n};
+    auto* h = new ProvHandle();
+    h->P = parse_program(R);
+    for (auto& pr : h->P.preds)
+      if (pr.trop) { delete h; *err = E_NOT_BOOL; return nullptr; }
+    std::vector<double> pv(probs, probs + n_prob);
+    for (double p : pv)
+      if (!(p >= 0.0 && p <= 1.0)) { delete h; *err = E_BAD_PROB; return nullptr; }
+    h->I.reset(new ProvInterp(h->P, pv, std::vector<int64_t>(modes, modes + h->P.preds.size()), max_proofs));
+    const long nf = (long)R.next();
+    int64_t leaf = 0;
+    for (long q = 0; q < nf; q++) {
+      const int pred = (int)R.next();
+      const int ar = (int)R.next();
+      Tuple t;
+      for (int c = 0; c < ar; c++) {
+        GV g;
+        g.tag = (uint8_t)R.next();
+        g.v = R.next();
+        t.push_back(g);
+      }
+      const int wk = (int)R.next();
+      (void)R.next();
+      if (wk == 3) {
+        if ((size_t)leaf >= n_prob) { delete h; *err = E_BAD_PROB; return nullptr; }
+        insert_minimal(h->I->db[(size_t)pred][t], Proof{leaf + 1});
+        leaf++;
+      } else {
+        insert_minimal(h->I->db[(size_t)pred][t], Proof{});
+      }
+    }
+    h->rounds = h->I->saturate();
+    if (rounds) *rounds = h->rounds;
+    return h;
+  } catch (const EvalError& e) {
+    *err = e.code;
+    return nullptr;
+  }
+}
+
+void sko_prov_free(void* h) { delete static_cast<ProvHandle*>(h); }
+
+// Proofs of pred(tuple) serialized as [n, (len, lits...)*]; -1 = no tuple.
+long sko_prov_proofs(void* hv, int pred, const int64_t* vals, int arity, int64_t* out, size_t cap) {
+  auto* h = static_cast<ProvHandle*>(hv);
+  Tuple t;
+  for (int c = 0; c < arity; c++) t.push_back(GV{(uint8_t)vals[2 * c], vals[2 * c + 1]});
+  auto it = h->I->db[(size_t)pred].find(t);
+  if (it == h->I->db[(size_t)pred].end()) return -1;
+  std::vector<int64_t> buf;
+  put_proofs(it->second, buf);
+  if (buf.size() <= cap) std::copy(buf.begin(), buf.end(), out);
+  return (long)buf.size();
+}
+
+// Every tuple of a predicate: [n_tuples, (arity values as tag,val..., proofs)*].
+long sko_prov_relation(void* hv, int pred, int64_t* out, size_t cap) {
+  auto* h = static_cast<ProvHandle*>(hv);
+  std::vector<int64_t> buf;
+  buf.push_back((int64_t)h->I->db[(size_t)pred].size());
+  for (auto& kv : h->I->db[(size_t)pred]) {
+    for (auto& v : kv.first) {
+      buf.push_back(v.tag);
+      buf.push_back(v.v);
+    }
+    put_proofs(kv.second, buf);
+  }
+  if (buf.size() <= cap) std::copy(buf.begin(), buf.end(), out);
+  return (long)buf.size();
+}
+
+// compile_exact + Circuit::grad on serialized proofs [n, (len, lits...)*].
+int sko_compile_grad(const int64_t* ser, size_t n_leaves, const double* probs, size_t max_nodes, double* p_out,
+                     double* grad_out, int64_t* nodes_out) {
+  try {
+    std::vector<Proof> proofs;
+    size_t i = 0;
+    const int64_t np = ser[i++];
+    for (int64_t q = 0; q < np; q++) {
+      const int64_t len = ser[i++];
+      proofs.emplace_back(ser + i, ser + i + len);
+      i += (size_t)len;
+    }
+    std::vector<Proof> dnf = dnf_normalize(proofs);
+    CircuitBuilder b;
+    Shannon sh{b, {}, max_nodes};
+    const size_t root = sh.run(dnf);
+    const size_t nl = std::max(n_leaves, b.num_leaves);
+    std::vector<double> pv(probs, probs + n_leaves);
+    pv.resize(nl, 0.0);
+    std::vector<double> g(nl, 0.0);
+    circuit_grad(b.nodes, root, pv, p_out, grad_out ? &g : nullptr);
+    if (grad_out) std::copy(g.begin(), g.begin() + (long)n_leaves, grad_out);
+    if (nodes_out) *nodes_out = (int64_t)b.nodes.size();
+    return 0;
+  } catch (const EvalError& e) {
+    return e.code;
+  }
+}
+
+// The TC-shaped capture restricted to `targets` (edge i has probability
+// probs[i] and literal i+1).  For each query q = (qs[q], qt[q]) writes the
+// serialized proofs of path(qs, qt) into a buffer (offsets in q_off, n+1).
+// Per-target rounds go to rounds[t].  Returns 0, or -1 when `cap` is short
+// (*need gets the size).
+long sko_prov_tc(uint32_t n, const uint32_t* src, const uint32_t* dst, size_t m, const double* probs, size_t k,
+                 const uint32_t* targets, size_t n_targets, const uint32_t* qs, const uint32_t* qt, size_t nq,
+                 int threads, int64_t* out, size_t cap, int64_t* q_off, long* rounds, size_t* need) {
+  TcProv tp;
+  tp.build(n, src, dst, m);
+  tp.prob.assign(probs, probs + m);
+  tp.k = k;
+  std::vector<std::vector<int64_t>> per_q(nq);
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    std::vector<ProofSet> state;
+    while (true) {
+      const size_t ti = next.fetch_add(1);
+      if (ti >= n_targets) break;
+      const uint32_t t = targets[ti];
+      const long r = tp.run_target(t, state);
+      if (rounds) rounds[ti] = r;
+      for (size_t q = 0; q < nq; q++)
+        if (qt[q] == t) put_proofs(qs[q] < n ? state[qs[q]] : ProofSet{}, per_q[q]);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int q = 0; q < std::max(1, threads); q++) th.emplace_back(work);
+  for (auto& x : th) x.join();
+  size_t total = 0;
+  for (size_t q = 0; q < nq; q++) {
+    q_off[q] = (int64_t)total;
+    total += per_q[q].size();
+  }
+  q_off[nq] = (int64_t)total;
+  *need = total;
+  if (total > cap) return -1;
+  for (size_t q = 0; q < nq; q++) std::copy(per_q[q].begin(), per_q[q].end(), out + q_off[q]);
+  return 0;
 }
 
 }  // extern "C"

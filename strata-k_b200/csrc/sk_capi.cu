@@ -179,13 +179,30 @@ strata_status strata_ctx_mem(const strata_ctx* ctx, uint64_t* in_use, uint64_t* 
 
 strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan) {
   if (!ctx) return STRATA_E_INVALID;
-  if (plan < 0 || plan > 2) return bad(ctx, "plan must be 0 (auto), 1 (sort-merge) or 2 (direct-addressed)");
+  if (plan < 0 || plan > 3)
+    return bad(ctx, "plan must be 0 (auto), 1 (sort-merge), 2 (direct-addressed) or 3 (bit rows)");
   ctx->plan = plan;
   return STRATA_OK;
 }
 
 strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value) {
   if (!ctx) return STRATA_E_INVALID;
+  if (knob == STRATA_KNOB_BATCH_GRAPH_ROUNDS) {
+    if (value != 0 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
+      return bad(ctx, "graph rounds must be 0 (default), 2, 4, 8, 16 or 32");
+    ctx->tune_bs_graph_rounds = value;
+    return STRATA_OK;
+  }
+  if (knob == STRATA_KNOB_BATCH_BLOCKS_PER_SM) {
+    if (value < 0 || value > 32) return bad(ctx, "blocks per SM must be 0 (default) .. 32");
+    ctx->tune_bs_blocks = value;
+    return STRATA_OK;
+  }
+  if (knob == STRATA_KNOB_BATCH_BUDGET_MB) {
+    if (value < 0) return bad(ctx, "the wave budget must be >= 0 MiB");
+    ctx->tune_bs_budget_mb = (uint64_t)value;
+    return STRATA_OK;
+  }
   if (knob == STRATA_KNOB_TRI_PROBE) {
     if (value < 0 || value > 2) return bad(ctx, "triangle probe must be 0 (default), 1 (hash set) or 2 (binary search)");
     ctx->tune_tri_probe = value;
@@ -402,6 +419,45 @@ strata_status strata_count_triangle_pattern_dev(strata_ctx* ctx, const uint32_t*
   if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
   SK_GUARD_BEGIN
   *out_count = sk::count_triangle_pattern(ctx, d_x, d_y, n);
+  SK_GUARD_END(ctx)
+}
+
+// ---- batched Bool reachability -----------------------------------------------------
+
+namespace {
+strata_status batch_check(strata_ctx* ctx, uint32_t n_inst, const uint32_t* nodes, const uint64_t* edge_off,
+                          const void* src, const void* dst) {
+  if (n_inst && (!nodes || !edge_off)) return bad(ctx, "NULL argument");
+  if (n_inst && edge_off[0] != 0) return bad(ctx, "edge_off[0] must be 0");
+  for (uint32_t i = 0; i < n_inst; i++)
+    if (edge_off[i + 1] < edge_off[i]) return bad(ctx, "edge offsets must be non-decreasing");
+  if (n_inst && edge_off[n_inst] && (!src || !dst)) return bad(ctx, "NULL argument");
+  return STRATA_OK;
+}
+}  // namespace
+
+strata_status strata_tc_bool_batch_dev(strata_ctx* ctx, uint32_t n_inst, const uint32_t* nodes,
+                                       const uint64_t* edge_off, const uint32_t* d_src, const uint32_t* d_dst,
+                                       int mode, uint64_t* counts, uint64_t* fps, uint32_t* rounds,
+                                       strata_batch_stats* stats) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (batch_check(ctx, n_inst, nodes, edge_off, d_src, d_dst) != STRATA_OK) return STRATA_E_INVALID;
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::tc_bool_batch(ctx, n_inst, nodes, edge_off, d_src, d_dst, mode, counts, fps, rounds, stats);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint32_t* nodes,
+                                   const uint64_t* edge_off, const uint32_t* src, const uint32_t* dst, int mode,
+                                   uint64_t* counts, uint64_t* fps, uint32_t* rounds, strata_batch_stats* stats) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (batch_check(ctx, n_inst, nodes, edge_off, src, dst) != STRATA_OK) return STRATA_E_INVALID;
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  const uint64_t m = n_inst ? edge_off[n_inst] : 0;
+  DBuf<uint32_t> ds = to_dev(ctx, src, m), dd = to_dev(ctx, dst, m);
+  sk::tc_bool_batch(ctx, n_inst, nodes, edge_off, ds.p, dd.p, mode, counts, fps, rounds, stats);
   SK_GUARD_END(ctx)
 }
 

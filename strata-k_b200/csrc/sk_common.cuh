@@ -79,7 +79,10 @@ struct strata_ctx {
   int plan = 0;                     // 0 auto, 1 sort-merge, 2 direct-addressed
   int tune_items4 = 0;              // radix keys per thread, u32 keys (0 = default)
   int tune_items8 = 0;              // radix keys per thread, u64 keys (0 = default)
-  int tune_tri_probe = 0;           // triangle membership test: 0/1 hash set, 2 binary search
+  int tune_tri_probe = 0;           // triangle membership test: 1 hash set, 0/2 binary search
+  int tune_bs_graph_rounds = 0;     // bit-row rounds per CUDA-graph replay (0 = 8)
+  int tune_bs_blocks = 0;           // resident round-kernel blocks per SM (0 = occupancy limit)
+  uint64_t tune_bs_budget_mb = 0;   // cap on a batch wave's device bytes, MiB (0 = 70% of free)
   bool profiling = false;
   uint64_t launches = 0;
   // Per-kernel CUDA-event accounting (enabled with profiling).
@@ -280,7 +283,8 @@ enum KernelId : int {
   K_RADIX_HIST = 5,
   K_TRI_COUNT = 6,
   K_EXPAND_DENSE = 7,
-  K_NUM = 8,
+  K_BS_ROUND = 8,
+  K_NUM = 9,
 };
 
 inline cudaEvent_t take_event(strata_ctx* ctx) {

@@ -327,6 +327,7 @@ constexpr double kDenseBudget = 16e9;
 inline bool want_dense(strata_ctx* ctx, bool trop, bool narrow, uint64_t n0, uint64_t n1) {
   const long double e = (long double)n0 * (long double)n1;
   const bool fits = (!trop || narrow) && e < 9.0e18L && dense_bytes(trop, (uint64_t)e) <= kDenseBudget;
+  if (ctx->plan == 3) fail(STRATA_E_UNSUPPORTED, "the bit-row plan applies to Bool transitive closure only");
   if (ctx->plan == 1) return false;
   if (ctx->plan == 2 && !fits)
     fail(STRATA_E_UNSUPPORTED, "the direct-addressed plan needs int32 weights and an index within 16 GB");
@@ -507,6 +508,27 @@ bool narrow_ok(uint64_t universe, uint64_t max_edge_w, uint64_t max_seed_w) {
   return bound < 2147483000.0L;
 }
 
+// Bool closure on bit rows (sk_bitset.cu); the result is compacted from the
+// final bit rows in (X, Z) order.
+template <class K>
+strata_rel* run_tc_bitset(strata_ctx* ctx, const EdgeCols& e, const Layout& L, strata_fix_stats* st, EventTimer& et,
+                          uint64_t l_start) {
+  Acct a;
+  Rel<K, int32_t> full;
+  full.k.ctx = full.w.ctx = ctx;
+  uint64_t rounds = 0, round_bytes = 0;
+  full.n = tc_bool_bitset<K>(ctx, e.src, e.dst, e.n, L.n_nodes_src, L.n_nodes, L.b1, full.k, &rounds, &round_bytes);
+  a.join_b = round_bytes;
+  const double ms = et.stop();
+  kprof_collect(ctx);
+  fill_stats(st, a, rounds, full.n, 0, L.b0 + L.b1, 0, ms, ctx->launches - l_start);
+  if (st) {
+    st->plan = 3;
+    st->join_ms = ms;
+  }
+  return finish_rel<K, int32_t, false>(ctx, full, L.b1);
+}
+
 }  // namespace
 
 strata_rel* fix_tc_bool(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats* st) {
@@ -519,6 +541,14 @@ strata_rel* fix_tc_bool(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats* st
     return rel;
   }
   const Layout L = tc_layout(ctx, e);
+  if (ctx->plan == 3 || ctx->plan == 0) {
+    const bool fits = tc_bool_bitset_fits(ctx, L.n_nodes_src, L.n_nodes, e.n);
+    if (ctx->plan == 3 && !fits) fail(STRATA_E_UNSUPPORTED, "the bit-row plan needs its bit matrices within 8 GB");
+    if (fits) {
+      if (!L.wide_key) return run_tc_bitset<uint32_t>(ctx, e, L, st, et, l_start);
+      return run_tc_bitset<uint64_t>(ctx, e, L, st, et, l_start);
+    }
+  }
   const bool dense = want_dense(ctx, false, true, L.n_nodes_src, L.n_nodes);
   if (!L.wide_key)
     return run_tc_shape<uint32_t, int32_t, false>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, 0, 0, st, et, l_start,

@@ -82,7 +82,10 @@ __global__ void __launch_bounds__(TC_NT)
   if (lane == 0 && count) atomicAdd(total, count);
 }
 
-// Hash-probe variant: the warp builds an open-addressing set of out(X) in
+// Hash-probe variant (STRATA_KNOB_TRI_PROBE = 1; measured slower than the
+// binary search on R-MAT-22, which stays the default: the 8 KB table per warp
+// cuts residency to 24 warps per SM and the probe loop diverges).  The warp
+// builds an open-addressing set of out(X) in
 // its shared-memory table (size the next power of two >= 2·d+(X), at most
 // TH_TAB, so at least half the slots stay empty and every probe chain ends at
 // an empty slot), then streams the successor lists of Y ∈ out(X) exactly as
@@ -325,7 +328,7 @@ uint64_t tri_from_sorted(strata_ctx* ctx, const K* keys, uint64_t m, int bits, u
   SK_CUDA(cudaMemsetAsync(acc.p, 0, 24, ctx->stream));
   const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(n_nodes, TC_WARPS), (uint64_t)ctx->num_sms * 8);
   const int kh = kprof_begin(ctx, K_TRI_COUNT);
-  if (ctx->tune_tri_probe == 2) {
+  if (ctx->tune_tri_probe != 1) {
     k_tri_count<<<grid ? grid : 1, TC_NT, 0, ctx->stream>>>(off.p, nbr.p, n_nodes,
                                                             reinterpret_cast<uint32_t*>(acc.p + 1),
                                                             reinterpret_cast<unsigned long long*>(acc.p));

@@ -7,7 +7,7 @@
 """
 from . import _lib  # noqa: F401
 from .gpu import (  # noqa: F401
-    POS_INF, BoolRelation, Cuda, DeviceRelation, Engine, GpuError, InvalidArgument,
+    POS_INF, BatchResult, BoolRelation, Cuda, DeviceRelation, Engine, GpuError, InvalidArgument,
     NegativeWeightCycle, NotBuilt, OutOfMemory, Timeout, TropOverflow, TropRelation, Unsupported,
     WeightRange, binary_plan_intermediate, count_4cliques, count_triangle_pattern, count_triangles,
     default_engine, intern_terms, mssp_trop, shortest_paths_trop, transitive_closure_bool,

@@ -26,11 +26,13 @@ E_UNSUPPORTED = 7
 E_NOT_BUILT = 8
 E_WEIGHT_RANGE = 9
 
-PLAN_AUTO, PLAN_SORT_MERGE, PLAN_DENSE = 0, 1, 2
+PLAN_AUTO, PLAN_SORT_MERGE, PLAN_DENSE, PLAN_BITS = 0, 1, 2, 3
 KNOB_SORT_ITEMS_U32, KNOB_SORT_ITEMS_U64, KNOB_TRI_PROBE = 1, 2, 3
+KNOB_BATCH_GRAPH_ROUNDS, KNOB_BATCH_BLOCKS_PER_SM, KNOB_BATCH_BUDGET_MB = 4, 5, 6
 
 KERNELS = {0: "k_onesweep", 1: "k_expand_emit", 2: "k_expand_offsets", 3: "k_reduce_runs",
-           4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count", 7: "k_expand_dense"}
+           4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count", 7: "k_expand_dense",
+           8: "k_bs_round"}
 
 STATUS_NAMES = {
     OK: "OK", E_INVALID: "INVALID", E_OOM: "OOM", E_CUDA: "CUDA", E_OVERFLOW: "OVERFLOW",
@@ -59,6 +61,19 @@ class FixStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class BatchStats(C.Structure):
+    """Mirror of ``strata_batch_stats``."""
+
+    _fields_ = [
+        ("instances", C.c_uint64), ("waves", C.c_uint64), ("graph_launches", C.c_uint64),
+        ("round_launches", C.c_uint64), ("rounds_max", C.c_uint64), ("result_tuples", C.c_uint64),
+        ("round_bytes", C.c_uint64), ("launches", C.c_uint64), ("device_ms", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 u8p = C.POINTER(C.c_uint8)
 u32p = C.POINTER(C.c_uint32)
 u64p = C.POINTER(C.c_uint64)
@@ -79,6 +94,10 @@ SIGNATURES = {
     "strata_ctx_set_profiling": (C.c_int, [ctxp, C.c_int]),
     "strata_ctx_set_plan": (C.c_int, [ctxp, C.c_int]),
     "strata_ctx_set_knob": (C.c_int, [ctxp, C.c_int, C.c_int]),
+    "strata_tc_bool_batch_dev": (C.c_int, [ctxp, C.c_uint32, u32p, u64p, vp, vp, C.c_int, u64p, u64p, u32p,
+                                           C.POINTER(BatchStats)]),
+    "strata_tc_bool_batch": (C.c_int, [ctxp, C.c_uint32, u32p, u64p, u32p, u32p, C.c_int, u64p, u64p, u32p,
+                                       C.POINTER(BatchStats)]),
     "strata_ctx_launches": (C.c_uint64, [ctxp]),
     "strata_ctx_kernel_stats": (C.c_int, [ctxp, C.c_int, u64p, C.POINTER(C.c_double), u64p]),
     "strata_ctx_reset_kernel_stats": (C.c_int, [ctxp]),

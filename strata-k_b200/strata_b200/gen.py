@@ -11,6 +11,9 @@
   pre-seeded symbols then the TSV cells row by row, column by column
   (strata-ir/src/dict.rs:35-43, strata-k/src/input.rs:109-149).
 * ``mssp_workload`` / ``tc_workload`` / ``triangle_workload`` — the configs.
+* ``batch_tc_workload`` — many independent directed ER instances (the
+  batched reachability config): node counts log-uniform, mean out-degree
+  uniform, each instance drawn from its own seed (seed, i).
 
 All randomness comes from ``numpy.random.default_rng(seed)`` (PCG64).
 """
@@ -149,3 +152,79 @@ def triangle_workload(scale=22, edge_factor=16, seed=3) -> Workload:
     x, y = orient_by_degree(lo, hi)
     _, (xi, yi), ns = intern_first_seen(x, y)
     return Workload(f"tri_rmat{scale}", xi, yi, n_symbols=ns, meta={"scale": scale, "edges": m, "seed": seed})
+
+
+@dataclass
+class BatchWorkload:
+    """Independent graphs: instance i has nodes [0, nodes[i]) and the edges
+    src/dst[edge_off[i]:edge_off[i+1]] (local ids, distinct, no self-loops)."""
+    name: str
+    nodes: np.ndarray     # u32 [n_inst]
+    edge_off: np.ndarray  # u64 [n_inst + 1]
+    src: np.ndarray       # u32 [sum m]
+    dst: np.ndarray       # u32 [sum m]
+    meta: dict | None = None
+
+    def __len__(self) -> int:
+        return len(self.nodes)
+
+    def instance(self, i: int) -> tuple[int, np.ndarray, np.ndarray]:
+        a, b = int(self.edge_off[i]), int(self.edge_off[i + 1])
+        return int(self.nodes[i]), self.src[a:b], self.dst[a:b]
+
+
+def _er_instance(n: int, m: int, rng) -> tuple[np.ndarray, np.ndarray]:
+    have = np.zeros(0, np.int64)
+    while len(have) < m:
+        need = int((m - len(have)) * 1.1) + 16
+        u = rng.integers(0, n, size=need, dtype=np.int64)
+        v = rng.integers(0, n, size=need, dtype=np.int64)
+        k = u * n + v
+        have = np.unique(np.concatenate([have, k[u != v]]))
+    k = have[rng.permutation(len(have))[:m]]
+    return (k // n).astype(np.uint32), (k % n).astype(np.uint32)
+
+
+def _batch_chunk(args):
+    seed, i0, i1, n_min, n_max, deg_min, deg_max = args
+    nodes, ms, srcs, dsts = [], [], [], []
+    for i in range(i0, i1):
+        rng = np.random.default_rng([seed, i])
+        n = int(round(float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))))
+        deg = float(rng.uniform(deg_min, deg_max))
+        m = min(int(round(n * deg)), n * (n - 1))
+        s_, d_ = _er_instance(n, m, rng)
+        nodes.append(n)
+        ms.append(m)
+        srcs.append(s_)
+        dsts.append(d_)
+    cat = (lambda xs: np.concatenate(xs) if xs else np.zeros(0, np.uint32))
+    return np.array(nodes, np.uint32), np.array(ms, np.uint64), cat(srcs), cat(dsts)
+
+
+def batch_tc_workload(n_inst=4096, n_min=100, n_max=50_000, deg_min=2.0, deg_max=8.0, seed=4,
+                      workers: int = 0) -> BatchWorkload:
+    """Instance i: n log-uniform in [n_min, n_max], mean out-degree uniform in
+    [deg_min, deg_max], m = round(n * degree) distinct directed non-loop edges
+    uniform over the n nodes; every draw of instance i comes from
+    default_rng([seed, i]), so the result does not depend on `workers`
+    (processes started with spawn; 0 = in this process)."""
+    step = 64
+    jobs = [(seed, a, min(a + step, n_inst), n_min, n_max, deg_min, deg_max) for a in range(0, n_inst, step)]
+    if workers > 1 and len(jobs) > 1:
+        import concurrent.futures as cf
+        import multiprocessing as mp
+        with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            parts = list(ex.map(_batch_chunk, jobs))
+    else:
+        parts = [_batch_chunk(j) for j in jobs]
+    nodes = np.concatenate([p[0] for p in parts]) if parts else np.zeros(0, np.uint32)
+    ms = np.concatenate([p[1] for p in parts]) if parts else np.zeros(0, np.uint64)
+    off = np.zeros(n_inst + 1, np.uint64)
+    off[1:] = np.cumsum(ms)
+    src = np.concatenate([p[2] for p in parts]) if parts else np.zeros(0, np.uint32)
+    dst = np.concatenate([p[3] for p in parts]) if parts else np.zeros(0, np.uint32)
+    return BatchWorkload(f"batch_tc_{n_inst}x_er_{n_min}_{n_max}", nodes, off, src, dst,
+                         meta={"instances": n_inst, "n_min": n_min, "n_max": n_max, "deg_min": deg_min,
+                               "deg_max": deg_max, "seed": seed, "edges": int(off[-1]),
+                               "sum_n2": float((nodes.astype(np.float64) ** 2).sum())})

@@ -215,7 +215,8 @@ class Engine:
         self._check(self.lib.strata_ctx_set_stream(self.ctx, C.c_void_p(stream_handle or 0)))
 
     def set_plan(self, plan: int):
-        """0 automatic, 1 sort-merge, 2 direct-addressed (results are identical)."""
+        """0 automatic, 1 sort-merge, 2 direct-addressed, 3 bit rows (Bool closure only);
+        results are identical."""
         self._check(self.lib.strata_ctx_set_plan(self.ctx, plan))
 
     def set_knob(self, knob: int, value: int):
@@ -348,6 +349,37 @@ class Engine:
             _dp(ew), _dp(einf), ne, C.byref(rel), C.byref(st)))
         return DeviceRelation(self, rel, st.as_dict())
 
+    # -- batched Bool reachability ---------------------------------------
+    def tc_bool_batch(self, nodes, edge_off, src, dst, mode: int = 0) -> "BatchResult":
+        """Closures of many independent graphs (instance i: nodes [0, nodes[i]),
+        edges src/dst[edge_off[i]:edge_off[i+1]]), summarised per instance by
+        |path|, Σ mix64(X)·c^Z and the round count.  ``src``/``dst`` may be
+        host arrays or device tensors.  mode 0 batched (graph-replayed
+        persistent rounds), 1 one instance per launch."""
+        nd = np.ascontiguousarray(nodes, dtype=np.uint32)
+        eo = np.ascontiguousarray(edge_off, dtype=np.uint64)
+        n_inst = len(nd)
+        if len(eo) != n_inst + 1:
+            raise InvalidArgument("edge_off needs one more entry than nodes")
+        m = int(eo[-1]) if n_inst else 0
+        if _len(src) != m or _len(dst) != m:
+            raise InvalidArgument("src and dst must hold edge_off[-1] edges")
+        counts = np.zeros(n_inst, np.uint64)
+        fps = np.zeros(n_inst, np.uint64)
+        rounds = np.zeros(n_inst, np.uint32)
+        st = L.BatchStats()
+        if hasattr(src, "data_ptr"):
+            self._check(self.lib.strata_tc_bool_batch_dev(
+                self.ctx, n_inst, _ptr(nd, C.c_uint32), _ptr(eo, C.c_uint64), _dp(src), _dp(dst), mode,
+                _ptr(counts, C.c_uint64), _ptr(fps, C.c_uint64), _ptr(rounds, C.c_uint32), C.byref(st)))
+        else:
+            s_, d_ = _u32(src), _u32(dst)
+            self._check(self.lib.strata_tc_bool_batch(
+                self.ctx, n_inst, _ptr(nd, C.c_uint32), _ptr(eo, C.c_uint64), _ptr(s_, C.c_uint32),
+                _ptr(d_, C.c_uint32), mode, _ptr(counts, C.c_uint64), _ptr(fps, C.c_uint64),
+                _ptr(rounds, C.c_uint32), C.byref(st)))
+        return BatchResult(counts, fps, rounds, st.as_dict())
+
     def count_triangle_pattern_dev(self, x, y, n=None) -> int:
         n = _len(x) if n is None else n
         out = C.c_uint64()
@@ -366,6 +398,16 @@ def _dp(t) -> C.c_void_p | None:
 
 def _len(t) -> int:
     return int(t.numel()) if hasattr(t, "numel") else len(t)
+
+
+class BatchResult:
+    """Per-instance closure summaries of a batched call."""
+
+    def __init__(self, counts, fps, rounds, stats):
+        self.counts, self.fps, self.rounds, self.stats = counts, fps, rounds, stats
+
+    def __len__(self) -> int:
+        return len(self.counts)
 
 
 class DeviceRelation:

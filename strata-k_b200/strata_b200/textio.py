@@ -131,3 +131,41 @@ def render_db(relations: dict, dictionary: SymbolDict, queries=None) -> str:
         cols, w, inf = relations[name]
         lines += render_relation(name, cols, dictionary, w, inf, queries)
     return "".join(l + "\n" for l in lines)
+
+
+def render_f64(x: float) -> str:
+    """A float as the reference prints one (Rust's `{}` for f64): the shortest
+    decimal that reads back to the same double, positional (no exponent),
+    integral values without a fraction (`1`, `0`, `-0`)."""
+    import math
+    from decimal import Decimal
+    x = float(x)
+    if math.isnan(x):
+        return "NaN"
+    if math.isinf(x):
+        return "inf" if x > 0 else "-inf"
+    if x == 0.0:
+        return "-0" if math.copysign(1.0, x) < 0 else "0"
+    r = repr(x)
+    if "e" in r or "E" in r:
+        r = format(Decimal(r), "f")
+    if r.endswith(".0"):
+        r = r[:-2]
+    return r
+
+
+def prob_line(p: float, pred: str, args: list[str], top_k: int | None = None) -> str:
+    """`p :: pred(a, b)` — and for a Prov_k predicate the declared lower bound
+    marker (strata-cli/src/prov.rs:64-82, render.rs:10)."""
+    s = f"{render_f64(p)} :: {pred}({', '.join(args)})"
+    if top_k is not None:
+        s += f"  (lower bound, top-{top_k})"
+    return s + "\n"
+
+
+def grad_line(fact_p: float, pred: str, args: list[str], g: float, model: str | None = None) -> str:
+    """One `?grad` line per probabilistic fact (strata-cli/src/prob.rs:174-189)."""
+    s = f"  ∂/∂[{render_f64(fact_p)} :: {pred}({', '.join(args)})] = {render_f64(g)}"
+    if model is not None:
+        s += f'  (→ model "{model}")'
+    return s + "\n"

@@ -17,9 +17,15 @@ import os
 from pathlib import Path
 
 KNOBS = {
-    # knob id: (key bytes, choices, significant key bits of the probe)
+    # radix tile keys per thread — knob id: (key bytes, choices, significant key bits of the probe)
     1: (4, (11, 15, 19, 23), 26),
     2: (8, (7, 9, 13), 40),
+}
+# other knobs: id -> choices (0 = the built-in default)
+OTHER = {
+    3: (1, 2),                # triangle membership test: hash set / binary search
+    4: (2, 4, 8, 16, 32),     # bit-row rounds per CUDA-graph replay (batched closure)
+    5: (0, 2, 4, 8),          # resident round-kernel blocks per SM (0 = occupancy limit)
 }
 
 
@@ -59,24 +65,66 @@ def _time_sort(eng, torch, n: int, key_bytes: int, bits: int, reps: int = 5) -> 
     return e0.elapsed_time(e1) / reps
 
 
-def sweep(n: int = 64_000_000, verbose: bool = True) -> dict:
+def _time_call(torch, fn, reps: int = 3) -> float:
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for _ in range(reps):
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def sweep(n: int = 64_000_000, verbose: bool = True, batch_instances: int = 512) -> dict:
     """Time every choice of every knob; return {knob: best value} plus timings."""
+    import numpy as np
     import torch
 
+    from . import gen
     from .gpu import Engine
     eng = Engine(0)
     best, timings = {}, {}
+
+    def record(knob, res):
+        best[knob] = min(res, key=res.get)
+        timings[knob] = res
+        if verbose:
+            for v, t in res.items():
+                print(f"knob {knob} = {v}: {t:.3f} ms")
+
     try:
         for knob, (kb, choices, bits) in KNOBS.items():
             res = {}
             for v in choices:
                 eng.set_knob(knob, v)
                 res[v] = _time_sort(eng, torch, n if kb == 4 else n // 2, kb, bits)
-                if verbose:
-                    print(f"knob {knob} = {v}: {res[v]:.3f} ms")
             eng.set_knob(knob, 0)
-            best[knob] = min(res, key=res.get)
-            timings[knob] = res
+            record(knob, res)
+        # triangle probe on an oriented R-MAT graph
+        tw = gen.triangle_workload(scale=18, seed=7)
+        tx = torch.from_numpy(tw.src.astype(np.int32)).cuda()
+        ty = torch.from_numpy(tw.dst.astype(np.int32)).cuda()
+        res = {}
+        for v in OTHER[3]:
+            eng.set_knob(3, v)
+            res[v] = _time_call(torch, lambda: eng.count_triangle_pattern_dev(tx, ty))
+        eng.set_knob(3, 0)
+        record(3, res)
+        # batched closure knobs on a mixed-size batch
+        bw = gen.batch_tc_workload(n_inst=batch_instances, n_min=100, n_max=20_000, seed=9)
+        bs = torch.from_numpy(bw.src.astype(np.int32)).cuda()
+        bd = torch.from_numpy(bw.dst.astype(np.int32)).cuda()
+        for knob in (4, 5):
+            res = {}
+            for v in OTHER[knob]:
+                eng.set_knob(knob, v)
+                res[v] = _time_call(torch, lambda: eng.tc_bool_batch(bw.nodes, bw.edge_off, bs, bd, mode=0), reps=2)
+            eng.set_knob(knob, 0)
+            record(knob, res)
     finally:
         eng.close()
     return {"gpu": _gpu_name(), "best": best, "timings_ms": timings, "n": n}
@@ -109,7 +157,7 @@ def load(path: Path | None = None, gpu: str | None = None) -> dict:
     out = {}
     for k, v in entry.items():
         k, v = int(k), int(v)
-        if k in KNOBS and v in KNOBS[k][1]:
+        if (k in KNOBS and v in KNOBS[k][1]) or (k in OTHER and v in OTHER[k]):
             out[k] = v
     return out
 

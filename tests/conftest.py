@@ -49,3 +49,12 @@ def peng(request, engine):
     engine.set_plan(request.param)
     yield engine
     engine.set_plan(0)
+
+
+@pytest.fixture(params=[0, 1, 2], ids=["auto-bitrows", "sortmerge", "dense"])
+def tceng(request, engine):
+    """Bool closure under every plan that applies to it: automatic (bit rows at
+    these sizes), sort-merge and direct-addressed; results must be identical."""
+    engine.set_plan(request.param)
+    yield engine
+    engine.set_plan(0)

@@ -1,0 +1,126 @@
+"""Batched Bool reachability and the bit-row closure plan against the oracle.
+
+Every instance's |path| and row-polynomial fingerprint must equal the SCC
+oracle's, and its round count the semi-naive restatement's (the reference's
+`run_semi_naive` schedule, strata-eval/src/seminaive.rs:29-106)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import strata_b200 as S
+from strata_b200 import gen
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(res, wl, rounds_sample=16):
+    counts, fps = O.closure_batch(wl.nodes, wl.edge_off, wl.src, wl.dst, threads=8)
+    assert np.array_equal(res.counts, counts)
+    assert np.array_equal(res.fps, fps)
+    for i in range(min(rounds_sample, len(wl))):
+        n, s, d = wl.instance(i)
+        if len(s):
+            _, _, r = O.fast_tc(s, d)
+            assert int(res.rounds[i]) == r, i
+        else:
+            assert int(res.rounds[i]) == 0
+
+
+def test_batch_matches_oracle(engine):
+    wl = gen.batch_tc_workload(n_inst=384, n_min=20, n_max=3000, seed=21)
+    res = engine.tc_bool_batch(wl.nodes, wl.edge_off, wl.src, wl.dst, mode=0)
+    _check(res, wl)
+    assert res.stats["instances"] == 384 and res.stats["graph_launches"] >= 1
+    assert res.stats["result_tuples"] == int(res.counts.sum())
+
+
+def test_batch_large_instances(engine):
+    """Rows wider than a warp's 32 × 128 bits (lanes loop over chunks)."""
+    wl = gen.batch_tc_workload(n_inst=5, n_min=9000, n_max=50_000, deg_min=1.5, deg_max=3.0, seed=5)
+    res = engine.tc_bool_batch(wl.nodes, wl.edge_off, wl.src, wl.dst, mode=0)
+    _check(res, wl, rounds_sample=2)
+
+
+def test_batch_one_per_launch_agrees(engine):
+    wl = gen.batch_tc_workload(n_inst=64, n_min=50, n_max=2000, seed=22)
+    a = engine.tc_bool_batch(wl.nodes, wl.edge_off, wl.src, wl.dst, mode=0)
+    b = engine.tc_bool_batch(wl.nodes, wl.edge_off, wl.src, wl.dst, mode=1)
+    assert np.array_equal(a.counts, b.counts) and np.array_equal(a.fps, b.fps)
+    assert np.array_equal(a.rounds, b.rounds)
+    assert b.stats["graph_launches"] == 0 and b.stats["waves"] == 64
+
+
+@pytest.mark.parametrize("knob,value", [(4, 2), (4, 32), (5, 1), (6, 1)])
+def test_batch_knobs_identical(engine, knob, value):
+    """Graph rounds, resident blocks and a 1 MiB wave budget (many waves)
+    change speed only."""
+    wl = gen.batch_tc_workload(n_inst=96, n_min=30, n_max=1500, seed=23)
+    base = engine.tc_bool_batch(wl.nodes, wl.edge_off, wl.src, wl.dst, mode=0)
+    engine.set_knob(knob, value)
+    try:
+        got = engine.tc_bool_batch(wl.nodes, wl.edge_off, wl.src, wl.dst, mode=0)
+    finally:
+        engine.set_knob(knob, 0)
+    assert np.array_equal(base.counts, got.counts) and np.array_equal(base.fps, got.fps)
+    assert np.array_equal(base.rounds, got.rounds)
+    if knob == 6:
+        assert got.stats["waves"] > 1
+
+
+def test_batch_edge_cases(engine):
+    """Empty instances, one node, self-loops, duplicate edges, a cycle (n^2
+    pairs), a chain (n(n-1)/2 pairs, n-1 rounds)."""
+    inst = [
+        (1, [], []),
+        (7, [], []),
+        (1, [0], [0]),
+        (3, [0, 0, 1], [1, 1, 2]),
+        (200, list(range(200)), [(i + 1) % 200 for i in range(200)]),
+        (300, list(range(299)), list(range(1, 300))),
+        (129, [0, 128, 64], [128, 64, 0]),
+    ]
+    nodes = np.array([n for n, _, _ in inst], np.uint32)
+    off = np.zeros(len(inst) + 1, np.uint64)
+    for i, (_, s, _) in enumerate(inst):
+        off[i + 1] = off[i] + len(s)
+    src = np.array([x for _, s, _ in inst for x in s], np.uint32)
+    dst = np.array([x for _, _, d in inst for x in d], np.uint32)
+    wl = gen.BatchWorkload("edge", nodes, off, src, dst)
+    res = engine.tc_bool_batch(nodes, off, src, dst, mode=0)
+    _check(res, wl, rounds_sample=len(inst))
+    assert res.counts.tolist()[:6] == [0, 0, 1, 3, 200 * 200, 300 * 299 // 2]
+    assert int(res.rounds[5]) == 299
+
+
+def test_batch_rejects_ids_outside_instance(engine):
+    with pytest.raises(S.InvalidArgument):
+        engine.tc_bool_batch([3, 3], [0, 1, 2], [0, 1], [1, 3])
+    with pytest.raises(S.InvalidArgument):
+        engine.tc_bool_batch([3], [0, 5], [0, 1], [1, 2])
+
+
+def test_batch_device_inputs(engine):
+    import torch
+    wl = gen.batch_tc_workload(n_inst=40, n_min=20, n_max=800, seed=24)
+    ds = torch.from_numpy(wl.src.astype(np.int32)).cuda()
+    dd = torch.from_numpy(wl.dst.astype(np.int32)).cuda()
+    res = engine.tc_bool_batch(wl.nodes, wl.edge_off, ds, dd, mode=0)
+    _check(res, wl, rounds_sample=4)
+
+
+def test_bit_row_plan_selected_and_exclusive(engine):
+    """Automatic planning uses bit rows for Bool closure; forcing them on a
+    tropical program is an error, and forcing them on closure is exact."""
+    s, d = gen.er_directed(3000, 9000, 31)
+    a, b, r = O.fast_tc(s, d)
+    got = engine.transitive_closure_bool((s, d))
+    assert got.stats["plan"] == 3 and got.stats["rounds"] == r
+    assert np.array_equal(got.src, a) and np.array_equal(got.dst, b)
+    engine.set_plan(3)
+    try:
+        got3 = engine.transitive_closure_bool((s, d))
+        assert np.array_equal(got3.src, a) and np.array_equal(got3.dst, b)
+        with pytest.raises(S.Unsupported):
+            engine.shortest_paths_trop([(0, 1, 1), (1, 2, 1)])
+    finally:
+        engine.set_plan(0)

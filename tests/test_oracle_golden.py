@@ -357,3 +357,144 @@ def test_naive_equals_semi_naive_fuzz():
         except O.OracleError as e:
             b, eb = None, e.kind
         assert (a, ea) == (b, eb), seed
+
+
+def test_closure_count_fp_matches_tuples(lcg):
+    """The batched-reachability summary oracle (SCC + DAG closure, count and
+    row-polynomial fingerprint) agrees with the reference's set fixpoint
+    (strata-gpu/tests/tc_diff.rs:12-29) and the interpreter-shaped fast TC."""
+    rng = lcg(0xC10541)
+    for trial in range(120):
+        n = 2 + rng.upto(40)
+        m = rng.upto(3 * n)
+        edges = sorted({(rng.upto(n), rng.upto(n)) for _ in range(m)})
+        s = np.array([e[0] for e in edges], np.uint32)
+        d = np.array([e[1] for e in edges], np.uint32)
+        want = _set_fixpoint(edges) if edges else []
+        wx = np.array([t[0] for t in want], np.uint64)
+        wz = np.array([t[1] for t in want], np.int64)
+        got = O.closure_count_fp(n, s, d)
+        assert got == (len(want), O.poly_fingerprint(wx, wz, n)), trial
+        if edges:
+            fx, fz, _ = O.fast_tc(s, d)
+            assert (len(fx), O.poly_fingerprint(fx, fz.astype(np.int64), n)) == got
+
+
+def test_closure_count_closed_forms():
+    """Chain of n nodes: n(n-1)/2 pairs (tc_diff.rs:86-102); a cycle: n^2."""
+    for n in (2, 17, 400):
+        s = np.arange(n - 1, dtype=np.uint32)
+        assert O.closure_count_fp(n, s, s + 1)[0] == n * (n - 1) // 2
+        c = np.arange(n, dtype=np.uint32)
+        assert O.closure_count_fp(n, c, (c + 1) % n)[0] == n * n
+
+
+def test_closure_batch_equals_per_instance():
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "strata-k_b200"))
+    from strata_b200 import gen
+    wl = gen.batch_tc_workload(n_inst=48, n_min=20, n_max=600, seed=11)
+    counts, fps = O.closure_batch(wl.nodes, wl.edge_off, wl.src, wl.dst, threads=4)
+    for i in range(len(wl)):
+        n, s, d = wl.instance(i)
+        assert (int(counts[i]), int(fps[i])) == O.closure_count_fp(n, s, d)
+        if i < 6:
+            fx, fz, _ = O.fast_tc(s, d)
+            assert int(counts[i]) == len(fx)
+            assert int(fps[i]) == O.poly_fingerprint(fx, fz.astype(np.int64), n)
+
+
+def _aml_program(fx):
+    """The AML workload program (examples/workloads/aml/aml.strata) over its
+    TSV inputs: symbols interned first-seen — the query constants at check
+    time, then the inputs in declaration order (strata-check/src/lib.rs:863-870,
+    strata-k/src/input.rs:109-149); flags are the probabilistic leaves in row
+    order."""
+    from strata_b200.textio import SymbolDict
+    d = SymbolDict()
+    for _, c in fx["queries"]:
+        d.intern(c)
+    p = (O.Prog().pred("entity", 1).pred("owns", 2).pred("sanctioned", 1).pred("flag", 1)
+         .pred("control", 2).pred("investigate", 1).pred("cleared", 1, stratum=1))
+    p.rule(("control", ["X", "Y"]), ("owns", ["X", "Y"]))
+    p.rule(("control", ["X", "Z"]), ("owns", ["X", "Y"]), ("control", ["Y", "Z"]))
+    p.rule(("investigate", ["X"]), ("flag", ["X"]))
+    p.rule(("investigate", ["X"]), ("control", ["X", "Y"]), ("flag", ["Y"]))
+    p.rule(("investigate", ["X"]), ("control", ["Y", "X"]), ("sanctioned", ["Y"]))
+    p.rule(("cleared", ["X"]), ("entity", ["X"]), ("not", "investigate", ["X"]))
+    for name in ("entity", "owns", "sanctioned"):
+        for row in fx[name]:
+            p.fact(name, [d.intern(v) for v in row])
+    probs, flags = [], []
+    for row in fx["flag"]:
+        p.fact("flag", [d.intern(row[0])], O.PROB)
+        probs.append(float(row[1]))
+        flags.append(row)
+    return p, d, probs, flags
+
+
+def test_aml_workload_pinned_lines():
+    """Provenance capture (Prov_k(4) with stratified negation over soft
+    evidence), exact compilation and the gradient reproduce the reference
+    CLI's pinned AML lines (crates/strata-cli/tests/workloads.rs:17-23)."""
+    from strata_b200.textio import grad_line, prob_line
+    fx = json.loads((GOLDEN / "aml.json").read_text())
+    p, d, probs, flags = _aml_program(fx)
+    db = O.ProvDb(p, probs, {"investigate": 4, "cleared": 4})
+    lines = []
+    for pred, c in fx["queries"]:
+        proofs = db.proofs(pred, [d.get(c)])
+        pr, g, _ = O.compile_grad(proofs, probs)
+        lines.append(prob_line(pr, pred, [c], top_k=4).rstrip("\n"))
+        if pred == "investigate":
+            for (name, fp), gv in zip(flags, g):
+                lines.append(grad_line(float(fp), "flag", [name], gv, model="aml_gnn").rstrip("\n"))
+    for want in fx["pinned"]:
+        assert want in lines, (want, lines)
+
+
+def test_prov_facade_and_bridge_values():
+    """path over {a->c, a->b, b->c}: 0.625 and d/d(direct) = 0.75
+    (strata-k/tests/facade.rs:38-52); owns acme->shell->target with a direct
+    0.3 stake: 0.804 (facade.rs:56-76); the DIAMOND 0.86 and dP/dp(ac) = 0.28
+    (strata-py/tests/test_bridge.py:42-54) — as Prov captures of path."""
+    def run(edges):
+        p = O.Prog().pred("edge", 2).pred("path", 2)
+        p.rule(("path", ["X", "Y"]), ("edge", ["X", "Y"]))
+        p.rule(("path", ["X", "Z"]), ("edge", ["X", "Y"]), ("path", ["Y", "Z"]))
+        for a, b, _ in edges:
+            p.fact("edge", [a, b], O.PROB)
+        db = O.ProvDb(p, [w for _, _, w in edges], {"path": 0})
+        return O.compile_grad(db.proofs("path", [0, 2]), [w for _, _, w in edges])
+    pr, g, _ = run([(0, 2, 0.5), (0, 1, 0.5), (1, 2, 0.5)])
+    assert abs(pr - 0.625) < 1e-12 and abs(g[0] - 0.75) < 1e-12
+    pr, _, _ = run([(0, 1, 0.9), (1, 2, 0.8), (0, 2, 0.3)])
+    assert abs(pr - 0.804) < 1e-12
+    pr, g, _ = run([(0, 1, 0.9), (1, 2, 0.8), (0, 2, 0.5)])
+    assert pr == pytest.approx(0.86) and g[2] == pytest.approx(0.28)
+
+
+def test_prov_tc_fast_matches_interpreter_capture():
+    """The target-restricted TC-shaped Prov_k capture equals the interpreter's
+    full capture (provenance.rs:286-362) on random graphs, for every k."""
+    rng = np.random.default_rng(5)
+    for trial in range(30):
+        n = int(rng.integers(3, 12))
+        m = int(rng.integers(1, 3 * n))
+        src = rng.integers(0, n, m)
+        dst = rng.integers(0, n, m)
+        probs = rng.uniform(0.05, 0.95, m)
+        k = int(rng.integers(1, 5))
+        p = O.Prog().pred("edge", 2).pred("path", 2)
+        p.rule(("path", ["X", "Y"]), ("edge", ["X", "Y"]))
+        p.rule(("path", ["X", "Z"]), ("edge", ["X", "Y"]), ("path", ["Y", "Z"]))
+        for a, b in zip(src, dst):
+            p.fact("edge", [int(a), int(b)], O.PROB)
+        db = O.ProvDb(p, probs, {"path": k})
+        rel = db.relation("path")
+        qs = np.repeat(np.arange(n), n)
+        qt = np.tile(np.arange(n), n)
+        got, _ = O.prov_tc(n, src, dst, probs, k, qs, qt, threads=2)
+        for q in range(len(qs)):
+            want = rel.get((int(qs[q]), int(qt[q])), [])
+            assert got[q] == want, (trial, qs[q], qt[q])
