@@ -47,10 +47,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["mssp", "tc", "tri", "batch"], default="mssp",
+    ap.add_argument("--workload", choices=["mssp", "tc", "tri", "batch", "prov"], default="mssp",
                     help="mssp: the headline Trop program; tc / tri / batch: the Bool closure, triangle-count "
                          "and batched-reachability configs")
     ap.add_argument("--instances", type=int, default=4096, help="batch: number of instances")
+    ap.add_argument("--queries", type=int, default=1024, help="prov: number of ?grad query pairs")
     ap.add_argument("--plan", choices=["auto", "sort-merge", "dense"], default="auto")
     ap.add_argument("--tuned", action="store_true", help="apply the autotuner's cached knob values")
     ap.add_argument("--scale", type=int, default=None, help="R-MAT scale (mssp: 20, tri: 22)")
@@ -78,6 +79,8 @@ def workload_for(rank: int, scale: int, n_sources: int, kind: str = "mssp"):
         return gen.tc_workload(seed=1 + 1000 * rank)
     if kind == "tri":
         return gen.triangle_workload(scale=scale, seed=3 + 1000 * rank)
+    if kind == "prov":
+        return gen.prov_workload(n_queries=n_sources, seed=5 + 1000 * rank)
     if kind == "batch":
         return gen.batch_tc_workload(n_inst=n_sources, seed=4 + 1000 * rank, workers=min(16, os.cpu_count() or 1))
     return gen.mssp_workload(scale=scale, n_sources=n_sources, seed=2 + 1000 * rank)
@@ -86,11 +89,20 @@ def workload_for(rank: int, scale: int, n_sources: int, kind: str = "mssp"):
 PLANS = {"auto": 0, "sort-merge": 1, "dense": 2}
 
 
+def units_arg(args) -> int:
+    return {"batch": args.instances, "prov": args.queries}.get(args.workload, args.sources)
+
+
+def unit_for(kind: str) -> str:
+    return "queries/s" if kind == "prov" else UNIT
+
+
 def metric_for(kind: str) -> str:
     return {"mssp": METRIC,
             "tc": "derived tuples/s (Bool transitive-closure fixpoint, |path| / device time)",
             "tri": "derived tuples/s (WCOJ triangle pattern count, triangles / device time)",
-            "batch": "derived tuples/s (batched Bool reachability, sum of |path| over instances / device time)"}[kind]
+            "batch": "derived tuples/s (batched Bool reachability, sum of |path| over instances / device time)",
+            "prov": "?grad/s (Prov_k(8) capture + exact circuits + FP32 forward/adjoint, queries / time)"}[kind]
 
 
 def config(args, world):
@@ -100,6 +112,12 @@ def config(args, world):
         return {"workload": "bool_tc_er_10000n_50000e",
                 "program": "path(X,Y) :- edge(X,Y). path(X,Z) :- edge(X,Y), path(Y,Z).",
                 "graph": "Erdos-Renyi directed, 10,000 nodes, 50,000 distinct edges, no self-loops", **common}
+    if args.workload == "prov":
+        return {"workload": f"prov_reach_er_20000n_80000e_{args.queries}q_k8",
+                "program": "path(X,Y) :- edge(X,Y). path(X,Z) :- edge(X,Y), path(Y,Z). (path: Prov_k(8), "
+                           "edge: probabilistic)",
+                "graph": "Erdos-Renyi directed, 20,000 nodes, 80,000 edges, p ~ Beta(2,5) as fp32",
+                "queries": args.queries, **common}
     if args.workload == "batch":
         return {"workload": f"batch_tc_{args.instances}x_er_n100_50000_deg2_8",
                 "program": "path(X,Y) :- edge(X,Y). path(X,Z) :- edge(X,Y), path(Y,Z). (per instance)",
@@ -197,6 +215,25 @@ def cpu_sample(kind: str, wl, threads: int, steps: int):
         prog = O.tc_program(wl.src, wl.dst)
         head, rounds = "path", 2
         sample = "bootstrap plus the first 2 delta rounds of the closure on the full graph"
+    elif kind == "prov":
+        # the FP64 restatement: capture for the first queries' targets, then
+        # compile + gradient per query, until ~10 s
+        import time as _t
+        t0 = _t.time()
+        done = 0
+        for q0 in range(0, len(wl.qs), 4):
+            qs, qt = wl.qs[q0:q0 + 4], wl.qt[q0:q0 + 4]
+            proofs, _ = O.prov_tc(wl.n, wl.src, wl.dst, wl.p64, 8, qs, qt, threads=threads)
+            for pr in proofs:
+                O.compile_grad(pr, wl.p64)
+            done += len(qs)
+            if _t.time() - t0 > 10.0:
+                break
+        secs = _t.time() - t0
+        rate = done / secs
+        sample = (f"Prov_k(8) capture (target-restricted naive rounds) + exact compilation + FP64 gradient "
+                  f"for {done} of {len(wl.qs)} queries")
+        return [rate] * steps, [secs] * steps, done, sample
     elif kind == "batch":
         # the interpreter on whole instances, smallest first, until ~10 s
         t_tup, t_sec, k = 0, 0.0, 0
@@ -237,20 +274,20 @@ def run_reference(args):
     if rank != 0:
         return 0
     cores = os.cpu_count() or 1
-    wl = workload_for(0, args.scale, args.instances if args.workload == "batch" else args.sources, args.workload)
+    wl = workload_for(0, args.scale, units_arg(args), args.workload)
     t0 = time.time()
     rates, secs, tup, sample = cpu_sample(args.workload, wl, cores, args.warmup + args.steps)
     timed = secs[args.warmup:]
     value = tup * len(timed) / sum(timed) if sum(timed) > 0 else 0.0
     sample = f"{sample}; {tup} tuples per step"
     line = {
-        "impl": "reference", "metric": metric_for(args.workload), "value": value, "unit": UNIT, "n_gpus": world,
+        "impl": "reference", "metric": metric_for(args.workload), "value": value, "unit": unit_for(args.workload), "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(timed) / max(1, len(timed)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "int64" if args.workload == "mssp" else "u32",
+        "dtype": {"mssp": "int64", "prov": "f64"}.get(args.workload, "u32"),
         "data": "synthetic", "config": config(args, world),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": unit_for(args.workload), "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": unit_for(args.workload), "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.time() - t0,
     }
     print(json.dumps(line), flush=True)
@@ -268,6 +305,12 @@ class Job:
         self.kind, self.wl, self.eng, self.torch = kind, wl, eng, torch
         i32, i64 = np.int32, np.int64
         self.mode = 0
+        if kind == "prov":
+            cols = (("src", wl.src, i32), ("dst", wl.dst, i32), ("p64", wl.p64, np.float64),
+                    ("p32", wl.p32, np.float32))
+            self.host = {k: torch.from_numpy(np.ascontiguousarray(v).astype(dt)).pin_memory() for k, v, dt in cols}
+            self.entry = "strata_prov_tc_capture + strata_circuits_compile/forward/grads"
+            return
         if kind == "mssp":
             cols = (("sources", wl.sources, i32), ("sw", wl.source_w, i64), ("src", wl.src, i32),
                     ("dst", wl.dst, i32), ("w", wl.w, i64))
@@ -283,6 +326,20 @@ class Job:
             rel = self.eng.mssp_dev(d["sources"], d["src"], d["dst"], d["w"], source_weights=d["sw"])
         elif self.kind == "tc":
             rel = self.eng.tc_bool_dev(d["src"], d["dst"])
+        elif self.kind == "prov":
+            t0 = time.perf_counter()
+            pr = self.eng.prov_capture(self.wl.n, d["src"], d["dst"], d["p64"], self.wl.qs, self.wl.qt, k=8)
+            t1 = time.perf_counter()
+            circ = self.eng.compile_circuits(pr, len(self.wl.src))
+            t2 = time.perf_counter()
+            P = circ.forward(d["p32"])
+            G = circ.grads(d["p32"])
+            self.torch.cuda.current_stream().synchronize()
+            self.last = (P, G)
+            nodes, levels = circ.shape()
+            return circ, len(self.wl.qs), {"prov": pr.stats, "capture_s": t1 - t0, "compile_s": t2 - t1,
+                                           "circuit_nodes": nodes, "circuit_levels": levels,
+                                           "proofs": int(pr.proof_off[-1])}
         elif self.kind == "batch":
             res = self.eng.tc_bool_batch(self.wl.nodes, self.wl.edge_off, d["src"], d["dst"], mode=self.mode)
             return None, int(res.counts.sum()), {"batch": res.stats}
@@ -297,7 +354,7 @@ class Job:
 
     def out_buffers(self, n):
         torch = self.torch
-        if self.kind in ("tri", "batch"):
+        if self.kind in ("tri", "batch", "prov"):
             return None
         trop = self.kind == "mssp"
         return (torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
@@ -311,6 +368,11 @@ class Job:
             return 8  # the u64 count, returned through the entry point's out-parameter
         if self.kind == "batch":
             return len(self.wl) * (8 + 8 + 4)  # per-instance count, fingerprint, rounds
+        if self.kind == "prov":
+            P, G = self.last
+            P.cpu()
+            G.cpu()
+            return P.numel() * P.element_size() + G.numel() * G.element_size()
         res = handle.to_host(out=out)
         assert len(res) == tuples
         return tuples * (4 + 4 + (8 + 1 if self.kind == "mssp" else 0))
@@ -352,7 +414,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
-    wl = workload_for(rank, args.scale, args.instances if args.workload == "batch" else args.sources, args.workload)
+    wl = workload_for(rank, args.scale, units_arg(args), args.workload)
     eng = S.Engine(local, tuned=args.tuned)
     eng.set_plan(PLANS[args.plan])
     stream = torch.cuda.Stream()
@@ -449,7 +511,7 @@ def run_ours(args):
             t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
             pg.all_reduce(t, op=pg.ReduceOp.MAX)
             e2e_val = all_tuples * args.steps / (float(t[0]) / 1000.0)
-        e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": e2e_val, "unit": unit_for(args.workload), "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
                "path": f"pinned host columns -> torch H2D -> {job.entry}"
                        + (" (count out-parameter)" if args.workload == "tri" else " -> strata_rel_to_host (pinned)")}
@@ -475,13 +537,13 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         rates, secs, tup, sample = cpu_sample(args.workload, wl, cores, 1)
-        cpu = {"value": rates[-1], "unit": UNIT, "cores": cores, "kind": "port",
+        cpu = {"value": rates[-1], "unit": unit_for(args.workload), "cores": cores, "kind": "port",
                "sample": f"{sample}: {tup} tuples in {secs[-1]:.2f} s"}
 
     if rank == 0:
         wb = stats.get("weight_bytes", 0) if stats else 0
         line = {
-            "metric": metric_for(args.workload), "value": value, "unit": UNIT, "n_gpus": world,
+            "metric": metric_for(args.workload), "value": value, "unit": unit_for(args.workload), "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": {4: "int32", 8: "int64"}.get(wb, "u32"),
@@ -489,7 +551,12 @@ def run_ours(args):
             "tuples_per_step": int(all_tuples),
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
         }
-        if stats and "batch" in stats:
+        if stats and "prov" in stats:
+            line.update({"dtype": "f32 (circuits), f64 (proof weights, root sums, leaf gradients)",
+                         "prov": {**stats["prov"], "capture_s": stats["capture_s"], "compile_s": stats["compile_s"],
+                                  "circuit_nodes": stats["circuit_nodes"], "circuit_levels": stats["circuit_levels"],
+                                  "proofs": stats["proofs"]}})
+        elif stats and "batch" in stats:
             b = stats["batch"]
             line.update({"dtype": "u32", "plan": "bit rows, batched waves",
                          "batch": {k: b[k] for k in ("instances", "waves", "graph_launches", "round_launches",

@@ -244,6 +244,63 @@ strata_status strata_tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint3
     const uint64_t* edge_off, const uint32_t* src, const uint32_t* dst, int mode,
     uint64_t* counts, uint64_t* fps, uint32_t* rounds, strata_batch_stats* stats);
 
+/* ---- Prov_k capture and provenance circuits -----------------------------
+ * The probabilistic reachability program
+ *     path(X,Y) :- edge(X,Y).   path(X,Z) :- edge(X,Y), path(Y,Z).
+ * with `path` Prov_k(k) (k <= 8) and every edge a probabilistic fact: edge i
+ * (0-based, input order) is the leaf with literal i+1 and probability
+ * d_prob[i].  Replaces `run_prov` (strata-eval/src/provenance.rs:217-283) +
+ * `ProvDb::query` for this program, with the same naive-round semantics,
+ * evaluated only for the targets of the query pairs (qs[q], qt[q]) (host
+ * arrays).  Edge tuples must be distinct (STRATA_E_UNSUPPORTED otherwise);
+ * proofs longer than 32 literals are refused (STRATA_E_UNSUPPORTED).
+ * target_rounds (optional, one per distinct target in ascending order)
+ * receives the rounds until that target's tuples stopped changing. */
+typedef struct strata_prov_stats {
+  uint64_t queries, targets, waves, rounds_max, max_proof_len, launches;
+  double device_ms;
+} strata_prov_stats;
+typedef struct strata_proofs strata_proofs;
+strata_status strata_prov_tc_capture(strata_ctx* ctx, uint32_t n_nodes, const uint32_t* d_src,
+    const uint32_t* d_dst, uint64_t n_edges, const double* d_prob, uint32_t k, uint32_t n_queries,
+    const uint32_t* qs, const uint32_t* qt, strata_proofs** out, uint32_t* target_rounds,
+    strata_prov_stats* stats);
+/* Sizes, then the flattened proof sets: query q owns proofs
+ * [proof_off[q], proof_off[q+1]), proof p the literals [lit_off[p], lit_off[p+1])
+ * (ascending; the proofs of a query in proof-set order). */
+strata_status strata_proofs_shape(const strata_proofs* pr, uint32_t* n_queries, uint64_t* n_proofs,
+    uint64_t* n_lits);
+strata_status strata_proofs_export(const strata_proofs* pr, uint64_t* proof_off, uint64_t* lit_off,
+    int64_t* lits);
+void strata_proofs_free(strata_proofs* pr);
+
+/* Exact compilation of each query's proof DNF (signed literals ±(leaf+1),
+ * host arrays in the layout above) to a deterministic, decomposable circuit
+ * by Shannon expansion (strata-prob/src/compile.rs:80-150), kept on the
+ * device.  max_nodes bounds each query's circuit (0 = 2^20, the reference's
+ * default); STRATA_E_UNSUPPORTED past it. */
+typedef struct strata_circuits strata_circuits;
+strata_status strata_circuits_compile(strata_ctx* ctx, uint32_t n_queries, const uint64_t* proof_off,
+    const uint64_t* lit_off, const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes,
+    strata_circuits** out);
+strata_status strata_circuits_shape(const strata_circuits* c, uint64_t* n_nodes, uint32_t* max_levels);
+/* Weighted model counts (Circuit::wmc, circuit.rs:57-63) of every query for
+ * leaf probabilities d_p (FP32, n_leaves): FP32 nodes, the root's sum in
+ * FP64; d_out (FP32) and/or d_out64 (FP64) per query.  Asynchronous on the
+ * context's stream; one circuit set must not be evaluated concurrently. */
+strata_status strata_circuits_forward(strata_ctx* ctx, const strata_circuits* c, const float* d_p,
+    float* d_out, double* d_out64);
+/* Vector-Jacobian product: d_grad64[i] = Σ_q d_seed[q] · ∂P_q/∂p_i (FP32
+ * adjoints, FP64 leaf sums; d_seed NULL = all ones); d_grad32 optional FP32
+ * copy.  The torch.autograd backward of the forward above. */
+strata_status strata_circuits_vjp(strata_ctx* ctx, const strata_circuits* c, const float* d_p,
+    const float* d_seed, double* d_grad64, float* d_grad32);
+/* Per-query gradients (Circuit::grad, circuit.rs:68-106): d_grads is
+ * [n_queries][n_leaves] FP64 (the `?grad` rows). */
+strata_status strata_circuits_grads(strata_ctx* ctx, const strata_circuits* c, const float* d_p,
+    double* d_grads);
+void strata_circuits_free(strata_ctx* ctx, strata_circuits* c);
+
 /* Relation handle accessors. */
 strata_status strata_rel_size(const strata_rel* rel, uint64_t* n);
 strata_status strata_rel_is_trop(const strata_rel* rel, int* is_trop);

@@ -8,6 +8,8 @@
 
 #include <cstdlib>
 #include <new>
+#include <vector>
+#include <algorithm>
 
 using sk::DBuf;
 using sk::SkError;
@@ -459,6 +461,124 @@ strata_status strata_tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint3
   DBuf<uint32_t> ds = to_dev(ctx, src, m), dd = to_dev(ctx, dst, m);
   sk::tc_bool_batch(ctx, n_inst, nodes, edge_off, ds.p, dd.p, mode, counts, fps, rounds, stats);
   SK_GUARD_END(ctx)
+}
+
+// ---- Prov_k capture and provenance circuits --------------------------------------
+
+struct strata_proofs {
+  std::vector<std::vector<std::vector<uint32_t>>> q;
+};
+
+strata_status strata_prov_tc_capture(strata_ctx* ctx, uint32_t n_nodes, const uint32_t* d_src,
+                                     const uint32_t* d_dst, uint64_t n_edges, const double* d_prob, uint32_t k,
+                                     uint32_t n_queries, const uint32_t* qs, const uint32_t* qt,
+                                     strata_proofs** out, uint32_t* target_rounds, strata_prov_stats* stats) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out || (n_edges && (!d_src || !d_dst || !d_prob)) || (n_queries && (!qs || !qt)))
+    return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  auto* pr = new strata_proofs();
+  std::vector<uint32_t> rounds;
+  try {
+    sk::prov_tc_capture(ctx, n_nodes, d_src, d_dst, n_edges, d_prob, k, n_queries, qs, qt, pr->q, rounds, stats);
+  } catch (...) {
+    delete pr;
+    throw;
+  }
+  if (target_rounds) std::copy(rounds.begin(), rounds.end(), target_rounds);
+  *out = pr;
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_proofs_shape(const strata_proofs* pr, uint32_t* n_queries, uint64_t* n_proofs,
+                                  uint64_t* n_lits) {
+  if (!pr) return STRATA_E_INVALID;
+  uint64_t np = 0, nl = 0;
+  for (auto& q : pr->q) {
+    np += q.size();
+    for (auto& p : q) nl += p.size();
+  }
+  if (n_queries) *n_queries = (uint32_t)pr->q.size();
+  if (n_proofs) *n_proofs = np;
+  if (n_lits) *n_lits = nl;
+  return STRATA_OK;
+}
+
+strata_status strata_proofs_export(const strata_proofs* pr, uint64_t* proof_off, uint64_t* lit_off, int64_t* lits) {
+  if (!pr || !proof_off || !lit_off) return STRATA_E_INVALID;
+  uint64_t np = 0, nl = 0;
+  for (size_t q = 0; q < pr->q.size(); q++) {
+    proof_off[q] = np;
+    for (auto& p : pr->q[q]) {
+      lit_off[np++] = nl;
+      for (auto l : p) {
+        if (lits) lits[nl] = (int64_t)l;
+        nl++;
+      }
+    }
+  }
+  proof_off[pr->q.size()] = np;
+  lit_off[np] = nl;
+  return STRATA_OK;
+}
+
+void strata_proofs_free(strata_proofs* pr) { delete pr; }
+
+strata_status strata_circuits_compile(strata_ctx* ctx, uint32_t n_queries, const uint64_t* proof_off,
+                                      const uint64_t* lit_off, const int64_t* lits, uint32_t n_leaves,
+                                      uint64_t max_nodes, strata_circuits** out) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out || (n_queries && (!proof_off || !lit_off))) return bad(ctx, "NULL argument");
+  if (n_queries && lit_off[proof_off[n_queries]] && !lits) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  *out = sk::circuits_compile(ctx, n_queries, proof_off, lit_off, lits, n_leaves, max_nodes ? max_nodes : (1u << 20));
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_circuits_shape(const strata_circuits* c, uint64_t* n_nodes, uint32_t* max_levels) {
+  if (!c) return STRATA_E_INVALID;
+  if (n_nodes) *n_nodes = c->n_nodes;
+  if (max_levels) *max_levels = c->max_levels;
+  return STRATA_OK;
+}
+
+strata_status strata_circuits_forward(strata_ctx* ctx, const strata_circuits* c, const float* d_p, float* d_out,
+                                      double* d_out64) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!c || (c->n_leaves && !d_p) || (!d_out && !d_out64)) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::circuits_forward(ctx, c, d_p, d_out, d_out64);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_circuits_vjp(strata_ctx* ctx, const strata_circuits* c, const float* d_p, const float* d_seed,
+                                  double* d_grad64, float* d_grad32) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!c || (c->n_leaves && (!d_p || !d_grad64))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::circuits_adjoint(ctx, c, d_p, d_seed, d_grad64, 0, d_grad32);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_circuits_grads(strata_ctx* ctx, const strata_circuits* c, const float* d_p, double* d_grads) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!c || (c->n_leaves && c->n_queries && (!d_p || !d_grads))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::circuits_adjoint(ctx, c, d_p, nullptr, d_grads, 1, nullptr);
+  SK_GUARD_END(ctx)
+}
+
+void strata_circuits_free(strata_ctx* ctx, strata_circuits* c) {
+  if (!ctx || !c) return;
+  try {
+    sk::circuits_free(ctx, c);
+  } catch (...) {
+  }
 }
 
 strata_status strata_rel_size(const strata_rel* rel, uint64_t* n) {

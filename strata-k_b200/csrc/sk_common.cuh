@@ -29,6 +29,7 @@ enum : uint32_t {
   ST_SENTINEL = 2u,          // a finite sum landed on the +inf encoding
   ST_LOOKBACK_TIMEOUT = 4u,  // decoupled look-back wait hit its iteration cap
   ST_BOUNDS = 8u,            // an index failed a bounds check and was skipped
+  ST_PROOF_LEN = 16u,        // a provenance proof exceeded its literal capacity
 };
 
 // Iteration cap of every spin-wait in device code.  A wait that reaches it
@@ -244,6 +245,7 @@ inline void sync_and_check(strata_ctx* ctx) {
   uint32_t s = *ctx->h_status;
   if (s & ST_LOOKBACK_TIMEOUT) fail(STRATA_E_TIMEOUT, "a device look-back wait reached its cap");
   if (s & ST_BOUNDS) fail(STRATA_E_CUDA, "a device bounds check failed (index skipped)");
+  if (s & ST_PROOF_LEN) fail(STRATA_E_UNSUPPORTED, "a provenance proof exceeded 32 literals");
   if (s & ST_OVERFLOW) fail(STRATA_E_OVERFLOW, "tropical weight overflow: a finite sum exceeds i64");
   if (s & ST_SENTINEL)
     fail(STRATA_E_WEIGHT_RANGE,
@@ -284,7 +286,9 @@ enum KernelId : int {
   K_TRI_COUNT = 6,
   K_EXPAND_DENSE = 7,
   K_BS_ROUND = 8,
-  K_NUM = 9,
+  K_PROV_ROUND = 9,
+  K_CIRCUIT = 10,
+  K_NUM = 11,
 };
 
 inline cudaEvent_t take_event(strata_ctx* ctx) {

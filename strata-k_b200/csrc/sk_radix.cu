@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(NT) k_radix_bins(const uint32_t* __restrict__ 
 }
 
 template <class K, class V, bool HAS_V, int ITEMS>
-__global__ void __launch_bounds__(NT) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
+__global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
                                                  const V* __restrict__ vin, V* __restrict__ vout,
                                                  uint32_t n, int shift, int dbits,
                                                  const uint32_t* __restrict__ binoff,

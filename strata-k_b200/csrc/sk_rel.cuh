@@ -17,6 +17,27 @@ struct strata_rel {
   void* w = nullptr;
 };
 
+// Compiled provenance circuits of a set of queries, levelled per query
+// (sk_circuit.cu).
+struct strata_circuits {
+  uint32_t n_queries = 0;
+  uint32_t n_leaves = 0;
+  uint64_t n_nodes = 0;
+  uint32_t max_levels = 0;
+  // device arrays
+  uint8_t* kind = nullptr;      // 0 leaf, 1 neg leaf, 2 and, 3 or, 4 true, 5 false
+  uint32_t* a = nullptr;        // leaf index, or first child (index into `ch`)
+  uint32_t* b = nullptr;        // child count
+  uint32_t* ch = nullptr;       // children (global node indices)
+  uint64_t* qnode = nullptr;    // first node of query q (n_queries + 1)
+  uint32_t* root = nullptr;     // root node of query q (global index)
+  uint64_t* qlevel = nullptr;   // first level of query q in `lvl` (n_queries + 1)
+  uint32_t* lvl = nullptr;      // level boundaries: node offsets relative to qnode[q]
+  float* val = nullptr;         // forward values
+  float* adj = nullptr;         // adjoints
+  uint64_t n_children = 0;
+};
+
 namespace sk {
 
 // Device columns of an input relation (weights / inf mask optional).
@@ -40,6 +61,17 @@ void tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint32_t* nodes, cons
                    const uint32_t* d_src, const uint32_t* d_dst, int mode, uint64_t* counts, uint64_t* fps,
                    uint32_t* rounds, strata_batch_stats* st);
 bool tc_bool_bitset_fits(strata_ctx* ctx, uint64_t n_src, uint64_t n_dst, uint64_t m);
+
+void prov_tc_capture(strata_ctx* ctx, uint32_t n, const uint32_t* d_src, const uint32_t* d_dst, uint64_t m,
+                     const double* d_prob, uint32_t k, uint32_t nq, const uint32_t* qs, const uint32_t* qt,
+                     std::vector<std::vector<std::vector<uint32_t>>>& out, std::vector<uint32_t>& rounds_out,
+                     strata_prov_stats* st);
+strata_circuits* circuits_compile(strata_ctx* ctx, uint32_t nq, const uint64_t* proof_off, const uint64_t* lit_off,
+                                  const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes);
+void circuits_free(strata_ctx* ctx, strata_circuits* c);
+void circuits_forward(strata_ctx* ctx, const strata_circuits* c, const float* d_p, float* out32, double* out64);
+void circuits_adjoint(strata_ctx* ctx, const strata_circuits* c, const float* d_p, const float* seed, double* grad,
+                      int per_query, float* grad32);
 template <class K>
 uint64_t tc_bool_bitset(strata_ctx* ctx, const uint32_t* d_src, const uint32_t* d_dst, uint64_t m, uint64_t n_src,
                         uint64_t n_dst, int b1, DBuf<K>& out, uint64_t* rounds, uint64_t* round_bytes);

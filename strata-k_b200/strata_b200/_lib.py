@@ -32,7 +32,7 @@ KNOB_BATCH_GRAPH_ROUNDS, KNOB_BATCH_BLOCKS_PER_SM, KNOB_BATCH_BUDGET_MB = 4, 5, 
 
 KERNELS = {0: "k_onesweep", 1: "k_expand_emit", 2: "k_expand_offsets", 3: "k_reduce_runs",
            4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count", 7: "k_expand_dense",
-           8: "k_bs_round"}
+           8: "k_bs_round", 9: "k_prov_round", 10: "k_circuit"}
 
 STATUS_NAMES = {
     OK: "OK", E_INVALID: "INVALID", E_OOM: "OOM", E_CUDA: "CUDA", E_OVERFLOW: "OVERFLOW",
@@ -74,6 +74,18 @@ class BatchStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class ProvStats(C.Structure):
+    """Mirror of ``strata_prov_stats``."""
+
+    _fields_ = [
+        ("queries", C.c_uint64), ("targets", C.c_uint64), ("waves", C.c_uint64), ("rounds_max", C.c_uint64),
+        ("max_proof_len", C.c_uint64), ("launches", C.c_uint64), ("device_ms", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 u8p = C.POINTER(C.c_uint8)
 u32p = C.POINTER(C.c_uint32)
 u64p = C.POINTER(C.c_uint64)
@@ -98,6 +110,18 @@ SIGNATURES = {
                                            C.POINTER(BatchStats)]),
     "strata_tc_bool_batch": (C.c_int, [ctxp, C.c_uint32, u32p, u64p, u32p, u32p, C.c_int, u64p, u64p, u32p,
                                        C.POINTER(BatchStats)]),
+    "strata_prov_tc_capture": (C.c_int, [ctxp, C.c_uint32, vp, vp, C.c_uint64, vp, C.c_uint32, C.c_uint32, u32p,
+                                         u32p, C.POINTER(vp), u32p, C.POINTER(ProvStats)]),
+    "strata_proofs_shape": (C.c_int, [vp, u32p, u64p, u64p]),
+    "strata_proofs_export": (C.c_int, [vp, u64p, u64p, i64p]),
+    "strata_proofs_free": (None, [vp]),
+    "strata_circuits_compile": (C.c_int, [ctxp, C.c_uint32, u64p, u64p, i64p, C.c_uint32, C.c_uint64,
+                                          C.POINTER(vp)]),
+    "strata_circuits_shape": (C.c_int, [vp, u64p, u32p]),
+    "strata_circuits_forward": (C.c_int, [ctxp, vp, vp, vp, vp]),
+    "strata_circuits_vjp": (C.c_int, [ctxp, vp, vp, vp, vp, vp]),
+    "strata_circuits_grads": (C.c_int, [ctxp, vp, vp, vp]),
+    "strata_circuits_free": (None, [ctxp, vp]),
     "strata_ctx_launches": (C.c_uint64, [ctxp]),
     "strata_ctx_kernel_stats": (C.c_int, [ctxp, C.c_int, u64p, C.POINTER(C.c_double), u64p]),
     "strata_ctx_reset_kernel_stats": (C.c_int, [ctxp]),

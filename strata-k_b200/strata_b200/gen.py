@@ -228,3 +228,30 @@ def batch_tc_workload(n_inst=4096, n_min=100, n_max=50_000, deg_min=2.0, deg_max
                          meta={"instances": n_inst, "n_min": n_min, "n_max": n_max, "deg_min": deg_min,
                                "deg_max": deg_max, "seed": seed, "edges": int(off[-1]),
                                "sum_n2": float((nodes.astype(np.float64) ** 2).sum())})
+
+
+@dataclass
+class ProvWorkload:
+    """Probabilistic reachability: edge i has probability p32[i] (fp32; the
+    FP64 view p64 is the same value), queries (qs[q], qt[q])."""
+    name: str
+    n: int
+    src: np.ndarray
+    dst: np.ndarray
+    p32: np.ndarray
+    p64: np.ndarray
+    qs: np.ndarray
+    qt: np.ndarray
+    meta: dict | None = None
+
+
+def prov_workload(n=20_000, m=80_000, n_queries=1024, seed=5) -> ProvWorkload:
+    """Directed ER(n, m) with independent edge probabilities ~ Beta(2, 5) drawn
+    as fp32, and n_queries (s, t) pairs drawn uniformly."""
+    s, d = er_directed(n, m, seed)
+    rng = np.random.default_rng(seed + 1)
+    p32 = rng.beta(2.0, 5.0, m).astype(np.float32)
+    qs = rng.integers(0, n, n_queries).astype(np.uint32)
+    qt = rng.integers(0, n, n_queries).astype(np.uint32)
+    return ProvWorkload(f"prov_er_{n}_{m}_{n_queries}q", n, s, d, p32, p32.astype(np.float64), qs, qt,
+                        meta={"nodes": n, "edges": m, "queries": n_queries, "seed": seed})

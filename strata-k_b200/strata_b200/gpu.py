@@ -380,6 +380,55 @@ class Engine:
                 _ptr(rounds, C.c_uint32), C.byref(st)))
         return BatchResult(counts, fps, rounds, st.as_dict())
 
+    # -- Prov_k capture and provenance circuits -----------------------------
+    def prov_capture(self, n_nodes: int, src, dst, prob, qs, qt, k: int = 8) -> "ProofSets":
+        """Prov_k(k) proofs of path(s, t) for the query pairs (qs[q], qt[q]) of
+        path(X,Y) :- edge(X,Y). path(X,Z) :- edge(X,Y), path(Y,Z). where edge
+        i is the leaf with literal i+1 and probability prob[i] (FP64).
+        src/dst/prob: device tensors or host arrays; qs/qt host arrays."""
+        import torch
+        if not hasattr(src, "data_ptr"):
+            src = torch.from_numpy(_u32(src).view(np.int32)).cuda()
+            dst = torch.from_numpy(_u32(dst).view(np.int32)).cuda()
+        if not hasattr(prob, "data_ptr"):
+            prob = torch.from_numpy(np.ascontiguousarray(prob, dtype=np.float64)).cuda()
+        if prob.dtype != torch.float64:
+            raise InvalidArgument("edge probabilities must be float64 (the FP64 of each input value)")
+        qs_, qt_ = _u32(qs), _u32(qt)
+        m = _len(src)
+        if _len(dst) != m or _len(prob) != m:
+            raise InvalidArgument("src, dst and prob must have one entry per edge")
+        if len(qs_) != len(qt_):
+            raise InvalidArgument("qs and qt must have the same length")
+        out = C.c_void_p()
+        st = L.ProvStats()
+        rounds = np.zeros(max(1, len(np.unique(qt_))), np.uint32)
+        self._check(self.lib.strata_prov_tc_capture(
+            self.ctx, n_nodes, _dp(src), _dp(dst), m, _dp(prob), k, len(qs_), _ptr(qs_, C.c_uint32),
+            _ptr(qt_, C.c_uint32), C.byref(out), _ptr(rounds, C.c_uint32), C.byref(st)))
+        try:
+            nq, np_, nl = C.c_uint32(), C.c_uint64(), C.c_uint64()
+            self._check(self.lib.strata_proofs_shape(out, C.byref(nq), C.byref(np_), C.byref(nl)))
+            po = np.zeros(nq.value + 1, np.uint64)
+            lo = np.zeros(np_.value + 1, np.uint64)
+            lits = np.zeros(max(1, nl.value), np.int64)
+            self._check(self.lib.strata_proofs_export(out, _ptr(po, C.c_uint64), _ptr(lo, C.c_uint64),
+                                                      _ptr(lits, C.c_int64)))
+        finally:
+            self.lib.strata_proofs_free(out)
+        return ProofSets(po, lo, lits, st.as_dict(), rounds[:len(np.unique(qt_))])
+
+    def compile_circuits(self, proofs, n_leaves: int, max_nodes: int = 0) -> "Circuits":
+        """Exact circuits of each query's proof DNF (a ProofSets, or a list of
+        lists of signed-literal lists)."""
+        if not isinstance(proofs, ProofSets):
+            proofs = ProofSets.from_lists(proofs)
+        out = C.c_void_p()
+        self._check(self.lib.strata_circuits_compile(
+            self.ctx, len(proofs), _ptr(proofs.proof_off, C.c_uint64), _ptr(proofs.lit_off, C.c_uint64),
+            _ptr(proofs.lits, C.c_int64), n_leaves, max_nodes, C.byref(out)))
+        return Circuits(self, out, len(proofs), n_leaves)
+
     def count_triangle_pattern_dev(self, x, y, n=None) -> int:
         n = _len(x) if n is None else n
         out = C.c_uint64()
@@ -398,6 +447,87 @@ def _dp(t) -> C.c_void_p | None:
 
 def _len(t) -> int:
     return int(t.numel()) if hasattr(t, "numel") else len(t)
+
+
+class ProofSets:
+    """Flattened per-query proof sets: query q owns proofs
+    [proof_off[q], proof_off[q+1]), proof p the literals [lit_off[p], lit_off[p+1])."""
+
+    def __init__(self, proof_off, lit_off, lits, stats=None, target_rounds=None):
+        self.proof_off = np.ascontiguousarray(proof_off, np.uint64)
+        self.lit_off = np.ascontiguousarray(lit_off, np.uint64)
+        self.lits = np.ascontiguousarray(lits, np.int64)
+        if len(self.lits) == 0:
+            self.lits = np.zeros(1, np.int64)
+        self.stats = stats or {}
+        self.target_rounds = target_rounds
+
+    @staticmethod
+    def from_lists(qs) -> "ProofSets":
+        po, lo, lits = [0], [0], []
+        for q in qs:
+            for p in q:
+                lits += [int(x) for x in p]
+                lo.append(len(lits))
+            po.append(len(lo) - 1)
+        return ProofSets(po, lo, lits)
+
+    def __len__(self) -> int:
+        return len(self.proof_off) - 1
+
+    def query(self, q: int) -> list:
+        a, b = int(self.proof_off[q]), int(self.proof_off[q + 1])
+        return [self.lits[int(self.lit_off[p]):int(self.lit_off[p + 1])].tolist() for p in range(a, b)]
+
+    def as_lists(self) -> list:
+        return [self.query(q) for q in range(len(self))]
+
+
+class Circuits:
+    """Compiled provenance circuits on the device (forward WMC, VJP, per-query grads)."""
+
+    def __init__(self, eng: Engine, handle, n_queries: int, n_leaves: int):
+        self.eng, self.h, self.n_queries, self.n_leaves = eng, handle, n_queries, n_leaves
+
+    def shape(self) -> tuple[int, int]:
+        n, lv = C.c_uint64(), C.c_uint32()
+        self.eng._check(self.eng.lib.strata_circuits_shape(self.h, C.byref(n), C.byref(lv)))
+        return int(n.value), int(lv.value)
+
+    def forward(self, p, out64: bool = False):
+        """P per query for FP32 leaf probabilities p (a CUDA tensor)."""
+        import torch
+        out = torch.empty(self.n_queries, dtype=torch.float64 if out64 else torch.float32, device=p.device)
+        self.eng._check(self.eng.lib.strata_circuits_forward(
+            self.eng.ctx, self.h, _dp(p), None if out64 else _dp(out), _dp(out) if out64 else None))
+        return out
+
+    def vjp(self, p, seed=None):
+        """Σ_q seed[q] · dP_q/dp (FP32 tensor of n_leaves; FP64 accumulation)."""
+        import torch
+        g64 = torch.empty(max(1, self.n_leaves), dtype=torch.float64, device=p.device)
+        g32 = torch.empty(max(1, self.n_leaves), dtype=torch.float32, device=p.device)
+        self.eng._check(self.eng.lib.strata_circuits_vjp(self.eng.ctx, self.h, _dp(p), _dp(seed), _dp(g64),
+                                                         _dp(g32)))
+        return g32[:self.n_leaves], g64[:self.n_leaves]
+
+    def grads(self, p):
+        """[n_queries, n_leaves] FP64 per-query gradients (the ?grad rows)."""
+        import torch
+        g = torch.empty((max(1, self.n_queries), max(1, self.n_leaves)), dtype=torch.float64, device=p.device)
+        self.eng._check(self.eng.lib.strata_circuits_grads(self.eng.ctx, self.h, _dp(p), _dp(g)))
+        return g[:self.n_queries, :self.n_leaves]
+
+    def free(self):
+        if self.h:
+            self.eng.lib.strata_circuits_free(self.eng.ctx, self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 class BatchResult:
