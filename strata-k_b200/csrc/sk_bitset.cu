@@ -130,15 +130,25 @@ __global__ void __launch_bounds__(BS_NT) k_bs_round(BsView v) {
       for (uint32_t c = sl; c < W; c += lpr) {
         uint4 acc = make_uint4(0u, 0u, 0u, 0u);
         active_edges = 0;
-        for (uint64_t e = e0; e < e1; e++) {
-          const uint32_t y = v.nbr[e];
-          if (y < n && fc[rb + y]) {
-            const uint4 d = Dc[vb + (uint64_t)y * W + c];
-            acc.x |= d.x;
-            acc.y |= d.y;
-            acc.z |= d.z;
-            acc.w |= d.w;
-            active_edges++;
+        // four edges at a time: their neighbour, flag and Δ-row loads are
+        // independent, so they are in flight together
+        for (uint64_t e = e0; e < e1; e += 4) {
+          uint32_t y[4];
+          bool on[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) y[q] = e + q < e1 ? v.nbr[e + q] : 0xffffffffu;
+#pragma unroll
+          for (int q = 0; q < 4; q++) on[q] = y[q] < n && fc[rb + y[q]] != 0;
+          uint4 d[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) d[q] = on[q] ? Dc[vb + (uint64_t)y[q] * W + c] : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            acc.x |= d[q].x;
+            acc.y |= d[q].y;
+            acc.z |= d[q].z;
+            acc.w |= d[q].w;
+            active_edges += on[q] ? 1u : 0u;
           }
         }
         uint4 nw = make_uint4(0u, 0u, 0u, 0u);
@@ -741,9 +751,7 @@ void bs_run(strata_ctx* ctx, const std::vector<InstSpec>& spec, const uint32_t* 
 }
 
 uint64_t bs_budget(strata_ctx* ctx) {
-  size_t fr = 0, tot = 0;
-  check_cuda(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
-  uint64_t b = (uint64_t)((double)fr * 0.7);
+  uint64_t b = (uint64_t)((double)reusable_device_bytes(ctx) * 0.7);
   if (ctx->cap && ctx->cap > ctx->in_use) b = std::min<uint64_t>(b, ctx->cap - ctx->in_use);
   if (ctx->tune_bs_budget_mb > 0) b = std::min<uint64_t>(b, (uint64_t)ctx->tune_bs_budget_mb << 20);
   return b;
@@ -768,6 +776,7 @@ void tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint32_t* nodes, cons
   check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
   check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
   check_cuda(cudaEventRecord(e0, ctx->stream), "cudaEventRecord");
+  release_all_cached(ctx);  // the waves are sized from what this context can reuse
   BsBuffers B(ctx);
   BsResult R;
   try {

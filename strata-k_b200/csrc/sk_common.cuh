@@ -117,6 +117,28 @@ inline void release_cached(strata_ctx* ctx, uint64_t need) {
   }
 }
 
+// Device bytes this context could obtain now: the device's free memory,
+// plus what its pool holds unused, plus the blocks it keeps cached.
+inline uint64_t reusable_device_bytes(strata_ctx* ctx) {
+  size_t fr = 0, tot = 0;
+  check_cuda(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+  uint64_t extra = ctx->cached;
+  if (ctx->pool) {
+    unsigned long long reserved = 0, used = 0;  // the attribute value type (cuuint64_t)
+    if (cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+      extra += reserved - used;
+  }
+  return (uint64_t)fr + extra;
+}
+
+// Give every cached block back to the pool (before sizing large buffers).
+inline void release_all_cached(strata_ctx* ctx) {
+  for (auto& kv : ctx->free_blocks) cudaFreeAsync(kv.second, ctx->stream);
+  ctx->free_blocks.clear();
+  ctx->cached = 0;
+}
+
 inline void* dev_alloc(strata_ctx* ctx, uint64_t bytes) {
   if (bytes == 0) bytes = 16;
   bytes = size_class(bytes);
@@ -151,6 +173,13 @@ inline void* dev_alloc(strata_ctx* ctx, uint64_t bytes) {
     ctx->cap = keep_cap;
     e = ctx->pool ? cudaMallocFromPoolAsync(&p, bytes, ctx->pool, ctx->stream)
                   : cudaMallocAsync(&p, bytes, ctx->stream);
+    if (e != cudaSuccess && ctx->pool) {
+      // The pool's free memory may be fragmented: return it to the device.
+      cudaGetLastError();
+      cudaStreamSynchronize(ctx->stream);
+      cudaMemPoolTrimTo(ctx->pool, 0);
+      e = cudaMallocFromPoolAsync(&p, bytes, ctx->pool, ctx->stream);
+    }
     if (e != cudaSuccess) {
       cudaGetLastError();
       fail(STRATA_E_OOM, std::string("cudaMallocAsync(") + std::to_string(bytes) +

@@ -61,10 +61,11 @@ __device__ __forceinline__ uint64_t dense_index(uint64_t key, const DenseLayout&
   return L.colmajor ? c1 * L.n0 + c0 : c0 * L.n1 + c1;
 }
 
-// Grouped expand.  pos[] comes from expand_offsets in grouped mode: only the
-// head of each group (a run of equal join value, split at multiples of
-// kGroupMax) carries the degree of its join value, so one expand output is
-// one (group, edge) pair.  A warp takes 32 consecutive outputs (one per
+// Grouped expand over the compacted group heads (dense_heads): a group is a
+// run of Δ rows with one join value, split at multiples of kGroupMax; its
+// head carries the degree of the join value, so one expand output is one
+// (group, edge) pair and the load balancing spends no merged positions on
+// the other members.  A warp takes 32 consecutive outputs (one per
 // lane), flattens their (edge, member) candidates with a warp prefix sum over
 // the group sizes and processes them 32 at a time: lanes that share an edge
 // handle consecutive members of its group, whose index entries are adjacent
@@ -72,21 +73,24 @@ __device__ __forceinline__ uint64_t dense_index(uint64_t key, const DenseLayout&
 // lines instead of 32.
 template <class K, bool TROP>
 __global__ void __launch_bounds__(NT, 6)
-    k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n,
-                   const uint64_t* __restrict__ pos, uint64_t total, const uint64_t* __restrict__ splits,
-                   int jshift, uint64_t jmask, int pshift, uint64_t pmask, int out_pshift, int out_vshift,
-                   const uint32_t* __restrict__ off, uint64_t n_nodes, const uint32_t* __restrict__ nbr,
-                   uint64_t n_nbr, const int32_t* __restrict__ nbr_w, DenseLayout lay, uint32_t* bits,
-                   int32_t* D, uint32_t* marks, uint32_t* status) {
+    k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n_rows,
+                   const uint32_t* __restrict__ hidx, const uint64_t* __restrict__ pos,
+                   const uint32_t* __restrict__ hseg, const uint8_t* __restrict__ hg, uint64_t n,
+                   uint64_t total, const uint64_t* __restrict__ splits, int pshift, uint64_t pmask, int out_pshift,
+                   int out_vshift, const uint32_t* __restrict__ nbr, uint64_t n_nbr,
+                   const int32_t* __restrict__ nbr_w, DenseLayout lay, uint32_t* bits, int32_t* D, uint32_t* marks,
+                   uint32_t* status) {
   // Dynamic shared memory (sizes in dense_expand_smem()):
-  //   s_pos   int32  pos of each local item relative to the tile's first output
-  //   s_seg   u32    CSR segment start of each local item
-  //   s_owner u16    local owner item of each output of the tile
-  //   s_g     u8     group size of each local head item (members incl. the head)
+  //   s_pos   int32  pos of each local head relative to the tile's first output
+  //   s_seg   u32    CSR segment start of each local head
+  //   s_h     u32    Δ row of each local head (its group's first member)
+  //   s_owner u16    local owner head of each output of the tile
+  //   s_g     u8     group size of each local head (members incl. the head)
   extern __shared__ __align__(16) unsigned char s_raw[];
   int32_t* s_pos = reinterpret_cast<int32_t*>(s_raw);
   uint32_t* s_seg = reinterpret_cast<uint32_t*>(s_pos + DE_TILE + 1);
-  uint16_t* s_owner = reinterpret_cast<uint16_t*>(s_seg + DE_TILE + 1);
+  uint32_t* s_h = s_seg + DE_TILE + 1;
+  uint16_t* s_owner = reinterpret_cast<uint16_t*>(s_h + DE_TILE + 1);
   uint8_t* s_g = reinterpret_cast<uint8_t*>(s_owner + DE_TILE);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t L = n + total;
@@ -102,21 +106,12 @@ __global__ void __launch_bounds__(NT, 6)
   const uint32_t cnt = (uint32_t)(i1 - a);
   for (uint32_t k = tid; k < cnt; k += NT) {
     const uint64_t i = a + k;
-    const uint64_t jv = ((uint64_t)dkeys[i] >> jshift) & jmask;
-    const int64_t rel = (int64_t)pos[i] - (int64_t)o0;  // one item's degree stays below 2^31
+    const int64_t rel = (int64_t)pos[i] - (int64_t)o0;  // one head's degree stays below 2^31
     if (rel < INT32_MIN || rel > INT32_MAX) atomicOr(status, ST_BOUNDS);
     s_pos[k] = (int32_t)rel;
-    s_seg[k] = jv < n_nodes ? off[jv] : 0u;
-    // Group size: the head and the following items with its join value, up
-    // to the next multiple of kGroupMax (non-heads own no outputs).
-    const bool head = (i % kGroupMax) == 0 || (((uint64_t)dkeys[i - 1] >> jshift) & jmask) != jv;
-    uint32_t g = 0;
-    if (head) {
-      const uint64_t lim = min(n - i, (uint64_t)(kGroupMax - i % kGroupMax));
-      g = 1;
-      while (g < lim && (((uint64_t)dkeys[i + g] >> jshift) & jmask) == jv) g++;
-    }
-    s_g[k] = (uint8_t)g;
+    s_seg[k] = hseg[i];
+    s_h[k] = hidx[i];
+    s_g[k] = hg[i];
   }
   __syncthreads();
   uint32_t flags = 0;
@@ -161,7 +156,11 @@ __global__ void __launch_bounds__(NT, 6)
         v = nbr[e];
         if constexpr (TROP) ew = nbr_w[e];
         g = s_g[li];
-        h = a + li;
+        h = s_h[li];
+        if (h + g > n_rows) {
+          flags |= ST_BOUNDS;
+          g = 0;
+        }
       }
     }
     const uint32_t incl = warp_incl_sum(g);
@@ -414,38 +413,186 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+// ---- group heads of a Δ sorted by join value ---------------------------------
+// A head is the first row of a run of equal join value, or a row at a
+// multiple of kGroupMax inside a run; heads whose join value has no edges
+// are dropped.  Reduce-then-scan: per-tile (count, degree) sums, one-block
+// scans, then the write of (row, degree prefix, segment start, group size).
+constexpr int HC_ITEMS = 8;
+constexpr uint32_t HC_TILE = NT * HC_ITEMS;
+
+template <class K>
+__device__ __forceinline__ uint32_t head_degree(const K* dkeys, uint64_t i, int jshift, uint64_t jmask,
+                                                const uint32_t* off, uint64_t n_nodes, uint64_t* jv_out,
+                                                uint32_t* full_deg) {
+  const uint64_t jv = ((uint64_t)dkeys[i] >> jshift) & jmask;
+  const uint32_t d = jv < n_nodes ? off[jv + 1] - off[jv] : 0u;
+  *jv_out = jv;
+  *full_deg = d;
+  if (d == 0) return 0;
+  const bool head = (i % kGroupMax) == 0 || (((uint64_t)dkeys[i - 1] >> jshift) & jmask) != jv;
+  return head ? d : 0u;
+}
+
+template <class K>
+__global__ void __launch_bounds__(NT)
+    k_heads_count(const K* __restrict__ dkeys, uint64_t n, int jshift, uint64_t jmask, const uint32_t* __restrict__ off,
+                  uint64_t n_nodes, uint64_t* __restrict__ tile_cnt, uint64_t* __restrict__ tile_deg,
+                  unsigned long long* cand_total) {
+  __shared__ uint64_t s_red[3][NT / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * HC_TILE + (uint64_t)warp * 32 * HC_ITEMS;
+  uint64_t c = 0, dsum = 0, cands = 0;
+#pragma unroll
+  for (int j = 0; j < HC_ITEMS; j++) {
+    const uint64_t i = base + (uint64_t)j * 32 + lane;
+    if (i < n) {
+      uint64_t jv;
+      uint32_t fd;
+      const uint32_t d = head_degree(dkeys, i, jshift, jmask, off, n_nodes, &jv, &fd);
+      c += d ? 1 : 0;
+      dsum += d;
+      cands += fd;
+    }
+  }
+  c = warp_sum(c);
+  dsum = warp_sum(dsum);
+  cands = warp_sum(cands);
+  if (lane == 0) {
+    s_red[0][warp] = c;
+    s_red[1][warp] = dsum;
+    s_red[2][warp] = cands;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint64_t a = 0, b = 0, e = 0;
+    for (int w = 0; w < NT / 32; w++) {
+      a += s_red[0][w];
+      b += s_red[1][w];
+      e += s_red[2][w];
+    }
+    tile_cnt[blockIdx.x] = a;
+    tile_deg[blockIdx.x] = b;
+    if (e) atomicAdd(cand_total, (unsigned long long)e);
+  }
+}
+
+template <class K>
+__global__ void __launch_bounds__(NT)
+    k_heads_write(const K* __restrict__ dkeys, uint64_t n, int jshift, uint64_t jmask, const uint32_t* __restrict__ off,
+                  uint64_t n_nodes, const uint64_t* __restrict__ tile_cnt, const uint64_t* __restrict__ tile_deg,
+                  uint64_t n_tiles, uint32_t* __restrict__ hidx, uint64_t* __restrict__ hpos,
+                  uint32_t* __restrict__ hseg, uint8_t* __restrict__ hg) {
+  __shared__ uint64_t s_wc[NT / 32], s_wd[NT / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * HC_TILE + (uint64_t)warp * 32 * HC_ITEMS;
+  uint32_t dg[HC_ITEMS];
+  uint64_t exc[HC_ITEMS], exd[HC_ITEMS];
+  uint64_t cc = 0, cd = 0;
+#pragma unroll
+  for (int j = 0; j < HC_ITEMS; j++) {
+    const uint64_t i = base + (uint64_t)j * 32 + lane;
+    uint32_t d = 0;
+    if (i < n) {
+      uint64_t jv;
+      uint32_t fd;
+      d = head_degree(dkeys, i, jshift, jmask, off, n_nodes, &jv, &fd);
+    }
+    dg[j] = d;
+    const uint64_t ic = warp_incl_sum((uint64_t)(d ? 1 : 0));
+    const uint64_t id = warp_incl_sum((uint64_t)d);
+    exc[j] = cc + ic - (d ? 1 : 0);
+    exd[j] = cd + id - d;
+    cc += __shfl_sync(kFull, ic, 31);
+    cd += __shfl_sync(kFull, id, 31);
+  }
+  if (lane == 0) {
+    s_wc[warp] = cc;
+    s_wd[warp] = cd;
+  }
+  __syncthreads();
+  uint64_t bc = tile_cnt[blockIdx.x], bd = tile_deg[blockIdx.x];
+  for (int w = 0; w < warp; w++) {
+    bc += s_wc[w];
+    bd += s_wd[w];
+  }
+#pragma unroll
+  for (int j = 0; j < HC_ITEMS; j++) {
+    if (!dg[j]) continue;
+    const uint64_t i = base + (uint64_t)j * 32 + lane;
+    const uint64_t k = bc + exc[j];
+    const uint64_t jv = ((uint64_t)dkeys[i] >> jshift) & jmask;
+    uint32_t g = 1;
+    const uint64_t lim = min(n - i, (uint64_t)(kGroupMax - i % kGroupMax));
+    while (g < lim && (((uint64_t)dkeys[i + g] >> jshift) & jmask) == jv) g++;
+    hidx[k] = (uint32_t)i;
+    hpos[k] = bd + exd[j];
+    hseg[k] = off[jv];
+    hg[k] = (uint8_t)g;
+  }
+  if (blockIdx.x == gridDim.x - 1 && tid == 0) hpos[tile_cnt[n_tiles]] = tile_deg[n_tiles];
+}
+
 inline unsigned grid1(uint64_t n) { return (unsigned)ceil_div(n ? n : 1, NT); }
 
-size_t dense_expand_smem() { return (DE_TILE + 1) * (4 + 4) + DE_TILE * 2 + (DE_TILE + 1) + 16; }
+size_t dense_expand_smem() { return (DE_TILE + 1) * (4 + 4 + 4) + DE_TILE * 2 + (DE_TILE + 1) + 16; }
 
 }  // namespace
 
 uint64_t dense_tile_size() { return DE_TILE; }
 uint32_t dense_group_max() { return kGroupMax; }
 
+template <class K>
+void dense_heads(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uint64_t jmask, const uint32_t* off,
+                 uint64_t n_nodes, uint64_t* sums, uint32_t* hidx, uint64_t* hpos, uint32_t* hseg, uint8_t* hg,
+                 uint64_t* out3) {
+  const uint64_t tiles = ceil_div(n ? n : 1, HC_TILE);
+  uint64_t* tc = sums;               // tiles + 1
+  uint64_t* td = sums + tiles + 1;   // tiles + 1
+  uint64_t* ct = sums + 2 * (tiles + 1);
+  SK_CUDA(cudaMemsetAsync(ct, 0, 8, ctx->stream));
+  k_heads_count<K><<<(unsigned)tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, tc, td,
+                                                            reinterpret_cast<unsigned long long*>(ct));
+  after_launch(ctx, "k_heads_count");
+  scan_tile_sums(ctx, tc, tiles);
+  scan_tile_sums(ctx, td, tiles);
+  k_heads_write<K><<<(unsigned)tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, tc, td, tiles,
+                                                            hidx, hpos, hseg, hg);
+  after_launch(ctx, "k_heads_write");
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, tc + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar + 1, td + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar + 2, ct, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  sync_and_check(ctx);
+  out3[0] = ctx->h_scalar[0];  // heads
+  out3[1] = ctx->h_scalar[1];  // (group, edge) outputs
+  out3[2] = ctx->h_scalar[2];  // candidates
+}
+
+uint64_t dense_heads_sums(uint64_t n) { return 2 * (ceil_div(n ? n : 1, HC_TILE) + 1) + 2; }
+
 template <class K, bool TROP>
-void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n, const uint64_t* pos,
-                  uint64_t total, uint64_t candidates, int jshift, uint64_t jmask, int pshift, uint64_t pmask,
-                  int out_pshift, int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr,
+void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n_rows, const uint32_t* hidx,
+                  const uint64_t* hpos, const uint32_t* hseg, const uint8_t* hg, uint64_t nh, uint64_t total,
+                  uint64_t candidates, int pshift, uint64_t pmask, int out_pshift, int out_vshift, const uint32_t* nbr,
                   uint64_t n_nbr, const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D,
                   uint32_t* marks, uint64_t* splits_buf) {
-  if (n == 0 || total == 0) return;
-  const uint64_t tiles = ceil_div(n + total, DE_TILE);
+  if (nh == 0 || total == 0) return;
+  const uint64_t tiles = ceil_div(nh + total, DE_TILE);
   if (tiles > 0x7fffffffull) fail(STRATA_E_UNSUPPORTED, "expand too large for one launch");
-  k_tile_splits<<<grid1(tiles + 1), NT, 0, ctx->stream>>>(pos, n, total, DE_TILE, tiles, splits_buf);
+  k_tile_splits<<<grid1(tiles + 1), NT, 0, ctx->stream>>>(hpos, nh, total, DE_TILE, tiles, splits_buf);
   after_launch(ctx, "k_tile_splits");
   const int kh = kprof_begin(ctx, K_EXPAND_DENSE);
   const size_t smem = dense_expand_smem();
   auto kern = k_expand_dense<K, TROP>;
   SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(dkeys, dw, n, pos, total, splits_buf, jshift, jmask, pshift,
-                                                   pmask, out_pshift, out_vshift, off, n_nodes, nbr, n_nbr, nbr_w,
-                                                   lay, bits, D, marks, ctx->d_status);
-  // Algorithmic bytes: every Δ row (key, weight, offsets), every CSR edge of
-  // a group read once (neighbour + weight), one 4-byte index probe per
-  // candidate (a candidate = one Δ row × one edge of its join value).
+  kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(dkeys, dw, n_rows, hidx, hpos, hseg, hg, nh, total, splits_buf,
+                                                   pshift, pmask, out_pshift, out_vshift, nbr, n_nbr, nbr_w, lay,
+                                                   bits, D, marks, ctx->d_status);
+  // Algorithmic bytes: every Δ row (key, weight) once, each head's record,
+  // every CSR edge of a group read once (neighbour + weight), one 4-byte
+  // index probe per candidate (a candidate = one Δ row × one edge).
   const uint64_t wsz = TROP ? 4 : 0;
-  kprof_end(ctx, kh, n * (sizeof(K) + wsz + 8 + 4) + total * (4 + wsz) + candidates * 4);
+  kprof_end(ctx, kh, n_rows * (sizeof(K) + wsz) + nh * (4 + 8 + 4 + 1) + total * (4 + wsz) + candidates * 4);
   after_launch(ctx, "k_expand_dense");
 }
 
@@ -497,16 +644,21 @@ uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, 
 }
 
 #define SK_INST_DENSE(K, T)                                                                                 \
-  template void dense_expand<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const uint64_t*,         \
-                                   uint64_t, uint64_t, int, uint64_t, int, uint64_t, int, int,               \
-                                   const uint32_t*, uint64_t, const uint32_t*, uint64_t, const int32_t*,     \
-                                   const DenseLayout&, uint32_t*, int32_t*, uint32_t*, uint64_t*);           \
+  template void dense_expand<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const uint32_t*,         \
+                                   const uint64_t*, const uint32_t*, const uint8_t*, uint64_t, uint64_t,     \
+                                   uint64_t, int, uint64_t, int, int, const uint32_t*, uint64_t,             \
+                                   const int32_t*, const DenseLayout&, uint32_t*, int32_t*, uint32_t*,       \
+                                   uint64_t*);                                                               \
   template uint64_t dense_marks_compact<K, T>(strata_ctx*, uint32_t*, const DenseLayout&, const int32_t*,    \
                                               K*, int32_t*, uint64_t, uint64_t*);                            \
   template void dense_seed<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const DenseLayout&,        \
                                  uint32_t*, int32_t*);                                                       \
   template uint64_t dense_compact<K, T>(strata_ctx*, const uint32_t*, const int32_t*, const DenseLayout&, K*, \
                                         int32_t*, uint64_t);
+template void dense_heads<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t,
+                                    uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint8_t*, uint64_t*);
+template void dense_heads<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t,
+                                    uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint8_t*, uint64_t*);
 SK_INST_DENSE(uint32_t, false)
 SK_INST_DENSE(uint32_t, true)
 SK_INST_DENSE(uint64_t, false)

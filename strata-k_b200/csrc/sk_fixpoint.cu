@@ -313,6 +313,9 @@ struct DenseIdx {
   DBuf<uint32_t> marks;  // changed in the current round
   DBuf<int32_t> D;       // Trop weights (INT32_MAX = absent)
   DBuf<uint64_t> states; // look-back words of the marks compaction
+  DBuf<uint32_t> hidx, hseg;  // group heads of the current Δ (row, CSR segment)
+  DBuf<uint8_t> hg;           // group sizes
+  DBuf<uint64_t> hsums;       // per-tile sums of the head compaction
   DenseLayout lay{};
   uint64_t entries = 0;
   uint64_t words() const { return (entries + 31) / 32; }
@@ -338,6 +341,7 @@ inline bool want_dense(strata_ctx* ctx, bool trop, bool narrow, uint64_t n0, uin
 template <bool TROP>
 void dense_alloc(strata_ctx* ctx, DenseIdx& X, uint64_t n0, uint64_t n1, int b1, bool colmajor) {
   X.bits.ctx = X.D.ctx = X.marks.ctx = X.states.ctx = ctx;
+  X.hidx.ctx = X.hseg.ctx = X.hg.ctx = X.hsums.ctx = ctx;
   X.entries = n0 * n1;
   X.lay = DenseLayout{b1, low_mask(b1), n0, n1, X.entries, colmajor};
   if (!TROP) {
@@ -359,29 +363,29 @@ uint64_t dense_round(strata_ctx* ctx, const K* dk, const int32_t* dw, uint64_t n
   const uint64_t l0 = ctx->launches;
   const int t = pt.begin(&a.join_ms);
   s.pos.reserve_grow(nd + 1);
-  SK_CUDA(cudaMemsetAsync(s.counts.p, 0, 16, ctx->stream));
-  expand_offsets<K>(ctx, dk, nd, js.jshift, js.jmask, csr.off.p, csr.n_nodes, s.pos.p, dense_group_max(),
-                    s.counts.p + 1);
-  SK_CUDA(cudaMemcpyAsync(s.counts.p, s.pos.p + nd, 8, cudaMemcpyDeviceToDevice, ctx->stream));
-  uint64_t tc[2] = {0, 0};
-  read_checked(ctx, s.counts.p, tc, 2);
-  const uint64_t T = tc[0], cands = tc[1];  // (group, edge) outputs; candidates
+  X.hidx.reserve_grow(nd + 1);
+  X.hseg.reserve_grow(nd + 1);
+  X.hg.reserve_grow(nd + 1);
+  X.hsums.reserve_grow(dense_heads_sums(nd));
+  uint64_t h3[3];
+  dense_heads<K>(ctx, dk, nd, js.jshift, js.jmask, csr.off.p, csr.n_nodes, X.hsums.p, X.hidx.p, s.pos.p, X.hseg.p,
+                 X.hg.p, h3);
+  const uint64_t nh = h3[0], T = h3[1], cands = h3[2];  // heads; (group, edge) outputs; candidates
   uint64_t cnt = 0;
   if (T) {
     const uint64_t cap = std::min<uint64_t>(cands, X.entries) + 1;
     out.reserve(cap, TROP);
-    splits.reserve_grow(ceil_div(nd + T, dense_tile_size()) + 2);
-    dense_expand<K, TROP>(ctx, dk, dw, nd, s.pos.p, T, cands, js.jshift, js.jmask, js.pshift, js.pmask,
-                          js.out_pshift, js.out_vshift, csr.off.p, csr.n_nodes, csr.nbr.p, csr.m,
-                          TROP ? csr.w.p : nullptr, X.lay, TROP ? nullptr : X.bits.p, TROP ? X.D.p : nullptr,
-                          X.marks.p, splits.p);
+    splits.reserve_grow(ceil_div(nh + T, dense_tile_size()) + 2);
+    dense_expand<K, TROP>(ctx, dk, dw, nd, X.hidx.p, s.pos.p, X.hseg.p, X.hg.p, nh, T, cands, js.pshift, js.pmask,
+                          js.out_pshift, js.out_vshift, csr.nbr.p, csr.m, TROP ? csr.w.p : nullptr, X.lay,
+                          TROP ? nullptr : X.bits.p, TROP ? X.D.p : nullptr, X.marks.p, splits.p);
     // Δ' sorted by the next join column, with merged weights; marks cleared.
     cnt = dense_marks_compact<K, TROP>(ctx, X.marks.p, X.lay, TROP ? X.D.p : nullptr, out.k.p,
                                        TROP ? out.w.p : nullptr, cap, X.states.p);
   }
   pt.end(t);
   const uint64_t wsz = TROP ? 4 : 0;
-  a.join_b += nd * (sizeof(K) + wsz + 16) + T * (4 + wsz) + cands * 4 + cnt * (sizeof(K) + 2 * wsz);
+  a.join_b += nd * (sizeof(K) + wsz) + nh * 17 + T * (4 + wsz) + cands * 4 + cnt * (sizeof(K) + 2 * wsz);
   a.join_l += (uint32_t)(ctx->launches - l0);
   a.cands += cands;
   return cnt;

@@ -42,10 +42,19 @@ struct DenseLayout {
 };
 uint64_t dense_tile_size();
 uint32_t dense_group_max();
+// Group heads of a Δ sorted by join value (see sk_dense.cu): writes hidx
+// (Δ row), hpos (exclusive degree prefix, hpos[nh] = total), hseg (CSR
+// segment start), hg (group size); out3 = {heads, outputs, candidates}.
+// `sums` holds dense_heads_sums(n) words.
+template <class K>
+void dense_heads(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uint64_t jmask, const uint32_t* off,
+                 uint64_t n_nodes, uint64_t* sums, uint32_t* hidx, uint64_t* hpos, uint32_t* hseg, uint8_t* hg,
+                 uint64_t* out3);
+uint64_t dense_heads_sums(uint64_t n);
 template <class K, bool TROP>
-void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n, const uint64_t* pos,
-                  uint64_t total, uint64_t candidates, int jshift, uint64_t jmask, int pshift, uint64_t pmask,
-                  int out_pshift, int out_vshift, const uint32_t* off, uint64_t n_nodes, const uint32_t* nbr,
+void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n_rows, const uint32_t* hidx,
+                  const uint64_t* hpos, const uint32_t* hseg, const uint8_t* hg, uint64_t nh, uint64_t total,
+                  uint64_t candidates, int pshift, uint64_t pmask, int out_pshift, int out_vshift, const uint32_t* nbr,
                   uint64_t n_nbr, const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D,
                   uint32_t* marks, uint64_t* splits_buf);
 template <class K, bool TROP>

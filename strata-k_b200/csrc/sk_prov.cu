@@ -355,9 +355,8 @@ void prov_tc_capture(strata_ctx* ctx, uint32_t n, const uint32_t* d_src, const u
   std::sort(targets.begin(), targets.end());
   targets.erase(std::unique(targets.begin(), targets.end()), targets.end());
   const uint64_t per_target = 2ull * n * (PV_KMAX * sizeof(ProofRec) + 1);
-  size_t fr = 0, tot = 0;
-  check_cuda(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
-  uint64_t budget = (uint64_t)((double)fr * 0.5);
+  release_all_cached(ctx);
+  uint64_t budget = (uint64_t)((double)reusable_device_bytes(ctx) * 0.5);
   if (ctx->cap && ctx->cap > ctx->in_use) budget = std::min<uint64_t>(budget, ctx->cap - ctx->in_use);
   if (ctx->tune_bs_budget_mb > 0) budget = std::min<uint64_t>(budget, ctx->tune_bs_budget_mb << 20);
   const uint64_t tw = std::max<uint64_t>(1, std::min<uint64_t>(targets.size() ? targets.size() : 1,

