@@ -328,6 +328,7 @@ class Job:
             rel = self.eng.tc_bool_dev(d["src"], d["dst"])
         elif self.kind == "prov":
             t0 = time.perf_counter()
+            self.eng.on_torch_stream()
             pr = self.eng.prov_capture(self.wl.n, d["src"], d["dst"], d["p64"], self.wl.qs, self.wl.qt, k=8)
             t1 = time.perf_counter()
             circ = self.eng.compile_circuits(pr, len(self.wl.src))
@@ -426,7 +427,8 @@ def run_ours(args):
     stream.synchronize()
 
     def step():
-        return job.run(d)
+        with torch.cuda.stream(stream):
+            return job.run(d)
 
     for _ in range(args.warmup):
         job.free(step()[0])

@@ -28,8 +28,12 @@
 #include "sk_rel.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <exception>
 #include <map>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 
@@ -41,6 +45,17 @@ using Dnf = std::vector<Lits>;  // sorted, absorption-minimal, ordered
 
 inline bool subset_of(const Lits& a, const Lits& b) { return std::includes(b.begin(), b.end(), a.begin(), a.end()); }
 
+struct DnfHash {
+  size_t operator()(const std::vector<std::vector<int64_t>>& d) const {
+    uint64_t h = 0x9e3779b97f4a7c15ull ^ d.size();
+    for (auto& p : d) {
+      h = (h ^ (0x100000001b3ull * p.size())) * 0xbf58476d1ce4e5b9ull;
+      for (auto l : p) h = (h ^ (uint64_t)l) * 0x94d049bb133111ebull;
+    }
+    return (size_t)(h ^ (h >> 31));
+  }
+};
+
 struct HNode {
   uint8_t kind;
   uint32_t leaf;
@@ -49,7 +64,7 @@ struct HNode {
 
 struct Compiler {
   std::vector<HNode> nodes;
-  std::map<Dnf, uint32_t> memo;
+  std::unordered_map<Dnf, uint32_t, DnfHash> memo;
   uint64_t max_nodes;
   uint32_t num_leaves = 0;
 
@@ -238,65 +253,121 @@ T* dev_upload(strata_ctx* ctx, const std::vector<T>& h) {
 
 }  // namespace
 
+// One query's circuit, levelled, with query-local node indices.
+struct QCircuit {
+  std::vector<uint8_t> kind;
+  std::vector<uint32_t> A, B, CH, lvl;
+  uint32_t root = 0, levels = 0;
+};
+
+static void compile_query(const uint64_t* proof_off, const uint64_t* lit_off, const int64_t* lits, uint32_t q,
+                          uint32_t n_leaves, uint64_t max_nodes, QCircuit& out) {
+  std::vector<Lits> proofs;
+  for (uint64_t pi = proof_off[q]; pi < proof_off[q + 1]; pi++) {
+    Lits p(lits + lit_off[pi], lits + lit_off[pi + 1]);
+    for (auto l : p)
+      if (l == 0 || (uint64_t)(l < 0 ? -l : l) > n_leaves)
+        fail(STRATA_E_INVALID, "a literal is 0 or names a leaf beyond n_leaves");
+    proofs.push_back(std::move(p));
+  }
+  Compiler cp;
+  cp.max_nodes = max_nodes;
+  const uint32_t r = cp.shannon(Compiler::normalize(proofs));
+  const uint32_t nn = (uint32_t)cp.nodes.size();
+  std::vector<uint32_t> level(nn, 0);
+  uint32_t top = 0;
+  for (uint32_t i = 0; i < nn; i++) {
+    uint32_t lv = 0;
+    for (auto c : cp.nodes[i].ch) lv = std::max(lv, level[c] + 1);
+    level[i] = lv;
+    top = std::max(top, lv);
+  }
+  // counting sort by level (stable)
+  std::vector<uint32_t> start(top + 2, 0), pos(nn);
+  for (uint32_t i = 0; i < nn; i++) start[level[i] + 1]++;
+  for (uint32_t L = 0; L <= top; L++) start[L + 1] += start[L];
+  out.lvl.assign(start.begin(), start.end());
+  {
+    std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+    for (uint32_t i = 0; i < nn; i++) pos[i] = fill[level[i]]++;
+  }
+  std::vector<uint32_t> order(nn);
+  for (uint32_t i = 0; i < nn; i++) order[pos[i]] = i;
+  out.kind.resize(nn);
+  out.A.resize(nn);
+  out.B.resize(nn);
+  for (uint32_t j = 0; j < nn; j++) {
+    const HNode& h = cp.nodes[order[j]];
+    out.kind[j] = h.kind;
+    if (h.kind <= 1) {
+      out.A[j] = h.leaf;
+      out.B[j] = 0;
+    } else {
+      out.A[j] = (uint32_t)out.CH.size();
+      out.B[j] = (uint32_t)h.ch.size();
+      for (auto c : h.ch) out.CH.push_back(pos[c]);
+    }
+  }
+  out.root = pos[r];
+  out.levels = top + 1;
+}
+
 // Compile every query's proofs (queries given as proof lists of signed
-// literals) into one levelled device DAG.
+// literals) into one levelled device DAG; queries compile in parallel on the
+// host threads.
 strata_circuits* circuits_compile(strata_ctx* ctx, uint32_t nq, const uint64_t* proof_off, const uint64_t* lit_off,
                                   const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes) {
-  std::vector<uint8_t> kind;
-  std::vector<uint32_t> A, B, CH, root(nq), lvl;
+  std::vector<QCircuit> qc(nq);
+  {
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const unsigned T = std::min<unsigned>(hw, std::max<uint32_t>(1, nq));
+    std::atomic<uint32_t> next{0};
+    std::vector<std::exception_ptr> errs(T);
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < T; t++)
+      th.emplace_back([&, t]() {
+        try {
+          while (true) {
+            const uint32_t q = next.fetch_add(1);
+            if (q >= nq) break;
+            compile_query(proof_off, lit_off, lits, q, n_leaves, max_nodes, qc[q]);
+          }
+        } catch (...) {
+          errs[t] = std::current_exception();
+          next.store(nq);
+        }
+      });
+    for (auto& x : th) x.join();
+    for (auto& e : errs)
+      if (e) std::rethrow_exception(e);
+  }
   std::vector<uint64_t> qnode(nq + 1, 0), qlevel(nq + 1, 0);
+  uint64_t total_ch = 0, total_lvl = 0;
   uint32_t max_levels = 0;
   for (uint32_t q = 0; q < nq; q++) {
-    std::vector<Lits> proofs;
-    for (uint64_t pi = proof_off[q]; pi < proof_off[q + 1]; pi++) {
-      Lits p(lits + lit_off[pi], lits + lit_off[pi + 1]);
-      for (auto l : p)
-        if (l == 0 || (uint64_t)(l < 0 ? -l : l) > n_leaves)
-          fail(STRATA_E_INVALID, "a literal is 0 or names a leaf beyond n_leaves");
-      proofs.push_back(std::move(p));
+    qnode[q + 1] = qnode[q] + qc[q].kind.size();
+    qlevel[q + 1] = qlevel[q] + qc[q].lvl.size();
+    total_ch += qc[q].CH.size();
+    max_levels = std::max(max_levels, qc[q].levels);
+  }
+  total_lvl = qlevel[nq];
+  if (qnode[nq] >= (1ull << 32) || total_ch >= (1ull << 32))
+    fail(STRATA_E_UNSUPPORTED, "circuits limited to 2^32 nodes in total");
+  std::vector<uint8_t> kind(qnode[nq]);
+  std::vector<uint32_t> A(qnode[nq]), B(qnode[nq]), CH(total_ch), root(nq), lvl(total_lvl);
+  uint64_t chb = 0;
+  for (uint32_t q = 0; q < nq; q++) {
+    const QCircuit& c = qc[q];
+    const uint64_t nb = qnode[q];
+    std::copy(c.kind.begin(), c.kind.end(), kind.begin() + (long)nb);
+    for (size_t j = 0; j < c.kind.size(); j++) {
+      A[nb + j] = c.kind[j] <= 1 ? c.A[j] : (uint32_t)(chb + c.A[j]);
+      B[nb + j] = c.B[j];
     }
-    Compiler cp;
-    cp.max_nodes = max_nodes;
-    const uint32_t r = cp.shannon(Compiler::normalize(proofs));
-    // level: leaves/constants 0, else 1 + max child level
-    const uint32_t nn = (uint32_t)cp.nodes.size();
-    std::vector<uint32_t> level(nn, 0);
-    uint32_t top = 0;
-    for (uint32_t i = 0; i < nn; i++) {
-      uint32_t lv = 0;
-      for (auto c : cp.nodes[i].ch) lv = std::max(lv, level[c] + 1);
-      level[i] = lv;
-      top = std::max(top, lv);
-    }
-    // stable order by level
-    std::vector<uint32_t> order(nn), pos(nn);
-    for (uint32_t i = 0; i < nn; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return level[x] < level[y]; });
-    for (uint32_t i = 0; i < nn; i++) pos[order[i]] = i;
-    const uint64_t base = qnode[q];
-    qnode[q + 1] = base + nn;
-    root[q] = (uint32_t)(base + pos[r]);
-    for (uint32_t i = 0; i < nn; i++) {
-      const HNode& h = cp.nodes[order[i]];
-      kind.push_back(h.kind);
-      if (h.kind <= 1) {
-        A.push_back(h.leaf);
-        B.push_back(0);
-      } else {
-        A.push_back((uint32_t)CH.size());
-        B.push_back((uint32_t)h.ch.size());
-        for (auto c : h.ch) CH.push_back((uint32_t)(base + pos[c]));
-      }
-    }
-    qlevel[q] = lvl.size();
-    for (uint32_t L = 0, i = 0; L <= top; L++) {
-      lvl.push_back(i);
-      while (i < nn && level[order[i]] == L) i++;
-    }
-    lvl.push_back(nn);
-    qlevel[q + 1] = lvl.size();
-    max_levels = std::max(max_levels, top + 1);
-    if (qnode[q + 1] >= (1ull << 32)) fail(STRATA_E_UNSUPPORTED, "circuits limited to 2^32 nodes in total");
+    for (size_t j = 0; j < c.CH.size(); j++) CH[chb + j] = (uint32_t)(nb + c.CH[j]);
+    chb += c.CH.size();
+    root[q] = (uint32_t)(nb + c.root);
+    std::copy(c.lvl.begin(), c.lvl.end(), lvl.begin() + (long)qlevel[q]);
   }
   auto* c = new strata_circuits();
   c->n_queries = nq;

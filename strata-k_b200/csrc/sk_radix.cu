@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
                                                  uint32_t n, int shift, int dbits,
                                                  const uint32_t* __restrict__ binoff,
                                                  uint32_t* lookback, uint32_t* tile_counter,
-                                                 uint32_t* status) {
+                                                 uint32_t* status, int match_rank) {
   constexpr uint32_t TILE = NT * ITEMS;
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_whist[NW][RADIX];
@@ -130,10 +130,24 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
     const uint32_t idx = wbase + j * 32 + lane;
     const bool valid = idx < n;
     const uint32_t d = (uint32_t)(key[j] >> shift) & dmask;
-    unsigned peers = __ballot_sync(kFull, valid);
-    for (int b = 0; b < dbits; b++) {
-      const unsigned bb = __ballot_sync(kFull, (d >> b) & 1u);
-      peers &= ((d >> b) & 1u) ? bb : ~bb;
+    unsigned peers;
+    if (match_rank) {
+      // one match instruction (invalid lanes carry a digit no valid lane has)
+      peers = __match_any_sync(kFull, valid ? d : (0x100u | (uint32_t)lane));
+    } else {
+      peers = __ballot_sync(kFull, valid);
+      if (dbits == 8) {
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+          const unsigned bb = __ballot_sync(kFull, (d >> b) & 1u);
+          peers &= ((d >> b) & 1u) ? bb : ~bb;
+        }
+      } else {
+        for (int b = 0; b < dbits; b++) {
+          const unsigned bb = __ballot_sync(kFull, (d >> b) & 1u);
+          peers &= ((d >> b) & 1u) ? bb : ~bb;
+        }
+      }
     }
     uint32_t prior = valid ? s_whist[warp][d] : 0u;
     rank[j] = prior + __popc(peers & lt);
@@ -264,13 +278,13 @@ void radix_sort_impl(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, boo
       SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, *vals, *valt, (uint32_t)n, 8 * p, dbits,
                                               binoff.p + p * RADIX, lookback.p, counters + p,
-                                              ctx->d_status);
+                                              ctx->d_status, ctx->tune_sort_match);
     } else {
       auto kern = k_onesweep<K, V, false, ITEMS>;
       SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, nullptr, nullptr, (uint32_t)n, 8 * p,
                                               dbits, binoff.p + p * RADIX, lookback.p,
-                                              counters + p, ctx->d_status);
+                                              counters + p, ctx->d_status, ctx->tune_sort_match);
     }
     kprof_end(ctx, kh, 2 * n * (sizeof(K) + (has_vals ? sizeof(V) : 0)));
     after_launch(ctx, "k_onesweep");
@@ -357,7 +371,7 @@ void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* ou
     check_cuda(cudaMemsetAsync(lookback, 0, sizeof(uint32_t) * ntiles * RADIX, stream), "cudaMemsetAsync");
     auto kern = k_onesweep<uint32_t, uint32_t, false, ITEMS>;
     kern<<<ntiles, NT, smem, stream>>>(src, dst, nullptr, nullptr, (uint32_t)n, 8 * p, std::min(8, bits - 8 * p),
-                                       binoff + p * RADIX, lookback, counters + p, status);
+                                       binoff + p * RADIX, lookback, counters + p, status, 0);
     src = dst;
   }
   check_cuda(cudaGetLastError(), "launch");

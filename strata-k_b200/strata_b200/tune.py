@@ -26,6 +26,7 @@ OTHER = {
     3: (1, 2),                # triangle membership test: hash set / binary search
     4: (2, 4, 8, 16, 32),     # bit-row rounds per CUDA-graph replay (batched closure)
     5: (0, 2, 4, 8),          # resident round-kernel blocks per SM (0 = occupancy limit)
+    7: (1, 2),                # radix digit ranking: ballots / match instruction
 }
 
 
@@ -104,6 +105,15 @@ def sweep(n: int = 64_000_000, verbose: bool = True, batch_instances: int = 512)
                 res[v] = _time_sort(eng, torch, n if kb == 4 else n // 2, kb, bits)
             eng.set_knob(knob, 0)
             record(knob, res)
+        # radix ranking method (u32 keys at the tuned tile size)
+        res = {}
+        eng.set_knob(1, best[1])
+        for v in OTHER[7]:
+            eng.set_knob(7, v)
+            res[v] = _time_sort(eng, torch, n, 4, 26)
+        eng.set_knob(7, 0)
+        eng.set_knob(1, 0)
+        record(7, res)
         # triangle probe on an oriented R-MAT graph
         tw = gen.triangle_workload(scale=18, seed=7)
         tx = torch.from_numpy(tw.src.astype(np.int32)).cuda()

@@ -502,3 +502,28 @@ def test_sort_knobs_fixpoint_identical(engine):
         assert np.array_equal(base.w, r.w)
     engine.set_knob(1, 0)
     engine.set_plan(0)
+
+
+@pytest.mark.parametrize("rank", [1, 2])
+def test_sort_rank_methods_identical(engine, rank):
+    """Ballot and match-instruction digit ranking sort identically (stable)."""
+    import ctypes as C
+    engine.set_knob(7, rank)
+    try:
+        for n, kb, bits in ((5000, 4, 27), (300_001, 4, 26), (70_001, 8, 45)):
+            rng = np.random.default_rng(n + rank)
+            kdt = np.uint32 if kb == 4 else np.uint64
+            keys = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(kdt)
+            keys[: n // 4] = keys[1]
+            vals = np.arange(n, dtype=np.uint32)
+            order = np.argsort(keys, kind="stable")
+            ki, vi = _dev(keys, np.int32 if kb == 4 else np.int64), _dev(vals, np.int32)
+            import torch
+            ko, vo = torch.empty_like(ki), torch.empty_like(vi)
+            engine._check(engine.lib.strata_op_sort(engine.ctx, kb, 4, C.c_void_p(ki.data_ptr()),
+                                                    C.c_void_p(vi.data_ptr()), C.c_void_p(ko.data_ptr()),
+                                                    C.c_void_p(vo.data_ptr()), n, bits))
+            assert np.array_equal(ko.cpu().numpy().view(kdt), keys[order])
+            assert np.array_equal(vo.cpu().numpy().view(np.uint32), vals[order])
+    finally:
+        engine.set_knob(7, 0)
