@@ -81,6 +81,8 @@ strata_status strata_ctx_create(int device, uint64_t mem_cap_bytes, strata_ctx**
 void strata_ctx_destroy(strata_ctx* ctx);
 /* Use an existing cudaStream_t (passed as void*) for all work; NULL = own stream. */
 strata_status strata_ctx_set_stream(strata_ctx* ctx, void* stream);
+/* Wait for all work queued on the context's stream (the asynchronous calls). */
+strata_status strata_ctx_synchronize(strata_ctx* ctx);
 const char* strata_last_error(const strata_ctx* ctx);
 /* Device bytes currently held and the high-water mark. */
 strata_status strata_ctx_mem(const strata_ctx* ctx, uint64_t* in_use, uint64_t* peak);

@@ -53,7 +53,6 @@ struct BsView {
   const uint8_t* lshift;  // log2(lanes per row)
   const uint64_t* row_base;
   const uint64_t* vec_base;
-  const uint64_t* mask_base;  // first chunk-mask word of the instance
   uint64_t* delta;   // |Δ'| of the current round
   uint64_t* total;   // |path| so far
   uint32_t* rounds;
@@ -72,8 +71,6 @@ struct BsView {
   uint4* D1;
   uint8_t* f0;
   uint8_t* f1;
-  uint32_t* M0;  // per Δ row, one bit per 128-bit chunk: the chunk is non-zero
-  uint32_t* M1;
   unsigned long long* bytes;  // algorithmic bytes of the rounds (profiling), or null
   uint32_t* status;
 };
@@ -96,7 +93,7 @@ __device__ __forceinline__ uint32_t unit_owner(const uint64_t* uprefix, uint32_t
 // One semi-naive round over every active instance of the wave.  Reads Δ from
 // (D_PAR, f_PAR), writes Δ' to the other buffer pair and updates F.
 template <int PAR>
-__global__ void __launch_bounds__(BS_NT, 4) k_bs_round(BsView v) {
+__global__ void __launch_bounds__(BS_NT) k_bs_round(BsView v) {
   const uint32_t n_act = *v.n_act;
   const uint64_t U = *v.u_total;
   const uint4* __restrict__ Dc = PAR ? v.D1 : v.D0;
@@ -128,21 +125,13 @@ __global__ void __launch_bounds__(BS_NT, 4) k_bs_round(BsView v) {
     const bool row_has = valid && (bal_y & smask) != 0u;
     bool row_any = false;
     uint32_t cnt = 0;
-    const uint32_t MW = (W + 31) >> 5;  // chunk-mask words per row
-    const uint64_t mb = v.mask_base[i];
-    const uint32_t* __restrict__ Mc = PAR ? v.M1 : v.M0;
-    uint32_t* __restrict__ Mn = PAR ? v.M0 : v.M1;
-    uint32_t loads = 0, mreads = 0, acc_words = 0, writes = 0;
-    // Chunk groups of lpr chunks; the loop count is the same for every lane
-    // of the warp (one instance), so the mask ballot below is converged.
-    for (uint32_t c0 = 0; c0 < W; c0 += lpr) {
-      const uint32_t c = c0 + sl;
-      bool nz = false;
-      if (row_has && c < W) {
+    if (row_has) {
+      uint32_t active_edges = 0, acc_words = 0;
+      for (uint32_t c = sl; c < W; c += lpr) {
         uint4 acc = make_uint4(0u, 0u, 0u, 0u);
-        const uint32_t mword = c >> 5, mbit = 1u << (c & 31);
-        // four edges at a time: neighbour, flag, chunk-mask and Δ-chunk loads
-        // of the four are independent, so they are in flight together
+        active_edges = 0;
+        // four edges at a time: their neighbour, flag and Δ-row loads are
+        // independent, so they are in flight together
         for (uint64_t e = e0; e < e1; e += 4) {
           uint32_t y[4];
           bool on[4];
@@ -150,13 +139,6 @@ __global__ void __launch_bounds__(BS_NT, 4) k_bs_round(BsView v) {
           for (int q = 0; q < 4; q++) y[q] = e + q < e1 ? v.nbr[e + q] : 0xffffffffu;
 #pragma unroll
           for (int q = 0; q < 4; q++) on[q] = y[q] < n && fc[rb + y[q]] != 0;
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            if (on[q]) {
-              mreads++;
-              on[q] = (Mc[mb + (uint64_t)y[q] * MW + mword] & mbit) != 0u;
-            }
-          }
           uint4 d[4];
 #pragma unroll
           for (int q = 0; q < 4; q++) d[q] = on[q] ? Dc[vb + (uint64_t)y[q] * W + c] : make_uint4(0u, 0u, 0u, 0u);
@@ -166,37 +148,30 @@ __global__ void __launch_bounds__(BS_NT, 4) k_bs_round(BsView v) {
             acc.y |= d[q].y;
             acc.z |= d[q].z;
             acc.w |= d[q].w;
-            loads += on[q] ? 1u : 0u;
+            active_edges += on[q] ? 1u : 0u;
           }
         }
+        uint4 nw = make_uint4(0u, 0u, 0u, 0u);
         if (any4(acc)) {
           acc_words++;
           uint4* fp = v.F + vb + X * W + c;
           uint4 f = *fp;
-          const uint4 nw = make_uint4(acc.x & ~f.x, acc.y & ~f.y, acc.z & ~f.z, acc.w & ~f.w);
+          nw = make_uint4(acc.x & ~f.x, acc.y & ~f.y, acc.z & ~f.z, acc.w & ~f.w);
           if (any4(nw)) {
             f = make_uint4(f.x | nw.x, f.y | nw.y, f.z | nw.z, f.w | nw.w);
             *fp = f;
             cnt += popc4(nw);
             row_any = true;
-            nz = true;
-            Dn[vb + X * W + c] = nw;  // zero chunks are not written: the mask says so
-            writes++;
           }
         }
+        Dn[vb + X * W + c] = nw;
       }
-      const unsigned b = __ballot_sync(kFull, nz);
-      if (row_has && sl == 0) {
-        const uint32_t bits = ls == 5 ? b : ((b >> (sub << ls)) & ((1u << lpr) - 1u));
-        Mn[mb + X * MW + (c0 >> 5)] = bits;
+      if (v.bytes) {
+        // this lane's words: Δ rows read, Δ' written, path read (and written
+        // where bits are new); its share of the edge list and flags
+        const uint64_t lw = (W > sl) ? (W - sl + lpr - 1) / lpr : 0;
+        moved += lw * 16ull * (active_edges + 1) + acc_words * 32ull + (sl == 0 ? (e1 - e0) * 5ull : 0ull);
       }
-    }
-    if (v.bytes && row_has) {
-      // Δ chunks and chunk-mask words read, path chunks read and written
-      // where the join is non-empty, Δ' chunks and mask words written, and
-      // (one lane per row) the edge list and the flags
-      moved += (uint64_t)loads * 16 + (uint64_t)mreads * 4 + (uint64_t)acc_words * 32 + (uint64_t)writes * 16 +
-               (sl == 0 ? (uint64_t)MW * 4 + (e1 - e0) * 5 : 0);
     }
     const unsigned bal = __ballot_sync(kFull, row_any);
     if (valid && sl == 0) fn[rb + X] = (bal & smask) != 0u ? 1 : 0;
@@ -344,8 +319,6 @@ __global__ void k_bs_seed(const uint32_t* __restrict__ src, const uint32_t* __re
         const uint32_t bit = 1u << (y & 31);
         const uint32_t old = atomicOr(&Fw[y >> 5], bit);
         fresh = (old & bit) ? 0u : 1u;
-        const uint32_t ch = y >> 7, mw = (v.w4[i] + 31) >> 5;
-        atomicOr(&v.M0[v.mask_base[i] + (uint64_t)x * mw + (ch >> 5)], 1u << (ch & 31));
       }
     }
     // per-instance distinct-edge counts (warp-aggregated when the warp is one instance)
@@ -426,14 +399,13 @@ inline uint32_t lanes_shift(uint32_t w4) {
 struct BsBuffers {
   DBuf<uint32_t> n_rows, n_cols, w4, act, n_act, deg, bad;
   DBuf<uint8_t> lshift, active, f0, f1;
-  DBuf<uint64_t> row_base, vec_base, mask_base, delta, total, uprefix, u_total, off, cursor, eoff, sums, bytes;
-  DBuf<uint32_t> rounds, nbr, M0, M1;
+  DBuf<uint64_t> row_base, vec_base, delta, total, uprefix, u_total, off, cursor, eoff, sums, bytes;
+  DBuf<uint32_t> rounds, nbr;
   DBuf<uint4> F, D0, D1;
   explicit BsBuffers(strata_ctx* c) {
-    for (auto* b : {&n_rows, &n_cols, &w4, &act, &n_act, &deg, &bad, &rounds, &nbr, &M0, &M1}) b->ctx = c;
+    for (auto* b : {&n_rows, &n_cols, &w4, &act, &n_act, &deg, &bad, &rounds, &nbr}) b->ctx = c;
     for (auto* b : {&lshift, &active, &f0, &f1}) b->ctx = c;
-    for (auto* b : {&row_base, &vec_base, &mask_base, &delta, &total, &uprefix, &u_total, &off, &cursor, &eoff,
-                    &sums, &bytes})
+    for (auto* b : {&row_base, &vec_base, &delta, &total, &uprefix, &u_total, &off, &cursor, &eoff, &sums, &bytes})
       b->ctx = c;
     F.ctx = D0.ctx = D1.ctx = c;
   }
@@ -445,7 +417,6 @@ struct BsBuffers {
     v.lshift = lshift.p;
     v.row_base = row_base.p;
     v.vec_base = vec_base.p;
-    v.mask_base = mask_base.p;
     v.delta = delta.p;
     v.total = total.p;
     v.rounds = rounds.p;
@@ -461,8 +432,6 @@ struct BsBuffers {
     v.D1 = D1.p;
     v.f0 = f0.p;
     v.f1 = f1.p;
-    v.M0 = M0.p;
-    v.M1 = M1.p;
     v.bytes = profile ? reinterpret_cast<unsigned long long*>(bytes.p) : nullptr;
     v.status = nullptr;
     return v;
@@ -476,9 +445,8 @@ struct InstSpec {
 
 inline uint64_t inst_w4(const InstSpec& s) { return std::max<uint64_t>(1, ceil_div(s.cols, 128)); }
 inline uint64_t inst_vecs(const InstSpec& s) { return (uint64_t)s.rows * inst_w4(s); }
-inline uint64_t inst_mask_words(const InstSpec& s) { return (uint64_t)s.rows * ((inst_w4(s) + 31) / 32); }
 inline uint64_t inst_bytes(const InstSpec& s) {
-  return 3 * inst_vecs(s) * 16 + inst_mask_words(s) * 8 + (uint64_t)s.rows * (2 + 4 + 16) + (s.e1 - s.e0) * 4 + 64;
+  return 3 * inst_vecs(s) * 16 + (uint64_t)s.rows * (2 + 4 + 16) + (s.e1 - s.e0) * 4 + 64;
 }
 
 struct BsResult {
@@ -547,19 +515,17 @@ void bs_run(strata_ctx* ctx, const std::vector<InstSpec>& spec, const uint32_t* 
     }
   }
   // size the fixed buffers for the largest wave
-  uint64_t max_rows = 1, max_vecs = 1, max_edges = 1, max_w32 = 1, max_masks = 1;
+  uint64_t max_rows = 1, max_vecs = 1, max_edges = 1, max_w32 = 1;
   uint32_t max_n = 1;
   for (auto& w : waves) {
-    uint64_t rows = 0, vecs = 0, edges = 0, masks = 0;
+    uint64_t rows = 0, vecs = 0, edges = 0;
     for (uint32_t k = w.first; k < w.second; k++) {
       const InstSpec& s = spec[order[k]];
       rows += s.rows;
       vecs += inst_vecs(s);
-      masks += inst_mask_words(s);
       edges += s.e1 - s.e0;
       max_w32 = std::max<uint64_t>(max_w32, 4 * inst_w4(s));
     }
-    max_masks = std::max(max_masks, masks);
     max_rows = std::max(max_rows, rows);
     max_vecs = std::max(max_vecs, vecs);
     max_edges = std::max(max_edges, edges);
@@ -572,9 +538,6 @@ void bs_run(strata_ctx* ctx, const std::vector<InstSpec>& spec, const uint32_t* 
   B.lshift.reserve(max_n);
   B.row_base.reserve(max_n);
   B.vec_base.reserve(max_n);
-  B.mask_base.reserve(max_n);
-  B.M0.reserve(max_masks);
-  B.M1.reserve(max_masks);
   B.delta.reserve(max_n);
   B.total.reserve(max_n);
   B.rounds.reserve(max_n);
@@ -634,7 +597,7 @@ void bs_run(strata_ctx* ctx, const std::vector<InstSpec>& spec, const uint32_t* 
 
   std::vector<uint32_t> h_rows, h_cols, h_w4;
   std::vector<uint8_t> h_ls, h_act;
-  std::vector<uint64_t> h_rb, h_vb, h_mb, h_eoff, h_up;
+  std::vector<uint64_t> h_rb, h_vb, h_eoff, h_up;
   std::vector<uint32_t> h_actl;
   for (auto& w : waves) {
     const uint32_t nw = w.second - w.first;
@@ -644,13 +607,10 @@ void bs_run(strata_ctx* ctx, const std::vector<InstSpec>& spec, const uint32_t* 
     h_ls.resize(nw);
     h_rb.resize(nw);
     h_vb.resize(nw);
-    h_mb.resize(nw);
     h_eoff.resize(nw + 1);
-    uint64_t rows = 0, vecs = 0, edges = 0, masks = 0;
+    uint64_t rows = 0, vecs = 0, edges = 0;
     for (uint32_t k = 0; k < nw; k++) {
       const InstSpec& s = spec[order[w.first + k]];
-      h_mb[k] = masks;
-      masks += inst_mask_words(s);
       h_rows[k] = s.rows;
       h_cols[k] = s.cols;
       h_w4[k] = (uint32_t)inst_w4(s);
@@ -670,8 +630,6 @@ void bs_run(strata_ctx* ctx, const std::vector<InstSpec>& spec, const uint32_t* 
     SK_CUDA(cudaMemcpyAsync(B.lshift.p, h_ls.data(), nw, cudaMemcpyHostToDevice, ctx->stream));
     SK_CUDA(cudaMemcpyAsync(B.row_base.p, h_rb.data(), nw * 8, cudaMemcpyHostToDevice, ctx->stream));
     SK_CUDA(cudaMemcpyAsync(B.vec_base.p, h_vb.data(), nw * 8, cudaMemcpyHostToDevice, ctx->stream));
-    SK_CUDA(cudaMemcpyAsync(B.mask_base.p, h_mb.data(), nw * 8, cudaMemcpyHostToDevice, ctx->stream));
-    SK_CUDA(cudaMemsetAsync(B.M0.p, 0, masks * 4, ctx->stream));
     SK_CUDA(cudaMemcpyAsync(B.eoff.p, h_eoff.data(), (nw + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
     d_src_w.reserve(edges + 1);
     d_dst_w.reserve(edges + 1);

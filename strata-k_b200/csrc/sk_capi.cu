@@ -168,6 +168,13 @@ strata_status strata_ctx_set_stream(strata_ctx* ctx, void* stream) {
   SK_GUARD_END(ctx)
 }
 
+strata_status strata_ctx_synchronize(strata_ctx* ctx) {
+  if (!ctx) return STRATA_E_INVALID;
+  SK_GUARD_BEGIN
+  sk::sync_and_check(ctx);
+  SK_GUARD_END(ctx)
+}
+
 const char* strata_last_error(const strata_ctx* ctx) {
   return ctx ? ctx->last_error.c_str() : "no context";
 }

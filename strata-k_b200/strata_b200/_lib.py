@@ -102,6 +102,7 @@ SIGNATURES = {
     "strata_ctx_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(ctxp)]),
     "strata_ctx_destroy": (None, [ctxp]),
     "strata_ctx_set_stream": (C.c_int, [ctxp, vp]),
+    "strata_ctx_synchronize": (C.c_int, [ctxp]),
     "strata_last_error": (C.c_char_p, [ctxp]),
     "strata_ctx_mem": (C.c_int, [ctxp, u64p, u64p]),
     "strata_ctx_set_profiling": (C.c_int, [ctxp, C.c_int]),

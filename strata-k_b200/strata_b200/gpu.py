@@ -215,14 +215,26 @@ class Engine:
         self._check(self.lib.strata_ctx_set_stream(self.ctx, C.c_void_p(stream_handle or 0)))
         self._stream = stream_handle or 0
 
-    def on_torch_stream(self):
-        """Make the context run on torch's current CUDA stream, so that
-        asynchronous calls (the circuit kernels) are ordered with the torch
-        work that produces their inputs and consumes their outputs."""
+    def synchronize(self):
+        """Wait for the work queued on the context's stream."""
+        self._check(self.lib.strata_ctx_synchronize(self.ctx))
+
+    def on_torch_stream(self) -> bool:
+        """Order the context's next asynchronous calls (the circuit kernels)
+        with torch's current CUDA stream: run on that stream when it is a
+        created stream; for the legacy default stream (handle 0, which a
+        non-blocking stream does not wait for) finish torch's queued work now
+        and return True — the caller then synchronizes after its call."""
         import torch
         h = torch.cuda.current_stream().cuda_stream
-        if getattr(self, "_stream", None) != h:
-            self.set_stream(h)
+        if h:
+            if getattr(self, "_stream", None) != h:
+                self.set_stream(h)
+            return False
+        torch.cuda.current_stream().synchronize()
+        if getattr(self, "_stream", None):
+            self.set_stream(None)
+        return True
 
     def set_plan(self, plan: int):
         """0 automatic, 1 sort-merge, 2 direct-addressed, 3 bit rows (Bool closure only);
@@ -508,27 +520,33 @@ class Circuits:
         """P per query for FP32 leaf probabilities p (a CUDA tensor)."""
         import torch
         out = torch.empty(self.n_queries, dtype=torch.float64 if out64 else torch.float32, device=p.device)
-        self.eng.on_torch_stream()
+        after = self.eng.on_torch_stream()
         self.eng._check(self.eng.lib.strata_circuits_forward(
             self.eng.ctx, self.h, _dp(p), None if out64 else _dp(out), _dp(out) if out64 else None))
+        if after:
+            self.eng.synchronize()
         return out
 
     def vjp(self, p, seed=None):
         """Σ_q seed[q] · dP_q/dp (FP32 tensor of n_leaves; FP64 accumulation)."""
         import torch
         g64 = torch.empty(max(1, self.n_leaves), dtype=torch.float64, device=p.device)
-        self.eng.on_torch_stream()
         g32 = torch.empty(max(1, self.n_leaves), dtype=torch.float32, device=p.device)
+        after = self.eng.on_torch_stream()
         self.eng._check(self.eng.lib.strata_circuits_vjp(self.eng.ctx, self.h, _dp(p), _dp(seed), _dp(g64),
                                                          _dp(g32)))
+        if after:
+            self.eng.synchronize()
         return g32[:self.n_leaves], g64[:self.n_leaves]
 
     def grads(self, p):
         """[n_queries, n_leaves] FP64 per-query gradients (the ?grad rows)."""
         import torch
         g = torch.empty((max(1, self.n_queries), max(1, self.n_leaves)), dtype=torch.float64, device=p.device)
-        self.eng.on_torch_stream()
+        after = self.eng.on_torch_stream()
         self.eng._check(self.eng.lib.strata_circuits_grads(self.eng.ctx, self.h, _dp(p), _dp(g)))
+        if after:
+            self.eng.synchronize()
         return g[:self.n_queries, :self.n_leaves]
 
     def free(self):
