@@ -327,20 +327,13 @@ class Job:
         elif self.kind == "tc":
             rel = self.eng.tc_bool_dev(d["src"], d["dst"])
         elif self.kind == "prov":
-            t0 = time.perf_counter()
             self.eng.on_torch_stream()
-            pr = self.eng.prov_capture(self.wl.n, d["src"], d["dst"], d["p64"], self.wl.qs, self.wl.qt, k=8)
-            t1 = time.perf_counter()
-            circ = self.eng.compile_circuits(pr, len(self.wl.src))
-            t2 = time.perf_counter()
-            P = circ.forward(d["p32"])
-            G = circ.grads(d["p32"])
+            P, G, circ, info = self.eng.grad_queries(self.wl.n, d["src"], d["dst"], d["p64"], d["p32"],
+                                                     self.wl.qs, self.wl.qt, k=8, chunks=4)
             self.torch.cuda.current_stream().synchronize()
             self.last = (P, G)
             nodes, levels = circ.shape()
-            return circ, len(self.wl.qs), {"prov": pr.stats, "capture_s": t1 - t0, "compile_s": t2 - t1,
-                                           "circuit_nodes": nodes, "circuit_levels": levels,
-                                           "proofs": int(pr.proof_off[-1])}
+            return circ, len(self.wl.qs), {"prov": info, "circuit_nodes": nodes, "circuit_levels": levels}
         elif self.kind == "batch":
             res = self.eng.tc_bool_batch(self.wl.nodes, self.wl.edge_off, d["src"], d["dst"], mode=self.mode)
             return None, int(res.counts.sum()), {"batch": res.stats}
@@ -555,9 +548,8 @@ def run_ours(args):
         }
         if stats and "prov" in stats:
             line.update({"dtype": "f32 (circuits), f64 (proof weights, root sums, leaf gradients)",
-                         "prov": {**stats["prov"], "capture_s": stats["capture_s"], "compile_s": stats["compile_s"],
-                                  "circuit_nodes": stats["circuit_nodes"], "circuit_levels": stats["circuit_levels"],
-                                  "proofs": stats["proofs"]}})
+                         "prov": {**stats["prov"], "circuit_nodes": stats["circuit_nodes"],
+                                  "circuit_levels": stats["circuit_levels"]}})
         elif stats and "batch" in stats:
             b = stats["batch"]
             line.update({"dtype": "u32", "plan": "bit rows, batched waves",

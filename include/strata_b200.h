@@ -287,6 +287,25 @@ typedef struct strata_circuits strata_circuits;
 strata_status strata_circuits_compile(strata_ctx* ctx, uint32_t n_queries, const uint64_t* proof_off,
     const uint64_t* lit_off, const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes,
     strata_circuits** out);
+/* The same in two steps, so the host compilation of one group of queries
+ * can run on another thread while the device captures the next group:
+ * strata_circuits_compile_host touches no device and no context (thread-safe;
+ * its error message is strata_circuit_parts_error() on the calling thread),
+ * strata_circuits_upload concatenates parts (queries in part order). */
+typedef struct strata_circuit_parts strata_circuit_parts;
+strata_status strata_circuits_compile_host(uint32_t n_queries, const uint64_t* proof_off,
+    const uint64_t* lit_off, const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes,
+    strata_circuit_parts** out);
+const char* strata_circuit_parts_error(void);
+strata_status strata_circuits_upload(strata_ctx* ctx, uint32_t n_parts, strata_circuit_parts* const* parts,
+    uint32_t n_leaves, strata_circuits** out);
+void strata_circuit_parts_free(strata_circuit_parts* parts);
+/* Node count / levels of host-compiled parts, and their FP64 evaluation on
+ * the host (P per query for FP64 leaf probabilities) — checks of the
+ * compiler that need no device. */
+strata_status strata_circuit_parts_shape(const strata_circuit_parts* parts, uint32_t* n_queries,
+    uint64_t* n_nodes, uint32_t* max_levels);
+strata_status strata_circuit_parts_eval64(const strata_circuit_parts* parts, const double* prob, double* out);
 strata_status strata_circuits_shape(const strata_circuits* c, uint64_t* n_nodes, uint32_t* max_levels);
 /* Weighted model counts (Circuit::wmc, circuit.rs:57-63) of every query for
  * leaf probabilities d_p (FP32, n_leaves): FP32 nodes, the root's sum in

@@ -8,6 +8,7 @@
 
 #include <cstdlib>
 #include <new>
+#include <string>
 #include <vector>
 #include <algorithm>
 
@@ -547,6 +548,85 @@ strata_status strata_circuits_compile(strata_ctx* ctx, uint32_t n_queries, const
   SK_GUARD_BEGIN
   *out = sk::circuits_compile(ctx, n_queries, proof_off, lit_off, lits, n_leaves, max_nodes ? max_nodes : (1u << 20));
   SK_GUARD_END(ctx)
+}
+
+struct strata_circuit_parts {
+  sk::CircuitParts* p = nullptr;
+};
+
+namespace {
+thread_local std::string g_parts_error;
+}
+
+strata_status strata_circuits_compile_host(uint32_t n_queries, const uint64_t* proof_off, const uint64_t* lit_off,
+                                           const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes,
+                                           strata_circuit_parts** out) {
+  if (!out || (n_queries && (!proof_off || !lit_off))) {
+    g_parts_error = "NULL argument";
+    return STRATA_E_INVALID;
+  }
+  if (n_queries && lit_off[proof_off[n_queries]] && !lits) {
+    g_parts_error = "NULL argument";
+    return STRATA_E_INVALID;
+  }
+  try {
+    auto* h = new strata_circuit_parts();
+    try {
+      h->p = sk::circuit_parts_compile(n_queries, proof_off, lit_off, lits, n_leaves,
+                                       max_nodes ? max_nodes : (1u << 20));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return STRATA_OK;
+  } catch (const SkError& err) {
+    g_parts_error = err.msg;
+    return err.code;
+  } catch (const std::bad_alloc&) {
+    g_parts_error = "host allocation failed";
+    return STRATA_E_OOM;
+  } catch (...) {
+    g_parts_error = "unexpected exception";
+    return STRATA_E_CUDA;
+  }
+}
+
+const char* strata_circuit_parts_error(void) { return g_parts_error.c_str(); }
+
+strata_status strata_circuits_upload(strata_ctx* ctx, uint32_t n_parts, strata_circuit_parts* const* parts,
+                                     uint32_t n_leaves, strata_circuits** out) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out || (n_parts && !parts)) return bad(ctx, "NULL argument");
+  for (uint32_t i = 0; i < n_parts; i++)
+    if (!parts[i] || !parts[i]->p) return bad(ctx, "NULL part");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  std::vector<sk::CircuitParts*> v;
+  for (uint32_t i = 0; i < n_parts; i++) v.push_back(parts[i]->p);
+  *out = sk::circuit_parts_upload(ctx, n_parts, v.data(), n_leaves);
+  SK_GUARD_END(ctx)
+}
+
+void strata_circuit_parts_free(strata_circuit_parts* parts) {
+  if (!parts) return;
+  sk::circuit_parts_free(parts->p);
+  delete parts;
+}
+
+strata_status strata_circuit_parts_shape(const strata_circuit_parts* parts, uint32_t* n_queries, uint64_t* n_nodes,
+                                        uint32_t* max_levels) {
+  if (!parts || !parts->p) return STRATA_E_INVALID;
+  const uint64_t n = sk::circuit_parts_nodes(parts->p, max_levels);
+  if (n_nodes) *n_nodes = n;
+  if (n_queries) *n_queries = sk::circuit_parts_queries(parts->p);
+  return STRATA_OK;
+}
+
+strata_status strata_circuit_parts_eval64(const strata_circuit_parts* parts, const double* prob, double* out) {
+  if (!parts || !parts->p || !out) return STRATA_E_INVALID;
+  sk::circuit_parts_eval64(parts->p, prob, out);
+  return STRATA_OK;
 }
 
 strata_status strata_circuits_shape(const strata_circuits* c, uint64_t* n_nodes, uint32_t* max_levels) {

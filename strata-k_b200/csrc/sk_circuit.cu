@@ -312,43 +312,50 @@ static void compile_query(const uint64_t* proof_off, const uint64_t* lit_off, co
   out.levels = top + 1;
 }
 
-// Compile every query's proofs (queries given as proof lists of signed
-// literals) into one levelled device DAG; queries compile in parallel on the
-// host threads.
-strata_circuits* circuits_compile(strata_ctx* ctx, uint32_t nq, const uint64_t* proof_off, const uint64_t* lit_off,
-                                  const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes) {
-  std::vector<QCircuit> qc(nq);
-  {
-    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    const unsigned T = std::min<unsigned>(hw, std::max<uint32_t>(1, nq));
-    std::atomic<uint32_t> next{0};
-    std::vector<std::exception_ptr> errs(T);
-    std::vector<std::thread> th;
-    for (unsigned t = 0; t < T; t++)
-      th.emplace_back([&, t]() {
-        try {
-          while (true) {
-            const uint32_t q = next.fetch_add(1);
-            if (q >= nq) break;
-            compile_query(proof_off, lit_off, lits, q, n_leaves, max_nodes, qc[q]);
-          }
-        } catch (...) {
-          errs[t] = std::current_exception();
-          next.store(nq);
+// Host part of the compilation: every query's levelled circuit, queries in
+// parallel on the host threads (no device work; safe beside other calls).
+void circuits_compile_host(uint32_t nq, const uint64_t* proof_off, const uint64_t* lit_off, const int64_t* lits,
+                           uint32_t n_leaves, uint64_t max_nodes, std::vector<QCircuit>& qc) {
+  qc.assign(nq, QCircuit{});
+  const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const unsigned T = std::min<unsigned>(hw, std::max<uint32_t>(1, nq));
+  std::atomic<uint32_t> next{0};
+  std::vector<std::exception_ptr> errs(T);
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < T; t++)
+    th.emplace_back([&, t]() {
+      try {
+        while (true) {
+          const uint32_t q = next.fetch_add(1);
+          if (q >= nq) break;
+          compile_query(proof_off, lit_off, lits, q, n_leaves, max_nodes, qc[q]);
         }
-      });
-    for (auto& x : th) x.join();
-    for (auto& e : errs)
-      if (e) std::rethrow_exception(e);
-  }
+      } catch (...) {
+        errs[t] = std::current_exception();
+        next.store(nq);
+      }
+    });
+  for (auto& x : th) x.join();
+  for (auto& e : errs)
+    if (e) std::rethrow_exception(e);
+}
+
+// Device part: concatenate host-compiled query circuits (parts in order) into
+// one levelled DAG on the device.
+strata_circuits* circuits_upload(strata_ctx* ctx, const std::vector<const std::vector<QCircuit>*>& parts,
+                                 uint32_t n_leaves) {
+  std::vector<const QCircuit*> all;
+  for (auto* p : parts)
+    for (auto& q : *p) all.push_back(&q);
+  const uint32_t nq = (uint32_t)all.size();
   std::vector<uint64_t> qnode(nq + 1, 0), qlevel(nq + 1, 0);
   uint64_t total_ch = 0, total_lvl = 0;
   uint32_t max_levels = 0;
   for (uint32_t q = 0; q < nq; q++) {
-    qnode[q + 1] = qnode[q] + qc[q].kind.size();
-    qlevel[q + 1] = qlevel[q] + qc[q].lvl.size();
-    total_ch += qc[q].CH.size();
-    max_levels = std::max(max_levels, qc[q].levels);
+    qnode[q + 1] = qnode[q] + all[q]->kind.size();
+    qlevel[q + 1] = qlevel[q] + all[q]->lvl.size();
+    total_ch += all[q]->CH.size();
+    max_levels = std::max(max_levels, all[q]->levels);
   }
   total_lvl = qlevel[nq];
   if (qnode[nq] >= (1ull << 32) || total_ch >= (1ull << 32))
@@ -357,7 +364,7 @@ strata_circuits* circuits_compile(strata_ctx* ctx, uint32_t nq, const uint64_t* 
   std::vector<uint32_t> A(qnode[nq]), B(qnode[nq]), CH(total_ch), root(nq), lvl(total_lvl);
   uint64_t chb = 0;
   for (uint32_t q = 0; q < nq; q++) {
-    const QCircuit& c = qc[q];
+    const QCircuit& c = *all[q];
     const uint64_t nb = qnode[q];
     std::copy(c.kind.begin(), c.kind.end(), kind.begin() + (long)nb);
     for (size_t j = 0; j < c.kind.size(); j++) {
@@ -392,6 +399,78 @@ strata_circuits* circuits_compile(strata_ctx* ctx, uint32_t nq, const uint64_t* 
     throw;
   }
   return c;
+}
+
+strata_circuits* circuits_compile(strata_ctx* ctx, uint32_t nq, const uint64_t* proof_off, const uint64_t* lit_off,
+                                  const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes) {
+  std::vector<QCircuit> qc;
+  circuits_compile_host(nq, proof_off, lit_off, lits, n_leaves, max_nodes, qc);
+  return circuits_upload(ctx, {&qc}, n_leaves);
+}
+
+struct CircuitParts {
+  std::vector<QCircuit> q;
+};
+
+CircuitParts* circuit_parts_compile(uint32_t nq, const uint64_t* proof_off, const uint64_t* lit_off,
+                                    const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes) {
+  auto* cp = new CircuitParts();
+  try {
+    circuits_compile_host(nq, proof_off, lit_off, lits, n_leaves, max_nodes, cp->q);
+  } catch (...) {
+    delete cp;
+    throw;
+  }
+  return cp;
+}
+
+void circuit_parts_free(CircuitParts* p) { delete p; }
+
+uint32_t circuit_parts_queries(const CircuitParts* p) { return (uint32_t)p->q.size(); }
+
+uint64_t circuit_parts_nodes(const CircuitParts* p, uint32_t* max_levels) {
+  uint64_t n = 0;
+  uint32_t lv = 0;
+  for (auto& q : p->q) {
+    n += q.kind.size();
+    lv = std::max(lv, q.levels);
+  }
+  if (max_levels) *max_levels = lv;
+  return n;
+}
+
+// FP64 evaluation of the host-compiled circuits (node order = a valid
+// topological order; And/Or fold their children in stored order), used to
+// check the compiler on machines without a GPU.
+void circuit_parts_eval64(const CircuitParts* p, const double* prob, double* out) {
+  for (size_t q = 0; q < p->q.size(); q++) {
+    const QCircuit& c = p->q[q];
+    std::vector<double> val(c.kind.size(), 0.0);
+    for (size_t i = 0; i < c.kind.size(); i++) {
+      const uint8_t k = c.kind[i];
+      if (k == 0) val[i] = prob[c.A[i]];
+      else if (k == 1) val[i] = 1.0 - prob[c.A[i]];
+      else if (k == 2) {
+        double a = 1.0;
+        for (uint32_t j = 0; j < c.B[i]; j++) a = a * val[c.CH[c.A[i] + j]];
+        val[i] = a;
+      } else if (k == 3) {
+        double a = 0.0;
+        for (uint32_t j = 0; j < c.B[i]; j++) a = a + val[c.CH[c.A[i] + j]];
+        val[i] = a;
+      } else {
+        val[i] = k == 4 ? 1.0 : 0.0;
+      }
+    }
+    out[q] = c.kind.empty() ? 0.0 : val[c.root];
+  }
+}
+
+strata_circuits* circuit_parts_upload(strata_ctx* ctx, uint32_t n_parts, CircuitParts* const* parts,
+                                      uint32_t n_leaves) {
+  std::vector<const std::vector<QCircuit>*> v;
+  for (uint32_t i = 0; i < n_parts; i++) v.push_back(&parts[i]->q);
+  return circuits_upload(ctx, v, n_leaves);
 }
 
 void circuits_free(strata_ctx* ctx, strata_circuits* c) {

@@ -69,6 +69,15 @@ void prov_tc_capture(strata_ctx* ctx, uint32_t n, const uint32_t* d_src, const u
 strata_circuits* circuits_compile(strata_ctx* ctx, uint32_t nq, const uint64_t* proof_off, const uint64_t* lit_off,
                                   const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes);
 void circuits_free(strata_ctx* ctx, strata_circuits* c);
+struct CircuitParts;
+CircuitParts* circuit_parts_compile(uint32_t nq, const uint64_t* proof_off, const uint64_t* lit_off,
+                                    const int64_t* lits, uint32_t n_leaves, uint64_t max_nodes);
+void circuit_parts_free(CircuitParts* p);
+uint64_t circuit_parts_nodes(const CircuitParts* p, uint32_t* max_levels);
+uint32_t circuit_parts_queries(const CircuitParts* p);
+void circuit_parts_eval64(const CircuitParts* p, const double* prob, double* out);
+strata_circuits* circuit_parts_upload(strata_ctx* ctx, uint32_t n_parts, CircuitParts* const* parts,
+                                      uint32_t n_leaves);
 void circuits_forward(strata_ctx* ctx, const strata_circuits* c, const float* d_p, float* out32, double* out64);
 void circuits_adjoint(strata_ctx* ctx, const strata_circuits* c, const float* d_p, const float* seed, double* grad,
                       int per_query, float* grad32);

@@ -120,6 +120,13 @@ SIGNATURES = {
     "strata_circuits_compile": (C.c_int, [ctxp, C.c_uint32, u64p, u64p, i64p, C.c_uint32, C.c_uint64,
                                           C.POINTER(vp)]),
     "strata_circuits_shape": (C.c_int, [vp, u64p, u32p]),
+    "strata_circuits_compile_host": (C.c_int, [C.c_uint32, u64p, u64p, i64p, C.c_uint32, C.c_uint64,
+                                               C.POINTER(vp)]),
+    "strata_circuit_parts_error": (C.c_char_p, []),
+    "strata_circuits_upload": (C.c_int, [ctxp, C.c_uint32, C.POINTER(vp), C.c_uint32, C.POINTER(vp)]),
+    "strata_circuit_parts_free": (None, [vp]),
+    "strata_circuit_parts_shape": (C.c_int, [vp, u32p, u64p, u32p]),
+    "strata_circuit_parts_eval64": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "strata_circuits_forward": (C.c_int, [ctxp, vp, vp, vp, vp]),
     "strata_circuits_vjp": (C.c_int, [ctxp, vp, vp, vp, vp, vp]),
     "strata_circuits_grads": (C.c_int, [ctxp, vp, vp, vp]),

@@ -451,6 +451,79 @@ class Engine:
             _ptr(proofs.lits, C.c_int64), n_leaves, max_nodes, C.byref(out)))
         return Circuits(self, out, len(proofs), n_leaves)
 
+    def compile_circuits_host(self, proofs, n_leaves: int, max_nodes: int = 0) -> "CircuitParts":
+        """Host half of compile_circuits (no device work, usable from another
+        thread while this engine runs a capture)."""
+        if not isinstance(proofs, ProofSets):
+            proofs = ProofSets.from_lists(proofs)
+        out = C.c_void_p()
+        rc = self.lib.strata_circuits_compile_host(
+            len(proofs), _ptr(proofs.proof_off, C.c_uint64), _ptr(proofs.lit_off, C.c_uint64),
+            _ptr(proofs.lits, C.c_int64), n_leaves, max_nodes, C.byref(out))
+        if rc != L.OK:
+            _raise(rc, self.lib.strata_circuit_parts_error().decode(errors="replace"))
+        return CircuitParts(self.lib, out, len(proofs))
+
+    def upload_circuits(self, parts, n_leaves: int) -> "Circuits":
+        """Concatenate host-compiled parts (queries in part order) on the device."""
+        arr = (C.c_void_p * max(1, len(parts)))(*[p.h for p in parts])
+        out = C.c_void_p()
+        self._check(self.lib.strata_circuits_upload(self.ctx, len(parts), arr, n_leaves, C.byref(out)))
+        return Circuits(self, out, sum(p.n_queries for p in parts), n_leaves)
+
+    def grad_queries(self, n_nodes: int, src, dst, prob64, prob32, qs, qt, k: int = 8, chunks: int = 4):
+        """`?grad path(s, t)` for every query pair: Prov_k capture, exact
+        compilation and the per-query gradient rows.  The queries are taken in
+        `chunks` groups; while the device captures group i+1, a host thread
+        compiles group i.  Returns (P [FP32, n_queries], G [FP64, n_queries x
+        n_edges], Circuits, info)."""
+        import queue
+        import threading
+        import time as _time
+        qs_, qt_ = _u32(qs), _u32(qt)
+        nq, m = len(qs_), _len(src)
+        bounds = [nq * i // max(1, chunks) for i in range(max(1, chunks) + 1)]
+        parts = [None] * max(1, chunks)
+        todo: queue.Queue = queue.Queue()
+        errors = []
+
+        def compile_worker():
+            while True:
+                item = todo.get()
+                if item is None:
+                    return
+                i, pr = item
+                try:
+                    parts[i] = self.compile_circuits_host(pr, m)
+                except Exception as e:  # reported after the join
+                    errors.append(e)
+
+        worker = threading.Thread(target=compile_worker, daemon=True)
+        worker.start()
+        t0 = _time.perf_counter()
+        stats = []
+        try:
+            for i in range(len(parts)):
+                a, b = bounds[i], bounds[i + 1]
+                pr = self.prov_capture(n_nodes, src, dst, prob64, qs_[a:b], qt_[a:b], k=k)
+                stats.append(pr.stats)
+                todo.put((i, pr))
+        finally:
+            todo.put(None)
+            worker.join()
+        if errors:
+            raise errors[0]
+        t1 = _time.perf_counter()
+        circ = self.upload_circuits(parts, m)
+        for part in parts:
+            part.free()
+        P = circ.forward(prob32)
+        G = circ.grads(prob32)
+        info = {"capture_and_compile_s": t1 - t0, "rounds_max": max((s_["rounds_max"] for s_ in stats), default=0),
+                "max_proof_len": max((s_["max_proof_len"] for s_ in stats), default=0),
+                "capture_device_ms": sum(s_["device_ms"] for s_ in stats), "chunks": len(parts)}
+        return P, G, circ, info
+
     def count_triangle_pattern_dev(self, x, y, n=None) -> int:
         n = _len(x) if n is None else n
         out = C.c_uint64()
@@ -503,6 +576,40 @@ class ProofSets:
 
     def as_lists(self) -> list:
         return [self.query(q) for q in range(len(self))]
+
+
+class CircuitParts:
+    """Host-compiled circuits of a group of queries (not yet on the device)."""
+
+    def __init__(self, lib, handle, n_queries: int):
+        self.lib, self.h, self.n_queries = lib, handle, n_queries
+
+    def shape(self) -> tuple[int, int]:
+        nq, nn, lv = C.c_uint32(), C.c_uint64(), C.c_uint32()
+        rc = self.lib.strata_circuit_parts_shape(self.h, C.byref(nq), C.byref(nn), C.byref(lv))
+        if rc != L.OK:
+            _raise(rc, "invalid circuit parts")
+        return int(nn.value), int(lv.value)
+
+    def eval64(self, prob) -> np.ndarray:
+        """FP64 P per query on the host (a check of the compiler)."""
+        pr = np.ascontiguousarray(prob, np.float64)
+        out = np.zeros(max(1, self.n_queries), np.float64)
+        rc = self.lib.strata_circuit_parts_eval64(self.h, _ptr(pr, C.c_double), _ptr(out, C.c_double))
+        if rc != L.OK:
+            _raise(rc, "invalid circuit parts")
+        return out[:self.n_queries]
+
+    def free(self):
+        if self.h:
+            self.lib.strata_circuit_parts_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 class Circuits:

@@ -166,3 +166,24 @@ def test_capture_rejects_bad_input(engine):
         engine.prov_capture(3, [0], [5], [0.5], [0], [1])
     with pytest.raises(S.InvalidArgument):  # query outside [0, n)
         engine.prov_capture(3, [0], [1], [0.5], [4], [1])
+
+
+def test_grad_queries_pipeline_equals_direct(engine):
+    """The chunked capture + host-compile pipeline gives the same P and
+    gradient rows as one capture and one compilation."""
+    import torch
+    n, m = 1200, 4800
+    s, d = gen.er_directed(n, m, 41)
+    p32, p64 = _probs(m, 42)
+    rng = np.random.default_rng(43)
+    qs = rng.integers(0, n, 37).astype(np.uint32)
+    qt = rng.integers(0, n, 37).astype(np.uint32)
+    pt = torch.from_numpy(p32).cuda()
+    P, G, circ, info = engine.grad_queries(n, s, d, p64, pt, qs, qt, k=8, chunks=5)
+    pr = engine.prov_capture(n, s, d, p64, qs, qt, k=8)
+    c2 = engine.compile_circuits(pr, m)
+    assert torch.equal(P, c2.forward(pt))
+    assert torch.allclose(G, c2.grads(pt), rtol=1e-12, atol=1e-15)  # FP64 atomic sums: order may differ
+    assert info["chunks"] == 5
+    circ.free()
+    c2.free()
