@@ -424,13 +424,13 @@ constexpr uint32_t HC_TILE = NT * HC_ITEMS;
 template <class K>
 __device__ __forceinline__ uint32_t head_degree(const K* dkeys, uint64_t i, int jshift, uint64_t jmask,
                                                 const uint32_t* off, uint64_t n_nodes, uint64_t* jv_out,
-                                                uint32_t* full_deg) {
+                                                uint32_t* full_deg, bool* raw_head = nullptr) {
   const uint64_t jv = ((uint64_t)dkeys[i] >> jshift) & jmask;
   const uint32_t d = jv < n_nodes ? off[jv + 1] - off[jv] : 0u;
   *jv_out = jv;
   *full_deg = d;
-  if (d == 0) return 0;
   const bool head = (i % kGroupMax) == 0 || (((uint64_t)dkeys[i - 1] >> jshift) & jmask) != jv;
+  if (raw_head) *raw_head = head;
   return head ? d : 0u;
 }
 
@@ -486,18 +486,24 @@ __global__ void __launch_bounds__(NT)
   __shared__ uint64_t s_wc[NT / 32], s_wd[NT / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t base = (uint64_t)blockIdx.x * HC_TILE + (uint64_t)warp * 32 * HC_ITEMS;
-  uint32_t dg[HC_ITEMS];
+  uint32_t dg[HC_ITEMS], gs[HC_ITEMS];
   uint64_t exc[HC_ITEMS], exd[HC_ITEMS];
   uint64_t cc = 0, cd = 0;
 #pragma unroll
   for (int j = 0; j < HC_ITEMS; j++) {
     const uint64_t i = base + (uint64_t)j * 32 + lane;
     uint32_t d = 0;
+    bool rh = false;
     if (i < n) {
       uint64_t jv;
       uint32_t fd;
-      d = head_degree(dkeys, i, jshift, jmask, off, n_nodes, &jv, &fd);
+      d = head_degree(dkeys, i, jshift, jmask, off, n_nodes, &jv, &fd, &rh);
     }
+    // The 32 lanes hold one kGroupMax-aligned block of rows, so a group runs
+    // from its head to the next head of the block (or the block's end).
+    const unsigned hm = __ballot_sync(kFull, rh || i >= n);
+    const unsigned above = lane == 31 ? 0u : (hm & (0xffffffffu << (lane + 1)));
+    gs[j] = (above ? (uint32_t)(__ffs(above) - 1) : 32u) - (uint32_t)lane;
     dg[j] = d;
     const uint64_t ic = warp_incl_sum((uint64_t)(d ? 1 : 0));
     const uint64_t id = warp_incl_sum((uint64_t)d);
@@ -522,9 +528,7 @@ __global__ void __launch_bounds__(NT)
     const uint64_t i = base + (uint64_t)j * 32 + lane;
     const uint64_t k = bc + exc[j];
     const uint64_t jv = ((uint64_t)dkeys[i] >> jshift) & jmask;
-    uint32_t g = 1;
-    const uint64_t lim = min(n - i, (uint64_t)(kGroupMax - i % kGroupMax));
-    while (g < lim && (((uint64_t)dkeys[i + g] >> jshift) & jmask) == jv) g++;
+    const uint32_t g = gs[j];
     hidx[k] = (uint32_t)i;
     hpos[k] = bd + exd[j];
     hseg[k] = off[jv];
