@@ -15,7 +15,9 @@ relation.  metric = |dist| / device time.
 
 Under torchrun every rank runs its own instance (its own graph seed and
 sources; no data-path collective) and `value` sums tuples over ranks divided
-by the max rank time ("scaling": "weak").  `--impl reference` times the
+by the max rank time ("scaling": "weak"); with --shard the ranks split one
+instance's independent units instead (sources, batch instances, query
+targets, triangle source vertices; "scaling": "strong").  `--impl reference` times the
 reference interpreter's algorithm (the CPU restatement in oracle/, nested
 loop `solve`, all host threads) on a bounded sample of the same workload.
 """
@@ -52,6 +54,9 @@ def parse():
                          "and batched-reachability configs")
     ap.add_argument("--instances", type=int, default=4096, help="batch: number of instances")
     ap.add_argument("--queries", type=int, default=1024, help="prov: number of ?grad query pairs")
+    ap.add_argument("--shard", action="store_true",
+                    help="N > 1: split one workload's independent units across the ranks (mssp sources, batch "
+                         "instances, prov query targets) instead of running a replica per rank")
     ap.add_argument("--plan", choices=["auto", "sort-merge", "dense"], default="auto")
     ap.add_argument("--tuned", action="store_true", help="apply the autotuner's cached knob values")
     ap.add_argument("--scale", type=int, default=None, help="R-MAT scale (mssp: 20, tri: 22)")
@@ -106,7 +111,8 @@ def metric_for(kind: str) -> str:
 
 
 def config(args, world):
-    common = {"parallelism": f"replicas{world}", "plan": args.plan,
+    sharded = bool(args.shard and world > 1 and args.workload in ("mssp", "batch", "prov", "tri"))
+    common = {"parallelism": f"sharded{world}" if sharded else f"replicas{world}", "plan": args.plan,
               "l2": "flushed (256 MiB write) before every timed step"}
     if args.workload == "tc":
         return {"workload": "bool_tc_er_10000n_50000e",
@@ -338,6 +344,8 @@ class Job:
             res = self.eng.tc_bool_batch(self.wl.nodes, self.wl.edge_off, d["src"], d["dst"], mode=self.mode)
             return None, int(res.counts.sum()), {"batch": res.stats}
         else:
+            if getattr(self, "x_range", None):
+                return None, self.eng.count_triangle_pattern_range_dev(d["src"], d["dst"], *self.x_range), None
             return None, self.eng.count_triangle_pattern_dev(d["src"], d["dst"]), None
         return rel, len(rel), rel.stats
 
@@ -408,12 +416,27 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
-    wl = workload_for(rank, args.scale, units_arg(args), args.workload)
+    sharded = bool(args.shard and world > 1 and args.workload in ("mssp", "batch", "prov", "tri"))
+    wl = workload_for(0 if sharded else rank, args.scale, units_arg(args), args.workload)
+    x_range = None
+    if sharded:
+        from strata_b200 import shard
+        if args.workload == "mssp":
+            mine, idx = shard.shard_sources(wl.sources, rank, world)
+            wl.sources, wl.source_w = mine, wl.source_w[idx]
+        elif args.workload == "batch":
+            wl = shard.batch_subset(wl, shard.shard_instances(wl.nodes, rank, world))
+        elif args.workload == "tri":
+            x_range = shard.shard_vertices(int(max(wl.src.max(), wl.dst.max())) + 1, rank, world)
+        else:
+            qi = shard.shard_queries(wl.qt, rank, world)
+            wl.qs, wl.qt = wl.qs[qi], wl.qt[qi]
     eng = S.Engine(local, tuned=args.tuned)
     eng.set_plan(PLANS[args.plan])
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
     job = Job(args.workload, wl, eng, torch)
+    job.x_range = x_range
     with torch.cuda.stream(stream):
         d = {k: v.to("cuda", non_blocking=True) for k, v in job.host.items()}
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
@@ -540,7 +563,7 @@ def run_ours(args):
         line = {
             "metric": metric_for(args.workload), "value": value, "unit": unit_for(args.workload), "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+            "scaling": "strong" if sharded else "weak", "vs_baseline": None,
             "dtype": {4: "int32", 8: "int64"}.get(wb, "u32"),
             "data": "synthetic", "config": config(args, world),
             "tuples_per_step": int(all_tuples),

@@ -211,6 +211,12 @@ strata_status strata_mssp_trop_dev(strata_ctx* ctx,
     uint64_t n_edges, strata_rel** out, strata_fix_stats* stats);
 strata_status strata_count_triangle_pattern_dev(strata_ctx* ctx,
     const uint32_t* d_x, const uint32_t* d_y, uint64_t n_edges, uint64_t* out_count);
+/* The bindings with X in [x_lo, x_hi) only: the share of one rank when the
+ * source vertices are split across GPUs (the edge list is replicated; the
+ * shares add up to the full count). */
+strata_status strata_count_triangle_pattern_range_dev(strata_ctx* ctx,
+    const uint32_t* d_x, const uint32_t* d_y, uint64_t n_edges, uint64_t x_lo, uint64_t x_hi,
+    uint64_t* out_count);
 
 /* ---- batched Bool reachability ------------------------------------------
  * Many independent transitive closures in one call (the reference computes

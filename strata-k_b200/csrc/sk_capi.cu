@@ -673,6 +673,17 @@ void strata_circuits_free(strata_ctx* ctx, strata_circuits* c) {
   }
 }
 
+strata_status strata_count_triangle_pattern_range_dev(strata_ctx* ctx, const uint32_t* d_x, const uint32_t* d_y,
+                                                      uint64_t n, uint64_t x_lo, uint64_t x_hi,
+                                                      uint64_t* out_count) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out_count || (n && (!d_x || !d_y))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  *out_count = sk::count_triangle_pattern_range(ctx, d_x, d_y, n, x_lo, x_hi);
+  SK_GUARD_END(ctx)
+}
+
 strata_status strata_rel_size(const strata_rel* rel, uint64_t* n) {
   if (!rel || !n) return STRATA_E_INVALID;
   *n = rel->n;

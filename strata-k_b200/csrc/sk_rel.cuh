@@ -56,6 +56,8 @@ strata_rel* fix_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
                      strata_fix_stats* st);
 
 uint64_t count_triangle_pattern(strata_ctx* ctx, const uint32_t* x, const uint32_t* y, uint64_t n);
+uint64_t count_triangle_pattern_range(strata_ctx* ctx, const uint32_t* x, const uint32_t* y, uint64_t n,
+                                      uint64_t u_lo, uint64_t u_hi);
 
 void tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint32_t* nodes, const uint64_t* edge_off,
                    const uint32_t* d_src, const uint32_t* d_dst, int mode, uint64_t* counts, uint64_t* fps,

@@ -33,15 +33,15 @@ __device__ __forceinline__ bool bsearch_u32(const uint32_t* a, uint32_t n, uint3
 
 __global__ void __launch_bounds__(TC_NT)
     k_tri_count(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr, uint64_t n_nodes,
-                uint32_t* counter, unsigned long long* total) {
+                uint32_t* counter, unsigned long long* total, uint32_t u_lo, uint32_t u_hi) {
   __shared__ uint32_t s_list[TC_WARPS][TC_STAGE];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned long long count = 0;
   while (true) {
     uint32_t u = 0;
-    if (lane == 0) u = atomicAdd(counter, 1u);
+    if (lane == 0) u = u_lo + atomicAdd(counter, 1u);
     u = __shfl_sync(kFull, u, 0);
-    if (u >= n_nodes) break;
+    if (u >= u_hi || u >= n_nodes) break;
     const uint32_t a0 = off[u], du = off[u + 1] - a0;
     if (du == 0) continue;
     const bool staged = du <= TC_STAGE;
@@ -99,16 +99,16 @@ __device__ __forceinline__ uint32_t tri_hash(uint32_t z, int lg) { return (z * 0
 
 __global__ void __launch_bounds__(TC_NT)
     k_tri_count_hash(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr, uint64_t n_nodes,
-                     uint32_t* counter, unsigned long long* total) {
+                     uint32_t* counter, unsigned long long* total, uint32_t u_lo, uint32_t u_hi) {
   extern __shared__ __align__(16) uint32_t s_tab[];  // TC_WARPS * TH_TAB
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t* tab = s_tab + warp * TH_TAB;
   unsigned long long count = 0;
   while (true) {
     uint32_t u = 0;
-    if (lane == 0) u = atomicAdd(counter, 1u);
+    if (lane == 0) u = u_lo + atomicAdd(counter, 1u);
     u = __shfl_sync(kFull, u, 0);
-    if (u >= n_nodes) break;
+    if (u >= u_hi || u >= n_nodes) break;
     const uint32_t a0 = off[u], du = off[u + 1] - a0;
     if (du == 0) continue;
     const bool hashed = du <= TH_TAB / 2;
@@ -321,7 +321,10 @@ uint64_t sort_unique(strata_ctx* ctx, DBuf<K>& keys, uint64_t n, int bits, DBuf<
 
 // Count via the warp-per-vertex kernel over a CSR built from sorted unique keys.
 template <class K>
-uint64_t tri_from_sorted(strata_ctx* ctx, const K* keys, uint64_t m, int bits, uint64_t n_nodes) {
+uint64_t tri_from_sorted(strata_ctx* ctx, const K* keys, uint64_t m, int bits, uint64_t n_nodes, uint64_t u_lo = 0,
+                         uint64_t u_hi = ~0ull) {
+  if (u_hi > n_nodes) u_hi = n_nodes;
+  if (u_lo >= u_hi) return 0;
   DBuf<uint32_t> off(ctx, n_nodes + 1), nbr(ctx, m + 1);
   build_csr<K>(ctx, keys, m, bits, n_nodes, off.p, nbr.p);
   DBuf<uint64_t> acc(ctx, 3);  // count, vertex counter, list-entry sum
@@ -331,13 +334,15 @@ uint64_t tri_from_sorted(strata_ctx* ctx, const K* keys, uint64_t m, int bits, u
   if (ctx->tune_tri_probe != 1) {
     k_tri_count<<<grid ? grid : 1, TC_NT, 0, ctx->stream>>>(off.p, nbr.p, n_nodes,
                                                             reinterpret_cast<uint32_t*>(acc.p + 1),
-                                                            reinterpret_cast<unsigned long long*>(acc.p));
+                                                            reinterpret_cast<unsigned long long*>(acc.p),
+                                                            (uint32_t)u_lo, (uint32_t)u_hi);
   } else {
     const size_t smem = (size_t)TC_WARPS * TH_TAB * sizeof(uint32_t);
     SK_CUDA(cudaFuncSetAttribute(k_tri_count_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_tri_count_hash<<<grid ? grid : 1, TC_NT, smem, ctx->stream>>>(off.p, nbr.p, n_nodes,
                                                                      reinterpret_cast<uint32_t*>(acc.p + 1),
-                                                                     reinterpret_cast<unsigned long long*>(acc.p));
+                                                                     reinterpret_cast<unsigned long long*>(acc.p),
+                                                                     (uint32_t)u_lo, (uint32_t)u_hi);
   }
   // Algorithmic bytes: every out-list once per incident oriented edge plus the
   // edge list and offsets, 4 B·Σ(d+(u)+d+(v)) + 8 B·M + 4 B·(N+1); the sum is
@@ -359,12 +364,12 @@ uint64_t tri_from_sorted(strata_ctx* ctx, const K* keys, uint64_t m, int bits, u
 
 template <class K>
 uint64_t pattern_impl(strata_ctx* ctx, const uint32_t* x, const uint32_t* y, uint64_t n, int b,
-                      uint64_t n_nodes) {
+                      uint64_t n_nodes, uint64_t u_lo = 0, uint64_t u_hi = ~0ull) {
   DBuf<K> keys(ctx, n + 1), uniq;
   uniq.ctx = ctx;
   pack_pairs<K, int32_t, false>(ctx, x, y, nullptr, nullptr, n, b, keys.p, nullptr);
   const uint64_t m = sort_unique<K>(ctx, keys, n, 2 * b, uniq);
-  return tri_from_sorted<K>(ctx, uniq.p, m, b, n_nodes);
+  return tri_from_sorted<K>(ctx, uniq.p, m, b, n_nodes, u_lo, u_hi);
 }
 
 // Canonicalize, dedup, drop self-loops, orient by (degree, id).  Leaves the
@@ -471,6 +476,15 @@ uint64_t count_triangle_pattern(strata_ctx* ctx, const uint32_t* x, const uint32
   const Ids I = id_space(ctx, x, y, n);
   if (2 * I.bits <= 32) return pattern_impl<uint32_t>(ctx, x, y, n, I.bits, I.n_nodes);
   return pattern_impl<uint64_t>(ctx, x, y, n, I.bits, I.n_nodes);
+}
+
+uint64_t count_triangle_pattern_range(strata_ctx* ctx, const uint32_t* x, const uint32_t* y, uint64_t n,
+                                      uint64_t u_lo, uint64_t u_hi) {
+  reset_status(ctx);
+  if (n == 0 || u_lo >= u_hi) return 0;
+  const Ids I = id_space(ctx, x, y, n);
+  if (2 * I.bits <= 32) return pattern_impl<uint32_t>(ctx, x, y, n, I.bits, I.n_nodes, u_lo, u_hi);
+  return pattern_impl<uint64_t>(ctx, x, y, n, I.bits, I.n_nodes, u_lo, u_hi);
 }
 
 uint64_t count_triangles_undirected(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n) {

@@ -120,6 +120,7 @@ SIGNATURES = {
     "strata_circuits_compile": (C.c_int, [ctxp, C.c_uint32, u64p, u64p, i64p, C.c_uint32, C.c_uint64,
                                           C.POINTER(vp)]),
     "strata_circuits_shape": (C.c_int, [vp, u64p, u32p]),
+    "strata_count_triangle_pattern_range_dev": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, C.c_uint64, u64p]),
     "strata_circuits_compile_host": (C.c_int, [C.c_uint32, u64p, u64p, i64p, C.c_uint32, C.c_uint64,
                                                C.POINTER(vp)]),
     "strata_circuit_parts_error": (C.c_char_p, []),

@@ -524,6 +524,14 @@ class Engine:
                 "capture_device_ms": sum(s_["device_ms"] for s_ in stats), "chunks": len(parts)}
         return P, G, circ, info
 
+    def count_triangle_pattern_range_dev(self, x, y, x_lo: int, x_hi: int, n=None) -> int:
+        """Bindings of the triangle pattern with X in [x_lo, x_hi)."""
+        n = _len(x) if n is None else n
+        out = C.c_uint64()
+        self._check(self.lib.strata_count_triangle_pattern_range_dev(self.ctx, _dp(x), _dp(y), n, x_lo, x_hi,
+                                                                     C.byref(out)))
+        return int(out.value)
+
     def count_triangle_pattern_dev(self, x, y, n=None) -> int:
         n = _len(x) if n is None else n
         out = C.c_uint64()

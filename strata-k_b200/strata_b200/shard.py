@@ -1,0 +1,100 @@
+"""Splitting the configs' independent units across ranks (one process per GPU).
+
+Every workload of the benchmark has units that need no exchange while they
+are computed, so N GPUs run them side by side and only the results meet:
+
+* MSSP: the sources.  dist(S, ·) depends on S's own facts and `edge` only,
+  so each rank runs the fixpoint for its share of the sources and the union
+  of the ranks' relations is the relation of the whole source set.
+* batched reachability: the instances (balanced by the n² bit-matrix work).
+* probabilistic reachability: the query targets (path(., t) depends only on
+  path(., t) and `edge`), so each rank captures its targets' queries.
+* triangles: the source vertices of the oriented edges, with the edge list
+  replicated; the counts add up.
+
+Bool transitive closure (one instance) is the exception: its rows need each
+other's Δ every round, so it runs as a replica per rank.
+
+The helpers are plain partition functions plus gather/reduce through
+torch.distributed (NCCL on GPUs, gloo in the CPU tests).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def shard_range(n: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous share [lo, hi) of n units for `rank`."""
+    return n * rank // world, n * (rank + 1) // world
+
+
+def shard_sources(sources, rank: int, world: int):
+    """The sources (and their positions) a rank runs: round robin, so every
+    rank gets an even share of the id range."""
+    idx = np.arange(rank, len(sources), world)
+    return np.asarray(sources)[idx], idx
+
+
+def shard_instances(nodes, rank: int, world: int) -> np.ndarray:
+    """Instance indices of `rank`: greedy longest-processing-time assignment
+    by the n² bit-matrix cost, deterministic for every rank."""
+    cost = np.asarray(nodes, np.float64) ** 2
+    order = np.argsort(-cost, kind="stable")
+    load = np.zeros(world)
+    owner = np.empty(len(cost), np.int64)
+    for i in order:
+        r = int(np.argmin(load))
+        owner[i] = r
+        load[r] += cost[i]
+    return np.flatnonzero(owner == rank)
+
+
+def shard_queries(qt, rank: int, world: int) -> np.ndarray:
+    """Query indices whose target a rank owns (target id modulo world), so a
+    target is captured by one rank only."""
+    return np.flatnonzero(np.asarray(qt, np.int64) % world == rank)
+
+
+def shard_vertices(n_nodes: int, rank: int, world: int) -> tuple[int, int]:
+    """The source-vertex range [lo, hi) of the triangle count a rank owns."""
+    return shard_range(n_nodes, rank, world)
+
+
+def batch_subset(wl, idx):
+    """The sub-batch of instances `idx` (in that order) of a BatchWorkload."""
+    from .gen import BatchWorkload
+    idx = np.asarray(idx, np.int64)
+    nodes = np.asarray(wl.nodes)[idx]
+    lens = (wl.edge_off[idx + 1] - wl.edge_off[idx]).astype(np.uint64)
+    off = np.zeros(len(idx) + 1, np.uint64)
+    off[1:] = np.cumsum(lens)
+    src = np.concatenate([wl.src[int(wl.edge_off[i]):int(wl.edge_off[i + 1])] for i in idx]) if len(idx) else \
+        np.zeros(0, np.uint32)
+    dst = np.concatenate([wl.dst[int(wl.edge_off[i]):int(wl.edge_off[i + 1])] for i in idx]) if len(idx) else \
+        np.zeros(0, np.uint32)
+    return BatchWorkload(f"{wl.name}[{len(idx)}]", nodes, off, src, dst, wl.meta)
+
+
+# ---- meeting of the results (torch.distributed) -----------------------------
+def allreduce_sum_u64(dist, value: int, device="cpu") -> int:
+    import torch
+    t = torch.tensor([int(value)], dtype=torch.int64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(t.item())
+
+
+def gather_objects(dist, obj, world: int) -> list:
+    """All ranks' Python objects (small results: per-instance summaries, proof
+    lists, relation columns of a test)."""
+    out = [None] * world
+    dist.all_gather_object(out, obj)
+    return out
+
+
+def merge_by_index(parts: list, n: int) -> list:
+    """[(indices, values)] from every rank → values in global index order."""
+    out = [None] * n
+    for idx, vals in parts:
+        for i, v in zip(idx, vals):
+            out[int(i)] = v
+    return out

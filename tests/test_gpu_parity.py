@@ -527,3 +527,19 @@ def test_sort_rank_methods_identical(engine, rank):
             assert np.array_equal(vo.cpu().numpy().view(np.uint32), vals[order])
     finally:
         engine.set_knob(7, 0)
+
+
+def test_triangle_pattern_vertex_ranges_add_up(engine):
+    """Shares of the source-vertex range (one per rank) add up to the count."""
+    import torch
+    wl = gen.triangle_workload(scale=12, edge_factor=16, seed=12)
+    x = torch.from_numpy(wl.src.astype(np.int32)).cuda()
+    y = torch.from_numpy(wl.dst.astype(np.int32)).cuda()
+    n = int(max(wl.src.max(), wl.dst.max())) + 1
+    total = engine.count_triangle_pattern_dev(x, y)
+    assert total == O.count_pattern(wl.src, wl.dst)
+    for world in (2, 3, 8):
+        parts = [engine.count_triangle_pattern_range_dev(x, y, n * r // world, n * (r + 1) // world)
+                 for r in range(world)]
+        assert sum(parts) == total
+    assert engine.count_triangle_pattern_range_dev(x, y, 5, 5) == 0
