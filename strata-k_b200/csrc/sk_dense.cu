@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(NT, 6)
     k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n_rows,
                    const uint32_t* __restrict__ hidx, const uint64_t* __restrict__ pos,
                    const uint32_t* __restrict__ hseg, const uint8_t* __restrict__ hg, uint64_t n,
-                   uint64_t total, const uint64_t* __restrict__ splits, int pshift, uint64_t pmask, int out_pshift,
-                   int out_vshift, const uint32_t* __restrict__ nbr, uint64_t n_nbr,
+                   uint64_t total, const uint64_t* __restrict__ splits, int pshift, uint64_t pmask, uint64_t ck,
+                   uint64_t cv, const uint32_t* __restrict__ nbr, uint64_t n_nbr,
                    const int32_t* __restrict__ nbr_w, DenseLayout lay, uint32_t* bits, int32_t* D, uint32_t* marks,
                    uint32_t* status) {
   // Dynamic shared memory (sizes in dense_expand_smem()):
@@ -191,9 +191,10 @@ __global__ void __launch_bounds__(NT, 6)
         if (ok[u]) {
           const uint64_t m = h_t + (j - ex_t);
           const K mk = dkeys[m];
-          const uint32_t kept = (uint32_t)(((uint64_t)mk >> pshift) & pmask);
-          const K key = (K)(((K)kept << out_pshift) | ((K)v_t << out_vshift));
-          ix[u] = dense_index((uint64_t)key, lay);
+          const uint32_t kept = (uint32_t)((mk >> pshift) & (K)pmask);
+          // index of the output key (kept, v) without packing it: one of the
+          // two coefficients is 1, the other the index's row width
+          ix[u] = (uint64_t)kept * ck + (uint64_t)v_t * cv;
           if (ix[u] >= lay.entries) {
             flags |= ST_BOUNDS;
             ok[u] = false;
@@ -589,9 +590,22 @@ void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n
   const size_t smem = dense_expand_smem();
   auto kern = k_expand_dense<K, TROP>;
   SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // (kept, v) → index entry: kept and v are the output key's two columns
+  // (which one depends on the rule shape), the layout row- or column-major.
+  uint64_t ck, cv;
+  const bool kept_is_c0 = out_pshift == lay.b1 && out_vshift == 0;
+  if (!kept_is_c0 && !(out_pshift == 0 && out_vshift == lay.b1))
+    fail(STRATA_E_UNSUPPORTED, "direct-addressed expand: unexpected output key layout");
+  if (kept_is_c0) {
+    ck = lay.colmajor ? 1 : lay.n1;
+    cv = lay.colmajor ? lay.n0 : 1;
+  } else {
+    ck = lay.colmajor ? lay.n0 : 1;
+    cv = lay.colmajor ? 1 : lay.n1;
+  }
   kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(dkeys, dw, n_rows, hidx, hpos, hseg, hg, nh, total, splits_buf,
-                                                   pshift, pmask, out_pshift, out_vshift, nbr, n_nbr, nbr_w, lay,
-                                                   bits, D, marks, ctx->d_status);
+                                                   pshift, pmask, ck, cv, nbr, n_nbr, nbr_w, lay, bits, D, marks,
+                                                   ctx->d_status);
   // Algorithmic bytes: every Δ row (key, weight) once, each head's record,
   // every CSR edge of a group read once (neighbour + weight), one 4-byte
   // index probe per candidate (a candidate = one Δ row × one edge).
