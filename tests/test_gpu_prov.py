@@ -183,7 +183,8 @@ def test_grad_queries_pipeline_equals_direct(engine):
     pr = engine.prov_capture(n, s, d, p64, qs, qt, k=8)
     c2 = engine.compile_circuits(pr, m)
     assert torch.equal(P, c2.forward(pt))
-    assert torch.allclose(G, c2.grads(pt), rtol=1e-12, atol=1e-15)  # FP64 atomic sums: order may differ
+    # FP64 atomic sums may add in another order: equal up to rounding of the sums
+    assert float((G - c2.grads(pt)).abs().max()) <= 1e-12
     assert info["chunks"] == 5
     circ.free()
     c2.free()
