@@ -183,8 +183,11 @@ def test_grad_queries_pipeline_equals_direct(engine):
     pr = engine.prov_capture(n, s, d, p64, qs, qt, k=8)
     c2 = engine.compile_circuits(pr, m)
     assert torch.equal(P, c2.forward(pt))
-    # FP64 atomic sums may add in another order: equal up to rounding of the sums
-    assert float((G - c2.grads(pt)).abs().max()) <= 1e-12
+    # node adjoints accumulate through FP32 atomics (and leaves through FP64
+    # ones) whose order changes from launch to launch: equal up to FP32
+    # rounding of the adjoints
+    G2 = c2.grads(pt)
+    assert torch.allclose(G, G2, rtol=1e-6, atol=1e-8), float((G - G2).abs().max())
     assert info["chunks"] == 5
     circ.free()
     c2.free()
