@@ -832,7 +832,7 @@ uint64_t tc_bool_bitset(strata_ctx* ctx, const uint32_t* d_src, const uint32_t* 
   *round_bytes = R.bytes;
   const uint64_t n = R.totals[0];
   const uint64_t w4 = inst_w4(spec[0]);
-  DenseLayout lay{b1, (b1 >= 64 ? ~0ull : ((1ull << b1) - 1)), n_src, w4 * 128, n_src * w4 * 128, false};
+  const DenseLayout lay = dense_layout(b1, n_src, w4 * 128, false);
   out.reserve(n + 1);
   DBuf<uint64_t> states(ctx, dense_marks_states(lay.entries));
   const uint64_t got = dense_marks_compact<K, false>(ctx, reinterpret_cast<uint32_t*>(B.F.p), lay, nullptr, out.p,

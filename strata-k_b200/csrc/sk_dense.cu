@@ -25,6 +25,8 @@
 // Δ tuples with the same join value as one group: each edge of that value is
 // read once for the whole group, and the group's probes of one edge all fall
 // in one index row (cache-resident).
+#include <type_traits>
+
 #include "sk_ops.cuh"
 #include "sk_prims.cuh"
 
@@ -58,47 +60,77 @@ __global__ void k_tile_splits(const uint64_t* __restrict__ pos, uint64_t n, uint
 
 __device__ __forceinline__ uint64_t dense_index(uint64_t key, const DenseLayout& L) {
   const uint64_t c0 = key >> L.b1, c1 = key & L.mask1;
-  return L.colmajor ? c1 * L.n0 + c0 : c0 * L.n1 + c1;
+  return L.colmajor ? c1 * L.width + c0 : c0 * L.width + c1;
 }
 
-// Grouped expand over the compacted group heads (dense_heads): a group is a
-// run of Δ rows with one join value, split at multiples of kGroupMax; its
-// head carries the degree of the join value, so one expand output is one
-// (group, edge) pair and the load balancing spends no merged positions on
-// the other members.  A warp takes 32 consecutive outputs (one per
-// lane), flattens their (edge, member) candidates with a warp prefix sum over
-// the group sizes and processes them 32 at a time: lanes that share an edge
-// handle consecutive members of its group, whose index entries are adjacent
-// in one index row, so a warp's probes and atomics touch one or two cache
-// lines instead of 32.
-template <class K, bool TROP>
+// Position of the k-th (0-based) set bit of w (k < popc(w)).
+__device__ __forceinline__ uint32_t select_bit(uint32_t w, uint32_t k) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (int sh = 16; sh >= 1; sh >>= 1) {
+    const uint32_t c = __popc((w >> pos) & ((1u << sh) - 1u));
+    if (k >= c) {
+      k -= c;
+      pos += sh;
+    }
+  }
+  return pos;
+}
+
+// Grouped expand over compacted group heads.  A head is either
+//   * a key head (dense_heads): a run of Δ rows with one join value, split
+//     at multiples of kGroupMax; its members are the rows h .. h+g-1, or
+//   * a word head (dense_word_heads): a nonzero 32-bit word of the marks in
+//     the index row of one join value; its members are the word's set bits,
+//     their weights in Dprev,
+// and carries the degree of its join value, so one expand output is one
+// (head, edge) pair and the load balancing spends no merged positions on the
+// other members.  A warp takes 32 consecutive outputs (one per lane) and
+// flattens their (edge, member) candidates: each lane writes one slot per
+// member of its output into the warp's slot table, (lane << 5) | member, at
+// its exclusive prefix of the group sizes, and the warp then processes the
+// slots 32 at a time.  Lanes that share an edge handle consecutive members
+// of its group, whose index entries are adjacent in one index row, so a
+// warp's probes and atomics touch one or two cache lines instead of 32.
+//
+// Every head has at least one edge, so the head events of a tile's 2,048
+// merged positions are at least two apart: a tile sees at most
+// DE_TILE / 2 + 1 heads (checked).
+constexpr uint32_t DE_HEADS = DE_TILE / 2 + 2;
+constexpr uint32_t kWarps = NT / 32;
+
+template <class K, bool TROP, bool WORDS>
 __global__ void __launch_bounds__(NT, 6)
     k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n_rows,
                    const uint32_t* __restrict__ hidx, const uint64_t* __restrict__ pos,
-                   const uint32_t* __restrict__ hseg, const uint8_t* __restrict__ hg, uint64_t n,
-                   uint64_t total, const uint64_t* __restrict__ splits, int pshift, uint64_t pmask, uint64_t ck,
-                   uint64_t cv, const uint32_t* __restrict__ nbr, uint64_t n_nbr,
-                   const int32_t* __restrict__ nbr_w, DenseLayout lay, uint32_t* bits, int32_t* D, uint32_t* marks,
+                   const uint32_t* __restrict__ hseg, const typename std::conditional<WORDS, uint32_t, uint8_t>::type* __restrict__ hg,
+                   uint64_t n, uint64_t total, const uint64_t* __restrict__ splits, int pshift, uint64_t pmask,
+                   uint64_t ck, uint64_t cv, uint32_t wpr, const uint32_t* __restrict__ nbr, uint64_t n_nbr,
+                   const int32_t* __restrict__ nbr_w, uint64_t entries, uint32_t* bits, int32_t* D, uint32_t* marks,
                    uint32_t* status) {
+  using GT = typename std::conditional<WORDS, uint32_t, uint8_t>::type;
   // Dynamic shared memory (sizes in dense_expand_smem()):
   //   s_pos   int32  pos of each local head relative to the tile's first output
   //   s_seg   u32    CSR segment start of each local head
-  //   s_h     u32    Δ row of each local head (its group's first member)
+  //   s_h     u32    Δ row (key head) or marks word (word head) of each local head
+  //   s_g     u8/u32 group size (key head) or member mask (word head)
   //   s_owner u16    local owner head of each output of the tile
-  //   s_g     u8     group size of each local head (members incl. the head)
+  //   s_slot  u16    per warp: the (lane, member) of each candidate of its chunk
   extern __shared__ __align__(16) unsigned char s_raw[];
   int32_t* s_pos = reinterpret_cast<int32_t*>(s_raw);
-  uint32_t* s_seg = reinterpret_cast<uint32_t*>(s_pos + DE_TILE + 1);
-  uint32_t* s_h = s_seg + DE_TILE + 1;
-  uint16_t* s_owner = reinterpret_cast<uint16_t*>(s_h + DE_TILE + 1);
-  uint8_t* s_g = reinterpret_cast<uint8_t*>(s_owner + DE_TILE);
+  uint32_t* s_seg = reinterpret_cast<uint32_t*>(s_pos + DE_HEADS);
+  uint32_t* s_h = s_seg + DE_HEADS;
+  GT* s_g = reinterpret_cast<GT*>(s_h + DE_HEADS);
+  uint16_t* s_owner = reinterpret_cast<uint16_t*>(s_g + DE_HEADS);
+  uint16_t* s_slot = s_owner + DE_TILE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint16_t* my_slots = s_slot + warp * (32 * kGroupMax);
   const uint64_t L = n + total;
   const uint64_t d0 = (uint64_t)blockIdx.x * DE_TILE;
   const uint64_t d1 = d0 + DE_TILE < L ? d0 + DE_TILE : L;
   const uint64_t i0 = splits[blockIdx.x], i1 = splits[blockIdx.x + 1];
   const uint64_t a = i0 > 0 ? i0 - 1 : 0;
-  if (i1 < a || i1 - a > DE_TILE + 1 || i1 > n || d1 < i1 || d0 < i0) {
+  if (i1 < a || i1 - a > DE_HEADS || i1 > n || d1 < i1 || d0 < i0) {
     if (tid == 0) atomicOr(status, ST_BOUNDS);
     return;
   }
@@ -144,9 +176,9 @@ __global__ void __launch_bounds__(NT, 6)
   const uint64_t o_end = o1 < total ? o1 : total;
   for (uint64_t c = o0 + (uint64_t)warp * 32; c < o_end; c += NT) {
     const uint64_t o = c + lane;
-    uint32_t g = 0, v = 0;
+    uint32_t mm = 0, v = 0;
     int32_t ew = 0;
-    uint64_t h = 0;
+    uint64_t h = 0, kb = 0;
     if (o < o_end) {
       const uint32_t li = s_owner[o - o0];
       const uint64_t e = (uint64_t)((int64_t)s_seg[li] + ((int64_t)(o - o0) - s_pos[li]));
@@ -155,19 +187,36 @@ __global__ void __launch_bounds__(NT, 6)
       } else {
         v = nbr[e];
         if constexpr (TROP) ew = nbr_w[e];
-        g = s_g[li];
         h = s_h[li];
-        if (h + g > n_rows) {
-          flags |= ST_BOUNDS;
-          g = 0;
+        if constexpr (WORDS) {
+          // members: the set bits of word h, columns (h mod wpr)*32 + bit of
+          // the head's row; kb = the output index of column 0 of the word
+          mm = s_g[li];
+          kb = (uint64_t)(((uint32_t)h % wpr) * 32u) * ck + (uint64_t)v * cv;
+          if (h * 32 + 32 > entries) {
+            flags |= ST_BOUNDS;
+            mm = 0;
+          }
+        } else {
+          const uint32_t g = s_g[li];
+          mm = g >= 32 ? kFull : (1u << g) - 1u;  // members h + r for the set bits r
+          if (g > kGroupMax || h + g > n_rows) {
+            flags |= ST_BOUNDS;
+            mm = 0;
+          }
         }
       }
     }
+    const uint32_t g = __popc(mm);
     const uint32_t incl = warp_incl_sum(g);
-    const uint32_t ex = incl - g;
     const uint32_t T = __shfl_sync(kFull, incl, 31);
-    // Candidates j = 0..T-1 of this chunk: owner lane t (first lane whose
-    // inclusive count exceeds j), member h_t + (j - ex_t), edge v_t.
+    {
+      uint32_t k = incl - g;
+      for (uint32_t r = mm; r; r &= r - 1) my_slots[k++] = (uint16_t)((lane << 5) | (__ffs(r) - 1));
+    }
+    __syncwarp();
+    // Candidates j = 0..T-1 of this chunk: slot j names the owner lane t and
+    // the member (row offset or bit) of t's head; the edge is v_t.
     for (uint32_t b0 = 0; b0 < T; b0 += 64) {
       uint64_t ix[2];
       int32_t cw[2], cur[2];
@@ -175,31 +224,41 @@ __global__ void __launch_bounds__(NT, 6)
 #pragma unroll
       for (int u = 0; u < 2; u++) {
         const uint32_t j = b0 + 32 * u + lane;
-        int t = 0;
-#pragma unroll
-        for (int st = 16; st > 0; st >>= 1) {
-          const uint32_t val = __shfl_sync(kFull, incl, t + st - 1);
-          if (val <= j) t += st;
-        }
-        const uint32_t ex_t = __shfl_sync(kFull, ex, t);
-        const uint64_t h_t = __shfl_sync(kFull, h, t);
-        const uint32_t v_t = __shfl_sync(kFull, v, t);
-        const int32_t ew_t = __shfl_sync(kFull, ew, t);
         ok[u] = j < T;
+        const uint32_t sl = ok[u] ? my_slots[j] : 0u;
+        const int t = (int)(sl >> 5);
+        const uint32_t r = sl & 31u;
+        const int32_t ew_t = TROP ? __shfl_sync(kFull, ew, t) : 0;
         ix[u] = 0;
         cw[u] = 0;
-        if (ok[u]) {
-          const uint64_t m = h_t + (j - ex_t);
-          const K mk = dkeys[m];
-          const uint32_t kept = (uint32_t)((mk >> pshift) & (K)pmask);
-          // index of the output key (kept, v) without packing it: one of the
-          // two coefficients is 1, the other the index's row width
-          ix[u] = (uint64_t)kept * ck + (uint64_t)v_t * cv;
-          if (ix[u] >= lay.entries) {
-            flags |= ST_BOUNDS;
-            ok[u] = false;
-          } else if constexpr (TROP) {
-            cw[u] = trop_mul(dw[m], ew_t, &flags);
+        if constexpr (WORDS) {
+          const uint64_t kb_t = __shfl_sync(kFull, kb, t);
+          const uint32_t w_t = TROP ? __shfl_sync(kFull, (uint32_t)h, t) : 0u;
+          if (ok[u]) {
+            ix[u] = kb_t + (uint64_t)r * ck;
+            if (ix[u] >= entries) {
+              flags |= ST_BOUNDS;
+              ok[u] = false;
+            } else if constexpr (TROP) {
+              cw[u] = trop_mul(dw[(uint64_t)w_t * 32 + r], ew_t, &flags);
+            }
+          }
+        } else {
+          const uint64_t h_t = __shfl_sync(kFull, h, t);
+          const uint32_t v_t = __shfl_sync(kFull, v, t);
+          if (ok[u]) {
+            const uint64_t m = h_t + r;
+            const K mk = dkeys[m];
+            const uint32_t kept = (uint32_t)((mk >> pshift) & (K)pmask);
+            // index of the output key (kept, v) without packing it: one of
+            // the two coefficients is 1, the other the index's row width
+            ix[u] = (uint64_t)kept * ck + (uint64_t)v_t * cv;
+            if (ix[u] >= entries) {
+              flags |= ST_BOUNDS;
+              ok[u] = false;
+            } else if constexpr (TROP) {
+              cw[u] = trop_mul(dw[m], ew_t, &flags);
+            }
           }
         }
       }
@@ -227,6 +286,7 @@ __global__ void __launch_bounds__(NT, 6)
         }
       }
     }
+    __syncwarp();  // the slot table is rewritten for the next chunk
   }
   if (flags) atomicOr(status, flags);
 }
@@ -252,20 +312,6 @@ __global__ void __launch_bounds__(NT) k_marks_count(const uint32_t* __restrict__
   }
 }
 
-// Position of the k-th (0-based) set bit of w (k < popc(w)).
-__device__ __forceinline__ uint32_t select_bit(uint32_t w, uint32_t k) {
-  uint32_t pos = 0;
-#pragma unroll
-  for (int sh = 16; sh >= 1; sh >>= 1) {
-    const uint32_t c = __popc((w >> pos) & ((1u << sh) - 1u));
-    if (k >= c) {
-      k -= c;
-      pos += sh;
-    }
-  }
-  return pos;
-}
-
 // Each warp enumerates the set bits of its 32 words in index order, 32 at a
 // time across the lanes, so the key stores and the weight gathers coalesce.
 template <class K, bool TROP>
@@ -283,7 +329,7 @@ __global__ void __launch_bounds__(NT)
   const uint32_t incl = warp_incl_sum(c);
   const uint32_t wtot = __shfl_sync(kFull, incl, 31);
   const uint64_t wbase = tile_sums[blockIdx.x] + __shfl_sync(kFull, ex, 0);
-  const uint64_t width = lay.colmajor ? lay.n0 : lay.n1;
+  const uint64_t width = lay.width;
   const uint64_t b = wi * 32;
   const uint64_t row_b = b / width, col_b = b - row_b * width;  // one division per word
   uint32_t flags = 0;
@@ -326,13 +372,15 @@ __global__ void __launch_bounds__(NT)
 // Seed the index from keys (and weights).
 template <class K, bool TROP>
 __global__ void k_dense_seed(const K* __restrict__ keys, const int32_t* __restrict__ w, uint64_t n,
-                             DenseLayout lay, uint32_t* bits, int32_t* D, uint32_t* status) {
+                             DenseLayout lay, uint32_t* bits, int32_t* D, uint32_t* marks, uint32_t* status) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const uint64_t c0 = (uint64_t)keys[i] >> lay.b1, c1 = (uint64_t)keys[i] & lay.mask1;
+  if (c0 >= lay.n0 || c1 >= lay.n1) { atomicOr(status, ST_BOUNDS); return; }
   const uint64_t ix = dense_index((uint64_t)keys[i], lay);
-  if (ix >= lay.entries) { atomicOr(status, ST_BOUNDS); return; }
   if constexpr (TROP) D[ix] = w[i];
   else atomicOr(&bits[ix >> 5], 1u << (ix & 31));
+  if (marks) atomicOr(&marks[ix >> 5], 1u << (ix & 31));
 }
 
 __global__ void k_fill_i32(int32_t* p, uint64_t n, int32_t v) {
@@ -359,6 +407,7 @@ __global__ void __launch_bounds__(NT)
   uint32_t present = 0;
   int32_t wv[DC_ITEMS];
   // (c0, c1) of ordinal b, then stepped: one division per thread.
+  const uint64_t logical = lay.n0 * lay.n1;
   uint64_t q0 = b / lay.n1, q1 = b - q0 * lay.n1;
 #pragma unroll
   for (int j = 0; j < DC_ITEMS; j++) {
@@ -371,8 +420,8 @@ __global__ void __launch_bounds__(NT)
         q0++;
       }
     }
-    if (q < lay.entries) {
-      const uint64_t ix = lay.colmajor ? q1 * lay.n0 + q0 : q;
+    if (q < logical) {
+      const uint64_t ix = lay.colmajor ? q1 * lay.width + q0 : q0 * lay.width + q1;
       if constexpr (TROP) {
         wv[j] = D[ix];
         p = wv[j] != INT32_MAX;
@@ -538,11 +587,182 @@ __global__ void __launch_bounds__(NT)
   if (blockIdx.x == gridDim.x - 1 && tid == 0) hpos[tile_cnt[n_tiles]] = tile_deg[n_tiles];
 }
 
+// ---- word heads of a Δ held in the marks ------------------------------------
+// Rounds after the first keep Δ where the expand left it, in the marks bitmap
+// (an entry is in Δ exactly when the round marked it), so Δ needs no key
+// compaction: a head is a nonzero marks word whose row (join value
+// word / wpr) has edges, and its members are the word's set bits.  Count,
+// scan, write as for key heads; the write also snapshots the members'
+// merged weights (D → Dprev, which the next expand reads while D changes
+// under it) and clears the words for the next round.
+template <bool TROP>
+__global__ void __launch_bounds__(NT)
+    k_words_count(const uint32_t* __restrict__ marks, uint64_t words, uint32_t wpr, const uint32_t* __restrict__ off,
+                  uint64_t n_nodes, uint64_t* __restrict__ tile_cnt, uint64_t* __restrict__ tile_deg,
+                  unsigned long long* totals) {
+  __shared__ uint64_t s_red[4][NT / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * HC_TILE + (uint64_t)warp * 32 * HC_ITEMS;
+  uint64_t c = 0, dsum = 0, cands = 0, tuples = 0;
+#pragma unroll
+  for (int j = 0; j < HC_ITEMS; j++) {
+    const uint64_t i = base + (uint64_t)j * 32 + lane;
+    const uint32_t m = i < words ? marks[i] : 0u;
+    if (m) {
+      const uint32_t row = (uint32_t)i / wpr;
+      const uint32_t d = row < n_nodes ? off[row + 1] - off[row] : 0u;
+      const uint32_t pc = __popc(m);
+      tuples += pc;
+      if (d) {
+        c++;
+        dsum += d;
+        cands += (uint64_t)pc * d;
+      }
+    }
+  }
+  c = warp_sum(c);
+  dsum = warp_sum(dsum);
+  cands = warp_sum(cands);
+  tuples = warp_sum(tuples);
+  if (lane == 0) {
+    s_red[0][warp] = c;
+    s_red[1][warp] = dsum;
+    s_red[2][warp] = cands;
+    s_red[3][warp] = tuples;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint64_t r[4] = {0, 0, 0, 0};
+    for (int w = 0; w < NT / 32; w++)
+      for (int q = 0; q < 4; q++) r[q] += s_red[q][w];
+    tile_cnt[blockIdx.x] = r[0];
+    tile_deg[blockIdx.x] = r[1];
+    if (r[2]) atomicAdd(&totals[0], (unsigned long long)r[2]);
+    if (r[3]) atomicAdd(&totals[1], (unsigned long long)r[3]);
+  }
+}
+
+template <bool TROP>
+__global__ void __launch_bounds__(NT)
+    k_words_write(uint32_t* marks, uint64_t words, uint32_t wpr, const uint32_t* __restrict__ off, uint64_t n_nodes,
+                  const uint64_t* __restrict__ tile_cnt, const uint64_t* __restrict__ tile_deg, uint64_t n_tiles,
+                  uint32_t* __restrict__ hword, uint32_t* __restrict__ hmask, uint64_t* __restrict__ hpos,
+                  uint32_t* __restrict__ hseg, const int32_t* __restrict__ D, int32_t* __restrict__ Dprev,
+                  unsigned long long* totals) {
+  __shared__ uint64_t s_wc[NT / 32], s_wd[NT / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * HC_TILE + (uint64_t)warp * 32 * HC_ITEMS;
+  uint32_t mk[HC_ITEMS], dg[HC_ITEMS], sg[HC_ITEMS];
+  uint64_t exc[HC_ITEMS], exd[HC_ITEMS];
+  uint64_t cc = 0, cd = 0;
+#pragma unroll
+  for (int j = 0; j < HC_ITEMS; j++) {
+    const uint64_t i = base + (uint64_t)j * 32 + lane;
+    const uint32_t m = i < words ? marks[i] : 0u;
+    uint32_t d = 0, seg = 0;
+    if (m) {
+      const uint32_t row = (uint32_t)i / wpr;
+      if (row < n_nodes) {
+        seg = off[row];
+        d = off[row + 1] - seg;
+      }
+      marks[i] = 0u;
+    }
+    mk[j] = d ? m : 0u;
+    dg[j] = d;
+    sg[j] = seg;
+    const uint64_t ic = warp_incl_sum((uint64_t)(d ? 1 : 0));
+    const uint64_t id = warp_incl_sum((uint64_t)d);
+    exc[j] = cc + ic - (d ? 1 : 0);
+    exd[j] = cd + id - d;
+    cc += __shfl_sync(kFull, ic, 31);
+    cd += __shfl_sync(kFull, id, 31);
+  }
+  if (lane == 0) {
+    s_wc[warp] = cc;
+    s_wd[warp] = cd;
+  }
+  __syncthreads();
+  uint64_t bc = tile_cnt[blockIdx.x], bd = tile_deg[blockIdx.x];
+  for (int w = 0; w < warp; w++) {
+    bc += s_wc[w];
+    bd += s_wd[w];
+  }
+#pragma unroll
+  for (int j = 0; j < HC_ITEMS; j++) {
+    const uint64_t i = base + (uint64_t)j * 32 + lane;
+    if (dg[j]) {
+      const uint64_t k = bc + exc[j];
+      hword[k] = (uint32_t)i;
+      hmask[k] = mk[j];
+      hpos[k] = bd + exd[j];
+      hseg[k] = sg[j];
+    }
+  }
+  if constexpr (TROP) {
+    // The warp copies the weights of its head words, one 128-byte line per
+    // word (one lane per entry; entries outside the mask are copied too and
+    // never read), eight lines in flight at a time.
+#pragma unroll
+    for (int j = 0; j < HC_ITEMS; j++) {
+      unsigned hb = __ballot_sync(kFull, dg[j] != 0);
+      const uint64_t wb = base + (uint64_t)j * 32;
+      while (hb) {
+        int t[8];
+        int32_t val[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          t[q] = hb ? __ffs(hb) - 1 : -1;
+          hb &= hb - 1;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+          if (t[q] >= 0) val[q] = D[(wb + t[q]) * 32 + lane];
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+          if (t[q] >= 0) Dprev[(wb + t[q]) * 32 + lane] = val[q];
+      }
+    }
+  }
+  if (blockIdx.x == gridDim.x - 1 && tid == 0) {
+    hpos[tile_cnt[n_tiles]] = tile_deg[n_tiles];
+    totals[2] = tile_cnt[n_tiles];
+    totals[3] = tile_deg[n_tiles];
+  }
+}
+
 inline unsigned grid1(uint64_t n) { return (unsigned)ceil_div(n ? n : 1, NT); }
 
-size_t dense_expand_smem() { return (DE_TILE + 1) * (4 + 4 + 4) + DE_TILE * 2 + (DE_TILE + 1) + 16; }
+size_t dense_expand_smem(bool words) {
+  return DE_HEADS * (4 + 4 + 4 + (words ? 4 : 1)) + DE_TILE * 2 + kWarps * 32 * kGroupMax * 2 + 16;
+}
+
+// (kept, v) → index entry: kept and v are the output key's two columns (which
+// one depends on the rule shape), the layout row- or column-major; one of the
+// two coefficients is 1, the other the row width.
+void out_coefficients(const DenseLayout& lay, int out_pshift, int out_vshift, uint64_t* ck, uint64_t* cv) {
+  const bool kept_is_c0 = out_pshift == lay.b1 && out_vshift == 0;
+  if (!kept_is_c0 && !(out_pshift == 0 && out_vshift == lay.b1))
+    fail(STRATA_E_UNSUPPORTED, "direct-addressed expand: unexpected output key layout");
+  const bool kept_is_col = kept_is_c0 == lay.colmajor;  // kept indexes within a row
+  *ck = kept_is_col ? 1 : lay.width;
+  *cv = kept_is_col ? lay.width : 1;
+}
 
 }  // namespace
+
+DenseLayout dense_layout(int b1, uint64_t n0, uint64_t n1, bool colmajor) {
+  DenseLayout L{};
+  L.b1 = b1;
+  L.mask1 = b1 >= 64 ? ~0ull : ((1ull << b1) - 1);
+  L.n0 = n0;
+  L.n1 = n1;
+  L.width = ((colmajor ? n0 : n1) + 31) & ~31ull;
+  L.rows = colmajor ? n1 : n0;
+  L.entries = L.width * L.rows;
+  L.colmajor = colmajor;
+  return L;
+}
 
 uint64_t dense_tile_size() { return DE_TILE; }
 uint32_t dense_group_max() { return kGroupMax; }
@@ -559,8 +779,7 @@ void dense_heads(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uint64
   k_heads_count<K><<<(unsigned)tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, tc, td,
                                                             reinterpret_cast<unsigned long long*>(ct));
   after_launch(ctx, "k_heads_count");
-  scan_tile_sums(ctx, tc, tiles);
-  scan_tile_sums(ctx, td, tiles);
+  scan_tile_sums(ctx, tc, tiles, 2);  // tc and td
   k_heads_write<K><<<(unsigned)tiles, NT, 0, ctx->stream>>>(dkeys, n, jshift, jmask, off, n_nodes, tc, td, tiles,
                                                             hidx, hpos, hseg, hg);
   after_launch(ctx, "k_heads_write");
@@ -584,33 +803,78 @@ void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n
   if (nh == 0 || total == 0) return;
   const uint64_t tiles = ceil_div(nh + total, DE_TILE);
   if (tiles > 0x7fffffffull) fail(STRATA_E_UNSUPPORTED, "expand too large for one launch");
+  uint64_t ck, cv;
+  out_coefficients(lay, out_pshift, out_vshift, &ck, &cv);
   k_tile_splits<<<grid1(tiles + 1), NT, 0, ctx->stream>>>(hpos, nh, total, DE_TILE, tiles, splits_buf);
   after_launch(ctx, "k_tile_splits");
   const int kh = kprof_begin(ctx, K_EXPAND_DENSE);
-  const size_t smem = dense_expand_smem();
-  auto kern = k_expand_dense<K, TROP>;
+  const size_t smem = dense_expand_smem(false);
+  auto kern = k_expand_dense<K, TROP, false>;
   SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  // (kept, v) → index entry: kept and v are the output key's two columns
-  // (which one depends on the rule shape), the layout row- or column-major.
-  uint64_t ck, cv;
-  const bool kept_is_c0 = out_pshift == lay.b1 && out_vshift == 0;
-  if (!kept_is_c0 && !(out_pshift == 0 && out_vshift == lay.b1))
-    fail(STRATA_E_UNSUPPORTED, "direct-addressed expand: unexpected output key layout");
-  if (kept_is_c0) {
-    ck = lay.colmajor ? 1 : lay.n1;
-    cv = lay.colmajor ? lay.n0 : 1;
-  } else {
-    ck = lay.colmajor ? lay.n0 : 1;
-    cv = lay.colmajor ? 1 : lay.n1;
-  }
   kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(dkeys, dw, n_rows, hidx, hpos, hseg, hg, nh, total, splits_buf,
-                                                   pshift, pmask, ck, cv, nbr, n_nbr, nbr_w, lay, bits, D, marks,
-                                                   ctx->d_status);
+                                                   pshift, pmask, ck, cv, 1u, nbr, n_nbr, nbr_w, lay.entries, bits, D,
+                                                   marks, ctx->d_status);
   // Algorithmic bytes: every Δ row (key, weight) once, each head's record,
   // every CSR edge of a group read once (neighbour + weight), one 4-byte
   // index probe per candidate (a candidate = one Δ row × one edge).
   const uint64_t wsz = TROP ? 4 : 0;
   kprof_end(ctx, kh, n_rows * (sizeof(K) + wsz) + nh * (4 + 8 + 4 + 1) + total * (4 + wsz) + candidates * 4);
+  after_launch(ctx, "k_expand_dense");
+}
+
+template <bool TROP>
+void dense_word_heads(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const uint32_t* off,
+                      uint64_t n_nodes, uint64_t* sums, uint32_t* hword, uint32_t* hmask, uint64_t* hpos,
+                      uint32_t* hseg, const int32_t* D, int32_t* Dprev, uint64_t* out4) {
+  const uint64_t words = lay.entries / 32;
+  if (words >= (1ull << 32)) fail(STRATA_E_UNSUPPORTED, "direct-addressed index beyond 2^37 entries");
+  const uint64_t tiles = ceil_div(words ? words : 1, HC_TILE);
+  uint64_t* tc = sums;
+  uint64_t* td = sums + tiles + 1;
+  auto* tot = reinterpret_cast<unsigned long long*>(sums + 2 * (tiles + 1));
+  SK_CUDA(cudaMemsetAsync(tot, 0, 4 * 8, ctx->stream));
+  const uint32_t wpr = (uint32_t)(lay.width / 32);
+  k_words_count<TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, wpr, off, n_nodes, tc, td, tot);
+  after_launch(ctx, "k_words_count");
+  scan_tile_sums(ctx, tc, tiles, 2);  // tc and td
+  k_words_write<TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, wpr, off, n_nodes, tc, td, tiles, hword,
+                                                               hmask, hpos, hseg, D, Dprev, tot);
+  after_launch(ctx, "k_words_write");
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, tot, 4 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  sync_and_check(ctx);
+  out4[0] = ctx->h_scalar[2];  // heads
+  out4[1] = ctx->h_scalar[3];  // (head, edge) outputs
+  out4[2] = ctx->h_scalar[0];  // candidates
+  out4[3] = ctx->h_scalar[1];  // Δ tuples
+}
+
+uint64_t dense_word_heads_sums(const DenseLayout& lay) { return 2 * (ceil_div(lay.entries / 32 + 1, HC_TILE) + 1) + 4; }
+
+template <bool TROP>
+void dense_expand_words(strata_ctx* ctx, const uint32_t* hword, const uint32_t* hmask, const uint64_t* hpos,
+                        const uint32_t* hseg, uint64_t nh, uint64_t total, uint64_t candidates, uint64_t n_delta,
+                        const int32_t* Dprev, int out_pshift, int out_vshift, const uint32_t* nbr, uint64_t n_nbr,
+                        const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D, uint32_t* marks,
+                        uint64_t* splits_buf) {
+  if (nh == 0 || total == 0) return;
+  const uint64_t tiles = ceil_div(nh + total, DE_TILE);
+  if (tiles > 0x7fffffffull) fail(STRATA_E_UNSUPPORTED, "expand too large for one launch");
+  uint64_t ck, cv;
+  out_coefficients(lay, out_pshift, out_vshift, &ck, &cv);
+  k_tile_splits<<<grid1(tiles + 1), NT, 0, ctx->stream>>>(hpos, nh, total, DE_TILE, tiles, splits_buf);
+  after_launch(ctx, "k_tile_splits");
+  const int kh = kprof_begin(ctx, K_EXPAND_DENSE);
+  const size_t smem = dense_expand_smem(true);
+  auto kern = k_expand_dense<uint32_t, TROP, true>;
+  SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(nullptr, Dprev, lay.entries, hword, hpos, hseg, hmask, nh, total,
+                                                   splits_buf, 0, 0, ck, cv, (uint32_t)(lay.width / 32), nbr, n_nbr,
+                                                   nbr_w, lay.entries, bits, D, marks, ctx->d_status);
+  // Algorithmic bytes: each head's record (word, mask, position, segment),
+  // every CSR edge of a head read once (neighbour + weight), each Δ weight
+  // once, one 4-byte index probe per candidate.
+  const uint64_t wsz = TROP ? 4 : 0;
+  kprof_end(ctx, kh, nh * (4 + 4 + 8 + 4) + total * (4 + wsz) + n_delta * wsz + candidates * 4);
   after_launch(ctx, "k_expand_dense");
 }
 
@@ -634,22 +898,23 @@ uint64_t dense_marks_states(uint64_t entries) { return ceil_div((entries + 31) /
 
 template <class K, bool TROP>
 void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, const DenseLayout& lay, uint32_t* bits,
-                int32_t* D) {
+                int32_t* D, uint32_t* marks) {
   if (TROP) {
     k_fill_i32<<<(unsigned)std::min<uint64_t>(ceil_div(lay.entries, NT), (uint64_t)ctx->num_sms * 16), NT, 0,
                  ctx->stream>>>(D, lay.entries, INT32_MAX);
     after_launch(ctx, "k_fill_i32");
   }
   if (!n) return;
-  k_dense_seed<K, TROP><<<grid1(n), NT, 0, ctx->stream>>>(keys, w, n, lay, bits, D, ctx->d_status);
+  k_dense_seed<K, TROP><<<grid1(n), NT, 0, ctx->stream>>>(keys, w, n, lay, bits, D, marks, ctx->d_status);
   after_launch(ctx, "k_dense_seed");
 }
 
 template <class K, bool TROP>
 uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, const DenseLayout& lay, K* out,
                        int32_t* out_w, uint64_t out_cap) {
-  if (!lay.entries) return 0;
-  const uint64_t tiles = ceil_div(lay.entries, DC_TILE);
+  const uint64_t logical = lay.n0 * lay.n1;
+  if (!logical) return 0;
+  const uint64_t tiles = ceil_div(logical, DC_TILE);
   DBuf<uint64_t> states(ctx, tiles + 2);
   uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles + 1);
   SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 2), ctx->stream));
@@ -670,7 +935,7 @@ uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, 
   template uint64_t dense_marks_compact<K, T>(strata_ctx*, uint32_t*, const DenseLayout&, const int32_t*,    \
                                               K*, int32_t*, uint64_t, uint64_t*);                            \
   template void dense_seed<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const DenseLayout&,        \
-                                 uint32_t*, int32_t*);                                                       \
+                                 uint32_t*, int32_t*, uint32_t*);                                            \
   template uint64_t dense_compact<K, T>(strata_ctx*, const uint32_t*, const int32_t*, const DenseLayout&, K*, \
                                         int32_t*, uint64_t);
 template void dense_heads<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t,
@@ -682,5 +947,16 @@ SK_INST_DENSE(uint32_t, true)
 SK_INST_DENSE(uint64_t, false)
 SK_INST_DENSE(uint64_t, true)
 #undef SK_INST_DENSE
+#define SK_INST_WORDS(T)                                                                                         \
+  template void dense_word_heads<T>(strata_ctx*, uint32_t*, const DenseLayout&, const uint32_t*, uint64_t,       \
+                                    uint64_t*, uint32_t*, uint32_t*, uint64_t*, uint32_t*, const int32_t*,       \
+                                    int32_t*, uint64_t*);                                                        \
+  template void dense_expand_words<T>(strata_ctx*, const uint32_t*, const uint32_t*, const uint64_t*,            \
+                                      const uint32_t*, uint64_t, uint64_t, uint64_t, uint64_t, const int32_t*,   \
+                                      int, int, const uint32_t*, uint64_t, const int32_t*, const DenseLayout&,   \
+                                      uint32_t*, int32_t*, uint32_t*, uint64_t*);
+SK_INST_WORDS(false)
+SK_INST_WORDS(true)
+#undef SK_INST_WORDS
 
 }  // namespace sk

@@ -306,30 +306,35 @@ void fill_stats(strata_fix_stats* st, const Acct& a, uint64_t rounds, uint64_t r
 }
 
 // ---- direct-addressed plan ---------------------------------------------------------
-// Index over (c0, c1) in [0, n0) × [0, n1): a bitmap (Bool relation, or the
-// per-round first-touch marks of a Trop relation) and an int32 weight array.
+// Index over (c0, c1) in [0, n0) × [0, n1): a membership bitmap (Bool), an
+// int32 weight array (Trop), the marks of the current Δ and, for Trop, the
+// snapshot of Δ's weights that the next round reads.
 struct DenseIdx {
   DBuf<uint32_t> bits;   // Bool membership
-  DBuf<uint32_t> marks;  // changed in the current round
+  DBuf<uint32_t> marks;  // Δ: the entries the last round marked
   DBuf<int32_t> D;       // Trop weights (INT32_MAX = absent)
-  DBuf<uint64_t> states; // look-back words of the marks compaction
-  DBuf<uint32_t> hidx, hseg;  // group heads of the current Δ (row, CSR segment)
-  DBuf<uint8_t> hg;           // group sizes
-  DBuf<uint64_t> hsums;       // per-tile sums of the head compaction
+  DBuf<int32_t> Dprev;   // Trop: Δ's weights as the round that made it left them
+  DBuf<uint32_t> hidx, hseg, hmask;  // heads (key-head row or marks word, CSR segment, member mask)
+  DBuf<uint8_t> hg;                  // key-head group sizes
+  DBuf<uint64_t> hpos, hsums;        // head degree prefix; per-tile sums of the head compaction
   DenseLayout lay{};
   uint64_t entries = 0;
-  uint64_t words() const { return (entries + 31) / 32; }
+  uint64_t words() const { return entries / 32; }
 };
 
 // Bytes the index needs; the plan is used when they stay within budget.
-inline double dense_bytes(bool trop, uint64_t entries) {
-  return (trop ? 4.0 * (double)entries : 0.0) + (double)entries / 8.0;
+inline double dense_bytes(bool trop, uint64_t n0, uint64_t n1) {
+  const double rows = (double)n1, width = (double)((n0 + 31) & ~31ull);  // the wider of the two layouts
+  const double rows2 = (double)n0, width2 = (double)((n1 + 31) & ~31ull);
+  const double e = std::max(rows * width, rows2 * width2);
+  return (trop ? 8.0 * e : e / 8.0) + e / 8.0;
 }
 constexpr double kDenseBudget = 16e9;
 
 inline bool want_dense(strata_ctx* ctx, bool trop, bool narrow, uint64_t n0, uint64_t n1) {
   const long double e = (long double)n0 * (long double)n1;
-  const bool fits = (!trop || narrow) && e < 9.0e18L && dense_bytes(trop, (uint64_t)e) <= kDenseBudget;
+  const bool fits = (!trop || narrow) && e < 9.0e18L && n0 < (1ull << 32) && n1 < (1ull << 32) &&
+                    dense_bytes(trop, n0, n1) <= kDenseBudget;
   if (ctx->plan == 3) fail(STRATA_E_UNSUPPORTED, "the bit-row plan applies to Bool transitive closure only");
   if (ctx->plan == 1) return false;
   if (ctx->plan == 2 && !fits)
@@ -337,75 +342,101 @@ inline bool want_dense(strata_ctx* ctx, bool trop, bool narrow, uint64_t n0, uin
   return fits;
 }
 
-// `colmajor`: the next round joins on c1 (store c1-major), else on c0.
+// `colmajor`: the next round joins on c1 (rows by c1), else on c0.
 template <bool TROP>
 void dense_alloc(strata_ctx* ctx, DenseIdx& X, uint64_t n0, uint64_t n1, int b1, bool colmajor) {
-  X.bits.ctx = X.D.ctx = X.marks.ctx = X.states.ctx = ctx;
-  X.hidx.ctx = X.hseg.ctx = X.hg.ctx = X.hsums.ctx = ctx;
-  X.entries = n0 * n1;
-  X.lay = DenseLayout{b1, low_mask(b1), n0, n1, X.entries, colmajor};
+  X.bits.ctx = X.D.ctx = X.Dprev.ctx = X.marks.ctx = ctx;
+  X.hidx.ctx = X.hseg.ctx = X.hmask.ctx = X.hg.ctx = X.hpos.ctx = X.hsums.ctx = ctx;
+  X.lay = dense_layout(b1, n0, n1, colmajor);
+  X.entries = X.lay.entries;
   if (!TROP) {
     X.bits.reserve(X.words() + 1);
     SK_CUDA(cudaMemsetAsync(X.bits.p, 0, (X.words() + 1) * 4, ctx->stream));
   }
   X.marks.reserve(X.words() + 1);
   SK_CUDA(cudaMemsetAsync(X.marks.p, 0, (X.words() + 1) * 4, ctx->stream));
-  X.states.reserve(dense_marks_states(X.entries));
-  if (TROP) X.D.reserve(X.entries + 1);
+  X.hsums.reserve(dense_word_heads_sums(X.lay));
+  if (TROP) {
+    X.D.reserve(X.entries + 1);
+    X.Dprev.reserve(X.entries + 1);
+  }
 }
 
-// One round on the index: Δ' (keys in first-touch order, weights from D).
+// A round whose Δ is a key list (the bootstrap src ⋈ edge): key heads, then
+// the expand, which marks the new / improved entries (the next Δ).  Returns
+// the candidate count (a bound on the marks set).
 template <class K, bool TROP>
-uint64_t dense_round(strata_ctx* ctx, const K* dk, const int32_t* dw, uint64_t nd, const Csr<int32_t>& csr,
-                     const JoinSpec& js, int b1, DenseIdx& X, Rel<K, int32_t>& out, Scratch<K, int32_t>& s,
-                     DBuf<uint64_t>& splits, PhaseTimer& pt, Acct& a) {
+uint64_t dense_round_keys(strata_ctx* ctx, const K* dk, const int32_t* dw, uint64_t nd, const Csr<int32_t>& csr,
+                          const JoinSpec& js, DenseIdx& X, DBuf<uint64_t>& splits, PhaseTimer& pt, Acct& a) {
   if (nd == 0) return 0;
   const uint64_t l0 = ctx->launches;
   const int t = pt.begin(&a.join_ms);
-  s.pos.reserve_grow(nd + 1);
+  X.hpos.reserve_grow(nd + 1);
   X.hidx.reserve_grow(nd + 1);
   X.hseg.reserve_grow(nd + 1);
   X.hg.reserve_grow(nd + 1);
-  X.hsums.reserve_grow(dense_heads_sums(nd));
+  DBuf<uint64_t> sums(ctx, dense_heads_sums(nd));
   uint64_t h3[3];
-  dense_heads<K>(ctx, dk, nd, js.jshift, js.jmask, csr.off.p, csr.n_nodes, X.hsums.p, X.hidx.p, s.pos.p, X.hseg.p,
+  dense_heads<K>(ctx, dk, nd, js.jshift, js.jmask, csr.off.p, csr.n_nodes, sums.p, X.hidx.p, X.hpos.p, X.hseg.p,
                  X.hg.p, h3);
   const uint64_t nh = h3[0], T = h3[1], cands = h3[2];  // heads; (group, edge) outputs; candidates
-  uint64_t cnt = 0;
   if (T) {
-    const uint64_t cap = std::min<uint64_t>(cands, X.entries) + 1;
-    out.reserve(cap, TROP);
     splits.reserve_grow(ceil_div(nh + T, dense_tile_size()) + 2);
-    dense_expand<K, TROP>(ctx, dk, dw, nd, X.hidx.p, s.pos.p, X.hseg.p, X.hg.p, nh, T, cands, js.pshift, js.pmask,
+    dense_expand<K, TROP>(ctx, dk, dw, nd, X.hidx.p, X.hpos.p, X.hseg.p, X.hg.p, nh, T, cands, js.pshift, js.pmask,
                           js.out_pshift, js.out_vshift, csr.nbr.p, csr.m, TROP ? csr.w.p : nullptr, X.lay,
                           TROP ? nullptr : X.bits.p, TROP ? X.D.p : nullptr, X.marks.p, splits.p);
-    // Δ' sorted by the next join column, with merged weights; marks cleared.
-    cnt = dense_marks_compact<K, TROP>(ctx, X.marks.p, X.lay, TROP ? X.D.p : nullptr, out.k.p,
-                                       TROP ? out.w.p : nullptr, cap, X.states.p);
   }
   pt.end(t);
   const uint64_t wsz = TROP ? 4 : 0;
-  a.join_b += nd * (sizeof(K) + wsz) + nh * 17 + T * (4 + wsz) + cands * 4 + cnt * (sizeof(K) + 2 * wsz);
+  a.join_b += nd * (sizeof(K) + wsz) + nh * 17 + T * (4 + wsz) + cands * 4;
   a.join_l += (uint32_t)(ctx->launches - l0);
   a.cands += cands;
-  return cnt;
+  return cands;
 }
 
-template <class K, bool TROP>
-void fix_loop_dense(strata_ctx* ctx, Rel<K, int32_t>& delta, const Csr<int32_t>& csr, const JoinSpec& js, int b1,
-                    DenseIdx& X, uint64_t cap, Scratch<K, int32_t>& s, PhaseTimer& pt, Acct& a,
-                    uint64_t* rounds_out) {
-  Rel<K, int32_t> dnext;
-  dnext.k.ctx = dnext.w.ctx = ctx;
+// Semi-naive rounds with Δ in the marks: word heads (which clear the marks
+// and snapshot Δ's weights), then the expand marks Δ'.  A round runs while
+// Δ is non-empty; `bound` is an upper bound on the entries marked now.
+template <bool TROP>
+void fix_loop_dense(strata_ctx* ctx, const Csr<int32_t>& csr, const JoinSpec& js, DenseIdx& X, uint64_t bound,
+                    uint64_t cap, PhaseTimer& pt, Acct& a, uint64_t* rounds_out) {
   DBuf<uint64_t> splits;
   splits.ctx = ctx;
   uint64_t rounds = 0;
-  while (delta.n > 0) {
+  for (;;) {
+    const uint64_t l0 = ctx->launches;
+    const int t = pt.begin(&a.join_ms);
+    const uint64_t hcap = std::min<uint64_t>(X.words(), bound) + 1;
+    X.hidx.reserve_grow(hcap);
+    X.hmask.reserve_grow(hcap);
+    X.hseg.reserve_grow(hcap);
+    X.hpos.reserve_grow(hcap);
+    uint64_t h4[4];
+    dense_word_heads<TROP>(ctx, X.marks.p, X.lay, csr.off.p, csr.n_nodes, X.hsums.p, X.hidx.p, X.hmask.p,
+                           X.hpos.p, X.hseg.p, TROP ? X.D.p : nullptr, TROP ? X.Dprev.p : nullptr, h4);
+    const uint64_t nh = h4[0], T = h4[1], cands = h4[2], nd = h4[3];
+    if (nd == 0) {
+      pt.end(t);
+      a.join_b += X.words() * 4;
+      a.join_l += (uint32_t)(ctx->launches - l0);
+      break;
+    }
     rounds++;
-    const uint64_t nd = dense_round<K, TROP>(ctx, delta.k.p, TROP ? delta.w.p : nullptr, delta.n, csr, js, b1, X,
-                                             dnext, s, splits, pt, a);
-    delta.swap(dnext);
-    delta.n = nd;
+    if (T) {
+      splits.reserve_grow(ceil_div(nh + T, dense_tile_size()) + 2);
+      dense_expand_words<TROP>(ctx, X.hidx.p, X.hmask.p, X.hpos.p, X.hseg.p, nh, T, cands, nd,
+                               TROP ? X.Dprev.p : nullptr, js.out_pshift, js.out_vshift, csr.nbr.p, csr.m,
+                               TROP ? csr.w.p : nullptr, X.lay, TROP ? nullptr : X.bits.p, TROP ? X.D.p : nullptr,
+                               X.marks.p, splits.p);
+    }
+    pt.end(t);
+    const uint64_t wsz = TROP ? 4 : 0;
+    // marks read and cleared, head records written and read, Δ weights
+    // snapshot (read, write, read), edges, probes
+    a.join_b += X.words() * 4 * 2 + nh * 20 * 2 + nd * 3 * wsz + T * (4 + wsz) + cands * 4;
+    a.join_l += (uint32_t)(ctx->launches - l0);
+    a.cands += cands;
+    bound = std::min<uint64_t>(cands, X.entries);
     if (TROP && cap && rounds > cap)
       fail(STRATA_E_NEG_CYCLE, "negative-weight cycle: tropical stratum diverges");
   }
@@ -416,7 +447,7 @@ void fix_loop_dense(strata_ctx* ctx, Rel<K, int32_t>& delta, const Csr<int32_t>&
 template <class K, bool TROP>
 void dense_finish(strata_ctx* ctx, DenseIdx& X, int b1, Rel<K, int32_t>& full, uint64_t upper) {
   (void)b1;
-  const uint64_t cap = std::min<uint64_t>(upper, X.entries) + 1;
+  const uint64_t cap = std::min<uint64_t>(upper, X.lay.n0 * X.lay.n1) + 1;
   full.reserve(cap, TROP);
   full.n = dense_compact<K, TROP>(ctx, X.bits.p, TROP ? X.D.p : nullptr, X.lay, full.k.p,
                                   TROP ? full.w.p : nullptr, cap);
@@ -464,10 +495,11 @@ strata_rel* run_tc_shape(strata_ctx* ctx, const EdgeCols& e, int b0, int b1, int
       DenseIdx X;
       // Δ(Y,Z) joins on c0: row-major index.
       dense_alloc<TROP>(ctx, X, n_nodes_src, n_nodes_dst, b1, false);
-      if (TROP) dense_seed<K, true>(ctx, full.k.p, full.w.p, full.n, X.lay, X.bits.p, X.D.p);
-      else dense_seed<K, false>(ctx, full.k.p, nullptr, full.n, X.lay, X.bits.p, nullptr);
+      // the seed is also the first Δ: its entries are marked
+      if (TROP) dense_seed<K, true>(ctx, full.k.p, full.w.p, full.n, X.lay, X.bits.p, X.D.p, X.marks.p);
+      else dense_seed<K, false>(ctx, full.k.p, nullptr, full.n, X.lay, X.bits.p, nullptr, X.marks.p);
       pt.end(a.setup_t);
-      fix_loop_dense<K, TROP>(ctx, delta, csr, js, b1, X, cap, s, pt, a, &rounds);
+      fix_loop_dense<TROP>(ctx, csr, js, X, full.n, cap, pt, a, &rounds);
       const int tf = pt.begin(&a.finish_ms);
       dense_finish<K, TROP>(ctx, X, b1, full, X.entries);
       pt.end(tf);
@@ -630,16 +662,17 @@ strata_rel* run_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
       DenseIdx X;
       // Δ(S,Y) joins on c1: column-major index, so Δ' comes out sorted by Y.
       dense_alloc<true>(ctx, X, n0, n1, b1, true);
-      dense_seed<K, true>(ctx, nullptr, nullptr, 0, X.lay, X.bits.p, X.D.p);
-      Rel<K, W> delta, full;
-      delta.k.ctx = delta.w.ctx = full.k.ctx = full.w.ctx = ctx;
+      dense_seed<K, true>(ctx, nullptr, nullptr, 0, X.lay, X.bits.p, X.D.p, nullptr);
+      Rel<K, W> full;
+      full.k.ctx = full.w.ctx = ctx;
       DBuf<uint64_t> splits;
       splits.ctx = ctx;
       pt.end(a.setup_t);
-      // Bootstrap: every derivation of src ⋈ edge, all new.
-      delta.n = dense_round<K, true>(ctx, srcu.k.p, srcu.w.p, srcu.n, csr, boot, b1, X, delta, s, splits, pt, a);
+      // Bootstrap: every derivation of src ⋈ edge, all new; its marks are
+      // the first Δ.
+      const uint64_t bound = dense_round_keys<K, true>(ctx, srcu.k.p, srcu.w.p, srcu.n, csr, boot, X, splits, pt, a);
       uint64_t rounds = 0;
-      fix_loop_dense<K, true>(ctx, delta, csr, step, b1, X, cap, s, pt, a, &rounds);
+      fix_loop_dense<true>(ctx, csr, step, X, std::min<uint64_t>(bound, X.entries), cap, pt, a, &rounds);
       const int tf = pt.begin(&a.finish_ms);
       dense_finish<K, true>(ctx, X, b1, full, X.entries);
       pt.end(tf);

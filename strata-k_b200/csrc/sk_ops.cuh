@@ -31,15 +31,21 @@ void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* ou
                            unsigned char* scratch, uint64_t max_n, uint32_t* h_status);
 
 // ---- direct-addressed plan (sk_dense.cu) ----
-// Index over (c0, c1) in [0, n0) × [0, n1); `colmajor` stores (c0, c1) at
-// c1 * n0 + c0 (the join column of the next round first), else c0 * n1 + c1.
+// Index over (c0, c1) in [0, n0) × [0, n1), stored as `rows` rows of `width`
+// entries: `colmajor` puts (c0, c1) at c1 * width + c0 (rows by the join
+// column of the next round), else at c0 * width + c1.  The width is the
+// row's column count rounded up to 32, so no 32-bit word of a bitmap over the
+// index spans two rows; the padding entries are never set.
 struct DenseLayout {
-  int b1;           // key = (c0 << b1) | c1
-  uint64_t mask1;   // (1 << b1) - 1
-  uint64_t n0, n1;  // column domain sizes
-  uint64_t entries; // n0 * n1
+  int b1;            // key = (c0 << b1) | c1
+  uint64_t mask1;    // (1 << b1) - 1
+  uint64_t n0, n1;   // column domain sizes
+  uint64_t width;    // entries per row (multiple of 32)
+  uint64_t rows;     // n1 (colmajor) or n0
+  uint64_t entries;  // rows * width
   bool colmajor;
 };
+DenseLayout dense_layout(int b1, uint64_t n0, uint64_t n1, bool colmajor);
 uint64_t dense_tile_size();
 uint32_t dense_group_max();
 // Group heads of a Δ sorted by join value (see sk_dense.cu): writes hidx
@@ -57,15 +63,39 @@ void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n
                   uint64_t candidates, int pshift, uint64_t pmask, int out_pshift, int out_vshift, const uint32_t* nbr,
                   uint64_t n_nbr, const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D,
                   uint32_t* marks, uint64_t* splits_buf);
+// The marked entries in index order (keys, Trop weights from D); clears the
+// marks.  Used for the bit-row plan's final relation.
 template <class K, bool TROP>
 uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const int32_t* D, K* out,
                              int32_t* out_w, uint64_t out_cap, uint64_t* states_buf);
 uint64_t dense_marks_states(uint64_t entries);
-// In-place exclusive scan of per-tile sums (one block); sums[count] = total.
-void scan_tile_sums(strata_ctx* ctx, uint64_t* sums, uint64_t count);
+// Heads of the Δ held in `marks` (the entries the last round marked): one
+// head per nonzero 32-bit word whose row (join value) has edges, carrying the
+// word's bits as its member mask; Trop copies the heads' member weights
+// D → Dprev (the values Δ carries through the next round).  Clears marks.
+// out4 = {heads, outputs, candidates, Δ tuples}.  `sums` holds
+// dense_word_heads_sums(lay) words.
+template <bool TROP>
+void dense_word_heads(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const uint32_t* off,
+                      uint64_t n_nodes, uint64_t* sums, uint32_t* hword, uint32_t* hmask, uint64_t* hpos,
+                      uint32_t* hseg, const int32_t* D, int32_t* Dprev, uint64_t* out4);
+uint64_t dense_word_heads_sums(const DenseLayout& lay);
+// One round over word heads: candidates (member, edge) of every head,
+// member weights from Dprev; new / improved entries set their marks.
+template <bool TROP>
+void dense_expand_words(strata_ctx* ctx, const uint32_t* hword, const uint32_t* hmask, const uint64_t* hpos,
+                        const uint32_t* hseg, uint64_t nh, uint64_t total, uint64_t candidates, uint64_t n_delta,
+                        const int32_t* Dprev, int out_pshift, int out_vshift, const uint32_t* nbr, uint64_t n_nbr,
+                        const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D, uint32_t* marks,
+                        uint64_t* splits_buf);
+// In-place exclusive scan of per-tile sums (one block per array); sums[count]
+// = total.  `arrays` consecutive arrays of count + 1 words each.
+void scan_tile_sums(strata_ctx* ctx, uint64_t* sums, uint64_t count, int arrays = 1);
+// Seed the index from keys (and weights); `marks` (optional) marks every
+// seeded entry, making the seed the first Δ of the word-head rounds.
 template <class K, bool TROP>
 void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, const DenseLayout& lay, uint32_t* bits,
-                int32_t* D);
+                int32_t* D, uint32_t* marks);
 template <class K, bool TROP>
 uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, const DenseLayout& lay, K* out,
                        int32_t* out_w, uint64_t out_cap);

@@ -134,8 +134,10 @@ __global__ void __launch_bounds__(NT)
 }
 
 // In-place exclusive scan of `count` tile sums in one block; sums[count] = total.
+// One block per array; array b starts at sums + b * (count + 1).
 __global__ void __launch_bounds__(1024) k_scan_tile_sums(uint64_t* sums, uint64_t count) {
   __shared__ uint64_t s_scratch[1024 / 32 + 1];
+  sums += (uint64_t)blockIdx.x * (count + 1);
   const uint64_t per = (count + 1023) / 1024;
   const uint64_t b = (uint64_t)threadIdx.x * per;
   uint64_t local = 0;
@@ -808,8 +810,8 @@ void expand_offsets(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uin
   after_launch(ctx, "k_deg_write");
 }
 
-void scan_tile_sums(strata_ctx* ctx, uint64_t* sums, uint64_t count) {
-  k_scan_tile_sums<<<1, 1024, 0, ctx->stream>>>(sums, count);
+void scan_tile_sums(strata_ctx* ctx, uint64_t* sums, uint64_t count, int arrays) {
+  k_scan_tile_sums<<<arrays, 1024, 0, ctx->stream>>>(sums, count);
   after_launch(ctx, "k_scan_tile_sums");
 }
 
