@@ -98,6 +98,10 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t w, uint32_t k) {
 // DE_TILE / 2 + 1 heads (checked).
 constexpr uint32_t DE_HEADS = DE_TILE / 2 + 2;
 constexpr uint32_t kWarps = NT / 32;
+// Word heads with at least this many members take the bit-lane path (one
+// warp iteration per output at popc / 32 lane use, no slot lookups); the
+// sparser ones are flattened.
+constexpr int kDenseMembers = 12;
 
 template <class K, bool TROP, bool WORDS>
 __global__ void __launch_bounds__(NT, 6)
@@ -193,7 +197,9 @@ __global__ void __launch_bounds__(NT, 6)
           // the head's row; kb = the output index of column 0 of the word
           mm = s_g[li];
           kb = (uint64_t)(((uint32_t)h % wpr) * 32u) * ck + (uint64_t)v * cv;
-          if (h * 32 + 32 > entries) {
+          // every member's entry (and Dprev slot) inside the index: checked
+          // once here for the highest member
+          if (h * 32 + 32 > entries || (mm && kb + (uint64_t)(31 - __clz(mm)) * ck >= entries)) {
             flags |= ST_BOUNDS;
             mm = 0;
           }
@@ -203,6 +209,58 @@ __global__ void __launch_bounds__(NT, 6)
           if (g > kGroupMax || h + g > n_rows) {
             flags |= ST_BOUNDS;
             mm = 0;
+          }
+        }
+      }
+    }
+    if constexpr (WORDS) {
+      // Dense words: lane l takes member bit l, and the warp walks the
+      // outputs (edges) of the dense lanes two at a time; each output's
+      // member weights and probes are one coalesced line.
+      const uint32_t md = mm;
+      unsigned dm = __ballot_sync(kFull, __popc(md) >= kDenseMembers);
+      if ((dm >> lane) & 1u) mm = 0;  // the flattened pass below takes the rest
+      while (dm) {
+        int t[2];
+        t[0] = __ffs(dm) - 1;
+        dm &= dm - 1;
+        t[1] = dm ? __ffs(dm) - 1 : t[0];
+        const bool two = dm != 0;
+        dm &= dm - 1;
+        bool act[2];
+        uint64_t ixd[2];
+        int32_t cwd[2], curd[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const uint32_t m_t = __shfl_sync(kFull, md, t[u]);
+          const uint64_t kb_t = __shfl_sync(kFull, kb, t[u]);
+          const int32_t ew_t = TROP ? __shfl_sync(kFull, ew, t[u]) : 0;
+          const uint32_t w_t = TROP ? __shfl_sync(kFull, (uint32_t)h, t[u]) : 0u;
+          act[u] = ((m_t >> lane) & 1u) && (u == 0 || two);
+          ixd[u] = kb_t + (uint64_t)lane * ck;
+          cwd[u] = 0;
+          if constexpr (TROP)
+            if (act[u]) cwd[u] = dw[(uint64_t)w_t * 32 + lane];
+          if (act[u]) {
+            if constexpr (TROP) curd[u] = D[ixd[u]];
+            else curd[u] = (int32_t)bits[ixd[u] >> 5];
+          }
+          if constexpr (TROP) cwd[u] = trop_mul(cwd[u], ew_t, &flags);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          if (!act[u]) continue;
+          const uint32_t bit = 1u << (ixd[u] & 31);
+          if constexpr (TROP) {
+            if (cwd[u] < curd[u]) {
+              const int32_t old = atomicMin(&D[ixd[u]], cwd[u]);
+              if (cwd[u] < old) atomicOr(&marks[ixd[u] >> 5], bit);
+            }
+          } else {
+            if (((uint32_t)curd[u] & bit) == 0) {
+              const uint32_t old = atomicOr(&bits[ixd[u] >> 5], bit);
+              if ((old & bit) == 0) atomicOr(&marks[ixd[u] >> 5], bit);
+            }
           }
         }
       }
@@ -235,13 +293,8 @@ __global__ void __launch_bounds__(NT, 6)
           const uint64_t kb_t = __shfl_sync(kFull, kb, t);
           const uint32_t w_t = TROP ? __shfl_sync(kFull, (uint32_t)h, t) : 0u;
           if (ok[u]) {
-            ix[u] = kb_t + (uint64_t)r * ck;
-            if (ix[u] >= entries) {
-              flags |= ST_BOUNDS;
-              ok[u] = false;
-            } else if constexpr (TROP) {
-              cw[u] = trop_mul(dw[(uint64_t)w_t * 32 + r], ew_t, &flags);
-            }
+            ix[u] = kb_t + (uint64_t)r * ck;  // inside the index: checked per output
+            if constexpr (TROP) cw[u] = trop_mul(dw[(uint64_t)w_t * 32 + r], ew_t, &flags);
           }
         } else {
           const uint64_t h_t = __shfl_sync(kFull, h, t);
