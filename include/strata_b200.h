@@ -106,8 +106,10 @@ strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan);
  *   STRATA_KNOB_BATCH_BLOCKS_PER_SM resident blocks per SM of the round kernel: 1..32
  *   STRATA_KNOB_BATCH_BUDGET_MB     cap on one batch wave's device bytes, in MiB (>= 1)
  *   STRATA_KNOB_SORT_RANK           radix digit ranking: 1 per-bit warp ballots, 2 match instruction
+ *   STRATA_KNOB_DENSE_WORD_MEMBERS  direct-addressed rounds: Δ words with at least this many
+ *                                   members take the bit-lane expand path: 1..33 (33 = never)
  * value 0 restores the default (15 / 9 / 2 / 8 / occupancy limit / 70% of
- * reusable memory / ballots).  Other values: STRATA_E_INVALID.
+ * reusable memory / ballots / 24).  Other values: STRATA_E_INVALID.
  * The autotuner (strata_b200.tune) sweeps these and caches the best per GPU.
  * No counterpart in the reference (its sort has no tile parameters). */
 #define STRATA_KNOB_SORT_ITEMS_U32 1
@@ -117,6 +119,7 @@ strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan);
 #define STRATA_KNOB_BATCH_BLOCKS_PER_SM 5
 #define STRATA_KNOB_BATCH_BUDGET_MB 6
 #define STRATA_KNOB_SORT_RANK 7
+#define STRATA_KNOB_DENSE_WORD_MEMBERS 8
 strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value);
 /* Enable per-phase CUDA-event timing in strata_fix_stats (adds event records). */
 strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled);

@@ -218,6 +218,11 @@ strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value) {
     ctx->tune_sort_match = value == 2 ? 1 : 0;
     return STRATA_OK;
   }
+  if (knob == STRATA_KNOB_DENSE_WORD_MEMBERS) {
+    if (value < 0 || value > 33) return bad(ctx, "dense word members must be 0 (default) .. 33");
+    ctx->tune_dense_members = value;
+    return STRATA_OK;
+  }
   if (knob == STRATA_KNOB_TRI_PROBE) {
     if (value < 0 || value > 2) return bad(ctx, "triangle probe must be 0 (default), 1 (hash set) or 2 (binary search)");
     ctx->tune_tri_probe = value;

@@ -85,6 +85,7 @@ struct strata_ctx {
   int tune_bs_graph_rounds = 0;     // bit-row rounds per CUDA-graph replay (0 = 8)
   int tune_bs_blocks = 0;           // resident round-kernel blocks per SM (0 = occupancy limit)
   uint64_t tune_bs_budget_mb = 0;   // cap on a batch wave's device bytes, MiB (0 = 70% of free)
+  int tune_dense_members = 0;       // members from which a Δ word takes the bit-lane expand (0 = 24)
   bool profiling = false;
   uint64_t launches = 0;
   // Per-kernel CUDA-event accounting (enabled with profiling).

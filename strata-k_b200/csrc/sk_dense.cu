@@ -93,6 +93,13 @@ __device__ __forceinline__ uint32_t select_bit(uint32_t w, uint32_t k) {
 // of its group, whose index entries are adjacent in one index row, so a
 // warp's probes and atomics touch one or two cache lines instead of 32.
 //
+// Marks.  A candidate marks its entry when it is below (Trop) or absent
+// from (Bool) the value the candidate read, and then merges with an atomic
+// whose result it does not wait for.  An entry is marked exactly when it
+// changed this round: a value read during the round is at most the round's
+// starting value, and the first candidate that lowers (sets) an entry read
+// the starting value, since only such candidates change it.
+//
 // Every head has at least one edge, so the head events of a tile's 2,048
 // merged positions are at least two apart: a tile sees at most
 // DE_TILE / 2 + 1 heads (checked).
@@ -100,8 +107,8 @@ constexpr uint32_t DE_HEADS = DE_TILE / 2 + 2;
 constexpr uint32_t kWarps = NT / 32;
 // Word heads with at least this many members take the bit-lane path (one
 // warp iteration per output at popc / 32 lane use, no slot lookups); the
-// sparser ones are flattened.
-constexpr int kDenseMembers = 12;
+// sparser ones are flattened.  Tunable (STRATA_KNOB_DENSE_WORD_MEMBERS).
+constexpr int kDenseMembers = 24;
 
 template <class K, bool TROP, bool WORDS>
 __global__ void __launch_bounds__(NT, 6)
@@ -109,7 +116,8 @@ __global__ void __launch_bounds__(NT, 6)
                    const uint32_t* __restrict__ hidx, const uint64_t* __restrict__ pos,
                    const uint32_t* __restrict__ hseg, const typename std::conditional<WORDS, uint32_t, uint8_t>::type* __restrict__ hg,
                    uint64_t n, uint64_t total, const uint64_t* __restrict__ splits, int pshift, uint64_t pmask,
-                   uint64_t ck, uint64_t cv, uint32_t wpr, const uint32_t* __restrict__ nbr, uint64_t n_nbr,
+                   uint64_t ck, uint64_t cv, uint32_t wpr, int dense_members, const uint32_t* __restrict__ nbr,
+                   uint64_t n_nbr,
                    const int32_t* __restrict__ nbr_w, uint64_t entries, uint32_t* bits, int32_t* D, uint32_t* marks,
                    uint32_t* status) {
   using GT = typename std::conditional<WORDS, uint32_t, uint8_t>::type;
@@ -218,7 +226,7 @@ __global__ void __launch_bounds__(NT, 6)
       // outputs (edges) of the dense lanes two at a time; each output's
       // member weights and probes are one coalesced line.
       const uint32_t md = mm;
-      unsigned dm = __ballot_sync(kFull, __popc(md) >= kDenseMembers);
+      unsigned dm = __ballot_sync(kFull, __popc(md) >= dense_members);
       if ((dm >> lane) & 1u) mm = 0;  // the flattened pass below takes the rest
       while (dm) {
         int t[2];
@@ -253,13 +261,13 @@ __global__ void __launch_bounds__(NT, 6)
           const uint32_t bit = 1u << (ixd[u] & 31);
           if constexpr (TROP) {
             if (cwd[u] < curd[u]) {
-              const int32_t old = atomicMin(&D[ixd[u]], cwd[u]);
-              if (cwd[u] < old) atomicOr(&marks[ixd[u] >> 5], bit);
+              atomicMin(&D[ixd[u]], cwd[u]);
+              atomicOr(&marks[ixd[u] >> 5], bit);
             }
           } else {
             if (((uint32_t)curd[u] & bit) == 0) {
-              const uint32_t old = atomicOr(&bits[ixd[u] >> 5], bit);
-              if ((old & bit) == 0) atomicOr(&marks[ixd[u] >> 5], bit);
+              atomicOr(&bits[ixd[u] >> 5], bit);
+              atomicOr(&marks[ixd[u] >> 5], bit);
             }
           }
         }
@@ -328,13 +336,13 @@ __global__ void __launch_bounds__(NT, 6)
         const uint32_t bit = 1u << (ix[u] & 31);
         if constexpr (TROP) {
           if (cw[u] < cur[u]) {
-            const int32_t old = atomicMin(&D[ix[u]], cw[u]);
-            if (cw[u] < old) atomicOr(&marks[ix[u] >> 5], bit);  // changed this round
+            atomicMin(&D[ix[u]], cw[u]);
+            atomicOr(&marks[ix[u] >> 5], bit);  // changed this round
           }
         } else {
           if (((uint32_t)cur[u] & bit) == 0) {
-            const uint32_t old = atomicOr(&bits[ix[u] >> 5], bit);
-            if ((old & bit) == 0) atomicOr(&marks[ix[u] >> 5], bit);  // new this round
+            atomicOr(&bits[ix[u] >> 5], bit);
+            atomicOr(&marks[ix[u] >> 5], bit);  // new this round
           }
         }
       }
@@ -865,7 +873,7 @@ void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n
   auto kern = k_expand_dense<K, TROP, false>;
   SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(dkeys, dw, n_rows, hidx, hpos, hseg, hg, nh, total, splits_buf,
-                                                   pshift, pmask, ck, cv, 1u, nbr, n_nbr, nbr_w, lay.entries, bits, D,
+                                                   pshift, pmask, ck, cv, 1u, 33, nbr, n_nbr, nbr_w, lay.entries, bits, D,
                                                    marks, ctx->d_status);
   // Algorithmic bytes: every Δ row (key, weight) once, each head's record,
   // every CSR edge of a group read once (neighbour + weight), one 4-byte
@@ -921,7 +929,8 @@ void dense_expand_words(strata_ctx* ctx, const uint32_t* hword, const uint32_t* 
   auto kern = k_expand_dense<uint32_t, TROP, true>;
   SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(nullptr, Dprev, lay.entries, hword, hpos, hseg, hmask, nh, total,
-                                                   splits_buf, 0, 0, ck, cv, (uint32_t)(lay.width / 32), nbr, n_nbr,
+                                                   splits_buf, 0, 0, ck, cv, (uint32_t)(lay.width / 32),
+                                                   ctx->tune_dense_members ? ctx->tune_dense_members : kDenseMembers, nbr, n_nbr,
                                                    nbr_w, lay.entries, bits, D, marks, ctx->d_status);
   // Algorithmic bytes: each head's record (word, mask, position, segment),
   // every CSR edge of a head read once (neighbour + weight), each Δ weight

@@ -27,6 +27,7 @@ OTHER = {
     4: (2, 4, 8, 16, 32),     # bit-row rounds per CUDA-graph replay (batched closure)
     5: (0, 2, 4, 8),          # resident round-kernel blocks per SM (0 = occupancy limit)
     7: (1, 2),                # radix digit ranking: ballots / match instruction
+    8: (8, 12, 16, 20, 24, 33),  # Δ-word members from which the bit-lane expand path runs (33 = never)
 }
 
 
@@ -135,6 +136,17 @@ def sweep(n: int = 64_000_000, verbose: bool = True, batch_instances: int = 512)
                 res[v] = _time_call(torch, lambda: eng.tc_bool_batch(bw.nodes, bw.edge_off, bs, bd, mode=0), reps=2)
             eng.set_knob(knob, 0)
             record(knob, res)
+        # direct-addressed Trop rounds: multi-source shortest paths on R-MAT-18
+        mw = gen.mssp_workload(scale=18, n_sources=64, seed=11)
+        t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a).astype(dt)).cuda()
+        ms = (t(mw.sources, np.int32), t(mw.src, np.int32), t(mw.dst, np.int32), t(mw.w, np.int64),
+              t(mw.source_w, np.int64))
+        res = {}
+        for v in OTHER[8]:
+            eng.set_knob(8, v)
+            res[v] = _time_call(torch, lambda: eng.mssp_dev(*ms[:4], source_weights=ms[4]).free())
+        eng.set_knob(8, 0)
+        record(8, res)
     finally:
         eng.close()
     return {"gpu": _gpu_name(), "best": best, "timings_ms": timings, "n": n}

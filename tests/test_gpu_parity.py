@@ -222,6 +222,32 @@ def test_mssp_rmat_scale12_exact(peng):
     assert got.stats["rounds"] == want[4]
 
 
+@pytest.mark.parametrize("members", [1, 20, 33])
+def test_mssp_dense_word_paths_identical(engine, members):
+    """Direct-addressed rounds: the bit-lane path for dense Δ words (from 1
+    member: every word; 33: none) gives the oracle's relation and rounds,
+    with sources spread over both marks words of an index row."""
+    wl = gen.mssp_workload(scale=13, n_sources=64, seed=8)
+    want = O.fast_trop(1, wl.src, wl.dst, wl.w, sources=wl.sources, source_w=wl.source_w)
+    engine.set_plan(2)
+    engine.set_knob(8, members)
+    try:
+        got = engine.mssp_trop(wl.sources, (wl.src, wl.dst, wl.w), source_weights=wl.source_w)
+        assert np.array_equal(got.src, want[0]) and np.array_equal(got.dst, want[1])
+        assert np.array_equal(got.w, want[2])
+        assert got.stats["rounds"] == want[4] and got.stats["plan"] == 2
+        # Bool closure on the direct-addressed index (rows padded to 32 columns)
+        s, d = gen.er_directed(777, 3000, members)
+        a, b, r = O.fast_tc(s, d)
+        tc = engine.transitive_closure_bool((s, d))
+        assert np.array_equal(tc.src, a) and np.array_equal(tc.dst, b) and tc.stats["rounds"] == r
+    finally:
+        engine.set_knob(8, 0)
+        engine.set_plan(0)
+    with pytest.raises(S.InvalidArgument):
+        engine.set_knob(8, 34)
+
+
 def test_mssp_rmat_scale16_matches_dijkstra(peng):
     engine = peng
     import torch
