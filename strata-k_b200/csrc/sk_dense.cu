@@ -449,8 +449,8 @@ __global__ void k_fill_i32(int32_t* p, uint64_t n, int32_t v) {
     p[i] = v;
 }
 
-// The final relation in key order: ordinal q enumerates (c0, c1) row-major,
-// whatever the index layout.
+// The final relation of a row-major index, in key order (= index order):
+// ordinal q enumerates (c0, c1) row-major.
 constexpr int DC_ITEMS = 8;
 constexpr uint32_t DC_TILE = NT * DC_ITEMS;
 
@@ -522,6 +522,115 @@ __global__ void __launch_bounds__(NT)
       at++;
     }
   }
+}
+
+// ---- final relation of a column-major index ---------------------------------
+// Key order (c0 major) runs down the columns of a column-major index, so
+// enumerating it in key order strides one row width per entry.  Instead a
+// warp reads a 32-row × 32-column sub-tile along its rows (lane = column,
+// coalesced): the first pass records, per (column, tile of 32 rows), the
+// rows present as a mask; the masks' popcounts are scanned in key order
+// (column major); the second pass re-reads the sub-tile, transposes it
+// through shared memory and writes each column's present entries as one
+// contiguous run of keys (and weights).
+constexpr int CM_ITEMS = 8;
+constexpr uint32_t CM_CHUNK = NT * CM_ITEMS;  // masks per scan block
+
+template <bool TROP>
+__device__ __forceinline__ bool cm_present(const uint32_t* bits, const int32_t* D, uint64_t ix) {
+  if constexpr (TROP) return D[ix] != INT32_MAX;
+  else return (bits[ix >> 5] >> (ix & 31)) & 1u;
+}
+
+template <bool TROP>
+__global__ void __launch_bounds__(NT)
+    k_cm_masks(const uint32_t* __restrict__ bits, const int32_t* __restrict__ D, DenseLayout lay, uint64_t T,
+               uint64_t subtiles, uint32_t* __restrict__ masks) {
+  const uint64_t g = ((uint64_t)blockIdx.x * NT + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= subtiles) return;
+  const uint64_t cw = lay.width / 32, t = g / cw, c = (g - t * cw) * 32 + lane;
+  uint32_t m = 0;
+#pragma unroll 8
+  for (int r = 0; r < 32; r++) {
+    const uint64_t row = t * 32 + r;
+    if (row < lay.rows && cm_present<TROP>(bits, D, row * lay.width + c)) m |= 1u << r;
+  }
+  if (c < lay.n0) masks[c * T + t] = m;
+}
+
+__global__ void __launch_bounds__(NT) k_cm_chunk_sums(const uint32_t* __restrict__ masks, uint64_t M,
+                                                      uint64_t* __restrict__ sums) {
+  __shared__ uint32_t s_red[NT / 32];
+  const uint64_t b = (uint64_t)blockIdx.x * CM_CHUNK + (uint64_t)threadIdx.x * CM_ITEMS;
+  uint32_t c = 0;
+#pragma unroll
+  for (int j = 0; j < CM_ITEMS; j++)
+    if (b + j < M) c += __popc(masks[b + j]);
+  c = warp_sum(c);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t t = 0;
+    for (int w = 0; w < NT / 32; w++) t += s_red[w];
+    sums[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(NT) k_cm_offsets(const uint32_t* __restrict__ masks, uint64_t M,
+                                                   const uint64_t* __restrict__ sums, uint64_t* __restrict__ offs) {
+  __shared__ uint32_t s_scan[NT / 32 + 1];
+  const uint64_t b = (uint64_t)blockIdx.x * CM_CHUNK + (uint64_t)threadIdx.x * CM_ITEMS;
+  uint32_t pc[CM_ITEMS], c = 0;
+#pragma unroll
+  for (int j = 0; j < CM_ITEMS; j++) {
+    pc[j] = b + j < M ? __popc(masks[b + j]) : 0u;
+    c += pc[j];
+  }
+  uint32_t tot;
+  uint64_t run = sums[blockIdx.x] + block_excl_sum<NT>(c, s_scan, &tot);
+#pragma unroll
+  for (int j = 0; j < CM_ITEMS; j++) {
+    if (b + j < M) offs[b + j] = run;
+    run += pc[j];
+  }
+}
+
+template <class K, bool TROP>
+__global__ void __launch_bounds__(NT)
+    k_cm_write(const uint32_t* __restrict__ bits, const int32_t* __restrict__ D, DenseLayout lay, uint64_t T,
+               uint64_t subtiles, const uint32_t* __restrict__ masks, const uint64_t* __restrict__ offs,
+               K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap, uint32_t* status) {
+  __shared__ int32_t s_w[NT / 32][32][33];
+  const uint64_t g = ((uint64_t)blockIdx.x * NT + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (g >= subtiles) return;
+  const uint64_t cw = lay.width / 32, t = g / cw, c0 = (g - t * cw) * 32, c = c0 + lane;
+  const uint32_t m = c < lay.n0 ? masks[c * T + t] : 0u;
+  const uint64_t off = c < lay.n0 ? offs[c * T + t] : 0ull;
+  if constexpr (TROP) {
+#pragma unroll 8
+    for (int r = 0; r < 32; r++) {
+      const uint64_t row = t * 32 + r;
+      s_w[warp][r][lane] = row < lay.rows ? D[row * lay.width + c] : INT32_MAX;
+    }
+    __syncwarp();
+  }
+  uint32_t flags = 0;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int j = 0; j < 32; j++) {
+    const uint32_t mj = __shfl_sync(kFull, m, j);
+    const uint64_t oj = __shfl_sync(kFull, off, j);
+    if (!((mj >> lane) & 1u)) continue;
+    const uint64_t at = oj + __popc(mj & lt);
+    if (at >= out_cap) {
+      flags |= ST_BOUNDS;
+      continue;
+    }
+    out[at] = (K)(((K)(c0 + j) << lay.b1) | (K)(t * 32 + lane));  // (c0, c1) = (column, row)
+    if constexpr (TROP) out_w[at] = s_w[warp][lane][j];
+  }
+  if (flags) atomicOr(status, flags);
 }
 
 // ---- group heads of a Δ sorted by join value ---------------------------------
@@ -649,6 +758,10 @@ __global__ void __launch_bounds__(NT)
 }
 
 // ---- word heads of a Δ held in the marks ------------------------------------
+// Two words per thread: a round's marks are a few MB, so small tiles give the
+// write (one dependent D-line copy per head word) several waves of blocks.
+constexpr int WH_ITEMS = 2;
+constexpr uint32_t WH_TILE = NT * WH_ITEMS;
 // Rounds after the first keep Δ where the expand left it, in the marks bitmap
 // (an entry is in Δ exactly when the round marked it), so Δ needs no key
 // compaction: a head is a nonzero marks word whose row (join value
@@ -663,10 +776,10 @@ __global__ void __launch_bounds__(NT)
                   unsigned long long* totals) {
   __shared__ uint64_t s_red[4][NT / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint64_t base = (uint64_t)blockIdx.x * HC_TILE + (uint64_t)warp * 32 * HC_ITEMS;
+  const uint64_t base = (uint64_t)blockIdx.x * WH_TILE + (uint64_t)warp * 32 * WH_ITEMS;
   uint64_t c = 0, dsum = 0, cands = 0, tuples = 0;
 #pragma unroll
-  for (int j = 0; j < HC_ITEMS; j++) {
+  for (int j = 0; j < WH_ITEMS; j++) {
     const uint64_t i = base + (uint64_t)j * 32 + lane;
     const uint32_t m = i < words ? marks[i] : 0u;
     if (m) {
@@ -712,12 +825,12 @@ __global__ void __launch_bounds__(NT)
                   unsigned long long* totals) {
   __shared__ uint64_t s_wc[NT / 32], s_wd[NT / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint64_t base = (uint64_t)blockIdx.x * HC_TILE + (uint64_t)warp * 32 * HC_ITEMS;
-  uint32_t mk[HC_ITEMS], dg[HC_ITEMS], sg[HC_ITEMS];
-  uint64_t exc[HC_ITEMS], exd[HC_ITEMS];
+  const uint64_t base = (uint64_t)blockIdx.x * WH_TILE + (uint64_t)warp * 32 * WH_ITEMS;
+  uint32_t mk[WH_ITEMS], dg[WH_ITEMS], sg[WH_ITEMS];
+  uint64_t exc[WH_ITEMS], exd[WH_ITEMS];
   uint64_t cc = 0, cd = 0;
 #pragma unroll
-  for (int j = 0; j < HC_ITEMS; j++) {
+  for (int j = 0; j < WH_ITEMS; j++) {
     const uint64_t i = base + (uint64_t)j * 32 + lane;
     const uint32_t m = i < words ? marks[i] : 0u;
     uint32_t d = 0, seg = 0;
@@ -750,7 +863,7 @@ __global__ void __launch_bounds__(NT)
     bd += s_wd[w];
   }
 #pragma unroll
-  for (int j = 0; j < HC_ITEMS; j++) {
+  for (int j = 0; j < WH_ITEMS; j++) {
     const uint64_t i = base + (uint64_t)j * 32 + lane;
     if (dg[j]) {
       const uint64_t k = bc + exc[j];
@@ -765,7 +878,7 @@ __global__ void __launch_bounds__(NT)
     // word (one lane per entry; entries outside the mask are copied too and
     // never read), eight lines in flight at a time.
 #pragma unroll
-    for (int j = 0; j < HC_ITEMS; j++) {
+    for (int j = 0; j < WH_ITEMS; j++) {
       unsigned hb = __ballot_sync(kFull, dg[j] != 0);
       const uint64_t wb = base + (uint64_t)j * 32;
       while (hb) {
@@ -889,7 +1002,7 @@ void dense_word_heads(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, 
                       uint32_t* hseg, const int32_t* D, int32_t* Dprev, uint64_t* out4) {
   const uint64_t words = lay.entries / 32;
   if (words >= (1ull << 32)) fail(STRATA_E_UNSUPPORTED, "direct-addressed index beyond 2^37 entries");
-  const uint64_t tiles = ceil_div(words ? words : 1, HC_TILE);
+  const uint64_t tiles = ceil_div(words ? words : 1, WH_TILE);
   uint64_t* tc = sums;
   uint64_t* td = sums + tiles + 1;
   auto* tot = reinterpret_cast<unsigned long long*>(sums + 2 * (tiles + 1));
@@ -909,7 +1022,7 @@ void dense_word_heads(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, 
   out4[3] = ctx->h_scalar[1];  // Δ tuples
 }
 
-uint64_t dense_word_heads_sums(const DenseLayout& lay) { return 2 * (ceil_div(lay.entries / 32 + 1, HC_TILE) + 1) + 4; }
+uint64_t dense_word_heads_sums(const DenseLayout& lay) { return 2 * (ceil_div(lay.entries / 32 + 1, WH_TILE) + 1) + 4; }
 
 template <bool TROP>
 void dense_expand_words(strata_ctx* ctx, const uint32_t* hword, const uint32_t* hmask, const uint64_t* hpos,
@@ -976,6 +1089,26 @@ uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, 
                        int32_t* out_w, uint64_t out_cap) {
   const uint64_t logical = lay.n0 * lay.n1;
   if (!logical) return 0;
+  if (lay.colmajor) {
+    const uint64_t T = ceil_div(lay.rows, 32), subtiles = T * (lay.width / 32), M = lay.n0 * T;
+    const uint64_t chunks = ceil_div(M, CM_CHUNK);
+    const unsigned blocks = (unsigned)ceil_div(subtiles, NT / 32);
+    DBuf<uint32_t> masks(ctx, M);
+    DBuf<uint64_t> offs(ctx, M), sums(ctx, chunks + 1);
+    k_cm_masks<TROP><<<blocks, NT, 0, ctx->stream>>>(bits, D, lay, T, subtiles, masks.p);
+    after_launch(ctx, "k_cm_masks");
+    k_cm_chunk_sums<<<(unsigned)chunks, NT, 0, ctx->stream>>>(masks.p, M, sums.p);
+    after_launch(ctx, "k_cm_chunk_sums");
+    scan_tile_sums(ctx, sums.p, chunks);
+    k_cm_offsets<<<(unsigned)chunks, NT, 0, ctx->stream>>>(masks.p, M, sums.p, offs.p);
+    after_launch(ctx, "k_cm_offsets");
+    k_cm_write<K, TROP><<<blocks, NT, 0, ctx->stream>>>(bits, D, lay, T, subtiles, masks.p, offs.p, out, out_w,
+                                                         out_cap, ctx->d_status);
+    after_launch(ctx, "k_cm_write");
+    SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, sums.p + chunks, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    sync_and_check(ctx);
+    return ctx->h_scalar[0];
+  }
   const uint64_t tiles = ceil_div(logical, DC_TILE);
   DBuf<uint64_t> states(ctx, tiles + 2);
   uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles + 1);
