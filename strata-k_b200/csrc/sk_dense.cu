@@ -110,17 +110,20 @@ constexpr uint32_t kWarps = NT / 32;
 // sparser ones are flattened.  Tunable (STRATA_KNOB_DENSE_WORD_MEMBERS).
 constexpr int kDenseMembers = 24;
 
-template <class K, bool TROP, bool WORDS>
+template <class K, bool TROP, bool WORDS, class IX>
 __global__ void __launch_bounds__(NT, 6)
     k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n_rows,
                    const uint32_t* __restrict__ hidx, const uint64_t* __restrict__ pos,
                    const uint32_t* __restrict__ hseg, const typename std::conditional<WORDS, uint32_t, uint8_t>::type* __restrict__ hg,
                    uint64_t n, uint64_t total, const uint64_t* __restrict__ splits, int pshift, uint64_t pmask,
-                   uint64_t ck, uint64_t cv, uint32_t wpr, int dense_members, const uint32_t* __restrict__ nbr,
+                   uint64_t ck, uint64_t cv, uint32_t wpr, int wpr_shift, int dense_members,
+                   const uint32_t* __restrict__ nbr,
                    uint64_t n_nbr,
                    const int32_t* __restrict__ nbr_w, uint64_t entries, uint32_t* bits, int32_t* D, uint32_t* marks,
                    uint32_t* status) {
   using GT = typename std::conditional<WORDS, uint32_t, uint8_t>::type;
+  // IX: the index type of entries (32-bit when the index has < 2^32 entries)
+  const IX ckx = (IX)ck;
   // Dynamic shared memory (sizes in dense_expand_smem()):
   //   s_pos   int32  pos of each local head relative to the tile's first output
   //   s_seg   u32    CSR segment start of each local head
@@ -204,7 +207,8 @@ __global__ void __launch_bounds__(NT, 6)
           // members: the set bits of word h, columns (h mod wpr)*32 + bit of
           // the head's row; kb = the output index of column 0 of the word
           mm = s_g[li];
-          kb = (uint64_t)(((uint32_t)h % wpr) * 32u) * ck + (uint64_t)v * cv;
+          const uint32_t wcol = wpr_shift >= 0 ? ((uint32_t)h & (wpr - 1u)) : (uint32_t)h % wpr;
+          kb = (uint64_t)(wcol * 32u) * ck + (uint64_t)v * cv;
           // every member's entry (and Dprev slot) inside the index: checked
           // once here for the highest member
           if (h * 32 + 32 > entries || (mm && kb + (uint64_t)(31 - __clz(mm)) * ck >= entries)) {
@@ -223,32 +227,40 @@ __global__ void __launch_bounds__(NT, 6)
     }
     if constexpr (WORDS) {
       // Dense words: lane l takes member bit l, and the warp walks the
-      // outputs (edges) of the dense lanes two at a time; each output's
+      // outputs (edges) of the dense lanes several at a time; each output's
       // member weights and probes are one coalesced line.
       const uint32_t md = mm;
       unsigned dm = __ballot_sync(kFull, __popc(md) >= dense_members);
       if ((dm >> lane) & 1u) mm = 0;  // the flattened pass below takes the rest
       while (dm) {
-        int t[2];
+        // outputs in flight: four with 32-bit indices, two with 64-bit
+        // ones (more would spill under the 40-register bound)
+        constexpr int U = sizeof(IX) == 4 ? 4 : 2;
+        int t[U];
+        bool live[U];
         t[0] = __ffs(dm) - 1;
+        live[0] = true;
         dm &= dm - 1;
-        t[1] = dm ? __ffs(dm) - 1 : t[0];
-        const bool two = dm != 0;
-        dm &= dm - 1;
-        bool act[2];
-        uint64_t ixd[2];
-        int32_t cwd[2], curd[2];
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
+        for (int u = 1; u < U; u++) {
+          live[u] = dm != 0;
+          t[u] = live[u] ? __ffs(dm) - 1 : t[0];
+          dm &= dm - 1;
+        }
+        bool act[U];
+        IX ixd[U];
+        int32_t cwd[U], curd[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
           const uint32_t m_t = __shfl_sync(kFull, md, t[u]);
-          const uint64_t kb_t = __shfl_sync(kFull, kb, t[u]);
+          const IX kb_t = __shfl_sync(kFull, (IX)kb, t[u]);
           const int32_t ew_t = TROP ? __shfl_sync(kFull, ew, t[u]) : 0;
           const uint32_t w_t = TROP ? __shfl_sync(kFull, (uint32_t)h, t[u]) : 0u;
-          act[u] = ((m_t >> lane) & 1u) && (u == 0 || two);
-          ixd[u] = kb_t + (uint64_t)lane * ck;
+          act[u] = ((m_t >> lane) & 1u) && live[u];
+          ixd[u] = kb_t + (IX)lane * ckx;
           cwd[u] = 0;
           if constexpr (TROP)
-            if (act[u]) cwd[u] = dw[(uint64_t)w_t * 32 + lane];
+            if (act[u]) cwd[u] = dw[(IX)w_t * 32 + (IX)lane];
           if (act[u]) {
             if constexpr (TROP) curd[u] = D[ixd[u]];
             else curd[u] = (int32_t)bits[ixd[u] >> 5];
@@ -256,7 +268,7 @@ __global__ void __launch_bounds__(NT, 6)
           if constexpr (TROP) cwd[u] = trop_mul(cwd[u], ew_t, &flags);
         }
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
+        for (int u = 0; u < U; u++) {
           if (!act[u]) continue;
           const uint32_t bit = 1u << (ixd[u] & 31);
           if constexpr (TROP) {
@@ -284,7 +296,7 @@ __global__ void __launch_bounds__(NT, 6)
     // Candidates j = 0..T-1 of this chunk: slot j names the owner lane t and
     // the member (row offset or bit) of t's head; the edge is v_t.
     for (uint32_t b0 = 0; b0 < T; b0 += 64) {
-      uint64_t ix[2];
+      IX ix[2];
       int32_t cw[2], cur[2];
       bool ok[2];
 #pragma unroll
@@ -298,11 +310,11 @@ __global__ void __launch_bounds__(NT, 6)
         ix[u] = 0;
         cw[u] = 0;
         if constexpr (WORDS) {
-          const uint64_t kb_t = __shfl_sync(kFull, kb, t);
+          const IX kb_t = __shfl_sync(kFull, (IX)kb, t);
           const uint32_t w_t = TROP ? __shfl_sync(kFull, (uint32_t)h, t) : 0u;
           if (ok[u]) {
-            ix[u] = kb_t + (uint64_t)r * ck;  // inside the index: checked per output
-            if constexpr (TROP) cw[u] = trop_mul(dw[(uint64_t)w_t * 32 + r], ew_t, &flags);
+            ix[u] = kb_t + (IX)r * ckx;  // inside the index: checked per output
+            if constexpr (TROP) cw[u] = trop_mul(dw[(IX)w_t * 32 + (IX)r], ew_t, &flags);
           }
         } else {
           const uint64_t h_t = __shfl_sync(kFull, h, t);
@@ -313,8 +325,9 @@ __global__ void __launch_bounds__(NT, 6)
             const uint32_t kept = (uint32_t)((mk >> pshift) & (K)pmask);
             // index of the output key (kept, v) without packing it: one of
             // the two coefficients is 1, the other the index's row width
-            ix[u] = (uint64_t)kept * ck + (uint64_t)v_t * cv;
-            if (ix[u] >= entries) {
+            const uint64_t ix64 = (uint64_t)kept * ck + (uint64_t)v_t * cv;
+            ix[u] = (IX)ix64;
+            if (ix64 >= entries) {
               flags |= ST_BOUNDS;
               ok[u] = false;
             } else if constexpr (TROP) {
@@ -983,11 +996,14 @@ void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n
   after_launch(ctx, "k_tile_splits");
   const int kh = kprof_begin(ctx, K_EXPAND_DENSE);
   const size_t smem = dense_expand_smem(false);
-  auto kern = k_expand_dense<K, TROP, false>;
-  SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(dkeys, dw, n_rows, hidx, hpos, hseg, hg, nh, total, splits_buf,
-                                                   pshift, pmask, ck, cv, 1u, 33, nbr, n_nbr, nbr_w, lay.entries, bits, D,
-                                                   marks, ctx->d_status);
+  auto launch = [&](auto kern) {
+    SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(dkeys, dw, n_rows, hidx, hpos, hseg, hg, nh, total, splits_buf,
+                                                     pshift, pmask, ck, cv, 1u, 0, 33, nbr, n_nbr, nbr_w, lay.entries,
+                                                     bits, D, marks, ctx->d_status);
+  };
+  if (lay.entries <= 0xffffffffull) launch(k_expand_dense<K, TROP, false, uint32_t>);
+  else launch(k_expand_dense<K, TROP, false, uint64_t>);
   // Algorithmic bytes: every Δ row (key, weight) once, each head's record,
   // every CSR edge of a group read once (neighbour + weight), one 4-byte
   // index probe per candidate (a candidate = one Δ row × one edge).
@@ -1039,12 +1055,17 @@ void dense_expand_words(strata_ctx* ctx, const uint32_t* hword, const uint32_t* 
   after_launch(ctx, "k_tile_splits");
   const int kh = kprof_begin(ctx, K_EXPAND_DENSE);
   const size_t smem = dense_expand_smem(true);
-  auto kern = k_expand_dense<uint32_t, TROP, true>;
-  SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(nullptr, Dprev, lay.entries, hword, hpos, hseg, hmask, nh, total,
-                                                   splits_buf, 0, 0, ck, cv, (uint32_t)(lay.width / 32),
-                                                   ctx->tune_dense_members ? ctx->tune_dense_members : kDenseMembers, nbr, n_nbr,
-                                                   nbr_w, lay.entries, bits, D, marks, ctx->d_status);
+  const uint32_t wpr = (uint32_t)(lay.width / 32);
+  const int wpr_shift = (wpr & (wpr - 1)) == 0 ? __builtin_ctz(wpr) : -1;
+  const int members = ctx->tune_dense_members ? ctx->tune_dense_members : kDenseMembers;
+  auto launch = [&](auto kern) {
+    SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(nullptr, Dprev, lay.entries, hword, hpos, hseg, hmask, nh, total,
+                                                     splits_buf, 0, 0, ck, cv, wpr, wpr_shift, members, nbr, n_nbr,
+                                                     nbr_w, lay.entries, bits, D, marks, ctx->d_status);
+  };
+  if (lay.entries <= 0xffffffffull) launch(k_expand_dense<uint32_t, TROP, true, uint32_t>);
+  else launch(k_expand_dense<uint32_t, TROP, true, uint64_t>);
   // Algorithmic bytes: each head's record (word, mask, position, segment),
   // every CSR edge of a head read once (neighbour + weight), each Δ weight
   // once, one 4-byte index probe per candidate.
