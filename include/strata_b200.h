@@ -257,6 +257,40 @@ strata_status strata_tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint3
     const uint64_t* edge_off, const uint32_t* src, const uint32_t* dst, int mode,
     uint64_t* counts, uint64_t* fps, uint32_t* rounds, strata_batch_stats* stats);
 
+/* ---- sharded Bool closure (one rank's share) -----------------------------
+ * Rank `rank` of `world` owns the path rows X in [rank*P, min((rank+1)*P,
+ * n_nodes)), P = ceil(n_nodes / world), as bit rows of `row_bytes` bytes
+ * over the Z domain.  The only exchange is once per round: the caller
+ * gathers every rank's Delta' slice (P rows, P row flags) into the full
+ * Delta (world*P rows and flags, in rank order) that the next round reads
+ * (an NCCL all-gather over NVLink), and sums the ranks' |Delta'|; the
+ * closure is done when that sum is 0.  The rounds, the summed |path| and the
+ * summed fingerprint sum mix64(X)*c^Z (mod 2^64, as strata_tc_bool_batch)
+ * equal the single-device closure's.
+ * Counterpart: the reference's sharding interface for joins
+ * (strata-gpu/src/partition.rs:35-83, a CPU specification: tuples
+ * hash-partitioned by join key, the whole join the union of the shard
+ * joins); here path is partitioned by row and Delta replicated by the gather.
+ * d_src / d_dst (m edges, device) must stay valid until the seed returns;
+ * endpoints outside [0, n_nodes): STRATA_E_INVALID. */
+typedef struct strata_tc_shard strata_tc_shard;
+strata_status strata_tc_shard_create(strata_ctx* ctx, uint32_t n_nodes, const uint32_t* d_src,
+    const uint32_t* d_dst, uint64_t m, uint32_t rank, uint32_t world, strata_tc_shard** out);
+strata_status strata_tc_shard_shape(const strata_tc_shard* sh, uint32_t* rows_per_rank, uint32_t* row_lo,
+    uint32_t* row_hi, uint64_t* row_bytes);
+/* Delta0 = path = the rank's edges: writes its Delta slice (P rows of
+ * row_bytes, 16-byte aligned) and P row flags; *n_delta = |Delta0| of its rows. */
+strata_status strata_tc_shard_seed(strata_ctx* ctx, strata_tc_shard* sh, void* d_delta_mine,
+    uint8_t* d_flags_mine, uint64_t* n_delta);
+/* One semi-naive round of the rank's rows from the gathered Delta (which must
+ * not overlap the outputs); *n_delta = |Delta'| of its rows. */
+strata_status strata_tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const void* d_delta_full,
+    const uint8_t* d_flags_full, void* d_delta_mine, uint8_t* d_flags_mine, uint64_t* n_delta);
+/* |path| of the rank's rows and their part of the fingerprint. */
+strata_status strata_tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count,
+    uint64_t* fingerprint);
+void strata_tc_shard_free(strata_tc_shard* sh);
+
 /* ---- Prov_k capture and provenance circuits -----------------------------
  * The probabilistic reachability program
  *     path(X,Y) :- edge(X,Y).   path(X,Z) :- edge(X,Y), path(Y,Z).

@@ -750,6 +750,165 @@ void bs_run(strata_ctx* ctx, const std::vector<InstSpec>& spec, const uint32_t* 
   if (exec) cudaGraphExecDestroy(exec);
 }
 
+// ---- one rank's share of a sharded closure ---------------------------------
+// The rank owns path rows X ∈ [lo, lo + rows) (local row x = X - lo), each W4
+// uint4 words over the Z domain.  A round reads Δ(Y) of every node from the
+// gathered matrix Dfull (all ranks' slices of the previous round, rank r's
+// slice = rows [r·per, r·per + per)) with its byte flags ffull, and writes
+// Δ'(X) of its own rows into Dmine / fmine:
+//     Δ'(X) = ( ∪_{Y ∈ out(X)} Δ(Y) ) ∖ path(X),   path(X) ∪= Δ'(X)
+// the same round as k_bs_round, one warp per unit of 32 / L rows.
+struct ShardView {
+  uint32_t rows, n, W;
+  int ls;                // log2(lanes per row)
+  const uint64_t* off;   // rows + 1, local rows
+  const uint32_t* nbr;   // global neighbour ids
+  uint4* F;              // rows × W
+  unsigned long long* delta;
+};
+
+__global__ void __launch_bounds__(BS_NT) k_shard_round(ShardView v, const uint4* __restrict__ Dfull,
+                                                       const uint8_t* __restrict__ ffull, uint4* __restrict__ Dmine,
+                                                       uint8_t* __restrict__ fmine) {
+  const int lane = threadIdx.x & 31;
+  const int ls = v.ls;
+  const uint32_t lpr = 1u << ls, sub = (uint32_t)lane >> ls, sl = (uint32_t)lane & (lpr - 1);
+  const unsigned smask = ls == 5 ? 0xffffffffu : (((1u << lpr) - 1u) << (sub << ls));
+  const uint32_t W = v.W;
+  const uint64_t units = ((uint64_t)v.rows + (32u >> ls) - 1) / (32u >> ls);
+  const uint64_t nwarps = (uint64_t)gridDim.x * (BS_NT / 32);
+  uint64_t cnt = 0;
+  for (uint64_t u = ((uint64_t)blockIdx.x * BS_NT + threadIdx.x) >> 5; u < units; u += nwarps) {
+    const uint64_t x = u * (32u >> ls) + sub;
+    const bool valid = x < v.rows;
+    const uint64_t e0 = valid ? v.off[x] : 0, e1 = valid ? v.off[x + 1] : 0;
+    bool any_y = false;
+    for (uint64_t e = e0 + sl; e < e1; e += lpr) {
+      const uint32_t y = v.nbr[e];
+      if (y < v.n && ffull[y]) any_y = true;
+    }
+    const unsigned bal_y = __ballot_sync(kFull, any_y);  // every lane takes part
+    const bool row_has = valid && (bal_y & smask) != 0u;
+    bool row_any = false;
+    if (valid) {
+      for (uint32_t c = sl; c < W; c += lpr) {
+        uint4 nw = make_uint4(0u, 0u, 0u, 0u);
+        if (row_has) {
+          uint4 acc = make_uint4(0u, 0u, 0u, 0u);
+          for (uint64_t e = e0; e < e1; e += 4) {
+            uint32_t y[4];
+            bool on[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) y[q] = e + q < e1 ? v.nbr[e + q] : 0xffffffffu;
+#pragma unroll
+            for (int q = 0; q < 4; q++) on[q] = y[q] < v.n && ffull[y[q]] != 0;
+            uint4 d[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) d[q] = on[q] ? Dfull[(uint64_t)y[q] * W + c] : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+              acc.x |= d[q].x;
+              acc.y |= d[q].y;
+              acc.z |= d[q].z;
+              acc.w |= d[q].w;
+            }
+          }
+          if (any4(acc)) {
+            uint4* fp = v.F + x * W + c;
+            uint4 f = *fp;
+            nw = make_uint4(acc.x & ~f.x, acc.y & ~f.y, acc.z & ~f.z, acc.w & ~f.w);
+            if (any4(nw)) {
+              *fp = make_uint4(f.x | nw.x, f.y | nw.y, f.z | nw.z, f.w | nw.w);
+              cnt += popc4(nw);
+              row_any = true;
+            }
+          }
+        }
+        Dmine[x * W + c] = nw;  // rows without Δ' are cleared too
+      }
+    }
+    const unsigned bal = __ballot_sync(kFull, row_any);
+    if (valid && sl == 0) fmine[x] = (bal & smask) != 0u ? 1 : 0;
+  }
+  cnt = warp_sum(cnt);
+  if (lane == 0 && cnt) atomicAdd(v.delta, (unsigned long long)cnt);
+}
+
+// Local out-degrees of the rank's rows; endpoints outside [0, n) set *bad.
+__global__ void k_shard_degree(const uint32_t* __restrict__ src, const uint32_t* __restrict__ dst, uint64_t m,
+                               uint32_t n, uint32_t lo, uint32_t hi, uint64_t* deg, uint32_t* bad) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t a = src[e], b = dst[e];
+    if (a >= n || b >= n) {
+      atomicOr(bad, 1u);
+      continue;
+    }
+    if (a >= lo && a < hi) atomicAdd(reinterpret_cast<unsigned long long*>(&deg[a - lo]), 1ull);
+  }
+}
+
+// CSR fill (neighbour order within a row is free: the round ORs them) and
+// the seed: path(X) = Δ0(X) = the out-neighbour bits of X.
+__global__ void k_shard_fill(const uint32_t* __restrict__ src, const uint32_t* __restrict__ dst, uint64_t m,
+                             uint32_t n, uint32_t lo, uint32_t hi, uint32_t W, const uint64_t* __restrict__ off,
+                             uint32_t* cursor, uint32_t* nbr, uint32_t* F, uint32_t* Dmine, uint8_t* fmine) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t a = src[e], b = dst[e];
+    if (a >= n || b >= n || a < lo || a >= hi) continue;
+    const uint32_t x = a - lo;
+    nbr[off[x] + atomicAdd(&cursor[x], 1u)] = b;
+    const uint64_t wd = (uint64_t)x * W * 4 + (b >> 5);
+    atomicOr(&F[wd], 1u << (b & 31));
+    atomicOr(&Dmine[wd], 1u << (b & 31));
+    fmine[x] = 1;
+  }
+}
+
+__global__ void k_shard_popc(const uint4* __restrict__ F, uint64_t words, unsigned long long* out) {
+  uint64_t c = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (uint64_t)gridDim.x * blockDim.x)
+    c += popc4(F[i]);
+  c = warp_sum(c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (unsigned long long)c);
+}
+
+// |path| and Σ mix64(X)·c^Z of the rank's rows (global X = lo + x); one warp
+// per row.
+__global__ void __launch_bounds__(BS_NT) k_shard_summary(const uint4* __restrict__ F, uint32_t rows, uint32_t W,
+                                                         uint32_t lo, const uint64_t* __restrict__ tpw,
+                                                         const uint64_t* __restrict__ tb_g, unsigned long long* out) {
+  __shared__ uint64_t tb[4][256];
+  for (int t = threadIdx.x; t < 1024; t += BS_NT) (&tb[0][0])[t] = tb_g[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = (uint64_t)gridDim.x * (BS_NT / 32);
+  for (uint64_t x = ((uint64_t)blockIdx.x * BS_NT + threadIdx.x) >> 5; x < rows; x += nwarps) {
+    uint64_t cnt = 0, poly = 0;
+    for (uint32_t c = lane; c < W; c += 32) {
+      const uint4 q = F[x * W + c];
+      const uint32_t wd[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        const uint32_t w = wd[h];
+        if (!w) continue;
+        cnt += __popc(w);
+        const uint64_t t = tb[0][w & 255] + tb[1][(w >> 8) & 255] + tb[2][(w >> 16) & 255] + tb[3][w >> 24];
+        poly += tpw[4 * (uint64_t)c + h] * t;
+      }
+    }
+    cnt = warp_sum(cnt);
+    poly = warp_sum(poly);
+    if (lane == 0) {
+      uint64_t z = (uint64_t)lo + x + kPolyC;  // splitmix64 finalizer of the global X
+      z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+      z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+      z ^= z >> 31;
+      if (cnt) atomicAdd(&out[0], (unsigned long long)cnt);
+      if (poly) atomicAdd(&out[1], (unsigned long long)(poly * z));
+    }
+  }
+}
+
 uint64_t bs_budget(strata_ctx* ctx) {
   uint64_t b = (uint64_t)((double)reusable_device_bytes(ctx) * 0.7);
   if (ctx->cap && ctx->cap > ctx->in_use) b = std::min<uint64_t>(b, ctx->cap - ctx->in_use);
@@ -839,6 +998,105 @@ uint64_t tc_bool_bitset(strata_ctx* ctx, const uint32_t* d_src, const uint32_t* 
                                                      nullptr, n + 1, states.p);
   if (got != n) fail(STRATA_E_CUDA, "bit-row compaction count disagrees with the summed Δ sizes");
   return n;
+}
+
+// ---- sharded closure: one rank's share ------------------------------------
+void tc_shard_init(strata_ctx* ctx, strata_tc_shard* sh, uint32_t n, const uint32_t* d_src, const uint32_t* d_dst,
+                   uint64_t m, uint32_t rank, uint32_t world) {
+  sh->n = n;
+  sh->rank = rank;
+  sh->world = world;
+  sh->per = (uint32_t)ceil_div(n, world);
+  sh->lo = std::min<uint64_t>((uint64_t)rank * sh->per, n);
+  sh->hi = std::min<uint64_t>((uint64_t)sh->lo + sh->per, n);
+  sh->w4 = (uint32_t)std::max<uint64_t>(1, ceil_div(n, 128));
+  const uint32_t rows = sh->hi - sh->lo;
+  sh->off.ctx = sh->nbr.ctx = sh->F.ctx = sh->acc.ctx = ctx;
+  sh->acc.reserve(4);
+  sh->off.reserve((uint64_t)rows + 2);
+  SK_CUDA(cudaMemsetAsync(sh->off.p, 0, ((uint64_t)rows + 2) * 8, ctx->stream));
+  SK_CUDA(cudaMemsetAsync(sh->acc.p, 0, 4 * 8, ctx->stream));
+  const unsigned g = (unsigned)std::min<uint64_t>(ceil_div(m ? m : 1, BS_NT), (uint64_t)ctx->num_sms * 8);
+  uint32_t* bad = reinterpret_cast<uint32_t*>(sh->acc.p + 3);
+  k_shard_degree<<<g, BS_NT, 0, ctx->stream>>>(d_src, d_dst, m, n, sh->lo, sh->hi, sh->off.p, bad);
+  after_launch(ctx, "k_shard_degree");
+  scan_tile_sums(ctx, sh->off.p, rows);  // off[rows] = the rank's edges
+  uint64_t edges, flag;
+  read_u64(ctx, sh->off.p + rows, &edges, 1);
+  read_u64(ctx, reinterpret_cast<const uint64_t*>(sh->acc.p + 3), &flag, 1);
+  if ((uint32_t)flag) fail(STRATA_E_INVALID, "an edge endpoint is outside [0, n_nodes)");
+  sh->n_edges = edges;
+  sh->nbr.reserve(edges + 1);
+  sh->F.reserve((uint64_t)sh->per * sh->w4 + 1);
+  sh->src = d_src;
+  sh->dst = d_dst;
+  sh->m = m;
+}
+
+uint64_t tc_shard_seed(strata_ctx* ctx, strata_tc_shard* sh, uint4* Dmine, uint8_t* fmine) {
+  const uint64_t vecs = (uint64_t)sh->per * sh->w4;
+  SK_CUDA(cudaMemsetAsync(sh->F.p, 0, vecs * 16, ctx->stream));
+  SK_CUDA(cudaMemsetAsync(Dmine, 0, vecs * 16, ctx->stream));
+  SK_CUDA(cudaMemsetAsync(fmine, 0, sh->per, ctx->stream));
+  DBuf<uint32_t> cursor(ctx, (uint64_t)(sh->hi - sh->lo) + 1);
+  SK_CUDA(cudaMemsetAsync(cursor.p, 0, ((uint64_t)(sh->hi - sh->lo) + 1) * 4, ctx->stream));
+  const unsigned g = (unsigned)std::min<uint64_t>(ceil_div(sh->m ? sh->m : 1, BS_NT), (uint64_t)ctx->num_sms * 8);
+  k_shard_fill<<<g, BS_NT, 0, ctx->stream>>>(sh->src, sh->dst, sh->m, sh->n, sh->lo, sh->hi, sh->w4, sh->off.p,
+                                             cursor.p, sh->nbr.p, reinterpret_cast<uint32_t*>(sh->F.p),
+                                             reinterpret_cast<uint32_t*>(Dmine), fmine);
+  after_launch(ctx, "k_shard_fill");
+  SK_CUDA(cudaMemsetAsync(sh->acc.p, 0, 8, ctx->stream));
+  k_shard_popc<<<(unsigned)std::min<uint64_t>(ceil_div(vecs ? vecs : 1, BS_NT), (uint64_t)ctx->num_sms * 8), BS_NT, 0,
+                 ctx->stream>>>(sh->F.p, vecs, sh->acc.p);
+  after_launch(ctx, "k_shard_popc");
+  uint64_t c;
+  read_u64(ctx, reinterpret_cast<const uint64_t*>(sh->acc.p), &c, 1);
+  sync_and_check(ctx);
+  return c;  // |Δ0| of the rank's rows (distinct edges)
+}
+
+uint64_t tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const uint4* Dfull, const uint8_t* ffull, uint4* Dmine,
+                        uint8_t* fmine) {
+  ShardView v{};
+  v.rows = sh->hi - sh->lo;
+  v.n = sh->n;
+  v.W = sh->w4;
+  v.ls = (int)lanes_shift(sh->w4);
+  v.off = sh->off.p;
+  v.nbr = sh->nbr.p;
+  v.F = sh->F.p;
+  v.delta = sh->acc.p;
+  SK_CUDA(cudaMemsetAsync(sh->acc.p, 0, 8, ctx->stream));
+  const uint64_t units = ceil_div((uint64_t)v.rows, 32u >> v.ls);
+  if (units) {
+    const unsigned g = (unsigned)std::min<uint64_t>(ceil_div(units, BS_NT / 32), (uint64_t)ctx->num_sms * 8);
+    k_shard_round<<<g, BS_NT, 0, ctx->stream>>>(v, Dfull, ffull, Dmine, fmine);
+    after_launch(ctx, "k_shard_round");
+  }
+  uint64_t c;
+  read_u64(ctx, reinterpret_cast<const uint64_t*>(sh->acc.p), &c, 1);
+  sync_and_check(ctx);
+  return c;
+}
+
+void tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count, uint64_t* fp) {
+  std::vector<uint64_t> tpw, tb;
+  poly_tables((uint64_t)sh->w4 * 4, tpw, tb);
+  DBuf<uint64_t> d_tpw(ctx, tpw.size()), d_tb(ctx, 1024);
+  SK_CUDA(cudaMemcpyAsync(d_tpw.p, tpw.data(), tpw.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  SK_CUDA(cudaMemcpyAsync(d_tb.p, tb.data(), 1024 * 8, cudaMemcpyHostToDevice, ctx->stream));
+  SK_CUDA(cudaMemsetAsync(sh->acc.p, 0, 16, ctx->stream));
+  const uint32_t rows = sh->hi - sh->lo;
+  if (rows) {
+    const unsigned g = (unsigned)std::min<uint64_t>(ceil_div(rows, BS_NT / 32), (uint64_t)ctx->num_sms * 8);
+    k_shard_summary<<<g, BS_NT, 0, ctx->stream>>>(sh->F.p, rows, sh->w4, sh->lo, d_tpw.p, d_tb.p, sh->acc.p);
+    after_launch(ctx, "k_shard_summary");
+  }
+  uint64_t h[2];
+  read_u64(ctx, reinterpret_cast<const uint64_t*>(sh->acc.p), h, 2);
+  sync_and_check(ctx);
+  *count = h[0];
+  *fp = h[1];
 }
 
 template uint64_t tc_bool_bitset<uint32_t>(strata_ctx*, const uint32_t*, const uint32_t*, uint64_t, uint64_t,

@@ -481,6 +481,98 @@ strata_status strata_tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint3
   SK_GUARD_END(ctx)
 }
 
+// ---- sharded Bool closure -------------------------------------------------------
+
+strata_status strata_tc_shard_create(strata_ctx* ctx, uint32_t n_nodes, const uint32_t* d_src,
+                                     const uint32_t* d_dst, uint64_t m, uint32_t rank, uint32_t world,
+                                     strata_tc_shard** out) {
+  if (!ctx || !out) return STRATA_E_INVALID;
+  *out = nullptr;
+  if (world == 0 || rank >= world || n_nodes == 0) return bad(ctx, "need world >= 1, rank < world and n_nodes >= 1");
+  if (m && (!d_src || !d_dst)) return bad(ctx, "null edge columns");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  auto* sh = new strata_tc_shard();
+  sh->ctx = ctx;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  sk::tc_shard_init(ctx, sh, n_nodes, d_src, d_dst, m, rank, world);
+  *out = sh;
+  return STRATA_OK;
+  }
+  catch (const SkError& err) {
+    delete sh;
+    ctx->last_error = err.msg;
+    cudaGetLastError();
+    return err.code;
+  }
+  catch (...) {
+    delete sh;
+    return STRATA_E_CUDA;
+  }
+}
+
+strata_status strata_tc_shard_shape(const strata_tc_shard* sh, uint32_t* rows_per_rank, uint32_t* row_lo,
+                                    uint32_t* row_hi, uint64_t* row_bytes) {
+  if (!sh) return STRATA_E_INVALID;
+  if (rows_per_rank) *rows_per_rank = sh->per;
+  if (row_lo) *row_lo = sh->lo;
+  if (row_hi) *row_hi = sh->hi;
+  if (row_bytes) *row_bytes = (uint64_t)sh->w4 * 16;
+  return STRATA_OK;
+}
+
+strata_status strata_tc_shard_seed(strata_ctx* ctx, strata_tc_shard* sh, void* d_delta_mine, uint8_t* d_flags_mine,
+                                   uint64_t* n_delta) {
+  if (!ctx || !sh || sh->ctx != ctx || !d_delta_mine || !d_flags_mine) return STRATA_E_INVALID;
+  if (reinterpret_cast<uintptr_t>(d_delta_mine) % 16) return bad(ctx, "the Delta slice must be 16-byte aligned");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  const uint64_t c = sk::tc_shard_seed(ctx, sh, static_cast<uint4*>(d_delta_mine), d_flags_mine);
+  if (n_delta) *n_delta = c;
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const void* d_delta_full,
+                                    const uint8_t* d_flags_full, void* d_delta_mine, uint8_t* d_flags_mine,
+                                    uint64_t* n_delta) {
+  if (!ctx || !sh || sh->ctx != ctx || !d_delta_full || !d_flags_full || !d_delta_mine || !d_flags_mine)
+    return STRATA_E_INVALID;
+  if (reinterpret_cast<uintptr_t>(d_delta_full) % 16 || reinterpret_cast<uintptr_t>(d_delta_mine) % 16)
+    return bad(ctx, "Delta buffers must be 16-byte aligned");
+  const uint64_t full_bytes = (uint64_t)sh->world * sh->per * sh->w4 * 16;
+  const auto f0 = reinterpret_cast<uintptr_t>(d_delta_full), m0 = reinterpret_cast<uintptr_t>(d_delta_mine);
+  const uint64_t mine_bytes = (uint64_t)sh->per * sh->w4 * 16;
+  if (m0 < f0 + full_bytes && f0 < m0 + mine_bytes) return bad(ctx, "the Delta slice overlaps the gathered Delta");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  const uint64_t c = sk::tc_shard_round(ctx, sh, static_cast<const uint4*>(d_delta_full), d_flags_full,
+                                        static_cast<uint4*>(d_delta_mine), d_flags_mine);
+  if (n_delta) *n_delta = c;
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count, uint64_t* fingerprint) {
+  if (!ctx || !sh || sh->ctx != ctx) return STRATA_E_INVALID;
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  uint64_t c, f;
+  sk::tc_shard_summary(ctx, sh, &c, &f);
+  if (count) *count = c;
+  if (fingerprint) *fingerprint = f;
+  SK_GUARD_END(ctx)
+}
+
+void strata_tc_shard_free(strata_tc_shard* sh) {
+  if (!sh) return;
+  try {
+    delete sh;  // device buffers go back to the context's pool
+  } catch (...) {
+  }
+}
+
 // ---- Prov_k capture and provenance circuits --------------------------------------
 
 struct strata_proofs {

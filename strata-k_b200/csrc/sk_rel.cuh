@@ -38,6 +38,21 @@ struct strata_circuits {
   uint64_t n_children = 0;
 };
 
+// One rank's share of a sharded bit-row closure (sk_bitset.cu): path rows
+// [lo, hi) of n nodes (per = ceil(n / world) rows per rank), the rows'
+// out-edge CSR with global neighbour ids, and the rank's path bit rows.
+struct strata_tc_shard {
+  strata_ctx* ctx = nullptr;
+  uint32_t n = 0, rank = 0, world = 0, per = 0, lo = 0, hi = 0, w4 = 0;
+  uint64_t n_edges = 0, m = 0;
+  const uint32_t* src = nullptr;  // the caller's edge columns (device)
+  const uint32_t* dst = nullptr;
+  sk::DBuf<uint64_t> off;
+  sk::DBuf<uint32_t> nbr;
+  sk::DBuf<uint4> F;
+  sk::DBuf<unsigned long long> acc;  // counters: Δ' size, summary, bad-edge flag
+};
+
 namespace sk {
 
 // Device columns of an input relation (weights / inf mask optional).
@@ -90,6 +105,13 @@ uint64_t count_triangles_undirected(strata_ctx* ctx, const uint32_t* a, const ui
 uint64_t count_4cliques_undirected(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n);
 uint64_t binary_plan_intermediate(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n);
 uint64_t intern_terms(strata_ctx* ctx, const uint64_t* keys, uint64_t n, uint32_t* ids);
+
+void tc_shard_init(strata_ctx* ctx, strata_tc_shard* sh, uint32_t n, const uint32_t* d_src, const uint32_t* d_dst,
+                   uint64_t m, uint32_t rank, uint32_t world);
+uint64_t tc_shard_seed(strata_ctx* ctx, strata_tc_shard* sh, uint4* Dmine, uint8_t* fmine);
+uint64_t tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const uint4* Dfull, const uint8_t* ffull, uint4* Dmine,
+                        uint8_t* fmine);
+void tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count, uint64_t* fp);
 
 void rel_to_host(strata_ctx* ctx, const strata_rel* rel, uint32_t* src, uint32_t* dst, int64_t* w,
                  uint8_t* inf);

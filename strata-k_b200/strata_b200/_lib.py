@@ -113,6 +113,13 @@ SIGNATURES = {
                                            C.POINTER(BatchStats)]),
     "strata_tc_bool_batch": (C.c_int, [ctxp, C.c_uint32, u32p, u64p, u32p, u32p, C.c_int, u64p, u64p, u32p,
                                        C.POINTER(BatchStats)]),
+    "strata_tc_shard_create": (C.c_int, [ctxp, C.c_uint32, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32,
+                                         C.POINTER(vp)]),
+    "strata_tc_shard_shape": (C.c_int, [vp, u32p, u32p, u32p, u64p]),
+    "strata_tc_shard_seed": (C.c_int, [ctxp, vp, vp, vp, u64p]),
+    "strata_tc_shard_round": (C.c_int, [ctxp, vp, vp, vp, vp, vp, u64p]),
+    "strata_tc_shard_summary": (C.c_int, [ctxp, vp, u64p, u64p]),
+    "strata_tc_shard_free": (None, [vp]),
     "strata_prov_tc_capture": (C.c_int, [ctxp, C.c_uint32, vp, vp, C.c_uint64, vp, C.c_uint32, C.c_uint32, u32p,
                                          u32p, C.POINTER(vp), u32p, C.POINTER(ProvStats)]),
     "strata_proofs_shape": (C.c_int, [vp, u32p, u64p, u64p]),

@@ -371,6 +371,21 @@ class Engine:
             _dp(ew), _dp(einf), ne, C.byref(rel), C.byref(st)))
         return DeviceRelation(self, rel, st.as_dict())
 
+    # -- sharded Bool closure (one rank's share) --------------------------
+    def tc_shard(self, n_nodes: int, src, dst, rank: int, world: int) -> "TcShard":
+        """Rank `rank`'s share of a Bool closure split by path rows over
+        `world` ranks (`strata_b200.shard.tc_bool_sharded` runs the rounds).
+        ``src``/``dst`` are device tensors (int32 or uint32 ids)."""
+        if not (hasattr(src, "data_ptr") and hasattr(dst, "data_ptr")):
+            raise InvalidArgument("tc_shard takes device tensors")
+        if _len(src) != _len(dst):
+            raise InvalidArgument("src and dst must have the same length")
+        _torch_sync(src)
+        out = C.c_void_p()
+        self._check(self.lib.strata_tc_shard_create(self.ctx, n_nodes, _dp(src), _dp(dst), _len(src), rank, world,
+                                                     C.byref(out)))
+        return TcShard(self, out, rank, world, keep=(src, dst))
+
     # -- batched Bool reachability ---------------------------------------
     def tc_bool_batch(self, nodes, edge_off, src, dst, mode: int = 0) -> "BatchResult":
         """Closures of many independent graphs (instance i: nodes [0, nodes[i]),
@@ -674,6 +689,57 @@ class Circuits:
             self.free()
         except Exception:
             pass
+
+
+def _torch_sync(*tensors):
+    """Finish torch's queued work on the tensors' device before the engine's
+    own stream reads them (the engine returns only after its stream is idle)."""
+    import torch
+    for t in tensors:
+        if hasattr(t, "is_cuda") and t.is_cuda:
+            torch.cuda.current_stream(t.device).synchronize()
+            return
+
+
+class TcShard:
+    """One rank's share of a sharded Bool closure (``strata_tc_shard``):
+    path rows [lo, hi) of n, ``per`` rows per rank, bit rows of
+    ``row_bytes`` bytes.  Δ slices are int32 device tensors of
+    per * row_bytes / 4 words, row flags uint8 tensors of ``per`` bytes."""
+
+    def __init__(self, eng: Engine, handle, rank: int, world: int, keep=()):
+        self.eng, self.h, self.rank, self.world = eng, handle, rank, world
+        self._keep = keep  # the edge columns stay alive until the seed has read them
+        per, lo, hi, rb = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint64()
+        eng._check(eng.lib.strata_tc_shard_shape(handle, C.byref(per), C.byref(lo), C.byref(hi), C.byref(rb)))
+        self.per, self.lo, self.hi, self.row_bytes = int(per.value), int(lo.value), int(hi.value), int(rb.value)
+
+    def shape(self) -> tuple[int, int, int, int]:
+        return self.per, self.lo, self.hi, self.row_bytes
+
+    def seed(self, mine, fmine) -> int:
+        n = C.c_uint64()
+        _torch_sync(mine)
+        self.eng._check(self.eng.lib.strata_tc_shard_seed(self.eng.ctx, self.h, _dp(mine), _dp(fmine), C.byref(n)))
+        self._keep = ()
+        return int(n.value)
+
+    def round(self, full, ffull, mine, fmine) -> int:
+        n = C.c_uint64()
+        _torch_sync(full)
+        self.eng._check(self.eng.lib.strata_tc_shard_round(self.eng.ctx, self.h, _dp(full), _dp(ffull), _dp(mine),
+                                                           _dp(fmine), C.byref(n)))
+        return int(n.value)
+
+    def summary(self) -> tuple[int, int]:
+        c, f = C.c_uint64(), C.c_uint64()
+        self.eng._check(self.eng.lib.strata_tc_shard_summary(self.eng.ctx, self.h, C.byref(c), C.byref(f)))
+        return int(c.value), int(f.value)
+
+    def free(self):
+        if self.h:
+            self.eng.lib.strata_tc_shard_free(self.h)
+            self.h = None
 
 
 class BatchResult:

@@ -12,8 +12,11 @@ are computed, so N GPUs run them side by side and only the results meet:
 * triangles: the source vertices of the oriented edges, with the edge list
   replicated; the counts add up.
 
-Bool transitive closure (one instance) is the exception: its rows need each
-other's Δ every round, so it runs as a replica per rank.
+* Bool transitive closure (one instance): its rows need each other's Δ
+  every round, so it has a real exchange step — each rank owns a range of
+  path rows (bit rows), and after every round the ranks' Δ' slices are
+  all-gathered into the full Δ the next round reads, and their |Δ'| summed
+  (`tc_bool_sharded`).
 
 The helpers are plain partition functions plus gather/reduce through
 torch.distributed (NCCL on GPUs, gloo in the CPU tests).
@@ -81,6 +84,61 @@ def allreduce_sum_u64(dist, value: int, device="cpu") -> int:
     t = torch.tensor([int(value)], dtype=torch.int64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return int(t.item())
+
+
+def allreduce_sum_mod64(dist, value: int, device="cpu") -> int:
+    """Sum of unsigned 64-bit values mod 2^64 (fingerprints), through int64."""
+    import torch
+    v = int(value) & 0xFFFFFFFFFFFFFFFF
+    t = torch.tensor([v - (1 << 64) if v >= 1 << 63 else v], dtype=torch.int64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(t.item()) & 0xFFFFFFFFFFFFFFFF
+
+
+def tc_bool_sharded(shards, dist=None, device=None) -> tuple[int, int, int]:
+    """Semi-naive Bool closure with path rows split across ranks.
+
+    `shards` are this process's rank shares (``TcShard`` objects, or any
+    object with ``world``, ``shape()``, ``seed``, ``round`` and ``summary``):
+    one under torch.distributed (`dist` given), whose Δ' slice and row flags
+    meet the other ranks' through an all-gather into the full Δ every round
+    (NCCL over NVLink on GPUs) and whose |Δ'| is summed by an all-reduce; or
+    all `world` shares in rank order with `dist` None, the slices then simply
+    concatenated (one process standing in for the ranks).  Every rank takes
+    the same collective steps in the same order until the summed |Δ'| is 0.
+    Returns (|path|, fingerprint Σ mix64(X)·c^Z mod 2^64, rounds)."""
+    import torch
+    per, _, _, row_bytes = shards[0].shape()
+    world = shards[0].world
+    words = per * row_bytes // 4
+    full = [torch.zeros(world * words, dtype=torch.int32, device=device) for _ in range(2)]
+    ffull = [torch.zeros(world * per, dtype=torch.uint8, device=device) for _ in range(2)]
+    mine = [torch.zeros(words, dtype=torch.int32, device=device) for _ in shards]
+    fmine = [torch.zeros(per, dtype=torch.uint8, device=device) for _ in shards]
+
+    def meet(k: int, counts: list[int]) -> int:
+        if dist is None:
+            torch.cat(mine, out=full[k])
+            torch.cat(fmine, out=ffull[k])
+            return sum(counts)
+        dist.all_gather_into_tensor(full[k], mine[0])
+        dist.all_gather_into_tensor(ffull[k], fmine[0])
+        return allreduce_sum_u64(dist, counts[0], device=device or "cpu")
+
+    total = meet(0, [s.seed(mine[i], fmine[i]) for i, s in enumerate(shards)])
+    cur, rounds = 0, 0
+    while total:
+        rounds += 1
+        counts = [s.round(full[cur], ffull[cur], mine[i], fmine[i]) for i, s in enumerate(shards)]
+        cur ^= 1
+        total = meet(cur, counts)
+    parts = [s.summary() for s in shards]
+    count = sum(c for c, _ in parts)
+    fp = sum(f for _, f in parts) & 0xFFFFFFFFFFFFFFFF
+    if dist is not None:
+        count = allreduce_sum_u64(dist, count, device=device or "cpu")
+        fp = allreduce_sum_mod64(dist, fp, device=device or "cpu")
+    return count, fp, rounds
 
 
 def gather_objects(dist, obj, world: int) -> list:

@@ -126,3 +126,49 @@ def test_bit_row_plan_selected_and_exclusive(engine):
             engine.shortest_paths_trop([(0, 1, 1), (1, 2, 1)])
     finally:
         engine.set_plan(0)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 5])
+def test_sharded_closure_ranks_on_one_gpu(engine, world):
+    """The sharded closure's device rounds, with every rank's share run in
+    this process (no rank waits on another; the Δ' slices are concatenated
+    where ranks would all-gather them): count, fingerprint and rounds equal
+    the oracle's and the single-device batch's."""
+    import torch
+
+    from strata_b200 import shard
+    for n, m, seed in ((3000, 9000, 41), (777, 2500, 42), (129, 400, 43)):
+        s, d = gen.er_directed(n, m, seed)
+        s, d = np.concatenate([s, s[:10]]), np.concatenate([d, d[:10]])  # duplicate edges
+        c, f = O.closure_batch([n], [0, len(s)], s, d, threads=8)
+        rounds = O.fast_tc(s, d)[2]
+        ts = torch.from_numpy(s.astype(np.int32)).cuda()
+        td = torch.from_numpy(d.astype(np.int32)).cuda()
+        parts = [engine.tc_shard(n, ts, td, r, world) for r in range(world)]
+        try:
+            got = shard.tc_bool_sharded(parts, device="cuda")
+        finally:
+            for p in parts:
+                p.free()
+        assert got == (int(c[0]), int(f[0]), rounds), (n, world)
+        one = engine.tc_bool_batch([n], [0, len(s)], s, d)
+        assert (int(one.counts[0]), int(one.fps[0]), int(one.rounds[0])) == got
+
+
+def test_sharded_closure_rejects_bad_input(engine):
+    import torch
+    ts = torch.tensor([0, 5], dtype=torch.int32, device="cuda")
+    td = torch.tensor([1, 1], dtype=torch.int32, device="cuda")
+    with pytest.raises(S.InvalidArgument):  # endpoint outside [0, n)
+        engine.tc_shard(3, ts, td, 0, 2)
+    with pytest.raises(S.InvalidArgument):  # rank >= world
+        engine.tc_shard(8, ts, td, 2, 2)
+    sh = engine.tc_shard(8, ts, td, 0, 2)
+    try:
+        per, _, _, rb = sh.shape()
+        full = torch.zeros(2 * per * rb // 4, dtype=torch.int32, device="cuda")
+        flags = torch.zeros(2 * per, dtype=torch.uint8, device="cuda")
+        with pytest.raises(S.InvalidArgument):  # the slice inside the gathered Δ
+            sh.round(full, flags, full[: per * rb // 4], flags[:per])
+    finally:
+        sh.free()

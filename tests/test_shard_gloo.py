@@ -21,6 +21,68 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
+class NumpyTcShard:
+    """CPU stand-in of one rank's ``TcShard`` with the same buffer layout
+    (bit rows of ceil(n / 128) · 16 bytes, bit Z of a row at word Z / 32, bit
+    Z % 32), so the orchestrator moves the same bytes as on GPUs."""
+
+    def __init__(self, n, src, dst, rank, world):
+        self.n, self.rank, self.world = n, rank, world
+        self.per = -(-n // world)
+        self.lo = min(rank * self.per, n)
+        self.hi = min(self.lo + self.per, n)
+        self.w4 = max(1, -(-n // 128))
+        self.row_bytes = self.w4 * 16
+        self.out = [[] for _ in range(self.hi - self.lo)]
+        for a, b in zip(np.asarray(src).tolist(), np.asarray(dst).tolist()):
+            if self.lo <= a < self.hi:
+                self.out[a - self.lo].append(b)
+        self.F = np.zeros((self.hi - self.lo, self.w4 * 128), bool)
+
+    def shape(self):
+        return self.per, self.lo, self.hi, self.row_bytes
+
+    def _emit(self, delta, mine, fmine):
+        import torch
+        rows = np.zeros((self.per, self.w4 * 128), bool)
+        rows[: len(delta)] = delta
+        packed = np.packbits(rows, axis=1, bitorder="little")
+        mine.copy_(torch.from_numpy(packed.reshape(-1).view(np.int32).copy()))
+        fmine.copy_(torch.from_numpy(rows.any(axis=1).astype(np.uint8)))
+        return int(delta.sum())
+
+    def seed(self, mine, fmine):
+        for x, ys in enumerate(self.out):
+            self.F[x, ys] = True
+        return self._emit(self.F.copy(), mine, fmine)
+
+    def round(self, full, ffull, mine, fmine):
+        D = np.unpackbits(full.numpy().view(np.uint8).reshape(-1, self.row_bytes), axis=1, bitorder="little")
+        D = D.astype(bool)
+        flags = ffull.numpy().astype(bool)
+        delta = np.zeros_like(self.F)
+        for x, ys in enumerate(self.out):
+            ys = [y for y in ys if flags[y]]
+            if ys:
+                delta[x] = D[ys].any(axis=0) & ~self.F[x]
+        self.F |= delta
+        return self._emit(delta, mine, fmine)
+
+    def summary(self):
+        import oracle as O
+        x, z = np.nonzero(self.F)
+        return int(len(x)), O.poly_fingerprint(x + self.lo, z, self.n)
+
+
+def _closure_graph(seed):
+    rng = np.random.default_rng(seed)
+    n = 300
+    s = rng.integers(0, n, 700)
+    d = rng.integers(0, n, 700)
+    s[:5], d[:5] = 7, 7  # self-loops and a duplicate
+    return n, s.astype(np.uint32), d.astype(np.uint32)
+
+
 def _worker(rank: int, world: int, port: int, out_dir: str):
     for p in (ROOT / "strata-k_b200", ROOT / "oracle"):
         sys.path.insert(0, str(p))
@@ -74,6 +136,12 @@ def _worker(rank: int, world: int, port: int, out_dir: str):
         total = shard.allreduce_sum_u64(dist, mine)
         if rank == 0:
             res["tri"] = total == O.count_pattern(tw.src, tw.dst)
+        # Bool closure: path rows per rank, Δ' all-gathered every round
+        n, cs, cd = _closure_graph(17)
+        got = shard.tc_bool_sharded([NumpyTcShard(n, cs, cd, rank, world)], dist)
+        if rank == 0:
+            c, f = O.closure_batch([n], [0, len(cs)], cs, cd, threads=2)
+            res["tc"] = got == (int(c[0]), int(f[0]), O.fast_tc(cs, cd)[2])
     finally:
         dist.destroy_process_group()
     if rank == 0:
@@ -85,7 +153,25 @@ def test_two_gloo_ranks_split_every_workload(tmp_path):
     port = _free_port()
     mp.start_processes(_worker, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn", join=True)
     res = eval((tmp_path / "result.txt").read_text())
-    assert res == {"mssp": True, "batch": True, "prov": True, "tri": True}, res
+    assert res == {"mssp": True, "batch": True, "prov": True, "tri": True, "tc": True}, res
+
+
+def test_sharded_closure_emulated_ranks():
+    """All ranks' shares in one process (slices concatenated): uneven row
+    splits, more ranks than rows, and an edge-free rank give the closure's
+    count, fingerprint and rounds."""
+    sys.path.insert(0, str(ROOT / "strata-k_b200"))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from strata_b200 import shard
+    n, cs, cd = _closure_graph(18)
+    c, f = O.closure_batch([n], [0, len(cs)], cs, cd, threads=2)
+    want = (int(c[0]), int(f[0]), O.fast_tc(cs, cd)[2])
+    for world in (1, 3, 7):
+        got = shard.tc_bool_sharded([NumpyTcShard(n, cs, cd, r, world) for r in range(world)])
+        assert got == want, world
+    tiny = shard.tc_bool_sharded([NumpyTcShard(2, [0], [1], r, 4) for r in range(4)])
+    assert tiny == (1, O.poly_fingerprint([0], [1], 2), 1)
 
 
 def test_partitions_cover_every_unit_once():
