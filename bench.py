@@ -16,8 +16,10 @@ relation.  metric = |dist| / device time.
 Under torchrun every rank runs its own instance (its own graph seed and
 sources; no data-path collective) and `value` sums tuples over ranks divided
 by the max rank time ("scaling": "weak"); with --shard the ranks split one
-instance's independent units instead (sources, batch instances, query
-targets, triangle source vertices; "scaling": "strong").  `--impl reference` times the
+instance instead ("scaling": "strong"): its independent units (sources,
+batch instances, query targets, triangle source vertices), or for the Bool
+closure its path rows, whose Δ' rows meet in an all-gather every round.
+`--impl reference` times the
 reference interpreter's algorithm (the CPU restatement in oracle/, nested
 loop `solve`, all host threads) on a bounded sample of the same workload.
 """
@@ -55,8 +57,9 @@ def parse():
     ap.add_argument("--instances", type=int, default=4096, help="batch: number of instances")
     ap.add_argument("--queries", type=int, default=1024, help="prov: number of ?grad query pairs")
     ap.add_argument("--shard", action="store_true",
-                    help="N > 1: split one workload's independent units across the ranks (mssp sources, batch "
-                         "instances, prov query targets) instead of running a replica per rank")
+                    help="N > 1: split one workload across the ranks (mssp sources, batch instances, prov "
+                         "query targets, triangle source vertices; tc path rows with the Δ' rows all-gathered "
+                         "every round) instead of running a replica per rank")
     ap.add_argument("--plan", choices=["auto", "sort-merge", "dense"], default="auto")
     ap.add_argument("--tuned", action="store_true", help="apply the autotuner's cached knob values")
     ap.add_argument("--scale", type=int, default=None, help="R-MAT scale (mssp: 20, tri: 22)")
@@ -111,7 +114,7 @@ def metric_for(kind: str) -> str:
 
 
 def config(args, world):
-    sharded = bool(args.shard and world > 1 and args.workload in ("mssp", "batch", "prov", "tri"))
+    sharded = bool(args.shard and world > 1 and args.workload in ("mssp", "tc", "batch", "prov", "tri"))
     common = {"parallelism": f"sharded{world}" if sharded else f"replicas{world}", "plan": args.plan,
               "l2": "flushed (256 MiB write) before every timed step"}
     if args.workload == "tc":
@@ -334,6 +337,7 @@ class Job:
                     ("dst", wl.dst, i32), ("w", wl.w, i64))
         else:
             cols = (("src", wl.src, i32), ("dst", wl.dst, i32))
+            self.n_nodes = int(max(wl.src.max(), wl.dst.max())) + 1 if len(wl.src) else 1
         self.host = {k: torch.from_numpy(np.ascontiguousarray(v).astype(dt)).pin_memory() for k, v, dt in cols}
         self.entry = {"mssp": "strata_mssp_trop_dev", "tc": "strata_tc_bool_dev",
                       "tri": "strata_count_triangle_pattern_dev", "batch": "strata_tc_bool_batch_dev"}[kind]
@@ -342,6 +346,18 @@ class Job:
         """One fixpoint on device columns `d`: returns (result handle, tuples, stats)."""
         if self.kind == "mssp":
             rel = self.eng.mssp_dev(d["sources"], d["src"], d["dst"], d["w"], source_weights=d["sw"])
+        elif self.kind == "tc" and getattr(self, "tc_shard", None):
+            # path rows split across the ranks, Δ' slices all-gathered each round
+            from strata_b200 import shard
+            rank, world, dist = self.tc_shard
+            part = self.eng.tc_shard(self.n_nodes, d["src"], d["dst"], rank, world)
+            try:
+                total, fp, rounds = shard.tc_bool_sharded([part], dist=dist, device="cuda")
+                mine = part.summary()[0]
+            finally:
+                part.free()
+            self.last = (total, fp, rounds)
+            return None, mine, {"rounds": rounds, "fingerprint": fp, "path_total": total}
         elif self.kind == "tc":
             rel = self.eng.tc_bool_dev(d["src"], d["dst"])
         elif self.kind == "prov":
@@ -382,6 +398,8 @@ class Job:
             return 8  # the u64 count, returned through the entry point's out-parameter
         if self.kind == "batch":
             return len(self.wl) * (8 + 8 + 4)  # per-instance count, fingerprint, rounds
+        if self.kind == "tc" and getattr(self, "tc_shard", None):
+            return 8 + 8 + 8  # |path|, fingerprint and rounds (a sharded closure stays on the ranks)
         if self.kind == "prov":
             P, G = self.last
             P.cpu()
@@ -428,7 +446,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
-    sharded = bool(args.shard and world > 1 and args.workload in ("mssp", "batch", "prov", "tri"))
+    sharded = bool(args.shard and world > 1 and args.workload in ("mssp", "tc", "batch", "prov", "tri"))
     wl = workload_for(0 if sharded else rank, args.scale, units_arg(args), args.workload)
     x_range = None
     if sharded:
@@ -440,6 +458,8 @@ def run_ours(args):
             wl = shard.batch_subset(wl, shard.shard_instances(wl.nodes, rank, world))
         elif args.workload == "tri":
             x_range = shard.shard_vertices(int(max(wl.src.max(), wl.dst.max())) + 1, rank, world)
+        elif args.workload == "tc":
+            pass  # the Job splits the path rows; the edge list is replicated
         else:
             qi = shard.shard_queries(wl.qt, rank, world)
             wl.qs, wl.qt = wl.qs[qi], wl.qt[qi]
@@ -449,6 +469,9 @@ def run_ours(args):
     eng.set_stream(stream.cuda_stream)
     job = Job(args.workload, wl, eng, torch)
     job.x_range = x_range
+    if sharded and args.workload == "tc":
+        job.tc_shard = (rank, world, pg)
+        job.entry = "strata_tc_shard_create/seed/round/summary + NCCL all-gather of the Δ' rows"
     with torch.cuda.stream(stream):
         d = {k: v.to("cuda", non_blocking=True) for k, v in job.host.items()}
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
@@ -478,7 +501,7 @@ def run_ours(args):
 
     # ---- the sort-merge plan on the same inputs (reported beside the headline)
     sort_plan = None
-    if not args.no_sort_plan and args.workload in ("mssp", "tc") and args.plan == "auto":
+    if not args.no_sort_plan and args.workload in ("mssp", "tc") and args.plan == "auto" and not sharded:
         eng.set_plan(PLANS["sort-merge"])
         job.free(step()[0])  # warm its buffers
         eng.set_profiling(True)
@@ -544,7 +567,9 @@ def run_ours(args):
         e2e = {"value": e2e_val, "unit": unit_for(args.workload), "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
                "path": f"pinned host columns -> torch H2D -> {job.entry}"
-                       + (" (count out-parameter)" if args.workload == "tri" else " -> strata_rel_to_host (pinned)")}
+                       + (" (count out-parameter)" if args.workload == "tri" else
+                          " (count, fingerprint, rounds)" if getattr(job, "tc_shard", None) else
+                          " -> strata_rel_to_host (pinned)")}
 
     # ---- roofline of the dominant kernel
     peaks = {}

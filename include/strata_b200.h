@@ -128,7 +128,8 @@ uint64_t strata_ctx_launches(const strata_ctx* ctx);
 /* Per-kernel accounting collected while profiling is on: launches, summed
  * CUDA-event duration and algorithmic bytes moved.  Kernel ids:
  * 0 radix pass, 1 expand emit, 2 expand offsets, 3 run reduction,
- * 4 merge/diff, 5 radix histogram, 6 triangle count, 7 direct-addressed expand. */
+ * 4 merge/diff, 5 radix histogram, 6 triangle count, 7 direct-addressed expand,
+ * 8 bit-row round, 9 Prov_k round, 10 circuit pass, 11 sharded bit-row round. */
 strata_status strata_ctx_kernel_stats(strata_ctx* ctx, int kernel, uint64_t* launches,
                                       double* ms, uint64_t* bytes);
 strata_status strata_ctx_reset_kernel_stats(strata_ctx* ctx);

@@ -765,6 +765,7 @@ struct ShardView {
   const uint32_t* nbr;   // global neighbour ids
   uint4* F;              // rows × W
   unsigned long long* delta;
+  unsigned long long* bytes;  // algorithmic bytes (as k_bs_round counts them), or null
 };
 
 __global__ void __launch_bounds__(BS_NT) k_shard_round(ShardView v, const uint4* __restrict__ Dfull,
@@ -778,6 +779,7 @@ __global__ void __launch_bounds__(BS_NT) k_shard_round(ShardView v, const uint4*
   const uint64_t units = ((uint64_t)v.rows + (32u >> ls) - 1) / (32u >> ls);
   const uint64_t nwarps = (uint64_t)gridDim.x * (BS_NT / 32);
   uint64_t cnt = 0;
+  unsigned long long moved = 0;
   for (uint64_t u = ((uint64_t)blockIdx.x * BS_NT + threadIdx.x) >> 5; u < units; u += nwarps) {
     const uint64_t x = u * (32u >> ls) + sub;
     const bool valid = x < v.rows;
@@ -791,10 +793,12 @@ __global__ void __launch_bounds__(BS_NT) k_shard_round(ShardView v, const uint4*
     const bool row_has = valid && (bal_y & smask) != 0u;
     bool row_any = false;
     if (valid) {
+      uint32_t active_edges = 0, acc_words = 0;
       for (uint32_t c = sl; c < W; c += lpr) {
         uint4 nw = make_uint4(0u, 0u, 0u, 0u);
         if (row_has) {
           uint4 acc = make_uint4(0u, 0u, 0u, 0u);
+          active_edges = 0;
           for (uint64_t e = e0; e < e1; e += 4) {
             uint32_t y[4];
             bool on[4];
@@ -811,9 +815,11 @@ __global__ void __launch_bounds__(BS_NT) k_shard_round(ShardView v, const uint4*
               acc.y |= d[q].y;
               acc.z |= d[q].z;
               acc.w |= d[q].w;
+              active_edges += on[q] ? 1u : 0u;
             }
           }
           if (any4(acc)) {
+            acc_words++;
             uint4* fp = v.F + x * W + c;
             uint4 f = *fp;
             nw = make_uint4(acc.x & ~f.x, acc.y & ~f.y, acc.z & ~f.z, acc.w & ~f.w);
@@ -826,12 +832,22 @@ __global__ void __launch_bounds__(BS_NT) k_shard_round(ShardView v, const uint4*
         }
         Dmine[x * W + c] = nw;  // rows without Δ' are cleared too
       }
+      if (v.bytes && row_has) {
+        // this lane's words: Δ rows read, Δ' written, path read (and written
+        // where bits are new); its share of the edge list and flags
+        const uint64_t lw = (W > sl) ? (W - sl + lpr - 1) / lpr : 0;
+        moved += lw * 16ull * (active_edges + 1) + acc_words * 32ull + (sl == 0 ? (e1 - e0) * 5ull : 0ull);
+      }
     }
     const unsigned bal = __ballot_sync(kFull, row_any);
     if (valid && sl == 0) fmine[x] = (bal & smask) != 0u ? 1 : 0;
   }
   cnt = warp_sum(cnt);
   if (lane == 0 && cnt) atomicAdd(v.delta, (unsigned long long)cnt);
+  if (v.bytes) {
+    moved = warp_sum(moved);
+    if (lane == 0 && moved) atomicAdd(v.bytes, moved);
+  }
 }
 
 // Local out-degrees of the rank's rows; endpoints outside [0, n) set *bad.
@@ -1066,17 +1082,22 @@ uint64_t tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const uint4* Dfull
   v.nbr = sh->nbr.p;
   v.F = sh->F.p;
   v.delta = sh->acc.p;
-  SK_CUDA(cudaMemsetAsync(sh->acc.p, 0, 8, ctx->stream));
+  v.bytes = ctx->profiling ? sh->acc.p + 1 : nullptr;
+  SK_CUDA(cudaMemsetAsync(sh->acc.p, 0, 16, ctx->stream));
   const uint64_t units = ceil_div((uint64_t)v.rows, 32u >> v.ls);
+  int kh = -1;
   if (units) {
     const unsigned g = (unsigned)std::min<uint64_t>(ceil_div(units, BS_NT / 32), (uint64_t)ctx->num_sms * 8);
+    kh = kprof_begin(ctx, K_SHARD_ROUND);
     k_shard_round<<<g, BS_NT, 0, ctx->stream>>>(v, Dfull, ffull, Dmine, fmine);
+    kprof_end(ctx, kh, 0);
     after_launch(ctx, "k_shard_round");
   }
-  uint64_t c;
-  read_u64(ctx, reinterpret_cast<const uint64_t*>(sh->acc.p), &c, 1);
+  uint64_t c[2];
+  read_u64(ctx, reinterpret_cast<const uint64_t*>(sh->acc.p), c, 2);
   sync_and_check(ctx);
-  return c;
+  if (kh >= 0) ctx->krecs[kh].bytes = c[1];
+  return c[0];
 }
 
 void tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count, uint64_t* fp) {

@@ -319,7 +319,8 @@ enum KernelId : int {
   K_BS_ROUND = 8,
   K_PROV_ROUND = 9,
   K_CIRCUIT = 10,
-  K_NUM = 11,
+  K_SHARD_ROUND = 11,
+  K_NUM = 12,
 };
 
 inline cudaEvent_t take_event(strata_ctx* ctx) {

@@ -34,7 +34,7 @@ KNOB_DENSE_WORD_MEMBERS = 8
 
 KERNELS = {0: "k_onesweep", 1: "k_expand_emit", 2: "k_expand_offsets", 3: "k_reduce_runs",
            4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count", 7: "k_expand_dense",
-           8: "k_bs_round", 9: "k_prov_round", 10: "k_circuit"}
+           8: "k_bs_round", 9: "k_prov_round", 10: "k_circuit", 11: "k_shard_round"}
 
 STATUS_NAMES = {
     OK: "OK", E_INVALID: "INVALID", E_OOM: "OOM", E_CUDA: "CUDA", E_OVERFLOW: "OVERFLOW",
