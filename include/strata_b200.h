@@ -290,6 +290,8 @@ strata_status strata_tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const 
 /* |path| of the rank's rows and their part of the fingerprint. */
 strata_status strata_tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count,
     uint64_t* fingerprint);
+/* Frees the share (its buffers return to the context's pool): call it before
+ * strata_ctx_destroy of the context that created it. */
 void strata_tc_shard_free(strata_tc_shard* sh);
 
 /* ---- Prov_k capture and provenance circuits -----------------------------
