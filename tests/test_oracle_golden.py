@@ -224,6 +224,35 @@ def test_routing_workload_pinned_lines():
 
 
 # ---------------------------------------------------------------- counts
+def test_stratified_negation_complement():
+    """reach(Y) :- edge(X,Y), reach(X).  unreach(X) :- node(X), not reach(X).
+    with nodes a, b, c, edge(a, b), reach(a): only c is unreachable and reach
+    saturates to {a, b} (strata-eval/tests/interp.rs:241-293; symbols
+    interned first-seen, so a, b, c = 0, 1, 2)."""
+    for semi in (True, False):
+        p = (O.Prog().pred("node", 1).pred("edge", 2).pred("reach", 1).pred("unreach", 1, stratum=1))
+        p.rule(("reach", ["Y"]), ("edge", ["X", "Y"]), ("reach", ["X"]))
+        p.rule(("unreach", ["X"]), ("node", ["X"]), ("not", "reach", ["X"]))
+        for v in (0, 1, 2):
+            p.fact("node", [v])
+        p.fact("edge", [0, 1]).fact("reach", [0])
+        db, _ = p.run(semi_naive=semi)
+        assert _pairs(db["unreach"]) == [(2,)]
+        assert len(db["reach"]) == 2
+
+
+def test_negation_against_same_stratum_is_rejected():
+    """p(X) :- q(X), not p(X) in one stratum is an error, naive and
+    semi-naive (strata-eval/tests/interp.rs:295-324)."""
+    for semi in (True, False):
+        p = O.Prog().pred("q", 1).pred("p", 1)
+        p.rule(("p", ["X"]), ("q", ["X"]), ("not", "p", ["X"]))
+        p.fact("q", [0])
+        with pytest.raises(O.OracleError) as e:
+            p.run(semi_naive=semi)
+        assert e.value.kind == "neg_not_stratified"
+
+
 def test_count_aggregate_outdegree():
     """outdeg(X, count<Y>) :- edge(X,Y) (interp.rs:327-362)."""
     p = O.Prog().pred("edge", 2).pred("outdeg", 2, stratum=1)
