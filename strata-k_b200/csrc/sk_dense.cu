@@ -6,25 +6,26 @@
 // for Trop (ABSENT = INT32_MAX, +inf = INT32_MAX-1).  One round then needs no
 // sort and no merge:
 //
-//   for every candidate (key, w) of Δ ⋈ E:              (load-balanced expand)
-//     Bool:  new = !atomicOr(bit(key))                  — dedup and Δ' = new∖full in one op
-//     Trop:  w < D[key] and w < atomicMin(D[key], w)    — ⊕ = min, strict improvement
-//     if new / improved: set mark(key)
-//   Δ' = the marked entries in index order, with their merged value from D
+//   for every candidate (entry, w) of Δ ⋈ E:            (load-balanced expand)
+//     Bool:  if entry absent from the value read:  set bit, set mark
+//     Trop:  if w < the value read:  atomicMin(D[entry], w), set mark
+//   Δ' = the marked entries; their merged weights are D at the round's end
 //
-// A key is marked exactly when some candidate is new (Bool) or strictly
-// below the value the key had when the round started (Trop): the
-// interpreter's `Relation::combine` change test (strata-eval/src/store.rs:34-48),
-// and Δ' carries the merged values (seminaive.rs:199-206), so rounds, Δ sets
-// and the round cap equal the sort-merge plan's.
+// An entry is marked exactly when it is new (Bool) or strictly below the
+// value it had when the round started (Trop): the interpreter's
+// `Relation::combine` change test (strata-eval/src/store.rs:34-48), and Δ'
+// carries the merged values (seminaive.rs:199-206), so rounds, Δ sets and
+// the round cap equal the sort-merge plan's.
 //
-// Layout.  The index is stored join-column-major: entry (c_j, c_other) at
-// c_j * n_other + c_other, where c_j is the column the NEXT round joins on
-// (c0 for TC's Δ(Y,Z), c1 for MSSP's Δ(S,Y)).  Δ' then comes out of the
-// marks compaction sorted by its join column, and the expand treats a run of
-// Δ tuples with the same join value as one group: each edge of that value is
-// read once for the whole group, and the group's probes of one edge all fall
-// in one index row (cache-resident).
+// Layout.  The index is stored as rows of the column the NEXT round joins on
+// (c0 for TC's Δ(Y,Z), c1 for MSSP's Δ(S,Y)), each row padded to a multiple
+// of 32 entries, so a 32-bit word of the marks holds Δ tuples of one join
+// value.  Δ stays in the marks: each round compacts the nonzero marks words
+// of rows with edges into word heads (dense_word_heads; the heads' weights
+// are copied to Dprev, which the expand reads while D changes), and the
+// expand reads each edge of a join value once for all members of a head,
+// whose probes of that edge fall in one index row (cache-resident).  Only
+// the bootstrap round expands a Δ given as keys (dense_heads).
 #include <type_traits>
 
 #include "sk_ops.cuh"
