@@ -366,8 +366,9 @@ __global__ void __launch_bounds__(NT, 6)
   if (flags) atomicOr(status, flags);
 }
 
-// Δ' of a round: the marked index entries in index order, with their merged
-// weight (Trop); the marks are cleared for the next round.  Reduce-then-scan:
+// The set bits of a bitmap over an index, as keys in index order (with their
+// weight from D for Trop); the bitmap is cleared.  The bit-row plan turns its
+// final path rows into the sorted relation with it.  Reduce-then-scan:
 // per-tile counts, one-block scan, then the write (no waiting between tiles).
 constexpr uint32_t MC_TILE = NT;  // bitmap words per tile (one per thread)
 
