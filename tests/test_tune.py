@@ -24,3 +24,18 @@ def test_corrupt_cache_is_ignored(tmp_path):
     p = tmp_path / "tune.json"
     p.write_text("{not json")
     assert tune.load(p, gpu="GPU A") == {}
+
+
+def test_load_keeps_every_swept_knob():
+    """Every knob the sweep times (radix tiles and ranking, triangle probe,
+    batch graph rounds and blocks, dense-word threshold) survives the cache
+    round trip; values outside a knob's choices are dropped."""
+    import tempfile
+    from pathlib import Path
+    best = {1: 15, 2: 9, 3: 2, 4: 4, 5: 2, 7: 1, 8: 24}
+    with tempfile.TemporaryDirectory() as d:
+        p = Path(d) / "tune.json"
+        tune.save({"gpu": "GPU A", "best": best}, p)
+        assert tune.load(p, gpu="GPU A") == best
+        p.write_text(json.dumps({"GPU A": {"8": 34, "4": 3}}))
+        assert tune.load(p, gpu="GPU A") == {}
