@@ -273,7 +273,9 @@ strata_status strata_tc_bool_batch(strata_ctx* ctx, uint32_t n_inst, const uint3
  * hash-partitioned by join key, the whole join the union of the shard
  * joins); here path is partitioned by row and Delta replicated by the gather.
  * d_src / d_dst (m edges, device) must stay valid until the seed returns;
- * endpoints outside [0, n_nodes): STRATA_E_INVALID. */
+ * endpoints outside [0, n_nodes): STRATA_E_INVALID.  The share is seeded
+ * exactly once: a second seed, or a round / summary before the seed, is
+ * STRATA_E_INVALID. */
 typedef struct strata_tc_shard strata_tc_shard;
 strata_status strata_tc_shard_create(strata_ctx* ctx, uint32_t n_nodes, const uint32_t* d_src,
     const uint32_t* d_dst, uint64_t m, uint32_t rank, uint32_t world, strata_tc_shard** out);
@@ -283,8 +285,9 @@ strata_status strata_tc_shard_shape(const strata_tc_shard* sh, uint32_t* rows_pe
  * row_bytes, 16-byte aligned) and P row flags; *n_delta = |Delta0| of its rows. */
 strata_status strata_tc_shard_seed(strata_ctx* ctx, strata_tc_shard* sh, void* d_delta_mine,
     uint8_t* d_flags_mine, uint64_t* n_delta);
-/* One semi-naive round of the rank's rows from the gathered Delta (which must
- * not overlap the outputs); *n_delta = |Delta'| of its rows. */
+/* One semi-naive round of the rank's rows from the gathered Delta and row
+ * flags (neither may overlap the rank's output slice of the same kind:
+ * STRATA_E_INVALID); *n_delta = |Delta'| of its rows. */
 strata_status strata_tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const void* d_delta_full,
     const uint8_t* d_flags_full, void* d_delta_mine, uint8_t* d_flags_mine, uint64_t* n_delta);
 /* |path| of the rank's rows and their part of the fingerprint. */
@@ -423,7 +426,8 @@ strata_status strata_op_merge(strata_ctx* ctx, int key_bytes,
  * embedders whose allocator owns the whole device, latency-critical loops
  * that must not enter the allocator): a stable ascending sort of u32 keys on
  * their low `key_bits` bits (0..32) from d_keys_in into d_keys_out (distinct
- * caller-owned device buffers; the input is left unchanged), run on `stream`
+ * caller-owned device buffers that must not overlap, else STRATA_E_INVALID;
+ * the input is left unchanged), run on `stream`
  * (a cudaStream_t; NULL = the legacy default stream) and finished before the
  * call returns.  It needs no context and calls no allocator: its temporaries
  * live in a fixed 4,483,200-byte array inside the library, which every GPU that

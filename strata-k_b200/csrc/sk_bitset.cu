@@ -1068,6 +1068,10 @@ uint64_t tc_shard_seed(strata_ctx* ctx, strata_tc_shard* sh, uint4* Dmine, uint8
   uint64_t c;
   read_u64(ctx, reinterpret_cast<const uint64_t*>(sh->acc.p), &c, 1);
   sync_and_check(ctx);
+  // The rounds read only nbr / F: drop the caller's columns, which need not
+  // outlive this call.
+  sh->src = sh->dst = nullptr;
+  sh->seeded = true;
   return c;  // |Δ0| of the rank's rows (distinct edges)
 }
 

@@ -525,6 +525,7 @@ strata_status strata_tc_shard_seed(strata_ctx* ctx, strata_tc_shard* sh, void* d
                                    uint64_t* n_delta) {
   if (!ctx || !sh || sh->ctx != ctx || !d_delta_mine || !d_flags_mine) return STRATA_E_INVALID;
   if (reinterpret_cast<uintptr_t>(d_delta_mine) % 16) return bad(ctx, "the Delta slice must be 16-byte aligned");
+  if (sh->seeded) return bad(ctx, "the share is already seeded (its edge columns were released)");
   if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
   SK_GUARD_BEGIN
   sk::reset_status(ctx);
@@ -544,6 +545,10 @@ strata_status strata_tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const 
   const auto f0 = reinterpret_cast<uintptr_t>(d_delta_full), m0 = reinterpret_cast<uintptr_t>(d_delta_mine);
   const uint64_t mine_bytes = (uint64_t)sh->per * sh->w4 * 16;
   if (m0 < f0 + full_bytes && f0 < m0 + mine_bytes) return bad(ctx, "the Delta slice overlaps the gathered Delta");
+  const auto g0 = reinterpret_cast<uintptr_t>(d_flags_full), h0 = reinterpret_cast<uintptr_t>(d_flags_mine);
+  const uint64_t gfull = (uint64_t)sh->world * sh->per, gmine = sh->per;
+  if (h0 < g0 + gfull && g0 < h0 + gmine) return bad(ctx, "the row flags slice overlaps the gathered row flags");
+  if (!sh->seeded) return bad(ctx, "round before seed: call strata_tc_shard_seed first");
   if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
   SK_GUARD_BEGIN
   sk::reset_status(ctx);
@@ -555,6 +560,7 @@ strata_status strata_tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const 
 
 strata_status strata_tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count, uint64_t* fingerprint) {
   if (!ctx || !sh || sh->ctx != ctx) return STRATA_E_INVALID;
+  if (!sh->seeded) return bad(ctx, "summary before seed: call strata_tc_shard_seed first");
   if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
   SK_GUARD_BEGIN
   sk::reset_status(ctx);

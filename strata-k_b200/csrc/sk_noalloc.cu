@@ -60,6 +60,12 @@ extern "C" strata_status strata_sort_u32_noalloc(const uint32_t* d_keys_in, uint
   if (n > kNoAllocMaxKeys) return STRATA_E_INVALID;  // beyond STRATA_NOALLOC_SORT_MAX_KEYS
   if (key_bits < 0 || key_bits > 32) return STRATA_E_INVALID;
   if (n && (!d_keys_in || !d_keys_out)) return STRATA_E_INVALID;
+  // The passes scatter into d_keys_out while other tiles still read their
+  // input: overlapping buffers would corrupt the keys without an error.
+  if (n) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(d_keys_in), b = reinterpret_cast<uintptr_t>(d_keys_out);
+    if (a < b + n * 4 && b < a + n * 4) return STRATA_E_INVALID;
+  }
   if (sk::radix_sort_u32_static_bytes(kNoAllocMaxKeys) > kScratchBytes) return STRATA_E_CUDA;
   if (n == 0) return STRATA_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);

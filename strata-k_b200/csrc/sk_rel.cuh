@@ -45,8 +45,11 @@ struct strata_tc_shard {
   strata_ctx* ctx = nullptr;
   uint32_t n = 0, rank = 0, world = 0, per = 0, lo = 0, hi = 0, w4 = 0;
   uint64_t n_edges = 0, m = 0;
-  const uint32_t* src = nullptr;  // the caller's edge columns (device)
+  // The caller's edge columns (device): valid only until the seed, which
+  // copies what the rounds need and clears these.
+  const uint32_t* src = nullptr;
   const uint32_t* dst = nullptr;
+  bool seeded = false;  // F, nbr and the Δ slice hold data only after the seed
   sk::DBuf<uint64_t> off;
   sk::DBuf<uint32_t> nbr;
   sk::DBuf<uint4> F;

@@ -1,8 +1,8 @@
 """Regenerate the golden fixtures of tests/golden/ from the reference tree.
 
-Run in a checkout that has the reference mounted (default /root/reference):
+Run with the root of a reference checkout as the one required argument:
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 
 Fixtures written (small, committed):
   routing.json — the routing workload's input rows (examples/workloads/routing/
@@ -74,4 +74,6 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT")
+    main(Path(sys.argv[1]))

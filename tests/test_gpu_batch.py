@@ -168,7 +168,19 @@ def test_sharded_closure_rejects_bad_input(engine):
         per, _, _, rb = sh.shape()
         full = torch.zeros(2 * per * rb // 4, dtype=torch.int32, device="cuda")
         flags = torch.zeros(2 * per, dtype=torch.uint8, device="cuda")
+        mine = torch.zeros(per * rb // 4, dtype=torch.int32, device="cuda")
+        fmine = torch.zeros(per, dtype=torch.uint8, device="cuda")
+        with pytest.raises(S.InvalidArgument):  # a round before the seed
+            sh.round(full, flags, mine, fmine)
+        with pytest.raises(S.InvalidArgument):  # a summary before the seed
+            sh.summary()
+        sh.seed(mine, fmine)
+        with pytest.raises(S.InvalidArgument):  # a second seed (its edge columns are gone)
+            sh.seed(mine, fmine)
         with pytest.raises(S.InvalidArgument):  # the slice inside the gathered Δ
-            sh.round(full, flags, full[: per * rb // 4], flags[:per])
+            sh.round(full, flags, full[: per * rb // 4], fmine)
+        with pytest.raises(S.InvalidArgument):  # the row flags inside the gathered flags
+            sh.round(full, flags, mine, flags[per:])
+        assert sh.round(full, flags, mine, fmine) == 0  # an empty gathered Δ derives nothing
     finally:
         sh.free()

@@ -62,12 +62,51 @@ def test_noalloc_sort_matches_allocating_sort_twice_in_a_row():
         eng.close()
 
 
-def test_noalloc_sort_rejects_oversized_input():
+def test_noalloc_sort_small_and_edge_cases():
+    import torch
+
+    import strata_b200 as S
+    from strata_b200 import _lib as L
+    lib = L.load()
+    eng = S.Engine(0)
+    try:
+        rng = np.random.default_rng(7)
+        # one key; key_bits 0 (a plain copy: the output equals the input);
+        # the full 32-bit range
+        for n, bits in ((1, 12), (1000, 0), (65_537, 32), (4097, 8)):
+            hi = 1 << max(bits, 1)
+            keys = rng.integers(0, hi, n, dtype=np.uint64).astype(np.uint32)
+            rc, got = _sort_noalloc(lib, torch, keys, bits)
+            assert rc == L.OK
+            want = keys.copy() if bits == 0 else np.sort(keys, kind="stable")
+            assert np.array_equal(got, want)
+            if bits:
+                assert np.array_equal(got, _sort_allocating(eng, torch, keys, bits))
+        # the legacy default stream (NULL), as the header allows
+        keys = rng.integers(0, 1 << 20, 50_000, dtype=np.uint64).astype(np.uint32)
+        src = torch.from_numpy(keys.view(np.int32)).cuda()
+        dst = torch.empty(len(keys), dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        assert lib.strata_sort_u32_noalloc(C.c_void_p(src.data_ptr()), C.c_void_p(dst.data_ptr()),
+                                           len(keys), 20, None) == L.OK
+        assert np.array_equal(dst.cpu().numpy().view(np.uint32), np.sort(keys))
+    finally:
+        eng.close()
+
+
+def test_noalloc_sort_rejects_oversized_or_overlapping_input():
     import torch
 
     from strata_b200 import _lib as L
     lib = L.load()
-    buf = torch.empty(16, dtype=torch.int32, device="cuda")
+    buf = torch.zeros(64, dtype=torch.int32, device="cuda")
     p = C.c_void_p(buf.data_ptr())
-    assert lib.strata_sort_u32_noalloc(p, p, MAX_KEYS + 1, 20, None) == L.E_INVALID
-    assert lib.strata_sort_u32_noalloc(p, p, 8, 33, None) == L.E_INVALID
+    assert lib.strata_sort_u32_noalloc(p, C.c_void_p(buf.data_ptr() + 128), MAX_KEYS + 1, 20, None) == L.E_INVALID
+    assert lib.strata_sort_u32_noalloc(p, C.c_void_p(buf.data_ptr() + 128), 8, 33, None) == L.E_INVALID
+    # in place, and partly overlapping ranges, are refused (17 bits = an odd
+    # pass count, the case that would scatter into the buffer being read)
+    assert lib.strata_sort_u32_noalloc(p, p, 16, 17, None) == L.E_INVALID
+    assert lib.strata_sort_u32_noalloc(p, C.c_void_p(buf.data_ptr() + 32), 16, 17, None) == L.E_INVALID
+    assert lib.strata_sort_u32_noalloc(C.c_void_p(buf.data_ptr() + 32), p, 16, 17, None) == L.E_INVALID
+    # adjacent, non-overlapping ranges are fine
+    assert lib.strata_sort_u32_noalloc(p, C.c_void_p(buf.data_ptr() + 64), 16, 17, None) == L.OK
