@@ -171,43 +171,90 @@ __global__ void __launch_bounds__(TC_NT)
   if (lane == 0 && count) atomicAdd(total, count);
 }
 
-// K4 on a degree-oriented DAG: one thread per oriented edge (u, v); for each
-// common successor w1 count |out(u) ∩ out(v) ∩ out(w1)| by a 3-way leapfrog.
-// The lists are sorted by id while the DAG follows (degree, id) rank, so the
-// leapfrog runs over the whole of out(u) and out(v): membership in out(w1)
-// already fixes rank(w2) > rank(w1), and each K4 is counted once.
-__global__ void k_k4_count(const uint32_t* __restrict__ eu, const uint32_t* __restrict__ ev, uint64_t m,
-                           const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
-                           unsigned long long* total) {
-  unsigned long long c = 0;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t u = eu[i], v = ev[i];
-    uint32_t a = off[u];
-    const uint32_t ae = off[u + 1];
-    uint32_t b = off[v];
-    const uint32_t be = off[v + 1];
-    while (a < ae && b < be) {
-      const uint32_t x = nbr[a], y = nbr[b];
-      if (x < y) { a++; continue; }
-      if (x > y) { b++; continue; }
-      const uint32_t w1 = x;
-      uint32_t p = off[u], q = off[v], r = off[w1];
-      const uint32_t re = off[w1 + 1];
-      while (p < ae && q < be && r < re) {
-        const uint32_t xp = nbr[p], xq = nbr[q], xr = nbr[r];
-        uint32_t mx = xp > xq ? xp : xq;
-        mx = xr > mx ? xr : mx;
-        if (xp < mx) p++;
-        else if (xq < mx) q++;
-        else if (xr < mx) r++;
-        else { c++; p++; q++; r++; }
+// K4 on a degree-oriented DAG, one warp per lowest-rank vertex u.  A 4-clique
+// a < b < c < d (rank order) is counted exactly once, at u = a, v = b, w = c,
+// z = d: the warp stages out(u) in shared memory, and for each v ∈ out(u)
+// builds the common-successor set C(u,v) = out(u) ∩ out(v) as a sorted list
+// in shared memory (the lanes stream out(v) with coalesced loads, probe the
+// staged out(u), and a ballot compacts the hits in order).  Then every
+// w ∈ C(u,v) expands its out-list with the same warp-cooperative expansion
+// as the triangle count (a warp scan over the 32 lanes' degrees, owner lane
+// found by a shuffle search) and each entry z is probed in C(u,v).
+//   count(u) = Σ_{v ∈ out(u)} Σ_{w ∈ C(u,v)} |out(w) ∩ C(u,v)|.
+// A launch handles the vertices whose out-degree lies in (d_lo, d_hi]; `cap`
+// (≥ d_hi, a multiple of 32) sizes the two per-warp lists in dynamic shared
+// memory: one launch with a small cap and 8 warps per block for the bulk of
+// the vertices, one with the largest out-degree as cap for the rest.
+__global__ void k_k4_warp(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr, uint64_t n_nodes,
+                          uint32_t d_lo, uint32_t d_hi, uint32_t cap, uint32_t* counter,
+                          unsigned long long* total) {
+  extern __shared__ __align__(16) uint32_t s_k4[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t* A = s_k4 + (size_t)warp * 2 * cap;  // out(u), staged
+  uint32_t* CL = A + cap;                       // C(u, v), sorted
+  unsigned long long count = 0;
+  while (true) {
+    uint32_t u = 0;
+    if (lane == 0) u = atomicAdd(counter, 1u);
+    u = __shfl_sync(kFull, u, 0);
+    if (u >= n_nodes) break;
+    const uint32_t a0 = off[u], du = off[u + 1] - a0;
+    if (du <= d_lo || du > d_hi || du < 3) continue;
+    for (uint32_t k = lane; k < du; k += 32) A[k] = nbr[a0 + k];
+    __syncwarp();
+    for (uint32_t i = 0; i + 2 < du; i++) {  // v = A[i]; two more members are needed after it
+      const uint32_t v = A[i];
+      if (v >= n_nodes) continue;
+      const uint32_t v0 = off[v], dv = off[v + 1] - v0;
+      uint32_t nc = 0;
+      for (uint32_t c = 0; c < dv; c += 32) {
+        const bool valid = c + lane < dv;
+        const uint32_t z = valid ? nbr[v0 + c + lane] : 0u;
+        const bool hit = valid && bsearch_u32(A, du, z);
+        const unsigned bal = __ballot_sync(kFull, hit);
+        const uint32_t pos = nc + __popc(bal & lanemask_lt());
+        if (hit && pos < cap) CL[pos] = z;  // distinct successors: nc <= du <= cap
+        nc += __popc(bal);
       }
-      a++;
-      b++;
+      __syncwarp();
+      nc = min(nc, cap);
+      if (nc < 2) continue;
+      for (uint32_t c = 0; c < nc; c += 32) {
+        const bool valid = c + lane < nc;
+        const uint32_t w = valid ? CL[c + lane] : 0u;
+        const bool inr = valid && w < n_nodes;
+        const uint32_t sw = inr ? off[w] : 0u;
+        const uint32_t dw = inr ? off[w + 1] - sw : 0u;
+        const uint32_t incl = warp_incl_sum(dw);
+        const uint32_t ex = incl - dw;
+        const uint32_t D = __shfl_sync(kFull, incl, 31);
+        for (uint32_t base = 0; base < D; base += 32) {
+          const uint32_t j = base + lane;
+          int t = 0;
+#pragma unroll
+          for (int st = 16; st > 0; st >>= 1) {
+            const uint32_t val = __shfl_sync(kFull, incl, t + st - 1);
+            if (val <= j) t += st;
+          }
+          const uint32_t ex_t = __shfl_sync(kFull, ex, t);
+          const uint32_t sw_t = __shfl_sync(kFull, sw, t);
+          if (j < D && bsearch_u32(CL, nc, nbr[sw_t + (j - ex_t)])) count++;
+        }
+      }
+      __syncwarp();
     }
+    __syncwarp();
   }
-  c = warp_sum(c);
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(total, c);
+  count = warp_sum(count);
+  if (lane == 0 && count) atomicAdd(total, count);
+}
+
+__global__ void k_max_outdeg(const uint32_t* __restrict__ off, uint64_t n_nodes, unsigned int* out) {
+  unsigned int m = 0;
+  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < n_nodes; u += (uint64_t)gridDim.x * blockDim.x)
+    m = max(m, off[u + 1] - off[u]);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(kFull, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
 // Canonical undirected edge key (min << b) | max; self-loops become the key
@@ -244,16 +291,6 @@ __global__ void k_orient(K* __restrict__ keys, uint64_t m, int bits, const uint3
   const uint32_t dx = deg[(uint64_t)x], dy = deg[(uint64_t)y];
   const bool x_first = dx < dy || (dx == dy && x < y);
   keys[i] = x_first ? (K)((x << bits) | y) : (K)((y << bits) | x);
-}
-
-template <class K>
-__global__ void k_split(const K* __restrict__ keys, uint64_t m, int bits, uint32_t* __restrict__ eu,
-                        uint32_t* __restrict__ ev) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  const K k = keys[i];
-  eu[i] = (uint32_t)(k >> bits);
-  ev[i] = (uint32_t)(k & (K)((K(1) << bits) - 1));
 }
 
 __global__ void k_sum_sq_deg(const uint32_t* __restrict__ off, uint64_t n_nodes, unsigned long long* out) {
@@ -426,16 +463,38 @@ uint64_t k4_impl(strata_ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t
   ori.ctx = ctx;
   const uint64_t m = oriented_edges<K>(ctx, a, b, n, bits, n_nodes, true, ori);
   if (m == 0) return 0;
-  DBuf<uint32_t> off(ctx, n_nodes + 1), nbr(ctx, m + 1), eu(ctx, m + 1), ev(ctx, m + 1);
+  DBuf<uint32_t> off(ctx, n_nodes + 1), nbr(ctx, m + 1);
   build_csr<K>(ctx, ori.p, m, bits, n_nodes, off.p, nbr.p);
-  k_split<K><<<blocks(m), 256, 0, ctx->stream>>>(ori.p, m, bits, eu.p, ev.p);
-  after_launch(ctx, "k_split");
-  DBuf<uint64_t> acc(ctx, 1);
-  SK_CUDA(cudaMemsetAsync(acc.p, 0, 8, ctx->stream));
-  const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(m, 256), (uint64_t)ctx->num_sms * 8);
-  k_k4_count<<<grid ? grid : 1, 256, 0, ctx->stream>>>(eu.p, ev.p, m, off.p, nbr.p,
+  DBuf<uint64_t> acc(ctx, 3);  // count, two vertex counters, largest out-degree
+  SK_CUDA(cudaMemsetAsync(acc.p, 0, 24, ctx->stream));
+  unsigned int* maxdeg = reinterpret_cast<unsigned int*>(acc.p + 2);
+  k_max_outdeg<<<(unsigned)std::min<uint64_t>(blocks(n_nodes), (uint64_t)ctx->num_sms * 8), 256, 0, ctx->stream>>>(
+      off.p, n_nodes, maxdeg);
+  after_launch(ctx, "k_max_outdeg");
+  uint64_t md;
+  read_u64(ctx, acc.p + 2, &md, 1);
+  md &= 0xffffffffull;
+  // Shared memory of one warp: two lists of `cap` ids.
+  constexpr uint32_t kSmallCap = 512;
+  constexpr size_t kSmemLimit = 200 * 1024;
+  const uint32_t big_cap = (uint32_t)ceil_div(std::max<uint64_t>(md, 1), 32) * 32;
+  if ((size_t)big_cap * 8 > kSmemLimit)
+    fail(STRATA_E_UNSUPPORTED, "4-clique count: an oriented out-degree above 25,600 does not fit shared memory");
+  const uint64_t grid_cap = (uint64_t)ctx->num_sms * 8;
+  auto launch = [&](uint32_t d_lo, uint32_t d_hi, uint32_t cap, int warps, uint32_t* counter) {
+    const size_t smem = (size_t)warps * 2 * cap * 4;
+    SK_CUDA(cudaFuncSetAttribute(k_k4_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(n_nodes, warps), grid_cap));
+    k_k4_warp<<<grid, warps * 32, smem, ctx->stream>>>(off.p, nbr.p, n_nodes, d_lo, d_hi, cap, counter,
                                                        reinterpret_cast<unsigned long long*>(acc.p));
-  after_launch(ctx, "k_k4_count");
+    after_launch(ctx, "k_k4_warp");
+  };
+  uint32_t* counters = reinterpret_cast<uint32_t*>(acc.p + 1);
+  launch(0, kSmallCap, kSmallCap, 8, counters);
+  if (md > kSmallCap) {
+    const int warps = (int)std::max<size_t>(1, std::min<size_t>(8, kSmemLimit / ((size_t)big_cap * 8)));
+    launch(kSmallCap, (uint32_t)md, big_cap, warps, counters + 1);
+  }
   SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, acc.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
   return ctx->h_scalar[0];

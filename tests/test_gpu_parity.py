@@ -343,6 +343,16 @@ def test_4cliques(engine, lcg):
     for n in (4, 10, 20, 40):
         e = [(a, b) for a in range(n) for b in range(a + 1, n)]
         assert engine.count_4cliques(e) == n * (n - 1) * (n - 2) * (n - 3) // 24
+    # a wide vertex (oriented out-degree above the small launch's 512-entry
+    # lists) goes through the second launch: K_600 has C(600, 4) 4-cliques
+    n = 600
+    e = np.stack(np.triu_indices(n, 1), 1)
+    assert engine.count_4cliques(e) == n * (n - 1) * (n - 2) * (n - 3) // 24
+    # K_40 planted in a random sparse graph, checked by brute force
+    rng0 = np.random.default_rng(44)
+    sp = rng0.integers(0, 300, (1500, 2))
+    e = np.concatenate([np.stack(np.triu_indices(40, 1), 1) * 7, sp])
+    assert engine.count_4cliques(e) == O.brute_4cliques(e[:, 0], e[:, 1], 300)
     rng = lcg(0x4C19999)
     for trial in range(100):
         n = 6 + rng.upto(18)
