@@ -74,6 +74,10 @@ def lib() -> C.CDLL:
         L.sko_dijkstra_mssp.restype = C.c_int
         L.sko_dijkstra_mssp.argtypes = [u32p, i64p, C.c_size_t, u32p, u32p, i64p, C.c_size_t,
                                         C.c_int, u64p, u64p]
+        L.sko_dijkstra_mssp_rows.restype = C.c_int
+        L.sko_dijkstra_mssp_rows.argtypes = [u32p, i64p, C.c_size_t, u32p, u32p, i64p, C.c_size_t, C.c_int,
+                                             C.POINTER(u32p), C.POINTER(u32p), C.POINTER(i64p),
+                                             C.POINTER(C.c_size_t)]
         L.sko_count_pattern.restype = C.c_uint64
         L.sko_count_pattern.argtypes = [u32p, u32p, C.c_size_t, C.c_int]
         L.sko_brute_triangles.restype = C.c_uint64
@@ -623,6 +627,26 @@ def dijkstra_mssp(sources, src, dst, w, source_w=None, threads=8):
     if rc:
         raise ValueError("Dijkstra oracle needs non-negative weights")
     return int(c.value), int(f.value)
+
+
+def dijkstra_mssp_rows(sources, src, dst, w, source_w=None, threads=8):
+    """(S, Z, dist) for every finite distance, sorted by (S, Z): numpy
+    columns uint32, uint32, int64 (Dijkstra per source, `threads` threads)."""
+    L = lib()
+    srcs = _col(sources, np.uint32)
+    sw = _col(np.zeros(len(srcs)) if source_w is None else source_w, np.int64)
+    s, d, ww = _col(src, np.uint32), _col(dst, np.uint32), _col(w, np.int64)
+    ps, pd, pw, n = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)(), C.POINTER(C.c_int64)(), C.c_size_t()
+    rc = L.sko_dijkstra_mssp_rows(_p(srcs, C.c_uint32), _p(sw, C.c_int64), len(srcs), _p(s, C.c_uint32),
+                                  _p(d, C.c_uint32), _p(ww, C.c_int64), len(s), threads, C.byref(ps), C.byref(pd),
+                                  C.byref(pw), C.byref(n))
+    if rc:
+        raise ValueError("Dijkstra oracle needs non-negative weights")
+    k = n.value
+    cols = [np.ctypeslib.as_array(p, shape=(max(k, 1),))[:k].copy() for p in (ps, pd, pw)]
+    for p in (ps, pd, pw):
+        L.sko_free(C.cast(p, C.c_void_p))
+    return cols[0], cols[1], cols[2]
 
 
 def count_pattern(x, y, threads=8) -> int:

@@ -1579,6 +1579,93 @@ int sko_dijkstra_mssp(const uint32_t* sources, const int64_t* sw, size_t ns, con
   return 0;
 }
 
+// The same shortest paths as rows: every (S, Z, dist) with a finite distance,
+// sorted by (S, Z), in malloc'd arrays (free with sko_free).  Independent of
+// the interpreter (layer C); with non-negative weights the semi-naive
+// fixpoint's minima are exactly these distances.
+int sko_dijkstra_mssp_rows(const uint32_t* sources, const int64_t* sw, size_t ns, const uint32_t* src,
+                           const uint32_t* dst, const int64_t* w, size_t n, int threads, uint32_t** out_s,
+                           uint32_t** out_d, int64_t** out_w, size_t* out_n) {
+  uint32_t maxid = 0;
+  for (size_t i = 0; i < n; i++) {
+    maxid = std::max(maxid, std::max(src[i], dst[i]));
+    if (w[i] < 0) return 1;
+  }
+  const size_t N = (size_t)maxid + 1;
+  std::vector<uint32_t> off(N + 1, 0), adj(n);
+  std::vector<int64_t> aw(n);
+  for (size_t i = 0; i < n; i++) off[src[i] + 1]++;
+  for (size_t v = 0; v < N; v++) off[v + 1] += off[v];
+  std::vector<uint32_t> fill(off.begin(), off.end() - 1);
+  for (size_t i = 0; i < n; i++) {
+    const uint32_t p = fill[src[i]]++;
+    adj[p] = dst[i];
+    aw[p] = w[i];
+  }
+  std::map<uint32_t, int64_t> seeds;
+  for (size_t i = 0; i < ns; i++) {
+    const int64_t x = sw ? sw[i] : 0;
+    auto it = seeds.find(sources[i]);
+    if (it == seeds.end() || x < it->second) seeds[sources[i]] = x;
+  }
+  std::vector<std::pair<uint32_t, int64_t>> sv(seeds.begin(), seeds.end());
+  std::vector<std::vector<std::pair<uint32_t, int64_t>>> res(sv.size());
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    std::vector<int64_t> dist(N, INT64_MAX);
+    std::vector<uint32_t> touched;
+    using QE = std::pair<int64_t, uint32_t>;
+    while (true) {
+      const size_t qi = next.fetch_add(1);
+      if (qi >= sv.size()) break;
+      const uint32_t s0 = sv[qi].first;
+      std::priority_queue<QE, std::vector<QE>, std::greater<QE>> pq;
+      auto relax = [&](uint32_t u, int64_t d) {
+        for (uint32_t k = off[u]; k < off[u + 1]; k++) {
+          const int64_t nd = d + aw[k];
+          if (nd < dist[adj[k]]) {
+            if (dist[adj[k]] == INT64_MAX) touched.push_back(adj[k]);
+            dist[adj[k]] = nd;
+            pq.emplace(nd, adj[k]);
+          }
+        }
+      };
+      if (s0 < N) relax(s0, sv[qi].second);
+      while (!pq.empty()) {
+        auto [d, u] = pq.top();
+        pq.pop();
+        if (d == dist[u]) relax(u, d);
+      }
+      std::sort(touched.begin(), touched.end());
+      auto& r = res[qi];
+      r.reserve(touched.size());
+      for (uint32_t v : touched) {
+        r.emplace_back(v, dist[v]);
+        dist[v] = INT64_MAX;
+      }
+      touched.clear();
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 0; t < std::max(1, threads); t++) th.emplace_back(work);
+  for (auto& t : th) t.join();
+  size_t total = 0;
+  for (auto& r : res) total += r.size();
+  *out_s = (uint32_t*)std::malloc(std::max<size_t>(1, total) * 4);
+  *out_d = (uint32_t*)std::malloc(std::max<size_t>(1, total) * 4);
+  *out_w = (int64_t*)std::malloc(std::max<size_t>(1, total) * 8);
+  size_t k = 0;
+  for (size_t qi = 0; qi < sv.size(); qi++)
+    for (auto& [v, d] : res[qi]) {
+      (*out_s)[k] = sv[qi].first;
+      (*out_d)[k] = v;
+      (*out_w)[k] = d;
+      k++;
+    }
+  *out_n = total;
+  return 0;
+}
+
 // Count aggregate  n(count<X>) :- e(X,Y), e(Y,Z), e(X,Z)  over the set e:
 // the number of bindings, by sorted-list intersection per edge (threads).
 uint64_t sko_count_pattern(const uint32_t* x, const uint32_t* y, size_t n, int threads) {

@@ -202,6 +202,8 @@ def test_mssp_shape_interp_matches_fast_and_dijkstra():
         assert r1 == r2
         c, fp = O.dijkstra_mssp(srcs, s, d, w)
         assert c == len(fs) and fp == O.fingerprint(fs, fd, fw, fi), trial
+        rs, rd, rw = O.dijkstra_mssp_rows(srcs, s, d, w)
+        assert np.array_equal(rs, fs) and np.array_equal(rd, fd) and np.array_equal(rw, fw), trial
 
 
 def test_routing_workload_pinned_lines():
