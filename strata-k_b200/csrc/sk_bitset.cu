@@ -1010,7 +1010,7 @@ uint64_t tc_bool_bitset(strata_ctx* ctx, const uint32_t* d_src, const uint32_t* 
   const DenseLayout lay = dense_layout(b1, n_src, w4 * 128, false);
   out.reserve(n + 1);
   DBuf<uint64_t> states(ctx, dense_marks_states(lay.entries));
-  const uint64_t got = dense_marks_compact<K, false>(ctx, reinterpret_cast<uint32_t*>(B.F.p), lay, nullptr, out.p,
+  const uint64_t got = dense_marks_compact<K, false, int32_t>(ctx, reinterpret_cast<uint32_t*>(B.F.p), lay, nullptr, out.p,
                                                      nullptr, n + 1, states.p);
   if (got != n) fail(STRATA_E_CUDA, "bit-row compaction count disagrees with the summed Δ sizes");
   return n;

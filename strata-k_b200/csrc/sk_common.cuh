@@ -26,7 +26,7 @@ namespace sk {
 // ---- device status bits -----------------------------------------------------
 enum : uint32_t {
   ST_OVERFLOW = 1u,          // finite Trop (x) overflowed int64
-  ST_SENTINEL = 2u,          // a finite sum landed on the +inf encoding
+  ST_SENTINEL = 2u,          // a finite input weight has no code in the fixpoint's weight lanes
   ST_LOOKBACK_TIMEOUT = 4u,  // decoupled look-back wait hit its iteration cap
   ST_BOUNDS = 8u,            // an index failed a bounds check and was skipped
   ST_PROOF_LEN = 16u,        // a provenance proof exceeded its literal capacity
@@ -86,6 +86,7 @@ struct strata_ctx {
   int tune_bs_blocks = 0;           // resident round-kernel blocks per SM (0 = occupancy limit)
   uint64_t tune_bs_budget_mb = 0;   // cap on a batch wave's device bytes, MiB (0 = 70% of free)
   int tune_dense_members = 0;       // members from which a Δ word takes the bit-lane expand (0 = 24)
+  int64_t wshift = 0;               // weight code shift of the running fixpoint (value = code + wshift)
   bool profiling = false;
   uint64_t launches = 0;
   // Per-kernel CUDA-event accounting (enabled with profiling).
@@ -280,7 +281,8 @@ inline void sync_and_check(strata_ctx* ctx) {
   if (s & ST_OVERFLOW) fail(STRATA_E_OVERFLOW, "tropical weight overflow: a finite sum exceeds i64");
   if (s & ST_SENTINEL)
     fail(STRATA_E_WEIGHT_RANGE,
-         "a finite tropical weight equal to i64::MAX cannot be told from +inf on the device");
+         "finite tropical weights span nearly all of i64 (sums within the round cap can reach both "
+         "i64::MIN and i64::MAX): no 64-bit code keeps them apart from +inf");
 }
 
 // Read `count` u64 values from device memory (synchronizing).

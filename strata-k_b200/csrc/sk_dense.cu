@@ -111,17 +111,23 @@ constexpr uint32_t kWarps = NT / 32;
 // sparser ones are flattened.  Tunable (STRATA_KNOB_DENSE_WORD_MEMBERS).
 constexpr int kDenseMembers = 24;
 
-template <class K, bool TROP, bool WORDS, class IX>
+// 64-bit atomic minimum for the wide lanes.
+__device__ __forceinline__ void atomic_min_w(int32_t* p, int32_t v) { atomicMin(p, v); }
+__device__ __forceinline__ void atomic_min_w(int64_t* p, int64_t v) {
+  atomicMin(reinterpret_cast<long long*>(p), (long long)v);
+}
+
+template <class K, bool TROP, bool WORDS, class IX, class W>
 __global__ void __launch_bounds__(NT, 6)
-    k_expand_dense(const K* __restrict__ dkeys, const int32_t* __restrict__ dw, uint64_t n_rows,
+    k_expand_dense(const K* __restrict__ dkeys, const W* __restrict__ dw, uint64_t n_rows,
                    const uint32_t* __restrict__ hidx, const uint64_t* __restrict__ pos,
                    const uint32_t* __restrict__ hseg, const typename std::conditional<WORDS, uint32_t, uint8_t>::type* __restrict__ hg,
                    uint64_t n, uint64_t total, const uint64_t* __restrict__ splits, int pshift, uint64_t pmask,
                    uint64_t ck, uint64_t cv, uint32_t wpr, int wpr_shift, int dense_members,
                    const uint32_t* __restrict__ nbr,
                    uint64_t n_nbr,
-                   const int32_t* __restrict__ nbr_w, uint64_t entries, uint32_t* bits, int32_t* D, uint32_t* marks,
-                   uint32_t* status) {
+                   const W* __restrict__ nbr_w, uint64_t entries, uint32_t* bits, W* D, uint32_t* marks,
+                   int64_t wshift, uint32_t* status) {
   using GT = typename std::conditional<WORDS, uint32_t, uint8_t>::type;
   // IX: the index type of entries (32-bit when the index has < 2^32 entries)
   const IX ckx = (IX)ck;
@@ -193,7 +199,7 @@ __global__ void __launch_bounds__(NT, 6)
   for (uint64_t c = o0 + (uint64_t)warp * 32; c < o_end; c += NT) {
     const uint64_t o = c + lane;
     uint32_t mm = 0, v = 0;
-    int32_t ew = 0;
+    W ew = 0;
     uint64_t h = 0, kb = 0;
     if (o < o_end) {
       const uint32_t li = s_owner[o - o0];
@@ -234,9 +240,9 @@ __global__ void __launch_bounds__(NT, 6)
       unsigned dm = __ballot_sync(kFull, __popc(md) >= dense_members);
       if ((dm >> lane) & 1u) mm = 0;  // the flattened pass below takes the rest
       while (dm) {
-        // outputs in flight: four with 32-bit indices, two with 64-bit
-        // ones (more would spill under the 40-register bound)
-        constexpr int U = sizeof(IX) == 4 ? 4 : 2;
+        // outputs in flight: four with 32-bit indices and weights, two
+        // otherwise (more would spill under the 40-register bound)
+        constexpr int U = (sizeof(IX) == 4 && sizeof(W) == 4) ? 4 : 2;
         int t[U];
         bool live[U];
         t[0] = __ffs(dm) - 1;
@@ -250,12 +256,12 @@ __global__ void __launch_bounds__(NT, 6)
         }
         bool act[U];
         IX ixd[U];
-        int32_t cwd[U], curd[U];
+        W cwd[U], curd[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
           const uint32_t m_t = __shfl_sync(kFull, md, t[u]);
           const IX kb_t = __shfl_sync(kFull, (IX)kb, t[u]);
-          const int32_t ew_t = TROP ? __shfl_sync(kFull, ew, t[u]) : 0;
+          const W ew_t = TROP ? __shfl_sync(kFull, ew, t[u]) : W(0);
           const uint32_t w_t = TROP ? __shfl_sync(kFull, (uint32_t)h, t[u]) : 0u;
           act[u] = ((m_t >> lane) & 1u) && live[u];
           ixd[u] = kb_t + (IX)lane * ckx;
@@ -264,9 +270,9 @@ __global__ void __launch_bounds__(NT, 6)
             if (act[u]) cwd[u] = dw[(IX)w_t * 32 + (IX)lane];
           if (act[u]) {
             if constexpr (TROP) curd[u] = D[ixd[u]];
-            else curd[u] = (int32_t)bits[ixd[u] >> 5];
+            else curd[u] = (W)bits[ixd[u] >> 5];
           }
-          if constexpr (TROP) cwd[u] = trop_mul(cwd[u], ew_t, &flags);
+          if constexpr (TROP) cwd[u] = trop_mul(cwd[u], ew_t, wshift, &flags);
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(NT, 6)
           const uint32_t bit = 1u << (ixd[u] & 31);
           if constexpr (TROP) {
             if (cwd[u] < curd[u]) {
-              atomicMin(&D[ixd[u]], cwd[u]);
+              atomic_min_w(&D[ixd[u]], cwd[u]);
               atomicOr(&marks[ixd[u] >> 5], bit);
             }
           } else {
@@ -298,7 +304,7 @@ __global__ void __launch_bounds__(NT, 6)
     // the member (row offset or bit) of t's head; the edge is v_t.
     for (uint32_t b0 = 0; b0 < T; b0 += 64) {
       IX ix[2];
-      int32_t cw[2], cur[2];
+      W cw[2], cur[2];
       bool ok[2];
 #pragma unroll
       for (int u = 0; u < 2; u++) {
@@ -307,7 +313,7 @@ __global__ void __launch_bounds__(NT, 6)
         const uint32_t sl = ok[u] ? my_slots[j] : 0u;
         const int t = (int)(sl >> 5);
         const uint32_t r = sl & 31u;
-        const int32_t ew_t = TROP ? __shfl_sync(kFull, ew, t) : 0;
+        const W ew_t = TROP ? __shfl_sync(kFull, ew, t) : W(0);
         ix[u] = 0;
         cw[u] = 0;
         if constexpr (WORDS) {
@@ -315,7 +321,7 @@ __global__ void __launch_bounds__(NT, 6)
           const uint32_t w_t = TROP ? __shfl_sync(kFull, (uint32_t)h, t) : 0u;
           if (ok[u]) {
             ix[u] = kb_t + (IX)r * ckx;  // inside the index: checked per output
-            if constexpr (TROP) cw[u] = trop_mul(dw[(IX)w_t * 32 + (IX)r], ew_t, &flags);
+            if constexpr (TROP) cw[u] = trop_mul(dw[(IX)w_t * 32 + (IX)r], ew_t, wshift, &flags);
           }
         } else {
           const uint64_t h_t = __shfl_sync(kFull, h, t);
@@ -332,7 +338,7 @@ __global__ void __launch_bounds__(NT, 6)
               flags |= ST_BOUNDS;
               ok[u] = false;
             } else if constexpr (TROP) {
-              cw[u] = trop_mul(dw[m], ew_t, &flags);
+              cw[u] = trop_mul(dw[m], ew_t, wshift, &flags);
             }
           }
         }
@@ -341,7 +347,7 @@ __global__ void __launch_bounds__(NT, 6)
       for (int u = 0; u < 2; u++) {
         if (ok[u]) {
           if constexpr (TROP) cur[u] = D[ix[u]];
-          else cur[u] = (int32_t)bits[ix[u] >> 5];
+          else cur[u] = (W)bits[ix[u] >> 5];
         }
       }
 #pragma unroll
@@ -350,7 +356,7 @@ __global__ void __launch_bounds__(NT, 6)
         const uint32_t bit = 1u << (ix[u] & 31);
         if constexpr (TROP) {
           if (cw[u] < cur[u]) {
-            atomicMin(&D[ix[u]], cw[u]);
+            atomic_min_w(&D[ix[u]], cw[u]);
             atomicOr(&marks[ix[u] >> 5], bit);  // changed this round
           }
         } else {
@@ -390,10 +396,10 @@ __global__ void __launch_bounds__(NT) k_marks_count(const uint32_t* __restrict__
 
 // Each warp enumerates the set bits of its 32 words in index order, 32 at a
 // time across the lanes, so the key stores and the weight gathers coalesce.
-template <class K, bool TROP>
+template <class K, bool TROP, class W>
 __global__ void __launch_bounds__(NT)
-    k_marks_write(uint32_t* marks, uint64_t words, DenseLayout lay, const int32_t* __restrict__ D,
-                  K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap,
+    k_marks_write(uint32_t* marks, uint64_t words, DenseLayout lay, const W* __restrict__ D,
+                  K* __restrict__ out, W* __restrict__ out_w, uint64_t out_cap,
                   const uint64_t* __restrict__ tile_sums, uint32_t* status) {
   __shared__ uint32_t s_scan[NT / 32 + 1];
   const int tid = threadIdx.x, lane = tid & 31;
@@ -446,9 +452,9 @@ __global__ void __launch_bounds__(NT)
 }
 
 // Seed the index from keys (and weights).
-template <class K, bool TROP>
-__global__ void k_dense_seed(const K* __restrict__ keys, const int32_t* __restrict__ w, uint64_t n,
-                             DenseLayout lay, uint32_t* bits, int32_t* D, uint32_t* marks, uint32_t* status) {
+template <class K, bool TROP, class W>
+__global__ void k_dense_seed(const K* __restrict__ keys, const W* __restrict__ w, uint64_t n,
+                             DenseLayout lay, uint32_t* bits, W* D, uint32_t* marks, uint32_t* status) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint64_t c0 = (uint64_t)keys[i] >> lay.b1, c1 = (uint64_t)keys[i] & lay.mask1;
@@ -459,7 +465,8 @@ __global__ void k_dense_seed(const K* __restrict__ keys, const int32_t* __restri
   if (marks) atomicOr(&marks[ix >> 5], 1u << (ix & 31));
 }
 
-__global__ void k_fill_i32(int32_t* p, uint64_t n, int32_t v) {
+template <class W>
+__global__ void k_fill_w(W* p, uint64_t n, W v) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     p[i] = v;
 }
@@ -469,10 +476,10 @@ __global__ void k_fill_i32(int32_t* p, uint64_t n, int32_t v) {
 constexpr int DC_ITEMS = 8;
 constexpr uint32_t DC_TILE = NT * DC_ITEMS;
 
-template <class K, bool TROP>
+template <class K, bool TROP, class W>
 __global__ void __launch_bounds__(NT)
-    k_dense_compact(const uint32_t* __restrict__ bits, const int32_t* __restrict__ D, DenseLayout lay,
-                    K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap, uint64_t* states,
+    k_dense_compact(const uint32_t* __restrict__ bits, const W* __restrict__ D, DenseLayout lay,
+                    K* __restrict__ out, W* __restrict__ out_w, uint64_t out_cap, uint64_t* states,
                     uint32_t* counter, uint64_t* d_count, uint32_t* status) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_scan[NT / 32 + 1];
@@ -481,7 +488,7 @@ __global__ void __launch_bounds__(NT)
   const uint32_t tile = claim_tile(counter, &s_tile);
   const uint64_t b = (uint64_t)tile * DC_TILE + (uint64_t)tid * DC_ITEMS;
   uint32_t present = 0;
-  int32_t wv[DC_ITEMS];
+  W wv[DC_ITEMS];
   // (c0, c1) of ordinal b, then stepped: one division per thread.
   const uint64_t logical = lay.n0 * lay.n1;
   uint64_t q0 = b / lay.n1, q1 = b - q0 * lay.n1;
@@ -500,7 +507,7 @@ __global__ void __launch_bounds__(NT)
       const uint64_t ix = lay.colmajor ? q1 * lay.width + q0 : q0 * lay.width + q1;
       if constexpr (TROP) {
         wv[j] = D[ix];
-        p = wv[j] != INT32_MAX;
+        p = wv[j] != WAbs<W>::v;
       } else {
         p = (bits[ix >> 5] >> (ix & 31)) & 1u;
       }
@@ -551,15 +558,15 @@ __global__ void __launch_bounds__(NT)
 constexpr int CM_ITEMS = 8;
 constexpr uint32_t CM_CHUNK = NT * CM_ITEMS;  // masks per scan block
 
-template <bool TROP>
-__device__ __forceinline__ bool cm_present(const uint32_t* bits, const int32_t* D, uint64_t ix) {
-  if constexpr (TROP) return D[ix] != INT32_MAX;
+template <bool TROP, class W>
+__device__ __forceinline__ bool cm_present(const uint32_t* bits, const W* D, uint64_t ix) {
+  if constexpr (TROP) return D[ix] != WAbs<W>::v;
   else return (bits[ix >> 5] >> (ix & 31)) & 1u;
 }
 
-template <bool TROP>
+template <bool TROP, class W>
 __global__ void __launch_bounds__(NT)
-    k_cm_masks(const uint32_t* __restrict__ bits, const int32_t* __restrict__ D, DenseLayout lay, uint64_t T,
+    k_cm_masks(const uint32_t* __restrict__ bits, const W* __restrict__ D, DenseLayout lay, uint64_t T,
                uint64_t subtiles, uint32_t* __restrict__ masks) {
   const uint64_t g = ((uint64_t)blockIdx.x * NT + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -569,7 +576,7 @@ __global__ void __launch_bounds__(NT)
 #pragma unroll 8
   for (int r = 0; r < 32; r++) {
     const uint64_t row = t * 32 + r;
-    if (row < lay.rows && cm_present<TROP>(bits, D, row * lay.width + c)) m |= 1u << r;
+    if (row < lay.rows && cm_present<TROP, W>(bits, D, row * lay.width + c)) m |= 1u << r;
   }
   if (c < lay.n0) masks[c * T + t] = m;
 }
@@ -611,12 +618,18 @@ __global__ void __launch_bounds__(NT) k_cm_offsets(const uint32_t* __restrict__ 
   }
 }
 
-template <class K, bool TROP>
+// Shared memory of k_cm_write: one 32 x 33 weight tile per warp (dynamic, so
+// the 64-bit lanes' 67.6 KB fit).
+template <class W>
+constexpr size_t cm_write_smem() { return (size_t)(NT / 32) * 32 * 33 * sizeof(W); }
+
+template <class K, bool TROP, class W>
 __global__ void __launch_bounds__(NT)
-    k_cm_write(const uint32_t* __restrict__ bits, const int32_t* __restrict__ D, DenseLayout lay, uint64_t T,
+    k_cm_write(const uint32_t* __restrict__ bits, const W* __restrict__ D, DenseLayout lay, uint64_t T,
                uint64_t subtiles, const uint32_t* __restrict__ masks, const uint64_t* __restrict__ offs,
-               K* __restrict__ out, int32_t* __restrict__ out_w, uint64_t out_cap, uint32_t* status) {
-  __shared__ int32_t s_w[NT / 32][32][33];
+               K* __restrict__ out, W* __restrict__ out_w, uint64_t out_cap, uint32_t* status) {
+  extern __shared__ __align__(16) unsigned char s_cm_raw[];
+  W (*s_w)[32][33] = reinterpret_cast<W (*)[32][33]>(s_cm_raw);
   const uint64_t g = ((uint64_t)blockIdx.x * NT + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (g >= subtiles) return;
@@ -627,7 +640,7 @@ __global__ void __launch_bounds__(NT)
 #pragma unroll 8
     for (int r = 0; r < 32; r++) {
       const uint64_t row = t * 32 + r;
-      s_w[warp][r][lane] = row < lay.rows ? D[row * lay.width + c] : INT32_MAX;
+      s_w[warp][r][lane] = row < lay.rows ? D[row * lay.width + c] : WAbs<W>::v;
     }
     __syncwarp();
   }
@@ -831,12 +844,12 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
-template <bool TROP>
+template <bool TROP, class W>
 __global__ void __launch_bounds__(NT)
     k_words_write(uint32_t* marks, uint64_t words, uint32_t wpr, const uint32_t* __restrict__ off, uint64_t n_nodes,
                   const uint64_t* __restrict__ tile_cnt, const uint64_t* __restrict__ tile_deg, uint64_t n_tiles,
                   uint32_t* __restrict__ hword, uint32_t* __restrict__ hmask, uint64_t* __restrict__ hpos,
-                  uint32_t* __restrict__ hseg, const int32_t* __restrict__ D, int32_t* __restrict__ Dprev,
+                  uint32_t* __restrict__ hseg, const W* __restrict__ D, W* __restrict__ Dprev,
                   unsigned long long* totals) {
   __shared__ uint64_t s_wc[NT / 32], s_wd[NT / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -898,7 +911,7 @@ __global__ void __launch_bounds__(NT)
       const uint64_t wb = base + (uint64_t)j * 32;
       while (hb) {
         int t[8];
-        int32_t val[8];
+        W val[8];
 #pragma unroll
         for (int q = 0; q < 8; q++) {
           t[q] = hb ? __ffs(hb) - 1 : -1;
@@ -983,11 +996,11 @@ void dense_heads(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uint64
 
 uint64_t dense_heads_sums(uint64_t n) { return 2 * (ceil_div(n ? n : 1, HC_TILE) + 1) + 2; }
 
-template <class K, bool TROP>
-void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n_rows, const uint32_t* hidx,
+template <class K, bool TROP, class W>
+void dense_expand(strata_ctx* ctx, const K* dkeys, const W* dw, uint64_t n_rows, const uint32_t* hidx,
                   const uint64_t* hpos, const uint32_t* hseg, const uint8_t* hg, uint64_t nh, uint64_t total,
                   uint64_t candidates, int pshift, uint64_t pmask, int out_pshift, int out_vshift, const uint32_t* nbr,
-                  uint64_t n_nbr, const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D,
+                  uint64_t n_nbr, const W* nbr_w, const DenseLayout& lay, uint32_t* bits, W* D,
                   uint32_t* marks, uint64_t* splits_buf) {
   if (nh == 0 || total == 0) return;
   const uint64_t tiles = ceil_div(nh + total, DE_TILE);
@@ -1002,22 +1015,24 @@ void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n
     SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(dkeys, dw, n_rows, hidx, hpos, hseg, hg, nh, total, splits_buf,
                                                      pshift, pmask, ck, cv, 1u, 0, 33, nbr, n_nbr, nbr_w, lay.entries,
-                                                     bits, D, marks, ctx->d_status);
+                                                     bits, D, marks, ctx->wshift, ctx->d_status);
   };
-  if (lay.entries <= 0xffffffffull) launch(k_expand_dense<K, TROP, false, uint32_t>);
-  else launch(k_expand_dense<K, TROP, false, uint64_t>);
+  if (lay.entries <= 0xffffffffull) launch(k_expand_dense<K, TROP, false, uint32_t, W>);
+  else launch(k_expand_dense<K, TROP, false, uint64_t, W>);
   // Algorithmic bytes: every Δ row (key, weight) once, each head's record,
-  // every CSR edge of a group read once (neighbour + weight), one 4-byte
-  // index probe per candidate (a candidate = one Δ row × one edge).
-  const uint64_t wsz = TROP ? 4 : 0;
-  kprof_end(ctx, kh, n_rows * (sizeof(K) + wsz) + nh * (4 + 8 + 4 + 1) + total * (4 + wsz) + candidates * 4);
+  // every CSR edge of a group read once (neighbour + weight), one index
+  // probe per candidate (a weight for Trop, a 4-byte bitmap word for Bool;
+  // a candidate = one Δ row × one edge).
+  const uint64_t wsz = TROP ? sizeof(W) : 0;
+  kprof_end(ctx, kh, n_rows * (sizeof(K) + wsz) + nh * (4 + 8 + 4 + 1) + total * (4 + wsz) +
+                         candidates * (TROP ? sizeof(W) : 4));
   after_launch(ctx, "k_expand_dense");
 }
 
-template <bool TROP>
+template <bool TROP, class W>
 void dense_word_heads(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const uint32_t* off,
                       uint64_t n_nodes, uint64_t* sums, uint32_t* hword, uint32_t* hmask, uint64_t* hpos,
-                      uint32_t* hseg, const int32_t* D, int32_t* Dprev, uint64_t* out4) {
+                      uint32_t* hseg, const W* D, W* Dprev, uint64_t* out4) {
   const uint64_t words = lay.entries / 32;
   if (words >= (1ull << 32)) fail(STRATA_E_UNSUPPORTED, "direct-addressed index beyond 2^37 entries");
   const uint64_t tiles = ceil_div(words ? words : 1, WH_TILE);
@@ -1029,8 +1044,8 @@ void dense_word_heads(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, 
   k_words_count<TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, wpr, off, n_nodes, tc, td, tot);
   after_launch(ctx, "k_words_count");
   scan_tile_sums(ctx, tc, tiles, 2);  // tc and td
-  k_words_write<TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, wpr, off, n_nodes, tc, td, tiles, hword,
-                                                               hmask, hpos, hseg, D, Dprev, tot);
+  k_words_write<TROP, W><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, wpr, off, n_nodes, tc, td, tiles,
+                                                                  hword, hmask, hpos, hseg, D, Dprev, tot);
   after_launch(ctx, "k_words_write");
   SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, tot, 4 * 8, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
@@ -1042,11 +1057,11 @@ void dense_word_heads(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, 
 
 uint64_t dense_word_heads_sums(const DenseLayout& lay) { return 2 * (ceil_div(lay.entries / 32 + 1, WH_TILE) + 1) + 4; }
 
-template <bool TROP>
+template <bool TROP, class W>
 void dense_expand_words(strata_ctx* ctx, const uint32_t* hword, const uint32_t* hmask, const uint64_t* hpos,
                         const uint32_t* hseg, uint64_t nh, uint64_t total, uint64_t candidates, uint64_t n_delta,
-                        const int32_t* Dprev, int out_pshift, int out_vshift, const uint32_t* nbr, uint64_t n_nbr,
-                        const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D, uint32_t* marks,
+                        const W* Dprev, int out_pshift, int out_vshift, const uint32_t* nbr, uint64_t n_nbr,
+                        const W* nbr_w, const DenseLayout& lay, uint32_t* bits, W* D, uint32_t* marks,
                         uint64_t* splits_buf) {
   if (nh == 0 || total == 0) return;
   const uint64_t tiles = ceil_div(nh + total, DE_TILE);
@@ -1064,28 +1079,29 @@ void dense_expand_words(strata_ctx* ctx, const uint32_t* hword, const uint32_t* 
     SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<(unsigned)tiles, NT, smem, ctx->stream>>>(nullptr, Dprev, lay.entries, hword, hpos, hseg, hmask, nh, total,
                                                      splits_buf, 0, 0, ck, cv, wpr, wpr_shift, members, nbr, n_nbr,
-                                                     nbr_w, lay.entries, bits, D, marks, ctx->d_status);
+                                                     nbr_w, lay.entries, bits, D, marks, ctx->wshift, ctx->d_status);
   };
-  if (lay.entries <= 0xffffffffull) launch(k_expand_dense<uint32_t, TROP, true, uint32_t>);
-  else launch(k_expand_dense<uint32_t, TROP, true, uint64_t>);
+  if (lay.entries <= 0xffffffffull) launch(k_expand_dense<uint32_t, TROP, true, uint32_t, W>);
+  else launch(k_expand_dense<uint32_t, TROP, true, uint64_t, W>);
   // Algorithmic bytes: each head's record (word, mask, position, segment),
   // every CSR edge of a head read once (neighbour + weight), each Δ weight
-  // once, one 4-byte index probe per candidate.
-  const uint64_t wsz = TROP ? 4 : 0;
-  kprof_end(ctx, kh, nh * (4 + 4 + 8 + 4) + total * (4 + wsz) + n_delta * wsz + candidates * 4);
+  // once, one index probe per candidate (a weight for Trop, a 4-byte bitmap
+  // word for Bool).
+  const uint64_t wsz = TROP ? sizeof(W) : 0;
+  kprof_end(ctx, kh, nh * (4 + 4 + 8 + 4) + total * (4 + wsz) + n_delta * wsz + candidates * (TROP ? sizeof(W) : 4));
   after_launch(ctx, "k_expand_dense");
 }
 
-template <class K, bool TROP>
-uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const int32_t* D, K* out,
-                             int32_t* out_w, uint64_t out_cap, uint64_t* sums) {
+template <class K, bool TROP, class W>
+uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const W* D, K* out,
+                             W* out_w, uint64_t out_cap, uint64_t* sums) {
   const uint64_t words = (lay.entries + 31) / 32;
   const uint64_t tiles = ceil_div(words, MC_TILE);
   k_marks_count<<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, sums);
   after_launch(ctx, "k_marks_count");
   scan_tile_sums(ctx, sums, tiles);
-  k_marks_write<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, lay, D, out, out_w, out_cap, sums,
-                                                                 ctx->d_status);
+  k_marks_write<K, TROP, W><<<(unsigned)tiles, NT, 0, ctx->stream>>>(marks, words, lay, D, out, out_w, out_cap,
+                                                                    sums, ctx->d_status);
   after_launch(ctx, "k_marks_write");
   SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, sums + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
@@ -1094,22 +1110,22 @@ uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout
 
 uint64_t dense_marks_states(uint64_t entries) { return ceil_div((entries + 31) / 32, MC_TILE) + 2; }
 
-template <class K, bool TROP>
-void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, const DenseLayout& lay, uint32_t* bits,
-                int32_t* D, uint32_t* marks) {
+template <class K, bool TROP, class W>
+void dense_seed(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, const DenseLayout& lay, uint32_t* bits,
+                W* D, uint32_t* marks) {
   if (TROP) {
-    k_fill_i32<<<(unsigned)std::min<uint64_t>(ceil_div(lay.entries, NT), (uint64_t)ctx->num_sms * 16), NT, 0,
-                 ctx->stream>>>(D, lay.entries, INT32_MAX);
-    after_launch(ctx, "k_fill_i32");
+    k_fill_w<W><<<(unsigned)std::min<uint64_t>(ceil_div(lay.entries, NT), (uint64_t)ctx->num_sms * 16), NT, 0,
+                  ctx->stream>>>(D, lay.entries, WAbs<W>::v);
+    after_launch(ctx, "k_fill_w");
   }
   if (!n) return;
-  k_dense_seed<K, TROP><<<grid1(n), NT, 0, ctx->stream>>>(keys, w, n, lay, bits, D, marks, ctx->d_status);
+  k_dense_seed<K, TROP, W><<<grid1(n), NT, 0, ctx->stream>>>(keys, w, n, lay, bits, D, marks, ctx->d_status);
   after_launch(ctx, "k_dense_seed");
 }
 
-template <class K, bool TROP>
-uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, const DenseLayout& lay, K* out,
-                       int32_t* out_w, uint64_t out_cap) {
+template <class K, bool TROP, class W>
+uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const W* D, const DenseLayout& lay, K* out,
+                       W* out_w, uint64_t out_cap) {
   const uint64_t logical = lay.n0 * lay.n1;
   if (!logical) return 0;
   if (lay.colmajor) {
@@ -1118,15 +1134,18 @@ uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, 
     const unsigned blocks = (unsigned)ceil_div(subtiles, NT / 32);
     DBuf<uint32_t> masks(ctx, M);
     DBuf<uint64_t> offs(ctx, M), sums(ctx, chunks + 1);
-    k_cm_masks<TROP><<<blocks, NT, 0, ctx->stream>>>(bits, D, lay, T, subtiles, masks.p);
+    k_cm_masks<TROP, W><<<blocks, NT, 0, ctx->stream>>>(bits, D, lay, T, subtiles, masks.p);
     after_launch(ctx, "k_cm_masks");
     k_cm_chunk_sums<<<(unsigned)chunks, NT, 0, ctx->stream>>>(masks.p, M, sums.p);
     after_launch(ctx, "k_cm_chunk_sums");
     scan_tile_sums(ctx, sums.p, chunks);
     k_cm_offsets<<<(unsigned)chunks, NT, 0, ctx->stream>>>(masks.p, M, sums.p, offs.p);
     after_launch(ctx, "k_cm_offsets");
-    k_cm_write<K, TROP><<<blocks, NT, 0, ctx->stream>>>(bits, D, lay, T, subtiles, masks.p, offs.p, out, out_w,
-                                                         out_cap, ctx->d_status);
+    const size_t smem = TROP ? cm_write_smem<W>() : 0;
+    if (smem > 48 * 1024)
+      SK_CUDA(cudaFuncSetAttribute(k_cm_write<K, TROP, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_cm_write<K, TROP, W><<<blocks, NT, smem, ctx->stream>>>(bits, D, lay, T, subtiles, masks.p, offs.p, out, out_w,
+                                                               out_cap, ctx->d_status);
     after_launch(ctx, "k_cm_write");
     SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, sums.p + chunks, 8, cudaMemcpyDeviceToHost, ctx->stream));
     sync_and_check(ctx);
@@ -1136,45 +1155,47 @@ uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, 
   DBuf<uint64_t> states(ctx, tiles + 2);
   uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles + 1);
   SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 2), ctx->stream));
-  k_dense_compact<K, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(bits, D, lay, out, out_w, out_cap, states.p,
-                                                                    counter, states.p + tiles, ctx->d_status);
+  k_dense_compact<K, TROP, W><<<(unsigned)tiles, NT, 0, ctx->stream>>>(bits, D, lay, out, out_w, out_cap, states.p,
+                                                                       counter, states.p + tiles, ctx->d_status);
   after_launch(ctx, "k_dense_compact");
   SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, states.p + tiles, 8, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
   return ctx->h_scalar[0];
 }
 
-#define SK_INST_DENSE(K, T)                                                                                 \
-  template void dense_expand<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const uint32_t*,         \
-                                   const uint64_t*, const uint32_t*, const uint8_t*, uint64_t, uint64_t,     \
-                                   uint64_t, int, uint64_t, int, int, const uint32_t*, uint64_t,             \
-                                   const int32_t*, const DenseLayout&, uint32_t*, int32_t*, uint32_t*,       \
-                                   uint64_t*);                                                               \
-  template uint64_t dense_marks_compact<K, T>(strata_ctx*, uint32_t*, const DenseLayout&, const int32_t*,    \
-                                              K*, int32_t*, uint64_t, uint64_t*);                            \
-  template void dense_seed<K, T>(strata_ctx*, const K*, const int32_t*, uint64_t, const DenseLayout&,        \
-                                 uint32_t*, int32_t*, uint32_t*);                                            \
-  template uint64_t dense_compact<K, T>(strata_ctx*, const uint32_t*, const int32_t*, const DenseLayout&, K*, \
-                                        int32_t*, uint64_t);
+#define SK_INST_DENSE(K, T, W)                                                                              \
+  template void dense_expand<K, T, W>(strata_ctx*, const K*, const W*, uint64_t, const uint32_t*, const uint64_t*, \
+                                      const uint32_t*, const uint8_t*, uint64_t, uint64_t, uint64_t, int, uint64_t, \
+                                      int, int, const uint32_t*, uint64_t, const W*, const DenseLayout&, uint32_t*, \
+                                      W*, uint32_t*, uint64_t*);                                                  \
+  template uint64_t dense_marks_compact<K, T, W>(strata_ctx*, uint32_t*, const DenseLayout&, const W*, K*, W*,     \
+                                                 uint64_t, uint64_t*);                                            \
+  template void dense_seed<K, T, W>(strata_ctx*, const K*, const W*, uint64_t, const DenseLayout&, uint32_t*, W*, \
+                                    uint32_t*);                                                                   \
+  template uint64_t dense_compact<K, T, W>(strata_ctx*, const uint32_t*, const W*, const DenseLayout&, K*, W*,     \
+                                           uint64_t);
 template void dense_heads<uint32_t>(strata_ctx*, const uint32_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t,
                                     uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint8_t*, uint64_t*);
 template void dense_heads<uint64_t>(strata_ctx*, const uint64_t*, uint64_t, int, uint64_t, const uint32_t*, uint64_t,
                                     uint64_t*, uint32_t*, uint64_t*, uint32_t*, uint8_t*, uint64_t*);
-SK_INST_DENSE(uint32_t, false)
-SK_INST_DENSE(uint32_t, true)
-SK_INST_DENSE(uint64_t, false)
-SK_INST_DENSE(uint64_t, true)
+SK_INST_DENSE(uint32_t, false, int32_t)
+SK_INST_DENSE(uint32_t, true, int32_t)
+SK_INST_DENSE(uint32_t, true, int64_t)
+SK_INST_DENSE(uint64_t, false, int32_t)
+SK_INST_DENSE(uint64_t, true, int32_t)
+SK_INST_DENSE(uint64_t, true, int64_t)
 #undef SK_INST_DENSE
-#define SK_INST_WORDS(T)                                                                                         \
-  template void dense_word_heads<T>(strata_ctx*, uint32_t*, const DenseLayout&, const uint32_t*, uint64_t,       \
-                                    uint64_t*, uint32_t*, uint32_t*, uint64_t*, uint32_t*, const int32_t*,       \
-                                    int32_t*, uint64_t*);                                                        \
-  template void dense_expand_words<T>(strata_ctx*, const uint32_t*, const uint32_t*, const uint64_t*,            \
-                                      const uint32_t*, uint64_t, uint64_t, uint64_t, uint64_t, const int32_t*,   \
-                                      int, int, const uint32_t*, uint64_t, const int32_t*, const DenseLayout&,   \
-                                      uint32_t*, int32_t*, uint32_t*, uint64_t*);
-SK_INST_WORDS(false)
-SK_INST_WORDS(true)
+#define SK_INST_WORDS(T, W)                                                                                     \
+  template void dense_word_heads<T, W>(strata_ctx*, uint32_t*, const DenseLayout&, const uint32_t*, uint64_t,   \
+                                       uint64_t*, uint32_t*, uint32_t*, uint64_t*, uint32_t*, const W*, W*,     \
+                                       uint64_t*);                                                              \
+  template void dense_expand_words<T, W>(strata_ctx*, const uint32_t*, const uint32_t*, const uint64_t*,        \
+                                         const uint32_t*, uint64_t, uint64_t, uint64_t, uint64_t, const W*, int, \
+                                         int, const uint32_t*, uint64_t, const W*, const DenseLayout&,          \
+                                         uint32_t*, W*, uint32_t*, uint64_t*);
+SK_INST_WORDS(false, int32_t)
+SK_INST_WORDS(true, int32_t)
+SK_INST_WORDS(true, int64_t)
 #undef SK_INST_WORDS
 
 }  // namespace sk

@@ -250,6 +250,7 @@ strata_rel* finish_rel(strata_ctx* ctx, Rel<K, W>& full, int shift) {
   rel->key_bytes = sizeof(K);
   rel->w_bytes = TROP ? sizeof(W) : 0;
   rel->shift = shift;
+  rel->wshift = TROP ? ctx->wshift : 0;
   rel->n = full.n;
   rel->keys = full.k.detach();
   rel->w = TROP ? (void*)full.w.detach() : nullptr;
@@ -309,11 +310,12 @@ void fill_stats(strata_fix_stats* st, const Acct& a, uint64_t rounds, uint64_t r
 // Index over (c0, c1) in [0, n0) × [0, n1): a membership bitmap (Bool), an
 // int32 weight array (Trop), the marks of the current Δ and, for Trop, the
 // snapshot of Δ's weights that the next round reads.
+template <class W>
 struct DenseIdx {
   DBuf<uint32_t> bits;   // Bool membership
   DBuf<uint32_t> marks;  // Δ: the entries the last round marked
-  DBuf<int32_t> D;       // Trop weights (INT32_MAX = absent)
-  DBuf<int32_t> Dprev;   // Trop: Δ's weights as the round that made it left them
+  DBuf<W> D;             // Trop weight codes (WAbs<W> = absent)
+  DBuf<W> Dprev;         // Trop: Δ's weights as the round that made it left them
   DBuf<uint32_t> hidx, hseg, hmask;  // heads (key-head row or marks word, CSR segment, member mask)
   DBuf<uint8_t> hg;                  // key-head group sizes
   DBuf<uint64_t> hpos, hsums;        // head degree prefix; per-tile sums of the head compaction
@@ -322,29 +324,29 @@ struct DenseIdx {
   uint64_t words() const { return entries / 32; }
 };
 
-// Bytes the index needs; the plan is used when they stay within budget.
-inline double dense_bytes(bool trop, uint64_t n0, uint64_t n1) {
+// Bytes the index needs (D and Dprev at `wbytes` per entry for Trop, the
+// bitmap for Bool, the marks); the plan is used when they stay within budget.
+inline double dense_bytes(bool trop, int wbytes, uint64_t n0, uint64_t n1) {
   const double rows = (double)n1, width = (double)((n0 + 31) & ~31ull);  // the wider of the two layouts
   const double rows2 = (double)n0, width2 = (double)((n1 + 31) & ~31ull);
   const double e = std::max(rows * width, rows2 * width2);
-  return (trop ? 8.0 * e : e / 8.0) + e / 8.0;
+  return (trop ? 2.0 * wbytes * e : e / 8.0) + e / 8.0;
 }
 constexpr double kDenseBudget = 16e9;
 
 inline bool want_dense(strata_ctx* ctx, bool trop, bool narrow, uint64_t n0, uint64_t n1) {
   const long double e = (long double)n0 * (long double)n1;
-  const bool fits = (!trop || narrow) && e < 9.0e18L && n0 < (1ull << 32) && n1 < (1ull << 32) &&
-                    dense_bytes(trop, n0, n1) <= kDenseBudget;
+  const bool fits = e < 9.0e18L && n0 < (1ull << 32) && n1 < (1ull << 32) &&
+                    dense_bytes(trop, narrow ? 4 : 8, n0, n1) <= kDenseBudget;
   if (ctx->plan == 3) fail(STRATA_E_UNSUPPORTED, "the bit-row plan applies to Bool transitive closure only");
   if (ctx->plan == 1) return false;
-  if (ctx->plan == 2 && !fits)
-    fail(STRATA_E_UNSUPPORTED, "the direct-addressed plan needs int32 weights and an index within 16 GB");
+  if (ctx->plan == 2 && !fits) fail(STRATA_E_UNSUPPORTED, "the direct-addressed plan needs an index within 16 GB");
   return fits;
 }
 
 // `colmajor`: the next round joins on c1 (rows by c1), else on c0.
-template <bool TROP>
-void dense_alloc(strata_ctx* ctx, DenseIdx& X, uint64_t n0, uint64_t n1, int b1, bool colmajor) {
+template <bool TROP, class W>
+void dense_alloc(strata_ctx* ctx, DenseIdx<W>& X, uint64_t n0, uint64_t n1, int b1, bool colmajor) {
   X.bits.ctx = X.D.ctx = X.Dprev.ctx = X.marks.ctx = ctx;
   X.hidx.ctx = X.hseg.ctx = X.hmask.ctx = X.hg.ctx = X.hpos.ctx = X.hsums.ctx = ctx;
   X.lay = dense_layout(b1, n0, n1, colmajor);
@@ -365,9 +367,9 @@ void dense_alloc(strata_ctx* ctx, DenseIdx& X, uint64_t n0, uint64_t n1, int b1,
 // A round whose Δ is a key list (the bootstrap src ⋈ edge): key heads, then
 // the expand, which marks the new / improved entries (the next Δ).  Returns
 // the candidate count (a bound on the marks set).
-template <class K, bool TROP>
-uint64_t dense_round_keys(strata_ctx* ctx, const K* dk, const int32_t* dw, uint64_t nd, const Csr<int32_t>& csr,
-                          const JoinSpec& js, DenseIdx& X, DBuf<uint64_t>& splits, PhaseTimer& pt, Acct& a) {
+template <class K, bool TROP, class W>
+uint64_t dense_round_keys(strata_ctx* ctx, const K* dk, const W* dw, uint64_t nd, const Csr<W>& csr,
+                          const JoinSpec& js, DenseIdx<W>& X, DBuf<uint64_t>& splits, PhaseTimer& pt, Acct& a) {
   if (nd == 0) return 0;
   const uint64_t l0 = ctx->launches;
   const int t = pt.begin(&a.join_ms);
@@ -382,13 +384,13 @@ uint64_t dense_round_keys(strata_ctx* ctx, const K* dk, const int32_t* dw, uint6
   const uint64_t nh = h3[0], T = h3[1], cands = h3[2];  // heads; (group, edge) outputs; candidates
   if (T) {
     splits.reserve_grow(ceil_div(nh + T, dense_tile_size()) + 2);
-    dense_expand<K, TROP>(ctx, dk, dw, nd, X.hidx.p, X.hpos.p, X.hseg.p, X.hg.p, nh, T, cands, js.pshift, js.pmask,
+    dense_expand<K, TROP, W>(ctx, dk, dw, nd, X.hidx.p, X.hpos.p, X.hseg.p, X.hg.p, nh, T, cands, js.pshift, js.pmask,
                           js.out_pshift, js.out_vshift, csr.nbr.p, csr.m, TROP ? csr.w.p : nullptr, X.lay,
                           TROP ? nullptr : X.bits.p, TROP ? X.D.p : nullptr, X.marks.p, splits.p);
   }
   pt.end(t);
-  const uint64_t wsz = TROP ? 4 : 0;
-  a.join_b += nd * (sizeof(K) + wsz) + nh * 17 + T * (4 + wsz) + cands * 4;
+  const uint64_t wsz = TROP ? sizeof(W) : 0;
+  a.join_b += nd * (sizeof(K) + wsz) + nh * 17 + T * (4 + wsz) + cands * (TROP ? sizeof(W) : 4);
   a.join_l += (uint32_t)(ctx->launches - l0);
   a.cands += cands;
   return cands;
@@ -397,8 +399,8 @@ uint64_t dense_round_keys(strata_ctx* ctx, const K* dk, const int32_t* dw, uint6
 // Semi-naive rounds with Δ in the marks: word heads (which clear the marks
 // and snapshot Δ's weights), then the expand marks Δ'.  A round runs while
 // Δ is non-empty; `bound` is an upper bound on the entries marked now.
-template <bool TROP>
-void fix_loop_dense(strata_ctx* ctx, const Csr<int32_t>& csr, const JoinSpec& js, DenseIdx& X, uint64_t bound,
+template <bool TROP, class W>
+void fix_loop_dense(strata_ctx* ctx, const Csr<W>& csr, const JoinSpec& js, DenseIdx<W>& X, uint64_t bound,
                     uint64_t cap, PhaseTimer& pt, Acct& a, uint64_t* rounds_out) {
   DBuf<uint64_t> splits;
   splits.ctx = ctx;
@@ -412,7 +414,7 @@ void fix_loop_dense(strata_ctx* ctx, const Csr<int32_t>& csr, const JoinSpec& js
     X.hseg.reserve_grow(hcap);
     X.hpos.reserve_grow(hcap);
     uint64_t h4[4];
-    dense_word_heads<TROP>(ctx, X.marks.p, X.lay, csr.off.p, csr.n_nodes, X.hsums.p, X.hidx.p, X.hmask.p,
+    dense_word_heads<TROP, W>(ctx, X.marks.p, X.lay, csr.off.p, csr.n_nodes, X.hsums.p, X.hidx.p, X.hmask.p,
                            X.hpos.p, X.hseg.p, TROP ? X.D.p : nullptr, TROP ? X.Dprev.p : nullptr, h4);
     const uint64_t nh = h4[0], T = h4[1], cands = h4[2], nd = h4[3];
     if (nd == 0) {
@@ -424,16 +426,16 @@ void fix_loop_dense(strata_ctx* ctx, const Csr<int32_t>& csr, const JoinSpec& js
     rounds++;
     if (T) {
       splits.reserve_grow(ceil_div(nh + T, dense_tile_size()) + 2);
-      dense_expand_words<TROP>(ctx, X.hidx.p, X.hmask.p, X.hpos.p, X.hseg.p, nh, T, cands, nd,
+      dense_expand_words<TROP, W>(ctx, X.hidx.p, X.hmask.p, X.hpos.p, X.hseg.p, nh, T, cands, nd,
                                TROP ? X.Dprev.p : nullptr, js.out_pshift, js.out_vshift, csr.nbr.p, csr.m,
                                TROP ? csr.w.p : nullptr, X.lay, TROP ? nullptr : X.bits.p, TROP ? X.D.p : nullptr,
                                X.marks.p, splits.p);
     }
     pt.end(t);
-    const uint64_t wsz = TROP ? 4 : 0;
+    const uint64_t wsz = TROP ? sizeof(W) : 0;
     // marks read and cleared, head records written and read, Δ weights
     // snapshot (read, write, read), edges, probes
-    a.join_b += X.words() * 4 * 2 + nh * 20 * 2 + nd * 3 * wsz + T * (4 + wsz) + cands * 4;
+    a.join_b += X.words() * 4 * 2 + nh * 20 * 2 + nd * 3 * wsz + T * (4 + wsz) + cands * (TROP ? sizeof(W) : 4);
     a.join_l += (uint32_t)(ctx->launches - l0);
     a.cands += cands;
     bound = std::min<uint64_t>(cands, X.entries);
@@ -444,13 +446,13 @@ void fix_loop_dense(strata_ctx* ctx, const Csr<int32_t>& csr, const JoinSpec& js
 }
 
 // Compact the index into a sorted relation.
-template <class K, bool TROP>
-void dense_finish(strata_ctx* ctx, DenseIdx& X, int b1, Rel<K, int32_t>& full, uint64_t upper) {
+template <class K, bool TROP, class W>
+void dense_finish(strata_ctx* ctx, DenseIdx<W>& X, int b1, Rel<K, W>& full, uint64_t upper) {
   (void)b1;
   const uint64_t cap = std::min<uint64_t>(upper, X.lay.n0 * X.lay.n1) + 1;
   full.reserve(cap, TROP);
-  full.n = dense_compact<K, TROP>(ctx, X.bits.p, TROP ? X.D.p : nullptr, X.lay, full.k.p,
-                                  TROP ? full.w.p : nullptr, cap);
+  full.n = dense_compact<K, TROP, W>(ctx, X.bits.p, TROP ? X.D.p : nullptr, X.lay, full.k.p,
+                                     TROP ? full.w.p : nullptr, cap);
 }
 
 // ---- TC-shaped drivers: head(X,Z) :- edge(X,Y), head(Y,Z) -----------------------
@@ -489,21 +491,19 @@ strata_rel* run_tc_shape(strata_ctx* ctx, const EdgeCols& e, int b0, int b1, int
   JoinSpec js{b1, low_mask(b0), 0, low_mask(b1), 0, b1};
   Scratch<K, W> s(ctx);
   uint64_t rounds = 0;
-  if constexpr (std::is_same<W, int32_t>::value) {
-    if (dense) {
-      plan = 2;
-      DenseIdx X;
-      // Δ(Y,Z) joins on c0: row-major index.
-      dense_alloc<TROP>(ctx, X, n_nodes_src, n_nodes_dst, b1, false);
-      // the seed is also the first Δ: its entries are marked
-      if (TROP) dense_seed<K, true>(ctx, full.k.p, full.w.p, full.n, X.lay, X.bits.p, X.D.p, X.marks.p);
-      else dense_seed<K, false>(ctx, full.k.p, nullptr, full.n, X.lay, X.bits.p, nullptr, X.marks.p);
-      pt.end(a.setup_t);
-      fix_loop_dense<TROP>(ctx, csr, js, X, full.n, cap, pt, a, &rounds);
-      const int tf = pt.begin(&a.finish_ms);
-      dense_finish<K, TROP>(ctx, X, b1, full, X.entries);
-      pt.end(tf);
-    }
+  if (dense) {
+    plan = 2;
+    DenseIdx<W> X;
+    // Δ(Y,Z) joins on c0: row-major index.
+    dense_alloc<TROP, W>(ctx, X, n_nodes_src, n_nodes_dst, b1, false);
+    // the seed is also the first Δ: its entries are marked
+    if (TROP) dense_seed<K, true, W>(ctx, full.k.p, full.w.p, full.n, X.lay, X.bits.p, X.D.p, X.marks.p);
+    else dense_seed<K, false, W>(ctx, full.k.p, nullptr, full.n, X.lay, X.bits.p, nullptr, X.marks.p);
+    pt.end(a.setup_t);
+    fix_loop_dense<TROP, W>(ctx, csr, js, X, full.n, cap, pt, a, &rounds);
+    const int tf = pt.begin(&a.finish_ms);
+    dense_finish<K, TROP, W>(ctx, X, b1, full, X.entries);
+    pt.end(tf);
   }
   if (plan == 1) {
     pt.end(a.setup_t);
@@ -534,6 +534,34 @@ Layout tc_layout(strata_ctx* ctx, const EdgeCols& e) {
   L.n_nodes_src = (uint64_t)ms + 1;
   L.wide_key = L.b0 + L.b1 > 32;
   return L;
+}
+
+// Weight code shift of a wide (int64) fixpoint.  Every value the schedule
+// forms within the round cap is one seed weight plus at most cap + 2 edge
+// weights (or cap + 3 edge weights for the edge-seeded shape); [lo, hi]
+// bounds all of them.  Codes are value - s with finite codes up to
+// INT64_MAX - 2 (sk_prims.cuh), so s = max(0, hi - (INT64_MAX - 2)) in
+// {0, 1, 2} keeps every value up to i64::MAX representable (a sum beyond it
+// is the reference's overflow error, detected on codes), and lo must still
+// have a code: lo >= INT64_MIN + s, else STRATA_E_WEIGHT_RANGE.
+int64_t wide_shift(strata_ctx* ctx, const int64_t* ew, const uint8_t* einf, uint64_t ne, const int64_t* sw,
+                   const uint8_t* sinf, uint64_t ns, uint64_t cap) {
+  int64_t emn = 0, emx = 0, smn = 0, smx = 0;
+  if (!weight_range(ctx, ew, einf, ne, &emn, &emx)) emn = emx = 0;
+  if (ns && !weight_range(ctx, sw, sinf, ns, &smn, &smx)) smn = smx = 0;
+  const __int128 L = (__int128)cap + 3;
+  const __int128 kMax = INT64_MAX, kMin = INT64_MIN;
+  __int128 hi = (__int128)std::max<int64_t>(smx, 0) + L * (__int128)std::max<int64_t>(emx, 0);
+  __int128 lo = (__int128)std::min<int64_t>(smn, 0) + L * (__int128)std::min<int64_t>(emn, 0);
+  if (hi > kMax) hi = kMax;
+  if (lo < kMin) lo = kMin;
+  const __int128 fin = kMax - 2;
+  const int64_t s = hi > fin ? (int64_t)(hi - fin) : 0;
+  if (lo < kMin + s)
+    fail(STRATA_E_WEIGHT_RANGE,
+         "finite tropical weights span nearly all of i64 (sums within the round cap can reach both i64::MIN and "
+         "i64::MAX): no 64-bit code keeps them apart from +inf");
+  return s;
 }
 
 // Narrow (int32) Trop weights are exact when every derived sum within the
@@ -571,6 +599,7 @@ strata_rel* fix_tc_bool(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats* st
   if (st) std::memset(st, 0, sizeof(*st));
   reset_status(ctx);
   const uint64_t l_start = ctx->launches;
+  ctx->wshift = 0;
   EventTimer et(ctx);
   if (e.n == 0) {
     strata_rel* rel = new strata_rel();
@@ -597,6 +626,7 @@ strata_rel* fix_trop_paths(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats*
   if (st) std::memset(st, 0, sizeof(*st));
   reset_status(ctx);
   const uint64_t l_start = ctx->launches;
+  ctx->wshift = 0;
   EventTimer et(ctx);
   if (e.n == 0) {
     strata_rel* rel = new strata_rel();
@@ -609,6 +639,7 @@ strata_rel* fix_trop_paths(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats*
   const uint64_t universe = count_distinct_ids(ctx, e.src, e.n, e.dst, e.n, nullptr, 0, limit);
   const uint64_t cap = universe + 2;
   const bool narrow = narrow_ok(universe, max_abs_weight(ctx, e.w, e.inf, e.n), 0);
+  ctx->wshift = narrow ? 0 : wide_shift(ctx, e.w, e.inf, e.n, nullptr, nullptr, 0, cap);
   const bool dense = want_dense(ctx, true, narrow, L.n_nodes_src, L.n_nodes);
   const uint64_t ns = L.n_nodes_src;
   if (!L.wide_key) {
@@ -616,13 +647,13 @@ strata_rel* fix_trop_paths(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats*
       return run_tc_shape<uint32_t, int32_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et,
                                                    l_start, ns, dense);
     return run_tc_shape<uint32_t, int64_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et,
-                                                 l_start, ns, false);
+                                                 l_start, ns, dense);
   }
   if (narrow)
     return run_tc_shape<uint64_t, int32_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et,
                                                  l_start, ns, dense);
   return run_tc_shape<uint64_t, int64_t, true>(ctx, e, L.b0, L.b1, L.bsrc, L.n_nodes, universe, cap, st, et,
-                                               l_start, ns, false);
+                                               l_start, ns, dense);
 }
 
 // ---- MSSP: dist(S,Y) :- src(S), edge(S,Y). dist(S,Z) :- dist(S,Y), edge(Y,Z). ----
@@ -657,32 +688,30 @@ strata_rel* run_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
   const JoinSpec boot{0, ~0ull, 0, ~0ull, b1, 0};
   // Δ(S,Y): join Y = key & mask(b1), kept S = key >> b1, out = (S << b1) | Z.
   const JoinSpec step{0, low_mask(b1), b1, low_mask(b0), b1, 0};
-  if constexpr (std::is_same<W, int32_t>::value) {
-    if (dense) {
-      DenseIdx X;
-      // Δ(S,Y) joins on c1: column-major index, so Δ' comes out sorted by Y.
-      dense_alloc<true>(ctx, X, n0, n1, b1, true);
-      dense_seed<K, true>(ctx, nullptr, nullptr, 0, X.lay, X.bits.p, X.D.p, nullptr);
-      Rel<K, W> full;
-      full.k.ctx = full.w.ctx = ctx;
-      DBuf<uint64_t> splits;
-      splits.ctx = ctx;
-      pt.end(a.setup_t);
-      // Bootstrap: every derivation of src ⋈ edge, all new; its marks are
-      // the first Δ.
-      const uint64_t bound = dense_round_keys<K, true>(ctx, srcu.k.p, srcu.w.p, srcu.n, csr, boot, X, splits, pt, a);
-      uint64_t rounds = 0;
-      fix_loop_dense<true>(ctx, csr, step, X, std::min<uint64_t>(bound, X.entries), cap, pt, a, &rounds);
-      const int tf = pt.begin(&a.finish_ms);
-      dense_finish<K, true>(ctx, X, b1, full, X.entries);
-      pt.end(tf);
-      const double ms = et.stop();
-      pt.collect();
-      kprof_collect(ctx);
-      fill_stats(st, a, rounds, full.n, universe, key_bits, sizeof(W), ms, ctx->launches - l_start);
-      if (st) st->plan = 2;
-      return finish_rel<K, W, true>(ctx, full, b1);
-    }
+  if (dense) {
+    DenseIdx<W> X;
+    // Δ(S,Y) joins on c1: column-major index, so Δ' comes out sorted by Y.
+    dense_alloc<true, W>(ctx, X, n0, n1, b1, true);
+    dense_seed<K, true, W>(ctx, nullptr, nullptr, 0, X.lay, X.bits.p, X.D.p, nullptr);
+    Rel<K, W> full;
+    full.k.ctx = full.w.ctx = ctx;
+    DBuf<uint64_t> splits;
+    splits.ctx = ctx;
+    pt.end(a.setup_t);
+    // Bootstrap: every derivation of src ⋈ edge, all new; its marks are
+    // the first Δ.
+    const uint64_t bound = dense_round_keys<K, true, W>(ctx, srcu.k.p, srcu.w.p, srcu.n, csr, boot, X, splits, pt, a);
+    uint64_t rounds = 0;
+    fix_loop_dense<true, W>(ctx, csr, step, X, std::min<uint64_t>(bound, X.entries), cap, pt, a, &rounds);
+    const int tf = pt.begin(&a.finish_ms);
+    dense_finish<K, true, W>(ctx, X, b1, full, X.entries);
+    pt.end(tf);
+    const double ms = et.stop();
+    pt.collect();
+    kprof_collect(ctx);
+    fill_stats(st, a, rounds, full.n, universe, key_bits, sizeof(W), ms, ctx->launches - l_start);
+    if (st) st->plan = 2;
+    return finish_rel<K, W, true>(ctx, full, b1);
   }
   pt.end(a.setup_t);
   // Bootstrap: dist0 = min-reduce(src ⋈ edge), all of it new.
@@ -715,6 +744,7 @@ strata_rel* fix_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
   if (st) std::memset(st, 0, sizeof(*st));
   reset_status(ctx);
   const uint64_t l_start = ctx->launches;
+  ctx->wshift = 0;
   EventTimer et(ctx);
   if (ns == 0 || e.n == 0) {
     strata_rel* rel = new strata_rel();
@@ -735,6 +765,7 @@ strata_rel* fix_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
   const uint64_t cap = universe + 2;
   const bool narrow = narrow_ok(universe, max_abs_weight(ctx, e.w, e.inf, e.n),
                                 max_abs_weight(ctx, src_w, src_inf, ns));
+  ctx->wshift = narrow ? 0 : wide_shift(ctx, e.w, e.inf, e.n, src_w, src_inf, ns, cap);
   const uint64_t nn = (uint64_t)mes + 1;
   const uint64_t n0 = (uint64_t)mS + 1, n1 = (uint64_t)med + 1;
   const bool dense = want_dense(ctx, true, narrow, n0, n1);
@@ -743,13 +774,13 @@ strata_rel* fix_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
       return run_mssp<uint32_t, int32_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st,
                                          et, l_start, n0, n1, dense);
     return run_mssp<uint32_t, int64_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st,
-                                       et, l_start, n0, n1, false);
+                                       et, l_start, n0, n1, dense);
   }
   if (narrow)
     return run_mssp<uint64_t, int32_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st, et,
                                        l_start, n0, n1, dense);
   return run_mssp<uint64_t, int64_t>(ctx, sources, src_w, src_inf, ns, e, b0, b1, besrc, nn, universe, cap, st, et,
-                                     l_start, n0, n1, false);
+                                     l_start, n0, n1, dense);
 }
 
 // ---- relation handles ---------------------------------------------------------------
@@ -757,6 +788,7 @@ strata_rel* fix_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
 void rel_to_host(strata_ctx* ctx, const strata_rel* rel, uint32_t* src, uint32_t* dst, int64_t* w,
                  uint8_t* inf) {
   const uint64_t n = rel->n;
+  ctx->wshift = rel->wshift;  // the codes of this relation decode with its own shift
   if (n == 0) return;
   DBuf<uint32_t> c0(ctx, n), c1(ctx, n);
   DBuf<int64_t> ow;
@@ -787,6 +819,7 @@ void rel_to_host(strata_ctx* ctx, const strata_rel* rel, uint32_t* src, uint32_t
 
 uint64_t rel_fingerprint(strata_ctx* ctx, const strata_rel* rel) {
   if (rel->n == 0) return 0;
+  ctx->wshift = rel->wshift;
   if (rel->key_bytes == 4) {
     const uint32_t* k = static_cast<const uint32_t*>(rel->keys);
     if (!rel->trop) return fingerprint<uint32_t, int32_t, false>(ctx, k, nullptr, rel->n, rel->shift);

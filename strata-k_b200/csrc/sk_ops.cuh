@@ -57,17 +57,19 @@ void dense_heads(strata_ctx* ctx, const K* dkeys, uint64_t n, int jshift, uint64
                  uint64_t n_nodes, uint64_t* sums, uint32_t* hidx, uint64_t* hpos, uint32_t* hseg, uint8_t* hg,
                  uint64_t* out3);
 uint64_t dense_heads_sums(uint64_t n);
-template <class K, bool TROP>
-void dense_expand(strata_ctx* ctx, const K* dkeys, const int32_t* dw, uint64_t n_rows, const uint32_t* hidx,
+// Weight lanes W: int32_t (narrow) or int64_t (wide); Bool uses int32_t and
+// ignores it.  D holds WAbs<W> for absent entries.
+template <class K, bool TROP, class W = int32_t>
+void dense_expand(strata_ctx* ctx, const K* dkeys, const W* dw, uint64_t n_rows, const uint32_t* hidx,
                   const uint64_t* hpos, const uint32_t* hseg, const uint8_t* hg, uint64_t nh, uint64_t total,
                   uint64_t candidates, int pshift, uint64_t pmask, int out_pshift, int out_vshift, const uint32_t* nbr,
-                  uint64_t n_nbr, const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D,
+                  uint64_t n_nbr, const W* nbr_w, const DenseLayout& lay, uint32_t* bits, W* D,
                   uint32_t* marks, uint64_t* splits_buf);
 // The marked entries in index order (keys, Trop weights from D); clears the
 // marks.  Used for the bit-row plan's final relation.
-template <class K, bool TROP>
-uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const int32_t* D, K* out,
-                             int32_t* out_w, uint64_t out_cap, uint64_t* states_buf);
+template <class K, bool TROP, class W = int32_t>
+uint64_t dense_marks_compact(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const W* D, K* out,
+                             W* out_w, uint64_t out_cap, uint64_t* states_buf);
 uint64_t dense_marks_states(uint64_t entries);
 // Heads of the Δ held in `marks` (the entries the last round marked): one
 // head per nonzero 32-bit word whose row (join value) has edges, carrying the
@@ -75,30 +77,30 @@ uint64_t dense_marks_states(uint64_t entries);
 // D → Dprev (the values Δ carries through the next round).  Clears marks.
 // out4 = {heads, outputs, candidates, Δ tuples}.  `sums` holds
 // dense_word_heads_sums(lay) words.
-template <bool TROP>
+template <bool TROP, class W = int32_t>
 void dense_word_heads(strata_ctx* ctx, uint32_t* marks, const DenseLayout& lay, const uint32_t* off,
                       uint64_t n_nodes, uint64_t* sums, uint32_t* hword, uint32_t* hmask, uint64_t* hpos,
-                      uint32_t* hseg, const int32_t* D, int32_t* Dprev, uint64_t* out4);
+                      uint32_t* hseg, const W* D, W* Dprev, uint64_t* out4);
 uint64_t dense_word_heads_sums(const DenseLayout& lay);
 // One round over word heads: candidates (member, edge) of every head,
 // member weights from Dprev; new / improved entries set their marks.
-template <bool TROP>
+template <bool TROP, class W = int32_t>
 void dense_expand_words(strata_ctx* ctx, const uint32_t* hword, const uint32_t* hmask, const uint64_t* hpos,
                         const uint32_t* hseg, uint64_t nh, uint64_t total, uint64_t candidates, uint64_t n_delta,
-                        const int32_t* Dprev, int out_pshift, int out_vshift, const uint32_t* nbr, uint64_t n_nbr,
-                        const int32_t* nbr_w, const DenseLayout& lay, uint32_t* bits, int32_t* D, uint32_t* marks,
+                        const W* Dprev, int out_pshift, int out_vshift, const uint32_t* nbr, uint64_t n_nbr,
+                        const W* nbr_w, const DenseLayout& lay, uint32_t* bits, W* D, uint32_t* marks,
                         uint64_t* splits_buf);
 // In-place exclusive scan of per-tile sums (one block per array); sums[count]
 // = total.  `arrays` consecutive arrays of count + 1 words each.
 void scan_tile_sums(strata_ctx* ctx, uint64_t* sums, uint64_t count, int arrays = 1);
 // Seed the index from keys (and weights); `marks` (optional) marks every
 // seeded entry, making the seed the first Δ of the word-head rounds.
-template <class K, bool TROP>
-void dense_seed(strata_ctx* ctx, const K* keys, const int32_t* w, uint64_t n, const DenseLayout& lay, uint32_t* bits,
-                int32_t* D, uint32_t* marks);
-template <class K, bool TROP>
-uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const int32_t* D, const DenseLayout& lay, K* out,
-                       int32_t* out_w, uint64_t out_cap);
+template <class K, bool TROP, class W = int32_t>
+void dense_seed(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, const DenseLayout& lay, uint32_t* bits,
+                W* D, uint32_t* marks);
+template <class K, bool TROP, class W = int32_t>
+uint64_t dense_compact(strata_ctx* ctx, const uint32_t* bits, const W* D, const DenseLayout& lay, K* out,
+                       W* out_w, uint64_t out_cap);
 
 // Exclusive scan of per-element expand degrees (see sk_relops.cu).
 // pos[i] = sum_{k<i} deg(i); pos[n] = total.  Returns nothing; read pos[n].
@@ -160,21 +162,26 @@ uint64_t count_distinct_ids(strata_ctx* ctx, const uint32_t* a, uint64_t na, con
 uint32_t max_u32(strata_ctx* ctx, const uint32_t* a, uint64_t n);
 
 // Pack two u32 columns into keys (c0 << shift) | c1, optional weight conversion
-// from (int64 w, u8 inf) to W (inf -> WInf<W>).  Sets ST_SENTINEL when a finite
-// weight equals INT64_MAX.
+// from (int64 w, u8 inf) to W codes (inf -> WInf<W>, finite v -> v - ctx->wshift).
+// Sets ST_SENTINEL when a finite weight has no code.
 template <class K, class W, bool TROP>
 void pack_pairs(strata_ctx* ctx, const uint32_t* c0, const uint32_t* c1, const int64_t* w,
                 const uint8_t* inf, uint64_t n, int shift, K* keys, W* ow);
 
-// Unpack keys to columns (and W weights to int64 + inf mask).
+// Unpack keys to columns (and W codes to int64 values + inf mask, adding
+// ctx->wshift to finite codes).
 template <class K, class W, bool TROP>
 void unpack_pairs(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int shift,
                   uint32_t* c0, uint32_t* c1, int64_t* ow, uint8_t* oinf);
 
+// Min and max finite weight over (w, inf) columns (synchronizing); false when
+// there is none (both 0).  NULL w: every weight is Finite(0).
+bool weight_range(strata_ctx* ctx, const int64_t* w, const uint8_t* inf, uint64_t n, int64_t* mn, int64_t* mx);
+
 // Max |finite weight| over (w, inf) columns (synchronizing); 0 when n == 0.
 uint64_t max_abs_weight(strata_ctx* ctx, const int64_t* w, const uint8_t* inf, uint64_t n);
 
-// Order-independent fingerprint of (keys, weights).
+// Order-independent fingerprint of (keys, weight values = codes + ctx->wshift).
 template <class K, class W, bool TROP>
 uint64_t fingerprint(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int shift);
 

@@ -146,28 +146,46 @@ __device__ __forceinline__ uint64_t upper_bound_dev(const K* a, uint64_t lo, uin
 }
 
 // ---- Trop weights ----------------------------------------------------------------
-// A weight type W encodes +inf as its maximum value.  Narrow (int32) weights
-// are only used when the host has proven every derived sum stays strictly
-// inside the range, so they need no overflow test.
+// A device lane holds a weight CODE.  The reference's Weight is Finite(i64) |
+// PosInf (strata-ir/src/trop.rs:35-40), so +inf must stay distinct from every
+// finite value.  The two largest codes of a lane type are reserved:
+//   WAbs = max      "absent" (the direct-addressed index's empty entry),
+//   WInf = max - 1  +inf,
+// and a finite value v is stored as the code v - s, at most max - 2.  The
+// host picks the shift s per fixpoint from bounds on every sum the schedule
+// can form (s in {0, 1, 2}: s > 0 only when those sums can reach i64::MAX,
+// so a finite i64::MAX is representable) and checks that the smallest such
+// sum still has a code.  Narrow (int32) lanes are only used with s = 0, when
+// the host has proven every derived sum stays far inside the range, so they
+// need no overflow test.
 template <class W> struct WInf;
-// int32 keeps INT32_MAX free for "absent" in the direct-addressed plan.
 template <> struct WInf<int32_t> { static constexpr int32_t v = 0x7ffffffe; };
-template <> struct WInf<int64_t> { static constexpr int64_t v = 0x7fffffffffffffffll; };
+template <> struct WInf<int64_t> { static constexpr int64_t v = 0x7ffffffffffffffell; };
+template <class W> struct WAbs;
+template <> struct WAbs<int32_t> { static constexpr int32_t v = 0x7fffffff; };
+template <> struct WAbs<int64_t> { static constexpr int64_t v = 0x7fffffffffffffffll; };
+template <class W> struct WFinMax;  // largest finite code
+template <> struct WFinMax<int32_t> { static constexpr int32_t v = 0x7ffffffd; };
+template <> struct WFinMax<int64_t> { static constexpr int64_t v = 0x7ffffffffffffffdll; };
 
-__device__ __forceinline__ int32_t trop_mul(int32_t a, int32_t b, uint32_t* flags) {
+__device__ __forceinline__ int32_t trop_mul(int32_t a, int32_t b, int64_t s, uint32_t* flags) {
   (void)flags;
+  (void)s;
   if (a == WInf<int32_t>::v || b == WInf<int32_t>::v) return WInf<int32_t>::v;
   return a + b;
 }
-// Checked i64 add with +inf absorption (strata-ir/src/trop.rs:52-62).
-__device__ __forceinline__ int64_t trop_mul(int64_t a, int64_t b, uint32_t* flags) {
+// Checked i64 add with +inf absorption (strata-ir/src/trop.rs:52-62) on codes:
+// values a + s and b + s, so the code of their sum is a + b + s.  A sum above
+// i64::MAX (a code above WFinMax) or below i64::MIN is the reference's
+// overflow error.
+__device__ __forceinline__ int64_t trop_mul(int64_t a, int64_t b, int64_t s, uint32_t* flags) {
   if (a == WInf<int64_t>::v || b == WInf<int64_t>::v) return WInf<int64_t>::v;
-  long long r = (long long)((unsigned long long)a + (unsigned long long)b);
-  if (((a ^ r) & (b ^ r)) < 0) {  // signs of both operands differ from the sum
+  const long long as = a + s;  // a <= WFinMax and s <= 2: no wrap
+  const long long r = (long long)((unsigned long long)as + (unsigned long long)b);
+  if ((((as ^ r) & (b ^ r)) < 0) || r > WFinMax<int64_t>::v) {  // wrapped, or past i64::MAX
     *flags |= ST_OVERFLOW;
     return WInf<int64_t>::v;
   }
-  if (r == WInf<int64_t>::v) *flags |= ST_SENTINEL;
   return r;
 }
 

@@ -12,6 +12,7 @@ struct strata_rel {
   int key_bytes = 4;
   int w_bytes = 0;
   int shift = 0;
+  int64_t wshift = 0;  // Trop: finite value = weight code + wshift
   uint64_t n = 0;
   void* keys = nullptr;
   void* w = nullptr;

@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(NT)
                   int pshift, uint64_t pmask, int out_pshift, int out_vshift,
                   const uint32_t* __restrict__ off, uint64_t n_nodes, const uint32_t* __restrict__ nbr,
                   uint64_t n_nbr, const W* __restrict__ nbr_w, K* __restrict__ out, W* __restrict__ out_w,
-                  uint32_t* status) {
+                  int64_t wshift, uint32_t* status) {
   __shared__ uint64_t s_pos[EE_TILE + 1];
   __shared__ uint32_t s_seg[EE_TILE + 1];
   __shared__ K s_kept[EE_TILE + 1];
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(NT)
     if (e >= n_nbr) { flags |= ST_BOUNDS; continue; }
     const uint32_t v = nbr[e];
     out[o] = (K)(((K)s_kept[li] << out_pshift) | ((K)v << out_vshift));
-    if constexpr (TROP) out_w[o] = trop_mul(s_w[li], nbr_w[e], &flags);
+    if constexpr (TROP) out_w[o] = trop_mul(s_w[li], nbr_w[e], wshift, &flags);
   }
   if (flags) atomicOr(status, flags);
 }
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(NT)
     if constexpr (TROP) {
       // Items past clen leave run unchanged; an empty thread contributes
       // the identity {false, +inf}.
-      SegMin<W> agg = (b < clen) ? run : SegMin<W>{false, WInf<W>::v};
+      SegMin<W> agg = (b < clen) ? run : SegMin<W>{false, WAbs<W>::v};
       SegMin<W> inc = agg;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -386,13 +386,13 @@ __global__ void __launch_bounds__(NT)
       }
       if (lane == 31) s_seg[warp] = inc;
       __syncthreads();
-      SegMin<W> wpre{false, WInf<W>::v};
+      SegMin<W> wpre{false, WAbs<W>::v};
       for (int q = 0; q < warp; q++) wpre = seg_combine(wpre, s_seg[q]);
       SegMin<W> ex;
       ex.h = __shfl_up_sync(kFull, inc.h, 1);
       ex.m = __shfl_up_sync(kFull, inc.m, 1);
-      if (lane == 0) ex = SegMin<W>{false, WInf<W>::v};
-      SegMin<W> pre = seg_combine(SegMin<W>{carry_h, carry_h ? carry_m : WInf<W>::v},
+      if (lane == 0) ex = SegMin<W>{false, WAbs<W>::v};
+      SegMin<W> pre = seg_combine(SegMin<W>{carry_h, carry_h ? carry_m : WAbs<W>::v},
                                   seg_combine(wpre, ex));
       // Apply the carry to this thread's items up to its first head.
 #pragma unroll
@@ -403,9 +403,9 @@ __global__ void __launch_bounds__(NT)
         }
       }
       // Carry for the next chunk: the block-inclusive state at the chunk end.
-      SegMin<W> tot{false, WInf<W>::v};
+      SegMin<W> tot{false, WAbs<W>::v};
       for (int q = 0; q < NT / 32; q++) tot = seg_combine(tot, s_seg[q]);
-      SegMin<W> nc = seg_combine(SegMin<W>{carry_h, carry_h ? carry_m : WInf<W>::v}, tot);
+      SegMin<W> nc = seg_combine(SegMin<W>{carry_h, carry_h ? carry_m : WAbs<W>::v}, tot);
       __syncthreads();
       carry_h = nc.h;
       carry_m = nc.m;
@@ -712,10 +712,35 @@ __global__ void k_max_abs_w(const int64_t* __restrict__ w, const uint8_t* __rest
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// Signed range of the finite weights: out[0] = min, out[1] = max (as
+// order-preserving unsigned images, v ^ sign bit), out[2] = 1 if any finite.
+__global__ void k_w_range(const int64_t* __restrict__ w, const uint8_t* __restrict__ inf, uint64_t n,
+                          unsigned long long* out) {
+  unsigned long long lo = ~0ull, hi = 0ull, any = 0ull;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (inf && inf[i]) continue;
+    const unsigned long long u = (unsigned long long)w[i] ^ 0x8000000000000000ull;
+    lo = u < lo ? u : lo;
+    hi = u > hi ? u : hi;
+    any = 1ull;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long a = __shfl_xor_sync(kFull, lo, o), b = __shfl_xor_sync(kFull, hi, o);
+    lo = a < lo ? a : lo;
+    hi = b > hi ? b : hi;
+    any |= __shfl_xor_sync(kFull, any, o);
+  }
+  if ((threadIdx.x & 31) == 0 && any) {
+    atomicMin(&out[0], lo);
+    atomicMax(&out[1], hi);
+    atomicOr(&out[2], 1ull);
+  }
+}
+
 template <class K, class W, bool TROP>
 __global__ void k_pack(const uint32_t* __restrict__ c0, const uint32_t* __restrict__ c1,
                        const int64_t* __restrict__ w, const uint8_t* __restrict__ inf, uint64_t n,
-                       int shift, K* __restrict__ keys, W* __restrict__ ow, uint32_t* status) {
+                       int shift, K* __restrict__ keys, W* __restrict__ ow, int64_t wshift, uint32_t* status) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   keys[i] = (K)((c0 ? ((K)c0[i] << shift) : K(0)) | (K)c1[i]);  // NULL c0: unary key
@@ -725,8 +750,11 @@ __global__ void k_pack(const uint32_t* __restrict__ c0, const uint32_t* __restri
     if (is_inf) {
       ow[i] = WInf<W>::v;
     } else {
-      if ((int64_t)(W)v == (int64_t)WInf<W>::v || (int64_t)(W)v != v) atomicOr(status, ST_SENTINEL);
-      ow[i] = (W)v;
+      // code = v - wshift; it must not wrap and must stay below the reserved codes
+      const bool low = v < INT64_MIN + wshift;
+      const int64_t code = low ? 0 : v - wshift;
+      if (low || code > (int64_t)WFinMax<W>::v || (int64_t)(W)code != code) atomicOr(status, ST_SENTINEL);
+      ow[i] = (W)code;
     }
   }
 }
@@ -734,7 +762,7 @@ __global__ void k_pack(const uint32_t* __restrict__ c0, const uint32_t* __restri
 template <class K, class W, bool TROP>
 __global__ void k_unpack(const K* __restrict__ keys, const W* __restrict__ w, uint64_t n, int shift,
                          uint32_t* __restrict__ c0, uint32_t* __restrict__ c1, int64_t* __restrict__ ow,
-                         uint8_t* __restrict__ oinf) {
+                         uint8_t* __restrict__ oinf, int64_t wshift) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const K k = keys[i];
@@ -744,7 +772,7 @@ __global__ void k_unpack(const K* __restrict__ keys, const W* __restrict__ w, ui
   if constexpr (TROP) {
     const W v = w[i];
     const bool is_inf = v == WInf<W>::v;
-    if (ow) ow[i] = is_inf ? 0 : (int64_t)v;
+    if (ow) ow[i] = is_inf ? 0 : (int64_t)v + wshift;
     if (oinf) oinf[i] = is_inf ? 1 : 0;
   }
 }
@@ -759,7 +787,7 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 
 template <class K, class W, bool TROP>
 __global__ void k_fingerprint(const K* __restrict__ keys, const W* __restrict__ w, uint64_t n, int shift,
-                              unsigned long long* out) {
+                              int64_t wshift, unsigned long long* out) {
   unsigned long long acc = 0;
   const K lowmask = (K)((K(1) << shift) - 1);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -768,7 +796,8 @@ __global__ void k_fingerprint(const K* __restrict__ keys, const W* __restrict__ 
     uint64_t h = mix64((src << 32) | dst);
     if constexpr (TROP) {
       const W v = w[i];
-      const uint64_t wv = v == WInf<W>::v ? 0xfffffffffffffffull : (uint64_t)(int64_t)v;
+      // hash the finite VALUE (code + shift); +inf hashes as a fixed constant
+      const uint64_t wv = v == WInf<W>::v ? 0xfffffffffffffffull : (uint64_t)((int64_t)v + wshift);
       h = mix64(h ^ mix64(wv + 0x51ull));
     }
     acc += h;
@@ -826,7 +855,7 @@ void expand_emit(strata_ctx* ctx, const K* dkeys, const W* dw, uint64_t n, const
   const int kh = kprof_begin(ctx, K_EXPAND_EMIT);
   k_expand_emit<K, W, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(
       dkeys, dw, n, pos, total, jshift, jmask, pshift, pmask, out_pshift, out_vshift, off, n_nodes,
-      nbr, n_nbr, nbr_w, out, out_w, ctx->d_status);
+      nbr, n_nbr, nbr_w, out, out_w, ctx->wshift, ctx->d_status);
   const uint64_t wsz = TROP ? sizeof(W) : 0;
   kprof_end(ctx, kh, n * (sizeof(K) + wsz + 8 + 4) + total * (4 + wsz) + total * (sizeof(K) + wsz));
   after_launch(ctx, "k_expand_emit");
@@ -972,12 +1001,29 @@ uint64_t max_abs_weight(strata_ctx* ctx, const int64_t* w, const uint8_t* inf, u
   return r;
 }
 
+bool weight_range(strata_ctx* ctx, const int64_t* w, const uint8_t* inf, uint64_t n, int64_t* mn, int64_t* mx) {
+  *mn = *mx = 0;
+  if (n == 0) return false;
+  if (!w) return true;  // NULL weights: every fact is Finite(0)
+  DBuf<unsigned long long> r(ctx, 3);
+  const unsigned long long init[3] = {~0ull, 0ull, 0ull};
+  SK_CUDA(cudaMemcpyAsync(r.p, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+  k_w_range<<<grid_for(ctx, n), NT, 0, ctx->stream>>>(w, inf, n, r.p);
+  after_launch(ctx, "k_w_range");
+  uint64_t h[3];
+  read_u64(ctx, reinterpret_cast<uint64_t*>(r.p), h, 3);
+  if (!h[2]) return false;
+  *mn = (int64_t)(h[0] ^ 0x8000000000000000ull);
+  *mx = (int64_t)(h[1] ^ 0x8000000000000000ull);
+  return true;
+}
+
 template <class K, class W, bool TROP>
 void pack_pairs(strata_ctx* ctx, const uint32_t* c0, const uint32_t* c1, const int64_t* w,
                 const uint8_t* inf, uint64_t n, int shift, K* keys, W* ow) {
   if (n == 0) return;
   k_pack<K, W, TROP><<<(unsigned)ceil_div(n, NT), NT, 0, ctx->stream>>>(c0, c1, w, inf, n, shift, keys, ow,
-                                                                       ctx->d_status);
+                                                                       ctx->wshift, ctx->d_status);
   after_launch(ctx, "k_pack");
 }
 
@@ -985,7 +1031,8 @@ template <class K, class W, bool TROP>
 void unpack_pairs(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int shift, uint32_t* c0,
                   uint32_t* c1, int64_t* ow, uint8_t* oinf) {
   if (n == 0) return;
-  k_unpack<K, W, TROP><<<(unsigned)ceil_div(n, NT), NT, 0, ctx->stream>>>(keys, w, n, shift, c0, c1, ow, oinf);
+  k_unpack<K, W, TROP><<<(unsigned)ceil_div(n, NT), NT, 0, ctx->stream>>>(keys, w, n, shift, c0, c1, ow, oinf,
+                                                                         ctx->wshift);
   after_launch(ctx, "k_unpack");
 }
 
@@ -994,7 +1041,7 @@ uint64_t fingerprint(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int
   DBuf<unsigned long long> acc(ctx, 1);
   SK_CUDA(cudaMemsetAsync(acc.p, 0, 8, ctx->stream));
   if (n) {
-    k_fingerprint<K, W, TROP><<<grid_for(ctx, n), NT, 0, ctx->stream>>>(keys, w, n, shift, acc.p);
+    k_fingerprint<K, W, TROP><<<grid_for(ctx, n), NT, 0, ctx->stream>>>(keys, w, n, shift, ctx->wshift, acc.p);
     after_launch(ctx, "k_fingerprint");
   }
   uint64_t r;

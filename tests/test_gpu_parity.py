@@ -160,9 +160,58 @@ def test_trop_pos_inf(peng):
     assert _trop(got) == [(0, 1, 3), (0, 2, 7), (1, 2, 4)]
 
 
-def test_trop_finite_i64_max_is_reported(engine):
+@pytest.mark.parametrize("plan", [0, 1, 2], ids=["auto", "sortmerge", "dense"])
+def test_trop_finite_i64_max_is_a_value(engine, plan):
+    """Finite(i64::MAX) is a legal weight distinct from +inf
+    (strata-ir/src/trop.rs:35-62): it is kept, ⊗ 0 keeps it, ⊗ 1 overflows."""
+    engine.set_plan(plan)
+    try:
+        for edges in ([(0, 1, I64_MAX)], [(0, 1, I64_MAX), (1, 2, 0)],
+                      [(0, 1, I64_MAX - 3), (1, 2, 3), (0, 3, O.POS_INF), (3, 2, 5)],
+                      [(0, 1, I64_MAX), (1, 2, 0), (2, 0, 0)]):
+            s = [e[0] for e in edges]
+            d = [e[1] for e in edges]
+            w = [0 if e[2] == O.POS_INF else e[2] for e in edges]
+            inf = [1 if e[2] == O.POS_INF else 0 for e in edges]
+            want = O.fast_trop(0, s, d, w, np.array(inf, np.uint8))
+            got = engine.shortest_paths_trop(edges)
+            assert _trop(got) == _otrop(want), edges
+            assert got.stats["weight_bytes"] == 8
+        with pytest.raises(S.TropOverflow):
+            engine.shortest_paths_trop([(0, 1, I64_MAX), (1, 2, 1)])
+        # MSSP: a source weight of 1 plus an edge of i64::MAX - 1 is finite i64::MAX
+        got = engine.mssp_trop([0], [(0, 1, I64_MAX - 1), (1, 2, 0)], source_weights=[1])
+        assert _trop(got) == [(0, 1, I64_MAX), (0, 2, I64_MAX)]
+        with pytest.raises(S.TropOverflow):
+            engine.mssp_trop([0], [(0, 1, I64_MAX - 1), (1, 2, 1)], source_weights=[1])
+    finally:
+        engine.set_plan(0)
+
+
+def test_trop_weights_spanning_all_of_i64_are_refused(engine):
+    """Sums that can reach both i64::MIN and i64::MAX within the round cap leave
+    no 64-bit code for +inf: reported, never mixed up."""
     with pytest.raises(S.WeightRange):
-        engine.shortest_paths_trop([(0, 1, I64_MAX)])
+        engine.shortest_paths_trop([(0, 1, I64_MAX), (1, 2, -2**63)])
+
+
+@pytest.mark.parametrize("plan", [0, 1, 2], ids=["auto", "sortmerge", "dense"])
+def test_mssp_wide_lanes_exact(engine, plan):
+    """Weights too large for int32 lanes (U[1, 2^40]) on every plan: exact rows
+    and rounds against the semi-naive restatement."""
+    wl = gen.mssp_workload(scale=13, n_sources=32, seed=17)
+    w = np.random.default_rng(18).integers(1, 1 << 40, len(wl.w), dtype=np.int64)
+    want = O.fast_trop(1, wl.src, wl.dst, w, sources=wl.sources, source_w=wl.source_w)
+    engine.set_plan(plan)
+    try:
+        got = engine.mssp_trop(wl.sources, (wl.src, wl.dst, w), source_weights=wl.source_w)
+    finally:
+        engine.set_plan(0)
+    assert got.stats["weight_bytes"] == 8
+    assert got.stats["plan"] == (1 if plan == 1 else 2)
+    assert np.array_equal(got.src, want[0]) and np.array_equal(got.dst, want[1])
+    assert np.array_equal(got.w, want[2]) and not got.inf.any()
+    assert got.stats["rounds"] == want[4]
 
 
 @pytest.mark.parametrize("scale_w", [100, 10**12])
@@ -487,12 +536,13 @@ def test_plans_pick_and_agree(engine):
     for p in (1, 2):
         assert np.array_equal(res[0].src, res[p].src) and np.array_equal(res[0].dst, res[p].dst)
         assert np.array_equal(res[0].w, res[p].w) and res[0].stats["rounds"] == res[p].stats["rounds"]
-    # wide weights cannot use the int32 index: forcing it is an error, auto falls back
+    # wide weights use the direct-addressed plan with int64 lanes
     engine.set_plan(2)
-    with pytest.raises(S.Unsupported):
-        engine.shortest_paths_trop([(0, 1, 10**13), (1, 2, 1)])
+    got = engine.shortest_paths_trop([(0, 1, 10**13), (1, 2, 1)])
+    assert got.stats["plan"] == 2 and got.stats["weight_bytes"] == 8
+    assert _trop(got) == [(0, 1, 10**13), (0, 2, 10**13 + 1), (1, 2, 1)]
     engine.set_plan(0)
-    assert engine.shortest_paths_trop([(0, 1, 10**13), (1, 2, 1)]).stats["plan"] == 1
+    assert engine.shortest_paths_trop([(0, 1, 10**13), (1, 2, 1)]).stats["plan"] == 2
 
 
 @pytest.mark.parametrize("kb,choices", [(4, (11, 15, 19, 23)), (8, (7, 9, 13))])
