@@ -651,6 +651,23 @@ def run_ours(args):
                      "phase_ms": {k: round(sp_stats[k + "_ms"], 3)
                                   for k in ("setup", "join", "sort", "diff", "merge", "finish")},
                      "kernels": _kernels(sk)}
+    # ---- the same fixpoint in int64 weight lanes (what weights beyond the
+    # int32 proof bound run in), reported beside the headline
+    wide = None
+    if args.workload == "mssp" and args.plan == "auto" and not sharded:
+        eng.set_knob(9, 8)
+        job.free(step()[0])  # warm its buffers
+        eng.set_profiling(True)
+        eng.reset_kernel_stats()
+        wd_ms, wd_tuples, wd_stats = _timed_steps(step, job.free, stream, flush, args.steps, torch)
+        assert wd_tuples == tuples
+        wk = eng.kernel_stats()
+        eng.set_profiling(False)
+        eng.set_knob(9, 0)
+        wide = {"lanes": "int64 weight lanes forced (STRATA_KNOB_WEIGHT_LANES = 8), same plan selection",
+                "plan": {1: "sort-merge", 2: "direct-addressed"}.get(wd_stats["plan"], "?"),
+                "weight_bytes": wd_stats["weight_bytes"], "ms_per_step": wd_ms / args.steps,
+                "value": tuples * args.steps / (wd_ms / 1000.0), "kernels": _kernels(wk)}
     # ---- batched form: the same instances one per launch (host-driven rounds)
     per_launch = None
     if args.workload == "batch":
@@ -765,7 +782,7 @@ def run_ours(args):
                 "key_bits": stats["key_bits"], "weight_bytes": stats["weight_bytes"],
                 "phase_ms": {k: round(stats[k + "_ms"], 3)
                              for k in ("setup", "join", "sort", "diff", "merge", "finish")},
-                "sort_merge_plan": sort_plan})
+                "sort_merge_plan": sort_plan, "wide_lanes": wide})
         print(json.dumps(line), flush=True)
         if args.out:
             Path(args.out).write_text(json.dumps(line) + "\n")

@@ -21,6 +21,10 @@
  *   - Every call runs on the context's stream and returns when its result is
  *     complete.  A context must not be used by two threads at once; separate
  *     contexts are independent (no process-global state).
+ *   - Finite(i64::MAX) is a legal weight.  STRATA_E_WEIGHT_RANGE is returned
+ *     only when the finite weights span nearly all of i64 (sums within the
+ *     round cap could reach both i64::MIN and i64::MAX), where no 64-bit
+ *     code keeps every value apart from +inf.
  *   - Errors are `strata_status` codes; `strata_last_error(ctx)` gives the
  *     message.  The codes map 1:1 onto the reference's error variants:
  *       STRATA_E_OVERFLOW   <- EvalError::Overflow      (strata-eval/src/naive.rs:31)
@@ -48,8 +52,8 @@ typedef enum strata_status {
   STRATA_E_TIMEOUT = 6,      /* a bounded device wait gave up (never a hang) */
   STRATA_E_UNSUPPORTED = 7,  /* rule shape / size outside what the engine runs */
   STRATA_E_NOT_BUILT = 8,    /* no CUDA device visible to this library */
-  STRATA_E_WEIGHT_RANGE = 9  /* a finite weight equal to INT64_MAX reached the
-                                device (its +inf encoding); never silently mixed */
+  STRATA_E_WEIGHT_RANGE = 9  /* finite weights spanning nearly all of i64: no
+                                64-bit code separates them from +inf */
 } strata_status;
 
 typedef struct strata_ctx strata_ctx;
@@ -108,8 +112,10 @@ strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan);
  *   STRATA_KNOB_SORT_RANK           radix digit ranking: 1 per-bit warp ballots, 2 match instruction
  *   STRATA_KNOB_DENSE_WORD_MEMBERS  direct-addressed rounds: Δ words with at least this many
  *                                   members take the bit-lane expand path: 1..33 (33 = never)
+ *   STRATA_KNOB_WEIGHT_LANES        Trop weight lanes: 8 = always int64 (otherwise int32 lanes
+ *                                   are used when every sum within the round cap provably fits)
  * value 0 restores the default (15 / 9 / 2 / 8 / occupancy limit / 70% of
- * reusable memory / ballots / 24).  Other values: STRATA_E_INVALID.
+ * reusable memory / ballots / 24 / automatic).  Other values: STRATA_E_INVALID.
  * The autotuner (strata_b200.tune) sweeps these and caches the best per GPU.
  * No counterpart in the reference (its sort has no tile parameters). */
 #define STRATA_KNOB_SORT_ITEMS_U32 1
@@ -120,6 +126,7 @@ strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan);
 #define STRATA_KNOB_BATCH_BUDGET_MB 6
 #define STRATA_KNOB_SORT_RANK 7
 #define STRATA_KNOB_DENSE_WORD_MEMBERS 8
+#define STRATA_KNOB_WEIGHT_LANES 9
 strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value);
 /* Enable per-phase CUDA-event timing in strata_fix_stats (adds event records). */
 strata_status strata_ctx_set_profiling(strata_ctx* ctx, int enabled);

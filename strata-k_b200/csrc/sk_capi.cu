@@ -223,6 +223,11 @@ strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value) {
     ctx->tune_dense_members = value;
     return STRATA_OK;
   }
+  if (knob == STRATA_KNOB_WEIGHT_LANES) {
+    if (value != 0 && value != 8) return bad(ctx, "weight lanes must be 0 (automatic) or 8 (always int64)");
+    ctx->force_wide = value == 8;
+    return STRATA_OK;
+  }
   if (knob == STRATA_KNOB_TRI_PROBE) {
     if (value < 0 || value > 2) return bad(ctx, "triangle probe must be 0 (default), 1 (hash set) or 2 (binary search)");
     ctx->tune_tri_probe = value;

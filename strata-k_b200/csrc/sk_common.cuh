@@ -87,6 +87,7 @@ struct strata_ctx {
   uint64_t tune_bs_budget_mb = 0;   // cap on a batch wave's device bytes, MiB (0 = 70% of free)
   int tune_dense_members = 0;       // members from which a Δ word takes the bit-lane expand (0 = 24)
   int64_t wshift = 0;               // weight code shift of the running fixpoint (value = code + wshift)
+  bool force_wide = false;          // Trop fixpoints always in int64 lanes (STRATA_KNOB_WEIGHT_LANES = 8)
   bool profiling = false;
   uint64_t launches = 0;
   // Per-kernel CUDA-event accounting (enabled with profiling).

@@ -638,7 +638,7 @@ strata_rel* fix_trop_paths(strata_ctx* ctx, const EdgeCols& e, strata_fix_stats*
   const uint64_t limit = (uint64_t)std::max(max_u32(ctx, e.src, e.n), (uint32_t)(L.n_nodes - 1)) + 1;
   const uint64_t universe = count_distinct_ids(ctx, e.src, e.n, e.dst, e.n, nullptr, 0, limit);
   const uint64_t cap = universe + 2;
-  const bool narrow = narrow_ok(universe, max_abs_weight(ctx, e.w, e.inf, e.n), 0);
+  const bool narrow = !ctx->force_wide && narrow_ok(universe, max_abs_weight(ctx, e.w, e.inf, e.n), 0);
   ctx->wshift = narrow ? 0 : wide_shift(ctx, e.w, e.inf, e.n, nullptr, nullptr, 0, cap);
   const bool dense = want_dense(ctx, true, narrow, L.n_nodes_src, L.n_nodes);
   const uint64_t ns = L.n_nodes_src;
@@ -763,8 +763,8 @@ strata_rel* fix_mssp(strata_ctx* ctx, const uint32_t* sources, const int64_t* sr
   const uint64_t limit = (uint64_t)std::max(mS, std::max(mes, med)) + 1;
   const uint64_t universe = count_distinct_ids(ctx, sources, ns, e.src, e.n, e.dst, e.n, limit);
   const uint64_t cap = universe + 2;
-  const bool narrow = narrow_ok(universe, max_abs_weight(ctx, e.w, e.inf, e.n),
-                                max_abs_weight(ctx, src_w, src_inf, ns));
+  const bool narrow = !ctx->force_wide && narrow_ok(universe, max_abs_weight(ctx, e.w, e.inf, e.n),
+                                                    max_abs_weight(ctx, src_w, src_inf, ns));
   ctx->wshift = narrow ? 0 : wide_shift(ctx, e.w, e.inf, e.n, src_w, src_inf, ns, cap);
   const uint64_t nn = (uint64_t)mes + 1;
   const uint64_t n0 = (uint64_t)mS + 1, n1 = (uint64_t)med + 1;

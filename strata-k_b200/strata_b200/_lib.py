@@ -31,6 +31,7 @@ KNOB_SORT_ITEMS_U32, KNOB_SORT_ITEMS_U64, KNOB_TRI_PROBE = 1, 2, 3
 KNOB_BATCH_GRAPH_ROUNDS, KNOB_BATCH_BLOCKS_PER_SM, KNOB_BATCH_BUDGET_MB = 4, 5, 6
 KNOB_SORT_RANK = 7
 KNOB_DENSE_WORD_MEMBERS = 8
+KNOB_WEIGHT_LANES = 9
 
 KERNELS = {0: "k_onesweep", 1: "k_expand_emit", 2: "k_expand_offsets", 3: "k_reduce_runs",
            4: "k_merge_diff", 5: "k_radix_hist", 6: "k_tri_count", 7: "k_expand_dense",

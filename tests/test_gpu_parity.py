@@ -188,6 +188,23 @@ def test_trop_finite_i64_max_is_a_value(engine, plan):
         engine.set_plan(0)
 
 
+def test_weight_lanes_knob_forces_int64_with_identical_results(engine):
+    wl = gen.mssp_workload(scale=12, n_sources=16, seed=19)
+    narrow = engine.mssp_trop(wl.sources, (wl.src, wl.dst, wl.w), source_weights=wl.source_w)
+    engine.set_knob(9, 8)
+    try:
+        wide = engine.mssp_trop(wl.sources, (wl.src, wl.dst, wl.w), source_weights=wl.source_w)
+    finally:
+        engine.set_knob(9, 0)
+    assert narrow.stats["weight_bytes"] == 4 and wide.stats["weight_bytes"] == 8
+    assert wide.stats["plan"] == narrow.stats["plan"] == 2
+    for a in ("src", "dst", "w", "inf"):
+        assert np.array_equal(getattr(narrow, a), getattr(wide, a))
+    assert narrow.stats["rounds"] == wide.stats["rounds"]
+    with pytest.raises(S.InvalidArgument):
+        engine.set_knob(9, 4)
+
+
 def test_trop_weights_spanning_all_of_i64_are_refused(engine):
     """Sums that can reach both i64::MIN and i64::MAX within the round cap leave
     no 64-bit code for +inf: reported, never mixed up."""
