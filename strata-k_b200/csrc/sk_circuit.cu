@@ -12,15 +12,25 @@
 //
 // Kernels (one thread block per query circuit, levels separated by block
 // barriers):
-//   forward  — node values in FP32: Leaf p, NegLeaf 1-p, And product, Or sum
-//              (circuit.rs:43-63); the root's own sum/product is formed in
-//              FP64 from its FP32 children;
+//   forward  — node values: Leaf p, NegLeaf 1-p, And product, Or sum
+//              (circuit.rs:43-63), each a compensated pair of FP32 values
+//              (float-float: an unevaluated sum hi + lo, kept exact to about
+//              2^-44 relative by the error-free TwoSum and FMA-based
+//              TwoProduct transformations, Dekker 1971 / Knuth TAOCP 4.2.2);
+//              the root's own sum/product is formed in FP64 from its
+//              children's pairs;
 //   adjoint  — reverse sweep from a per-query seed: And children receive
 //              g · Π(siblings) (siblings' product formed without the child,
 //              exact when a child is zero), Or children g, Leaf += g,
-//              NegLeaf -= g (circuit.rs:68-106); node adjoints in FP32,
-//              leaf gradients accumulated in FP64, where the +g/-g
-//              contributions of a decision variable cancel.
+//              NegLeaf -= g (circuit.rs:68-106); node adjoints in FP32.
+//              A Leaf / NegLeaf child of an And takes g times its sibling's
+//              float-float value straight into its FP64 leaf gradient: the
+//              leaf's gradient from a decision node is g·(hi − lo), the
+//              difference of the two cofactors, and plain FP32 cofactor
+//              values lose most of their digits in that difference when the
+//              cofactors are close.  Every other term of a gradient is
+//              non-negative for the monotone proof DNFs here, so the FP32
+//              adjoints add no cancellation of their own.
 // A vector-Jacobian product (seeds = dL/dP per query, one leaf-gradient
 // vector) serves torch.autograd; per-query gradient rows serve `?grad`.
 #include "sk_ops.cuh"
@@ -156,6 +166,37 @@ struct Compiler {
 
 constexpr int CK_NT = 256;
 
+// ---- float-float arithmetic (a value is the unevaluated sum hi + lo) -------
+struct ff {
+  float hi, lo;
+};
+// Knuth's TwoSum: s + e == a + b exactly.
+__device__ __forceinline__ ff ff_two_sum(float a, float b) {
+  const float s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  const float e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  return ff{s, e};
+}
+// Dekker's FastTwoSum (|a| >= |b|): s + e == a + b exactly.
+__device__ __forceinline__ ff ff_fast_two_sum(float a, float b) {
+  const float s = __fadd_rn(a, b);
+  return ff{s, __fsub_rn(b, __fsub_rn(s, a))};
+}
+__device__ __forceinline__ ff ff_add(ff x, ff y) {
+  ff s = ff_two_sum(x.hi, y.hi);
+  const float e = __fadd_rn(s.lo, __fadd_rn(x.lo, y.lo));
+  return ff_fast_two_sum(s.hi, e);
+}
+// TwoProduct with an FMA: p + e == a * b exactly.
+__device__ __forceinline__ ff ff_mul(ff x, ff y) {
+  const float p = __fmul_rn(x.hi, y.hi);
+  const float e = __fmaf_rn(x.hi, y.hi, -p);
+  const float t = __fadd_rn(e, __fadd_rn(__fmul_rn(x.hi, y.lo), __fmul_rn(x.lo, y.hi)));
+  return ff_fast_two_sum(p, t);
+}
+__device__ __forceinline__ ff ff_load(const strata_circuits& c, uint64_t i) { return ff{c.val[i], c.val_lo[i]}; }
+__device__ __forceinline__ double ff_to_f64(ff x) { return (double)x.hi + (double)x.lo; }
+
 __global__ void __launch_bounds__(CK_NT) k_circuit_forward(strata_circuits c, const float* __restrict__ p,
                                                            float* out32, double* out64) {
   const uint32_t q = blockIdx.x;
@@ -165,34 +206,35 @@ __global__ void __launch_bounds__(CK_NT) k_circuit_forward(strata_circuits c, co
     const uint64_t a = n0 + c.lvl[L], b = n0 + c.lvl[L + 1];
     for (uint64_t i = a + threadIdx.x; i < b; i += CK_NT) {
       const uint8_t kd = c.kind[i];
-      float x;
+      ff x;
       if (kd == 0) {
-        x = p[c.a[i]];
+        x = ff{p[c.a[i]], 0.0f};
       } else if (kd == 1) {
-        x = 1.0f - p[c.a[i]];
+        x = ff_two_sum(1.0f, -p[c.a[i]]);  // 1 - p, exactly
       } else if (kd == 2) {
-        x = 1.0f;
-        for (uint32_t j = 0; j < c.b[i]; j++) x = x * c.val[c.ch[c.a[i] + j]];
+        x = ff{1.0f, 0.0f};
+        for (uint32_t j = 0; j < c.b[i]; j++) x = ff_mul(x, ff_load(c, c.ch[c.a[i] + j]));
       } else if (kd == 3) {
-        x = 0.0f;
-        for (uint32_t j = 0; j < c.b[i]; j++) x = x + c.val[c.ch[c.a[i] + j]];
+        x = ff{0.0f, 0.0f};
+        for (uint32_t j = 0; j < c.b[i]; j++) x = ff_add(x, ff_load(c, c.ch[c.a[i] + j]));
       } else {
-        x = kd == 4 ? 1.0f : 0.0f;
+        x = ff{kd == 4 ? 1.0f : 0.0f, 0.0f};
       }
-      c.val[i] = x;
+      c.val[i] = x.hi;
+      c.val_lo[i] = x.lo;
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     const uint32_t r = c.root[q];
     const uint8_t kd = c.kind[r];
-    double x = (double)c.val[r];
+    double x = ff_to_f64(ff_load(c, r));
     if (kd == 2) {
       x = 1.0;
-      for (uint32_t j = 0; j < c.b[r]; j++) x = x * (double)c.val[c.ch[c.a[r] + j]];
+      for (uint32_t j = 0; j < c.b[r]; j++) x = x * ff_to_f64(ff_load(c, c.ch[c.a[r] + j]));
     } else if (kd == 3) {
       x = 0.0;
-      for (uint32_t j = 0; j < c.b[r]; j++) x = x + (double)c.val[c.ch[c.a[r] + j]];
+      for (uint32_t j = 0; j < c.b[r]; j++) x = x + ff_to_f64(ff_load(c, c.ch[c.a[r] + j]));
     }
     if (out32) out32[q] = (float)x;
     if (out64) out64[q] = x;
@@ -224,10 +266,23 @@ __global__ void __launch_bounds__(CK_NT) k_circuit_adjoint(strata_circuits c, co
       } else if (kd == 2) {
         const uint32_t f = c.a[i], nc = c.b[i];
         for (uint32_t j = 0; j < nc; j++) {
-          float sib = 1.0f;
-          for (uint32_t k = 0; k < nc; k++)
-            if (k != j) sib = sib * c.val[c.ch[f + k]];
-          atomicAdd(&c.adj[c.ch[f + j]], gi * sib);
+          const uint32_t cj = c.ch[f + j];
+          const uint8_t kj = c.kind[cj];
+          if (kj == 0 || kj == 1) {
+            // a leaf child: its gradient term in FP64 from the siblings'
+            // float-float product (no FP32 rounding before the cofactor
+            // difference forms in the leaf's sum)
+            ff sib{1.0f, 0.0f};
+            for (uint32_t k = 0; k < nc; k++)
+              if (k != j) sib = ff_mul(sib, ff_load(c, c.ch[f + k]));
+            const double t = (double)gi * ff_to_f64(sib);
+            atomicAdd(&g_out[c.a[cj]], kj == 0 ? t : -t);
+          } else {
+            float sib = 1.0f;
+            for (uint32_t k = 0; k < nc; k++)
+              if (k != j) sib = sib * c.val[c.ch[f + k]];
+            atomicAdd(&c.adj[cj], gi * sib);
+          }
         }
       } else if (kd == 3) {
         const uint32_t f = c.a[i], nc = c.b[i];
@@ -392,6 +447,7 @@ strata_circuits* circuits_upload(strata_ctx* ctx, const std::vector<const std::v
     c->qlevel = dev_upload(ctx, qlevel);
     c->lvl = dev_upload(ctx, lvl);
     c->val = static_cast<float*>(dev_alloc(ctx, std::max<uint64_t>(1, c->n_nodes) * 4));
+    c->val_lo = static_cast<float*>(dev_alloc(ctx, std::max<uint64_t>(1, c->n_nodes) * 4));
     c->adj = static_cast<float*>(dev_alloc(ctx, std::max<uint64_t>(1, c->n_nodes) * 4));
     sync_and_check(ctx);
   } catch (...) {
@@ -476,7 +532,7 @@ strata_circuits* circuit_parts_upload(strata_ctx* ctx, uint32_t n_parts, Circuit
 void circuits_free(strata_ctx* ctx, strata_circuits* c) {
   if (!c) return;
   for (void* p : {(void*)c->kind, (void*)c->a, (void*)c->b, (void*)c->ch, (void*)c->qnode, (void*)c->root,
-                  (void*)c->qlevel, (void*)c->lvl, (void*)c->val, (void*)c->adj})
+                  (void*)c->qlevel, (void*)c->lvl, (void*)c->val, (void*)c->val_lo, (void*)c->adj})
     if (p) dev_free(ctx, p);
   delete c;
 }

@@ -34,7 +34,8 @@ struct strata_circuits {
   uint32_t* root = nullptr;     // root node of query q (global index)
   uint64_t* qlevel = nullptr;   // first level of query q in `lvl` (n_queries + 1)
   uint32_t* lvl = nullptr;      // level boundaries: node offsets relative to qnode[q]
-  float* val = nullptr;         // forward values
+  float* val = nullptr;         // forward values: high parts of the float-float pairs
+  float* val_lo = nullptr;      // forward values: low parts (value = val + val_lo)
   float* adj = nullptr;         // adjoints
   uint64_t n_children = 0;
 };

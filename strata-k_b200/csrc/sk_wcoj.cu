@@ -202,7 +202,7 @@ __global__ void k_k4_warp(const uint32_t* __restrict__ off, const uint32_t* __re
     if (du <= d_lo || du > d_hi || du < 3) continue;
     for (uint32_t k = lane; k < du; k += 32) A[k] = nbr[a0 + k];
     __syncwarp();
-    for (uint32_t i = 0; i + 2 < du; i++) {  // v = A[i]; two more members are needed after it
+    for (uint32_t i = 0; i < du; i++) {  // v = A[i] (lists are in id order, not rank order)
       const uint32_t v = A[i];
       if (v >= n_nodes) continue;
       const uint32_t v0 = off[v], dv = off[v + 1] - v0;
