@@ -421,6 +421,58 @@ strata_status strata_op_min_improve(strata_ctx* ctx, int key_bytes,
     const void* d_full, int64_t* d_full_w, uint64_t n_full,
     void* d_out_keys, int64_t* d_out_w, uint64_t* out_n);
 
+/* ⊕-combine a batch of derivations (Relation::combine, store.rs:34-48): from
+ * sorted keys with duplicates, one row per key — Bool: the distinct keys;
+ * Trop (d_w given): the minimum weight.  *out_n = distinct keys (capacity n). */
+strata_status strata_op_reduce(strata_ctx* ctx, int key_bytes, const void* d_keys, const int64_t* d_w, uint64_t n,
+    void* d_out, int64_t* d_out_w, uint64_t* out_n);
+
+/* Apply a round's reduced derivations to a relation and take the next Δ
+ * (apply_round, seminaive.rs:183-208): full_out = full ⊕ cand (Bool union;
+ * Trop min per key), delta = the keys of cand new to full (Trop: or strictly
+ * below full's weight) with their merged values.  Both inputs sorted and
+ * unique; capacities n_full + n_cand (full_out) and n_cand (delta). */
+strata_status strata_op_merge_diff(strata_ctx* ctx, int key_bytes, const void* d_full, const int64_t* d_full_w,
+    uint64_t n_full, const void* d_cand, const int64_t* d_cand_w, uint64_t n_cand,
+    void* d_full_out, int64_t* d_full_out_w, void* d_delta, int64_t* d_delta_w,
+    uint64_t* out_full_n, uint64_t* out_delta_n);
+
+/* One binary rule body  h(X,Z) :- a(X,Y), b(Y,Z)  (`solve` over two atoms,
+ * strata-eval/src/seminaive.rs:215-298, with the head built as (X, Z),
+ * `build_head` naive.rs:526).  a = (X << a_shift) | Y in any order (a Δ, or
+ * a full relation); b = (Y << b_shift) | Z sorted ascending (strata_op_sort).
+ * Every binding is written as (X << out_shift) | Z, in a's order, unsorted
+ * and with duplicates; with weights (both d_aw and d_bw, int64, INT64_MAX =
+ * +inf) the output weight is the Trop product (checked i64 add,
+ * STRATA_E_OVERFLOW; Ann::otimes, value.rs:56).  *out_n receives the binding
+ * count; pass d_out = NULL to size the output first.  out_cap below the
+ * count is STRATA_E_INVALID (nothing written).  Shifts lie in [1, key bits);
+ * the caller picks out_shift so the output keys fit.  Finite weights on this
+ * surface are at most INT64_MAX - 2 (STRATA_E_WEIGHT_RANGE otherwise). */
+strata_status strata_op_join(strata_ctx* ctx, int key_bytes, const void* d_a, const int64_t* d_aw, uint64_t na,
+    int a_shift, const void* d_b, const int64_t* d_bw, uint64_t nb, int b_shift, int out_shift,
+    void* d_out, int64_t* d_out_w, uint64_t out_cap, uint64_t* out_n);
+
+/* The head of a one-atom body (`build_head`, strata-eval/src/naive.rs:526):
+ * out[i] = (col(sel_hi) << out_shift) | col(sel_lo) with col 0 = c0 =
+ * key >> in_shift, 1 = c1 = the low in_shift bits, 2 = the constant const_hi
+ * / const_lo; sel_hi = 3 writes col(sel_lo) alone (a unary head).  A unary
+ * input uses in_shift = its key bits (the whole key is c1).  Output keys
+ * keep the input order: sort + dedup them for the head relation. */
+strata_status strata_op_project(strata_ctx* ctx, int key_bytes_in, const void* d_in, uint64_t n, int in_shift,
+    int sel_hi, int sel_lo, uint64_t const_hi, uint64_t const_lo, int key_bytes_out, int out_shift, void* d_out);
+
+/* Aggregate rule  H(G, agg<V>) :- body  (`eval_aggregate_rule` +
+ * `fold_aggregate`, strata-eval/src/naive.rs:300-391) over its bindings as
+ * sorted keys: the group of a binding is key >> group_shift (group_shift =
+ * key bits: one group).  op 0 = count (the number of bindings per group),
+ * 1 = sum (wrapping i64), 2 = min, 3 = max of d_vals (one int64 aggregand per
+ * binding; unused for count).  Writes the distinct groups ascending to
+ * d_groups and their results to d_out (capacity n each); *out_n = groups.
+ * Unsorted keys: STRATA_E_CUDA (a bounds status), nothing written. */
+strata_status strata_op_aggregate(strata_ctx* ctx, int key_bytes, const void* d_keys, const int64_t* d_vals,
+    uint64_t n, int group_shift, int op, void* d_groups, int64_t* d_out, uint64_t* out_n);
+
 /* Merge two sorted, disjoint key runs (with optional int64 weights) into out. */
 strata_status strata_op_merge(strata_ctx* ctx, int key_bytes,
     const void* d_a, const int64_t* d_aw, uint64_t na,

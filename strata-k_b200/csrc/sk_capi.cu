@@ -916,6 +916,141 @@ strata_status strata_op_min_improve(strata_ctx* ctx, int key_bytes, const void* 
   SK_GUARD_END(ctx)
 }
 
+strata_status strata_op_reduce(strata_ctx* ctx, int key_bytes, const void* d_keys, const int64_t* d_w, uint64_t n,
+                               void* d_out, int64_t* d_out_w, uint64_t* out_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  if (!out_n || (n && (!d_keys || !d_out || (d_w && !d_out_w)))) return bad(ctx, "NULL argument");
+  if (n > sk::kMaxSortN) return bad(ctx, "n is limited to 2^30 - 1 per call");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  DBuf<uint64_t> cnt(ctx, 1);
+  if (key_bytes == 4) {
+    if (d_w) sk::reduce_runs<uint32_t, int64_t, true>(ctx, (const uint32_t*)d_keys, d_w, n, (uint32_t*)d_out, d_out_w, cnt.p);
+    else sk::reduce_runs<uint32_t, int32_t, false>(ctx, (const uint32_t*)d_keys, nullptr, n, (uint32_t*)d_out, nullptr, cnt.p);
+  } else {
+    if (d_w) sk::reduce_runs<uint64_t, int64_t, true>(ctx, (const uint64_t*)d_keys, d_w, n, (uint64_t*)d_out, d_out_w, cnt.p);
+    else sk::reduce_runs<uint64_t, int32_t, false>(ctx, (const uint64_t*)d_keys, nullptr, n, (uint64_t*)d_out, nullptr, cnt.p);
+  }
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, cnt.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  sk::sync_and_check(ctx);
+  *out_n = ctx->h_scalar[0];
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_op_merge_diff(strata_ctx* ctx, int key_bytes, const void* d_full, const int64_t* d_full_w,
+                                   uint64_t n_full, const void* d_cand, const int64_t* d_cand_w, uint64_t n_cand,
+                                   void* d_full_out, int64_t* d_full_out_w, void* d_delta, int64_t* d_delta_w,
+                                   uint64_t* out_full_n, uint64_t* out_delta_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  const bool trop = d_cand_w != nullptr;
+  if (!out_full_n || !out_delta_n || (n_full && !d_full) || (n_cand && !d_cand) || !d_full_out || !d_delta)
+    return bad(ctx, "NULL argument");
+  if (trop && ((n_full && !d_full_w) || !d_full_out_w || !d_delta_w)) return bad(ctx, "NULL weight column");
+  if (n_full + n_cand > sk::kMaxSortN) return bad(ctx, "n is limited to 2^30 - 1 per call");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  DBuf<uint64_t> cnt(ctx, 2);
+  if (key_bytes == 4) {
+    if (trop) sk::merge_diff<uint32_t, int64_t, true>(ctx, (const uint32_t*)d_full, d_full_w, n_full, (const uint32_t*)d_cand,
+                                                      d_cand_w, n_cand, (uint32_t*)d_full_out, d_full_out_w,
+                                                      (uint32_t*)d_delta, d_delta_w, cnt.p);
+    else sk::merge_diff<uint32_t, int32_t, false>(ctx, (const uint32_t*)d_full, nullptr, n_full, (const uint32_t*)d_cand,
+                                                  nullptr, n_cand, (uint32_t*)d_full_out, nullptr, (uint32_t*)d_delta,
+                                                  nullptr, cnt.p);
+  } else {
+    if (trop) sk::merge_diff<uint64_t, int64_t, true>(ctx, (const uint64_t*)d_full, d_full_w, n_full, (const uint64_t*)d_cand,
+                                                      d_cand_w, n_cand, (uint64_t*)d_full_out, d_full_out_w,
+                                                      (uint64_t*)d_delta, d_delta_w, cnt.p);
+    else sk::merge_diff<uint64_t, int32_t, false>(ctx, (const uint64_t*)d_full, nullptr, n_full, (const uint64_t*)d_cand,
+                                                  nullptr, n_cand, (uint64_t*)d_full_out, nullptr, (uint64_t*)d_delta,
+                                                  nullptr, cnt.p);
+  }
+  SK_CUDA(cudaMemcpyAsync(ctx->h_scalar, cnt.p, 16, cudaMemcpyDeviceToHost, ctx->stream));
+  sk::sync_and_check(ctx);
+  *out_full_n = ctx->h_scalar[0];
+  *out_delta_n = ctx->h_scalar[1];
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_op_join(strata_ctx* ctx, int key_bytes, const void* d_a, const int64_t* d_aw, uint64_t na,
+                             int a_shift, const void* d_b, const int64_t* d_bw, uint64_t nb, int b_shift, int out_shift,
+                             void* d_out, int64_t* d_out_w, uint64_t out_cap, uint64_t* out_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  const int kbits = 8 * key_bytes;
+  if (a_shift < 1 || a_shift >= kbits || b_shift < 1 || b_shift >= kbits || out_shift < 1 || out_shift >= kbits)
+    return bad(ctx, "column shifts must lie in [1, key bits)");
+  if (!out_n || (na && !d_a) || (nb && !d_b)) return bad(ctx, "NULL argument");
+  if ((d_aw == nullptr) != (d_bw == nullptr)) return bad(ctx, "weights for both inputs or for neither");
+  if (d_out && d_aw && !d_out_w) return bad(ctx, "Trop join needs an output weight column");
+  if (na > sk::kMaxSortN || nb > sk::kMaxSortN) return bad(ctx, "n is limited to 2^30 - 1 per call");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  bool written = false;
+  uint64_t t;
+  if (key_bytes == 4)
+    t = sk::op_join<uint32_t>(ctx, (const uint32_t*)d_a, d_aw, na, a_shift, (const uint32_t*)d_b, d_bw, nb, b_shift,
+                              out_shift, (uint32_t*)d_out, d_out_w, out_cap, &written);
+  else
+    t = sk::op_join<uint64_t>(ctx, (const uint64_t*)d_a, d_aw, na, a_shift, (const uint64_t*)d_b, d_bw, nb, b_shift,
+                              out_shift, (uint64_t*)d_out, d_out_w, out_cap, &written);
+  *out_n = t;
+  if (d_out && !written) return bad(ctx, "output capacity below the binding count (returned in *out_n)");
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_op_project(strata_ctx* ctx, int key_bytes_in, const void* d_in, uint64_t n, int in_shift,
+                                int sel_hi, int sel_lo, uint64_t const_hi, uint64_t const_lo, int key_bytes_out,
+                                int out_shift, void* d_out) {
+  if (!ctx) return STRATA_E_INVALID;
+  if ((key_bytes_in != 4 && key_bytes_in != 8) || (key_bytes_out != 4 && key_bytes_out != 8))
+    return bad(ctx, "key bytes must be 4 or 8");
+  if (sel_lo < 0 || sel_lo > 2 || sel_hi < 0 || sel_hi > 3) return bad(ctx, "column selectors: 0 c0, 1 c1, 2 constant (3: none, hi only)");
+  if (in_shift < 0 || in_shift > 8 * key_bytes_in) return bad(ctx, "in_shift outside [0, key bits]");
+  if (sel_hi != 3 && (out_shift < 1 || out_shift >= 8 * key_bytes_out)) return bad(ctx, "out_shift outside [1, key bits)");
+  if (n && (!d_in || !d_out)) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  if (key_bytes_in == 4 && key_bytes_out == 4)
+    sk::op_project<uint32_t, uint32_t>(ctx, (const uint32_t*)d_in, n, in_shift, sel_hi, sel_lo, const_hi, const_lo,
+                                       out_shift, (uint32_t*)d_out);
+  else if (key_bytes_in == 4)
+    sk::op_project<uint32_t, uint64_t>(ctx, (const uint32_t*)d_in, n, in_shift, sel_hi, sel_lo, const_hi, const_lo,
+                                       out_shift, (uint64_t*)d_out);
+  else if (key_bytes_out == 4)
+    sk::op_project<uint64_t, uint32_t>(ctx, (const uint64_t*)d_in, n, in_shift, sel_hi, sel_lo, const_hi, const_lo,
+                                       out_shift, (uint32_t*)d_out);
+  else
+    sk::op_project<uint64_t, uint64_t>(ctx, (const uint64_t*)d_in, n, in_shift, sel_hi, sel_lo, const_hi, const_lo,
+                                       out_shift, (uint64_t*)d_out);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_op_aggregate(strata_ctx* ctx, int key_bytes, const void* d_keys, const int64_t* d_vals,
+                                  uint64_t n, int group_shift, int op, void* d_groups, int64_t* d_out, uint64_t* out_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  if (op < 0 || op > 3) return bad(ctx, "op must be 0 count, 1 sum, 2 min or 3 max");
+  if (group_shift < 0 || group_shift > 8 * key_bytes) return bad(ctx, "group_shift outside [0, key bits]");
+  if (!out_n || (n && (!d_keys || !d_groups || !d_out || (op && !d_vals)))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  if (key_bytes == 4)
+    *out_n = sk::op_aggregate<uint32_t>(ctx, (const uint32_t*)d_keys, d_vals, n, group_shift, op, (uint32_t*)d_groups,
+                                        d_out);
+  else
+    *out_n = sk::op_aggregate<uint64_t>(ctx, (const uint64_t*)d_keys, d_vals, n, group_shift, op, (uint64_t*)d_groups,
+                                        d_out);
+  SK_GUARD_END(ctx)
+}
+
 strata_status strata_op_merge(strata_ctx* ctx, int key_bytes, const void* d_a, const int64_t* d_aw, uint64_t na,
                               const void* d_b, const int64_t* d_bw, uint64_t nb, void* d_out, int64_t* d_out_w) {
   if (!ctx) return STRATA_E_INVALID;

@@ -185,4 +185,25 @@ uint64_t max_abs_weight(strata_ctx* ctx, const int64_t* w, const uint8_t* inf, u
 template <class K, class W, bool TROP>
 uint64_t fingerprint(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int shift);
 
+// ---- operator surface (sk_opsurf.cu) ----
+// One binary body  h(X,Z) :- a(X,Y), b(Y,Z):  a = (X << d_shift) | Y (any
+// order), b = (Y << r_shift) | Z sorted ascending; output (X << out_shift) | Z
+// with ⊗ weights (Trop when dw != NULL; int64, INT64_MAX = +inf) in a's
+// order.  Returns the binding count; writes only when out != NULL and
+// out_cap >= count (*written says whether it did).
+template <class K>
+uint64_t op_join(strata_ctx* ctx, const K* dk, const int64_t* dw, uint64_t nd, int d_shift, const K* rk,
+                 const int64_t* rw, uint64_t nr, int r_shift, int out_shift, K* out, int64_t* out_w, uint64_t out_cap,
+                 bool* written);
+// out[i] = (col(sel_hi) << out_shift) | col(sel_lo), col 0 = c0, 1 = c1,
+// 2 = the constant; sel_hi 3 = a one-column output (col(sel_lo) alone).
+template <class KI, class KO>
+void op_project(strata_ctx* ctx, const KI* in, uint64_t n, int in_shift, int sel_hi, int sel_lo, uint64_t const_hi,
+                uint64_t const_lo, int out_shift, KO* out);
+// Groups key >> gshift of sorted keys with count / sum / min / max (op 0..3)
+// of vals; returns the number of groups.
+template <class K>
+uint64_t op_aggregate(strata_ctx* ctx, const K* keys, const int64_t* vals, uint64_t n, int gshift, int op, K* groups,
+                      int64_t* out_vals);
+
 }  // namespace sk

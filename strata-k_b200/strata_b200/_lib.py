@@ -177,6 +177,15 @@ SIGNATURES = {
     "strata_op_min_improve": (
         C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp, u64p]),
     "strata_op_merge": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp]),
+    "strata_op_reduce": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.POINTER(C.c_uint64)]),
+    "strata_op_merge_diff": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp, vp, vp,
+                                       C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "strata_op_join": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, C.c_int, vp, vp, C.c_uint64, C.c_int, C.c_int,
+                                 vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "strata_op_project": (C.c_int, [ctxp, C.c_int, vp, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_uint64,
+                                    C.c_uint64, C.c_int, C.c_int, vp]),
+    "strata_op_aggregate": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, C.c_int, C.c_int, vp, vp,
+                                      C.POINTER(C.c_uint64)]),
     "strata_sort_u32_noalloc": (C.c_int, [vp, vp, C.c_uint64, C.c_int, vp]),
 }
 
