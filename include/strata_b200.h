@@ -437,6 +437,21 @@ strata_status strata_op_merge_diff(strata_ctx* ctx, int key_bytes, const void* d
     void* d_full_out, int64_t* d_full_out_w, void* d_delta, int64_t* d_delta_w,
     uint64_t* out_full_n, uint64_t* out_delta_n);
 
+/* Scan with unification (`unify`, strata-eval/src/naive.rs:407-455) for an
+ * atom with a repeated variable or a constant: the rows of packed keys
+ * (c0 << shift) | c1 with c0 == c1 (mode 0), c0 == value (mode 1) or
+ * c1 == value (mode 2), in input order, weights carried (optional).
+ * *out_n = rows kept (capacity n). */
+strata_status strata_op_select(strata_ctx* ctx, int key_bytes, const void* d_in, const int64_t* d_w, uint64_t n,
+    int shift, int mode, uint64_t value, void* d_out, int64_t* d_out_w, uint64_t* out_n);
+
+/* Two atoms over the same variables, p(X,Y), q(X,Y) (`solve` binding both
+ * columns): the keys of a (any order) that are in b (sorted ascending), in
+ * a's order; with weights on both, the Trop product (INT64_MAX = +inf,
+ * STRATA_E_OVERFLOW on a finite sum past i64).  *out_n = rows kept. */
+strata_status strata_op_intersect(strata_ctx* ctx, int key_bytes, const void* d_a, const int64_t* d_aw, uint64_t na,
+    const void* d_b, const int64_t* d_bw, uint64_t nb, void* d_out, int64_t* d_out_w, uint64_t* out_n);
+
 /* One binary rule body  h(X,Z) :- a(X,Y), b(Y,Z)  (`solve` over two atoms,
  * strata-eval/src/seminaive.rs:215-298, with the head built as (X, Z),
  * `build_head` naive.rs:526).  a = (X << a_shift) | Y in any order (a Δ, or

@@ -976,6 +976,42 @@ strata_status strata_op_merge_diff(strata_ctx* ctx, int key_bytes, const void* d
   SK_GUARD_END(ctx)
 }
 
+strata_status strata_op_select(strata_ctx* ctx, int key_bytes, const void* d_in, const int64_t* d_w, uint64_t n,
+                               int shift, int mode, uint64_t value, void* d_out, int64_t* d_out_w, uint64_t* out_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  if (mode < 0 || mode > 2) return bad(ctx, "mode must be 0 (c0 == c1), 1 (c0 == value) or 2 (c1 == value)");
+  if (shift < 0 || shift > 8 * key_bytes) return bad(ctx, "shift outside [0, key bits]");
+  if (!out_n || (n && (!d_in || !d_out || (d_w && !d_out_w)))) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  if (key_bytes == 4)
+    *out_n = sk::op_select<uint32_t>(ctx, (const uint32_t*)d_in, d_w, n, shift, mode, value, (uint32_t*)d_out, d_out_w);
+  else
+    *out_n = sk::op_select<uint64_t>(ctx, (const uint64_t*)d_in, d_w, n, shift, mode, value, (uint64_t*)d_out, d_out_w);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_op_intersect(strata_ctx* ctx, int key_bytes, const void* d_a, const int64_t* d_aw, uint64_t na,
+                                  const void* d_b, const int64_t* d_bw, uint64_t nb, void* d_out, int64_t* d_out_w,
+                                  uint64_t* out_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  if ((d_aw == nullptr) != (d_bw == nullptr)) return bad(ctx, "weights for both inputs or for neither");
+  if (!out_n || (na && (!d_a || !d_out || (d_aw && !d_out_w))) || (nb && !d_b)) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  if (key_bytes == 4)
+    *out_n = sk::op_intersect<uint32_t>(ctx, (const uint32_t*)d_a, d_aw, na, (const uint32_t*)d_b, d_bw, nb,
+                                        (uint32_t*)d_out, d_out_w);
+  else
+    *out_n = sk::op_intersect<uint64_t>(ctx, (const uint64_t*)d_a, d_aw, na, (const uint64_t*)d_b, d_bw, nb,
+                                        (uint64_t*)d_out, d_out_w);
+  SK_GUARD_END(ctx)
+}
+
 strata_status strata_op_join(strata_ctx* ctx, int key_bytes, const void* d_a, const int64_t* d_aw, uint64_t na,
                              int a_shift, const void* d_b, const int64_t* d_bw, uint64_t nb, int b_shift, int out_shift,
                              void* d_out, int64_t* d_out_w, uint64_t out_cap, uint64_t* out_n) {

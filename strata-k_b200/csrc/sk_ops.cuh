@@ -200,6 +200,14 @@ uint64_t op_join(strata_ctx* ctx, const K* dk, const int64_t* dw, uint64_t nd, i
 template <class KI, class KO>
 void op_project(strata_ctx* ctx, const KI* in, uint64_t n, int in_shift, int sel_hi, int sel_lo, uint64_t const_hi,
                 uint64_t const_lo, int out_shift, KO* out);
+// Rows with c0 == c1 (mode 0), c0 == k (1) or c1 == k (2), in input order.
+template <class K>
+uint64_t op_select(strata_ctx* ctx, const K* keys, const int64_t* w, uint64_t n, int shift, int mode, uint64_t k,
+                   K* out, int64_t* out_w);
+// Rows of a whose key is in the sorted b; Trop: weight a.w ⊗ b.w.
+template <class K>
+uint64_t op_intersect(strata_ctx* ctx, const K* a, const int64_t* aw, uint64_t na, const K* b, const int64_t* bw,
+                      uint64_t nb, K* out, int64_t* out_w);
 // Groups key >> gshift of sorted keys with count / sum / min / max (op 0..3)
 // of vals; returns the number of groups.
 template <class K>

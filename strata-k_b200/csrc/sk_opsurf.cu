@@ -17,6 +17,13 @@
 // project — the head built from one body atom's binding: each output column
 //   is an input column or a constant (build_head for a single-atom body).
 //
+// select — `unify` of one atom with a repeated variable or a constant
+//   (naive.rs:407-455): the rows whose two columns agree, or whose column
+//   equals a constant.
+//
+// intersect — two atoms over the same two variables: the rows of a also in
+//   b (sorted), with the Trop product of both weights.
+//
 // aggregate — `eval_aggregate_rule` + `fold_aggregate` (naive.rs:300-391):
 //   over bindings sorted by key, the group is key >> group_shift; count is
 //   the number of bindings of the group, sum / min / max fold an int64
@@ -158,6 +165,123 @@ __global__ void __launch_bounds__(NT) k_ag_fold(const uint64_t* __restrict__ sta
   }
 }
 
+// Row filter + compaction shared by select and intersect: `keep` decides a
+// row (and its output weight); per-tile counts, one scan, then the write in
+// input order (a thread owns SE_ITEMS consecutive rows).
+constexpr int SE_ITEMS = 8;
+constexpr uint32_t SE_TILE = NT * SE_ITEMS;
+
+// unify of one atom with a repeated variable or a constant
+// (strata-eval/src/naive.rs:407-455): mode 0 keeps c0 == c1, 1 keeps
+// c0 == k, 2 keeps c1 == k.
+template <class K>
+struct SelectRow {
+  int shift, mode;
+  uint64_t k;
+  __device__ bool keep(K key, const int64_t* w, uint64_t i, int64_t* ow, uint32_t*) const {
+    const uint64_t x = (uint64_t)key;
+    const uint64_t c0 = shift >= 64 ? 0ull : (x >> shift);
+    const uint64_t c1 = x & (shift >= 64 ? ~0ull : ((1ull << shift) - 1));
+    if (w) *ow = w[i];
+    return mode == 0 ? c0 == c1 : mode == 1 ? c0 == k : c1 == k;
+  }
+};
+
+// a ∩ b on whole keys (two atoms over the same variables): binary search of
+// each a key in the sorted b; Trop weight a.w ⊗ b.w on the operator
+// surface's codes.
+template <class K>
+struct IntersectRow {
+  const K* b;
+  const int64_t* bw;
+  uint64_t nb;
+  __device__ bool keep(K key, const int64_t* w, uint64_t i, int64_t* ow, uint32_t* flags) const {
+    const uint64_t j = lower_bound_dev(b, 0, nb, key);
+    if (j >= nb || b[j] != key) return false;
+    if (w) {
+      const int64_t x = w[i], y = bw[j];
+      if (x == INT64_MAX || y == INT64_MAX) {
+        *ow = INT64_MAX;
+      } else {
+        const int64_t xa = x > WFinMax<int64_t>::v ? 0 : x, ya = y > WFinMax<int64_t>::v ? 0 : y;
+        if (x > WFinMax<int64_t>::v || y > WFinMax<int64_t>::v) *flags |= ST_SENTINEL;
+        *ow = trop_mul(xa, ya, 0, flags);
+        if (*ow == WInf<int64_t>::v) *ow = INT64_MAX;
+      }
+    }
+    return true;
+  }
+};
+
+template <class K, class P>
+__global__ void __launch_bounds__(NT) k_filter_count(const K* __restrict__ keys, const int64_t* __restrict__ w,
+                                                     uint64_t n, P pred, uint64_t* __restrict__ tile_cnt,
+                                                     uint32_t* status) {
+  __shared__ uint32_t s_red[NT / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t b = (uint64_t)blockIdx.x * SE_TILE + (uint64_t)tid * SE_ITEMS;
+  uint32_t c = 0, flags = 0;
+  for (int j = 0; j < SE_ITEMS; j++) {
+    int64_t ow;
+    if (b + j < n && pred.keep(keys[b + j], w, b + j, &ow, &flags)) c++;
+  }
+  c = warp_sum(c);
+  if (lane == 0) s_red[warp] = c;
+  if (flags) atomicOr(status, flags);
+  __syncthreads();
+  if (tid == 0) {
+    uint64_t t = 0;
+    for (int q = 0; q < NT / 32; q++) t += s_red[q];
+    tile_cnt[blockIdx.x] = t;
+  }
+}
+
+template <class K, class P>
+__global__ void __launch_bounds__(NT) k_filter_write(const K* __restrict__ keys, const int64_t* __restrict__ w,
+                                                     uint64_t n, P pred, const uint64_t* __restrict__ tile_off,
+                                                     K* __restrict__ out, int64_t* __restrict__ out_w,
+                                                     uint32_t* status) {
+  __shared__ uint32_t s_scan[NT / 32 + 1];
+  const int tid = threadIdx.x;
+  const uint64_t b = (uint64_t)blockIdx.x * SE_TILE + (uint64_t)tid * SE_ITEMS;
+  uint32_t km = 0, flags = 0;
+  int64_t ws[SE_ITEMS];
+#pragma unroll
+  for (int j = 0; j < SE_ITEMS; j++) {
+    ws[j] = 0;
+    if (b + j < n && pred.keep(keys[b + j], w, b + j, &ws[j], &flags)) km |= 1u << j;
+  }
+  uint32_t tot;
+  const uint32_t ex = block_excl_sum<NT>((uint32_t)__popc(km), s_scan, &tot);
+  uint64_t at = tile_off[blockIdx.x] + ex;
+#pragma unroll
+  for (int j = 0; j < SE_ITEMS; j++) {
+    if ((km >> j) & 1u) {
+      out[at] = keys[b + j];
+      if (w) out_w[at] = ws[j];
+      at++;
+    }
+  }
+  if (flags) atomicOr(status, flags);
+}
+
+template <class K, class P>
+uint64_t filter_rows(strata_ctx* ctx, const K* keys, const int64_t* w, uint64_t n, const P& pred, K* out,
+                     int64_t* out_w) {
+  if (n == 0) return 0;
+  const uint64_t tiles = ceil_div(n, SE_TILE);
+  DBuf<uint64_t> toff(ctx, tiles + 1);
+  k_filter_count<K, P><<<(unsigned)tiles, NT, 0, ctx->stream>>>(keys, w, n, pred, toff.p, ctx->d_status);
+  after_launch(ctx, "k_filter_count");
+  scan_tile_sums(ctx, toff.p, tiles);
+  k_filter_write<K, P><<<(unsigned)tiles, NT, 0, ctx->stream>>>(keys, w, n, pred, toff.p, out, out_w, ctx->d_status);
+  after_launch(ctx, "k_filter_write");
+  uint64_t r;
+  read_u64(ctx, toff.p + tiles, &r, 1);
+  sync_and_check(ctx);
+  return r;
+}
+
 }  // namespace
 
 template <class K>
@@ -237,6 +361,27 @@ uint64_t op_aggregate(strata_ctx* ctx, const K* keys, const int64_t* vals, uint6
   return ng;
 }
 
+template <class K>
+uint64_t op_select(strata_ctx* ctx, const K* keys, const int64_t* w, uint64_t n, int shift, int mode, uint64_t k,
+                   K* out, int64_t* out_w) {
+  return filter_rows<K, SelectRow<K>>(ctx, keys, w, n, SelectRow<K>{shift, mode, k}, out, out_w);
+}
+
+template <class K>
+uint64_t op_intersect(strata_ctx* ctx, const K* a, const int64_t* aw, uint64_t na, const K* b, const int64_t* bw,
+                      uint64_t nb, K* out, int64_t* out_w) {
+  if (nb == 0) return 0;
+  return filter_rows<K, IntersectRow<K>>(ctx, a, aw, na, IntersectRow<K>{b, bw, nb}, out, out_w);
+}
+
+template uint64_t op_select<uint32_t>(strata_ctx*, const uint32_t*, const int64_t*, uint64_t, int, int, uint64_t,
+                                      uint32_t*, int64_t*);
+template uint64_t op_select<uint64_t>(strata_ctx*, const uint64_t*, const int64_t*, uint64_t, int, int, uint64_t,
+                                      uint64_t*, int64_t*);
+template uint64_t op_intersect<uint32_t>(strata_ctx*, const uint32_t*, const int64_t*, uint64_t, const uint32_t*,
+                                         const int64_t*, uint64_t, uint32_t*, int64_t*);
+template uint64_t op_intersect<uint64_t>(strata_ctx*, const uint64_t*, const int64_t*, uint64_t, const uint64_t*,
+                                         const int64_t*, uint64_t, uint64_t*, int64_t*);
 template uint64_t op_join<uint32_t>(strata_ctx*, const uint32_t*, const int64_t*, uint64_t, int, const uint32_t*,
                                     const int64_t*, uint64_t, int, int, uint32_t*, int64_t*, uint64_t, bool*);
 template uint64_t op_join<uint64_t>(strata_ctx*, const uint64_t*, const int64_t*, uint64_t, int, const uint64_t*,

@@ -180,6 +180,10 @@ SIGNATURES = {
     "strata_op_reduce": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.POINTER(C.c_uint64)]),
     "strata_op_merge_diff": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp, vp, vp,
                                        C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "strata_op_select": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, C.c_int, C.c_int, C.c_uint64, vp, vp,
+                                   C.POINTER(C.c_uint64)]),
+    "strata_op_intersect": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp,
+                                      C.POINTER(C.c_uint64)]),
     "strata_op_join": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, C.c_int, vp, vp, C.c_uint64, C.c_int, C.c_int,
                                  vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]),
     "strata_op_project": (C.c_int, [ctxp, C.c_int, vp, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_uint64,
