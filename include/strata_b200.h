@@ -452,6 +452,14 @@ strata_status strata_op_select(strata_ctx* ctx, int key_bytes, const void* d_in,
 strata_status strata_op_intersect(strata_ctx* ctx, int key_bytes, const void* d_a, const int64_t* d_aw, uint64_t na,
     const void* d_b, const int64_t* d_bw, uint64_t nb, void* d_out, int64_t* d_out_w, uint64_t* out_n);
 
+/* Stratified negation (`negation_holds`, strata-eval/src/naive.rs:537-566):
+ * keep row i of d_rows (weights carried) when probe[i] — the key of the
+ * negated atom under row i's binding, from strata_op_project; NULL = the row
+ * key itself — is absent from the sorted relation b (anti != 0), or present
+ * (anti == 0, a semi-join).  In input order; *out_n = rows kept. */
+strata_status strata_op_semijoin(strata_ctx* ctx, int key_bytes, const void* d_rows, const int64_t* d_w, uint64_t n,
+    const void* d_probe, const void* d_b, uint64_t nb, int anti, void* d_out, int64_t* d_out_w, uint64_t* out_n);
+
 /* One binary rule body  h(X,Z) :- a(X,Y), b(Y,Z)  (`solve` over two atoms,
  * strata-eval/src/seminaive.rs:215-298, with the head built as (X, Z),
  * `build_head` naive.rs:526).  a = (X << a_shift) | Y in any order (a Δ, or

@@ -1012,6 +1012,24 @@ strata_status strata_op_intersect(strata_ctx* ctx, int key_bytes, const void* d_
   SK_GUARD_END(ctx)
 }
 
+strata_status strata_op_semijoin(strata_ctx* ctx, int key_bytes, const void* d_rows, const int64_t* d_w, uint64_t n,
+                                 const void* d_probe, const void* d_b, uint64_t nb, int anti, void* d_out,
+                                 int64_t* d_out_w, uint64_t* out_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
+  if (!out_n || (n && (!d_rows || !d_out || (d_w && !d_out_w))) || (nb && !d_b)) return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  if (key_bytes == 4)
+    *out_n = sk::op_semijoin<uint32_t>(ctx, (const uint32_t*)d_rows, d_w, n, (const uint32_t*)d_probe,
+                                       (const uint32_t*)d_b, nb, anti != 0, (uint32_t*)d_out, d_out_w);
+  else
+    *out_n = sk::op_semijoin<uint64_t>(ctx, (const uint64_t*)d_rows, d_w, n, (const uint64_t*)d_probe,
+                                       (const uint64_t*)d_b, nb, anti != 0, (uint64_t*)d_out, d_out_w);
+  SK_GUARD_END(ctx)
+}
+
 strata_status strata_op_join(strata_ctx* ctx, int key_bytes, const void* d_a, const int64_t* d_aw, uint64_t na,
                              int a_shift, const void* d_b, const int64_t* d_bw, uint64_t nb, int b_shift, int out_shift,
                              void* d_out, int64_t* d_out_w, uint64_t out_cap, uint64_t* out_n) {

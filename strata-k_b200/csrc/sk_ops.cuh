@@ -208,6 +208,10 @@ uint64_t op_select(strata_ctx* ctx, const K* keys, const int64_t* w, uint64_t n,
 template <class K>
 uint64_t op_intersect(strata_ctx* ctx, const K* a, const int64_t* aw, uint64_t na, const K* b, const int64_t* bw,
                       uint64_t nb, K* out, int64_t* out_w);
+// Rows whose probe key (NULL: the row key) is in (anti: absent from) sorted b.
+template <class K>
+uint64_t op_semijoin(strata_ctx* ctx, const K* rows, const int64_t* w, uint64_t n, const K* probe, const K* b,
+                     uint64_t nb, bool anti, K* out, int64_t* out_w);
 // Groups key >> gshift of sorted keys with count / sum / min / max (op 0..3)
 // of vals; returns the number of groups.
 template <class K>

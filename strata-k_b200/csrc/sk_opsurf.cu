@@ -24,6 +24,9 @@
 // intersect — two atoms over the same two variables: the rows of a also in
 //   b (sorted), with the Trop product of both weights.
 //
+// semijoin — a negated (or existence-only) atom: the rows whose probe key is
+//   absent from (present in) a sorted relation.
+//
 // aggregate — `eval_aggregate_rule` + `fold_aggregate` (naive.rs:300-391):
 //   over bindings sorted by key, the group is key >> group_shift; count is
 //   the number of bindings of the group, sum / min / max fold an int64
@@ -213,6 +216,24 @@ struct IntersectRow {
   }
 };
 
+// Stratified negation / semi-join (negation_holds, naive.rs:537-566): keep
+// row i when probe[i] (the row's own key when probe is NULL) is absent from
+// (anti) or present in the sorted b; weights pass through unchanged.
+template <class K>
+struct SemiRow {
+  const K* probe;
+  const K* b;
+  uint64_t nb;
+  bool anti;
+  __device__ bool keep(K key, const int64_t* w, uint64_t i, int64_t* ow, uint32_t*) const {
+    const K pk = probe ? probe[i] : key;
+    const uint64_t j = nb ? lower_bound_dev(b, 0, nb, pk) : 0;
+    const bool found = j < nb && b[j] == pk;
+    if (w) *ow = w[i];
+    return anti ? !found : found;
+  }
+};
+
 template <class K, class P>
 __global__ void __launch_bounds__(NT) k_filter_count(const K* __restrict__ keys, const int64_t* __restrict__ w,
                                                      uint64_t n, P pred, uint64_t* __restrict__ tile_cnt,
@@ -374,6 +395,16 @@ uint64_t op_intersect(strata_ctx* ctx, const K* a, const int64_t* aw, uint64_t n
   return filter_rows<K, IntersectRow<K>>(ctx, a, aw, na, IntersectRow<K>{b, bw, nb}, out, out_w);
 }
 
+template <class K>
+uint64_t op_semijoin(strata_ctx* ctx, const K* rows, const int64_t* w, uint64_t n, const K* probe, const K* b,
+                     uint64_t nb, bool anti, K* out, int64_t* out_w) {
+  return filter_rows<K, SemiRow<K>>(ctx, rows, w, n, SemiRow<K>{probe, b, nb, anti}, out, out_w);
+}
+
+template uint64_t op_semijoin<uint32_t>(strata_ctx*, const uint32_t*, const int64_t*, uint64_t, const uint32_t*,
+                                        const uint32_t*, uint64_t, bool, uint32_t*, int64_t*);
+template uint64_t op_semijoin<uint64_t>(strata_ctx*, const uint64_t*, const int64_t*, uint64_t, const uint64_t*,
+                                        const uint64_t*, uint64_t, bool, uint64_t*, int64_t*);
 template uint64_t op_select<uint32_t>(strata_ctx*, const uint32_t*, const int64_t*, uint64_t, int, int, uint64_t,
                                       uint32_t*, int64_t*);
 template uint64_t op_select<uint64_t>(strata_ctx*, const uint64_t*, const int64_t*, uint64_t, int, int, uint64_t,

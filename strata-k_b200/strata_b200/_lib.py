@@ -184,6 +184,8 @@ SIGNATURES = {
                                    C.POINTER(C.c_uint64)]),
     "strata_op_intersect": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, vp, vp,
                                       C.POINTER(C.c_uint64)]),
+    "strata_op_semijoin": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, C.c_int, vp, vp,
+                                     C.POINTER(C.c_uint64)]),
     "strata_op_join": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, C.c_int, vp, vp, C.c_uint64, C.c_int, C.c_int,
                                  vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]),
     "strata_op_project": (C.c_int, [ctxp, C.c_int, vp, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_uint64,
