@@ -1,7 +1,9 @@
 """strata_b200 — B200 relational fixpoint engine for Strata/K's semi-naive hot path.
 
 ``gpu``      the reference GPU crate's API (transitive_closure_bool, …) on CUDA.
-``engine``   a drop-in ``run_semi_naive`` for the rule shapes the engine runs.
+``ops``      the interpreter's rule evaluation composed from the device
+             operator surface (select / join / intersect / semijoin /
+             project / sort / reduce / merge-diff / aggregate).
 ``gen``      seeded synthetic inputs of the benchmark shapes.
 ``textio``   the TSV input contract and the canonical text renderer.
 """

@@ -82,7 +82,7 @@ class Unsupported(GpuError):
 
 
 class WeightRange(GpuError):
-    """A finite weight equal to i64::MAX cannot be told from +inf on the device."""
+    """Finite weights spanning nearly all of i64: no 64-bit code keeps them apart from +inf."""
 
     code = L.E_WEIGHT_RANGE
 
