@@ -380,6 +380,35 @@ strata_status strata_circuits_grads(strata_ctx* ctx, const strata_circuits* c, c
     double* d_grads);
 void strata_circuits_free(strata_ctx* ctx, strata_circuits* c);
 
+/* ---- input and output contracts on the device ----------------------------
+ * One Soufflé TSV input file (strata-k/src/input.rs:53-197, 216-232): lines
+ * split on '\n' with trailing '\r's dropped and empty lines skipped; each row
+ * `arity` (1 or 2) tab-separated symbol cells, plus a trailing weight cell
+ * parsed as `trim().parse::<i64>()` when `trop`.  Symbols are interned
+ * first-seen (strata-ir/src/dict.rs:35-43) in row order, column order, after
+ * the n_dict strings of the current dictionary (string i =
+ * dict_bytes[dict_off[i] .. dict_off[i+1]), id i).  Returns malloc'd (free
+ * with strata_free): out_cols (column-major: column c of row r at
+ * c * out_rows + r), out_w (trop), and the new symbols in id order (ids n_dict
+ * .. n_dict + n_new - 1: new_bytes[new_off[j] .. new_off[j+1]), n_new + 1
+ * offsets).  A bad row returns STRATA_E_INVALID with *err_line = its 1-based
+ * line (the first one) and *err_col the empty column (else 0); nothing is
+ * returned and the dictionary is not extended.  The interning hashes are
+ * verified byte by byte: ids are exact. */
+strata_status strata_tsv_load(strata_ctx* ctx, const char* text, uint64_t text_len, uint32_t arity, int trop,
+    const char* dict_bytes, const uint64_t* dict_off, uint64_t n_dict, uint32_t** out_cols, int64_t** out_w,
+    uint64_t* out_rows, char** new_bytes, uint64_t** new_off, uint64_t* n_new, uint64_t* err_line,
+    uint32_t* err_col);
+
+/* The canonical text of a binary relation (render_db for one relation,
+ * strata-cli/src/render.rs:29-54, 87-92): one line per tuple in id order,
+ * `name(a, b)\n`, with ` = w` or ` = inf` for Trop; symbol names from the
+ * dictionary (n_dict strings as above; an id it lacks prints `?`).  Built on
+ * the device; *out_text is malloc'd and NUL-terminated (free with
+ * strata_free), *out_len its length without the NUL. */
+strata_status strata_rel_render(strata_ctx* ctx, const strata_rel* rel, const char* name, const char* dict_bytes,
+    const uint64_t* dict_off, uint64_t n_dict, char** out_text, uint64_t* out_len);
+
 /* Relation handle accessors. */
 strata_status strata_rel_size(const strata_rel* rel, uint64_t* n);
 strata_status strata_rel_is_trop(const strata_rel* rel, int* is_trop);

@@ -976,6 +976,51 @@ strata_status strata_op_merge_diff(strata_ctx* ctx, int key_bytes, const void* d
   SK_GUARD_END(ctx)
 }
 
+strata_status strata_tsv_load(strata_ctx* ctx, const char* text, uint64_t text_len, uint32_t arity, int trop,
+                              const char* dict_bytes, const uint64_t* dict_off, uint64_t n_dict, uint32_t** out_cols,
+                              int64_t** out_w, uint64_t* out_rows, char** new_bytes, uint64_t** new_off,
+                              uint64_t* n_new, uint64_t* err_line, uint32_t* err_col) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (arity < 1 || arity > 2) return bad(ctx, "arity must be 1 or 2");
+  if ((text_len && !text) || (n_dict && (!dict_bytes || !dict_off)) || !out_cols || !out_rows || !new_bytes ||
+      !new_off || !n_new || (trop && !out_w))
+    return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  if (err_line) *err_line = 0;
+  if (err_col) *err_col = 0;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  sk::TsvResult r = sk::tsv_load(ctx, text, text_len, arity, trop != 0, dict_bytes, dict_off, n_dict);
+  if (r.err_kind) {
+    if (err_line) *err_line = r.err_line;
+    if (err_col) *err_col = r.err_col;
+    const std::string at = "line " + std::to_string(r.err_line) + ": ";
+    if (r.err_kind == 1) return bad(ctx, (at + "expects " + std::to_string(arity + (trop ? 1 : 0)) + " column(s)").c_str());
+    if (r.err_kind == 2) return bad(ctx, (at + "empty value in column " + std::to_string(r.err_col)).c_str());
+    return bad(ctx, (at + "needs a trailing integer weight").c_str());
+  }
+  *out_cols = r.cols;
+  if (out_w) *out_w = r.w;
+  else std::free(r.w);
+  *out_rows = r.rows;
+  *new_bytes = r.new_bytes;
+  *new_off = r.new_off;
+  *n_new = r.n_new;
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_rel_render(strata_ctx* ctx, const strata_rel* rel, const char* name, const char* dict_bytes,
+                                const uint64_t* dict_off, uint64_t n_dict, char** out_text, uint64_t* out_len) {
+  if (!ctx || !rel || !name || !out_text || !out_len || (n_dict && (!dict_bytes || !dict_off)))
+    return bad(ctx, "NULL argument");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  static const uint64_t zero = 0;
+  *out_len = sk::render_rel(ctx, rel, name, dict_bytes, n_dict ? dict_off : &zero, n_dict, out_text);
+  SK_GUARD_END(ctx)
+}
+
 strata_status strata_op_select(strata_ctx* ctx, int key_bytes, const void* d_in, const int64_t* d_w, uint64_t n,
                                int shift, int mode, uint64_t value, void* d_out, int64_t* d_out_w, uint64_t* out_n) {
   if (!ctx) return STRATA_E_INVALID;

@@ -218,4 +218,29 @@ template <class K>
 uint64_t op_aggregate(strata_ctx* ctx, const K* keys, const int64_t* vals, uint64_t n, int gshift, int op, K* groups,
                       int64_t* out_vals);
 
+// ---- text input / output (sk_text.cu) ----
+// One Soufflé TSV load: rows of `arity` symbol cells (+ a trailing i64 weight
+// when trop), interned first-seen after the n_dict dictionary strings.  On a
+// bad row err_kind = 1 (cell count), 2 (empty symbol cell err_col) or 3
+// (weight) with its 1-based line; else cols (column-major, rows x arity),
+// w, and the new symbols (n_new strings in id order, bytes + offsets), all
+// malloc'd for the caller.
+struct TsvResult {
+  uint64_t rows = 0;
+  uint32_t* cols = nullptr;
+  int64_t* w = nullptr;
+  uint64_t n_new = 0;
+  char* new_bytes = nullptr;
+  uint64_t* new_off = nullptr;
+  uint64_t err_line = 0;
+  uint32_t err_col = 0;
+  int err_kind = 0;
+};
+TsvResult tsv_load(strata_ctx* ctx, const char* text, uint64_t text_len, uint32_t arity, bool trop,
+                   const char* dict_bytes, const uint64_t* dict_off, uint64_t n_dict);
+// The canonical text of a binary relation handle (malloc'd, NUL-terminated);
+// returns its length.
+uint64_t render_rel(strata_ctx* ctx, const strata_rel* rel, const char* name, const char* dict_bytes,
+                    const uint64_t* dict_off, uint64_t n_dict, char** out_text);
+
 }  // namespace sk

@@ -5,6 +5,8 @@
 * ``load_tsv`` — Soufflé TSV rows split on tab, empty lines skipped, a Trop
   predicate's trailing column parsed as an i64 weight, a neural predicate's
   as a probability in [0, 1] (strata-k/src/input.rs:53-197, 204-234).
+* ``load_tsv_device`` / ``render_relation_device`` — the same two contracts
+  on the GPU (strata_tsv_load, strata_rel_render).
 * ``render_db`` — canonical text: relations in name order, tuples in id order,
   ``pred(a, b)`` with `` = w`` / `` = inf`` for Trop (strata-cli/src/render.rs:29-92,
   strata-ir/src/output.rs:11).  A non-empty ``queries`` list filters the
@@ -92,6 +94,62 @@ def load_tsv(source, arity: int, dictionary: SymbolDict, trop: bool = False,
                 raise InputError(f"{lineno}: probability {p} is outside [0, 1]")
             weights[k] = p
     return cols, weights
+
+
+def _dict_buffers(dictionary: SymbolDict):
+    enc = [x.encode() for x in dictionary.by_id]
+    off = np.zeros(len(enc) + 1, np.uint64)
+    if enc:
+        off[1:] = np.cumsum([len(e) for e in enc])
+    return b"".join(enc), off
+
+
+def load_tsv_device(eng, text, arity: int, dictionary: SymbolDict, trop: bool = False):
+    """``load_tsv`` on the device (strata_tsv_load): the same rows, ids and
+    errors; new symbols are appended to ``dictionary`` in first-seen order."""
+    import ctypes as C
+
+    from . import _lib as L
+    data = text.encode() if isinstance(text, str) else bytes(text)
+    dbytes, doff = _dict_buffers(dictionary)
+    cols_p, w_p = C.POINTER(C.c_uint32)(), C.POINTER(C.c_int64)()
+    rows, n_new, eline, ecol = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint32()
+    nb, no = C.c_void_p(), C.POINTER(C.c_uint64)()
+    rc = eng.lib.strata_tsv_load(eng.ctx, data, len(data), arity, 1 if trop else 0, dbytes or None,
+                                 doff.ctypes.data_as(C.c_void_p), len(dictionary), C.byref(cols_p),
+                                 C.byref(w_p) if trop else None, C.byref(rows), C.byref(nb), C.byref(no),
+                                 C.byref(n_new), C.byref(eline), C.byref(ecol))
+    if rc == L.E_INVALID and eline.value:
+        raise InputError(eng.lib.strata_last_error(eng.ctx).decode())
+    eng._check(rc)
+    n = rows.value
+    flat = np.ctypeslib.as_array(cols_p, shape=(max(1, n * arity),))[:n * arity].copy()
+    eng.lib.strata_free(C.cast(cols_p, C.c_void_p))
+    weights = None
+    if trop:
+        weights = np.ctypeslib.as_array(w_p, shape=(max(1, n),))[:n].copy()
+        eng.lib.strata_free(C.cast(w_p, C.c_void_p))
+    k = n_new.value
+    offs = np.ctypeslib.as_array(no, shape=(k + 1,)).copy()
+    raw = C.string_at(nb, int(offs[-1])) if k else b""
+    for j in range(k):
+        dictionary.intern(raw[int(offs[j]):int(offs[j + 1])].decode())
+    eng.lib.strata_free(nb)
+    eng.lib.strata_free(C.cast(no, C.c_void_p))
+    return [flat[c * n:(c + 1) * n].astype(np.uint32) for c in range(arity)], weights
+
+
+def render_relation_device(eng, rel, name: str, dictionary: SymbolDict) -> str:
+    """The canonical text of a device relation (strata_rel_render): the same
+    lines ``render_relation`` prints, built on the GPU."""
+    import ctypes as C
+    dbytes, doff = _dict_buffers(dictionary)
+    out, n = C.c_void_p(), C.c_uint64()
+    eng._check(eng.lib.strata_rel_render(eng.ctx, rel.rel, name.encode(), dbytes or None,
+                                         doff.ctypes.data_as(C.c_void_p), len(dictionary), C.byref(out), C.byref(n)))
+    text = C.string_at(out, n.value).decode()
+    eng.lib.strata_free(out)
+    return text
 
 
 def render_weight(w: int, inf: bool) -> str:
