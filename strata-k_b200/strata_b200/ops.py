@@ -311,6 +311,16 @@ class Program:
                 raise Unsupported(f"unknown predicate {name}")
             return delta[name] if i == pos else db[name]
 
+        # join order: the planner's cost-based variable order (plan.body_order,
+        # over the atoms' current sizes) when a chain of two live variables
+        # can follow it, else the written order; bindings do not depend on it
+        from .plan import body_order
+        sizes = [rel_of(i, b[0]).n for i, b in posl]
+        universe = getattr(self, "_universe", 1)
+        planned = [posl[j] for j in body_order([[v for v in b[1] if _is_var(v)] for _, b in posl], sizes, universe)]
+        if planned != posl and self._chain_ok(planned, head_vars, neg_vars, agg is not None):
+            posl = planned
+
         def needed(after):
             vs = set(head_vars) | set(neg_vars)
             for _, (_, args) in posl[after:]:
@@ -379,6 +389,42 @@ class Program:
             k, w, n = ops.semijoin(k, w, n, probe, db[name], True)
         return k, w, n, cols
 
+    @staticmethod
+    def _chain_ok(posl, head_vars, neg_vars, is_agg) -> bool:
+        """Whether the left-deep chain over `posl` keeps at most two live
+        variables per step (host-side dry run of _body's cases)."""
+        def atom_vars(args):
+            return list(dict.fromkeys(v for v in args if _is_var(v)))
+
+        state = atom_vars(posl[0][1][1])
+        for step in range(1, len(posl)):
+            nxt = atom_vars(posl[step][1][1])
+            need = set(head_vars) | set(neg_vars)
+            for _, (_, args) in posl[step + 1:]:
+                need |= {v for v in args if _is_var(v)}
+            shared = [v for v in state if v in nxt]
+            if len(shared) == 1:
+                y = shared[0]
+                x = next((v for v in state if v != y), y)
+                z = next((v for v in nxt if v != y), y)
+                keep = [v for v in dict.fromkeys((x, y, z)) if v in need]
+                if len(keep) > 2:
+                    return False
+                p = x if x in keep else y
+                q = z if z in keep else y
+                state = [p] if p == q else [p, q]
+            elif len(shared) == 2:
+                if len(state) != 2 or len(nxt) != 2:
+                    return False
+                state = shared
+            else:
+                kl = [v for v in state if v in need]
+                kr = [v for v in nxt if v in need]
+                if is_agg or len(kl) > 1 or len(kr) > 1:
+                    return False
+                state = kl + kr
+        return all(v in state for v in neg_vars) and all(v in state for v in head_vars)
+
     def _head(self, ops, k, n, cols, hargs):
         """Head tuples (build_head, naive.rs:526) from body rows."""
 
@@ -400,6 +446,7 @@ class Program:
         methods as Operators)."""
         ops = ops if ops is not None else Operators(eng)
         db, universe = self._edb(ops)
+        self._universe = universe
         strata = sorted({st for _, _, st in self.preds.values()})
         total_rounds = 0
         agg_out: dict[str, list] = {}
