@@ -153,9 +153,11 @@ def config(args, world):
 
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of
-# the dominant kernel, from one ncu capture of the named workload; absent
-# (null) when no capture of that workload and kernel exists.
-TRAFFIC: dict = {}
+# the dominant kernel, from one ncu capture of the named workload (the 16
+# k_expand_dense launches of one MSSP R-MAT-20 fixpoint: 3.57 GB in total, so
+# 223 MB per launch against 550 MB of algorithmic bytes — the index probes hit
+# in L2); absent (null) when no capture of that workload and kernel exists.
+TRAFFIC: dict = {("mssp", "k_expand_dense"): 223_022_176}
 
 
 # ---------------------------------------------------------------- clocks
