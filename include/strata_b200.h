@@ -380,6 +380,21 @@ strata_status strata_circuits_grads(strata_ctx* ctx, const strata_circuits* c, c
     double* d_grads);
 void strata_circuits_free(strata_ctx* ctx, strata_circuits* c);
 
+/* ---- ASP grounding-simplify filter ----------------------------------------
+ * Replaces `simplify_filter` (strata-gpu/src/asp.rs:121-136, semantics of
+ * simplify_filter_cpu / keep_literal :53-100) for a ground
+ * program in CSR form: rule i has head[i] (atom id, -1 for a constraint) and
+ * the signed body literals body_lit[body_start[i] .. body_start[i+1]) (+(a+1)
+ * positive, -(a+1) negative).  A rule whose positive atom is impossible
+ * (poss[a] == 0) or whose negative atom is certain (cert[a] != 0) is dropped;
+ * a surviving rule loses its certain positive and impossible negative
+ * literals.  Returns malloc'd arrays (free with strata_free) in rule order;
+ * a literal naming no atom (0 or beyond n_atoms) is STRATA_E_CUDA with a
+ * bounds message and nothing is returned. */
+strata_status strata_asp_simplify_filter(strata_ctx* ctx, uint64_t n_rules, const int32_t* head,
+    const uint32_t* body_start, const int32_t* body_lit, uint64_t n_atoms, const uint8_t* poss, const uint8_t* cert,
+    int32_t** out_head, uint32_t** out_body_start, int32_t** out_body_lit, uint64_t* out_n);
+
 /* ---- input and output contracts on the device ----------------------------
  * One Soufflé TSV input file (strata-k/src/input.rs:53-197, 216-232): lines
  * split on '\n' with trailing '\r's dropped and empty lines skipped; each row

@@ -665,3 +665,32 @@ def brute_4cliques(a, b, nodes) -> int:
     L = lib()
     x, y = _col(a, np.uint32), _col(b, np.uint32)
     return int(L.sko_brute_4cliques(_p(x, C.c_uint32), _p(y, C.c_uint32), len(x), nodes))
+
+
+def asp_simplify_filter(head, body_start, body_lit, poss, cert):
+    """The grounding-simplify filter as the reference's CPU path computes it
+    (crates/strata-gpu/src/asp.rs:53-100, keep_literal + simplify_filter_cpu):
+    returns (head, body_start, body_lit) of the surviving rules."""
+    oh, os_, ol = [], [0], []
+    for i in range(len(head)):
+        kept, alive = [], True
+        for lit in body_lit[body_start[i]:body_start[i + 1]]:
+            a, pos = abs(int(lit)) - 1, lit > 0
+            if pos:
+                if poss[a] == 0:
+                    alive = False
+                    break
+                if cert[a] == 0:
+                    kept.append(int(lit))
+            else:
+                if cert[a] != 0:
+                    alive = False
+                    break
+                if poss[a] != 0:
+                    kept.append(int(lit))
+        if not alive:
+            continue
+        oh.append(int(head[i]))
+        ol.extend(kept)
+        os_.append(len(ol))
+    return oh, os_, ol

@@ -976,6 +976,27 @@ strata_status strata_op_merge_diff(strata_ctx* ctx, int key_bytes, const void* d
   SK_GUARD_END(ctx)
 }
 
+strata_status strata_asp_simplify_filter(strata_ctx* ctx, uint64_t n_rules, const int32_t* head,
+                                         const uint32_t* body_start, const int32_t* body_lit, uint64_t n_atoms,
+                                         const uint8_t* poss, const uint8_t* cert, int32_t** out_head,
+                                         uint32_t** out_body_start, int32_t** out_body_lit, uint64_t* out_n) {
+  if (!ctx) return STRATA_E_INVALID;
+  if (!out_head || !out_body_start || !out_body_lit || !out_n || (n_rules && (!head || !body_start)) ||
+      (n_atoms && (!poss || !cert)))
+    return bad(ctx, "NULL argument");
+  if (n_rules && body_start[n_rules] && !body_lit) return bad(ctx, "NULL body literals");
+  if (n_rules >= 0xffffffffull) return bad(ctx, "at most 2^32 - 2 rules per call");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  sk::AspResult r = sk::asp_simplify(ctx, n_rules, head, body_start, body_lit, n_atoms, poss, cert);
+  *out_head = r.head;
+  *out_body_start = r.body_start;
+  *out_body_lit = r.body_lit;
+  *out_n = r.n_rules;
+  SK_GUARD_END(ctx)
+}
+
 strata_status strata_tsv_load(strata_ctx* ctx, const char* text, uint64_t text_len, uint32_t arity, int trop,
                               const char* dict_bytes, const uint64_t* dict_off, uint64_t n_dict, uint32_t** out_cols,
                               int64_t** out_w, uint64_t* out_rows, char** new_bytes, uint64_t** new_off,

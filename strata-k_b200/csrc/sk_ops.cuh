@@ -90,6 +90,9 @@ void dense_expand_words(strata_ctx* ctx, const uint32_t* hword, const uint32_t* 
                         const W* Dprev, int out_pshift, int out_vshift, const uint32_t* nbr, uint64_t n_nbr,
                         const W* nbr_w, const DenseLayout& lay, uint32_t* bits, W* D, uint32_t* marks,
                         uint64_t* splits_buf);
+// out[i] = sum of v[0..i) (exclusive) or v[0..i] (inclusive); *total (if
+// given, synchronizing) = the sum of all n.
+void scan_u64(strata_ctx* ctx, const uint64_t* v, uint64_t n, uint64_t* out, bool inclusive, uint64_t* total);
 // In-place exclusive scan of per-tile sums (one block per array); sums[count]
 // = total.  `arrays` consecutive arrays of count + 1 words each.
 void scan_tile_sums(strata_ctx* ctx, uint64_t* sums, uint64_t count, int arrays = 1);
@@ -217,6 +220,16 @@ uint64_t op_semijoin(strata_ctx* ctx, const K* rows, const int64_t* w, uint64_t 
 template <class K>
 uint64_t op_aggregate(strata_ctx* ctx, const K* keys, const int64_t* vals, uint64_t n, int gshift, int op, K* groups,
                       int64_t* out_vals);
+
+// ---- ASP grounding-simplify filter (sk_asp.cu) ----
+struct AspResult {
+  uint64_t n_rules = 0;
+  int32_t* head = nullptr;        // malloc'd, n_rules
+  uint32_t* body_start = nullptr;  // malloc'd, n_rules + 1
+  int32_t* body_lit = nullptr;     // malloc'd, body_start[n_rules]
+};
+AspResult asp_simplify(strata_ctx* ctx, uint64_t n_rules, const int32_t* head, const uint32_t* bstart,
+                       const int32_t* lit, uint64_t n_atoms, const uint8_t* poss, const uint8_t* cert);
 
 // ---- text input / output (sk_text.cu) ----
 // One Soufflé TSV load: rows of `arity` symbol cells (+ a trailing i64 weight

@@ -806,6 +806,45 @@ __global__ void k_fingerprint(const K* __restrict__ keys, const W* __restrict__ 
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
 }
 
+// Scan of u64 values (exclusive or inclusive) through the tile-sum scan:
+// per-tile partials in one pass, the tile offsets scanned, the values
+// rewritten.
+constexpr int SC_ITEMS = 8;
+constexpr uint32_t SC_TILE = NT * SC_ITEMS;
+__global__ void __launch_bounds__(NT) k_scan_part(const uint64_t* __restrict__ v, uint64_t n,
+                                                  uint64_t* __restrict__ tile_sum) {
+  __shared__ uint64_t s_red[NT / 32];
+  const uint64_t b = (uint64_t)blockIdx.x * SC_TILE + (uint64_t)threadIdx.x * SC_ITEMS;
+  uint64_t k = 0;
+  for (int j = 0; j < SC_ITEMS; j++)
+    if (b + j < n) k += v[b + j];
+  k = warp_sum(k);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = k;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t s = 0;
+    for (int w = 0; w < NT / 32; w++) s += s_red[w];
+    tile_sum[blockIdx.x] = s;
+  }
+}
+__global__ void __launch_bounds__(NT) k_scan_apply(const uint64_t* __restrict__ v, uint64_t n,
+                                                   const uint64_t* __restrict__ tile_off, uint64_t* __restrict__ out,
+                                                   int inclusive) {
+  __shared__ uint64_t s_scan[NT / 32 + 1];
+  const uint64_t b = (uint64_t)blockIdx.x * SC_TILE + (uint64_t)threadIdx.x * SC_ITEMS;
+  uint64_t loc[SC_ITEMS], k = 0;
+  for (int j = 0; j < SC_ITEMS; j++) {
+    loc[j] = b + j < n ? v[b + j] : 0;
+    k += loc[j];
+  }
+  uint64_t tot;
+  uint64_t run = tile_off[blockIdx.x] + block_excl_sum<NT>(k, s_scan, &tot);
+  for (int j = 0; j < SC_ITEMS; j++) {
+    if (b + j < n) out[b + j] = inclusive ? run + loc[j] : run;
+    run += loc[j];
+  }
+}
+
 inline int grid_for(strata_ctx* ctx, uint64_t n, int per_block = NT) {
   uint64_t b = ceil_div(n, per_block);
   const uint64_t cap = (uint64_t)ctx->num_sms * 8;
@@ -1047,6 +1086,17 @@ uint64_t fingerprint(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, int
   uint64_t r;
   read_u64(ctx, reinterpret_cast<uint64_t*>(acc.p), &r, 1);
   return r;
+}
+
+void scan_u64(strata_ctx* ctx, const uint64_t* v, uint64_t n, uint64_t* out, bool inclusive, uint64_t* total) {
+  const uint64_t tiles = ceil_div(n ? n : 1, SC_TILE);
+  DBuf<uint64_t> ts(ctx, tiles + 1);
+  k_scan_part<<<(unsigned)tiles, NT, 0, ctx->stream>>>(v, n, ts.p);
+  after_launch(ctx, "k_scan_part");
+  scan_tile_sums(ctx, ts.p, tiles);
+  k_scan_apply<<<(unsigned)tiles, NT, 0, ctx->stream>>>(v, n, ts.p, out, inclusive ? 1 : 0);
+  after_launch(ctx, "k_scan_apply");
+  if (total) read_u64(ctx, ts.p + tiles, total, 1);
 }
 
 // ---- explicit instantiations ----------------------------------------------------

@@ -345,44 +345,6 @@ __global__ void k_u32_to_u64(const uint32_t* __restrict__ a, uint64_t n, uint64_
   if (i < n) b[i] = a[i];
 }
 
-// exclusive scan of u64 values through the tile-sum scan: per-tile partials
-// in one pass, the tile offsets scanned, the values rewritten.
-constexpr int SC_ITEMS = 8;
-constexpr uint32_t SC_TILE = NT * SC_ITEMS;
-__global__ void __launch_bounds__(NT) k_scan_part(const uint64_t* __restrict__ v, uint64_t n,
-                                                  uint64_t* __restrict__ tile_sum) {
-  __shared__ uint64_t s_red[NT / 32];
-  const uint64_t b = (uint64_t)blockIdx.x * SC_TILE + (uint64_t)threadIdx.x * SC_ITEMS;
-  uint64_t k = 0;
-  for (int j = 0; j < SC_ITEMS; j++)
-    if (b + j < n) k += v[b + j];
-  k = warp_sum(k);
-  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = k;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint64_t s = 0;
-    for (int w = 0; w < NT / 32; w++) s += s_red[w];
-    tile_sum[blockIdx.x] = s;
-  }
-}
-__global__ void __launch_bounds__(NT) k_scan_apply(const uint64_t* __restrict__ v, uint64_t n,
-                                                   const uint64_t* __restrict__ tile_off, uint64_t* __restrict__ out,
-                                                   int inclusive) {
-  __shared__ uint64_t s_scan[NT / 32 + 1];
-  const uint64_t b = (uint64_t)blockIdx.x * SC_TILE + (uint64_t)threadIdx.x * SC_ITEMS;
-  uint64_t loc[SC_ITEMS], k = 0;
-  for (int j = 0; j < SC_ITEMS; j++) {
-    loc[j] = b + j < n ? v[b + j] : 0;
-    k += loc[j];
-  }
-  uint64_t tot;
-  uint64_t run = tile_off[blockIdx.x] + block_excl_sum<NT>(k, s_scan, &tot);
-  for (int j = 0; j < SC_ITEMS; j++) {
-    if (b + j < n) out[b + j] = inclusive ? run + loc[j] : run;
-    run += loc[j];
-  }
-}
-
 // ---- rendering ----------------------------------------------------------------
 __device__ __forceinline__ uint32_t dec_len(uint64_t m) {
   uint32_t k = 1;
@@ -474,17 +436,6 @@ __global__ void k_render_write(RenderSpec R, const uint32_t* __restrict__ c0, co
     }
   }
   *o = '\n';
-}
-
-void excl_scan_u64(strata_ctx* ctx, const uint64_t* v, uint64_t n, uint64_t* out, bool inclusive, uint64_t* total) {
-  const uint64_t tiles = ceil_div(n ? n : 1, SC_TILE);
-  DBuf<uint64_t> ts(ctx, tiles + 1);
-  k_scan_part<<<(unsigned)tiles, NT, 0, ctx->stream>>>(v, n, ts.p);
-  after_launch(ctx, "k_scan_part");
-  scan_tile_sums(ctx, ts.p, tiles);
-  k_scan_apply<<<(unsigned)tiles, NT, 0, ctx->stream>>>(v, n, ts.p, out, inclusive ? 1 : 0);
-  after_launch(ctx, "k_scan_apply");
-  if (total) read_u64(ctx, ts.p + tiles, total, 1);
 }
 
 // Ordered positions of byte `c` in t[0, n).
@@ -597,14 +548,14 @@ TsvResult tsv_load(strata_ctx* ctx, const char* text, uint64_t text_len, uint32_
   k_u32_to_u64<<<gridn(n_cells, NT), NT, 0, ctx->stream>>>(head.p, n_cells, h64.p);
   after_launch(ctx, "k_u32_to_u64");
   // run_of[i] = heads at or before sorted position i = the run's index + 1
-  excl_scan_u64(ctx, h64.p, n_cells, run_of.p, true, nullptr);
+  scan_u64(ctx, h64.p, n_cells, run_of.p, true, nullptr);
   SK_CUDA(cudaMemsetAsync(newhead.p, 0, (n_cells + 1) * 4, ctx->stream));
   k_new_heads<<<gridn(n_cells, NT), NT, 0, ctx->stream>>>(head.p, pp, n_cells, n_dict, newhead.p);
   after_launch(ctx, "k_new_heads");
   k_u32_to_u64<<<gridn(n_cells, NT), NT, 0, ctx->stream>>>(newhead.p, n_cells, nh64.p);
   after_launch(ctx, "k_u32_to_u64");
   uint64_t n_new;
-  excl_scan_u64(ctx, nh64.p, n_cells, rank.p, false, &n_new);
+  scan_u64(ctx, nh64.p, n_cells, rank.p, false, &n_new);
   R.n_new = n_new;
   k_run_ids<<<gridn(n_cells, NT), NT, 0, ctx->stream>>>(head.p, run_of.p, pp, rank.p, n_cells, n_dict, run_id.p);
   after_launch(ctx, "k_run_ids");
@@ -625,7 +576,7 @@ TsvResult tsv_load(strata_ctx* ctx, const char* text, uint64_t text_len, uint32_
     after_launch(ctx, "k_new_syms");
     k_u32_to_u64<<<gridn(n_new, NT), NT, 0, ctx->stream>>>(nlen.p, n_new, nlen64.p);
     after_launch(ctx, "k_u32_to_u64");
-    excl_scan_u64(ctx, nlen64.p, n_new, noff.p, false, &new_bytes);
+    scan_u64(ctx, nlen64.p, n_new, noff.p, false, &new_bytes);
   }
   DBuf<uint8_t> nbytes(ctx, new_bytes + 1);
   if (n_new) {
@@ -683,7 +634,7 @@ uint64_t render_rel(strata_ctx* ctx, const strata_rel* rel, const char* name, co
     k_render_len<<<gridn(n, NT), NT, 0, ctx->stream>>>(R, c0.p, c1.p, rel->trop ? w.p : nullptr,
                                                        rel->trop ? inf.p : nullptr, n, len.p);
     after_launch(ctx, "k_render_len");
-    excl_scan_u64(ctx, len.p, n, start.p, false, &total);
+    scan_u64(ctx, len.p, n, start.p, false, &total);
   }
   DBuf<uint8_t> out(ctx, total + 1);
   if (n) {

@@ -186,6 +186,9 @@ SIGNATURES = {
                                       C.POINTER(C.c_uint64)]),
     "strata_op_semijoin": (C.c_int, [ctxp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64, C.c_int, vp, vp,
                                      C.POINTER(C.c_uint64)]),
+    "strata_asp_simplify_filter": (C.c_int, [ctxp, C.c_uint64, vp, vp, vp, C.c_uint64, vp, vp,
+                                             C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.POINTER(C.c_uint32)),
+                                             C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.c_uint64)]),
     "strata_tsv_load": (C.c_int, [ctxp, C.c_char_p, C.c_uint64, C.c_uint32, C.c_int, C.c_char_p, vp, C.c_uint64,
                                   C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.POINTER(C.c_int64)),
                                   C.POINTER(C.c_uint64), C.POINTER(C.c_void_p), C.POINTER(C.POINTER(C.c_uint64)),

@@ -539,6 +539,24 @@ class Engine:
                 "capture_device_ms": sum(s_["device_ms"] for s_ in stats), "chunks": len(parts)}
         return P, G, circ, info
 
+    def asp_simplify_filter(self, head, body_start, body_lit, poss, cert):
+        """``simplify_filter`` (strata-gpu/src/asp.rs:121) on the device:
+        (head, body_start, body_lit) of the rules that survive, literals
+        trimmed."""
+        h = np.ascontiguousarray(head, np.int32)
+        bs = np.ascontiguousarray(body_start, np.uint32)
+        bl = np.ascontiguousarray(body_lit, np.int32)
+        ps = np.ascontiguousarray(poss, np.uint8)
+        ce = np.ascontiguousarray(cert, np.uint8)
+        oh, ob, ol = C.POINTER(C.c_int32)(), C.POINTER(C.c_uint32)(), C.POINTER(C.c_int32)()
+        n = C.c_uint64()
+        self._check(self.lib.strata_asp_simplify_filter(
+            self.ctx, len(h), _ptr(h, C.c_int32), _ptr(bs, C.c_uint32), _ptr(bl, C.c_int32), len(ps),
+            _ptr(ps, C.c_uint8), _ptr(ce, C.c_uint8), C.byref(oh), C.byref(ob), C.byref(ol), C.byref(n)))
+        m = n.value
+        start = self._take(ob, m + 1, np.uint32)
+        return self._take(oh, m, np.int32), start, self._take(ol, int(start[-1]), np.int32)
+
     def count_triangle_pattern_range_dev(self, x, y, x_lo: int, x_hi: int, n=None) -> int:
         """Bindings of the triangle pattern with X in [x_lo, x_hi)."""
         n = _len(x) if n is None else n

@@ -529,3 +529,11 @@ def test_prov_tc_fast_matches_interpreter_capture():
         for q in range(len(qs)):
             want = rel.get((int(qs[q]), int(qt[q])), [])
             assert got[q] == want, (trial, qs[q], qt[q])
+
+
+def test_asp_simplify_filter_reference_case():
+    """crates/strata-gpu/src/asp.rs tests: r :- p, not s  keeps an empty body;
+    r :- q, s  dies (s impossible)."""
+    poss, cert = [1, 1, 0, 1], [1, 1, 0, 0]
+    h, s, l = O.asp_simplify_filter([3, 3], [0, 2, 4], [1, -3, 2, 3], poss, cert)
+    assert h == [3] and s == [0, 0] and l == []
