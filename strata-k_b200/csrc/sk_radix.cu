@@ -6,11 +6,13 @@
 //   * one upfront kernel computes the digit histograms of every pass from a
 //     single read of the keys (warp-privatised shared-memory counters with
 //     match-any aggregation);
-//   * each 8-bit pass is ONE kernel: a tile of NT*ITEMS keys is loaded
-//     warp-striped (coalesced), ranked with warp-level multisplit (8 ballots
-//     per item), the tile's per-digit counts are published for a decoupled
-//     look-back, keys are staged in shared memory in digit order and written
-//     out in runs (coalesced per digit);
+//   * each 8-bit pass is ONE kernel: a tile of NT*ITEMS keys (and its
+//     values) arrives in shared memory by one bulk asynchronous copy each,
+//     is ranked with warp-level multisplit (8 ballots per item), the tile's
+//     per-digit counts are published for a decoupled look-back, keys are
+//     staged in shared memory in digit order with their source slot and
+//     written out in runs (coalesced per digit), values fetched through the
+//     source slot — no per-key value state stays in registers;
 //   * only the significant `bits` of the key are sorted (a 26-bit key takes 4
 //     passes, not 64) and passes whose digit is constant are skipped.
 #include "sk_ops.cuh"
@@ -92,43 +94,138 @@ __global__ void __launch_bounds__(NT) k_radix_bins(const uint32_t* __restrict__ 
   binoff[blockIdx.x * RADIX + threadIdx.x] = block_excl_sum<NT>(v, scratch, &tot);
 }
 
+// ---- bulk asynchronous copy of a tile into shared memory ---------------------
+// One thread issues cp.async.bulk (global -> shared, completion counted in
+// bytes on an mbarrier); the block waits on the barrier's phase with an
+// iteration cap.  Addresses and sizes must be multiples of 16 bytes.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// true once phase `parity` of the barrier has completed; false after the cap
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < kSpinLimit; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// Shared-memory layout of one pass: the tile's keys (loaded, then reused for
+// the keys in digit order), its values in load order and, per sorted slot,
+// the tile-local index the key came from.
+template <class K, class V, bool HAS_V, int ITEMS>
+constexpr size_t onesweep_smem() {
+  constexpr size_t T = (size_t)NT * ITEMS;
+  return T * sizeof(K) + (HAS_V ? T * sizeof(V) + T * sizeof(uint16_t) : 0);
+}
+
+// One stable 8-bit pass over tile `tile` (claimed in launch order).
+//  1. thread 0 starts bulk copies of the tile's keys and values into shared
+//     memory (full tiles with 16-byte aligned rows; otherwise plain loads);
+//  2. every warp ranks its 32*ITEMS keys (warp-striped, so a warp's keys are
+//     consecutive) with a warp multisplit against per-warp digit counters;
+//  3. the tile's digit counts go out for the decoupled look-back and come
+//     back as this tile's global base per digit;
+//  4. keys are staged in digit order (with their source slot when values
+//     ride along) and written out in runs, each value fetched from shared
+//     memory through its source slot.
 template <class K, class V, bool HAS_V, int ITEMS>
 __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
                                                  const V* __restrict__ vin, V* __restrict__ vout,
                                                  uint32_t n, int shift, int dbits,
                                                  const uint32_t* __restrict__ binoff,
                                                  uint32_t* lookback, uint32_t* tile_counter,
-                                                 uint32_t* status, int match_rank) {
+                                                 uint32_t* status, int match_rank, int bulk_ok) {
   constexpr uint32_t TILE = NT * ITEMS;
+  static_assert(TILE <= 65536, "source slots are 16-bit");
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_whist[NW][RADIX];
   __shared__ uint32_t s_dstart[RADIX];
   __shared__ uint32_t s_gbase[RADIX];
   __shared__ uint32_t s_scan[NW + 1];
+  __shared__ __align__(8) uint64_t s_bar[2];
   extern __shared__ __align__(16) unsigned char s_raw[];
   K* s_keys = reinterpret_cast<K*>(s_raw);
-  V* s_vals = reinterpret_cast<V*>(s_raw);
+  V* s_vin = reinterpret_cast<V*>(s_raw + (size_t)TILE * sizeof(K));
+  uint16_t* s_src = reinterpret_cast<uint16_t*>(s_raw + (size_t)TILE * (sizeof(K) + sizeof(V)));
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < NW * RADIX; i += NT) (&s_whist[0][0])[i] = 0;
-  const uint32_t tile = claim_tile(tile_counter, &s_tile);
+  if (tid == 0) {
+    s_tile = atomicAdd(tile_counter, 1u);
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const uint32_t tile = s_tile;
   const uint32_t base = tile * TILE;
+  const uint32_t tile_n = min(TILE, n - base);
+  const bool bulk = bulk_ok && tile_n == TILE;
+  if (bulk) {
+    if (tid == 0) {
+      mbar_expect_tx(&s_bar[0], TILE * (uint32_t)sizeof(K));
+      bulk_g2s(s_keys, kin + base, TILE * (uint32_t)sizeof(K), &s_bar[0]);
+      if constexpr (HAS_V) {
+        mbar_expect_tx(&s_bar[1], TILE * (uint32_t)sizeof(V));
+        bulk_g2s(s_vin, vin + base, TILE * (uint32_t)sizeof(V), &s_bar[1]);
+      }
+    }
+  } else {
+    for (uint32_t i = tid; i < tile_n; i += NT) {
+      s_keys[i] = kin[base + i];
+      if constexpr (HAS_V) s_vin[i] = vin[base + i];
+    }
+  }
   const uint32_t dmask = (1u << dbits) - 1;
-  const uint32_t wbase = base + (uint32_t)warp * 32u * ITEMS;
+  const uint32_t wloc = (uint32_t)warp * 32u * ITEMS;  // this warp's first tile slot
   const unsigned lt = lanemask_lt();
+  // every thread sees the keys (barrier phase, or the block barrier itself)
+  const bool ok = __syncthreads_and(bulk ? mbar_wait(&s_bar[0], 0) : true);
+  if (!ok) {
+    // the copy never completed: record it, give the values' copy a bounded
+    // wait too, and leave (successors' look-back waits are capped as well)
+    if (tid == 0) atomicOr(status, ST_LOOKBACK_TIMEOUT);
+    if (HAS_V) mbar_wait(&s_bar[1], 0);
+    return;
+  }
 
   K key[ITEMS];
   uint32_t rank[ITEMS];
 #pragma unroll
   for (int j = 0; j < ITEMS; j++) {
-    const uint32_t idx = wbase + j * 32 + lane;
-    key[j] = (idx < n) ? kin[idx] : K(0);
+    const uint32_t li = wloc + j * 32 + lane;
+    key[j] = li < tile_n ? s_keys[li] : K(0);
   }
   // Warp-level multisplit: peers = lanes of this warp holding the same digit.
 #pragma unroll
   for (int j = 0; j < ITEMS; j++) {
-    const uint32_t idx = wbase + j * 32 + lane;
-    const bool valid = idx < n;
+    const bool valid = wloc + j * 32 + lane < tile_n;
     const uint32_t d = (uint32_t)(key[j] >> shift) & dmask;
     unsigned peers;
     if (match_rank) {
@@ -149,13 +246,13 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
         }
       }
     }
-    uint32_t prior = valid ? s_whist[warp][d] : 0u;
+    const uint32_t prior = valid ? s_whist[warp][d] : 0u;
     rank[j] = prior + __popc(peers & lt);
     __syncwarp();
     if (valid && (peers & lt) == 0) s_whist[warp][d] = prior + __popc(peers);
     __syncwarp();
   }
-  __syncthreads();
+  __syncthreads();  // counters complete; every key of s_keys is in registers
 
   // Thread tid owns digit tid: warp-exclusive offsets and the tile count.
   uint32_t cnt = 0;
@@ -186,45 +283,36 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
     st_volatile(&lb[tid], kLb32P | (excl + cnt));
   }
   s_gbase[tid] = binoff[tid] + excl;
-  __syncthreads();
+  __syncthreads();  // s_dstart, s_gbase, warp offsets visible
 
-  // Stage keys in digit order, then write runs out.
-  uint32_t pos[ITEMS];
+  // Stage keys in digit order (and where each came from).
 #pragma unroll
   for (int j = 0; j < ITEMS; j++) {
-    const uint32_t idx = wbase + j * 32 + lane;
-    if (idx < n) {
+    const uint32_t li = wloc + j * 32 + lane;
+    if (li < tile_n) {
       const uint32_t d = (uint32_t)(key[j] >> shift) & dmask;
-      pos[j] = s_dstart[d] + s_whist[warp][d] + rank[j];
-      s_keys[pos[j]] = key[j];
+      const uint32_t pos = s_dstart[d] + s_whist[warp][d] + rank[j];
+      s_keys[pos] = key[j];
+      if constexpr (HAS_V) s_src[pos] = (uint16_t)li;
     }
   }
+  if constexpr (HAS_V) {
+    if (bulk && !mbar_wait(&s_bar[1], 0) && tid == 0) atomicOr(status, ST_LOOKBACK_TIMEOUT);
+  }
   __syncthreads();
-  const uint32_t tile_n = min(TILE, n - base);
-  uint32_t dst[ITEMS];
-#pragma unroll
+#pragma unroll 4
   for (int j = 0; j < ITEMS; j++) {
     const uint32_t i = j * NT + tid;
     if (i < tile_n) {
       const K k = s_keys[i];
       const uint32_t d = (uint32_t)(k >> shift) & dmask;
-      dst[j] = s_gbase[d] + (i - s_dstart[d]);
-      if (dst[j] < n) kout[dst[j]] = k;
-      else atomicOr(status, ST_BOUNDS);
-    }
-  }
-  if constexpr (HAS_V) {
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < ITEMS; j++) {
-      const uint32_t idx = wbase + j * 32 + lane;
-      if (idx < n) s_vals[pos[j]] = vin[idx];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < ITEMS; j++) {
-      const uint32_t i = j * NT + tid;
-      if (i < tile_n && dst[j] < n) vout[dst[j]] = s_vals[i];
+      const uint32_t dst = s_gbase[d] + (i - s_dstart[d]);
+      if (dst < n) {
+        kout[dst] = k;
+        if constexpr (HAS_V) vout[dst] = s_vin[s_src[i]];
+      } else {
+        atomicOr(status, ST_BOUNDS);
+      }
     }
   }
 }
@@ -267,7 +355,7 @@ void radix_sort_impl(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, boo
 
   const uint32_t ntiles = (uint32_t)ceil_div(n, TILE);
   DBuf<uint32_t> lookback(ctx, (uint64_t)ntiles * RADIX);
-  const size_t smem = (size_t)TILE * (has_vals ? std::max(sizeof(K), sizeof(V)) : sizeof(K));
+  const size_t smem = has_vals ? onesweep_smem<K, V, true, ITEMS>() : onesweep_smem<K, V, false, ITEMS>();
   for (int p = 0; p < passes; p++) {
     if (trivial[p]) continue;
     SK_CUDA(cudaMemsetAsync(lookback.p, 0, sizeof(uint32_t) * ntiles * RADIX, ctx->stream));
@@ -278,13 +366,15 @@ void radix_sort_impl(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, boo
       SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, *vals, *valt, (uint32_t)n, 8 * p, dbits,
                                               binoff.p + p * RADIX, lookback.p, counters + p,
-                                              ctx->d_status, ctx->tune_sort_match);
+                                              ctx->d_status, ctx->tune_sort_match,
+                                              aligned16(*keys) && aligned16(*vals) ? 1 : 0);
     } else {
       auto kern = k_onesweep<K, V, false, ITEMS>;
       SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, nullptr, nullptr, (uint32_t)n, 8 * p,
                                               dbits, binoff.p + p * RADIX, lookback.p,
-                                              counters + p, ctx->d_status, ctx->tune_sort_match);
+                                              counters + p, ctx->d_status, ctx->tune_sort_match,
+                                              aligned16(*keys) ? 1 : 0);
     }
     kprof_end(ctx, kh, 2 * n * (sizeof(K) + (has_vals ? sizeof(V) : 0)));
     after_launch(ctx, "k_onesweep");
@@ -363,7 +453,7 @@ void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* ou
   const int hblocks = (int)std::min<uint64_t>(ceil_div(n, NT * 16), 148 * 4);
   k_radix_hist<uint32_t><<<hblocks, NT, 0, stream>>>(in, n, 0, passes, hist);
   k_radix_bins<<<passes, NT, 0, stream>>>(hist, binoff);
-  const size_t smem = (size_t)TILE * sizeof(uint32_t);
+  const size_t smem = onesweep_smem<uint32_t, uint32_t, false, ITEMS>();
   const uint32_t* src = in;
   for (int p = 0; p < passes; p++) {
     // Ping-pong so that the last pass writes `out`.
@@ -371,7 +461,8 @@ void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* ou
     check_cuda(cudaMemsetAsync(lookback, 0, sizeof(uint32_t) * ntiles * RADIX, stream), "cudaMemsetAsync");
     auto kern = k_onesweep<uint32_t, uint32_t, false, ITEMS>;
     kern<<<ntiles, NT, smem, stream>>>(src, dst, nullptr, nullptr, (uint32_t)n, 8 * p, std::min(8, bits - 8 * p),
-                                       binoff + p * RADIX, lookback, counters + p, status, 0);
+                                       binoff + p * RADIX, lookback, counters + p, status, 0,
+                                       aligned16(src) ? 1 : 0);
     src = dst;
   }
   check_cuda(cudaGetLastError(), "launch");

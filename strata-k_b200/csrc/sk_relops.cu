@@ -298,6 +298,17 @@ __device__ uint64_t first_head_from(const K* keys, uint64_t n, uint64_t p) {
   return upper_bound_dev(keys, lo, hi, prev);
 }
 
+// Run-head boundaries of every reduce tile at once (one thread per boundary):
+// bounds[t] = first run head at or after t * tile_len, bounds[tiles] = n.
+template <class K>
+__global__ void k_rr_bounds(const K* __restrict__ keys, uint64_t n, uint32_t tiles, uint32_t tile_len,
+                            uint64_t* __restrict__ bounds) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > tiles) return;
+  const uint64_t p = t * tile_len;
+  bounds[t] = first_head_from(keys, n, p < n ? p : n);
+}
+
 template <class W>
 struct SegMin {  // segmented-min scan state: has a run start, min since it
   bool h;
@@ -314,8 +325,8 @@ __device__ __forceinline__ SegMin<W> seg_combine(SegMin<W> a, SegMin<W> b) {
 template <class K, class W, bool TROP>
 __global__ void __launch_bounds__(NT)
     k_reduce_runs(const K* __restrict__ keys, const W* __restrict__ w, uint64_t n, K* __restrict__ out,
-                  W* __restrict__ out_w, uint64_t* states, uint32_t* counter, uint64_t* d_count,
-                  uint32_t* status) {
+                  W* __restrict__ out_w, const uint64_t* __restrict__ bounds, uint64_t* states,
+                  uint32_t* counter, uint64_t* d_count, uint32_t* status) {
   constexpr int RR_ITEMS = RRCfg<K, W, TROP>::ITEMS;
   constexpr uint32_t RR_TILE = RRCfg<K, W, TROP>::TILE;
   __shared__ uint32_t s_tile;
@@ -325,26 +336,23 @@ __global__ void __launch_bounds__(NT)
   __shared__ W s_ow[TROP ? RR_TILE : 1];
   __shared__ uint32_t s_scan[NT / 32 + 1];
   __shared__ SegMin<W> s_seg[NT / 32];
-  __shared__ uint64_t s_se[2];
   __shared__ uint64_t s_excl;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t tile = claim_tile(counter, &s_tile);
-  if (tid == 0) {
-    const uint64_t p0 = (uint64_t)tile * RR_TILE;
-    const uint64_t p1 = p0 + RR_TILE < n ? p0 + RR_TILE : n;
-    s_se[0] = first_head_from(keys, n, p0);
-    s_se[1] = first_head_from(keys, n, p1);
-  }
-  __syncthreads();
-  const uint64_t s = s_se[0], e = s_se[1];
+  // this tile reduces the runs whose head lies in [tile*TILE, (tile+1)*TILE)
+  const uint64_t s = bounds[tile], e = bounds[tile + 1];
   uint32_t nout = 0;       // rows staged so far (uniform)
   W carry_m = W(0);        // min of the open run entering this chunk (Trop)
   bool carry_h = false;
   for (uint64_t c = s; c < e; c += RR_TILE) {
     const uint32_t clen = (uint32_t)((e - c) < RR_TILE ? (e - c) : RR_TILE);
-    for (uint32_t k = tid; k < clen; k += NT) {
-      s_k[k] = keys[c + k];
-      if constexpr (TROP) s_w[k] = w[c + k];
+#pragma unroll
+    for (int q = 0; q < RR_ITEMS; q++) {
+      const uint32_t k = q * NT + tid;
+      if (k < clen) {
+        s_k[k] = keys[c + k];
+        if constexpr (TROP) s_w[k] = w[c + k];
+      }
     }
     __syncthreads();
     const uint32_t b = tid * RR_ITEMS;
@@ -473,12 +481,24 @@ __device__ void md_split(const K* A, uint64_t na, const K* B, uint64_t nb, uint6
   *oj = j;
 }
 
+// Merge-path splits of every tile boundary at once (one thread per
+// diagonal): splits[2t], splits[2t+1] = md_split of diagonal min(t*MD_TILE, na+nb).
+template <class K>
+__global__ void k_md_bounds(const K* __restrict__ A, uint64_t na, const K* __restrict__ B, uint64_t nb,
+                            uint32_t tiles, uint64_t* __restrict__ splits) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > tiles) return;
+  const uint64_t L = na + nb, d = t * MD_TILE < L ? t * MD_TILE : L;
+  md_split(A, na, B, nb, d, &splits[2 * t], &splits[2 * t + 1]);
+}
+
 template <class K, class W, bool TROP, bool WRITE_FULL, bool WRITE_DELTA, bool INPLACE>
 __global__ void __launch_bounds__(NT)
     k_merge_diff(const K* __restrict__ A, W* Aw, uint64_t na, const K* __restrict__ B,
                  const W* __restrict__ Bw, uint64_t nb, K* __restrict__ fout, W* __restrict__ fout_w,
-                 K* __restrict__ dout, W* __restrict__ dout_w, uint64_t* fstates, uint64_t* dstates,
-                 uint32_t* counter, uint64_t* d_counts, uint32_t* status) {
+                 K* __restrict__ dout, W* __restrict__ dout_w, const uint64_t* __restrict__ splits,
+                 uint64_t* fstates, uint64_t* dstates, uint32_t* counter, uint64_t* d_counts,
+                 uint32_t* status) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   constexpr uint32_t CAP = MD_TILE + 2;
   K* s_a = reinterpret_cast<K*>(s_raw);
@@ -488,21 +508,11 @@ __global__ void __launch_bounds__(NT)
   uint32_t* s_mpre = reinterpret_cast<uint32_t*>(s_bw + (TROP ? CAP : 0));  // CAP + 1
   uint32_t* s_dpre = s_mpre + CAP + 1;                                      // CAP
   __shared__ uint32_t s_tile;
-  __shared__ uint64_t s_r[4];
   __shared__ uint32_t s_scan[NT / 32 + 1];
   __shared__ uint64_t s_ex[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t tile = claim_tile(counter, &s_tile);
-  const uint64_t L = na + nb;
-  if (tid == 0) {
-    const uint64_t d0 = (uint64_t)tile * MD_TILE;
-    const uint64_t d1 = d0 + MD_TILE < L ? d0 + MD_TILE : L;
-    uint64_t i0, j0, i1, j1;
-    md_split(A, na, B, nb, d0, &i0, &j0);
-    md_split(A, na, B, nb, d1, &i1, &j1);
-    s_r[0] = i0; s_r[1] = j0; s_r[2] = i1; s_r[3] = j1;
-  }
-  __syncthreads();
+  const uint64_t s_r[4] = {splits[2 * tile], splits[2 * tile + 1], splits[2 * tile + 2], splits[2 * tile + 3]};
   const uint64_t i0 = s_r[0], j0 = s_r[1];
   // Impossible for sorted unique inputs; checked so unsorted input cannot
   // index past shared memory.
@@ -511,17 +521,21 @@ __global__ void __launch_bounds__(NT)
   if (oversize && tid == 0) atomicOr(status, ST_BOUNDS);
   const uint32_t acnt = oversize ? 0u : (uint32_t)(s_r[2] - i0);
   const uint32_t bcnt = oversize ? 0u : (uint32_t)(s_r[3] - j0);
-  for (uint32_t k = tid; k < acnt; k += NT) {
-    s_a[k] = A[i0 + k];
-    if constexpr (TROP) s_aw[k] = Aw[i0 + k];
-  }
-  for (uint32_t k = tid; k < bcnt; k += NT) {
-    s_b[k] = B[j0 + k];
-    if constexpr (TROP) s_bw[k] = Bw[j0 + k];
+  constexpr int BI = (MD_TILE + 2 + NT - 1) / NT;
+#pragma unroll
+  for (int q = 0; q < BI; q++) {
+    const uint32_t k = q * NT + tid;
+    if (k < acnt) {
+      s_a[k] = A[i0 + k];
+      if constexpr (TROP) s_aw[k] = Aw[i0 + k];
+    }
+    if (k < bcnt) {
+      s_b[k] = B[j0 + k];
+      if constexpr (TROP) s_bw[k] = Bw[j0 + k];
+    }
   }
   __syncthreads();
   // Per B element: rank in A, matched?, delta?
-  constexpr int BI = (MD_TILE + 2 + NT - 1) / NT;
   uint32_t b_ra[BI];
   uint32_t mflag = 0, dflag = 0;  // bit per item
   uint32_t mcount = 0, dcount = 0;
@@ -908,12 +922,16 @@ void reduce_runs(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, K* out,
     return;
   }
   const uint32_t tiles = (uint32_t)ceil_div(n, RRCfg<K, W, TROP>::TILE);
-  DBuf<uint64_t> states(ctx, tiles + 1);
+  DBuf<uint64_t> states(ctx, 2ull * tiles + 2);
+  uint64_t* bounds = states.p + tiles + 1;  // tiles + 1 entries
   uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles);
   SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 1), ctx->stream));
+  k_rr_bounds<K><<<(unsigned)ceil_div(tiles + 1, NT), NT, 0, ctx->stream>>>(keys, n, tiles,
+                                                                           RRCfg<K, W, TROP>::TILE, bounds);
+  after_launch(ctx, "k_rr_bounds");
   const int kh = kprof_begin(ctx, K_REDUCE_RUNS);
-  k_reduce_runs<K, W, TROP><<<tiles, NT, 0, ctx->stream>>>(keys, w, n, out, out_w, states.p, counter,
-                                                           d_count, ctx->d_status);
+  k_reduce_runs<K, W, TROP><<<tiles, NT, 0, ctx->stream>>>(keys, w, n, out, out_w, bounds, states.p,
+                                                           counter, d_count, ctx->d_status);
   kprof_end(ctx, kh, n * (sizeof(K) + (TROP ? sizeof(W) : 0)));  // reads; writes added on read-back
   after_launch(ctx, "k_reduce_runs");
 }
@@ -927,16 +945,19 @@ static void launch_merge(strata_ctx* ctx, const K* full, W* full_w, uint64_t nf,
     return;
   }
   const uint32_t tiles = (uint32_t)ceil_div(nf + nc, MD_TILE);
-  DBuf<uint64_t> states(ctx, 2ull * tiles + 1);
+  DBuf<uint64_t> states(ctx, 2ull * tiles + 1 + 2ull * (tiles + 1));
   uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + 2ull * tiles);
+  uint64_t* splits = states.p + 2ull * tiles + 1;
   SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (2ull * tiles + 1), ctx->stream));
+  k_md_bounds<K><<<(unsigned)ceil_div(tiles + 1, NT), NT, 0, ctx->stream>>>(full, nf, cand, nc, tiles, splits);
+  after_launch(ctx, "k_md_bounds");
   constexpr uint32_t CAP = MD_TILE + 2;
   const size_t smem = 2 * CAP * sizeof(K) + (TROP ? 2 * CAP * sizeof(W) : 0) + (2 * CAP + 1) * sizeof(uint32_t);
   auto kern = k_merge_diff<K, W, TROP, WF, WD, IP>;
   SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int kh = kprof_begin(ctx, K_MERGE_DIFF);
   kern<<<tiles, NT, smem, ctx->stream>>>(full, full_w, nf, cand, cand_w, nc, fout, fout_w, dout,
-                                         dout_w, states.p, states.p + tiles, counter, d_counts,
+                                         dout_w, splits, states.p, states.p + tiles, counter, d_counts,
                                          ctx->d_status);
   kprof_end(ctx, kh, (nf + nc) * (sizeof(K) + (TROP ? sizeof(W) : 0)));  // reads; writes added on read-back
   after_launch(ctx, "k_merge_diff");
