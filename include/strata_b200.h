@@ -105,17 +105,19 @@ strata_status strata_ctx_set_plan(strata_ctx* ctx, int plan);
  *   STRATA_KNOB_SORT_ITEMS_U32  keys per thread of a radix tile, u32 keys: 11, 15, 19, 23
  *   STRATA_KNOB_SORT_ITEMS_U64  keys per thread of a radix tile, u64 keys: 7, 9, 13
  *   STRATA_KNOB_TRI_PROBE       triangle membership test: 1 shared-memory hash set,
- *                               2 binary search of the sorted out-list
+ *                               2 binary search of the sorted out-list, 3 shared-memory
+ *                               bitmap filter with queued binary searches
  *   STRATA_KNOB_BATCH_GRAPH_ROUNDS  bit-row rounds per CUDA-graph replay: 2, 4, 8, 16, 32
  *   STRATA_KNOB_BATCH_BLOCKS_PER_SM resident blocks per SM of the round kernel: 1..32
  *   STRATA_KNOB_BATCH_BUDGET_MB     cap on one batch wave's device bytes, in MiB (>= 1)
- *   STRATA_KNOB_SORT_RANK           radix digit ranking: 1 per-bit warp ballots, 2 match instruction
+ *   STRATA_KNOB_SORT_RANK           radix digit ranking: 1 per-bit warp ballots, 2 match instruction,
+ *                                   3 shared-memory peer masks
  *   STRATA_KNOB_DENSE_WORD_MEMBERS  direct-addressed rounds: Δ words with at least this many
  *                                   members take the bit-lane expand path: 1..33 (33 = never)
  *   STRATA_KNOB_WEIGHT_LANES        Trop weight lanes: 8 = always int64 (otherwise int32 lanes
  *                                   are used when every sum within the round cap provably fits)
- * value 0 restores the default (15 / 9 / 2 / 8 / occupancy limit / 70% of
- * reusable memory / ballots / 24 / automatic).  Other values: STRATA_E_INVALID.
+ * value 0 restores the default (15 / 9 / 3 / 8 / occupancy limit / 70% of
+ * reusable memory / shared masks / 24 / automatic).  Other values: STRATA_E_INVALID.
  * The autotuner (strata_b200.tune) sweeps these and caches the best per GPU.
  * No counterpart in the reference (its sort has no tile parameters). */
 #define STRATA_KNOB_SORT_ITEMS_U32 1

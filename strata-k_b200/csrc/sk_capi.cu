@@ -214,8 +214,9 @@ strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value) {
     return STRATA_OK;
   }
   if (knob == STRATA_KNOB_SORT_RANK) {
-    if (value < 0 || value > 2) return bad(ctx, "radix ranking must be 0 (default), 1 (ballots) or 2 (match)");
-    ctx->tune_sort_match = value == 2 ? 1 : 0;
+    if (value < 0 || value > 3)
+      return bad(ctx, "radix ranking must be 0 (default), 1 (ballots), 2 (match) or 3 (shared masks)");
+    ctx->tune_sort_rank = value == 1 ? 0 : value == 2 ? 1 : 2;
     return STRATA_OK;
   }
   if (knob == STRATA_KNOB_DENSE_WORD_MEMBERS) {
@@ -229,7 +230,8 @@ strata_status strata_ctx_set_knob(strata_ctx* ctx, int knob, int value) {
     return STRATA_OK;
   }
   if (knob == STRATA_KNOB_TRI_PROBE) {
-    if (value < 0 || value > 2) return bad(ctx, "triangle probe must be 0 (default), 1 (hash set) or 2 (binary search)");
+    if (value < 0 || value > 3)
+      return bad(ctx, "triangle probe must be 0 (default), 1 (hash set), 2 (binary search) or 3 (bitmap filter)");
     ctx->tune_tri_probe = value;
     return STRATA_OK;
   }

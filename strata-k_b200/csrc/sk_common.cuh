@@ -80,8 +80,8 @@ struct strata_ctx {
   int plan = 0;                     // 0 auto, 1 sort-merge, 2 direct-addressed
   int tune_items4 = 0;              // radix keys per thread, u32 keys (0 = default)
   int tune_items8 = 0;              // radix keys per thread, u64 keys (0 = default)
-  int tune_sort_match = 0;          // radix ranking: 0 bit ballots, 1 match instruction
-  int tune_tri_probe = 0;           // triangle membership test: 1 hash set, 0/2 binary search
+  int tune_sort_rank = 2;           // radix ranking: 0 bit ballots, 1 match instruction, 2 shared masks
+  int tune_tri_probe = 0;           // triangle membership test: 1 hash set, 2 binary search, 0/3 bitmap filter
   int tune_bs_graph_rounds = 0;     // bit-row rounds per CUDA-graph replay (0 = 8)
   int tune_bs_blocks = 0;           // resident round-kernel blocks per SM (0 = occupancy limit)
   uint64_t tune_bs_budget_mb = 0;   // cap on a batch wave's device bytes, MiB (0 = 70% of free)

@@ -18,6 +18,7 @@
 #include "sk_ops.cuh"
 #include "sk_prims.cuh"
 
+#include <type_traits>
 #include <vector>
 
 namespace sk {
@@ -138,10 +139,14 @@ inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 // Shared-memory layout of one pass: the tile's keys (loaded, then reused for
 // the keys in digit order), its values in load order and, per sorted slot,
 // the tile-local index the key came from.
+// The source-slot region doubles as the per-warp peer masks of the
+// shared-mask ranking, so it is at least NW * RADIX words.
 template <class K, class V, bool HAS_V, int ITEMS>
 constexpr size_t onesweep_smem() {
   constexpr size_t T = (size_t)NT * ITEMS;
-  return T * sizeof(K) + (HAS_V ? T * sizeof(V) + T * sizeof(uint16_t) : 0);
+  constexpr size_t src = HAS_V ? T * sizeof(uint16_t) : 0;
+  constexpr size_t peer = (size_t)NW * RADIX * sizeof(uint32_t);
+  return T * sizeof(K) + (HAS_V ? T * sizeof(V) : 0) + (src > peer ? src : peer);
 }
 
 // One stable 8-bit pass over tile `tile` (claimed in launch order).
@@ -154,13 +159,14 @@ constexpr size_t onesweep_smem() {
 //  4. keys are staged in digit order (with their source slot when values
 //     ride along) and written out in runs, each value fetched from shared
 //     memory through its source slot.
-template <class K, class V, bool HAS_V, int ITEMS>
+template <class K, class V, bool HAS_V, int ITEMS, int RANK>
 __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
                                                  const V* __restrict__ vin, V* __restrict__ vout,
                                                  uint32_t n, int shift, int dbits,
                                                  const uint32_t* __restrict__ binoff,
                                                  uint32_t* lookback, uint32_t* tile_counter,
-                                                 uint32_t* status, int match_rank, int bulk_ok) {
+                                                 uint32_t* status, int bulk_ok) {
+  constexpr int rank_mode = RANK;  // 0 ballots, 1 match instruction, 2 shared masks
   constexpr uint32_t TILE = NT * ITEMS;
   static_assert(TILE <= 65536, "source slots are 16-bit");
   __shared__ uint32_t s_tile;
@@ -172,10 +178,13 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
   extern __shared__ __align__(16) unsigned char s_raw[];
   K* s_keys = reinterpret_cast<K*>(s_raw);
   V* s_vin = reinterpret_cast<V*>(s_raw + (size_t)TILE * sizeof(K));
-  uint16_t* s_src = reinterpret_cast<uint16_t*>(s_raw + (size_t)TILE * (sizeof(K) + sizeof(V)));
+  uint16_t* s_src = reinterpret_cast<uint16_t*>(s_raw + (size_t)TILE * (sizeof(K) + (HAS_V ? sizeof(V) : 0)));
+  uint32_t* s_peer = reinterpret_cast<uint32_t*>(s_src);  // [NW][RADIX], ranking only
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < NW * RADIX; i += NT) (&s_whist[0][0])[i] = 0;
+  if (rank_mode == 2)
+    for (int i = tid; i < NW * RADIX; i += NT) s_peer[i] = 0;
   if (tid == 0) {
     s_tile = atomicAdd(tile_counter, 1u);
     mbar_init(&s_bar[0], 1);
@@ -228,7 +237,14 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
     const bool valid = wloc + j * 32 + lane < tile_n;
     const uint32_t d = (uint32_t)(key[j] >> shift) & dmask;
     unsigned peers;
-    if (match_rank) {
+    if (rank_mode == 2) {
+      // shared-mask ranking: each lane ORs its bit into its digit's mask;
+      // after the warp barrier the mask is the set of peers
+      uint32_t* pm = &s_peer[warp * RADIX + d];
+      if (valid) atomicOr(pm, 1u << lane);
+      __syncwarp();
+      peers = valid ? *pm : 0u;
+    } else if (rank_mode == 1) {
       // one match instruction (invalid lanes carry a digit no valid lane has)
       peers = __match_any_sync(kFull, valid ? d : (0x100u | (uint32_t)lane));
     } else {
@@ -249,7 +265,10 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
     const uint32_t prior = valid ? s_whist[warp][d] : 0u;
     rank[j] = prior + __popc(peers & lt);
     __syncwarp();
-    if (valid && (peers & lt) == 0) s_whist[warp][d] = prior + __popc(peers);
+    if (valid && (peers & lt) == 0) {
+      s_whist[warp][d] = prior + __popc(peers);
+      if (rank_mode == 2) s_peer[warp * RADIX + d] = 0u;
+    }
     __syncwarp();
   }
   __syncthreads();  // counters complete; every key of s_keys is in registers
@@ -361,20 +380,26 @@ void radix_sort_impl(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, boo
     SK_CUDA(cudaMemsetAsync(lookback.p, 0, sizeof(uint32_t) * ntiles * RADIX, ctx->stream));
     const int dbits = std::min(8, bits - 8 * p);
     const int kh = kprof_begin(ctx, K_ONESWEEP);
-    if (has_vals) {
-      auto kern = k_onesweep<K, V, true, ITEMS>;
-      SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, *vals, *valt, (uint32_t)n, 8 * p, dbits,
-                                              binoff.p + p * RADIX, lookback.p, counters + p,
-                                              ctx->d_status, ctx->tune_sort_match,
-                                              aligned16(*keys) && aligned16(*vals) ? 1 : 0);
-    } else {
-      auto kern = k_onesweep<K, V, false, ITEMS>;
-      SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, nullptr, nullptr, (uint32_t)n, 8 * p,
-                                              dbits, binoff.p + p * RADIX, lookback.p,
-                                              counters + p, ctx->d_status, ctx->tune_sort_match,
-                                              aligned16(*keys) ? 1 : 0);
+    auto go = [&](auto rank_tag) {
+      constexpr int RK = decltype(rank_tag)::value;
+      if (has_vals) {
+        auto kern = k_onesweep<K, V, true, ITEMS, RK>;
+        SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, *vals, *valt, (uint32_t)n, 8 * p, dbits,
+                                                binoff.p + p * RADIX, lookback.p, counters + p, ctx->d_status,
+                                                aligned16(*keys) && aligned16(*vals) ? 1 : 0);
+      } else {
+        auto kern = k_onesweep<K, V, false, ITEMS, RK>;
+        SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, nullptr, nullptr, (uint32_t)n, 8 * p, dbits,
+                                                binoff.p + p * RADIX, lookback.p, counters + p, ctx->d_status,
+                                                aligned16(*keys) ? 1 : 0);
+      }
+    };
+    switch (ctx->tune_sort_rank) {
+      case 0: go(std::integral_constant<int, 0>{}); break;
+      case 1: go(std::integral_constant<int, 1>{}); break;
+      default: go(std::integral_constant<int, 2>{}); break;
     }
     kprof_end(ctx, kh, 2 * n * (sizeof(K) + (has_vals ? sizeof(V) : 0)));
     after_launch(ctx, "k_onesweep");
@@ -459,9 +484,9 @@ void radix_sort_u32_static(cudaStream_t stream, const uint32_t* in, uint32_t* ou
     // Ping-pong so that the last pass writes `out`.
     uint32_t* dst = ((passes - 1 - p) % 2 == 0) ? out : alt;
     check_cuda(cudaMemsetAsync(lookback, 0, sizeof(uint32_t) * ntiles * RADIX, stream), "cudaMemsetAsync");
-    auto kern = k_onesweep<uint32_t, uint32_t, false, ITEMS>;
+    auto kern = k_onesweep<uint32_t, uint32_t, false, ITEMS, 2>;
     kern<<<ntiles, NT, smem, stream>>>(src, dst, nullptr, nullptr, (uint32_t)n, 8 * p, std::min(8, bits - 8 * p),
-                                       binoff + p * RADIX, lookback, counters + p, status, 0,
+                                       binoff + p * RADIX, lookback, counters + p, status,
                                        aligned16(src) ? 1 : 0);
     src = dst;
   }

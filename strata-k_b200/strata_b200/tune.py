@@ -23,10 +23,10 @@ KNOBS = {
 }
 # other knobs: id -> choices (0 = the built-in default)
 OTHER = {
-    3: (1, 2),                # triangle membership test: hash set / binary search
+    3: (1, 2, 3),             # triangle membership test: hash set / binary search / bitmap filter
     4: (2, 4, 8, 16, 32),     # bit-row rounds per CUDA-graph replay (batched closure)
     5: (0, 2, 4, 8),          # resident round-kernel blocks per SM (0 = occupancy limit)
-    7: (1, 2),                # radix digit ranking: ballots / match instruction
+    7: (1, 2, 3),             # radix digit ranking: ballots / match instruction / shared masks
     8: (8, 12, 16, 20, 24, 33),  # Δ-word members from which the bit-lane expand path runs (33 = never)
 }
 

@@ -377,11 +377,13 @@ def test_triangle_pattern_rmat_oriented(engine):
     assert engine.count_triangles((wl.src, wl.dst)) == want
 
 
-@pytest.mark.parametrize("probe", [1, 2])
+@pytest.mark.parametrize("probe", [1, 2, 3])
 def test_triangle_probe_knob(engine, probe):
-    """Both membership tests (shared-memory hash set, binary search) give the
-    oracle's count, including a vertex whose out-list exceeds the hash table
-    (it falls back to the binary search) and R-MAT skew."""
+    """Every membership test (shared-memory hash set, binary search, bitmap
+    filter with queued searches) gives the oracle's count, including a vertex
+    whose out-list exceeds the staged list (it falls back to the binary
+    search), R-MAT skew and a dense graph whose warps fill the search queue
+    many times over."""
     engine.set_knob(3, probe)
     try:
         big = 3000  # X=0 -> 1..3000, i -> i+1: 2999 triangles through the wide vertex
@@ -391,6 +393,8 @@ def test_triangle_probe_knob(engine, probe):
         wl = gen.triangle_workload(scale=13, edge_factor=16, seed=4)
         assert engine.count_triangle_pattern((wl.src, wl.dst)) == O.count_pattern(wl.src, wl.dst)
         rng = np.random.default_rng(probe)
+        a, b = rng.integers(0, 400, 40_000), rng.integers(0, 400, 40_000)
+        assert engine.count_triangle_pattern((a, b)) == O.count_pattern(a, b)
         for _ in range(10):
             n = int(rng.integers(5, 2000))
             m = int(rng.integers(1, 20 * n))
@@ -613,9 +617,9 @@ def test_sort_knobs_fixpoint_identical(engine):
     engine.set_plan(0)
 
 
-@pytest.mark.parametrize("rank", [1, 2])
+@pytest.mark.parametrize("rank", [1, 2, 3])
 def test_sort_rank_methods_identical(engine, rank):
-    """Ballot and match-instruction digit ranking sort identically (stable)."""
+    """Ballot, match-instruction and shared-mask digit ranking sort identically (stable)."""
     import ctypes as C
     engine.set_knob(7, rank)
     try:
