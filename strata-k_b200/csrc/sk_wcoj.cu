@@ -82,6 +82,104 @@ __global__ void __launch_bounds__(TC_NT)
   if (lane == 0 && count) atomicAdd(total, count);
 }
 
+// Filtered probe (default).  Most candidates Z of a warp's expansion are not
+// in out(X): the warp also sets one bit per out(X) entry in a small
+// shared-memory bitmap (hash of Z, 16 bits per entry up to 8,192 bits, so a
+// non-member passes with probability <= 1 - e^(-1/16) ~ 6 %, a member always),
+// answers most candidates with one shared-memory load, and queues the ones
+// that pass; whenever 32 are queued the whole warp binary-searches them
+// together, so the searches run without idle lanes.  Exact: the bitmap has no
+// false negatives and every queued candidate is searched once.
+constexpr uint32_t TF_WORDS = 256;  // 8,192-bit filter per warp
+constexpr uint32_t TF_MIN = 16;     // out-degree from which the filter pays for its setup
+
+__device__ __forceinline__ uint32_t tf_hash(uint32_t z, int lg) { return (z * 0x85EBCA77u) >> (32 - lg); }
+
+__global__ void __launch_bounds__(TC_NT)
+    k_tri_count_filt(const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr, uint64_t n_nodes,
+                     uint32_t* counter, unsigned long long* total, uint32_t u_lo, uint32_t u_hi) {
+  __shared__ uint32_t s_list[TC_WARPS][TC_STAGE];
+  __shared__ uint32_t s_filt[TC_WARPS][TF_WORDS];
+  __shared__ uint32_t s_q[TC_WARPS][64];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = lanemask_lt();
+  uint32_t* q = s_q[warp];
+  uint32_t* F = s_filt[warp];
+  unsigned long long count = 0;
+  while (true) {
+    uint32_t u = 0;
+    if (lane == 0) u = u_lo + atomicAdd(counter, 1u);
+    u = __shfl_sync(kFull, u, 0);
+    if (u >= u_hi || u >= n_nodes) break;
+    const uint32_t a0 = off[u], du = off[u + 1] - a0;
+    if (du == 0) continue;
+    const bool staged = du <= TC_STAGE;
+    const bool filt = staged && du >= TF_MIN;
+    // filter size: 16 bits per entry, 512 .. 8,192 bits
+    int lg = 9;
+    while (filt && lg < 13 && (1u << lg) < 16u * du) lg++;
+    if (staged) {
+      for (uint32_t k = lane; k < du; k += 32) s_list[warp][k] = nbr[a0 + k];
+    }
+    if (filt) {
+      for (uint32_t k = lane; k < (1u << (lg - 5)); k += 32) F[k] = 0u;
+      __syncwarp();
+      for (uint32_t k = lane; k < du; k += 32) {
+        const uint32_t h = tf_hash(s_list[warp][k], lg);
+        atomicOr(&F[h >> 5], 1u << (h & 31));
+      }
+    }
+    __syncwarp();
+    const uint32_t* A = staged ? s_list[warp] : nbr + a0;
+    uint32_t qn = 0;  // queued candidates (uniform)
+    for (uint32_t c = 0; c < du; c += 32) {
+      const uint32_t i = c + lane;
+      const bool valid = i < du;
+      const uint32_t v = valid ? A[i] : 0u;
+      const uint32_t dv = (valid && v < n_nodes) ? off[v + 1] - off[v] : 0u;
+      const uint32_t sv = (valid && v < n_nodes) ? off[v] : 0u;
+      const uint32_t incl = warp_incl_sum(dv);
+      const uint32_t ex = incl - dv;
+      const uint32_t D = __shfl_sync(kFull, incl, 31);
+      for (uint32_t base = 0; base < D; base += 32) {
+        const uint32_t j = base + lane;
+        const bool ok = j < D;
+        // owner lane t = number of lanes whose inclusive prefix is <= j
+        int t = 0;
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+          const uint32_t val = __shfl_sync(kFull, incl, t + s - 1);
+          if (val <= j) t += s;
+        }
+        const uint32_t ex_t = __shfl_sync(kFull, ex, t);
+        const uint32_t sv_t = __shfl_sync(kFull, sv, t);
+        const uint32_t w = ok ? nbr[sv_t + (j - ex_t)] : 0u;
+        if (!filt) {
+          if (ok && bsearch_u32(A, du, w)) count++;
+          continue;
+        }
+        const uint32_t h = tf_hash(w, lg);
+        const bool pass = ok && ((F[h >> 5] >> (h & 31)) & 1u);
+        const unsigned bal = __ballot_sync(kFull, pass);
+        if (pass) q[qn + __popc(bal & lt)] = w;
+        qn += __popc(bal);
+        __syncwarp();
+        if (qn >= 32) {
+          if (bsearch_u32(A, du, q[lane])) count++;
+          __syncwarp();
+          if ((uint32_t)lane + 32 < qn) q[lane] = q[lane + 32];
+          qn -= 32;
+          __syncwarp();
+        }
+      }
+    }
+    if (qn > 0 && (uint32_t)lane < qn && bsearch_u32(A, du, q[lane])) count++;
+    __syncwarp();
+  }
+  count = warp_sum(count);
+  if (lane == 0 && count) atomicAdd(total, count);
+}
+
 // Hash-probe variant (STRATA_KNOB_TRI_PROBE = 1; measured slower than the
 // binary search on R-MAT-22, which stays the default: the 8 KB table per warp
 // cuts residency to 24 warps per SM and the probe loop diverges).  The warp
@@ -368,7 +466,12 @@ uint64_t tri_from_sorted(strata_ctx* ctx, const K* keys, uint64_t m, int bits, u
   SK_CUDA(cudaMemsetAsync(acc.p, 0, 24, ctx->stream));
   const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(n_nodes, TC_WARPS), (uint64_t)ctx->num_sms * 8);
   const int kh = kprof_begin(ctx, K_TRI_COUNT);
-  if (ctx->tune_tri_probe != 1) {
+  if (ctx->tune_tri_probe == 0 || ctx->tune_tri_probe == 3) {
+    k_tri_count_filt<<<grid ? grid : 1, TC_NT, 0, ctx->stream>>>(off.p, nbr.p, n_nodes,
+                                                                 reinterpret_cast<uint32_t*>(acc.p + 1),
+                                                                 reinterpret_cast<unsigned long long*>(acc.p),
+                                                                 (uint32_t)u_lo, (uint32_t)u_hi);
+  } else if (ctx->tune_tri_probe == 2) {
     k_tri_count<<<grid ? grid : 1, TC_NT, 0, ctx->stream>>>(off.p, nbr.p, n_nodes,
                                                             reinterpret_cast<uint32_t*>(acc.p + 1),
                                                             reinterpret_cast<unsigned long long*>(acc.p),
