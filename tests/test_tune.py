@@ -32,7 +32,7 @@ def test_load_keeps_every_swept_knob():
     round trip; values outside a knob's choices are dropped."""
     import tempfile
     from pathlib import Path
-    best = {1: 15, 2: 9, 3: 2, 4: 4, 5: 2, 7: 1, 8: 24}
+    best = {1: 15, 2: 9, 3: 3, 4: 4, 5: 2, 7: 3, 8: 24}
     with tempfile.TemporaryDirectory() as d:
         p = Path(d) / "tune.json"
         tune.save({"gpu": "GPU A", "best": best}, p)
