@@ -94,6 +94,8 @@ struct PvView {
   const uint32_t* live;    // [τ] target still changing
   uint32_t* changed;       // [τ] a tuple of τ changed this round
   uint32_t* status;
+  uint32_t* last;          // [τ * n + X] last round in which (τ, X) changed (0: never)
+  uint32_t round;          // this round, 1-based
 };
 
 __global__ void __launch_bounds__(PV_NT) k_prov_round(PvView v) {
@@ -110,6 +112,21 @@ __global__ void __launch_bounds__(PV_NT) k_prov_round(PvView v) {
     const uint32_t tau = (uint32_t)(pair / v.n);
     const uint32_t X = (uint32_t)(pair - (uint64_t)tau * v.n);
     if (!v.live[tau]) continue;  // uniform per half-warp
+    // A tuple none of whose inputs — itself and path(Y, t) for its edges
+    // (X, Y); the rule-1 edge never changes — changed in the previous round
+    // re-derives exactly what it derived then, and its slot in the buffer
+    // being written still holds that set (it did not change either): skip
+    // it.  A stamp read while another half-warp raises it to this round is
+    // >= round - 1 and only makes the test conservative.
+    if (v.round >= 2) {
+      const uint32_t lim = v.round - 1;
+      bool hot = hl == 0 && v.last[pair] >= lim;
+      for (uint32_t e = v.off[X] + hl; e < v.off[X + 1]; e += 16) {
+        const uint32_t y = v.nbr[e];
+        if (y < v.n && v.last[(uint64_t)tau * v.n + y] >= lim) hot = true;
+      }
+      if ((__ballot_sync(hmask, hot) & hmask) == 0u) continue;
+    }
     const uint32_t t = v.tgt[tau];
     int bank = 0;
     uint32_t s_cnt = v.cnt_prev[pair];
@@ -275,7 +292,10 @@ __global__ void __launch_bounds__(PV_NT) k_prov_round(PvView v) {
       r->sig = sig;
       r->w = w;
     }
-    if (changed && hl == 0) atomicOr(&v.changed[tau], 1u);
+    if (changed && hl == 0) {
+      atomicOr(&v.changed[tau], 1u);
+      v.last[pair] = v.round;
+    }
     __syncwarp(hmask);
   }
   if (flags) atomicOr(v.status, flags);
@@ -354,7 +374,7 @@ void prov_tc_capture(strata_ctx* ctx, uint32_t n, const uint32_t* d_src, const u
   std::vector<uint32_t> targets(qt, qt + nq);
   std::sort(targets.begin(), targets.end());
   targets.erase(std::unique(targets.begin(), targets.end()), targets.end());
-  const uint64_t per_target = 2ull * n * (PV_KMAX * sizeof(ProofRec) + 1);
+  const uint64_t per_target = 2ull * n * (PV_KMAX * sizeof(ProofRec) + 1) + 4ull * n;
   release_all_cached(ctx);
   uint64_t budget = (uint64_t)((double)reusable_device_bytes(ctx) * 0.5);
   if (ctx->cap && ctx->cap > ctx->in_use) budget = std::min<uint64_t>(budget, ctx->cap - ctx->in_use);
@@ -364,7 +384,7 @@ void prov_tc_capture(strata_ctx* ctx, uint32_t n, const uint32_t* d_src, const u
   if (per_target > budget) fail(STRATA_E_OOM, "one target's proof states exceed the memory budget");
   DBuf<uint8_t> cntA(ctx, tw * n + 1), cntB(ctx, tw * n + 1);
   DBuf<ProofRec> recA(ctx, tw * n * PV_KMAX + 1), recB(ctx, tw * n * PV_KMAX + 1);
-  DBuf<uint32_t> d_tgt(ctx, tw), d_live(ctx, tw), d_changed(ctx, tw);
+  DBuf<uint32_t> d_tgt(ctx, tw), d_live(ctx, tw), d_changed(ctx, tw), d_last(ctx, tw * n + 1);
   DBuf<uint32_t> d_qtau(ctx, nq + 1), d_qs(ctx, nq + 1);
   DBuf<uint8_t> d_ocnt(ctx, nq + 1);
   DBuf<ProofRec> d_orec(ctx, (uint64_t)nq * PV_KMAX + 1);
@@ -385,15 +405,17 @@ void prov_tc_capture(strata_ctx* ctx, uint32_t n, const uint32_t* d_src, const u
     SK_CUDA(cudaMemcpyAsync(d_tgt.p, targets.data() + w0, nt * 4, cudaMemcpyHostToDevice, ctx->stream));
     SK_CUDA(cudaMemsetAsync(cntA.p, 0, (uint64_t)nt * n, ctx->stream));
     SK_CUDA(cudaMemsetAsync(cntB.p, 0, (uint64_t)nt * n, ctx->stream));
+    SK_CUDA(cudaMemsetAsync(d_last.p, 0, (uint64_t)nt * n * 4, ctx->stream));
     std::fill(h_live.begin(), h_live.end(), 1u);
     SK_CUDA(cudaMemcpyAsync(d_live.p, h_live.data(), nt * 4, cudaMemcpyHostToDevice, ctx->stream));
     PvView v{n, off.p, nbr.p, idx.p, d_prob, d_tgt.p, nt, k, cntA.p, recA.p, cntB.p, recB.p,
-             d_live.p, d_changed.p, ctx->d_status};
+             d_live.p, d_changed.p, ctx->d_status, d_last.p, 0};
     bool a_is_prev = true;
     uint32_t live_count = nt;
     uint32_t r = 0;
     while (live_count) {
       r++;
+      v.round = r;
       v.cnt_prev = a_is_prev ? cntA.p : cntB.p;
       v.rec_prev = a_is_prev ? recA.p : recB.p;
       v.cnt_next = a_is_prev ? cntB.p : cntA.p;
