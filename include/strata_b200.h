@@ -299,6 +299,18 @@ strata_status strata_tc_shard_seed(strata_ctx* ctx, strata_tc_shard* sh, void* d
  * STRATA_E_INVALID); *n_delta = |Delta'| of its rows. */
 strata_status strata_tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const void* d_delta_full,
     const uint8_t* d_flags_full, void* d_delta_mine, uint8_t* d_flags_mine, uint64_t* n_delta);
+/* Sparse exchange of a round's Delta': the rank's nonzero 128-bit words as
+ * (global word index, low 64 bits, high 64 bits) int64 triples.  pack writes
+ * min(count, cap) triples to d_out (cap x 3 int64; slots past the count get
+ * index -1) and *n_words = the count, so cap = 0 only counts.  unpack clears
+ * the gathered Delta and row flags and scatters n triples (index -1 skipped)
+ * into them; the triples may not overlap the gathered Delta.  Used instead of
+ * the slice all-gather when the largest rank's count x 24 bytes is well below
+ * the slice size. */
+strata_status strata_tc_shard_pack(strata_ctx* ctx, strata_tc_shard* sh, const void* d_delta_mine,
+    int64_t* d_out, uint64_t cap, uint64_t* n_words);
+strata_status strata_tc_shard_unpack(strata_ctx* ctx, strata_tc_shard* sh, const int64_t* d_in, uint64_t n,
+    void* d_delta_full, uint8_t* d_flags_full);
 /* |path| of the rank's rows and their part of the fingerprint. */
 strata_status strata_tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count,
     uint64_t* fingerprint);

@@ -1124,6 +1124,89 @@ void tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count, uin
   *fp = h[1];
 }
 
+// ---- sparse Δ exchange -------------------------------------------------------
+// When a round's Δ' is sparse, the ranks exchange only its nonzero 128-bit
+// words: each rank packs (global word index, low 64 bits, high 64 bits)
+// triples of its slice, the triples of all ranks are gathered, and every rank
+// rebuilds the full Δ and its row flags from them.  The bytes on the wire are
+// 24 per nonzero word instead of the whole slice.
+
+// Nonzero words of the slice, written at claimed slots below `cap`; *count
+// receives the total (which may exceed cap).
+__global__ void k_shard_pack(const uint4* __restrict__ D, uint64_t words, uint64_t row0_word, uint64_t cap,
+                             long long* __restrict__ out, unsigned long long* count) {
+  const int lane = threadIdx.x & 31;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < words; base += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t w = base + threadIdx.x;
+    uint4 q = make_uint4(0u, 0u, 0u, 0u);
+    if (w < words) q = D[w];
+    const bool nz = any4(q);
+    const unsigned bal = __ballot_sync(kFull, nz);
+    if (!bal) continue;
+    unsigned long long first = 0;
+    if (lane == 0) first = atomicAdd(count, (unsigned long long)__popc(bal));
+    first = __shfl_sync(kFull, first, 0);
+    if (nz) {
+      const uint64_t slot = first + __popc(bal & lanemask_lt());
+      if (slot < cap) {
+        out[3 * slot] = (long long)(row0_word + w);
+        out[3 * slot + 1] = (long long)(((uint64_t)q.y << 32) | q.x);
+        out[3 * slot + 2] = (long long)(((uint64_t)q.w << 32) | q.z);
+      }
+    }
+  }
+}
+
+// Scatter gathered triples into the (cleared) full Δ; entries with index -1
+// are padding, indexes past the matrix are skipped and flagged.
+__global__ void k_shard_unpack(const long long* __restrict__ in, uint64_t n, uint4* __restrict__ D, uint64_t words,
+                               uint32_t W, uint8_t* __restrict__ flags, uint32_t* status) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const long long idx = in[3 * i];
+    if (idx < 0) continue;
+    if ((uint64_t)idx >= words) {
+      atomicOr(status, ST_BOUNDS);
+      continue;
+    }
+    const uint64_t lo = (uint64_t)in[3 * i + 1], hi = (uint64_t)in[3 * i + 2];
+    D[idx] = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+    flags[(uint64_t)idx / W] = 1;
+  }
+}
+
+uint64_t tc_shard_pack(strata_ctx* ctx, strata_tc_shard* sh, const uint4* Dmine, int64_t* out, uint64_t cap) {
+  const uint64_t per = sh->per;
+  const uint64_t words = per * sh->w4;
+  DBuf<uint64_t> cnt(ctx, 1);
+  SK_CUDA(cudaMemsetAsync(cnt.p, 0, 8, ctx->stream));
+  if (cap) SK_CUDA(cudaMemsetAsync(out, 0xff, cap * 24, ctx->stream));  // padding: index -1
+  if (words) {
+    const unsigned g = (unsigned)std::min<uint64_t>(ceil_div(words, 256), (uint64_t)ctx->num_sms * 8);
+    k_shard_pack<<<g, 256, 0, ctx->stream>>>(Dmine, words, (uint64_t)sh->rank * per * sh->w4, cap,
+                                             reinterpret_cast<long long*>(out),
+                                             reinterpret_cast<unsigned long long*>(cnt.p));
+    after_launch(ctx, "k_shard_pack");
+  }
+  uint64_t c;
+  read_u64(ctx, cnt.p, &c, 1);
+  sync_and_check(ctx);
+  return c;
+}
+
+void tc_shard_unpack(strata_ctx* ctx, strata_tc_shard* sh, const int64_t* in, uint64_t n, uint4* Dfull,
+                     uint8_t* ffull) {
+  const uint64_t rows = (uint64_t)sh->per * sh->world, words = rows * sh->w4;
+  SK_CUDA(cudaMemsetAsync(Dfull, 0, words * 16, ctx->stream));
+  SK_CUDA(cudaMemsetAsync(ffull, 0, rows, ctx->stream));
+  if (n) {
+    const unsigned g = (unsigned)std::min<uint64_t>(ceil_div(n, 256), (uint64_t)ctx->num_sms * 8);
+    k_shard_unpack<<<g, 256, 0, ctx->stream>>>(reinterpret_cast<const long long*>(in), n, Dfull, words, sh->w4,
+                                               ffull, ctx->d_status);
+    after_launch(ctx, "k_shard_unpack");
+  }
+  sync_and_check(ctx);
+}
+
 template uint64_t tc_bool_bitset<uint32_t>(strata_ctx*, const uint32_t*, const uint32_t*, uint64_t, uint64_t,
                                            uint64_t, int, DBuf<uint32_t>&, uint64_t*, uint64_t*);
 template uint64_t tc_bool_bitset<uint64_t>(strata_ctx*, const uint32_t*, const uint32_t*, uint64_t, uint64_t,

@@ -565,6 +565,32 @@ strata_status strata_tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const 
   SK_GUARD_END(ctx)
 }
 
+strata_status strata_tc_shard_pack(strata_ctx* ctx, strata_tc_shard* sh, const void* d_delta_mine,
+                                   int64_t* d_out, uint64_t cap, uint64_t* n_words) {
+  if (!ctx || !sh || sh->ctx != ctx || !d_delta_mine || !n_words || (cap && !d_out)) return STRATA_E_INVALID;
+  if (reinterpret_cast<uintptr_t>(d_delta_mine) % 16) return bad(ctx, "Delta buffers must be 16-byte aligned");
+  if (!sh->seeded) return bad(ctx, "pack before seed: call strata_tc_shard_seed first");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  *n_words = sk::tc_shard_pack(ctx, sh, static_cast<const uint4*>(d_delta_mine), d_out, cap);
+  SK_GUARD_END(ctx)
+}
+
+strata_status strata_tc_shard_unpack(strata_ctx* ctx, strata_tc_shard* sh, const int64_t* d_in, uint64_t n,
+                                     void* d_delta_full, uint8_t* d_flags_full) {
+  if (!ctx || !sh || sh->ctx != ctx || !d_delta_full || !d_flags_full || (n && !d_in)) return STRATA_E_INVALID;
+  if (reinterpret_cast<uintptr_t>(d_delta_full) % 16) return bad(ctx, "Delta buffers must be 16-byte aligned");
+  const uint64_t full_bytes = (uint64_t)sh->world * sh->per * sh->w4 * 16;
+  const auto f0 = reinterpret_cast<uintptr_t>(d_delta_full), i0 = reinterpret_cast<uintptr_t>(d_in);
+  if (n && i0 < f0 + full_bytes && f0 < i0 + n * 24) return bad(ctx, "the packed words overlap the gathered Delta");
+  if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
+  SK_GUARD_BEGIN
+  sk::reset_status(ctx);
+  sk::tc_shard_unpack(ctx, sh, d_in, n, static_cast<uint4*>(d_delta_full), d_flags_full);
+  SK_GUARD_END(ctx)
+}
+
 strata_status strata_tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count, uint64_t* fingerprint) {
   if (!ctx || !sh || sh->ctx != ctx) return STRATA_E_INVALID;
   if (!sh->seeded) return bad(ctx, "summary before seed: call strata_tc_shard_seed first");

@@ -19,7 +19,10 @@
 // query pairs yields the same proof sets for the queried tuples.  Targets
 // are processed in memory-bounded waves; a target none of whose tuples
 // changed in a round is final (both state buffers then hold it) and is
-// skipped from then on.
+// skipped from then on.  Within a live target, a tuple that did not change
+// in the previous round and none of whose inputs did is skipped for the
+// round: under the Jacobi schedule its derivation would repeat the previous
+// one exactly, and the buffer being written already holds its set.
 //
 // Mapping: a half-warp (16 lanes, its own shuffle group) owns one tuple
 // (target, X).  Lanes 0..7 hold the current proof set S, lanes 8..15 the

@@ -117,6 +117,9 @@ uint64_t tc_shard_seed(strata_ctx* ctx, strata_tc_shard* sh, uint4* Dmine, uint8
 uint64_t tc_shard_round(strata_ctx* ctx, strata_tc_shard* sh, const uint4* Dfull, const uint8_t* ffull, uint4* Dmine,
                         uint8_t* fmine);
 void tc_shard_summary(strata_ctx* ctx, strata_tc_shard* sh, uint64_t* count, uint64_t* fp);
+uint64_t tc_shard_pack(strata_ctx* ctx, strata_tc_shard* sh, const uint4* Dmine, int64_t* out, uint64_t cap);
+void tc_shard_unpack(strata_ctx* ctx, strata_tc_shard* sh, const int64_t* in, uint64_t n, uint4* Dfull,
+                     uint8_t* ffull);
 
 void rel_to_host(strata_ctx* ctx, const strata_rel* rel, uint32_t* src, uint32_t* dst, int64_t* w,
                  uint8_t* inf);

@@ -120,6 +120,8 @@ SIGNATURES = {
     "strata_tc_shard_seed": (C.c_int, [ctxp, vp, vp, vp, u64p]),
     "strata_tc_shard_round": (C.c_int, [ctxp, vp, vp, vp, vp, vp, u64p]),
     "strata_tc_shard_summary": (C.c_int, [ctxp, vp, u64p, u64p]),
+    "strata_tc_shard_pack": (C.c_int, [ctxp, vp, vp, vp, C.c_uint64, u64p]),
+    "strata_tc_shard_unpack": (C.c_int, [ctxp, vp, vp, C.c_uint64, vp, vp]),
     "strata_tc_shard_free": (None, [vp]),
     "strata_prov_tc_capture": (C.c_int, [ctxp, C.c_uint32, vp, vp, C.c_uint64, vp, C.c_uint32, C.c_uint32, u32p,
                                          u32p, C.POINTER(vp), u32p, C.POINTER(ProvStats)]),

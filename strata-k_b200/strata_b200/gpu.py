@@ -754,6 +754,32 @@ class TcShard:
         self.eng._check(self.eng.lib.strata_tc_shard_summary(self.eng.ctx, self.h, C.byref(c), C.byref(f)))
         return int(c.value), int(f.value)
 
+    def pack_count(self, mine) -> int:
+        """Nonzero 128-bit words of this rank's Δ' slice."""
+        n = C.c_uint64()
+        _torch_sync(mine)
+        self.eng._check(self.eng.lib.strata_tc_shard_pack(self.eng.ctx, self.h, _dp(mine), None, 0, C.byref(n)))
+        return int(n.value)
+
+    def pack(self, mine, cap: int):
+        """(cap, 3) int64 device tensor of (global word index, low, high)
+        triples of the slice's nonzero words, padded with index -1."""
+        import torch
+        out = torch.empty((max(cap, 1), 3), dtype=torch.int64, device=mine.device)
+        n = C.c_uint64()
+        _torch_sync(mine)
+        self.eng._check(self.eng.lib.strata_tc_shard_pack(self.eng.ctx, self.h, _dp(mine), _dp(out), cap,
+                                                          C.byref(n)))
+        if int(n.value) > cap:
+            raise InvalidArgument(f"{int(n.value)} nonzero words exceed the capacity {cap}")
+        return out[:cap]
+
+    def unpack(self, triples, full, ffull):
+        """Rebuild the gathered Δ and its row flags from all ranks' triples."""
+        _torch_sync(triples)
+        self.eng._check(self.eng.lib.strata_tc_shard_unpack(self.eng.ctx, self.h, _dp(triples), triples.shape[0],
+                                                            _dp(full), _dp(ffull)))
+
     def free(self):
         if self.h:
             self.eng.lib.strata_tc_shard_free(self.h)

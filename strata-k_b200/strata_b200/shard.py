@@ -95,35 +95,75 @@ def allreduce_sum_mod64(dist, value: int, device="cpu") -> int:
     return int(t.item()) & 0xFFFFFFFFFFFFFFFF
 
 
-def tc_bool_sharded(shards, dist=None, device=None) -> tuple[int, int, int]:
+def tc_bool_sharded(shards, dist=None, device=None, exchange: str = "auto") -> tuple[int, int, int]:
     """Semi-naive Bool closure with path rows split across ranks.
 
     `shards` are this process's rank shares (``TcShard`` objects, or any
-    object with ``world``, ``shape()``, ``seed``, ``round`` and ``summary``):
-    one under torch.distributed (`dist` given), whose Δ' slice and row flags
-    meet the other ranks' through an all-gather into the full Δ every round
-    (NCCL over NVLink on GPUs) and whose |Δ'| is summed by an all-reduce; or
-    all `world` shares in rank order with `dist` None, the slices then simply
-    concatenated (one process standing in for the ranks).  Every rank takes
-    the same collective steps in the same order until the summed |Δ'| is 0.
+    object with ``world``, ``shape()``, ``seed``, ``round``, ``summary``,
+    ``pack_count``, ``pack`` and ``unpack``): one under torch.distributed
+    (`dist` given), whose Δ' meets the other ranks' through an all-gather into
+    the full Δ every round (NCCL over NVLink on GPUs); or all `world` shares in
+    rank order with `dist` None, the parts then simply concatenated (one
+    process standing in for the ranks).
+
+    Each round the ranks first gather every rank's (|Δ'|, nonzero Δ' words),
+    one small all-gather.  Then, with `exchange` "auto", a round whose largest
+    rank has few nonzero words exchanges only those words — 24 bytes each,
+    (word index, 128 bits) — and every rank rebuilds the full Δ from them
+    (``pack`` / ``unpack``); a dense round all-gathers the whole Δ' slices and
+    row flags.  "dense" and "sparse" force one form.  Every rank takes the
+    same collective steps in the same order until the summed |Δ'| is 0.
     Returns (|path|, fingerprint Σ mix64(X)·c^Z mod 2^64, rounds)."""
     import torch
+    if exchange not in ("auto", "dense", "sparse"):
+        raise ValueError("exchange must be auto, dense or sparse")
     per, _, _, row_bytes = shards[0].shape()
     world = shards[0].world
     words = per * row_bytes // 4
+    slice_bytes = per * row_bytes + per
     full = [torch.zeros(world * words, dtype=torch.int32, device=device) for _ in range(2)]
     ffull = [torch.zeros(world * per, dtype=torch.uint8, device=device) for _ in range(2)]
     mine = [torch.zeros(words, dtype=torch.int32, device=device) for _ in shards]
     fmine = [torch.zeros(per, dtype=torch.uint8, device=device) for _ in shards]
+    stats = {"dense_rounds": 0, "sparse_rounds": 0, "bytes_per_rank": 0}
+
+    def sparse_wins(m_max: int) -> bool:
+        if exchange != "auto":
+            return exchange == "sparse"
+        return 24 * m_max * 2 <= slice_bytes
 
     def meet(k: int, counts: list[int]) -> int:
+        nnz = [s.pack_count(mine[i]) for i, s in enumerate(shards)]
         if dist is None:
-            torch.cat(mine, out=full[k])
-            torch.cat(fmine, out=ffull[k])
-            return sum(counts)
-        dist.all_gather_into_tensor(full[k], mine[0])
-        dist.all_gather_into_tensor(ffull[k], fmine[0])
-        return allreduce_sum_u64(dist, counts[0], device=device or "cpu")
+            total, m_max = sum(counts), max(nnz)
+        else:
+            info = torch.tensor([counts[0], nnz[0]], dtype=torch.int64, device=device)
+            every = torch.empty(2 * world, dtype=torch.int64, device=device)
+            dist.all_gather_into_tensor(every, info)
+            every = every.cpu()
+            total, m_max = int(every[0::2].sum()), int(every[1::2].max())
+        if m_max == 0:  # no rank has a Δ' word: nothing to exchange
+            shards[0].unpack(torch.zeros((0, 3), dtype=torch.int64, device=device), full[k], ffull[k])
+        elif sparse_wins(m_max):
+            stats["sparse_rounds"] += 1
+            stats["bytes_per_rank"] += 24 * m_max
+            packs = [s.pack(mine[i], m_max) for i, s in enumerate(shards)]
+            if dist is None:
+                triples = torch.cat(packs)
+            else:
+                triples = torch.empty((world * m_max, 3), dtype=torch.int64, device=device)
+                dist.all_gather_into_tensor(triples, packs[0].contiguous())
+            shards[0].unpack(triples, full[k], ffull[k])
+        else:
+            stats["dense_rounds"] += 1
+            stats["bytes_per_rank"] += slice_bytes
+            if dist is None:
+                torch.cat(mine, out=full[k])
+                torch.cat(fmine, out=ffull[k])
+            else:
+                dist.all_gather_into_tensor(full[k], mine[0])
+                dist.all_gather_into_tensor(ffull[k], fmine[0])
+        return total
 
     total = meet(0, [s.seed(mine[i], fmine[i]) for i, s in enumerate(shards)])
     cur, rounds = 0, 0
@@ -132,6 +172,7 @@ def tc_bool_sharded(shards, dist=None, device=None) -> tuple[int, int, int]:
         counts = [s.round(full[cur], ffull[cur], mine[i], fmine[i]) for i, s in enumerate(shards)]
         cur ^= 1
         total = meet(cur, counts)
+    tc_bool_sharded.last_stats = stats
     parts = [s.summary() for s in shards]
     count = sum(c for c, _ in parts)
     fp = sum(f for _, f in parts) & 0xFFFFFFFFFFFFFFFF

@@ -133,11 +133,13 @@ def test_sharded_closure_ranks_on_one_gpu(engine, world):
     """The sharded closure's device rounds, with every rank's share run in
     this process (no rank waits on another; the Δ' slices are concatenated
     where ranks would all-gather them): count, fingerprint and rounds equal
-    the oracle's and the single-device batch's."""
+    the oracle's and the single-device batch's, whether Δ' moves as whole
+    slices, as packed nonzero words, or as the smaller of the two."""
     import torch
 
     from strata_b200 import shard
-    for n, m, seed in ((3000, 9000, 41), (777, 2500, 42), (129, 400, 43)):
+    for (n, m, seed), x in zip(((3000, 9000, 41), (777, 2500, 42), (129, 400, 43), (2000, 2600, 44)),
+                               ("auto", "sparse", "dense", "auto")):
         s, d = gen.er_directed(n, m, seed)
         s, d = np.concatenate([s, s[:10]]), np.concatenate([d, d[:10]])  # duplicate edges
         c, f = O.closure_batch([n], [0, len(s)], s, d, threads=8)
@@ -146,7 +148,7 @@ def test_sharded_closure_ranks_on_one_gpu(engine, world):
         td = torch.from_numpy(d.astype(np.int32)).cuda()
         parts = [engine.tc_shard(n, ts, td, r, world) for r in range(world)]
         try:
-            got = shard.tc_bool_sharded(parts, device="cuda")
+            got = shard.tc_bool_sharded(parts, device="cuda", exchange=x)
         finally:
             for p in parts:
                 p.free()
@@ -174,7 +176,16 @@ def test_sharded_closure_rejects_bad_input(engine):
             sh.round(full, flags, mine, fmine)
         with pytest.raises(S.InvalidArgument):  # a summary before the seed
             sh.summary()
+        with pytest.raises(S.InvalidArgument):  # a pack before the seed
+            sh.pack_count(mine)
         sh.seed(mine, fmine)
+        assert sh.pack_count(mine) >= 1  # row 0 holds its edge to 1
+        with pytest.raises(S.InvalidArgument):  # more nonzero words than the capacity
+            sh.pack(mine, 0)
+        trip = sh.pack(mine, sh.pack_count(mine) + 2)
+        assert int((trip[:, 0] < 0).sum()) == 2  # padding
+        with pytest.raises(S.InvalidArgument):  # triples inside the gathered Δ
+            sh.unpack(full.view(torch.int64)[: 3 * 2].view(2, 3), full, flags)
         with pytest.raises(S.InvalidArgument):  # a second seed (its edge columns are gone)
             sh.seed(mine, fmine)
         with pytest.raises(S.InvalidArgument):  # the slice inside the gathered Δ

@@ -73,6 +73,42 @@ class NumpyTcShard:
         x, z = np.nonzero(self.F)
         return int(len(x)), O.poly_fingerprint(x + self.lo, z, self.n)
 
+    def _words(self, mine):
+        return mine.numpy().view(np.uint32).reshape(-1, 4)
+
+    def pack_count(self, mine):
+        return int(self._words(mine).any(axis=1).sum())
+
+    def pack(self, mine, cap):
+        """(word index, low 64, high 64) of the nonzero 128-bit words, as the
+        device pack writes them, padded with index -1."""
+        import torch
+        w = self._words(mine).astype(np.uint64)
+        nz = np.nonzero(w.any(axis=1))[0]
+        out = np.full((cap, 3), -1, np.int64)
+        out[: len(nz), 0] = nz + self.rank * self.per * self.w4
+        out[: len(nz), 1] = (w[nz, 0] | (w[nz, 1] << np.uint64(32))).view(np.int64)
+        out[: len(nz), 2] = (w[nz, 2] | (w[nz, 3] << np.uint64(32))).view(np.int64)
+        return torch.from_numpy(out)
+
+    def unpack(self, triples, full, ffull):
+        t = triples.numpy()
+        t = t[t[:, 0] >= 0]
+        w = np.zeros((full.numel() // 4, 4), np.uint32)
+        lo, hi = t[:, 1].view(np.uint64), t[:, 2].view(np.uint64)
+        idx = t[:, 0]
+        w[idx, 0], w[idx, 1] = lo & np.uint64(0xFFFFFFFF), lo >> np.uint64(32)
+        w[idx, 2], w[idx, 3] = hi & np.uint64(0xFFFFFFFF), hi >> np.uint64(32)
+        full.copy_(torch_from(w.reshape(-1).view(np.int32)))
+        f = np.zeros(ffull.numel(), np.uint8)
+        f[idx // self.w4] = 1
+        ffull.copy_(torch_from(f))
+
+
+def torch_from(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a))
+
 
 def _closure_graph(seed):
     rng = np.random.default_rng(seed)
@@ -136,12 +172,15 @@ def _worker(rank: int, world: int, port: int, out_dir: str):
         total = shard.allreduce_sum_u64(dist, mine)
         if rank == 0:
             res["tri"] = total == O.count_pattern(tw.src, tw.dst)
-        # Bool closure: path rows per rank, Δ' all-gathered every round
+        # Bool closure: path rows per rank, Δ' exchanged every round (dense
+        # slices, sparse nonzero words, or whichever is smaller)
         n, cs, cd = _closure_graph(17)
-        got = shard.tc_bool_sharded([NumpyTcShard(n, cs, cd, rank, world)], dist)
+        got = {x: shard.tc_bool_sharded([NumpyTcShard(n, cs, cd, rank, world)], dist, exchange=x)
+               for x in ("auto", "dense", "sparse")}
         if rank == 0:
             c, f = O.closure_batch([n], [0, len(cs)], cs, cd, threads=2)
-            res["tc"] = got == (int(c[0]), int(f[0]), O.fast_tc(cs, cd)[2])
+            want = (int(c[0]), int(f[0]), O.fast_tc(cs, cd)[2])
+            res["tc"] = all(g == want for g in got.values())
     finally:
         dist.destroy_process_group()
     if rank == 0:
@@ -167,11 +206,18 @@ def test_sharded_closure_emulated_ranks():
     n, cs, cd = _closure_graph(18)
     c, f = O.closure_batch([n], [0, len(cs)], cs, cd, threads=2)
     want = (int(c[0]), int(f[0]), O.fast_tc(cs, cd)[2])
+    forms = set()
     for world in (1, 3, 7):
-        got = shard.tc_bool_sharded([NumpyTcShard(n, cs, cd, r, world) for r in range(world)])
-        assert got == want, world
-    tiny = shard.tc_bool_sharded([NumpyTcShard(2, [0], [1], r, 4) for r in range(4)])
-    assert tiny == (1, O.poly_fingerprint([0], [1], 2), 1)
+        for x in ("auto", "dense", "sparse"):
+            got = shard.tc_bool_sharded([NumpyTcShard(n, cs, cd, r, world) for r in range(world)], exchange=x)
+            assert got == want, (world, x)
+            st = shard.tc_bool_sharded.last_stats
+            if x == "auto":
+                forms |= {k for k in ("dense_rounds", "sparse_rounds") if st[k]}
+    assert forms == {"dense_rounds", "sparse_rounds"}  # auto used both forms
+    for x in ("auto", "dense", "sparse"):
+        tiny = shard.tc_bool_sharded([NumpyTcShard(2, [0], [1], r, 4) for r in range(4)], exchange=x)
+        assert tiny == (1, O.poly_fingerprint([0], [1], 2), 1)
 
 
 def test_partitions_cover_every_unit_once():
