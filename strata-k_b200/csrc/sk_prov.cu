@@ -215,12 +215,15 @@ __global__ void __launch_bounds__(PV_NT) k_prov_round(PvView v) {
       }
       __syncwarp(hmask);
       // ---- subset matrix: bit y of subof = proof(y) ⊆ proof(me); eqof = equal
+      // (only the valid lanes are visited: the set bits of the half-warp's
+      // ballot, the same on all its lanes)
       uint32_t subof = 0, eqof = 0;
-      for (int yl = 0; yl < 16; yl++) {
-        const bool vy = __shfl_sync(hmask, valid, yl, 16);
+      const uint32_t vmask = (__ballot_sync(hmask, valid) >> hbase) & 0xffffu;
+      for (uint32_t vm = vmask; vm; vm &= vm - 1) {
+        const int yl = __ffs(vm) - 1;
         const uint32_t ly = __shfl_sync(hmask, len, yl, 16);
         const uint64_t sy = __shfl_sync(hmask, sig, yl, 16);
-        if (valid && vy && yl != hl && ly <= len && (sy & ~sig) == 0 &&
+        if (valid && yl != hl && ly <= len && (sy & ~sig) == 0 &&
             sub_list(s_lists[hw][bank][yl], ly, Lc, len)) {
           subof |= 1u << yl;
           if (ly == len) eqof |= 1u << yl;
@@ -246,10 +249,11 @@ __global__ void __launch_bounds__(PV_NT) k_prov_round(PvView v) {
       if (acc && ns > v.k) {
         // prune_top_k: rank by (weight desc, literals asc)
         uint32_t rank = 0;
-        for (int yl = 0; yl < 16; yl++) {
+        for (uint32_t vm = sv; vm; vm &= vm - 1) {
+          const int yl = __ffs(vm) - 1;
           const double wy = __shfl_sync(hmask, w, yl, 16);
           const uint32_t ly = __shfl_sync(hmask, len, yl, 16);
-          if (!surv || yl == hl || !(sv >> yl & 1u)) continue;
+          if (!surv || yl == hl) continue;
           if (wy > w || (wy == w && lex_less(s_lists[hw][bank][yl], ly, Lc, len))) rank++;
         }
         keep = (__ballot_sync(hmask, surv && rank < v.k) >> hbase) & 0xffffu;
