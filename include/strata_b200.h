@@ -454,7 +454,7 @@ void strata_rel_free(strata_ctx* ctx, strata_rel* rel);
  * The interpreter's operators (strata-eval/src/seminaive.rs:114-298,
  * store.rs:34-48) on packed sorted key columns.  A packed key is
  * (c0 << shift) | c1 in a u32 (key_bytes = 4) or u64 (key_bytes = 8).
- * `n` is limited to 2^30 - 1 per call. */
+ * `n` is limited to 2^30 - 1 per call, except for strata_op_sort (2^32 - 1). */
 
 /* Stable LSD radix sort of keys (and optional 4- or 8-byte values) on the low
  * `key_bits` bits.  Sorted output goes to keys_out / vals_out; the inputs are

@@ -865,7 +865,7 @@ strata_status strata_op_sort(strata_ctx* ctx, int key_bytes, int val_bytes, cons
   if (n && (!d_keys_in || !d_keys_out || (val_bytes && (!d_vals_in || !d_vals_out))))
     return bad(ctx, "NULL argument");
   if (key_bits < 0 || key_bits > 8 * key_bytes) return bad(ctx, "key_bits out of range");
-  if (n > sk::kMaxSortN) return bad(ctx, "n exceeds 2^30-1");
+  if (n > sk::kMaxSortKeys) return bad(ctx, "n exceeds 2^32-1");
   if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
   SK_GUARD_BEGIN
   sk::reset_status(ctx);

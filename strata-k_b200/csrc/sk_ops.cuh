@@ -10,6 +10,8 @@ namespace sk {
 
 // Radix sort limit per call (the onesweep look-back words carry 30-bit counts).
 constexpr uint64_t kMaxSortN = (1ull << 30) - 1;
+// strata_op_sort and the radix sort itself (64-bit look-back words past kMaxSortN)
+constexpr uint64_t kMaxSortKeys = (1ull << 32) - 1;
 
 // Stable LSD radix sort (onesweep) of `n` keys on their low `bits` bits, with
 // optional values (V = uint32_t or uint64_t; has_vals selects them).  keys/alt

@@ -8,7 +8,9 @@
 //     match-any aggregation);
 //   * each 8-bit pass is ONE kernel: a tile of NT*ITEMS keys (and its
 //     values) arrives in shared memory by one bulk asynchronous copy each,
-//     is ranked with warp-level multisplit (8 ballots per item), the tile's
+//     is ranked with a warp-level multisplit (by default each lane ORs its
+//     bit into its digit's shared-memory peer mask; 8 ballots per item and
+//     the match instruction are knob choices), the tile's
 //     per-digit counts are published for a decoupled look-back, keys are
 //     staged in shared memory in digit order with their source slot and
 //     written out in runs (coalesced per digit), values fetched through the
@@ -27,9 +29,16 @@ namespace {
 constexpr int RADIX = 256;
 constexpr int NT = 256;  // threads per block == RADIX (one digit per thread)
 constexpr int NW = NT / 32;
-constexpr uint32_t kLb32A = 1u << 30;
-constexpr uint32_t kLb32P = 2u << 30;
-constexpr uint32_t kLb32Mask = (1u << 30) - 1;
+// Look-back words: a 2-bit state (A = tile count ready, P = inclusive prefix
+// ready) above the count.  32-bit words carry counts below 2^30 (sorts of at
+// most 2^30 - 1 keys); 64-bit words take the larger sorts.
+template <class LB> struct LbTag { using type = LB; };
+template <class LB> struct LbBits {
+  static constexpr int S = 8 * sizeof(LB) - 2;
+  static constexpr LB A = LB(1) << S;
+  static constexpr LB P = LB(2) << S;
+  static constexpr LB M = (LB(1) << S) - 1;
+};
 
 template <class K> struct RCfg;
 template <> struct RCfg<uint32_t> { static constexpr int ITEMS = 15; };
@@ -159,12 +168,12 @@ constexpr size_t onesweep_smem() {
 //  4. keys are staged in digit order (with their source slot when values
 //     ride along) and written out in runs, each value fetched from shared
 //     memory through its source slot.
-template <class K, class V, bool HAS_V, int ITEMS, int RANK>
+template <class K, class V, bool HAS_V, int ITEMS, int RANK, class LB = uint32_t>
 __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
                                                  const V* __restrict__ vin, V* __restrict__ vout,
                                                  uint32_t n, int shift, int dbits,
                                                  const uint32_t* __restrict__ binoff,
-                                                 uint32_t* lookback, uint32_t* tile_counter,
+                                                 LB* lookback, uint32_t* tile_counter,
                                                  uint32_t* status, int bulk_ok) {
   constexpr int rank_mode = RANK;  // 0 ballots, 1 match instruction, 2 shared masks
   constexpr uint32_t TILE = NT * ITEMS;
@@ -172,7 +181,7 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_whist[NW][RADIX];
   __shared__ uint32_t s_dstart[RADIX];
-  __shared__ uint32_t s_gbase[RADIX];
+  __shared__ uint32_t s_goff[RADIX];
   __shared__ uint32_t s_scan[NW + 1];
   __shared__ __align__(8) uint64_t s_bar[2];
   extern __shared__ __align__(16) unsigned char s_raw[];
@@ -281,27 +290,29 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
     s_whist[w][tid] = cnt;
     cnt += c;
   }
-  uint32_t* lb = lookback + (size_t)tile * RADIX;
-  st_volatile(&lb[tid], (tile == 0 ? kLb32P : kLb32A) | cnt);
+  using LBB = LbBits<LB>;
+  LB* lb = lookback + (size_t)tile * RADIX;
+  st_volatile(&lb[tid], (tile == 0 ? LBB::P : LBB::A) | (LB)cnt);
   uint32_t tot;
   s_dstart[tid] = block_excl_sum<NT>(cnt, s_scan, &tot);
 
-  uint32_t excl = 0;
+  LB excl = 0;  // keys of this digit in earlier tiles: below n < 2^32
   if (tile > 0) {
     bool timed_out = false;
     for (int64_t t = (int64_t)tile - 1; t >= 0; t--) {
-      uint32_t v, it = 0;
+      LB v;
+      uint32_t it = 0;
       do {
         v = ld_volatile(&lookback[(size_t)t * RADIX + tid]);
-      } while ((v >> 30) == 0 && ++it < kSpinLimit);
-      if ((v >> 30) == 0) { timed_out = true; break; }
-      excl += v & kLb32Mask;
-      if ((v >> 30) == 2) break;
+      } while ((v >> LBB::S) == 0 && ++it < kSpinLimit);
+      if ((v >> LBB::S) == 0) { timed_out = true; break; }
+      excl += v & LBB::M;
+      if ((v >> LBB::S) == 2) break;
     }
     if (timed_out) atomicOr(status, ST_LOOKBACK_TIMEOUT);
-    st_volatile(&lb[tid], kLb32P | (excl + cnt));
+    st_volatile(&lb[tid], LBB::P | (excl + (LB)cnt));
   }
-  s_gbase[tid] = binoff[tid] + excl;
+  s_goff[tid] = binoff[tid] + (uint32_t)excl - s_dstart[tid];
   __syncthreads();  // s_dstart, s_gbase, warp offsets visible
 
   // Stage keys in digit order (and where each came from).
@@ -325,7 +336,7 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
     if (i < tile_n) {
       const K k = s_keys[i];
       const uint32_t d = (uint32_t)(k >> shift) & dmask;
-      const uint32_t dst = s_gbase[d] + (i - s_dstart[d]);
+      const uint32_t dst = s_goff[d] + i;
       if (dst < n) {
         kout[dst] = k;
         if constexpr (HAS_V) vout[dst] = s_vin[s_src[i]];
@@ -373,34 +384,43 @@ void radix_sort_impl(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, boo
   }
 
   const uint32_t ntiles = (uint32_t)ceil_div(n, TILE);
-  DBuf<uint32_t> lookback(ctx, (uint64_t)ntiles * RADIX);
+  // 64-bit look-back words once a digit's count can reach 2^30
+  const bool wide_lb = n > kMaxSortN;
+  const uint64_t lb_words = (uint64_t)ntiles * RADIX;
+  const size_t lb_bytes = lb_words * (wide_lb ? 8 : 4);
+  DBuf<uint64_t> lookback(ctx, (lb_bytes + 7) / 8);
   const size_t smem = has_vals ? onesweep_smem<K, V, true, ITEMS>() : onesweep_smem<K, V, false, ITEMS>();
   for (int p = 0; p < passes; p++) {
     if (trivial[p]) continue;
-    SK_CUDA(cudaMemsetAsync(lookback.p, 0, sizeof(uint32_t) * ntiles * RADIX, ctx->stream));
+    SK_CUDA(cudaMemsetAsync(lookback.p, 0, lb_bytes, ctx->stream));
     const int dbits = std::min(8, bits - 8 * p);
     const int kh = kprof_begin(ctx, K_ONESWEEP);
-    auto go = [&](auto rank_tag) {
+    auto go = [&](auto rank_tag, auto lb_tag) {
       constexpr int RK = decltype(rank_tag)::value;
+      using LB = typename decltype(lb_tag)::type;
+      LB* lbp = reinterpret_cast<LB*>(lookback.p);
       if (has_vals) {
-        auto kern = k_onesweep<K, V, true, ITEMS, RK>;
+        auto kern = k_onesweep<K, V, true, ITEMS, RK, LB>;
         SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, *vals, *valt, (uint32_t)n, 8 * p, dbits,
-                                                binoff.p + p * RADIX, lookback.p, counters + p, ctx->d_status,
+                                                binoff.p + p * RADIX, lbp, counters + p, ctx->d_status,
                                                 aligned16(*keys) && aligned16(*vals) ? 1 : 0);
       } else {
-        auto kern = k_onesweep<K, V, false, ITEMS, RK>;
+        auto kern = k_onesweep<K, V, false, ITEMS, RK, LB>;
         SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<ntiles, NT, smem, ctx->stream>>>(*keys, *alt, nullptr, nullptr, (uint32_t)n, 8 * p, dbits,
-                                                binoff.p + p * RADIX, lookback.p, counters + p, ctx->d_status,
+                                                binoff.p + p * RADIX, lbp, counters + p, ctx->d_status,
                                                 aligned16(*keys) ? 1 : 0);
       }
     };
-    switch (ctx->tune_sort_rank) {
-      case 0: go(std::integral_constant<int, 0>{}); break;
-      case 1: go(std::integral_constant<int, 1>{}); break;
-      default: go(std::integral_constant<int, 2>{}); break;
-    }
+    if (wide_lb)  // the large sorts take the default ranking
+      go(std::integral_constant<int, 2>{}, LbTag<uint64_t>{});
+    else
+      switch (ctx->tune_sort_rank) {
+        case 0: go(std::integral_constant<int, 0>{}, LbTag<uint32_t>{}); break;
+        case 1: go(std::integral_constant<int, 1>{}, LbTag<uint32_t>{}); break;
+        default: go(std::integral_constant<int, 2>{}, LbTag<uint32_t>{}); break;
+      }
     kprof_end(ctx, kh, 2 * n * (sizeof(K) + (has_vals ? sizeof(V) : 0)));
     after_launch(ctx, "k_onesweep");
     std::swap(*keys, *alt);
@@ -425,7 +445,7 @@ template <class K, class V>
 void radix_sort(strata_ctx* ctx, K** keys, K** alt, V** vals, V** valt, bool has_vals,
                 uint64_t n, int bits, bool skip_trivial) {
   if (n <= 1 || bits <= 0) return;
-  if (n > kMaxSortN) fail(STRATA_E_UNSUPPORTED, "radix sort call limited to 2^30-1 keys");
+  if (n > kMaxSortKeys) fail(STRATA_E_UNSUPPORTED, "radix sort call limited to 2^32-1 keys");
   if (bits > (int)(8 * sizeof(K))) bits = 8 * sizeof(K);
   if constexpr (sizeof(K) == 4) {
     switch (ctx->tune_items4) {

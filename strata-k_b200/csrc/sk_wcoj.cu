@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(TC_NT)
 // together, so the searches run without idle lanes.  Exact: the bitmap has no
 // false negatives and every queued candidate is searched once.
 constexpr uint32_t TF_WORDS = 256;  // 8,192-bit filter per warp
-constexpr uint32_t TF_MIN = 16;     // out-degree from which the filter pays for its setup
+constexpr uint32_t TF_MIN = 8;      // out-degree from which the filter pays for its setup
 
 __device__ __forceinline__ uint32_t tf_hash(uint32_t z, int lg) { return (z * 0x85EBCA77u) >> (32 - lg); }
 

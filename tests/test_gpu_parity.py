@@ -490,6 +490,36 @@ def test_op_sort_stable(engine, n, kb, vb):
         assert np.array_equal(vo.cpu().numpy().view(vals.dtype)[:n], vals[order])
 
 
+def test_op_sort_beyond_2_30_keys(engine):
+    """A sort of 2^30 + 4,097 keys whose most frequent digit occurs more than
+    2^30 times (the look-back then needs its 64-bit words): keys and the
+    values riding along come out in stable order."""
+    import ctypes as C
+    import torch
+    n = (1 << 30) + 4097
+    tail = 100
+    keys = torch.zeros(n, dtype=torch.int32, device="cuda")
+    keys[n - tail:] = torch.arange(tail, dtype=torch.int32, device="cuda") % 4
+    vals = torch.arange(n, dtype=torch.int32, device="cuda")
+    ko, vo = torch.empty_like(keys), torch.empty_like(vals)
+    engine._check(engine.lib.strata_op_sort(engine.ctx, 4, 4, C.c_void_p(keys.data_ptr()), C.c_void_p(vals.data_ptr()),
+                                            C.c_void_p(ko.data_ptr()), C.c_void_p(vo.data_ptr()), n, 2))
+    j = torch.arange(tail, dtype=torch.int32, device="cuda")
+    want_v = torch.cat([torch.arange(n - tail, dtype=torch.int32, device="cuda")] +
+                       [(n - tail + j[j % 4 == d]).to(torch.int32) for d in range(4)])
+    want_k = torch.cat([torch.zeros(n - tail + 25, dtype=torch.int32, device="cuda")] +
+                       [torch.full((25,), d, dtype=torch.int32, device="cuda") for d in (1, 2, 3)])
+    assert int((want_k == 0).sum()) > (1 << 30)
+    assert torch.equal(ko, want_k)
+    assert torch.equal(vo, want_v)
+    del keys, vals, ko, vo, want_v, want_k
+    torch.cuda.empty_cache()
+    small = torch.zeros(16, dtype=torch.int32, device="cuda")
+    with pytest.raises(S.InvalidArgument):  # past 2^32 - 1 keys (refused before any key is read)
+        engine._check(engine.lib.strata_op_sort(engine.ctx, 4, 0, C.c_void_p(small.data_ptr()), None,
+                                                C.c_void_p(small.data_ptr()), None, 1 << 32, 32))
+
+
 def test_op_dedup_diff_and_min_improve(engine):
     import ctypes as C
     import torch
