@@ -279,36 +279,6 @@ struct RRCfg {
   static constexpr uint32_t TILE = NT * ITEMS;
 };
 
-// First run head at or after p (keys sorted); galloping then binary search.
-template <class K>
-__device__ uint64_t first_head_from(const K* keys, uint64_t n, uint64_t p) {
-  if (p == 0) return 0;
-  if (p >= n) return n;
-  const K prev = keys[p - 1];
-  if (keys[p] != prev) return p;
-  uint64_t step = 1, lo = p, hi;
-  while (true) {
-    hi = lo + step;
-    if (hi >= n) { hi = n; break; }
-    if (keys[hi] != prev) break;
-    lo = hi;
-    step <<= 1;
-  }
-  // keys[lo] == prev, keys[hi] != prev (or hi == n)
-  return upper_bound_dev(keys, lo, hi, prev);
-}
-
-// Run-head boundaries of every reduce tile at once (one thread per boundary):
-// bounds[t] = first run head at or after t * tile_len, bounds[tiles] = n.
-template <class K>
-__global__ void k_rr_bounds(const K* __restrict__ keys, uint64_t n, uint32_t tiles, uint32_t tile_len,
-                            uint64_t* __restrict__ bounds) {
-  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t > tiles) return;
-  const uint64_t p = t * tile_len;
-  bounds[t] = first_head_from(keys, n, p < n ? p : n);
-}
-
 template <class W>
 struct SegMin {  // segmented-min scan state: has a run start, min since it
   bool h;
@@ -322,140 +292,168 @@ __device__ __forceinline__ SegMin<W> seg_combine(SegMin<W> a, SegMin<W> b) {
   return r;
 }
 
+// Run reduction over fixed tiles, reduce-then-scan (no tile waits on
+// another, so a run of any length costs no more than its items):
+//   k_rr_heads   run heads per tile (key differs from its predecessor);
+//   scan         exclusive head counts = the output rank of each tile's first run;
+//   k_rr_span    (Trop) the output slot of every run crossing a tile boundary
+//                starts at the absent code;
+//   k_rr_write   each tile stages its heads' keys and the minima of the runs
+//                it holds whole, writes them coalesced at its rank, and merges
+//                the part of a boundary-crossing run it holds with atomicMin.
+__device__ __forceinline__ void atomic_min_w(int32_t* p, int32_t v) { atomicMin(p, v); }
+__device__ __forceinline__ void atomic_min_w(int64_t* p, int64_t v) {
+  atomicMin(reinterpret_cast<long long*>(p), (long long)v);
+}
+
+template <class K, int ITEMS>
+__global__ void __launch_bounds__(NT) k_rr_heads(const K* __restrict__ keys, uint64_t n,
+                                                 uint64_t* __restrict__ tile_heads) {
+  __shared__ uint32_t s_red[NT / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t t0 = (uint64_t)blockIdx.x * (NT * ITEMS);
+  uint32_t c = 0;
+#pragma unroll
+  for (int q = 0; q < ITEMS; q++) {
+    const uint64_t i = t0 + (uint64_t)q * NT + tid;
+    if (i < n) c += (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+  }
+  c = warp_sum(c);
+  if (lane == 0) s_red[warp] = c;
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t t = 0;
+#pragma unroll
+    for (int w = 0; w < NT / 32; w++) t += s_red[w];
+    tile_heads[blockIdx.x] = t;
+  }
+}
+
+template <class K, class W>
+__global__ void k_rr_span(const K* __restrict__ keys, uint64_t n, uint32_t tile_len, uint64_t tiles,
+                          const uint64_t* __restrict__ rank0, W* __restrict__ out_w) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1;  // boundary before tile t
+  if (t >= tiles) return;
+  const uint64_t p = t * tile_len;
+  if (p < n && keys[p] == keys[p - 1]) out_w[rank0[t] - 1] = WAbs<W>::v;
+}
+
 template <class K, class W, bool TROP>
 __global__ void __launch_bounds__(NT)
     k_reduce_runs(const K* __restrict__ keys, const W* __restrict__ w, uint64_t n, K* __restrict__ out,
-                  W* __restrict__ out_w, const uint64_t* __restrict__ bounds, uint64_t* states,
-                  uint32_t* counter, uint64_t* d_count, uint32_t* status) {
+                  W* __restrict__ out_w, const uint64_t* __restrict__ rank0, uint32_t* status) {
   constexpr int RR_ITEMS = RRCfg<K, W, TROP>::ITEMS;
   constexpr uint32_t RR_TILE = RRCfg<K, W, TROP>::TILE;
-  __shared__ uint32_t s_tile;
   __shared__ K s_k[RR_TILE];
   __shared__ W s_w[TROP ? RR_TILE : 1];
   __shared__ K s_ok[RR_TILE];
   __shared__ W s_ow[TROP ? RR_TILE : 1];
   __shared__ uint32_t s_scan[NT / 32 + 1];
   __shared__ SegMin<W> s_seg[NT / 32];
-  __shared__ uint64_t s_excl;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t tile = claim_tile(counter, &s_tile);
-  // this tile reduces the runs whose head lies in [tile*TILE, (tile+1)*TILE)
-  const uint64_t s = bounds[tile], e = bounds[tile + 1];
-  uint32_t nout = 0;       // rows staged so far (uniform)
-  W carry_m = W(0);        // min of the open run entering this chunk (Trop)
-  bool carry_h = false;
-  for (uint64_t c = s; c < e; c += RR_TILE) {
-    const uint32_t clen = (uint32_t)((e - c) < RR_TILE ? (e - c) : RR_TILE);
+  const uint64_t t0 = (uint64_t)blockIdx.x * RR_TILE;
+  const uint32_t len = (uint32_t)(n - t0 < RR_TILE ? n - t0 : RR_TILE);
+  const uint64_t base = rank0[blockIdx.x];  // output rank of this tile's first head
 #pragma unroll
-    for (int q = 0; q < RR_ITEMS; q++) {
-      const uint32_t k = q * NT + tid;
-      if (k < clen) {
-        s_k[k] = keys[c + k];
-        if constexpr (TROP) s_w[k] = w[c + k];
-      }
-    }
-    __syncthreads();
-    const uint32_t b = tid * RR_ITEMS;
-    bool head[RR_ITEMS], last[RR_ITEMS];
-    W incl[RR_ITEMS];
-    SegMin<W> run{false, W(0)};
-#pragma unroll
-    for (int j = 0; j < RR_ITEMS; j++) {
-      const uint32_t li = b + j;
-      head[j] = false;
-      last[j] = false;
-      if (li < clen) {
-        const uint64_t gi = c + li;
-        const K kk = s_k[li];
-        head[j] = (gi == s) || (kk != (li > 0 ? s_k[li - 1] : keys[gi - 1]));
-        const uint64_t gn = gi + 1;
-        last[j] = (gn >= e) || (kk != (li + 1 < clen ? s_k[li + 1] : keys[gn]));
-        if constexpr (TROP) {
-          const W wv = s_w[li];
-          if (head[j]) run = SegMin<W>{true, wv};
-          else if (j == 0) run = SegMin<W>{false, wv};  // partial run entering the thread
-          else run = SegMin<W>{run.h, run.m < wv ? run.m : wv};
-          incl[j] = run.m;
-        }
-      }
-    }
-    // Trop: block-wide exclusive segmented scan of the thread aggregates.
-    if constexpr (TROP) {
-      // Items past clen leave run unchanged; an empty thread contributes
-      // the identity {false, +inf}.
-      SegMin<W> agg = (b < clen) ? run : SegMin<W>{false, WAbs<W>::v};
-      SegMin<W> inc = agg;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        SegMin<W> t;
-        t.h = __shfl_up_sync(kFull, inc.h, o);
-        t.m = __shfl_up_sync(kFull, inc.m, o);
-        if (lane >= o) inc = seg_combine(t, inc);
-      }
-      if (lane == 31) s_seg[warp] = inc;
-      __syncthreads();
-      SegMin<W> wpre{false, WAbs<W>::v};
-      for (int q = 0; q < warp; q++) wpre = seg_combine(wpre, s_seg[q]);
-      SegMin<W> ex;
-      ex.h = __shfl_up_sync(kFull, inc.h, 1);
-      ex.m = __shfl_up_sync(kFull, inc.m, 1);
-      if (lane == 0) ex = SegMin<W>{false, WAbs<W>::v};
-      SegMin<W> pre = seg_combine(SegMin<W>{carry_h, carry_h ? carry_m : WAbs<W>::v},
-                                  seg_combine(wpre, ex));
-      // Apply the carry to this thread's items up to its first head.
-#pragma unroll
-      for (int j = 0; j < RR_ITEMS; j++) {
-        if (b + j < clen) {
-          if (head[j]) break;
-          incl[j] = pre.m < incl[j] ? pre.m : incl[j];
-        }
-      }
-      // Carry for the next chunk: the block-inclusive state at the chunk end.
-      SegMin<W> tot{false, WAbs<W>::v};
-      for (int q = 0; q < NT / 32; q++) tot = seg_combine(tot, s_seg[q]);
-      SegMin<W> nc = seg_combine(SegMin<W>{carry_h, carry_h ? carry_m : WAbs<W>::v}, tot);
-      __syncthreads();
-      carry_h = nc.h;
-      carry_m = nc.m;
-    }
-    // Stage the run ends in order.
-    uint32_t mine = 0;
-#pragma unroll
-    for (int j = 0; j < RR_ITEMS; j++) mine += last[j] ? 1u : 0u;
-    uint32_t tot_c;
-    uint32_t at = nout + block_excl_sum<NT>(mine, s_scan, &tot_c);
-#pragma unroll
-    for (int j = 0; j < RR_ITEMS; j++) {
-      if (last[j]) {
-        if (at < RR_TILE) {
-          s_ok[at] = s_k[b + j];
-          if constexpr (TROP) s_ow[at] = incl[j];
-        } else {
-          atomicOr(status, ST_BOUNDS);
-        }
-        at++;
-      }
-    }
-    nout += tot_c;
-    __syncthreads();
-  }
-  if (warp == 0) {
-    const uint64_t ex = warp_lookback(states, tile, (uint64_t)nout, status);
-    if (lane == 0) {
-      s_excl = ex;
-      if (tile == gridDim.x - 1) *d_count = ex + nout;
+  for (int q = 0; q < RR_ITEMS; q++) {
+    const uint32_t k = q * NT + tid;
+    if (k < len) {
+      s_k[k] = keys[t0 + k];
+      if constexpr (TROP) s_w[k] = w[t0 + k];
     }
   }
   __syncthreads();
-  const uint64_t ob = s_excl;
-  const uint32_t lim = nout < RR_TILE ? nout : RR_TILE;
-  for (uint32_t k = tid; k < lim; k += NT) {
-    if (ob + k >= n) {  // more runs than keys: only unsorted input gets here
+  const uint32_t b = tid * RR_ITEMS;
+  bool head[RR_ITEMS], last[RR_ITEMS];
+  W incl[RR_ITEMS];
+  SegMin<W> run{false, W(0)};
+  uint32_t nh = 0;  // heads among this thread's items
+#pragma unroll
+  for (int j = 0; j < RR_ITEMS; j++) {
+    const uint32_t li = b + j;
+    head[j] = false;
+    last[j] = false;
+    incl[j] = W(0);
+    if (li < len) {
+      const uint64_t gi = t0 + li;
+      const K kk = s_k[li];
+      head[j] = (gi == 0) || (kk != (li > 0 ? s_k[li - 1] : keys[gi - 1]));
+      last[j] = (gi + 1 >= n) || (kk != (li + 1 < len ? s_k[li + 1] : keys[gi + 1]));
+      nh += head[j] ? 1u : 0u;
+      if constexpr (TROP) {
+        const W wv = s_w[li];
+        if (head[j]) run = SegMin<W>{true, wv};
+        else if (j == 0) run = SegMin<W>{false, wv};  // partial run entering the thread
+        else run = SegMin<W>{run.h, run.m < wv ? run.m : wv};
+        incl[j] = run.m;
+      }
+    }
+  }
+  if constexpr (TROP) {
+    // Block-wide exclusive segmented min of the thread aggregates; the tile's
+    // first run part starts at the tile (nothing enters from before it).
+    SegMin<W> agg = (b < len) ? run : SegMin<W>{false, WAbs<W>::v};
+    SegMin<W> inc = agg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      SegMin<W> t;
+      t.h = __shfl_up_sync(kFull, inc.h, o);
+      t.m = __shfl_up_sync(kFull, inc.m, o);
+      if (lane >= o) inc = seg_combine(t, inc);
+    }
+    if (lane == 31) s_seg[warp] = inc;
+    __syncthreads();
+    SegMin<W> wpre{false, WAbs<W>::v};
+    for (int q = 0; q < warp; q++) wpre = seg_combine(wpre, s_seg[q]);
+    SegMin<W> ex;
+    ex.h = __shfl_up_sync(kFull, inc.h, 1);
+    ex.m = __shfl_up_sync(kFull, inc.m, 1);
+    if (lane == 0) ex = SegMin<W>{false, WAbs<W>::v};
+    const SegMin<W> pre = seg_combine(wpre, ex);
+#pragma unroll
+    for (int j = 0; j < RR_ITEMS; j++) {
+      if (b + j < len) {
+        if (head[j]) break;
+        incl[j] = pre.m < incl[j] ? pre.m : incl[j];
+      }
+    }
+  }
+  uint32_t tile_nh;
+  uint32_t r = block_excl_sum<NT>(nh, s_scan, &tile_nh);  // heads in the tile before this thread
+#pragma unroll
+  for (int j = 0; j < RR_ITEMS; j++) {
+    const uint32_t li = b + j;
+    if (li >= len) continue;
+    if (head[j]) {
+      s_ok[r] = s_k[li];
+      r++;
+    }
+    if constexpr (TROP) {
+      // item li belongs to the tile's run r - 1, or (r == 0) to the run that
+      // entered the tile from before it
+      const bool tile_end = li + 1 == len;
+      if (last[j] && r > 0) {
+        s_ow[r - 1] = incl[j];  // a run held whole by the tile: written below
+      } else if (last[j] || tile_end) {
+        // the part of a run that crosses a tile boundary: merged into its slot
+        const uint64_t slot = base + r - 1;  // r == 0: base >= 1 (tile 0 starts with a head)
+        if (slot < n) atomic_min_w(&out_w[slot], incl[j]);
+        else atomicOr(status, ST_BOUNDS);
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = tid; k < tile_nh; k += NT) {
+    if (base + k >= n) {
       atomicOr(status, ST_BOUNDS);
       break;
     }
-    out[ob + k] = s_ok[k];
-    if constexpr (TROP) out_w[ob + k] = s_ow[k];
+    out[base + k] = s_ok[k];
+    if constexpr (TROP) {
+      // the tile's last run is written here only if it ends inside the tile
+      // (otherwise its slot is merged by atomicMin from every tile it spans)
+      if (k + 1 < tile_nh || t0 + len >= n || s_k[len - 1] != keys[t0 + len]) out_w[base + k] = s_ow[k];
+    }
   }
 }
 
@@ -921,19 +919,22 @@ void reduce_runs(strata_ctx* ctx, const K* keys, const W* w, uint64_t n, K* out,
     SK_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), ctx->stream));
     return;
   }
-  const uint32_t tiles = (uint32_t)ceil_div(n, RRCfg<K, W, TROP>::TILE);
-  DBuf<uint64_t> states(ctx, 2ull * tiles + 2);
-  uint64_t* bounds = states.p + tiles + 1;  // tiles + 1 entries
-  uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + tiles);
-  SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (tiles + 1), ctx->stream));
-  k_rr_bounds<K><<<(unsigned)ceil_div(tiles + 1, NT), NT, 0, ctx->stream>>>(keys, n, tiles,
-                                                                           RRCfg<K, W, TROP>::TILE, bounds);
-  after_launch(ctx, "k_rr_bounds");
+  constexpr uint32_t TILE = RRCfg<K, W, TROP>::TILE;
+  const uint64_t tiles = ceil_div(n, TILE);
+  DBuf<uint64_t> rank0(ctx, tiles + 1);
+  k_rr_heads<K, RRCfg<K, W, TROP>::ITEMS><<<(unsigned)tiles, NT, 0, ctx->stream>>>(keys, n, rank0.p);
+  after_launch(ctx, "k_rr_heads");
+  scan_tile_sums(ctx, rank0.p, tiles);  // exclusive; rank0[tiles] = number of runs
+  if (TROP && tiles > 1) {
+    k_rr_span<K, W><<<(unsigned)ceil_div(tiles, 256), 256, 0, ctx->stream>>>(keys, n, TILE, tiles, rank0.p, out_w);
+    after_launch(ctx, "k_rr_span");
+  }
   const int kh = kprof_begin(ctx, K_REDUCE_RUNS);
-  k_reduce_runs<K, W, TROP><<<tiles, NT, 0, ctx->stream>>>(keys, w, n, out, out_w, bounds, states.p,
-                                                           counter, d_count, ctx->d_status);
+  k_reduce_runs<K, W, TROP><<<(unsigned)tiles, NT, 0, ctx->stream>>>(keys, w, n, out, out_w, rank0.p,
+                                                                    ctx->d_status);
   kprof_end(ctx, kh, n * (sizeof(K) + (TROP ? sizeof(W) : 0)));  // reads; writes added on read-back
   after_launch(ctx, "k_reduce_runs");
+  SK_CUDA(cudaMemcpyAsync(d_count, rank0.p + tiles, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
 }
 
 template <class K, class W, bool TROP, bool WF, bool WD, bool IP>

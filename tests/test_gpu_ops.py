@@ -117,6 +117,27 @@ def test_project_select_intersect_semijoin(ops):
     assert np.array_equal(kk[:m].cpu().numpy().view(np.uint64), k[~np.isin(c1 << SH, u.astype(np.int64))])
 
 
+def test_reduce_long_runs_across_tiles(ops):
+    """Runs longer than a reduction tile, runs ending exactly at tile ends,
+    tiles without a run head, unsorted weights inside a run and +inf
+    weights: one row per key, the minimum weight (Trop) or the distinct keys
+    (Bool)."""
+    rng = np.random.default_rng(11)
+    lens = [1, 3, 1279, 1280, 1281, 2303, 2304, 2305, 40_000, 1, 1, 7, 100_000, 2, 4608, 1]
+    keys = np.repeat(np.arange(len(lens), dtype=np.uint64) * np.uint64(7) + np.uint64(5), lens)
+    w = rng.integers(-10**12, 10**12, len(keys))
+    w[rng.random(len(keys)) < 0.01] = np.iinfo(np.int64).max  # +inf
+    r = ops.upload(keys, w)
+    red = ops.reduce(r.keys, r.w, r.n)
+    kk, ww = ops.download(red)
+    starts = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    assert np.array_equal(kk, keys[starts])
+    assert np.array_equal(ww, np.minimum.reduceat(w, starts))
+    b = ops.reduce(ops.upload(keys).keys, None, len(keys))
+    assert b.n == len(lens)
+    assert np.array_equal(ops.download(b)[0], keys[starts])
+
+
 def test_reduce_merge_diff_and_aggregate(ops):
     rng = np.random.default_rng(3)
     cand = np.sort(_keys(rng.integers(0, 30, 2000), rng.integers(0, 30, 2000)))
