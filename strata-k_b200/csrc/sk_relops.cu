@@ -490,13 +490,16 @@ __global__ void k_md_bounds(const K* __restrict__ A, uint64_t na, const K* __res
   md_split(A, na, B, nb, d, &splits[2 * t], &splits[2 * t + 1]);
 }
 
-template <class K, class W, bool TROP, bool WRITE_FULL, bool WRITE_DELTA, bool INPLACE>
+// Two passes over the same tiles, reduce-then-scan (no tile waits on
+// another): PASS 0 counts each tile's full-out rows and Δ' rows into
+// tile_full / tile_delta; after their exclusive scan, PASS 1 recomputes the tile
+// and writes its rows at the scanned offsets.
+template <class K, class W, bool TROP, bool WRITE_FULL, bool WRITE_DELTA, bool INPLACE, int PASS>
 __global__ void __launch_bounds__(NT)
     k_merge_diff(const K* __restrict__ A, W* Aw, uint64_t na, const K* __restrict__ B,
                  const W* __restrict__ Bw, uint64_t nb, K* __restrict__ fout, W* __restrict__ fout_w,
                  K* __restrict__ dout, W* __restrict__ dout_w, const uint64_t* __restrict__ splits,
-                 uint64_t* fstates, uint64_t* dstates, uint32_t* counter, uint64_t* d_counts,
-                 uint32_t* status) {
+                 uint64_t* tile_full, uint64_t* tile_delta, uint32_t* status) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   constexpr uint32_t CAP = MD_TILE + 2;
   K* s_a = reinterpret_cast<K*>(s_raw);
@@ -505,11 +508,9 @@ __global__ void __launch_bounds__(NT)
   W* s_bw = s_aw + (TROP ? CAP : 0);
   uint32_t* s_mpre = reinterpret_cast<uint32_t*>(s_bw + (TROP ? CAP : 0));  // CAP + 1
   uint32_t* s_dpre = s_mpre + CAP + 1;                                      // CAP
-  __shared__ uint32_t s_tile;
   __shared__ uint32_t s_scan[NT / 32 + 1];
-  __shared__ uint64_t s_ex[2];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t tile = claim_tile(counter, &s_tile);
+  const int tid = threadIdx.x;
+  const uint32_t tile = blockIdx.x;
   const uint64_t s_r[4] = {splits[2 * tile], splits[2 * tile + 1], splits[2 * tile + 2], splits[2 * tile + 3]};
   const uint64_t i0 = s_r[0], j0 = s_r[1];
   // Impossible for sorted unique inputs; checked so unsorted input cannot
@@ -575,21 +576,15 @@ __global__ void __launch_bounds__(NT)
     if (tid == 0) s_mpre[bcnt] = mtot;
   }
   const uint32_t fcnt = acnt + bcnt - mtot;
-  if (warp == 0) {
-    uint64_t ex = 0;
-    if (WRITE_FULL) ex = warp_lookback(fstates, tile, fcnt, status);
-    if (lane == 0) s_ex[0] = ex;
-  } else if (warp == 1) {
-    uint64_t ex = 0;
-    if (WRITE_DELTA) ex = warp_lookback(dstates, tile, dtot, status);
-    if (lane == 0) s_ex[1] = ex;
+  if constexpr (PASS == 0) {
+    if (tid == 0) {
+      tile_full[tile] = fcnt;
+      tile_delta[tile] = dtot;
+    }
+    return;
   }
-  __syncthreads();
-  const uint64_t fex = s_ex[0], dexg = s_ex[1];
-  if (tile == gridDim.x - 1 && tid == 0) {
-    d_counts[0] = fex + fcnt;
-    d_counts[1] = dexg + dtot;
-  }
+  const uint64_t fex = tile_full[tile], dexg = tile_delta[tile];
+  __syncthreads();  // every thread's s_mpre / s_dpre entries are read below
   // B elements: unmatched -> full_out; delta -> delta out.
 #pragma unroll
   for (int q = 0; q < BI; q++) {
@@ -946,22 +941,31 @@ static void launch_merge(strata_ctx* ctx, const K* full, W* full_w, uint64_t nf,
     return;
   }
   const uint32_t tiles = (uint32_t)ceil_div(nf + nc, MD_TILE);
-  DBuf<uint64_t> states(ctx, 2ull * tiles + 1 + 2ull * (tiles + 1));
-  uint32_t* counter = reinterpret_cast<uint32_t*>(states.p + 2ull * tiles);
-  uint64_t* splits = states.p + 2ull * tiles + 1;
-  SK_CUDA(cudaMemsetAsync(states.p, 0, sizeof(uint64_t) * (2ull * tiles + 1), ctx->stream));
+  // per-tile counts (full, Δ'), each array tiles + 1 long for the scan total;
+  // then the merge-path splits
+  DBuf<uint64_t> buf(ctx, 2ull * (tiles + 1) + 2ull * (tiles + 1));
+  uint64_t* fcount = buf.p;
+  uint64_t* dcount = buf.p + tiles + 1;
+  uint64_t* splits = buf.p + 2ull * (tiles + 1);
   k_md_bounds<K><<<(unsigned)ceil_div(tiles + 1, NT), NT, 0, ctx->stream>>>(full, nf, cand, nc, tiles, splits);
   after_launch(ctx, "k_md_bounds");
   constexpr uint32_t CAP = MD_TILE + 2;
   const size_t smem = 2 * CAP * sizeof(K) + (TROP ? 2 * CAP * sizeof(W) : 0) + (2 * CAP + 1) * sizeof(uint32_t);
-  auto kern = k_merge_diff<K, W, TROP, WF, WD, IP>;
-  SK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  auto count = k_merge_diff<K, W, TROP, WF, WD, IP, 0>;
+  auto write = k_merge_diff<K, W, TROP, WF, WD, IP, 1>;
+  SK_CUDA(cudaFuncSetAttribute(count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SK_CUDA(cudaFuncSetAttribute(write, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int kh = kprof_begin(ctx, K_MERGE_DIFF);
-  kern<<<tiles, NT, smem, ctx->stream>>>(full, full_w, nf, cand, cand_w, nc, fout, fout_w, dout,
-                                         dout_w, splits, states.p, states.p + tiles, counter, d_counts,
-                                         ctx->d_status);
+  count<<<tiles, NT, smem, ctx->stream>>>(full, full_w, nf, cand, cand_w, nc, fout, fout_w, dout, dout_w, splits,
+                                          fcount, dcount, ctx->d_status);
+  scan_tile_sums(ctx, buf.p, tiles, 2);
+  write<<<tiles, NT, smem, ctx->stream>>>(full, full_w, nf, cand, cand_w, nc, fout, fout_w, dout, dout_w, splits,
+                                          fcount, dcount, ctx->d_status);
   kprof_end(ctx, kh, (nf + nc) * (sizeof(K) + (TROP ? sizeof(W) : 0)));  // reads; writes added on read-back
   after_launch(ctx, "k_merge_diff");
+  ctx->launches += 1;  // the counting pass
+  SK_CUDA(cudaMemcpyAsync(d_counts, fcount + tiles, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
+  SK_CUDA(cudaMemcpyAsync(d_counts + 1, dcount + tiles, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
 }
 
 template <class K, class W, bool TROP>
