@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(NT, 4) k_onesweep(const K* __restrict__ kin, K
     st_volatile(&lb[tid], LBB::P | (excl + (LB)cnt));
   }
   s_goff[tid] = binoff[tid] + (uint32_t)excl - s_dstart[tid];
-  __syncthreads();  // s_dstart, s_gbase, warp offsets visible
+  __syncthreads();  // s_dstart, s_goff, warp offsets visible
 
   // Stage keys in digit order (and where each came from).
 #pragma unroll
