@@ -298,7 +298,7 @@ __device__ __forceinline__ SegMin<W> seg_combine(SegMin<W> a, SegMin<W> b) {
 //   scan         exclusive head counts = the output rank of each tile's first run;
 //   k_rr_span    (Trop) the output slot of every run crossing a tile boundary
 //                starts at the absent code;
-//   k_rr_write   each tile stages its heads' keys and the minima of the runs
+//   k_reduce_runs  each tile stages its heads' keys and the minima of the runs
 //                it holds whole, writes them coalesced at its rank, and merges
 //                the part of a boundary-crossing run it holds with atomicMin.
 __device__ __forceinline__ void atomic_min_w(int32_t* p, int32_t v) { atomicMin(p, v); }
