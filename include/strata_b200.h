@@ -481,7 +481,8 @@ strata_status strata_op_min_improve(strata_ctx* ctx, int key_bytes,
 
 /* ⊕-combine a batch of derivations (Relation::combine, store.rs:34-48): from
  * sorted keys with duplicates, one row per key — Bool: the distinct keys;
- * Trop (d_w given): the minimum weight.  *out_n = distinct keys (capacity n). */
+ * Trop (d_w given): the minimum weight.  *out_n = distinct keys (capacity n).
+ * The outputs may not overlap the inputs (STRATA_E_INVALID). */
 strata_status strata_op_reduce(strata_ctx* ctx, int key_bytes, const void* d_keys, const int64_t* d_w, uint64_t n,
     void* d_out, int64_t* d_out_w, uint64_t* out_n);
 

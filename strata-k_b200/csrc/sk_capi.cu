@@ -950,6 +950,16 @@ strata_status strata_op_reduce(strata_ctx* ctx, int key_bytes, const void* d_key
   if (key_bytes != 4 && key_bytes != 8) return bad(ctx, "key_bytes must be 4 or 8");
   if (!out_n || (n && (!d_keys || !d_out || (d_w && !d_out_w)))) return bad(ctx, "NULL argument");
   if (n > sk::kMaxSortN) return bad(ctx, "n is limited to 2^30 - 1 per call");
+  {
+    // tiles write their output while other tiles still read their input
+    auto ov = [](const void* a, uint64_t an, const void* b, uint64_t bn) {
+      const auto x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+      return a && b && an && bn && x < y + bn && y < x + an;
+    };
+    const uint64_t kb = n * (uint64_t)key_bytes, wb = n * 8;
+    if (ov(d_keys, kb, d_out, kb) || ov(d_keys, kb, d_out_w, wb) || ov(d_w, wb, d_out, kb) || ov(d_w, wb, d_out_w, wb))
+      return bad(ctx, "the output buffers overlap the input buffers");
+  }
   if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
   SK_GUARD_BEGIN
   sk::reset_status(ctx);

@@ -136,6 +136,12 @@ def test_reduce_long_runs_across_tiles(ops):
     b = ops.reduce(ops.upload(keys).keys, None, len(keys))
     assert b.n == len(lens)
     assert np.array_equal(ops.download(b)[0], keys[starts])
+    # in place is refused: tiles write while other tiles still read
+    import ctypes as C
+    m = C.c_uint64()
+    rc = ops.lib.strata_op_reduce(ops.eng.ctx, 8, C.c_void_p(r.keys.data_ptr()), None, len(keys),
+                                  C.c_void_p(r.keys.data_ptr()), None, C.byref(m))
+    assert rc == S._lib.E_INVALID
 
 
 def test_reduce_merge_diff_and_aggregate(ops):
