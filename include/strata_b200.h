@@ -490,7 +490,8 @@ strata_status strata_op_reduce(strata_ctx* ctx, int key_bytes, const void* d_key
  * (apply_round, seminaive.rs:183-208): full_out = full ⊕ cand (Bool union;
  * Trop min per key), delta = the keys of cand new to full (Trop: or strictly
  * below full's weight) with their merged values.  Both inputs sorted and
- * unique; capacities n_full + n_cand (full_out) and n_cand (delta). */
+ * unique; capacities n_full + n_cand (full_out) and n_cand (delta); the
+ * outputs may not overlap the inputs (STRATA_E_INVALID). */
 strata_status strata_op_merge_diff(strata_ctx* ctx, int key_bytes, const void* d_full, const int64_t* d_full_w,
     uint64_t n_full, const void* d_cand, const int64_t* d_cand_w, uint64_t n_cand,
     void* d_full_out, int64_t* d_full_out_w, void* d_delta, int64_t* d_delta_w,

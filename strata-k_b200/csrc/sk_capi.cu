@@ -900,6 +900,12 @@ strata_status strata_op_sort(strata_ctx* ctx, int key_bytes, int val_bytes, cons
   SK_GUARD_END(ctx)
 }
 
+// [a, a + an) and [b, b + bn) share a byte (null or empty spans share none).
+static bool spans_overlap(const void* a, uint64_t an, const void* b, uint64_t bn) {
+  const auto x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return a && b && an && bn && x < y + bn && y < x + an;
+}
+
 strata_status strata_op_dedup_diff(strata_ctx* ctx, int key_bytes, const void* d_cand, uint64_t n,
                                    const void* d_full, uint64_t n_full, void* d_out, uint64_t* out_n) {
   if (!ctx) return STRATA_E_INVALID;
@@ -952,12 +958,9 @@ strata_status strata_op_reduce(strata_ctx* ctx, int key_bytes, const void* d_key
   if (n > sk::kMaxSortN) return bad(ctx, "n is limited to 2^30 - 1 per call");
   {
     // tiles write their output while other tiles still read their input
-    auto ov = [](const void* a, uint64_t an, const void* b, uint64_t bn) {
-      const auto x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
-      return a && b && an && bn && x < y + bn && y < x + an;
-    };
     const uint64_t kb = n * (uint64_t)key_bytes, wb = n * 8;
-    if (ov(d_keys, kb, d_out, kb) || ov(d_keys, kb, d_out_w, wb) || ov(d_w, wb, d_out, kb) || ov(d_w, wb, d_out_w, wb))
+    if (spans_overlap(d_keys, kb, d_out, kb) || spans_overlap(d_keys, kb, d_out_w, wb) ||
+        spans_overlap(d_w, wb, d_out, kb) || spans_overlap(d_w, wb, d_out_w, wb))
       return bad(ctx, "the output buffers overlap the input buffers");
   }
   if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
@@ -988,6 +991,18 @@ strata_status strata_op_merge_diff(strata_ctx* ctx, int key_bytes, const void* d
     return bad(ctx, "NULL argument");
   if (trop && ((n_full && !d_full_w) || !d_full_out_w || !d_delta_w)) return bad(ctx, "NULL weight column");
   if (n_full + n_cand > sk::kMaxSortN) return bad(ctx, "n is limited to 2^30 - 1 per call");
+  {
+    // tiles write their output while other tiles still read their input
+    const uint64_t kb = key_bytes, fo = n_full + n_cand;
+    const void* in[4] = {d_full, d_full_w, d_cand, d_cand_w};
+    const uint64_t in_b[4] = {n_full * kb, n_full * 8, n_cand * kb, n_cand * 8};
+    const void* out[4] = {d_full_out, d_full_out_w, d_delta, d_delta_w};
+    const uint64_t out_b[4] = {fo * kb, fo * 8, n_cand * kb, n_cand * 8};
+    for (int a = 0; a < 4; a++)
+      for (int b = 0; b < 4; b++)
+        if (spans_overlap(in[a], in_b[a], out[b], out_b[b]))
+          return bad(ctx, "the output buffers overlap the input buffers");
+  }
   if (set_device(ctx) != STRATA_OK) return STRATA_E_CUDA;
   SK_GUARD_BEGIN
   sk::reset_status(ctx);

@@ -142,6 +142,13 @@ def test_reduce_long_runs_across_tiles(ops):
     rc = ops.lib.strata_op_reduce(ops.eng.ctx, 8, C.c_void_p(r.keys.data_ptr()), None, len(keys),
                                   C.c_void_p(r.keys.data_ptr()), None, C.byref(m))
     assert rc == S._lib.E_INVALID
+    nf, nd = C.c_uint64(), C.c_uint64()
+    rc = ops.lib.strata_op_merge_diff(ops.eng.ctx, 8, C.c_void_p(r.keys.data_ptr()), C.c_void_p(r.w.data_ptr()), 10,
+                                      C.c_void_p(r.keys.data_ptr() + 80), C.c_void_p(r.w.data_ptr() + 80), 10,
+                                      C.c_void_p(r.keys.data_ptr() + 80), C.c_void_p(r.w.data_ptr() + 800),
+                                      C.c_void_p(r.keys.data_ptr() + 1600), C.c_void_p(r.w.data_ptr() + 1600),
+                                      C.byref(nf), C.byref(nd))
+    assert rc == S._lib.E_INVALID  # full_out over cand
 
 
 def test_reduce_merge_diff_and_aggregate(ops):
